@@ -1,0 +1,909 @@
+"""NumPy/SciPy restatement of Rayleigh's timestep hot path (test infrastructure).
+
+Every function cites the reference file:line it restates (paths inside the
+geodynamics/Rayleigh 1.2.0 source tree).  Layouts follow the reference's
+Fortran buffers, written here in C order with the axes reversed:
+
+* ``p1`` (solve configuration, ``Spherical_Buffer.F90`` p1a/p1b):
+  ``[field][lm][re/im][r]`` with the (l, m) pairs l-major, m ascending
+  (``Load_Balance.F90:357-368``).
+* ``s2`` (spectral, one array per m, ``s2a(mp)%data(m:l_max, r, imi, f)``):
+  ``s2[m]`` has shape ``(nf, 2, n_r, l_max - m + 1)``.
+* ``p2`` (hybrid, ``p2a(theta, nrhs, m)`` with nrhs = (r, imi, f)):
+  ``[m][f][ri][r][theta]``.
+* ``p3`` (physical, ``p3a(1:n_phi+2, r, theta, f)``): ``[f][theta][r][n_phi+2]``.
+
+The REAL*16 parts of the reference (Gauss-Legendre roots, P_l^m recurrence)
+are carried in ``numpy.longdouble`` (x86 80-bit), as the reference's own
+NumPy port ``post_processing/spectral_utils.py:577-620,1887-2005`` does.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+import scipy.linalg as sla
+
+LD = np.longdouble
+PI_LD = LD("3.14159265358979323846264338327950288")
+
+# Field indices of the forward-leg buffers, 0-based restatement of
+# Fields.F90:232-335 (hydro, no scalars).
+WVAR, PVAR, TVAR, ZVAR = 0, 1, 2, 3
+# equation ids (Fields.F90:86-88), 0-based
+WEQ, PEQ, TEQ, ZEQ, CEQ, AEQ = 0, 1, 2, 3, 4, 5
+
+
+@dataclass
+class Config:
+    """Problem description (restates the namelist values the path reads)."""
+
+    n_r: int = 48
+    l_max: int = 63
+    n_theta: int = 0                 # 3(l_max+1)/2 when 0 (ProblemSize.F90:431-452)
+    aspect_ratio: float = 0.35
+    shell_depth: float = 1.0
+    rayleigh: float = 1.0e5          # Rayleigh_Number (Ra/Pr is the buoyancy coefficient)
+    ekman: float = 1.0e-3
+    prandtl: float = 1.0
+    magnetic_prandtl: float = 1.0
+    gravity_power: float = 1.0
+    rotation: bool = True
+    magnetism: bool = False
+    momentum_advection: bool = True
+    no_slip_top: bool = True
+    no_slip_bottom: bool = True
+    fix_tvar_top: bool = True
+    fix_tvar_bottom: bool = True
+    t_top: float = 0.0
+    t_bottom: float = 1.0
+    dtdr_top: float = 0.0
+    dtdr_bottom: float = 0.0
+    dt: float = 1.0e-4
+    alpha_implicit: float = 0.5
+
+    def __post_init__(self):
+        if self.n_theta <= 0:
+            self.n_theta = (3 * (self.l_max + 1)) // 2
+        if self.n_theta % 2:
+            raise ValueError("n_theta must be even")
+        if self.n_r % 2:
+            raise ValueError("n_r must be even (single Chebyshev domain, parity split)")
+
+    @property
+    def n_phi(self):
+        return 2 * self.n_theta
+
+    @property
+    def n_m(self):
+        return self.l_max + 1
+
+
+# ---------------------------------------------------------------------------
+# Horizontal grid: Gauss-Legendre nodes and P_l^m tables
+# ---------------------------------------------------------------------------
+
+def _nth_legendre(x, n):
+    """Legendre_Polynomials.F90:377-393 (nth_legendre)."""
+    pn = LD(1)
+    pm1 = LD(0)
+    for j in range(1, n + 1):
+        pm2 = pm1
+        pm1 = pn
+        pn = ((LD(2 * j) - 1) * x * pm1 - (LD(j) - 1) * pm2) / LD(j)
+    dpn = n * (x * pn - pm1) / (x * x - 1)
+    return pn, dpn
+
+
+def gauss_legendre(n, eps="3e-14"):
+    """Find_Colocation (Legendre_Polynomials.F90:332-373): nodes ascending in (-1, 1).
+
+    ``eps`` is the Newton stopping tolerance (3e-14 in the Fortran; the
+    reference's NumPy port uses 3e-15).  The weight of each pass uses the
+    derivative at the pre-update root, as the reference does, so the weights
+    carry an O(eps) relative difference between the two.
+    """
+    x = np.zeros(n, dtype=LD)
+    w = np.zeros(n, dtype=LD)
+    eps = LD(eps)
+    for i in range(1, (n + 1) // 2 + 1):
+        root = np.cos(PI_LD * (LD(i) - LD("0.25")) / (LD(n) + LD("0.5")))
+        while True:
+            pn, dpn = _nth_legendre(root, n)
+            new = root - pn / dpn
+            delta = abs(root - new)
+            root = new
+            x[i - 1] = -root
+            x[n - i] = root
+            w[i - 1] = 2 / ((1 - root * root) * dpn * dpn)
+            w[n - i] = w[i - 1]
+            if delta <= eps:
+                break
+    return x, w
+
+
+class Horizontal:
+    """Gauss-Legendre grid plus parity-split P_l^m tables for one (l_max, n_theta)."""
+
+    def __init__(self, l_max, n_theta, eps="3e-14"):
+        self.l_max = l_max
+        self.n_theta = n_theta
+        self.n_phi = 2 * n_theta
+        self.n_m = l_max + 1
+        xq, wq = gauss_legendre(n_theta, eps)
+        self.xq, self.wq = xq, wq
+        self.costheta = xq.astype(np.float64)           # ProblemSize.F90:490
+        self.sintheta = np.sqrt(1.0 - self.costheta ** 2)
+        self.csctheta = 1.0 / self.sintheta
+        self.cottheta = self.costheta / self.sintheta
+        nth2 = n_theta // 2
+        self.p_even, self.p_odd, self.ip_even, self.ip_odd = [], [], [], []
+        self.l_even, self.l_odd = [], []
+        x = xq[:nth2]
+        renorm = 2 * PI_LD * wq[:nth2]
+        for m in range(self.n_m):
+            nl = l_max - m + 1
+            pq = np.zeros((nl, nth2), dtype=LD)
+            # closed form for l = m (Legendre_Polynomials.F90:190-212)
+            ratio = LD(1)
+            for i in range(1, m + 1):
+                ratio = ratio * np.sqrt((LD(i) - LD("0.5")) / LD(i))
+            amp = np.sqrt((LD(m) + LD("0.5")) / (2 * PI_LD)) * ratio
+            tmp = 1 - x * x
+            if m % 2 == 1:
+                pq[0] = -amp * tmp ** (LD(m // 2) + LD("0.5"))
+            else:
+                pq[0] = amp * tmp ** LD(m // 2)
+            if m < l_max:
+                pq[1] = pq[0] * x * np.sqrt(LD(2 * m + 3))
+            # three-term recurrence (Legendre_Polynomials.F90:215-226)
+            for l in range(m + 2, l_max + 1):
+                a = (LD(l - 1) ** 2 - LD(m * m)) / (4 * LD(l - 1) ** 2 - 1)
+                a = np.sqrt(a)
+                t = pq[l - 1 - m] * x - a * pq[l - 2 - m]
+                b = (4 * LD(l) * LD(l) - 1) / (LD(l * l) - LD(m * m))
+                pq[l - m] = t * np.sqrt(b)
+            # the normalisations are double-precision literals stored into REAL*16 (:270-276)
+            if m == 0:
+                pts = LD(np.float64(1.0) / (2.0 * n_theta))
+                stp = LD(1)
+            else:
+                pts = LD(np.float64(1.0) / n_theta)
+                stp = LD("0.5")
+            ev = pq[0::2]
+            od = pq[1::2]
+            self.l_even.append(np.arange(m, l_max + 1, 2))
+            self.l_odd.append(np.arange(m + 1, l_max + 1, 2))
+            self.p_even.append((ev * stp).astype(np.float64))
+            self.p_odd.append((od * stp).astype(np.float64))
+            self.ip_even.append(((ev * renorm) * pts).T.astype(np.float64).copy())
+            self.ip_odd.append(((od * renorm) * pts).T.astype(np.float64).copy())
+        # angular derivative coefficients (Spectral_Derivatives.F90:49-83)
+        self.dcoef, self.sdcoef = [], []
+        for m in range(self.n_m):
+            ls = np.arange(m, l_max + 1, dtype=np.float64)
+            num = (ls + m) * (ls - m)
+            den = (2 * ls + 1) * (2 * ls - 1)
+            c1 = np.sqrt(num / den)
+            num2 = (ls + 1 + m) * (ls + 1 - m)
+            den2 = (2 * ls + 1) * (2 * ls + 3)
+            c2 = np.sqrt(num2 / den2)
+            self.dcoef.append(((ls - 1) * c1, -(ls + 2) * c2))
+            self.sdcoef.append(((ls + 1) * c1, -ls * c2))
+
+    # ----- Legendre transforms (Legendre_Transforms.F90:968-1175) -----
+    def s2p(self, s2):
+        """StP_4d_dgp2: spectral s2[m] (nf,2,nr,nl) -> p2 [m][nf][2][nr][theta]."""
+        nth, nth2 = self.n_theta, self.n_theta // 2
+        out = []
+        for m in range(self.n_m):
+            a = s2[m]
+            nf, _, nr, nl = a.shape
+            a2 = a.reshape(-1, nl).T           # (nl, nrhs)
+            o = np.zeros((nth, a2.shape[1]))
+            if len(self.l_even[m]):
+                te = self.p_even[m].T @ a2[0::2]       # (nth2, nrhs) :1028
+                o[:nth2] = te
+                o[nth - 1:nth2 - 1:-1] = te             # reflect about the equator :1030-1036
+            if len(self.l_odd[m]):
+                to = self.p_odd[m].T @ a2[1::2]         # :1058
+                o[:nth2] += to
+                o[nth - 1:nth2 - 1:-1] -= to            # :1059-1064
+            out.append(o.T.reshape(nf, 2, nr, nth))
+        return out
+
+    def p2s(self, p2):
+        """PtS_4d_dgpv3: p2 [m](nf,2,nr,theta) -> s2[m] (nf,2,nr,nl)."""
+        nth, nth2 = self.n_theta, self.n_theta // 2
+        out = []
+        for m in range(self.n_m):
+            d = p2[m]
+            nf, _, nr, _ = d.shape
+            d2 = d.reshape(-1, nth).T          # (nth, nrhs)
+            south = d2[:nth2]
+            north = d2[nth - 1:nth2 - 1:-1]
+            fe = south + north                 # :1109-1122
+            fo = south - north
+            nl = self.l_max - m + 1
+            o = np.zeros((nl, d2.shape[1]))
+            if len(self.l_even[m]):
+                o[0::2] = self.ip_even[m].T @ fe   # :1130
+            if len(self.l_odd[m]):
+                o[1::2] = self.ip_odd[m].T @ fo    # :1150
+            out.append(o.T.reshape(nf, 2, nr, nl))
+        return out
+
+    # ----- angular derivatives in (l, m) space -----
+    def d_by_dtheta(self, a, m):
+        """sin(theta) d/dtheta (Spectral_Derivatives.F90:329-350); a[..., l-m]."""
+        return self._ell_couple(a, m, self.dcoef[m])
+
+    def d_by_sdtheta(self, a, m):
+        """(1/sin) d(sin^2 .)/dtheta (Spectral_Derivatives.F90:381-401)."""
+        return self._ell_couple(a, m, self.sdcoef[m])
+
+    def _ell_couple(self, a, m, coef):
+        c1, c2 = coef
+        out = np.zeros_like(a)
+        if m == self.l_max:
+            return out
+        # interior l = m+1 .. lmax-1
+        out[..., 1:-1] = a[..., 0:-2] * c1[1:-1] + a[..., 2:] * c2[1:-1]
+        out[..., 0] = a[..., 1] * c2[0]
+        out[..., -1] = a[..., -2] * c1[-1]
+        return out
+
+    @staticmethod
+    def d_by_dphi(a, m):
+        """d/dphi on (re, im) pairs (Spectral_Derivatives.F90:495-509); a[..., ri, r, l]."""
+        out = np.empty_like(a)
+        out[..., 0, :, :] = -m * a[..., 1, :, :]
+        out[..., 1, :, :] = m * a[..., 0, :, :]
+        return out
+
+
+# ---------------------------------------------------------------------------
+# FFT in phi (Fourier_Transform.F90:100-183): unnormalised, packed n+2 layout
+# ---------------------------------------------------------------------------
+
+def fft_c2r(p3, n_phi):
+    """c2r_ip4D_fftw: last axis (n_phi+2 packed re/im) -> n_phi real values (unnormalised)."""
+    c = p3[..., 0::2] + 1j * p3[..., 1::2]
+    y = np.fft.irfft(c, n=n_phi, axis=-1) * n_phi
+    out = np.zeros_like(p3)
+    out[..., :n_phi] = y
+    return out
+
+
+def fft_r2c(p3, n_phi):
+    """r2c_ip4D_fftw: first n_phi real values -> packed spectrum (unnormalised)."""
+    c = np.fft.rfft(p3[..., :n_phi], axis=-1)
+    out = np.empty(p3.shape[:-1] + (n_phi + 2,))
+    out[..., 0::2] = c.real
+    out[..., 1::2] = c.imag
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Chebyshev grid (Chebyshev_Polynomials.F90:65-644), single domain
+# ---------------------------------------------------------------------------
+
+class Chebyshev:
+    def __init__(self, n, rmin, rmax, dmax=3):
+        self.n = n
+        # Gen_Colocation_Points: zeros of T_N, theta accumulated by repeated addition (:233-244)
+        dth = math.pi / n
+        arg = dth * 0.5
+        theta = np.zeros(n)
+        for i in range(n):
+            theta[i] = arg
+            arg = arg + dth
+        self.theta = theta
+        x = np.cos(theta)
+        self.x = x
+        # Gen_Tn (:251-297)
+        k = np.arange(n)
+        cheby = np.cos(k[None, :] * theta[:, None])      # cheby(r, i) = cos((i-1) theta_r)
+        n_odd = n // 2
+        n_even = n_odd + n % 2
+        self.n_even, self.n_odd = n_even, n_odd
+        self.cheby_even = cheby[:n_even, 0::2].copy()     # (n_x, n_even)
+        self.cheby_odd = cheby[:n_even, 1::2].copy()
+        # Gen_Tn_Deriv_Arrays (:299-351)
+        alpha = np.zeros((n, n))
+        alpha[n - 2, n - 1] = 2.0 * (n - 1)
+        for kk in range(n - 3, -1, -1):                   # Fortran k = N-2 .. 1
+            alpha[kk, kk + 1] = 2.0 * (kk + 1)
+            alpha[kk, :] = alpha[kk, :] + alpha[kk + 2, :]
+        d = np.zeros((dmax + 1, n, n))
+        d[0] = cheby.copy()
+        d[0][:, 0] -= 0.5                                  # -c_0/2 of from_spectral (:332-333)
+        for dd in range(1, dmax + 1):
+            d[dd] = d[dd - 1] @ alpha
+        # grid and scalings (Initialize_Cheby_Grid :168-200); bounds reversed: r(1) = rmax
+        xmin, xmax = x[n - 1], x[0]
+        delta = rmax - rmin
+        scaling = delta / (xmax - xmin)
+        self.radius = (x - xmin) * scaling + rmin
+        inv = 1.0 / scaling
+        for dd in range(1, dmax + 1):
+            d[dd] = d[dd] * inv ** dd
+        self.dcheby = d                                    # dcheby[d][r, n]
+        self.deriv_scaling = inv
+        self.rda = (2 * n) // 3 + 1                        # 1-based dealias index (:128)
+
+    def dealias(self, c):
+        """dealias_buffer4d (:353-374): zero coefficients rda..N (1-based) along the last axis."""
+        c = c.copy()
+        c[..., self.rda - 1:] = 0.0
+        return c
+
+    def to_spectral(self, f):
+        """To_Spectral4D (:375-448): grid values (last axis r) -> coefficients."""
+        n, nx = self.n, self.n_even
+        alpha = 2.0 / n
+        fe = f[..., :nx] + f[..., n - 1:n - 1 - nx:-1]
+        fo = f[..., :nx] - f[..., n - 1:n - 1 - nx:-1]
+        c = np.empty_like(f)
+        c[..., 0::2] = alpha * (fe @ self.cheby_even)
+        c[..., 1::2] = alpha * (fo @ self.cheby_odd)
+        return c
+
+    def from_spectral(self, c):
+        """From_Spectral4D (:450-558): coefficients -> grid values (even N)."""
+        n, nx = self.n, self.n_even
+        fe = c[..., 0::2] @ self.cheby_even.T
+        fo = c[..., 1::2] @ self.cheby_odd.T
+        f = np.empty_like(c)
+        f[..., :nx] = fe
+        f[..., n - 1:n - 1 - nx:-1] = fe
+        f[..., :nx] += fo
+        f[..., n - 1:n - 1 - nx:-1] -= fo
+        return f - c[..., 0:1] / 2.0
+
+    def deriv(self, c, order):
+        """Cheby_Deriv_Buffer_4D (:560-644): coefficient recursion, then scaling**order."""
+        n = self.n
+        cur = c
+        for _ in range(order):
+            d = np.zeros_like(cur)
+            d[..., n - 2] = 2.0 * (n - 1) * cur[..., n - 1]
+            for i in range(n - 3, -1, -1):
+                d[..., i] = d[..., i + 2] + 2.0 * (i + 1) * cur[..., i + 1]
+            cur = d
+        return cur * self.deriv_scaling ** order
+
+
+# ---------------------------------------------------------------------------
+# The time stepper
+# ---------------------------------------------------------------------------
+
+def lm_pairs(l_max):
+    """(l, m) ordering of the solve configuration (Load_Balance.F90:357-368)."""
+    ls, ms = [], []
+    for l in range(l_max + 1):
+        for m in range(l + 1):
+            ls.append(l)
+            ms.append(m)
+    return np.array(ls), np.array(ms)
+
+
+class Oracle:
+    """Boussinesq (reference_type 1) rotating convection, hydro, single Chebyshev domain."""
+
+    NF1A = 8     # W P T Z W' T' Z' W''  (Fields.F90:244-252, aliases :317-335)
+    NF2A = 12
+    NFB = 4
+
+    def __init__(self, cfg: Config, horizontal: Horizontal | None = None):
+        if cfg.magnetism:
+            raise NotImplementedError("oracle covers the hydrodynamic equation set")
+        self.cfg = cfg
+        self.h = horizontal if horizontal is not None else Horizontal(cfg.l_max, cfg.n_theta)
+        rmax = cfg.shell_depth / (1.0 - cfg.aspect_ratio)
+        rmin = rmax * cfg.aspect_ratio
+        self.rmin, self.rmax = rmin, rmax
+        self.cg = Chebyshev(cfg.n_r, rmin, rmax)
+        r = self.cg.radius
+        self.radius = r
+        nr = cfg.n_r
+        # Delta_r (ProblemSize.F90:541-549)
+        dr = np.empty(nr)
+        dr[0] = r[0] - r[1]
+        dr[1:] = r[:-1] - r[1:]
+        self.delta_r = dr
+        # Constant_Reference (PDE_Coefficients.F90:335-435)
+        self.density = np.ones(nr)
+        self.dlnrho = np.zeros(nr)
+        self.buoy = (cfg.rayleigh / cfg.prandtl) * (r / r[0]) ** cfg.gravity_power
+        pscaling = 1.0 / cfg.ekman if cfg.rotation else 1.0
+        self.dpdr_w_term = self.density * pscaling
+        self.pressure_dwdr_term = -1.0 * self.density * pscaling
+        self.coriolis = 2.0 / cfg.ekman
+        self.nu = np.ones(nr)
+        self.kappa = np.full(nr, 1.0 / cfg.prandtl)
+        r_out, r_in = r[0], r[-1]
+        pref = r_out * r_in / (r_in - r_out)
+        self.s_conductive = pref * (1.0 / r_out - 1.0 / r)
+        # transport-derived diffusion coefficients are zero for constant nu, kappa, rho
+        self.ls, self.ms = lm_pairs(cfg.l_max)
+        self.n_lm = len(self.ls)
+        self.l_start = np.searchsorted(self.ls, np.arange(cfg.l_max + 1))
+        # index maps between l-major lm and per-m blocks
+        self.old_dt = cfg.dt
+        self.dt = cfg.dt
+        self.iteration = 1
+        self._build_linear()
+        self.last_cfl = 0.0
+
+    # ----- linear system (Sphere_Linear_Terms.F90:79-537, Linear_Solve.F90:494-539) -----
+    def _build_linear(self):
+        cfg, nr, cg = self.cfg, self.cfg.n_r, self.cg
+        r = self.radius
+        dt, a = self.dt, cfg.alpha_implicit
+        lf = -dt * a
+        rf = dt * (1.0 - a)
+        D = cg.dcheby
+        rda = cg.rda
+        self.coefs = []     # per l: dict (eq, var, d) -> vector(r)
+        self.lu_wpt = []
+        self.lu_z = []
+        self.mat_wpt = []
+        self.mat_z = []
+        over_r2 = 1.0 / r ** 2
+        for l in range(cfg.l_max + 1):
+            coefs = {}
+            A = np.zeros((3 * nr, 3 * nr))
+            Z = np.zeros((nr, nr))
+            blk = {WEQ: 0, PEQ: nr, TEQ: 2 * nr, WVAR: 0, PVAR: nr, TVAR: 2 * nr}
+
+            def add(eq, var, d, amp, static=False, mat=None, rb=None, cb=None):
+                key = (eq, var, d)
+                coefs[key] = coefs.get(key, 0.0) + (amp if static else amp * rf)
+                fac = amp if static else amp * lf
+                mm = A if mat is None else mat
+                r0 = blk[eq] if rb is None else rb
+                c0 = blk[var] if cb is None else cb
+                mm[r0:r0 + nr, c0:c0 + nr] += fac[:, None] * D[d]      # Load_Interior_Rows_Cheby
+
+            ones = np.ones(nr)
+            H = -l * (l + 1) * over_r2
+            if l == 0:
+                add(TEQ, TVAR, 0, ones, static=True)
+                add(TEQ, TVAR, 1, 2.0 / r * self.kappa)
+                add(TEQ, TVAR, 2, 1.0 * self.kappa)
+                add(TEQ, TVAR, 1, np.zeros(nr))            # S_Diffusion_Coefs_1 = 0
+                add(PEQ, TVAR, 0, -self.buoy, static=True)
+                add(PEQ, PVAR, 1, self.dpdr_w_term, static=True)
+                add(WEQ, WVAR, 0, ones, static=True)
+            else:
+                add(WEQ, TVAR, 0, -self.buoy / H)
+                add(WEQ, PVAR, 1, self.dpdr_w_term / H)
+                add(WEQ, WVAR, 0, ones, static=True)
+                add(WEQ, WVAR, 0, H * self.nu)
+                add(WEQ, WVAR, 2, self.nu)
+                add(WEQ, WVAR, 0, np.zeros(nr))            # W_Diffusion_Coefs_0
+                add(WEQ, WVAR, 1, np.zeros(nr))            # W_Diffusion_Coefs_1
+                add(PEQ, PVAR, 0, self.pressure_dwdr_term)
+                add(PEQ, WVAR, 1, ones, static=True)
+                add(PEQ, WVAR, 0, -self.nu * H * 2.0 / r)
+                add(PEQ, WVAR, 1, H * self.nu)
+                add(PEQ, WVAR, 3, self.nu)
+                add(PEQ, WVAR, 0, np.zeros(nr))            # dW_Diffusion_Coefs_0*H
+                add(PEQ, WVAR, 1, np.zeros(nr))
+                add(PEQ, WVAR, 2, np.zeros(nr))
+                add(TEQ, TVAR, 0, ones, static=True)
+                add(TEQ, TVAR, 0, H * self.kappa)
+                add(TEQ, TVAR, 1, 2.0 / r * self.kappa)
+                add(TEQ, TVAR, 2, self.kappa)
+                add(TEQ, TVAR, 1, np.zeros(nr))
+                add(ZEQ, ZVAR, 0, ones, static=True, mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 0, H * self.nu, mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 2, self.nu, mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 0, np.zeros(nr), mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 1, np.zeros(nr), mat=Z, rb=0, cb=0)
+            # Set_Boundary_Conditions (Sphere_Linear_Terms.F90:539-1100)
+            def bc(mat, row, col0, d, amp):
+                # Load_Single_Row_Cheby (Linear_Solve.F90:1483-1522): dealiased columns only
+                mat[row, col0:col0 + rda - 1] += amp * D[d][row % nr, :rda - 1]
+
+            top, bot = 0, nr - 1
+            if l == 0:
+                A[nr + top, :] = 0.0
+                A[2 * nr + top, :] = 0.0
+                A[2 * nr + bot, :] = 0.0
+                if cfg.fix_tvar_top:
+                    bc(A, 2 * nr + top, 2 * nr, 0, 1.0)
+                else:
+                    bc(A, 2 * nr + top, 2 * nr, 1, 1.0)
+                if cfg.fix_tvar_bottom:
+                    bc(A, 2 * nr + bot, 2 * nr, 0, 1.0)
+                else:
+                    bc(A, 2 * nr + bot, 2 * nr, 1, 1.0)
+                bc(A, nr + top, nr, 0, 1.0)                  # pressure node at the top
+            else:
+                for rb in (0, nr, 2 * nr):
+                    A[rb + top, :] = 0.0
+                    A[rb + bot, :] = 0.0
+                Z[top, :] = 0.0
+                Z[bot, :] = 0.0
+                if cfg.fix_tvar_top:
+                    bc(A, 2 * nr + top, 2 * nr, 0, 1.0)
+                else:
+                    bc(A, 2 * nr + top, 2 * nr, 1, 1.0)
+                if cfg.fix_tvar_bottom:
+                    bc(A, 2 * nr + bot, 2 * nr, 0, 1.0)
+                else:
+                    bc(A, 2 * nr + bot, 2 * nr, 1, 1.0)
+                bc(A, top, 0, 0, 1.0)                       # impenetrable
+                bc(A, bot, 0, 0, 1.0)
+                if cfg.no_slip_top:
+                    bc(Z, top, 0, 0, 1.0)
+                    bc(A, nr + top, 0, 1, 1.0)
+                else:
+                    samp = -(2.0 / r[top] + self.dlnrho[top])
+                    bc(A, nr + top, 0, 2, 1.0)
+                    bc(A, nr + top, 0, 1, samp)
+                    bc(Z, top, 0, 1, 1.0)
+                    bc(Z, top, 0, 0, samp)
+                if cfg.no_slip_bottom:
+                    bc(A, nr + bot, 0, 1, 1.0)
+                    bc(Z, bot, 0, 0, 1.0)
+                else:
+                    samp = -(2.0 / r[bot] + self.dlnrho[bot])
+                    bc(A, nr + bot, 0, 2, 1.0)
+                    bc(A, nr + bot, 0, 1, samp)
+                    bc(Z, bot, 0, 1, 1.0)
+                    bc(Z, bot, 0, 0, samp)
+            self.coefs.append(coefs)
+            self.mat_wpt.append(A)
+            self.mat_z.append(Z)
+            # LU_Decompose_full -> DGETRF (Linear_Solve.F90:1028-1036)
+            self.lu_wpt.append(sla.lu_factor(A, check_finite=False))
+            self.lu_z.append(sla.lu_factor(Z, check_finite=False) if l > 0 else None)
+        # bc_values (BoundaryConditions.F90:364-402): only l=0 T rows carry values
+        self.bc_t = (cfg.t_top * math.sqrt(4 * math.pi) if cfg.fix_tvar_top else cfg.dtdr_top * math.sqrt(4 * math.pi),
+                     cfg.t_bottom * math.sqrt(4 * math.pi) if cfg.fix_tvar_bottom else cfg.dtdr_bottom * math.sqrt(4 * math.pi))
+
+    def set_dt(self, dt):
+        """Reset_Linear_Equations (Sphere_Linear_Terms.F90:67-76) for a new dt."""
+        self.dt = dt
+        self._build_linear()
+
+    # ----- state -----
+    def init_state(self, wpt_coeffs, z_coeffs, ab=None):
+        """State in the equation-set RHS layout: wpt[lm, ri, 3nr], z[lm, ri, nr] (Chebyshev coefficients)."""
+        nr = self.cfg.n_r
+        self.rhs_wpt = np.array(wpt_coeffs, dtype=np.float64).reshape(self.n_lm, 2, 3 * nr)
+        self.rhs_z = np.array(z_coeffs, dtype=np.float64).reshape(self.n_lm, 2, nr)
+        self.ab = np.zeros((self.NFB, self.n_lm, 2, nr)) if ab is None else np.array(ab, dtype=np.float64)
+
+    def get_all_rhs(self):
+        """Get_All_RHS (Linear_Solve.F90:691-711) -> p1 [f][lm][ri][r] for W P T Z."""
+        nr = self.cfg.n_r
+        p = np.empty((4, self.n_lm, 2, nr))
+        p[WVAR] = self.rhs_wpt[:, :, 0:nr]
+        p[PVAR] = self.rhs_wpt[:, :, nr:2 * nr]
+        p[TVAR] = self.rhs_wpt[:, :, 2 * nr:3 * nr]
+        p[ZVAR] = self.rhs_z
+        return p
+
+    def _coef(self, l, eq, var, d):
+        return self.coefs[l].get((eq, var, d))
+
+    def _add_derivative(self, addto, eq, var, d, dfield):
+        """Add_Derivative (Linear_Solve.F90:758-796): addto[eq] += coef(r) * dfield per l block."""
+        for l in range(self.cfg.l_max + 1):
+            c = self._coef(l, eq, var, d)
+            if c is None:
+                continue
+            s, e = self.l_start[l], self.l_start[l] + l + 1
+            addto[eq, s:e] += dfield[s:e] * c
+
+    # ----- the five stages of one step (Sphere_Driver.F90:305-328) -----
+    def post_solve(self):
+        """Sphere_Spectral_Space.F90:178-413 (Chebyshev branch), ending with Transpose_1a2a."""
+        cg = self.cg
+        if self.iteration == 1:
+            self.new_ab, self.old_ab = self.dt, 0.0
+        else:
+            self.new_ab = 0.5 * self.dt * (2 + self.dt / self.old_dt)
+            self.old_ab = -0.5 * self.dt ** 2 / self.old_dt
+        p1b = self.ab * self.old_ab
+        c = cg.dealias(self.get_all_rhs())                    # :217-221
+        W, P, T, Z = c[WVAR], c[PVAR], c[TVAR], c[ZVAR]
+        d3w = cg.deriv(W, 3)
+        dw = cg.deriv(W, 1)
+        d2w = cg.deriv(W, 2)
+        dp = cg.deriv(P, 1)
+        d2t = cg.deriv(T, 2)
+        dt_ = cg.deriv(T, 1)
+        d2z = cg.deriv(Z, 2)
+        dz = cg.deriv(Z, 1)
+        ctemp = cg.from_spectral(cg.dealias(np.stack([d3w, dp, d2t, d2z])))   # :277-283
+        self._add_derivative(p1b, PEQ, WVAR, 3, ctemp[0])
+        self._add_derivative(p1b, WEQ, PVAR, 1, ctemp[1])
+        self._add_derivative(p1b, TEQ, TVAR, 2, ctemp[2])
+        self._add_derivative(p1b, ZEQ, ZVAR, 2, ctemp[3])
+        g = cg.from_spectral(cg.dealias(np.stack([W, P, T, Z, dw, dt_, dz, d2w])))  # :301-309
+        Wg, Pg, Tg, Zg, dWg, dTg, dZg, d2Wg = g
+        self._add_derivative(p1b, PEQ, WVAR, 0, Wg)
+        self._add_derivative(p1b, PEQ, WVAR, 1, dWg)
+        self._add_derivative(p1b, PEQ, WVAR, 2, d2Wg)
+        self._add_derivative(p1b, WEQ, WVAR, 0, Wg)
+        self._add_derivative(p1b, WEQ, WVAR, 1, dWg)
+        self._add_derivative(p1b, WEQ, WVAR, 2, d2Wg)
+        self._add_derivative(p1b, PEQ, PVAR, 0, Pg)
+        self._add_derivative(p1b, TEQ, TVAR, 1, dTg)
+        self._add_derivative(p1b, TEQ, TVAR, 0, Tg)
+        self._add_derivative(p1b, WEQ, TVAR, 0, Tg)
+        self._add_derivative(p1b, ZEQ, ZVAR, 0, Zg)
+        self._add_derivative(p1b, ZEQ, ZVAR, 1, dZg)
+        self._set_all_rhs(p1b)                                  # :391
+        return g                                                # p1a grid fields (8)
+
+    def _set_all_rhs(self, p1b):
+        nr = self.cfg.n_r
+        self.rhs_wpt[:, :, 0:nr] = p1b[WEQ]
+        self.rhs_wpt[:, :, nr:2 * nr] = p1b[PEQ]
+        self.rhs_wpt[:, :, 2 * nr:3 * nr] = p1b[TEQ]
+        self.rhs_z[:] = p1b[ZEQ]
+
+    def transpose_1a2a(self, p1):
+        """Transpose_1a2a (Spherical_Buffer.F90:849-949): p1[f][lm][ri][r] -> s2[m](f,2,r,l)."""
+        nf = p1.shape[0]
+        L = self.cfg.l_max
+        s2 = []
+        for m in range(L + 1):
+            idx = self.l_start[m:] + m            # lm index of (l, m) for l = m..L
+            s2.append(np.ascontiguousarray(p1[:, idx].transpose(0, 2, 3, 1)))
+        return s2
+
+    def transpose_2b1b(self, s2):
+        """Transpose_2b1b (Spherical_Buffer.F90:705-847): s2[m](f,2,r,l) -> p1[f][lm][ri][r]."""
+        nf = s2[0].shape[0]
+        L = self.cfg.l_max
+        p1 = np.empty((nf, self.n_lm, 2, self.cfg.n_r))
+        for m in range(L + 1):
+            idx = self.l_start[m:] + m
+            p1[:, idx] = s2[m].transpose(0, 3, 1, 2)
+        return p1
+
+    def rlm_spacea(self, s2):
+        """Sphere_Hybrid_Space.F90:64-125 (hydro): 8 fields -> 12 fields, then StP."""
+        h, L = self.h, self.cfg.l_max
+        r = self.radius
+        over_rhorsq = (1.0 / r ** 2 / self.density)[:, None]
+        over_rhor = (1.0 / r / self.density)[:, None]
+        drho = (self.dlnrho + 1.0 / r)[:, None]
+        two_over_r = (2.0 / r)[:, None]
+        out = []
+        for m in range(L + 1):
+            a = s2[m].copy()
+            a[..., -1] = 0.0                                          # zero l_max (:73-75)
+            ls = np.arange(m, L + 1, dtype=np.float64)
+            llp1 = ls * (ls + 1)
+            W, P, T, Z = a[0], a[1], a[2], a[3]
+            dW, dT, dZ, d2W = a[4], a[5], a[6], a[7]
+            b = np.zeros((12,) + W.shape)
+            vr = llp1 * W * over_rhorsq                               # Velocity_Components :246-248
+            vt = (h.d_by_dtheta(dW, m) + h.d_by_dphi(Z[None], m)[0]) * over_rhor
+            vp = (h.d_by_dphi(dW[None], m)[0] - h.d_by_dtheta(Z, m)) * over_rhor
+            dvtdr = (h.d_by_dtheta(d2W, m) + h.d_by_dphi(dZ[None], m)[0]) * over_rhor
+            dvtdr = dvtdr - vt * drho                                  # :295-297
+            dvpdr = (h.d_by_dphi(d2W[None], m)[0] - h.d_by_dtheta(dZ, m)) * over_rhor
+            dvpdr = dvpdr - vp * drho
+            dvrdr = llp1 * dW * over_rhorsq
+            dvrdr = dvrdr - vr * two_over_r
+            dvrdr = dvrdr - vr * self.dlnrho[:, None]
+            dvrdt = h.d_by_dtheta(vr, m)
+            omr = llp1 * Z * over_rhorsq
+            dtdt = h.d_by_dtheta(T, m)
+            b[0] = vr            # vr   (wvar)
+            b[1] = P             # pvar
+            b[2] = T             # tvar
+            b[3] = omr           # zvar -> omega_r
+            b[4] = dvrdr         # dwdr slot
+            b[5] = dT            # dtdr
+            b[6] = dvrdt         # dzdr slot
+            b[7] = dtdt          # d2wdr2 slot
+            b[8] = vt
+            b[9] = vp
+            b[10] = dvtdr
+            b[11] = dvpdr
+            b[..., -1] = 0.0                                          # :100-102
+            out.append(b)
+        return out
+
+    def physical_space(self, p3):
+        """Sphere_Physical_Space.F90:98-224 (hydro): p3a (18 fields) -> p3b (4 fields) + CFL."""
+        cfg, h = self.cfg, self.h
+        nphi = cfg.n_phi
+        L = cfg.l_max
+        # Phi_Derivatives (:745-759) in packed m-space
+        mvec = np.repeat(np.arange(nphi // 2 + 1), 2).astype(np.float64)
+        def dphi(a):
+            o = np.empty_like(a)
+            o[..., 0::2] = -mvec[0::2] * a[..., 1::2]
+            o[..., 1::2] = mvec[1::2] * a[..., 0::2]
+            return o
+        f = {}
+        names = ["vr", "p", "t", "omr", "dvrdr", "dtdr", "dvrdt", "dtdt", "vt", "vp", "dvtdr", "dvpdr"]
+        for i, n in enumerate(names):
+            f[n] = p3[i]
+        f["dvrdp"] = dphi(f["vr"])
+        f["dvtdp"] = dphi(f["vt"])
+        f["dvpdp"] = dphi(f["vp"])
+        f["dtdp"] = dphi(f["t"])
+        for k in list(f.keys()):
+            f[k] = fft_c2r(f[k], nphi)[..., :nphi]
+        csc = h.csctheta[:, None, None]
+        cot = h.cottheta[:, None, None]
+        sin = h.sintheta[:, None, None]
+        cos = h.costheta[:, None, None]
+        for k in ("vt", "vp", "dvtdr", "dvpdr", "dtdt", "dvrdt", "dvpdp", "dvtdp"):
+            f[k] = f[k] * csc                                          # sintheta_div (:119-126)
+        r = self.radius[None, :, None]
+        dlnrho = self.dlnrho[None, :, None]
+        one_over_r = 1.0 / r
+        r2 = r * r
+        rho = self.density[None, :, None]
+        # CFL (Find_MyMinDT :784-813)
+        llp1max = L * (L + 1.0)
+        ovht2 = (np.max(f["vt"] ** 2 + f["vp"] ** 2, axis=(0, 2)) / self.radius ** 2 * llp1max)
+        ovrt2 = np.max(f["vr"] ** 2, axis=(0, 2)) / self.delta_r ** 2
+        self.last_cfl = float(max(ovht2.max(), ovrt2.max(), 0.0))
+        vr, vt, vp = f["vr"], f["vt"], f["vp"]
+        out = np.zeros((4,) + vr.shape)
+        # Temperature_Advection (:303-318)
+        out[TVAR] = -vr * f["dtdr"] - one_over_r * (f["dtdt"] * vt + vp * f["dtdp"] * csc)
+        # Momentum_Advection_Radial (:466-529)
+        w = -vr * f["dvrdr"] * r2 - vt * (f["dvrdt"] - vt) * r - vp * (f["dvrdp"] * csc - vp) * r
+        if cfg.rotation:
+            w = w + self.coriolis * sin * vp * r2
+        out[WVAR] = w * rho
+        # Momentum_Advection_Theta (:583-645)
+        pth = f["dvrdr"] + (f["dvpdp"] * csc + vt * cot + vr) * one_over_r + vr * dlnrho
+        pth = -pth * vt + vr * f["dvtdr"] + vp * (f["dvtdp"] * csc - vp * cot) * one_over_r
+        if cfg.rotation:
+            pth = pth - self.coriolis * cos * vp
+        pth = pth * rho
+        out[PVAR] = pth * r * csc
+        # Momentum_Advection_Phi (:648-700)
+        z = vt * (f["omr"] + f["dvtdp"] * csc * one_over_r) + vr * f["dvpdr"] + vp * (f["dvpdp"] * csc + vr) * one_over_r
+        if cfg.rotation:
+            z = z + self.coriolis * cos * vt + self.coriolis * sin * vr
+        z = z * rho
+        out[ZVAR] = z * r * csc
+        pad = np.zeros(out.shape[:-1] + (nphi + 2,))
+        pad[..., :nphi] = out
+        return fft_r2c(pad, nphi)
+
+    def transpose_2a3a(self, p2):
+        """Transpose_2a3a (Spherical_Buffer.F90:196-316): p2[m](f,2,r,theta) -> p3[f][theta][r][nphi+2]."""
+        nf, _, nr, nth = p2[0].shape
+        P = np.stack(p2, axis=0)                       # (m, f, 2, r, th)
+        p3 = np.zeros((nf, nth, nr, self.cfg.n_phi + 2))
+        M = P.shape[0]
+        p3[..., 0:2 * M:2] = P[:, :, 0].transpose(1, 3, 2, 0)
+        p3[..., 1:2 * M:2] = P[:, :, 1].transpose(1, 3, 2, 0)
+        return p3
+
+    def transpose_3b2b(self, p3):
+        """Transpose_3b2b (Spherical_Buffer.F90:461-581): m > l_max discarded."""
+        M = self.cfg.l_max + 1
+        re = p3[..., 0:2 * M:2]          # (f, th, r, m)
+        im = p3[..., 1:2 * M:2]
+        P = np.stack([re, im], axis=0).transpose(4, 1, 0, 3, 2)   # (m, f, 2, r, th)
+        return [np.ascontiguousarray(P[m]) for m in range(M)]
+
+    def rlm_spaceb(self, s2):
+        """Sphere_Hybrid_Space.F90:127-222 (hydro): curl algebra on the NL terms."""
+        h, L = self.h, self.cfg.l_max
+        out = []
+        for m in range(L + 1):
+            a = s2[m].copy()
+            ls = np.arange(m, L + 1, dtype=np.float64)
+            ollp1 = np.zeros_like(ls)
+            ollp1[ls > 0] = 1.0 / (ls[ls > 0] * (ls[ls > 0] + 1))
+            ollp1[ls == 0] = 1.0                              # over_l_l_plus1(0) = 1 (ProblemSize.F90:506)
+            a[WVAR] = a[WVAR] * ollp1
+            ft1 = h.d_by_sdtheta(a[ZVAR], m)
+            ft2 = h.d_by_dphi(a[PVAR][None], m)[0]
+            ft1 = (ft2 - ft1) * ollp1
+            ft2 = h.d_by_dphi(a[ZVAR][None], m)[0]
+            zsd = h.d_by_sdtheta(a[PVAR], m)
+            a[PVAR] = (zsd + ft2) * ollp1
+            a[ZVAR] = ft1
+            if m == 0:
+                a[PVAR][..., 0] = 0.0
+                a[WVAR][..., 0] = 0.0
+                a[ZVAR][..., 0] = 0.0
+            a[..., -1] = 0.0
+            out.append(a)
+        return out
+
+    def advance_time(self, p1b_new):
+        """AdvanceTime (Sphere_Spectral_Space.F90:415-435): add AB term, BCs, solve."""
+        nr = self.cfg.n_r
+        self.ab = p1b_new
+        nab = self.new_ab
+        self.rhs_wpt[:, :, 0:nr] += nab * p1b_new[WEQ]
+        self.rhs_wpt[:, :, nr:2 * nr] += nab * p1b_new[PEQ]
+        self.rhs_wpt[:, :, 2 * nr:3 * nr] += nab * p1b_new[TEQ]
+        self.rhs_z += nab * p1b_new[ZEQ]
+        # Apply_Boundary_Mask (Linear_Solve.F90:401-418)
+        for b in (0, nr, 2 * nr):
+            self.rhs_wpt[:, :, b] = 0.0
+            self.rhs_wpt[:, :, b + nr - 1] = 0.0
+        self.rhs_z[:, :, 0] = 0.0
+        self.rhs_z[:, :, nr - 1] = 0.0
+        self.rhs_wpt[0, 0, 2 * nr] = self.bc_t[0]          # l=0, m=0, real, top
+        self.rhs_wpt[0, 0, 3 * nr - 1] = self.bc_t[1]
+        # Implicit_Solve -> DGETRS (Linear_Solve.F90:423-457,1088-1110)
+        for l in range(self.cfg.l_max + 1):
+            s, e = self.l_start[l], self.l_start[l] + l + 1
+            b = self.rhs_wpt[s:e].reshape(-1, 3 * nr).T
+            x = sla.lu_solve(self.lu_wpt[l], b, check_finite=False)
+            self.rhs_wpt[s:e] = x.T.reshape(e - s, 2, 3 * nr)
+            if l > 0:
+                bz = self.rhs_z[s:e].reshape(-1, nr).T
+                xz = sla.lu_solve(self.lu_z[l], bz, check_finite=False)
+                self.rhs_z[s:e] = xz.T.reshape(e - s, 2, nr)
+
+    def step(self):
+        """One pass of Main_Loop_Sphere (Sphere_Driver.F90:305-328) at fixed dt."""
+        g = self.post_solve()
+        s2a = self.transpose_1a2a(g)
+        s2a12 = self.rlm_spacea(s2a)
+        p2a = self.h.s2p(s2a12)
+        p3a = self.transpose_2a3a(p2a)
+        p3b = self.physical_space(p3a)
+        p2b = self.transpose_3b2b(p3b)
+        s2b = self.h.p2s(p2b)
+        s2b = self.rlm_spaceb(s2b)
+        p1b = self.transpose_2b1b(s2b)
+        self.advance_time(p1b)
+        self.old_dt = self.dt
+        self.iteration += 1
+        return self.last_cfl
+
+
+def seeded_state(cfg: Config, seed=0x5241594C, amp=1.0e-3, lmin=1, lmax_pert=20, cheby=None):
+    """Seeded initial state: conductive T plus a Gaussian perturbation on l in [lmin, lmax_pert].
+
+    Returns (wpt[lm,2,3nr], z[lm,2,nr]) in Chebyshev-coefficient form.  The
+    perturbation is a random set of Chebyshev coefficients on the dealiased
+    modes with amplitude amp*(l+1)^-2 that vanishes at both boundaries
+    (multiplied by the grid function (r-rmin)(rmax-r) before the transform).
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nr = cfg.n_r
+    rmax = cfg.shell_depth / (1.0 - cfg.aspect_ratio)
+    rmin = rmax * cfg.aspect_ratio
+    cg = cheby if cheby is not None else Chebyshev(nr, rmin, rmax)
+    r = cg.radius
+    ls, ms = lm_pairs(cfg.l_max)
+    n_lm = len(ls)
+    wpt = np.zeros((n_lm, 2, 3 * nr))
+    z = np.zeros((n_lm, 2, nr))
+    r_out, r_in = r[0], r[-1]
+    pref = r_out * r_in / (r_in - r_out)
+    tcond = pref * (1.0 / r_out - 1.0 / r) * math.sqrt(4 * math.pi)
+    tgrid = np.zeros((n_lm, 2, nr))
+    tgrid[0, 0] = tcond
+    shape = (r - rmin) * (rmax - r)
+    shape = shape / shape.max()
+    radial = np.sin(np.pi * (r - rmin) / (rmax - rmin))
+    for i in range(n_lm):
+        l, m = ls[i], ms[i]
+        if lmin <= l <= lmax_pert:
+            a = amp * (l + 1.0) ** -2
+            re, im = rng.standard_normal(2) * a
+            if m == 0:
+                im = 0.0
+            tgrid[i, 0] += re * radial * shape
+            tgrid[i, 1] += im * radial * shape
+    wpt[:, :, 2 * nr:] = cg.to_spectral(tgrid)
+    return wpt, z

@@ -1,0 +1,163 @@
+/*
+ * rayleigh_b200.h -- C ABI of the B200 (sm_100a) implementation of Rayleigh's
+ * per-timestep spectral-transform + implicit-solve path.
+ *
+ * Every entry point returns 0 on success and a negative RA_ERR_* code on
+ * failure; ra_last_error() gives the message.  A context owns all device
+ * buffers; calls on one context are not thread-safe and run on the
+ * context's CUDA stream.  Host pointers are plain double arrays in the
+ * reference's Fortran layouts (described per call, written here with the
+ * fastest index first).
+ *
+ * The entry points replace the Fortran module procedures that the
+ * reference's main loop calls (paths inside geodynamics/Rayleigh 1.2.0):
+ *   Post_Solve              src/Physics/Sphere_Spectral_Space.F90:178
+ *   rlm_spacea              src/Physics/Sphere_Hybrid_Space.F90:64
+ *   physical_space          src/Physics/Sphere_Physical_Space.F90:98
+ *   rlm_spaceb              src/Physics/Sphere_Hybrid_Space.F90:127
+ *   AdvanceTime             src/Physics/Sphere_Spectral_Space.F90:415
+ *   Reset_Linear_Equations  src/Physics/Sphere_Linear_Terms.F90:67
+ * and, for unit-level parity, the math-layer calls
+ *   Legendre_Transform      src/Math_Layer/Legendre_Transforms.F90:37-40 (StP_4d_dgp2 :968, PtS_4d_dgpv3 :1077)
+ *   FFT_To_Physical/Spectral src/Math_Layer/Fourier_Transform.F90:25-35 (c2r :142, r2c :100)
+ *   Cheby_Grid%to_spectral/from_spectral/d_by_dr_cp
+ *                           src/Math_Layer/Chebyshev_Polynomials.F90:375,450,560
+ */
+#ifndef RAYLEIGH_B200_H
+#define RAYLEIGH_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RA_OK               0
+#define RA_ERR_ARG         -1   /* invalid argument or unsupported configuration */
+#define RA_ERR_CUDA        -2   /* a CUDA runtime call failed */
+#define RA_ERR_SINGULAR    -3   /* a zero pivot in a per-l implicit matrix */
+#define RA_ERR_NOMEM       -4   /* device allocation failed */
+#define RA_ERR_STATE       -5   /* call out of order (e.g. step before put_state) */
+#define RA_ERR_NONFINITE   -6   /* NaN/Inf detected in the state */
+
+#define RA_PREC_FP64   0        /* every product in FP64 */
+#define RA_PREC_MIXED  1        /* split-precision tensor-core products, FP64 state */
+
+typedef struct ra_ctx ra_ctx;
+
+/* Problem description: the namelist values the path reads
+ * (ProblemSize_Namelist, Physical_Controls, Temporal_Controls,
+ *  Boundary_Conditions, Reference_Namelist with reference_type = 1). */
+typedef struct ra_config {
+    int    n_r;              /* Chebyshev collocation points (even), one domain */
+    int    l_max;            /* maximum spherical-harmonic degree */
+    int    n_theta;          /* 0 -> 3(l_max+1)/2 (ProblemSize.F90:444-450) */
+    double aspect_ratio;     /* r_min / r_max */
+    double shell_depth;      /* r_max - r_min */
+    double rayleigh;         /* Rayleigh_Number (buoyancy = Ra/Pr (r/r_o)^gravity_power) */
+    double ekman;
+    double prandtl;
+    double magnetic_prandtl;
+    double gravity_power;
+    int    rotation;         /* Coriolis terms on/off */
+    int    magnetism;        /* must be 0: the hydrodynamic equation set */
+    int    no_slip_top, no_slip_bottom;    /* else stress-free */
+    int    fix_tvar_top, fix_tvar_bottom;  /* else fixed dT/dr */
+    double t_top, t_bottom, dtdr_top, dtdr_bottom;
+    double dt;               /* time step (fixed; ra_set_dt changes it) */
+    double alpha_implicit;   /* Crank-Nicolson weight, 0.5 */
+    int    precision;        /* RA_PREC_FP64 or RA_PREC_MIXED */
+    int    use_graph;        /* capture the steady AB2 step as a CUDA graph */
+    int    device;           /* CUDA device ordinal */
+} ra_config;
+
+/* Fills *cfg with the defaults of the reference (Controls.F90, PDE_Coefficients.F90). */
+int ra_default_config(ra_config* cfg);
+
+/* Creates a context: builds the grids, the P_l^m tables (on the device),
+ * the radial coefficient profiles, the per-l implicit matrices and their
+ * inverses (Reset_Linear_Equations).  Replaces Main_Initialization's grid,
+ * Legendre and linear-system set-up (src/Physics/Main.F90:71-117). */
+int ra_create(ra_ctx** ctx, const ra_config* cfg);
+int ra_destroy(ra_ctx* ctx);
+int ra_last_error(const ra_ctx* ctx, char* msg, int len);
+
+/* Sizes of the state arrays: n_lm = (l_max+1)(l_max+2)/2 (l-major, m ascending). */
+int ra_sizes(const ra_ctx* ctx, long* n_lm, int* n_r, int* n_theta, int* n_phi);
+
+/* New time step: Reset_Linear_Equations (Sphere_Linear_Terms.F90:67-76):
+ * rebuild LHS = I - alpha dt L with boundary rows and invert it per l. */
+int ra_set_dt(ra_ctx* ctx, double dt);
+
+/* State exchange in the equation-set RHS layout (Linear_Solve.F90:355-386):
+ *   wpt[3 n_r][2][n_lm]  W, P, T Chebyshev coefficients of the linked l-block
+ *   z  [  n_r][2][n_lm]  Z coefficients
+ *   ab [n_r][2][n_lm][4] Adams-Bashforth term p1b (W, P, T, Z RHS); may be NULL (zero)
+ * iteration: the reference's iteration counter (1 = Euler first step). */
+int ra_put_state(ra_ctx* ctx, const double* wpt, const double* z, const double* ab, int iteration);
+int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab);
+
+/* One full step, the five stage calls of Main_Loop_Sphere
+ * (Sphere_Driver.F90:305-328) at the current dt, nsteps times.  cfl (may be
+ * NULL) receives the CFL cargo global_msgs(1) of the last step
+ * (Sphere_Physical_Space.F90:784-813). */
+int ra_step(ra_ctx* ctx, int nsteps, double* cfl);
+
+/* The stages, for a driver that interleaves its own work between them. */
+int ra_post_solve(ra_ctx* ctx);                 /* Post_Solve + Transpose_1a2a */
+int ra_rlm_a(ra_ctx* ctx);                      /* rlm_spacea + StP Legendre + Transpose_2a3a */
+int ra_physical(ra_ctx* ctx, double* cfl);      /* physical_space: FFTs, NL terms, CFL, 3b2b */
+int ra_rlm_b(ra_ctx* ctx);                      /* PtS Legendre + rlm_spaceb + Transpose_2b1b */
+int ra_advance(ra_ctx* ctx);                    /* AdvanceTime: AB term, BCs, Implicit_Solve */
+
+/* Blocks until the context's stream is idle; returns the first device error. */
+int ra_sync(ra_ctx* ctx);
+
+/* ---- math-layer operators (host buffers in the reference layouts) ---- */
+
+/* StP_4d_dgp2 (Legendre_Transforms.F90:968-1074).
+ * s: concatenation over m = 0..l_max of s2a(m)%data(m:l_max, nr, 2, nf)
+ * p: p2a(n_theta, nr*2*nf, l_max+1)  (nrhs = (r, re/im, field), r fastest) */
+int ra_legendre_s2p(ra_ctx* ctx, const double* s, double* p, int nf, int nr);
+/* PtS_4d_dgpv3 (Legendre_Transforms.F90:1077-1175): layouts as above, reversed. */
+int ra_legendre_p2s(ra_ctx* ctx, const double* p, double* s, int nf, int nr);
+
+/* c2r_ip4D_fftw / r2c_ip4D_fftw (Fourier_Transform.F90:100-183): in place on
+ * x(n_phi+2, howmany), unnormalised, FFTW's packed (re, im) layout. */
+int ra_fft_c2r(ra_ctx* ctx, double* x, long howmany);
+int ra_fft_r2c(ra_ctx* ctx, double* x, long howmany);
+
+/* Chebyshev_Polynomials.F90: To_Spectral4D (:375), From_Spectral4D (:450) and
+ * Cheby_Deriv_Buffer_4D (:560) of order 1..3 on columns f(n_r, ncols). */
+int ra_cheby_to_spectral(ra_ctx* ctx, const double* f, double* c, long ncols);
+int ra_cheby_from_spectral(ra_ctx* ctx, const double* c, double* f, long ncols);
+int ra_cheby_deriv(ra_ctx* ctx, const double* c, double* dc, int order, long ncols);
+
+/* Radial grid of the context: radius(n_r), r(1) = r_max (Chebyshev_Polynomials.F90:168-200). */
+int ra_radius(const ra_ctx* ctx, double* radius);
+/* Gauss-Legendre nodes cos(theta) (n_theta) as used by the context. */
+int ra_costheta(const ra_ctx* ctx, double* costheta);
+
+/* Number of kernel launches issued by the last ra_step call (for accounting). */
+long ra_launch_count(const ra_ctx* ctx);
+
+/* Diagnostics: copies internal device buffer `which` (RA_BUF_*) to host
+ * memory; n is the capacity of out in doubles, *n_out receives the size.
+ * With out == NULL only the size is returned.  Used by the parity tests to
+ * compare every stage of a step with the CPU restatement; the reference
+ * exposes the same data as its Spherical_Buffer configurations. */
+#define RA_BUF_GRID    0   /* [12][n_lm][2][n_r]  W, dW, d2W, d3W, P, dP, T, dT, d2T, Z, dZ, d2Z on the grid */
+#define RA_BUF_S2A     1   /* [row][7][n_r][2]    after Post_Solve: W, T, Z, dW, dT, dZ, d2W */
+#define RA_BUF_S2A11   2   /* [row][11][n_r][2]   after rlm_spacea */
+#define RA_BUF_P2A     3   /* [m][n_theta][11][n_r][2] */
+#define RA_BUF_P2B     4   /* [m][n_theta][4][n_r][2]  */
+#define RA_BUF_S2B     5   /* [row][4][n_r][2]    */
+#define RA_BUF_AB      6   /* [4][n_lm][2][n_r]   */
+#define RA_BUF_RHS_WPT 7   /* [n_lm][2][3 n_r]    */
+#define RA_BUF_RHS_Z   8   /* [n_lm][2][n_r]      */
+#define RA_BUF_PTAB    9   /* [row][n_theta/2]    P_l^m (times 1/2 for m > 0) */
+#define RA_BUF_IPTAB  10   /* [row][n_theta/2]    weighted P_l^m with the FFT normalisation */
+int ra_debug_buffer(ra_ctx* ctx, int which, double* out, long n, long* n_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RAYLEIGH_B200_H */

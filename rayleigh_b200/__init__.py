@@ -1,0 +1,323 @@
+"""rayleigh_b200 -- B200 (sm_100a) implementation of Rayleigh's per-timestep
+spectral-transform + implicit-solve path, behind the C ABI declared in
+``include/rayleigh_b200.h``.
+
+This module is the Python mirror of the host side: it loads the in-tree
+``librayleigh_b200.so`` through ctypes and exposes the stage calls that the
+reference's main loop makes (``Post_Solve``, ``rlm_spacea``,
+``physical_space``, ``rlm_spaceb``, ``AdvanceTime``; Sphere_Driver.F90:305-328)
+and the math-layer operators (Legendre transforms, phi FFTs, Chebyshev
+transforms).  There is no CPU fallback: if the shared library or a CUDA device
+is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librayleigh_b200.so")
+
+RA_OK = 0
+RA_ERR_ARG = -1
+RA_ERR_CUDA = -2
+RA_ERR_SINGULAR = -3
+RA_ERR_NOMEM = -4
+RA_ERR_STATE = -5
+RA_ERR_NONFINITE = -6
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class RayleighError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rayleigh_b200 error {code}: {msg}")
+        self.code = code
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("n_r", ctypes.c_int), ("l_max", ctypes.c_int), ("n_theta", ctypes.c_int),
+        ("aspect_ratio", ctypes.c_double), ("shell_depth", ctypes.c_double),
+        ("rayleigh", ctypes.c_double), ("ekman", ctypes.c_double), ("prandtl", ctypes.c_double),
+        ("magnetic_prandtl", ctypes.c_double), ("gravity_power", ctypes.c_double),
+        ("rotation", ctypes.c_int), ("magnetism", ctypes.c_int),
+        ("no_slip_top", ctypes.c_int), ("no_slip_bottom", ctypes.c_int),
+        ("fix_tvar_top", ctypes.c_int), ("fix_tvar_bottom", ctypes.c_int),
+        ("t_top", ctypes.c_double), ("t_bottom", ctypes.c_double),
+        ("dtdr_top", ctypes.c_double), ("dtdr_bottom", ctypes.c_double),
+        ("dt", ctypes.c_double), ("alpha_implicit", ctypes.c_double),
+        ("precision", ctypes.c_int), ("use_graph", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+@dataclass
+class Config:
+    """Namelist values the path reads (defaults follow the reference's Controls/PDE_Coefficients)."""
+
+    n_r: int = 48
+    l_max: int = 63
+    n_theta: int = 0
+    aspect_ratio: float = 0.35
+    shell_depth: float = 1.0
+    rayleigh: float = 1.0e5
+    ekman: float = 1.0e-3
+    prandtl: float = 1.0
+    magnetic_prandtl: float = 1.0
+    gravity_power: float = 1.0
+    rotation: bool = True
+    magnetism: bool = False
+    no_slip_top: bool = True
+    no_slip_bottom: bool = True
+    fix_tvar_top: bool = True
+    fix_tvar_bottom: bool = True
+    t_top: float = 0.0
+    t_bottom: float = 1.0
+    dtdr_top: float = 0.0
+    dtdr_bottom: float = 0.0
+    dt: float = 1.0e-4
+    alpha_implicit: float = 0.5
+    precision: int = PREC_FP64
+    use_graph: bool = True
+    device: int = 0
+
+    def to_c(self):
+        c = _Config()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            setattr(c, f.name, int(v) if isinstance(v, bool) else v)
+        return c
+
+
+_lib = None
+_DP = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+
+
+def load_library(path: str | None = None):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RayleighError(RA_ERR_STATE, f"{p} is missing; build it with `python -m rayleigh_b200.build`")
+    lib = ctypes.CDLL(p)
+    sig = {
+        "ra_default_config": ([ctypes.POINTER(_Config)], ctypes.c_int),
+        "ra_create": ([ctypes.POINTER(_VP), ctypes.POINTER(_Config)], ctypes.c_int),
+        "ra_destroy": ([_VP], ctypes.c_int),
+        "ra_last_error": ([_VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "ra_sizes": ([_VP, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int),
+                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "ra_set_dt": ([_VP, ctypes.c_double], ctypes.c_int),
+        "ra_put_state": ([_VP, _VP, _VP, _VP, ctypes.c_int], ctypes.c_int),
+        "ra_get_state": ([_VP, _VP, _VP, _VP], ctypes.c_int),
+        "ra_step": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
+        "ra_post_solve": ([_VP], ctypes.c_int),
+        "ra_rlm_a": ([_VP], ctypes.c_int),
+        "ra_physical": ([_VP, _DP], ctypes.c_int),
+        "ra_rlm_b": ([_VP], ctypes.c_int),
+        "ra_advance": ([_VP], ctypes.c_int),
+        "ra_sync": ([_VP], ctypes.c_int),
+        "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "ra_fft_c2r": ([_VP, _VP, ctypes.c_long], ctypes.c_int),
+        "ra_fft_r2c": ([_VP, _VP, ctypes.c_long], ctypes.c_int),
+        "ra_cheby_to_spectral": ([_VP, _VP, _VP, ctypes.c_long], ctypes.c_int),
+        "ra_cheby_from_spectral": ([_VP, _VP, _VP, ctypes.c_long], ctypes.c_int),
+        "ra_cheby_deriv": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_long], ctypes.c_int),
+        "ra_radius": ([_VP, _VP], ctypes.c_int),
+        "ra_costheta": ([_VP, _VP], ctypes.c_int),
+        "ra_launch_count": ([_VP], ctypes.c_long),
+        "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_VP) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Rayleigh:
+    """One simulation context on one GPU (mirrors the reference's module state)."""
+
+    def __init__(self, cfg: Config):
+        self.lib = load_library()
+        self.cfg = cfg
+        self._c = cfg.to_c()
+        h = _VP()
+        rc = self.lib.ra_create(ctypes.byref(h), ctypes.byref(self._c))
+        self.h = h
+        if rc != RA_OK:
+            msg = self._err()
+            self.lib.ra_destroy(h)
+            self.h = None
+            raise RayleighError(rc, msg)
+        n_lm = ctypes.c_long()
+        nr, nth, nphi = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.ra_sizes(h, ctypes.byref(n_lm), ctypes.byref(nr), ctypes.byref(nth), ctypes.byref(nphi)))
+        self.n_lm, self.n_r, self.n_theta, self.n_phi = n_lm.value, nr.value, nth.value, nphi.value
+        self.l_max = cfg.l_max
+
+    def _err(self):
+        buf = ctypes.create_string_buffer(1024)
+        if self.h:
+            self.lib.ra_last_error(self.h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc):
+        if rc != RA_OK:
+            raise RayleighError(rc, self._err())
+
+    def close(self):
+        if self.h:
+            self.lib.ra_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state (equation-set RHS layout: wpt[lm][ri][3 nr], z[lm][ri][nr], ab[4][lm][ri][nr]) ----
+    def put_state(self, wpt, z, ab=None, iteration=1):
+        self._wpt = _f64(wpt)
+        self._z = _f64(z)
+        self._ab = None if ab is None else _f64(ab)
+        if self._wpt.size != self.n_lm * 2 * 3 * self.n_r or self._z.size != self.n_lm * 2 * self.n_r:
+            raise ValueError("state arrays have the wrong size")
+        self._check(self.lib.ra_put_state(self.h, _ptr(self._wpt), _ptr(self._z), _ptr(self._ab), int(iteration)))
+
+    def get_state(self):
+        wpt = np.empty((self.n_lm, 2, 3 * self.n_r))
+        z = np.empty((self.n_lm, 2, self.n_r))
+        ab = np.empty((4, self.n_lm, 2, self.n_r))
+        self._check(self.lib.ra_get_state(self.h, _ptr(wpt), _ptr(z), _ptr(ab)))
+        return wpt, z, ab
+
+    def step(self, nsteps=1):
+        cfl = ctypes.c_double()
+        self._check(self.lib.ra_step(self.h, int(nsteps), ctypes.byref(cfl)))
+        return cfl.value
+
+    def set_dt(self, dt):
+        self._check(self.lib.ra_set_dt(self.h, float(dt)))
+
+    def sync(self):
+        self._check(self.lib.ra_sync(self.h))
+
+    def launch_count(self):
+        return self.lib.ra_launch_count(self.h)
+
+    # the five stage calls
+    def post_solve(self):
+        self._check(self.lib.ra_post_solve(self.h))
+
+    def rlm_spacea(self):
+        self._check(self.lib.ra_rlm_a(self.h))
+
+    def physical_space(self):
+        cfl = ctypes.c_double()
+        self._check(self.lib.ra_physical(self.h, ctypes.byref(cfl)))
+        return cfl.value
+
+    def rlm_spaceb(self):
+        self._check(self.lib.ra_rlm_b(self.h))
+
+    def advance_time(self):
+        self._check(self.lib.ra_advance(self.h))
+
+    BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,
+               "rhs_wpt": 7, "rhs_z": 8, "ptab": 9, "iptab": 10}
+
+    def debug_buffer(self, name):
+        """Copy of an internal device buffer (diagnostics for the stage-by-stage parity tests)."""
+        which = self.BUFFERS[name]
+        n = ctypes.c_long()
+        self._check(self.lib.ra_debug_buffer(self.h, which, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value)
+        self._check(self.lib.ra_debug_buffer(self.h, which, _ptr(out), n.value, ctypes.byref(n)))
+        return out
+
+    # ---- grids ----
+    def radius(self):
+        r = np.empty(self.n_r)
+        self._check(self.lib.ra_radius(self.h, _ptr(r)))
+        return r
+
+    def costheta(self):
+        c = np.empty(self.n_theta)
+        self._check(self.lib.ra_costheta(self.h, _ptr(c)))
+        return c
+
+    # ---- math-layer operators on reference layouts ----
+    def legendre_s2p(self, s2):
+        """StP: s2 = list over m of arrays (nf, 2, nr, l_max-m+1) -> list over m of (nf, 2, nr, n_theta)."""
+        nf, _, nr, _ = s2[0].shape
+        flat = _f64(np.concatenate([np.ascontiguousarray(a).ravel() for a in s2]))
+        out = np.empty(((self.l_max + 1), nf, 2, nr, self.n_theta))
+        self._check(self.lib.ra_legendre_s2p(self.h, _ptr(flat), _ptr(out), nf, nr))
+        return [out[m] for m in range(self.l_max + 1)]
+
+    def legendre_p2s(self, p2):
+        nf, _, nr, _ = p2[0].shape
+        flat = _f64(np.stack(p2))
+        out = np.empty(sum(nf * 2 * nr * (self.l_max + 1 - m) for m in range(self.l_max + 1)))
+        self._check(self.lib.ra_legendre_p2s(self.h, _ptr(flat), _ptr(out), nf, nr))
+        res, off = [], 0
+        for m in range(self.l_max + 1):
+            n = nf * 2 * nr * (self.l_max + 1 - m)
+            res.append(out[off:off + n].reshape(nf, 2, nr, self.l_max + 1 - m))
+            off += n
+        return res
+
+    def fft_c2r(self, x):
+        x = _f64(x).copy()
+        self._check(self.lib.ra_fft_c2r(self.h, _ptr(x), x.size // (self.n_phi + 2)))
+        return x
+
+    def fft_r2c(self, x):
+        x = _f64(x).copy()
+        self._check(self.lib.ra_fft_r2c(self.h, _ptr(x), x.size // (self.n_phi + 2)))
+        return x
+
+    def cheby_to_spectral(self, f):
+        f = _f64(f)
+        out = np.empty_like(f)
+        self._check(self.lib.ra_cheby_to_spectral(self.h, _ptr(f), _ptr(out), f.size // self.n_r))
+        return out
+
+    def cheby_from_spectral(self, c):
+        c = _f64(c)
+        out = np.empty_like(c)
+        self._check(self.lib.ra_cheby_from_spectral(self.h, _ptr(c), _ptr(out), c.size // self.n_r))
+        return out
+
+    def cheby_deriv(self, c, order):
+        c = _f64(c)
+        out = np.empty_like(c)
+        self._check(self.lib.ra_cheby_deriv(self.h, _ptr(c), _ptr(out), int(order), c.size // self.n_r))
+        return out
+
+
+__all__ = ["Config", "Rayleigh", "RayleighError", "load_library", "LIB_PATH", "PREC_FP64", "PREC_MIXED"]

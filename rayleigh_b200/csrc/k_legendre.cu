@@ -1,0 +1,215 @@
+// Legendre path: P_l^m table generation and the two Legendre transforms.
+//
+//  * plm_kernel  restates Compute_Plms + Parity_Resort
+//    (src/Math_Layer/Legendre_Polynomials.F90:146-331) in FP64 with a carried
+//    binary exponent, so the sin^m(theta) underflow that the reference avoids
+//    with REAL*16 is handled without quad precision.
+//  * lt_inverse_kernel restates StP_4d_dgp2 (Legendre_Transforms.F90:968-1074):
+//    per m, an even-l and an odd-l product, then the equatorial mirror
+//    (south = e + o, north = e - o).
+//  * lt_forward_kernel restates PtS_4d_dgpv3 (Legendre_Transforms.F90:1077-1175):
+//    equatorial fold (f_even = s + n, f_odd = s - n) in the operand load, then
+//    the per-parity product with the weighted tables.
+//  All m share one launch; K (the number of l of one parity) is ragged and the
+//  grid is ordered by m so that the long products start first.
+#include "ra_internal.h"
+#include "gemm_f64.cuh"
+
+namespace ra {
+
+__global__ void plm_kernel(const double* __restrict__ x, const double* __restrict__ s,
+                           const double* __restrict__ w2pi, int L, int nth,
+                           double* __restrict__ Ptab, double* __restrict__ iPtab) {
+    const int nth2 = nth / 2;
+    const int th = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (th >= nth2 || m >= L) return;
+    const int lmax = L - 1;
+    const double xv = x[th], sv = s[th];
+    const double wt = w2pi[th];
+    const double stp = (m == 0) ? 1.0 : 0.5;
+    const double pts = (m == 0) ? 1.0 / (2.0 * nth) : 1.0 / (double)nth;
+    const double TWO600 = 0x1p600, TWOM600 = 0x1p-600;
+    // P_m^m = (-1)^m sqrt((m+1/2)/(2 pi)) prod_{i<=m} sqrt((i-1/2)/i) sin^m(theta)
+    double p = sqrt((m + 0.5) / (2.0 * 3.14159265358979323846));
+    int e = 0;
+    for (int i = 1; i <= m; ++i) {
+        p *= sqrt((i - 0.5) / (double)i) * sv;
+        if (p < TWOM600) {
+            p *= TWO600;
+            e -= 600;
+        }
+    }
+    if (m & 1) p = -p;
+    auto store = [&](int l, double v) {
+        const long row = row_index(m, l, L);
+        const double a = ldexp(v, e);
+        Ptab[row * nth2 + th] = a * stp;
+        iPtab[row * nth2 + th] = (a * wt) * pts;
+    };
+    store(m, p);
+    if (m == lmax) return;
+    double p1 = p * xv * sqrt(2.0 * m + 3.0);  // P_{m+1}^m
+    double p0 = p;
+    store(m + 1, p1);
+    for (int l = m + 2; l <= lmax; ++l) {
+        const double lm1 = (double)(l - 1);
+        double a = (lm1 * lm1 - (double)m * m) / (4.0 * lm1 * lm1 - 1.0);
+        a = sqrt(a);
+        const double t = p1 * xv - a * p0;
+        const double b = (4.0 * (double)l * l - 1.0) / ((double)l * l - (double)m * m);
+        const double pn = t * sqrt(b);
+        p0 = p1;
+        p1 = pn;
+        if (e < 0 && fabs(p1) > TWO600) {
+            p1 *= TWOM600;
+            p0 *= TWOM600;
+            e += 600;
+        }
+        store(l, p1);
+    }
+}
+
+void launch_plm(Ctx& c, const double* d_x, const double* d_w) {
+    // d_x holds [x | s] (2 * nth2 doubles); d_w holds 2 pi w (nth2 doubles)
+    const int nth2 = c.d.nth2;
+    dim3 grid((nth2 + 127) / 128, c.d.L);
+    plm_kernel<<<grid, 128, 0, c.stream>>>(d_x, d_x + nth2, d_w, c.d.L, c.d.nth, c.d_Ptab, c.d_iPtab);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// Inverse transform: p2[m][theta][col] = sum_l P(l, theta) s2[row(m, l)][col]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(GEMM_THREADS) lt_inverse_kernel(const double* __restrict__ Ptab,
+                                                                  const double* __restrict__ s2,
+                                                                  double* __restrict__ p2, int L, int nth,
+                                                                  int ncol) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
+    const int m = blockIdx.z;
+    const int th0 = blockIdx.y * BM;
+    const int c0 = blockIdx.x * BN;
+    const int nth2 = nth / 2;
+    const long off = m_off(m, L);
+    const int ne = n_even(m, L), no = n_odd(m, L);
+    Acc ae, ao;
+    ae.zero();
+    ao.zero();
+    {
+        const double* pa = Ptab + off * nth2;
+        const double* pb = s2 + off * ncol;
+        auto fa = [&](int k, int x) -> double {
+            const int th = th0 + x;
+            return (k < ne && th < nth2) ? __ldg(pa + (long)k * nth2 + th) : 0.0;
+        };
+        auto fb = [&](int k, int y) -> double {
+            const int col = c0 + y;
+            return (k < ne && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
+        };
+        gemm_tile<true, true>(ae, fa, fb, ne, sm);
+    }
+    {
+        const double* pa = Ptab + (off + ne) * nth2;
+        const double* pb = s2 + (off + ne) * ncol;
+        auto fa = [&](int k, int x) -> double {
+            const int th = th0 + x;
+            return (k < no && th < nth2) ? __ldg(pa + (long)k * nth2 + th) : 0.0;
+        };
+        auto fb = [&](int k, int y) -> double {
+            const int col = c0 + y;
+            return (k < no && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
+        };
+        gemm_tile<true, true>(ao, fa, fb, no, sm);
+    }
+    double* out = p2 + (long)m * nth * ncol;
+    acc_foreach2(ae, ao, [&](int x, int y, double e, double o) {
+        const int th = th0 + x, col = c0 + y;
+        if (th < nth2 && col < ncol) {
+            out[(long)th * ncol + col] = e + o;
+            out[(long)(nth - 1 - th) * ncol + col] = e - o;
+        }
+    });
+}
+
+void launch_lt_inverse(Ctx& c, const double* s2, double* p2, int ncol) {
+    dim3 grid((ncol + BN - 1) / BN, (c.d.nth2 + BM - 1) / BM, c.d.L);
+    lt_inverse_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(c.d_Ptab, s2, p2, c.d.L, c.d.nth, ncol);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// Forward transform: s2[row(m, l)][col] = sum_th iP(l, th) fold_par(p2[m])[th][col]
+// tiles: (m, parity, l-tile) in descending-K order
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* __restrict__ iPtab,
+                                                                  const double* __restrict__ p2,
+                                                                  double* __restrict__ s2,
+                                                                  const int4* __restrict__ tiles, int L,
+                                                                  int nth, int ncol) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
+    const int4 tl = tiles[blockIdx.y];
+    const int m = tl.x, par = tl.y, l0 = tl.z * BM;
+    const int c0 = blockIdx.x * BN;
+    const int nth2 = nth / 2;
+    const int ne = n_even(m, L);
+    const int nl = par ? n_odd(m, L) : ne;
+    const long roff = m_off(m, L) + (par ? ne : 0) + l0;
+    const double sgn = par ? -1.0 : 1.0;
+    const double* pa = iPtab + roff * nth2;
+    const double* pm = p2 + (long)m * nth * ncol;
+    Acc acc;
+    acc.zero();
+    auto fa = [&](int k, int x) -> double {
+        return (l0 + x < nl && k < nth2) ? __ldg(pa + (long)x * nth2 + k) : 0.0;
+    };
+    auto fb = [&](int k, int y) -> double {
+        const int col = c0 + y;
+        if (k >= nth2 || col >= ncol) return 0.0;
+        const double s = __ldg(pm + (long)k * ncol + col);
+        const double n = __ldg(pm + (long)(nth - 1 - k) * ncol + col);
+        return par ? (s - n) : (s + n);
+    };
+    (void)sgn;
+    gemm_tile<false, true>(acc, fa, fb, nth2, sm);
+    double* out = s2 + roff * ncol;
+    acc_foreach(acc, [&](int x, int y, double v) {
+        const int col = c0 + y;
+        if (l0 + x < nl && col < ncol) out[(long)x * ncol + col] = v;
+    });
+}
+
+static std::vector<int> forward_tiles(int L) {
+    std::vector<int> t;
+    for (int m = 0; m < L; ++m) {
+        for (int par = 0; par < 2; ++par) {
+            const int nl = par ? n_odd(m, L) : n_even(m, L);
+            for (int lt = 0; lt * BM < nl; ++lt) {
+                t.push_back(m);
+                t.push_back(par);
+                t.push_back(lt);
+                t.push_back(0);
+            }
+        }
+    }
+    return t;
+}
+
+void launch_lt_forward(Ctx& c, const double* p2, double* s2, int ncol) {
+    if (!c.d_fwd_tiles) {
+        std::vector<int> t = forward_tiles(c.d.L);
+        c.n_fwd_tiles = (int)(t.size() / 4);
+        RA_CUDA(cudaMalloc(&c.d_fwd_tiles, t.size() * sizeof(int)));
+        RA_CUDA(cudaMemcpy(c.d_fwd_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    dim3 grid((ncol + BN - 1) / BN, c.n_fwd_tiles);
+    lt_forward_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
+        c.d_iPtab, p2, s2, reinterpret_cast<const int4*>(c.d_fwd_tiles), c.d.L, c.d.nth, ncol);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+}  // namespace ra

@@ -1,0 +1,511 @@
+// Spectral-space stages of the step:
+//   cheb_synthesis_kernel  d^k/dr^k on the collocation grid of the solved
+//                          Chebyshev coefficients (K5 + K7 fused: the derivative
+//                          recursion of Cheby_Deriv_Buffer_4D followed by
+//                          From_Spectral4D equals one product with the derivative
+//                          matrices dcheby(:,:,k); Chebyshev_Polynomials.F90:299-351,
+//                          450-644), parity split about the mid-shell.
+//   post_assemble_kernel   Add_Derivative x16 + Set_All_RHS + Transpose_1a2a
+//                          (Sphere_Spectral_Space.F90:204-410, Linear_Solve.F90:758-796).
+//   rlm_a_kernel           rlm_spacea algebra (Sphere_Hybrid_Space.F90:64-355).
+//   rlm_b_kernel           rlm_spaceb algebra + Transpose_2b1b (Sphere_Hybrid_Space.F90:127-222).
+//   solve_kernel           AdvanceTime: Add_To_All_RHS, Apply_Boundary_Mask,
+//                          Implicit_Solve (Sphere_Spectral_Space.F90:415-435,
+//                          Linear_Solve.F90:401-457) as x = A^{-1} b per l.
+//   gj_invert_kernel       the per-l inverse used above (LU_Decompose_Matrices,
+//                          Linear_Solve.F90:459-480): Gauss-Jordan, partial pivoting.
+#include <cmath>
+
+#include "ra_internal.h"
+#include "gemm_f64.cuh"
+
+namespace ra {
+
+__device__ __forceinline__ int ell_of_lm(long lm) {
+    int l = (int)floor((sqrt(8.0 * (double)lm + 1.0) - 1.0) * 0.5);
+    while ((long)(l + 1) * (l + 2) / 2 <= lm) ++l;
+    while ((long)l * (l + 1) / 2 > lm) --l;
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// Chebyshev synthesis of the 12 grid outputs (W W' W'' W''' P P' T T' T'' Z Z' Z'')
+// ---------------------------------------------------------------------------
+struct ChebOut { int var, d; };
+__constant__ ChebOut kChebOut[NG] = {{0, 0}, {0, 1}, {0, 2}, {0, 3}, {1, 0}, {1, 1},
+                                     {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {3, 2}};
+
+__global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const double* __restrict__ D,
+                                                                      const double* __restrict__ sol_wpt,
+                                                                      const double* __restrict__ sol_z,
+                                                                      double* __restrict__ g, int nr, int kc,
+                                                                      long ncols) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
+    const int o = blockIdx.z;
+    const int var = kChebOut[o].var, d = kChebOut[o].d;
+    const int r0 = blockIdx.y * BM;
+    const long c0 = (long)blockIdx.x * BN;
+    const int nr2 = nr / 2;
+    const int ke = (kc + 1) / 2, ko = kc / 2;
+    const double* Dd = D + (long)d * nr * nr;
+    const double* src;
+    long cstride;
+    if (var < 3) {
+        src = sol_wpt + (long)var * nr;
+        cstride = 3L * nr;
+    } else {
+        src = sol_z;
+        cstride = nr;
+    }
+    Acc ae, ao;
+    ae.zero();
+    ao.zero();
+    for (int par = 0; par < 2; ++par) {
+        const int kk = par ? ko : ke;
+        auto fa = [&](int k, int x) -> double {
+            const int r = r0 + x;
+            return (k < kk && r < nr2) ? __ldg(Dd + (long)r * nr + 2 * k + par) : 0.0;
+        };
+        auto fb = [&](int k, int y) -> double {
+            const long col = c0 + y;
+            return (k < kk && col < ncols) ? __ldg(src + col * cstride + 2 * k + par) : 0.0;
+        };
+        gemm_tile<false, false>(par ? ao : ae, fa, fb, kk, sm);
+    }
+    const double sgn = (d & 1) ? -1.0 : 1.0;
+    double* out = g + (long)o * ncols * nr;
+    acc_foreach2(ae, ao, [&](int x, int y, double e, double od) {
+        const int r = r0 + x;
+        const long col = c0 + y;
+        if (r < nr2 && col < ncols) {
+            out[col * nr + r] = e + od;
+            out[col * nr + (nr - 1 - r)] = sgn * (e - od);
+        }
+    });
+}
+
+void launch_cheb_synthesis(Ctx& c) {
+    const long ncols = 2 * c.d.nlm;
+    dim3 grid((unsigned)((ncols + BN - 1) / BN), (c.d.nr / 2 + BM - 1) / BM, NG);
+    cheb_synthesis_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(c.d_D, c.d_sol_wpt, c.d_sol_z, c.d_g,
+                                                                               c.d.nr, c.d.kc, ncols);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// RHS assembly + transpose to the m-major spectral layout
+// ---------------------------------------------------------------------------
+__constant__ Slot kSlotsDev[NSLOT] = {
+    {EQ_W, G_W0}, {EQ_W, G_W1}, {EQ_W, G_W2}, {EQ_W, G_P1}, {EQ_W, G_T0},
+    {EQ_P, G_W0}, {EQ_P, G_W1}, {EQ_P, G_W2}, {EQ_P, G_W3}, {EQ_P, G_P0},
+    {EQ_T, G_T0}, {EQ_T, G_T1}, {EQ_T, G_T2},
+    {EQ_Z, G_Z0}, {EQ_Z, G_Z1}, {EQ_Z, G_Z2}};
+
+__global__ void post_assemble_kernel(const double* __restrict__ g, const double* __restrict__ ab,
+                                     const double* __restrict__ coef, double* __restrict__ rhs_wpt,
+                                     double* __restrict__ rhs_z, double* __restrict__ s2a, long nlm, int nr,
+                                     int L, double old_ab) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, ri, r), r fastest
+    const long total = nlm * 2 * nr;
+    if (idx >= total) return;
+    const int r = (int)(idx % nr);
+    const long col = idx / nr;          // lm * 2 + ri
+    const int ri = (int)(col & 1);
+    const long lm = col >> 1;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const long plane = nlm * 2 * nr;    // one field of g / ab
+    double gv[NG];
+#pragma unroll
+    for (int o = 0; o < NG; ++o) gv[o] = g[o * plane + idx];
+    double acc[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[e] = ab[e * plane + idx] * old_ab;
+    const double* cf = coef + (long)l * NSLOT * nr + r;
+#pragma unroll
+    for (int s = 0; s < NSLOT; ++s) acc[kSlotsDev[s].eq] += cf[s * nr] * gv[kSlotsDev[s].g];
+    const long base = col * 3L * nr;
+    rhs_wpt[base + r] = acc[EQ_W];
+    rhs_wpt[base + nr + r] = acc[EQ_P];
+    rhs_wpt[base + 2 * nr + r] = acc[EQ_T];
+    rhs_z[col * nr + r] = acc[EQ_Z];
+    // s2a[row][f][r][ri] with f = W T Z W' T' Z' W''
+    const long row = row_index(m, l, L);
+    double* o = s2a + row * (long)NS2A * nr * 2 + (long)r * 2 + ri;
+    const long fs = 2L * nr;
+    o[S_W * fs] = gv[G_W0];
+    o[S_T * fs] = gv[G_T0];
+    o[S_Z * fs] = gv[G_Z0];
+    o[S_W1 * fs] = gv[G_W1];
+    o[S_T1 * fs] = gv[G_T1];
+    o[S_Z1 * fs] = gv[G_Z1];
+    o[S_W2 * fs] = gv[G_W2];
+}
+
+void launch_post_assemble(Ctx& c, double old_ab) {
+    const long total = c.d.nlm * 2 * c.d.nr;
+    post_assemble_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
+        c.d_g, c.d_ab, c.d_coef, c.d_rhs_wpt, c.d_rhs_z, c.d_s2a, c.d.nlm, c.d.nr, c.d.L, old_ab);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// rlm_spacea: 7 spectral fields -> the 11 fields the inverse transform carries
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dth_c1(int l, int m) {   // sin(theta) d/dtheta, l-1 coefficient
+    const double num = (double)(l + m) * (l - m), den = (double)(2 * l + 1) * (2 * l - 1);
+    return (l - 1) * sqrt(num / den);
+}
+__device__ __forceinline__ double dth_c2(int l, int m) {   // l+1 coefficient
+    const double num = (double)(l + 1 + m) * (l + 1 - m), den = (double)(2 * l + 1) * (2 * l + 3);
+    return -(l + 2) * sqrt(num / den);
+}
+__device__ __forceinline__ double sdth_c1(int l, int m) {
+    const double num = (double)(l + m) * (l - m), den = (double)(2 * l + 1) * (2 * l - 1);
+    return (l + 1) * sqrt(num / den);
+}
+__device__ __forceinline__ double sdth_c2(int l, int m) {
+    const double num = (double)(l + 1 + m) * (l + 1 - m), den = (double)(2 * l + 1) * (2 * l + 3);
+    return -l * sqrt(num / den);
+}
+
+__global__ void rlm_a_kernel(const double* __restrict__ s2a, double* __restrict__ s2o,
+                             const double* __restrict__ radial, long nlm, int nr, int L) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    const long lm = idx / nr;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const int lmax = L - 1;
+    const long fsz = 2L * nr;   // one field of one row
+    const long rsz = (long)NS2A * fsz;
+    auto get = [&](int f, int ll, int ri) -> double {
+        if (ll < m || ll >= lmax) return 0.0;   // l_max zeroed on entry (Sphere_Hybrid_Space.F90:73-75)
+        return s2a[row_index(m, ll, L) * rsz + f * fsz + r * 2 + ri];
+    };
+    const double orsq = radial[R_OVER_RHORSQ * nr + r];
+    const double orr = radial[R_OVER_RHOR * nr + r];
+    const double drho = radial[R_DRHO_TERM * nr + r];
+    const double two_r = radial[R_TWO_OVER_R * nr + r];
+    const double dlnrho = radial[R_DLNRHO * nr + r];
+    const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
+    const double llp1 = (double)l * (l + 1);
+    const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
+    const long orow = row_index(m, l, L) * (long)NP2A * fsz + r * 2;
+    double out[NP2A][2];
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const double sg = ri ? (double)m : -(double)m;   // d/dphi: (re, im) -> (-m im, m re)
+        const int rj = 1 - ri;
+        const double W = get(S_W, l, ri), T = get(S_T, l, ri), Z = get(S_Z, l, ri);
+        const double W1 = get(S_W1, l, ri), T1 = get(S_T1, l, ri);
+        const double vr = llp1 * W * orsq;
+        double dvrdr = llp1 * W1 * orsq;
+        dvrdr = dvrdr - vr * two_r;
+        dvrdr = dvrdr - vr * dlnrho;
+        const double vrm = llm * get(S_W, l - 1, ri) * orsq;
+        const double vrp = llq * get(S_W, l + 1, ri) * orsq;
+        const double dth_w1 = get(S_W1, l - 1, ri) * c1 + get(S_W1, l + 1, ri) * c2;
+        const double dth_z = get(S_Z, l - 1, ri) * c1 + get(S_Z, l + 1, ri) * c2;
+        const double dth_w2 = get(S_W2, l - 1, ri) * c1 + get(S_W2, l + 1, ri) * c2;
+        const double dth_z1 = get(S_Z1, l - 1, ri) * c1 + get(S_Z1, l + 1, ri) * c2;
+        const double vt = (dth_w1 + sg * get(S_Z, l, rj)) * orr;
+        const double vp = (sg * get(S_W1, l, rj) - dth_z) * orr;
+        double dvtdr = (dth_w2 + sg * get(S_Z1, l, rj)) * orr;
+        dvtdr = dvtdr - vt * drho;
+        double dvpdr = (sg * get(S_W2, l, rj) - dth_z1) * orr;
+        dvpdr = dvpdr - vp * drho;
+        out[A_VR][ri] = vr;
+        out[A_T][ri] = T;
+        out[A_OMR][ri] = llp1 * Z * orsq;
+        out[A_DVRDR][ri] = dvrdr;
+        out[A_DTDR][ri] = T1;
+        out[A_DVRDT][ri] = vrm * c1 + vrp * c2;
+        out[A_DTDT][ri] = get(S_T, l - 1, ri) * c1 + get(S_T, l + 1, ri) * c2;
+        out[A_VT][ri] = vt;
+        out[A_VP][ri] = vp;
+        out[A_DVTDR][ri] = dvtdr;
+        out[A_DVPDR][ri] = dvpdr;
+    }
+    const bool zero = (l == lmax);   // Sphere_Hybrid_Space.F90:100-102
+#pragma unroll
+    for (int f = 0; f < NP2A; ++f) {
+        double2 v = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
+        *reinterpret_cast<double2*>(s2o + orow + f * fsz) = v;
+    }
+}
+
+void launch_rlm_a(Ctx& c) {
+    const long total = c.d.nlm * c.d.nr;
+    rlm_a_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm,
+                                                                        c.d.nr, c.d.L);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// rlm_spaceb: curl algebra on the transformed NL terms, written l-major (p1b)
+// ---------------------------------------------------------------------------
+__global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict__ ab, long nlm, int nr, int L) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    const long lm = idx / nr;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const int lmax = L - 1;
+    const long fsz = 2L * nr, rsz = 4L * fsz;
+    auto get = [&](int f, int ll, int ri) -> double {
+        if (ll < m || ll > lmax) return 0.0;
+        return s2b[row_index(m, ll, L) * rsz + f * fsz + r * 2 + ri];
+    };
+    const double ollp1 = (l > 0) ? 1.0 / ((double)l * (l + 1)) : 1.0;
+    const double c1 = sdth_c1(l, m), c2 = sdth_c2(l, m);
+    const long plane = nlm * 2 * nr;
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const double sg = ri ? (double)m : -(double)m;
+        const int rj = 1 - ri;
+        double W = get(0, l, ri) * ollp1;
+        const double T = get(2, l, ri);
+        const double sd_z = get(3, l - 1, ri) * c1 + get(3, l + 1, ri) * c2;
+        const double sd_p = get(1, l - 1, ri) * c1 + get(1, l + 1, ri) * c2;
+        const double dphi_p = sg * get(1, l, rj);
+        const double dphi_z = sg * get(3, l, rj);
+        double Z = (dphi_p - sd_z) * ollp1;
+        double P = (sd_p + dphi_z) * ollp1;
+        double Tt = T;
+        if (l == 0) {   // m = 0 here: W, P and Z of l = 0 carry no RHS (:186-193)
+            W = 0.0;
+            P = 0.0;
+            Z = 0.0;
+        }
+        if (l == lmax) {   // :205-208
+            W = P = Tt = Z = 0.0;
+        }
+        const long o = (lm * 2 + ri) * nr + r;
+        ab[0 * plane + o] = W;
+        ab[1 * plane + o] = P;
+        ab[2 * plane + o] = Tt;
+        ab[3 * plane + o] = Z;
+    }
+}
+
+void launch_rlm_b(Ctx& c) {
+    const long total = c.d.nlm * c.d.nr;
+    rlm_b_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2b, c.d_ab, c.d.nlm, c.d.nr, c.d.L);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// AdvanceTime: b = rhs + new_ab * ab with boundary rows, x = A_l^{-1} b
+// tiles: (sys, l, mt, nt); sys 0 = W-P-T block (n = 3 nr), 1 = Z (n = nr)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(GEMM_THREADS) solve_kernel(const int4* __restrict__ tiles,
+                                                             const double* __restrict__ Awpt,
+                                                             const double* __restrict__ Az,
+                                                             const double* __restrict__ rhs_wpt,
+                                                             const double* __restrict__ rhs_z,
+                                                             const double* __restrict__ ab,
+                                                             double* __restrict__ sol_wpt,
+                                                             double* __restrict__ sol_z, long nlm, int nr,
+                                                             double new_ab, double bc_top, double bc_bot) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
+    const int4 tl = tiles[blockIdx.x];
+    const int sys = tl.x, l = tl.y, i0 = tl.z * BM, n0 = tl.w * BN;
+    const int n = sys ? nr : 3 * nr;
+    const int ncol = 2 * (l + 1);
+    const long lstart = (long)l * (l + 1) / 2;
+    const double* A = (sys ? Az : Awpt) + (long)l * n * n;
+    const double* rhs = sys ? rhs_z : rhs_wpt;
+    double* sol = sys ? sol_z : sol_wpt;
+    const long plane = nlm * 2 * nr;
+    Acc acc;
+    acc.zero();
+    auto fa = [&](int k, int x) -> double {
+        const int i = i0 + x;
+        return (k < n && i < n) ? __ldg(A + (long)i * n + k) : 0.0;
+    };
+    auto fb = [&](int k, int y) -> double {
+        const int cc = n0 + y;
+        if (k >= n || cc >= ncol) return 0.0;
+        const long col = lstart * 2 + cc;     // (lm, ri)
+        const int eq = sys ? 3 : k / nr;
+        const int r = sys ? k : k % nr;
+        if (r == 0 || r == nr - 1) {          // Apply_Boundary_Mask: only l = 0 T carries values
+            if (eq == 2 && col == 0) return (r == 0) ? bc_top : bc_bot;
+            return 0.0;
+        }
+        return rhs[col * n + k] + new_ab * ab[eq * plane + col * nr + r];
+    };
+    gemm_tile<false, false>(acc, fa, fb, n, sm);
+    acc_foreach(acc, [&](int x, int y, double v) {
+        const int i = i0 + x, cc = n0 + y;
+        if (i < n && cc < ncol) sol[(lstart * 2 + cc) * n + i] = v;
+    });
+}
+
+static std::vector<int> solve_tiles(int L, int nr) {
+    std::vector<int> t;
+    for (int sys = 0; sys < 2; ++sys) {
+        const int n = sys ? nr : 3 * nr;
+        for (int l = L - 1; l >= 0; --l) {
+            const int ncol = 2 * (l + 1);
+            for (int mt = 0; mt * BM < n; ++mt)
+                for (int nt = 0; nt * BN < ncol; ++nt) {
+                    t.push_back(sys);
+                    t.push_back(l);
+                    t.push_back(mt);
+                    t.push_back(nt);
+                }
+        }
+    }
+    return t;
+}
+
+void launch_solve(Ctx& c, double new_ab) {
+    if (!c.d_solve_tiles) {
+        std::vector<int> t = solve_tiles(c.d.L, c.d.nr);
+        c.n_solve_tiles = (int)(t.size() / 4);
+        RA_CUDA(cudaMalloc(&c.d_solve_tiles, t.size() * sizeof(int)));
+        RA_CUDA(cudaMemcpy(c.d_solve_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    const double s4pi = std::sqrt(4.0 * M_PI);
+    const double bc_top = (c.cfg.fix_tvar_top ? c.cfg.t_top : c.cfg.dtdr_top) * s4pi;
+    const double bc_bot = (c.cfg.fix_tvar_bottom ? c.cfg.t_bottom : c.cfg.dtdr_bottom) * s4pi;
+    solve_kernel<<<c.n_solve_tiles, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
+        reinterpret_cast<const int4*>(c.d_solve_tiles), c.d_Awpt, c.d_Az, c.d_rhs_wpt, c.d_rhs_z, c.d_ab,
+        c.d_sol_wpt, c.d_sol_z, c.d.nlm, c.d.nr, new_ab, bc_top, bc_bot);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// ---------------------------------------------------------------------------
+// In-place Gauss-Jordan inversion with partial (row) pivoting, one CTA per matrix.
+// status[mat] = 0 ok, 1 zero pivot.
+// ---------------------------------------------------------------------------
+constexpr int GJ_THREADS = 512;
+
+__global__ void __launch_bounds__(GJ_THREADS) gj_invert_kernel(double* __restrict__ mats, int n,
+                                                               const int* __restrict__ skip,
+                                                               int* __restrict__ status, int* __restrict__ piv_all) {
+    const int mat = blockIdx.x;
+    double* A = mats + (long)mat * n * n;
+    int* piv = piv_all + (long)mat * n;
+    extern __shared__ double gsm[];
+    double* rowk = gsm;           // n
+    double* colk = gsm + n;       // n
+    __shared__ double red_v[GJ_THREADS / 32];
+    __shared__ int red_i[GJ_THREADS / 32];
+    __shared__ int s_p;
+    __shared__ int s_bad;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (skip && skip[mat]) {      // identity (an equation that is not solved for this l)
+        for (long e = t; e < (long)n * n; e += blockDim.x) A[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+        if (t == 0) status[mat] = 0;
+        return;
+    }
+    if (t == 0) s_bad = 0;
+    for (int k = 0; k < n; ++k) {
+        // pivot search: max |A[i][k]|, i >= k (first index on ties, as IDAMAX)
+        double bv = -1.0;
+        int bi = n;
+        for (int i = k + t; i < n; i += blockDim.x) {
+            const double v = fabs(A[(long)i * n + k]);
+            if (v > bv) { bv = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[w] = bv; red_i[w] = bi; }
+        __syncthreads();
+        if (t == 0) {
+            double v = red_v[0];
+            int ii = red_i[0];
+            for (int q = 1; q < (int)(blockDim.x / 32); ++q)
+                if (red_v[q] > v || (red_v[q] == v && red_i[q] < ii)) { v = red_v[q]; ii = red_i[q]; }
+            s_p = ii;
+            piv[k] = ii;
+            if (!(v > 0.0)) s_bad = 1;
+        }
+        __syncthreads();
+        const int p = s_p;
+        if (s_bad) break;
+        if (p != k) {
+            for (int j = t; j < n; j += blockDim.x) {
+                const double a = A[(long)k * n + j], b = A[(long)p * n + j];
+                A[(long)k * n + j] = b;
+                A[(long)p * n + j] = a;
+            }
+            __syncthreads();
+        }
+        const double inv = 1.0 / A[(long)k * n + k];
+        __syncthreads();
+        for (int j = t; j < n; j += blockDim.x) {
+            const double v = (j == k) ? inv : A[(long)k * n + j] * inv;
+            rowk[j] = v;
+            A[(long)k * n + j] = v;
+            colk[j] = A[(long)j * n + k];
+        }
+        __syncthreads();
+        // eliminate column k from every other row
+        for (long e = t; e < (long)n * n; e += blockDim.x) {
+            const int i = (int)(e / n), j = (int)(e % n);
+            if (i == k) continue;
+            const double f = colk[i];
+            if (j == k) A[e] = -f * rowk[k];
+            else A[e] = A[e] - f * rowk[j];
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (t == 0) status[mat] = 1;
+        return;
+    }
+    // undo the row interchanges as column interchanges, in reverse order
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k) {
+            for (int i = t; i < n; i += blockDim.x) {
+                const double a = A[(long)i * n + k], b = A[(long)i * n + p];
+                A[(long)i * n + k] = b;
+                A[(long)i * n + p] = a;
+            }
+        }
+        __syncthreads();
+    }
+    if (t == 0) status[mat] = 0;
+}
+
+int invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip_h) {
+    int *d_status = nullptr, *d_piv = nullptr, *d_skip = nullptr;
+    RA_CUDA(cudaMalloc(&d_status, count * sizeof(int)));
+    RA_CUDA(cudaMalloc(&d_piv, (long)count * n * sizeof(int)));
+    if (skip_h) {
+        RA_CUDA(cudaMalloc(&d_skip, count * sizeof(int)));
+        RA_CUDA(cudaMemcpyAsync(d_skip, skip_h, count * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    }
+    gj_invert_kernel<<<count, GJ_THREADS, 2 * n * sizeof(double), c.stream>>>(d_mats, n, d_skip, d_status, d_piv);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+    std::vector<int> st(count);
+    RA_CUDA(cudaMemcpyAsync(st.data(), d_status, count * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(d_status);
+    cudaFree(d_piv);
+    if (d_skip) cudaFree(d_skip);
+    for (int i = 0; i < count; ++i)
+        if (st[i]) return i + 1;
+    return 0;
+}
+
+}  // namespace ra

@@ -1,0 +1,860 @@
+// C ABI, context set-up and step orchestration of librayleigh_b200.
+//
+// Set-up restates the reference's initialisation of the path:
+//   grid sizes                 ProblemSize.F90:334-464
+//   Gauss-Legendre nodes       Legendre_Polynomials.F90:332-393 (in long double)
+//   Chebyshev grid/matrices    Chebyshev_Polynomials.F90:65-351
+//   Boussinesq reference state PDE_Coefficients.F90:335-435
+//   implicit matrices + BCs    Sphere_Linear_Terms.F90:196-1100, Linear_Solve.F90:494-539,1459-1522
+// Host work here is configuration-time only (O(n_r^2 l_max) matrix entries);
+// every per-step operation runs on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "ra_internal.h"
+
+using namespace ra;
+
+struct ra_ctx {
+    Ctx c;
+};
+
+namespace ra {
+
+static void check_config(const ra_config& cfg) {
+    if (cfg.n_r < 8 || (cfg.n_r & 1)) throw ArgError("n_r must be even and >= 8");
+    if (cfg.l_max < 3) throw ArgError("l_max must be >= 3");
+    if (cfg.magnetism) throw ArgError("magnetism is not supported: the hydrodynamic equation set only");
+    if (!(cfg.aspect_ratio > 0 && cfg.aspect_ratio < 1)) throw ArgError("aspect_ratio must lie in (0, 1)");
+    if (!(cfg.shell_depth > 0)) throw ArgError("shell_depth must be positive");
+    if (!(cfg.dt > 0)) throw ArgError("dt must be positive");
+    if (cfg.precision != RA_PREC_FP64 && cfg.precision != RA_PREC_MIXED) throw ArgError("unknown precision mode");
+}
+
+static Dims make_dims(const ra_config& cfg) {
+    Dims d{};
+    d.lmax = cfg.l_max;
+    d.L = cfg.l_max + 1;
+    d.nth = cfg.n_theta > 0 ? cfg.n_theta : (3 * (cfg.l_max + 1)) / 2;
+    if (d.nth & 1) throw ArgError("n_theta must be even");
+    if (d.nth < d.L) throw ArgError("n_theta must be >= l_max + 1");
+    d.nth2 = d.nth / 2;
+    d.nphi = 2 * d.nth;
+    d.nr = cfg.n_r;
+    d.nlm = (long)d.L * (d.L + 1) / 2;
+    d.rda = (2 * d.nr) / 3 + 1;
+    d.kc = d.rda - 1;
+    return d;
+}
+
+// Find_Colocation + nth_legendre (Legendre_Polynomials.F90:332-393) in long double.
+static void gauss_legendre(int n, std::vector<long double>& x, std::vector<long double>& w) {
+    x.assign(n, 0.0L);
+    w.assign(n, 0.0L);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    const long double eps = 3e-14L;
+    for (int i = 1; i <= (n + 1) / 2; ++i) {
+        long double root = cosl(PI * (i - 0.25L) / (n + 0.5L));
+        for (int it = 0; it < 100; ++it) {
+            long double pn = 1.0L, pm1 = 0.0L;
+            for (int j = 1; j <= n; ++j) {
+                const long double pm2 = pm1;
+                pm1 = pn;
+                pn = ((2.0L * j - 1.0L) * root * pm1 - (j - 1.0L) * pm2) / j;
+            }
+            const long double dpn = n * (root * pn - pm1) / (root * root - 1.0L);
+            const long double nw = root - pn / dpn;
+            const long double del = fabsl(root - nw);
+            root = nw;
+            x[i - 1] = -root;
+            x[n - i] = root;
+            w[i - 1] = 2.0L / ((1.0L - root * root) * dpn * dpn);
+            w[n - i] = w[i - 1];
+            if (del <= eps) break;
+        }
+    }
+}
+
+// Chebyshev collocation grid and derivative matrices dcheby(r, n, d), d = 0..3
+// (Chebyshev_Polynomials.F90:65-351; single domain, zeros of T_N).
+static void chebyshev_setup(Ctx& c, double rmin, double rmax) {
+    const int n = c.d.nr;
+    std::vector<double> theta(n), x(n);
+    const double dth = M_PI / n;
+    double arg = dth * 0.5;
+    for (int i = 0; i < n; ++i) {   // accumulated as in Gen_Colocation_Points
+        theta[i] = arg;
+        x[i] = cos(arg);
+        arg = arg + dth;
+    }
+    std::vector<double> alpha((size_t)n * n, 0.0);
+    alpha[(size_t)(n - 2) * n + (n - 1)] = 2.0 * (n - 1);
+    for (int k = n - 3; k >= 0; --k) {
+        alpha[(size_t)k * n + k + 1] = 2.0 * (k + 1);
+        for (int j = 0; j < n; ++j) alpha[(size_t)k * n + j] += alpha[(size_t)(k + 2) * n + j];
+    }
+    c.cheb_D.assign((size_t)4 * n * n, 0.0);
+    double* D0 = c.cheb_D.data();
+    for (int r = 0; r < n; ++r)
+        for (int k = 0; k < n; ++k) D0[(size_t)r * n + k] = cos(k * theta[r]);
+    for (int r = 0; r < n; ++r) D0[(size_t)r * n] -= 0.5;
+    for (int d = 1; d < 4; ++d) {
+        const double* Dp = c.cheb_D.data() + (size_t)(d - 1) * n * n;
+        double* Dd = c.cheb_D.data() + (size_t)d * n * n;
+        for (int r = 0; r < n; ++r)
+            for (int j = 0; j < n; ++j) {
+                double s = 0.0;
+                for (int i = 0; i < n; ++i) s += Dp[(size_t)r * n + i] * alpha[(size_t)i * n + j];
+                Dd[(size_t)r * n + j] = s;
+            }
+    }
+    const double xmin = x[n - 1], xmax = x[0];
+    double scaling = (rmax - rmin) / (xmax - xmin);
+    c.rad.radius.resize(n);
+    for (int i = 0; i < n; ++i) c.rad.radius[i] = (x[i] - xmin) * scaling + rmin;
+    scaling = 1.0 / scaling;
+    c.deriv_scaling = scaling;
+    for (int d = 1; d < 4; ++d) {
+        const double s = pow(scaling, d);
+        double* Dd = c.cheb_D.data() + (size_t)d * n * n;
+        for (size_t e = 0; e < (size_t)n * n; ++e) Dd[e] *= s;
+    }
+}
+
+// Boussinesq reference state and transport coefficients (PDE_Coefficients.F90:335-435, 1766-2098).
+static void reference_setup(Ctx& c) {
+    const ra_config& cfg = c.cfg;
+    const int n = c.d.nr;
+    Radial& R = c.rad;
+    const std::vector<double>& r = R.radius;
+    R.delta_r.resize(n);
+    R.delta_r[0] = r[0] - r[1];
+    for (int i = 1; i < n; ++i) R.delta_r[i] = r[i - 1] - r[i];
+    R.density.assign(n, 1.0);
+    R.dlnrho.assign(n, 0.0);
+    R.buoy.resize(n);
+    for (int i = 0; i < n; ++i) R.buoy[i] = (cfg.rayleigh / cfg.prandtl) * pow(r[i] / r[0], cfg.gravity_power);
+    const double pscaling = cfg.rotation ? 1.0 / cfg.ekman : 1.0;
+    R.dpdr_w.resize(n);
+    R.pdwdr.resize(n);
+    for (int i = 0; i < n; ++i) {
+        R.dpdr_w[i] = R.density[i] * pscaling;
+        R.pdwdr[i] = -1.0 * R.density[i] * pscaling;
+    }
+    R.coriolis = 2.0 / cfg.ekman;
+    R.nu.assign(n, 1.0);
+    R.kappa.assign(n, 1.0 / cfg.prandtl);
+}
+
+// One l of the implicit system: LHS (row-major) and the Post_Solve RHS coefficients.
+static void build_l(const Ctx& c, int l, std::vector<double>& A, std::vector<double>& Z, double* coef) {
+    const int nr = c.d.nr, n3 = 3 * nr, rda = c.d.rda;
+    const ra_config& cfg = c.cfg;
+    const Radial& R = c.rad;
+    const std::vector<double>& r = R.radius;
+    const double dt = c.dt, al = cfg.alpha_implicit;
+    const double lf = -dt * al, rf = dt * (1.0 - al);
+    const double* D = c.cheb_D.data();
+    A.assign((size_t)n3 * n3, 0.0);
+    Z.assign((size_t)nr * nr, 0.0);
+    std::fill(coef, coef + (size_t)NSLOT * nr, 0.0);
+    // slot lookup for (eq, var, d); var/d given as the grid source
+    auto slot_of = [&](int eq, int var, int d) -> int {
+        static const int gsrc[4][4] = {{G_W0, G_W1, G_W2, G_W3}, {G_P0, G_P1, -1, -1},
+                                       {G_T0, G_T1, G_T2, -1}, {G_Z0, G_Z1, G_Z2, -1}};
+        const int gs = gsrc[var][d];
+        for (int s = 0; s < NSLOT; ++s)
+            if (kSlots[s].eq == eq && kSlots[s].g == gs) return s;
+        return -1;
+    };
+    // Add_Implicit_Term: LHS += amp*(static ? 1 : lf)*D_d in rows of eq, columns of var;
+    // Post_Solve coefficient += amp*(static ? 1 : rf)
+    auto add = [&](int eq, int var, int d, const std::vector<double>& amp, bool stat) {
+        const int s = slot_of(eq, var, d);
+        if (s >= 0)
+            for (int i = 0; i < nr; ++i) coef[(size_t)s * nr + i] += stat ? amp[i] : amp[i] * rf;
+        const double fac = stat ? 1.0 : lf;
+        const double* Dd = D + (size_t)d * nr * nr;
+        if (eq == EQ_Z) {
+            for (int i = 0; i < nr; ++i)
+                for (int j = 0; j < nr; ++j) Z[(size_t)i * nr + j] += amp[i] * fac * Dd[(size_t)i * nr + j];
+        } else {
+            const int rb = eq * nr, cb = var * nr;
+            for (int i = 0; i < nr; ++i)
+                for (int j = 0; j < nr; ++j)
+                    A[(size_t)(rb + i) * n3 + cb + j] += amp[i] * fac * Dd[(size_t)i * nr + j];
+        }
+    };
+    std::vector<double> ones(nr, 1.0), zero(nr, 0.0), v(nr);
+    const double llp1 = (double)l * (l + 1);
+    std::vector<double> H(nr);
+    for (int i = 0; i < nr; ++i) H[i] = -llp1 / (r[i] * r[i]);
+    auto vec = [&](auto f) {
+        for (int i = 0; i < nr; ++i) v[i] = f(i);
+        return v;
+    };
+    const int W_ = 0, P_ = 1, T_ = 2, Z_ = 3;
+    if (l == 0) {
+        add(EQ_T, T_, 0, ones, true);
+        add(EQ_T, T_, 1, vec([&](int i) { return 2.0 / r[i] * R.kappa[i]; }), false);
+        add(EQ_T, T_, 2, vec([&](int i) { return 1.0 * R.kappa[i]; }), false);
+        add(EQ_T, T_, 1, zero, false);
+        add(EQ_P, T_, 0, vec([&](int i) { return -R.buoy[i]; }), true);
+        add(EQ_P, P_, 1, R.dpdr_w, true);
+        add(EQ_W, W_, 0, ones, true);
+    } else {
+        add(EQ_W, T_, 0, vec([&](int i) { return -R.buoy[i] / H[i]; }), false);
+        add(EQ_W, P_, 1, vec([&](int i) { return R.dpdr_w[i] / H[i]; }), false);
+        add(EQ_W, W_, 0, ones, true);
+        add(EQ_W, W_, 0, vec([&](int i) { return H[i] * R.nu[i]; }), false);
+        add(EQ_W, W_, 2, R.nu, false);
+        add(EQ_W, W_, 0, zero, false);
+        add(EQ_W, W_, 1, zero, false);
+        add(EQ_P, P_, 0, R.pdwdr, false);
+        add(EQ_P, W_, 1, ones, true);
+        add(EQ_P, W_, 0, vec([&](int i) { return -R.nu[i] * H[i] * 2.0 / r[i]; }), false);
+        add(EQ_P, W_, 1, vec([&](int i) { return H[i] * R.nu[i]; }), false);
+        add(EQ_P, W_, 3, R.nu, false);
+        add(EQ_P, W_, 0, zero, false);
+        add(EQ_P, W_, 1, zero, false);
+        add(EQ_P, W_, 2, zero, false);
+        add(EQ_T, T_, 0, ones, true);
+        add(EQ_T, T_, 0, vec([&](int i) { return H[i] * R.kappa[i]; }), false);
+        add(EQ_T, T_, 1, vec([&](int i) { return 2.0 / r[i] * R.kappa[i]; }), false);
+        add(EQ_T, T_, 2, R.kappa, false);
+        add(EQ_T, T_, 1, zero, false);
+        add(EQ_Z, Z_, 0, ones, true);
+        add(EQ_Z, Z_, 0, vec([&](int i) { return H[i] * R.nu[i]; }), false);
+        add(EQ_Z, Z_, 2, R.nu, false);
+        add(EQ_Z, Z_, 0, zero, false);
+        add(EQ_Z, Z_, 1, zero, false);
+    }
+    // Set_Boundary_Conditions (Sphere_Linear_Terms.F90:539-1100):
+    // clear boundary rows, then Load_Single_Row_Cheby over the dealiased columns
+    auto clear = [&](std::vector<double>& M, int ncols, int row) {
+        std::fill(M.begin() + (size_t)row * ncols, M.begin() + (size_t)(row + 1) * ncols, 0.0);
+    };
+    auto bc = [&](std::vector<double>& M, int ncols, int row, int col0, int d, double amp) {
+        const double* Dd = D + (size_t)d * nr * nr;
+        const int rr = row % nr;
+        for (int j = 0; j < rda - 1; ++j) M[(size_t)row * ncols + col0 + j] += amp * Dd[(size_t)rr * nr + j];
+    };
+    const int top = 0, bot = nr - 1;
+    if (l == 0) {
+        clear(A, n3, nr + top);
+        clear(A, n3, 2 * nr + top);
+        clear(A, n3, 2 * nr + bot);
+        bc(A, n3, 2 * nr + top, 2 * nr, cfg.fix_tvar_top ? 0 : 1, 1.0);
+        bc(A, n3, 2 * nr + bot, 2 * nr, cfg.fix_tvar_bottom ? 0 : 1, 1.0);
+        bc(A, n3, nr + top, nr, 0, 1.0);   // pressure node at the top
+    } else {
+        for (int rb = 0; rb < n3; rb += nr) {
+            clear(A, n3, rb + top);
+            clear(A, n3, rb + bot);
+        }
+        clear(Z, nr, top);
+        clear(Z, nr, bot);
+        bc(A, n3, 2 * nr + top, 2 * nr, cfg.fix_tvar_top ? 0 : 1, 1.0);
+        bc(A, n3, 2 * nr + bot, 2 * nr, cfg.fix_tvar_bottom ? 0 : 1, 1.0);
+        bc(A, n3, top, 0, 0, 1.0);   // impenetrable: W = 0
+        bc(A, n3, bot, 0, 0, 1.0);
+        if (cfg.no_slip_top) {
+            bc(Z, nr, top, 0, 0, 1.0);
+            bc(A, n3, nr + top, 0, 1, 1.0);
+        } else {
+            const double samp = -(2.0 / r[top] + R.dlnrho[top]);
+            bc(A, n3, nr + top, 0, 2, 1.0);
+            bc(A, n3, nr + top, 0, 1, samp);
+            bc(Z, nr, top, 0, 1, 1.0);
+            bc(Z, nr, top, 0, 0, samp);
+        }
+        if (cfg.no_slip_bottom) {
+            bc(A, n3, nr + bot, 0, 1, 1.0);
+            bc(Z, nr, bot, 0, 0, 1.0);
+        } else {
+            const double samp = -(2.0 / r[bot] + R.dlnrho[bot]);
+            bc(A, n3, nr + bot, 0, 2, 1.0);
+            bc(A, n3, nr + bot, 0, 1, samp);
+            bc(Z, nr, bot, 0, 1, 1.0);
+            bc(Z, nr, bot, 0, 0, samp);
+        }
+    }
+}
+
+// Reset_Linear_Equations: build every l, upload, invert on the device.
+static void linear_setup(Ctx& c) {
+    const int L = c.d.L, nr = c.d.nr, n3 = 3 * nr;
+    std::vector<double> coef((size_t)L * NSLOT * nr);
+    std::vector<double> Aall((size_t)L * n3 * n3), Zall((size_t)L * nr * nr);
+    std::vector<double> A, Z;
+    for (int l = 0; l < L; ++l) {
+        build_l(c, l, A, Z, coef.data() + (size_t)l * NSLOT * nr);
+        std::copy(A.begin(), A.end(), Aall.begin() + (size_t)l * n3 * n3);
+        std::copy(Z.begin(), Z.end(), Zall.begin() + (size_t)l * nr * nr);
+    }
+    RA_CUDA(cudaMemcpyAsync(c.d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_Awpt, Aall.data(), Aall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_Az, Zall.data(), Zall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    int bad = invert_matrices(c, c.d_Awpt, n3, L, nullptr);
+    if (bad) throw ArgError("singular W-P-T matrix at l = " + std::to_string(bad - 1));
+    std::vector<int> skip(L, 0);
+    skip[0] = 1;   // Z is not solved for at l = 0 (Sphere_Linear_Terms.F90:116-150)
+    bad = invert_matrices(c, c.d_Az, nr, L, skip.data());
+    if (bad) throw ArgError("singular Z matrix at l = " + std::to_string(bad - 1));
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+template <class T>
+static void dalloc(T*& p, size_t count) {
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc", __FILE__, __LINE__);
+}
+
+static void setup(Ctx& c) {
+    const Dims& d = c.d;
+    RA_CUDA(cudaSetDevice(c.cfg.device));
+    RA_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.dt = c.cfg.dt;
+    c.old_dt = c.cfg.dt;
+    const double rmax = c.cfg.shell_depth / (1.0 - c.cfg.aspect_ratio);
+    const double rmin = rmax * c.cfg.aspect_ratio;
+    chebyshev_setup(c, rmin, rmax);
+    reference_setup(c);
+    // horizontal grid
+    std::vector<long double> xq, wq;
+    gauss_legendre(d.nth, xq, wq);
+    c.costheta_h.resize(d.nth);
+    for (int i = 0; i < d.nth; ++i) c.costheta_h[i] = (double)xq[i];
+    std::vector<double> xs(2 * d.nth2), w2(d.nth2);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < d.nth2; ++i) {
+        xs[i] = (double)xq[i];
+        xs[d.nth2 + i] = (double)sqrtl((1.0L - xq[i]) * (1.0L + xq[i]));
+        w2[i] = (double)(2.0L * PI * wq[i]);
+    }
+    // trig tables as the reference computes them in double (ProblemSize.F90:489-495)
+    std::vector<double> trig(4 * (size_t)d.nth);
+    for (int i = 0; i < d.nth; ++i) {
+        const double ct = c.costheta_h[i];
+        const double s2 = 1.0 - ct * ct;
+        const double st = sqrt(s2);
+        trig[i] = ct;
+        trig[d.nth + i] = st;
+        trig[2 * d.nth + i] = 1.0 / st;
+        trig[3 * d.nth + i] = ct / st;
+    }
+    std::vector<double> twid(2 * (size_t)d.nth);
+    for (int k = 0; k < d.nth; ++k) {
+        const long double a = 2.0L * PI * k / (long double)d.nphi;
+        twid[2 * k] = (double)cosl(a);
+        twid[2 * k + 1] = (double)sinl(a);
+    }
+    // radial profiles
+    const int nr = d.nr;
+    std::vector<double> rp((size_t)R_COUNT * nr);
+    for (int i = 0; i < nr; ++i) {
+        const double r = c.rad.radius[i];
+        const double oor = 1.0 / r;
+        const double oor2 = 1.0 / (r * r);
+        rp[R_RADIUS * nr + i] = r;
+        rp[R_OVER_R * nr + i] = oor;
+        rp[R_DELTA_R * nr + i] = c.rad.delta_r[i];
+        rp[R_DENSITY * nr + i] = c.rad.density[i];
+        rp[R_DLNRHO * nr + i] = c.rad.dlnrho[i];
+        rp[R_OVER_RHOR * nr + i] = oor / c.rad.density[i];
+        rp[R_OVER_RHORSQ * nr + i] = oor2 / c.rad.density[i];
+        rp[R_DRHO_TERM * nr + i] = c.rad.dlnrho[i] + oor;
+        rp[R_TWO_OVER_R * nr + i] = 2.0 / r;
+    }
+    // device buffers
+    const long nlm = d.nlm;
+    dalloc(c.d_Ptab, (size_t)nlm * d.nth2);
+    dalloc(c.d_iPtab, (size_t)nlm * d.nth2);
+    dalloc(c.d_D, c.cheb_D.size());
+    dalloc(c.d_coef, (size_t)d.L * NSLOT * nr);
+    dalloc(c.d_radial, rp.size());
+    dalloc(c.d_costh, trig.size());
+    dalloc(c.d_twid, twid.size());
+    dalloc(c.d_Awpt, (size_t)d.L * 9 * nr * nr);
+    dalloc(c.d_Az, (size_t)d.L * nr * nr);
+    dalloc(c.d_sol_wpt, (size_t)nlm * 2 * 3 * nr);
+    dalloc(c.d_sol_z, (size_t)nlm * 2 * nr);
+    dalloc(c.d_rhs_wpt, (size_t)nlm * 2 * 3 * nr);
+    dalloc(c.d_rhs_z, (size_t)nlm * 2 * nr);
+    dalloc(c.d_ab, (size_t)4 * nlm * 2 * nr);
+    dalloc(c.d_g, (size_t)NG * nlm * 2 * nr);
+    dalloc(c.d_s2a, (size_t)nlm * NS2A * 2 * nr);
+    dalloc(c.d_s2a11, (size_t)nlm * NP2A * 2 * nr);
+    dalloc(c.d_p2a, (size_t)d.L * d.nth * NP2A * 2 * nr);
+    dalloc(c.d_p2b, (size_t)d.L * d.nth * NP2B * 2 * nr);
+    dalloc(c.d_s2b, (size_t)nlm * NP2B * 2 * nr);
+    dalloc(c.d_cfl, 1);
+    RA_CUDA(cudaMemsetAsync(c.d_ab, 0, (size_t)4 * nlm * 2 * nr * sizeof(double), c.stream));
+    RA_CUDA(cudaMemsetAsync(c.d_sol_wpt, 0, (size_t)nlm * 2 * 3 * nr * sizeof(double), c.stream));
+    RA_CUDA(cudaMemsetAsync(c.d_sol_z, 0, (size_t)nlm * 2 * nr * sizeof(double), c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_D, c.cheb_D.data(), c.cheb_D.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_radial, rp.data(), rp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_costh, trig.data(), trig.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_twid, twid.data(), twid.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    double *d_x = nullptr, *d_w = nullptr;
+    dalloc(d_x, xs.size());
+    dalloc(d_w, w2.size());
+    RA_CUDA(cudaMemcpyAsync(d_x, xs.data(), xs.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(d_w, w2.data(), w2.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    launch_plm(c, d_x, d_w);
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(d_x);
+    cudaFree(d_w);
+    // kernels that need more than 48 KB of dynamic shared memory
+    linear_setup(c);
+}
+
+static void release(Ctx& c) {
+    if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_Awpt, c.d_Az,
+                      c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
+                      c.d_p2a, c.d_p2b, c.d_s2b};
+    for (double* b : bufs)
+        if (b) cudaFree(b);
+    int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status};
+    for (int* b : ibufs)
+        if (b) cudaFree(b);
+    if (c.d_cfl) cudaFree(c.d_cfl);
+    if (c.stream) cudaStreamDestroy(c.stream);
+}
+
+// AB2 factors (Sphere_Spectral_Space.F90:204-211)
+static void ab_factors(const Ctx& c, double& new_ab, double& old_ab) {
+    if (c.iteration == 1) {
+        new_ab = c.dt;
+        old_ab = 0.0;
+    } else {
+        new_ab = 0.5 * c.dt * (2.0 + c.dt / c.old_dt);
+        old_ab = -0.5 * c.dt * c.dt / c.old_dt;
+    }
+}
+
+static void enqueue_step(Ctx& c, double new_ab, double old_ab) {
+    launch_cheb_synthesis(c);
+    launch_post_assemble(c, old_ab);
+    launch_rlm_a(c);
+    launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
+    RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
+    launch_physics(c);
+    launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+    launch_rlm_b(c);
+    launch_solve(c, new_ab);
+}
+
+static void run_steps(Ctx& c, int nsteps, double* cfl) {
+    if (!c.have_state) throw ArgError("ra_put_state must be called before stepping");
+    for (int s = 0; s < nsteps; ++s) {
+        double new_ab, old_ab;
+        ab_factors(c, new_ab, old_ab);
+        const bool graphable = c.cfg.use_graph && c.iteration > 1;
+        if (graphable) {
+            if (c.graph_exec && (c.graph_new_ab != new_ab || c.graph_old_ab != old_ab)) {
+                cudaGraphExecDestroy(c.graph_exec);
+                cudaGraphDestroy(c.graph);
+                c.graph_exec = nullptr;
+                c.graph = nullptr;
+            }
+            if (!c.graph_exec) {
+                const long before = c.launches;
+                RA_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+                enqueue_step(c, new_ab, old_ab);
+                RA_CUDA(cudaStreamEndCapture(c.stream, &c.graph));
+                RA_CUDA(cudaGraphInstantiate(&c.graph_exec, c.graph, 0));
+                c.graph_new_ab = new_ab;
+                c.graph_old_ab = old_ab;
+                c.launches = before;
+            }
+            RA_CUDA(cudaGraphLaunch(c.graph_exec, c.stream));
+            c.launches += 8;
+        } else {
+            enqueue_step(c, new_ab, old_ab);
+        }
+        c.old_dt = c.dt;
+        ++c.iteration;
+    }
+    if (cfl) {
+        unsigned long long bits = 0;
+        RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        double v;
+        std::memcpy(&v, &bits, sizeof(v));
+        *cfl = v;
+    }
+}
+
+}  // namespace ra
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+template <class F>
+static int guarded(ra_ctx* ctx, F f) {
+    try {
+        f();
+        return RA_OK;
+    } catch (const ArgError& e) {
+        if (ctx) ctx->c.err = e.what;
+        return RA_ERR_ARG;
+    } catch (const CudaError& e) {
+        if (ctx) ctx->c.err = e.what;
+        return e.code == cudaErrorMemoryAllocation ? RA_ERR_NOMEM : RA_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->c.err = "host allocation failed";
+        return RA_ERR_NOMEM;
+    }
+}
+
+extern "C" {
+
+int ra_default_config(ra_config* cfg) {
+    if (!cfg) return RA_ERR_ARG;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->n_r = 48;
+    cfg->l_max = 63;
+    cfg->n_theta = 0;
+    cfg->aspect_ratio = 0.35;
+    cfg->shell_depth = 1.0;
+    cfg->rayleigh = 1.0e5;
+    cfg->ekman = 1.0e-3;
+    cfg->prandtl = 1.0;
+    cfg->magnetic_prandtl = 1.0;
+    cfg->gravity_power = 1.0;
+    cfg->rotation = 1;
+    cfg->magnetism = 0;
+    cfg->no_slip_top = cfg->no_slip_bottom = 1;
+    cfg->fix_tvar_top = cfg->fix_tvar_bottom = 1;
+    cfg->t_top = 0.0;
+    cfg->t_bottom = 1.0;
+    cfg->dt = 1.0e-4;
+    cfg->alpha_implicit = 0.5;
+    cfg->precision = RA_PREC_FP64;
+    cfg->use_graph = 1;
+    cfg->device = 0;
+    return RA_OK;
+}
+
+int ra_create(ra_ctx** out, const ra_config* cfg) {
+    if (!out || !cfg) return RA_ERR_ARG;
+    *out = nullptr;
+    ra_ctx* ctx = new (std::nothrow) ra_ctx();
+    if (!ctx) return RA_ERR_NOMEM;
+    int rc = guarded(ctx, [&] {
+        check_config(*cfg);
+        ctx->c.cfg = *cfg;
+        ctx->c.d = make_dims(*cfg);
+        setup(ctx->c);
+    });
+    if (rc != RA_OK) {
+        // keep the context so the caller can read the message, but free device memory
+        release(ctx->c);
+        Ctx fresh;
+        fresh.err = ctx->c.err;
+        ctx->c = fresh;
+    }
+    *out = ctx;
+    return rc;
+}
+
+int ra_destroy(ra_ctx* ctx) {
+    if (!ctx) return RA_OK;
+    release(ctx->c);
+    delete ctx;
+    return RA_OK;
+}
+
+int ra_last_error(const ra_ctx* ctx, char* msg, int len) {
+    if (!ctx || !msg || len <= 0) return RA_ERR_ARG;
+    std::strncpy(msg, ctx->c.err.c_str(), (size_t)len - 1);
+    msg[len - 1] = 0;
+    return RA_OK;
+}
+
+int ra_sizes(const ra_ctx* ctx, long* n_lm, int* n_r, int* n_theta, int* n_phi) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (n_lm) *n_lm = ctx->c.d.nlm;
+    if (n_r) *n_r = ctx->c.d.nr;
+    if (n_theta) *n_theta = ctx->c.d.nth;
+    if (n_phi) *n_phi = ctx->c.d.nphi;
+    return RA_OK;
+}
+
+int ra_set_dt(ra_ctx* ctx, double dt) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        if (!(dt > 0)) throw ArgError("dt must be positive");
+        ctx->c.dt = dt;
+        linear_setup(ctx->c);
+    });
+}
+
+int ra_put_state(ra_ctx* ctx, const double* wpt, const double* z, const double* ab, int iteration) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!wpt || !z) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const size_t nw = (size_t)c.d.nlm * 2 * 3 * c.d.nr, nz = (size_t)c.d.nlm * 2 * c.d.nr;
+        RA_CUDA(cudaMemcpyAsync(c.d_sol_wpt, wpt, nw * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(c.d_sol_z, z, nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        if (ab) RA_CUDA(cudaMemcpyAsync(c.d_ab, ab, 4 * nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        else RA_CUDA(cudaMemsetAsync(c.d_ab, 0, 4 * nz * sizeof(double), c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        c.iteration = iteration > 0 ? iteration : 1;
+        c.have_state = true;
+    });
+}
+
+int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const size_t nw = (size_t)c.d.nlm * 2 * 3 * c.d.nr, nz = (size_t)c.d.nlm * 2 * c.d.nr;
+        if (wpt) RA_CUDA(cudaMemcpyAsync(wpt, c.d_sol_wpt, nw * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (z) RA_CUDA(cudaMemcpyAsync(z, c.d_sol_z, nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (ab) RA_CUDA(cudaMemcpyAsync(ab, c.d_ab, 4 * nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int ra_step(ra_ctx* ctx, int nsteps, double* cfl) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (nsteps < 0) return RA_ERR_ARG;
+    int rc = guarded(ctx, [&] {
+        ctx->c.launches = 0;
+        run_steps(ctx->c, nsteps, cfl);
+    });
+    if (rc == RA_ERR_ARG && !ctx->c.have_state) return RA_ERR_STATE;
+    return rc;
+}
+
+int ra_post_solve(ra_ctx* ctx) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        double n, o;
+        ab_factors(ctx->c, n, o);
+        launch_cheb_synthesis(ctx->c);
+        launch_post_assemble(ctx->c, o);
+    });
+}
+
+int ra_rlm_a(ra_ctx* ctx) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        launch_rlm_a(ctx->c);
+        launch_lt_inverse(ctx->c, ctx->c.d_s2a11, ctx->c.d_p2a, NP2A * ctx->c.d.nr * 2);
+    });
+}
+
+int ra_physical(ra_ctx* ctx, double* cfl) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
+        launch_physics(c);
+        if (cfl) {
+            unsigned long long bits = 0;
+            RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));
+            std::memcpy(cfl, &bits, sizeof(double));
+        }
+    });
+}
+
+int ra_rlm_b(ra_ctx* ctx) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        launch_lt_forward(ctx->c, ctx->c.d_p2b, ctx->c.d_s2b, NP2B * ctx->c.d.nr * 2);
+        launch_rlm_b(ctx->c);
+    });
+}
+
+int ra_advance(ra_ctx* ctx) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        double n, o;
+        ab_factors(ctx->c, n, o);
+        launch_solve(ctx->c, n);
+        ctx->c.old_dt = ctx->c.dt;
+        ++ctx->c.iteration;
+    });
+}
+
+int ra_sync(ra_ctx* ctx) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] { RA_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+
+long ra_launch_count(const ra_ctx* ctx) { return ctx ? ctx->c.launches : -1; }
+
+int ra_debug_buffer(ra_ctx* ctx, int which, double* out, long n, long* n_out) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const long nlm = c.d.nlm, nr = c.d.nr, L = c.d.L, nth = c.d.nth;
+        const double* src = nullptr;
+        long size = 0;
+        switch (which) {
+            case RA_BUF_GRID: src = c.d_g; size = NG * nlm * 2 * nr; break;
+            case RA_BUF_S2A: src = c.d_s2a; size = nlm * NS2A * 2 * nr; break;
+            case RA_BUF_S2A11: src = c.d_s2a11; size = nlm * NP2A * 2 * nr; break;
+            case RA_BUF_P2A: src = c.d_p2a; size = L * nth * NP2A * 2 * nr; break;
+            case RA_BUF_P2B: src = c.d_p2b; size = L * nth * NP2B * 2 * nr; break;
+            case RA_BUF_S2B: src = c.d_s2b; size = nlm * NP2B * 2 * nr; break;
+            case RA_BUF_AB: src = c.d_ab; size = 4 * nlm * 2 * nr; break;
+            case RA_BUF_RHS_WPT: src = c.d_rhs_wpt; size = nlm * 2 * 3 * nr; break;
+            case RA_BUF_RHS_Z: src = c.d_rhs_z; size = nlm * 2 * nr; break;
+            case RA_BUF_PTAB: src = c.d_Ptab; size = nlm * c.d.nth2; break;
+            case RA_BUF_IPTAB: src = c.d_iPtab; size = nlm * c.d.nth2; break;
+            default: throw ArgError("unknown buffer id");
+        }
+        if (n_out) *n_out = size;
+        if (!out) return;
+        if (n < size) throw ArgError("output capacity too small");
+        RA_CUDA(cudaMemcpyAsync(out, src, size * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int ra_radius(const ra_ctx* ctx, double* radius) {
+    if (!ctx || ctx->c.d.L == 0 || !radius) return RA_ERR_ARG;
+    std::copy(ctx->c.rad.radius.begin(), ctx->c.rad.radius.end(), radius);
+    return RA_OK;
+}
+
+int ra_costheta(const ra_ctx* ctx, double* ct) {
+    if (!ctx || ctx->c.d.L == 0 || !ct) return RA_ERR_ARG;
+    std::copy(ctx->c.costheta_h.begin(), ctx->c.costheta_h.end(), ct);
+    return RA_OK;
+}
+
+// ---- math-layer operators ----
+int ra_legendre_s2p(ra_ctx* ctx, const double* s, double* p, int nf, int nr) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!s || !p || nf <= 0 || nr <= 0) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const int L = c.d.L, nth = c.d.nth;
+        const int ncol = nf * nr * 2;
+        std::vector<double> hs((size_t)c.d.nlm * ncol), hp((size_t)L * nth * ncol);
+        // host s: per m, Fortran (l, r, ri, f) -> device s2[row(m,l)][f][r][ri]
+        size_t off = 0;
+        for (int m = 0; m < L; ++m) {
+            const int nl = L - m;
+            for (int f = 0; f < nf; ++f)
+                for (int ri = 0; ri < 2; ++ri)
+                    for (int r = 0; r < nr; ++r)
+                        for (int j = 0; j < nl; ++j)
+                            hs[(size_t)row_index(m, m + j, L) * ncol + ((size_t)f * nr + r) * 2 + ri] =
+                                s[off + (((size_t)f * 2 + ri) * nr + r) * nl + j];
+            off += (size_t)nl * nr * 2 * nf;
+        }
+        double *ds = nullptr, *dp = nullptr;
+        dalloc(ds, hs.size());
+        dalloc(dp, hp.size());
+        RA_CUDA(cudaMemcpyAsync(ds, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        launch_lt_inverse(c, ds, dp, ncol);
+        RA_CUDA(cudaMemcpyAsync(hp.data(), dp, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        cudaFree(ds);
+        cudaFree(dp);
+        // device p2[m][th][f][r][ri] -> host p2a(th, (r, ri, f), m)
+        for (int m = 0; m < L; ++m)
+            for (int f = 0; f < nf; ++f)
+                for (int ri = 0; ri < 2; ++ri)
+                    for (int r = 0; r < nr; ++r)
+                        for (int th = 0; th < nth; ++th)
+                            p[((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth + th] =
+                                hp[((size_t)m * nth + th) * ncol + ((size_t)f * nr + r) * 2 + ri];
+    });
+}
+
+int ra_legendre_p2s(ra_ctx* ctx, const double* p, double* s, int nf, int nr) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!s || !p || nf <= 0 || nr <= 0) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const int L = c.d.L, nth = c.d.nth;
+        const int ncol = nf * nr * 2;
+        std::vector<double> hs((size_t)c.d.nlm * ncol), hp((size_t)L * nth * ncol);
+        for (int m = 0; m < L; ++m)
+            for (int f = 0; f < nf; ++f)
+                for (int ri = 0; ri < 2; ++ri)
+                    for (int r = 0; r < nr; ++r)
+                        for (int th = 0; th < nth; ++th)
+                            hp[((size_t)m * nth + th) * ncol + ((size_t)f * nr + r) * 2 + ri] =
+                                p[((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth + th];
+        double *ds = nullptr, *dp = nullptr;
+        dalloc(ds, hs.size());
+        dalloc(dp, hp.size());
+        RA_CUDA(cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        launch_lt_forward(c, dp, ds, ncol);
+        RA_CUDA(cudaMemcpyAsync(hs.data(), ds, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        cudaFree(ds);
+        cudaFree(dp);
+        size_t off = 0;
+        for (int m = 0; m < L; ++m) {
+            const int nl = L - m;
+            for (int f = 0; f < nf; ++f)
+                for (int ri = 0; ri < 2; ++ri)
+                    for (int r = 0; r < nr; ++r)
+                        for (int j = 0; j < nl; ++j)
+                            s[off + (((size_t)f * 2 + ri) * nr + r) * nl + j] =
+                                hs[(size_t)row_index(m, m + j, L) * ncol + ((size_t)f * nr + r) * 2 + ri];
+            off += (size_t)nl * nr * 2 * nf;
+        }
+    });
+}
+
+static int fft_op(ra_ctx* ctx, double* x, long howmany, int inverse) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!x || howmany <= 0) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const size_t n = (size_t)howmany * (c.d.nphi + 2);
+        double* dx = nullptr;
+        dalloc(dx, n);
+        RA_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        launch_fft_rows(c, dx, howmany, inverse);
+        RA_CUDA(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        cudaFree(dx);
+    });
+}
+
+int ra_fft_c2r(ra_ctx* ctx, double* x, long howmany) { return fft_op(ctx, x, howmany, 1); }
+int ra_fft_r2c(ra_ctx* ctx, double* x, long howmany) { return fft_op(ctx, x, howmany, 0); }
+
+static int cheb_op(ra_ctx* ctx, const double* in, double* out, long ncols, int mode, int order) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!in || !out || ncols <= 0) return RA_ERR_ARG;
+    if (mode == 2 && (order < 1 || order > 3)) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const size_t n = (size_t)ncols * c.d.nr;
+        double *di = nullptr, *dout = nullptr;
+        dalloc(di, n);
+        dalloc(dout, n);
+        RA_CUDA(cudaMemcpyAsync(di, in, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        launch_cheb_columns(c, di, dout, ncols, mode, order);
+        RA_CUDA(cudaMemcpyAsync(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        cudaFree(di);
+        cudaFree(dout);
+    });
+}
+
+int ra_cheby_to_spectral(ra_ctx* ctx, const double* f, double* cc, long ncols) { return cheb_op(ctx, f, cc, ncols, 0, 0); }
+int ra_cheby_from_spectral(ra_ctx* ctx, const double* cc, double* f, long ncols) { return cheb_op(ctx, cc, f, ncols, 1, 0); }
+int ra_cheby_deriv(ra_ctx* ctx, const double* cc, double* dc, int order, long ncols) {
+    return cheb_op(ctx, cc, dc, ncols, 2, order);
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+// Internal declarations shared by the CUDA translation units of librayleigh_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/rayleigh_b200.h"
+
+namespace ra {
+
+// ---------------------------------------------------------------------------
+// Sizes and index maps
+// ---------------------------------------------------------------------------
+//  L    = l_max + 1  (number of m values, and of l values)
+//  n_lm = L (L + 1) / 2
+//  "lm"  index : l-major, m ascending      lm(l, m) = l (l + 1) / 2 + m
+//  "row" index : m-major, parity sorted    row(m, l) = off(m) + (l - m even ? (l - m)/2 : ne(m) + (l - m - 1)/2)
+//                off(m) = m L - m (m - 1) / 2,  ne(m) = (L - m + 1) / 2
+struct Dims {
+    int L, lmax, nr, nth, nth2, nphi;
+    long nlm;
+    int rda;          // 1-based dealiasing index of the Chebyshev grid: coefficients n >= rda-1 are zero
+    int kc;           // number of retained Chebyshev coefficients = rda - 1
+};
+
+__host__ __device__ inline long lm_index(int l, int m) { return (long)l * (l + 1) / 2 + m; }
+__host__ __device__ inline long m_off(int m, int L) { return (long)m * L - (long)m * (m - 1) / 2; }
+__host__ __device__ inline int n_even(int m, int L) { return (L - m + 1) / 2; }
+__host__ __device__ inline int n_odd(int m, int L) { return (L - m) / 2; }
+__host__ __device__ inline long row_index(int m, int l, int L) {
+    int d = l - m;
+    return m_off(m, L) + ((d & 1) ? (n_even(m, L) + (d - 1) / 2) : (d / 2));
+}
+
+// Number of grid outputs of the Chebyshev synthesis and the layout of the
+// post-solve grid buffer g[o][lm][ri][r]:
+//   0 W  1 W'  2 W''  3 W'''  4 P  5 P'  6 T  7 T'  8 T''  9 Z  10 Z'  11 Z''
+enum { G_W0, G_W1, G_W2, G_W3, G_P0, G_P1, G_T0, G_T1, G_T2, G_Z0, G_Z1, G_Z2, NG };
+// RHS terms of Post_Solve (Add_Derivative calls, Sphere_Spectral_Space.F90:285-389):
+// (equation, grid source).  coef[l][slot][r].
+enum { EQ_W = 0, EQ_P = 1, EQ_T = 2, EQ_Z = 3 };
+constexpr int NSLOT = 16;
+struct Slot { int eq, g; };
+constexpr Slot kSlots[NSLOT] = {
+    {EQ_W, G_W0}, {EQ_W, G_W1}, {EQ_W, G_W2}, {EQ_W, G_P1}, {EQ_W, G_T0},
+    {EQ_P, G_W0}, {EQ_P, G_W1}, {EQ_P, G_W2}, {EQ_P, G_W3}, {EQ_P, G_P0},
+    {EQ_T, G_T0}, {EQ_T, G_T1}, {EQ_T, G_T2},
+    {EQ_Z, G_Z0}, {EQ_Z, G_Z1}, {EQ_Z, G_Z2}};
+
+// Spectral forward-leg fields after Post_Solve (s2a, 7 fields; P is not carried
+// because the hydrodynamic non-output step never transforms it):
+enum { S_W, S_T, S_Z, S_W1, S_T1, S_Z1, S_W2, NS2A };
+// Fields of the inverse Legendre transform (p2a, 11 fields):
+enum { A_VR, A_T, A_OMR, A_DVRDR, A_DTDR, A_DVRDT, A_DTDT, A_VT, A_VP, A_DVTDR, A_DVPDR, NP2A };
+// Return-leg fields (p2b / s2b / ab): W P T Z
+constexpr int NP2B = 4;
+
+struct Radial {
+    std::vector<double> radius, delta_r, density, dlnrho, buoy, dpdr_w, pdwdr, nu, kappa;
+    double coriolis;
+};
+
+struct GemmTile { int item, mt, nt, par; };
+
+struct Ctx {
+    ra_config cfg;
+    Dims d;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    double dt = 0, old_dt = 0;
+    int iteration = 1;
+    bool have_state = false;
+    long launches = 0;
+
+    Radial rad;
+    std::vector<double> costheta_h;     // Gauss-Legendre nodes (double)
+    std::vector<double> cheb_D;         // [4][nr][nr] dcheby(r, n, d) with scalings
+    double deriv_scaling = 1.0;
+
+    // device constants
+    double *d_Ptab = nullptr, *d_iPtab = nullptr;     // [row][nth2]
+    double *d_D = nullptr;                            // [4][nr][nr]
+    double *d_coef = nullptr;                         // [L][NSLOT][nr]
+    double *d_radial = nullptr;                       // packed radial profiles (see kRadial*)
+    double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot
+    double *d_twid = nullptr;                         // [nth] complex exp(2 pi i k / nphi)
+    double *d_Awpt = nullptr, *d_Az = nullptr;        // inverses [L][3nr][3nr], [L][nr][nr]
+    int *d_ltiles = nullptr;                          // LT tile lists
+    int n_inv_tiles = 0, n_fwd_tiles = 0, n_cheb_tiles = 0, n_solve_tiles = 0;
+    int *d_inv_tiles = nullptr, *d_fwd_tiles = nullptr, *d_cheb_tiles = nullptr, *d_solve_tiles = nullptr;
+
+    // device state and step buffers
+    double *d_sol_wpt = nullptr, *d_sol_z = nullptr;  // [lm][2][3nr], [lm][2][nr]
+    double *d_rhs_wpt = nullptr, *d_rhs_z = nullptr;
+    double *d_ab = nullptr;                           // [4][lm][2][nr]
+    double *d_g = nullptr;                            // [NG][lm][2][nr]
+    double *d_s2a = nullptr;                          // [row][NS2A][nr][2]
+    double *d_s2a11 = nullptr;                        // [row][NP2A][nr][2]
+    double *d_p2a = nullptr;                          // [m][nth][NP2A][nr][2]
+    double *d_p2b = nullptr;                          // [m][nth][4][nr][2]
+    double *d_s2b = nullptr;                          // [row][4][nr][2]
+    unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
+    int *d_status = nullptr;                          // device error word
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_old_ab = 0, graph_new_ab = 0;
+};
+
+// radial profile packing in d_radial: index k * nr + r
+enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R, R_COUNT };
+
+// ---- kernels / launchers (defined in the .cu files) ----
+void launch_plm(Ctx& c, const double* d_x, const double* d_w);
+void launch_lt_inverse(Ctx& c, const double* s2, double* p2, int ncol);
+void launch_lt_forward(Ctx& c, const double* p2, double* s2, int ncol);
+void launch_cheb_synthesis(Ctx& c);
+void launch_post_assemble(Ctx& c, double old_ab);
+void launch_rlm_a(Ctx& c);
+void launch_physics(Ctx& c);
+void launch_rlm_b(Ctx& c);
+void launch_solve(Ctx& c, double new_ab);
+int  invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip);
+void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse);
+void launch_cheb_columns(Ctx& c, const double* d_in, double* d_out, long ncols, int mode, int order);
+
+#define RA_CUDA(call)                                                             \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) {                                                  \
+            throw ra::CudaError(e_, #call, __FILE__, __LINE__);                   \
+        }                                                                         \
+    } while (0)
+
+struct CudaError {
+    cudaError_t code;
+    std::string what;
+    CudaError(cudaError_t e, const char* call, const char* file, int line) : code(e) {
+        what = std::string(call) + " failed at " + file + ":" + std::to_string(line) + ": " + cudaGetErrorString(e);
+    }
+};
+
+struct ArgError {
+    std::string what;
+    explicit ArgError(std::string w) : what(std::move(w)) {}
+};
+
+}  // namespace ra

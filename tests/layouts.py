@@ -1,0 +1,42 @@
+"""Layout helpers shared by the GPU parity tests: convert the oracle's
+reference-layout arrays into the device buffer layouts that
+``Rayleigh.debug_buffer`` returns (see include/rayleigh_b200.h, RA_BUF_*)."""
+import numpy as np
+
+
+def m_off(m, L):
+    return m * L - m * (m - 1) // 2
+
+
+def row_index(m, l, L):
+    d = l - m
+    ne = (L - m + 1) // 2
+    return m_off(m, L) + ((ne + (d - 1) // 2) if (d & 1) else d // 2)
+
+
+def s2_to_rows(s2, fields):
+    """list over m of (nf, 2, nr, nl) -> [row][len(fields)][nr][2]."""
+    L = len(s2)
+    nr = s2[0].shape[2]
+    nlm = L * (L + 1) // 2
+    out = np.zeros((nlm, len(fields), nr, 2))
+    for m in range(L):
+        a = s2[m][list(fields)]                      # (F, 2, nr, nl)
+        rows = [row_index(m, m + j, L) for j in range(L - m)]
+        out[rows] = a.transpose(3, 0, 2, 1)
+    return out
+
+
+def p2_to_dev(p2, fields):
+    """list over m of (nf, 2, nr, nth) -> [m][nth][F][nr][2]."""
+    P = np.stack([p[list(fields)] for p in p2])     # (m, F, 2, nr, nth)
+    return P.transpose(0, 4, 1, 3, 2).copy()
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = np.linalg.norm(b.ravel())
+    if den == 0:
+        return float(np.linalg.norm(a.ravel()))
+    return float(np.linalg.norm((a - b).ravel()) / den)

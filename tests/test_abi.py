@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every symbol that include/*.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:int|long|void)\s+\**\s*(ra_\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for must in ("ra_create", "ra_step", "ra_post_solve", "ra_rlm_a", "ra_physical", "ra_rlm_b", "ra_advance",
+                 "ra_legendre_s2p", "ra_legendre_p2s", "ra_fft_c2r", "ra_fft_r2c", "ra_set_dt"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from rayleigh_b200 import build
+    lib_path = build.build()
+    lib = ctypes.CDLL(lib_path)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_config_and_argument_errors_without_gpu():
+    import rayleigh_b200 as rb
+    lib = rb.load_library()
+    cfg = rb._Config()
+    assert lib.ra_default_config(ctypes.byref(cfg)) == 0
+    assert cfg.n_r == 48 and cfg.l_max == 63 and abs(cfg.alpha_implicit - 0.5) < 1e-15
+    assert lib.ra_default_config(None) == rb.RA_ERR_ARG
+    # a context-less call reports a state error instead of touching the device
+    assert lib.ra_step(None, 1, None) == rb.RA_ERR_STATE
+    # an invalid configuration is rejected before any CUDA call
+    bad = rb.Config(n_r=7).to_c()
+    h = ctypes.c_void_p()
+    assert lib.ra_create(ctypes.byref(h), ctypes.byref(bad)) == rb.RA_ERR_ARG
+    buf = ctypes.create_string_buffer(256)
+    lib.ra_last_error(h, buf, 256)
+    assert b"n_r" in buf.value
+    lib.ra_destroy(h)

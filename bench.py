@@ -1,0 +1,420 @@
+"""Benchmark: Rayleigh timesteps/s at l_max = 511, N_r = 192 on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--impl ours|reference] [--lmax 511] [--nr 192]
+
+One JSON line on rank 0.  A step is one pass of the hot path (Post_Solve,
+rlm_spacea, physical_space, rlm_spaceb, AdvanceTime) over the whole state;
+the state (~35 GB of buffers) stays resident in HBM and is far larger than L2.
+``--impl reference`` times the reference algorithm on the host cores: the
+NumPy restatement under ``oracle/`` (the Fortran reference cannot be built in
+this image), sampled per stage and scaled to one full step.
+With N > 1 (torchrun) every rank runs an independent simulation, as the
+reference's multi-run mode does (-nruns); the value sums the ranks' steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "steps/s at lmax=511,N_r=192: mixed-prec vs FP64 GPU at rel err≤1e-9; % roofline"
+SEED = 0x5241594C
+
+
+def headline_config(lmax, nr, precision):
+    """Boussinesq rotating convection at the headline grid (BASELINE config 5 sizes, hydrodynamic)."""
+    return dict(n_r=nr, l_max=lmax, aspect_ratio=0.35, shell_depth=1.0, rayleigh=2.0e8, ekman=1.0e-5,
+                prandtl=1.0, gravity_power=1.0, rotation=True, no_slip_top=True, no_slip_bottom=True,
+                fix_tvar_top=True, fix_tvar_bottom=True, t_top=0.0, t_bottom=1.0, dt=1.0e-6,
+                precision=precision)
+
+
+def initial_state(ctx, lmax, nr, rng):
+    """Conductive T plus a seeded perturbation on l in [1, 20] with (l+1)^-2 decay (coefficient space)."""
+    n_lm = (lmax + 1) * (lmax + 2) // 2
+    wpt = np.zeros((n_lm, 2, 3 * nr))
+    z = np.zeros((n_lm, 2, nr))
+    r = ctx.radius()
+    r_out, r_in = r[0], r[-1]
+    tcond = r_out * r_in / (r_in - r_out) * (1.0 / r_out - 1.0 / r) * math.sqrt(4 * math.pi)
+    wpt[0, 0, 2 * nr:] = ctx.cheby_to_spectral(tcond[None])[0]
+    ncoef = min(16, nr // 2)
+    for l in range(1, min(20, lmax) + 1):
+        s = l * (l + 1) // 2
+        amp = 1e-3 * (l + 1.0) ** -2
+        block = rng.standard_normal((l + 1, 2, ncoef)) * amp / (1.0 + np.arange(ncoef)) ** 2
+        block[0, 1] = 0.0
+        wpt[s:s + l + 1, :, 2 * nr:2 * nr + ncoef] = block
+    return wpt, z
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work per kernel (one launch = one step), FP64
+# ---------------------------------------------------------------------------
+def kernel_work(lmax, nr, nth):
+    L = lmax + 1
+    n_lm = L * (L + 1) // 2
+    nth2 = nth // 2
+    kc = (2 * nr) // 3
+    cols = 2 * n_lm
+    w = {}
+    w["lt_inverse"] = ("tensor", 2.0 * nth2 * (11 * nr * 2) * n_lm)
+    w["lt_forward"] = ("tensor", 2.0 * nth2 * (4 * nr * 2) * n_lm)
+    w["cheb_synthesis"] = ("tensor", 12 * 2.0 * (nr // 2) * kc * cols)
+    w["solve"] = ("tensor", 2.0 * (9 + 1) * nr * nr * cols)
+    plane = n_lm * 2 * nr * 8.0
+    w["post_assemble"] = ("hbm", (12 + 4 + 4 + 7) * plane)
+    w["rlm_a"] = ("hbm", (7 + 11) * plane)
+    w["rlm_b"] = ("hbm", (4 + 4) * plane)
+    w["physics"] = ("hbm", L * nth * (11 + 4) * nr * 2 * 8.0)
+    return w
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM 8192^3 on this GPU (best of 5): the FP64 tensor-pipe denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU leg: the oracle, sampled per stage and scaled to a full step
+# ---------------------------------------------------------------------------
+class CpuSample:
+    def __init__(self, lmax, nr, stride=32, ntheta_rows=2):
+        import oracle as O
+        self.O = O
+        cfg = O.Config(**{k: v for k, v in headline_config(lmax, nr, 0).items() if k in O.Config.__dataclass_fields__})
+        t0 = time.perf_counter()
+        self.o = O.Oracle(cfg)
+        self.init_s = time.perf_counter() - t0
+        self.cfg = cfg
+        L = lmax + 1
+        self.L = L
+        n_lm = L * (L + 1) // 2
+        self.ms = list(range(0, L, stride))
+        self.ls = list(range(stride // 2, L, stride))
+        self.f_m = sum(L - m for m in self.ms) / n_lm
+        self.f_l = sum(l + 1 for l in self.ls) / n_lm
+        self.thetas = np.linspace(0, cfg.n_theta - 1, ntheta_rows).astype(int)
+        self.f_t = ntheta_rows / cfg.n_theta
+        rng = np.random.Generator(np.random.PCG64(SEED))
+        self.s2a = {m: rng.standard_normal((8, 2, nr, L - m)) for m in self.ms}
+        self.s2a12 = {m: rng.standard_normal((12, 2, nr, L - m)) for m in self.ms}
+        self.p2b = {m: rng.standard_normal((4, 2, nr, cfg.n_theta)) for m in self.ms}
+        self.s2b = {m: rng.standard_normal((4, 2, nr, L - m)) for m in self.ms}
+        self.p3a = rng.standard_normal((12, ntheta_rows, nr, cfg.n_phi + 2))
+        lm_idx = np.concatenate([np.arange(l * (l + 1) // 2, l * (l + 1) // 2 + l + 1) for l in self.ls])
+        self.lm_idx = lm_idx
+        self.c = rng.standard_normal((4, len(lm_idx), 2, nr))
+        self.ab = rng.standard_normal((4, len(lm_idx), 2, nr))
+        self.rhs = {l: rng.standard_normal((3 * nr, 2 * (l + 1))) for l in self.ls}
+        self.rhsz = {l: rng.standard_normal((nr, 2 * (l + 1))) for l in self.ls}
+        self.sample = (f"per step: Post_Solve on l = {self.ls[0]}::{stride} ({self.f_l:.3f} of the (l,m) columns), "
+                       f"rlm_spacea/StP/PtS/rlm_spaceb on m = 0::{stride} ({self.f_m:.3f} of the (l,m) rows), "
+                       f"physical_space on {ntheta_rows} of {cfg.n_theta} theta rows, Implicit_Solve on l = "
+                       f"{self.ls[0]}::{stride}; each stage time scaled by its work fraction")
+
+    def step_seconds(self):
+        import scipy.linalg as sla
+        O, o, cg = self.O, self.o, self.o.cg
+        t = {}
+        # Post_Solve: radial derivatives, From_Spectral, Add_Derivative on the sampled columns
+        t0 = time.perf_counter()
+        c = cg.dealias(self.c)
+        W, P, T, Z = c
+        ctemp = cg.from_spectral(cg.dealias(np.stack([cg.deriv(W, 3), cg.deriv(P, 1), cg.deriv(T, 2), cg.deriv(Z, 2)])))
+        g = cg.from_spectral(cg.dealias(np.stack([W, P, T, Z, cg.deriv(W, 1), cg.deriv(T, 1), cg.deriv(Z, 1),
+                                                  cg.deriv(W, 2)])))
+        p1b = self.ab * 0.5
+        src = {(0, 0): g[0], (0, 1): g[4], (0, 2): g[7], (0, 3): ctemp[0], (1, 0): g[1], (1, 1): ctemp[1],
+               (2, 0): g[2], (2, 1): g[5], (2, 2): ctemp[2], (3, 0): g[3], (3, 1): g[6], (3, 2): ctemp[3]}
+        off = 0
+        for l in self.ls:
+            sl = slice(off, off + l + 1)
+            for (eq, var, d), cf in o.coefs[l].items():
+                if (var, d) in src:
+                    p1b[eq, sl] += src[(var, d)][sl] * cf
+            off += l + 1
+        t["post_solve"] = (time.perf_counter() - t0) / self.f_l
+        t0 = time.perf_counter()
+        o.rlm_spacea(self.s2a, ms=self.ms)
+        t["rlm_a"] = (time.perf_counter() - t0) / self.f_m
+        t0 = time.perf_counter()
+        o.h.s2p(self.s2a12, ms=self.ms)
+        t["lt_inverse"] = (time.perf_counter() - t0) / self.f_m
+        t0 = time.perf_counter()
+        o.physical_space(self.p3a, thetas=self.thetas)
+        t["physics"] = (time.perf_counter() - t0) / self.f_t
+        t0 = time.perf_counter()
+        o.h.p2s(self.p2b, ms=self.ms)
+        t["lt_forward"] = (time.perf_counter() - t0) / self.f_m
+        t0 = time.perf_counter()
+        o.rlm_spaceb(self.s2b, ms=self.ms)
+        t["rlm_b"] = (time.perf_counter() - t0) / self.f_m
+        t0 = time.perf_counter()
+        for l in self.ls:
+            sla.lu_solve(o.lu_wpt[l], self.rhs[l], check_finite=False)
+            if l > 0:
+                sla.lu_solve(o.lu_z[l], self.rhsz[l], check_finite=False)
+        t["solve"] = (time.perf_counter() - t0) / self.f_l
+        return sum(t.values()), t
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    cs = CpuSample(args.lmax, args.nr)
+    for _ in range(args.warmup):
+        cs.step_seconds()
+    times = []
+    for _ in range(args.steps):
+        s, parts = cs.step_seconds()
+        times.append(s)
+    sec = float(np.mean(times))
+    value = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
+                   "n_r": args.nr, "n_theta": cs.cfg.n_theta, "n_phi": cs.cfg.n_phi,
+                   "l2": "working set larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": cs.sample, "stage_seconds": {k: round(v, 4) for k, v in parts.items()}},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, torch, dist):
+    import rayleigh_b200 as rb
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    prec = rb.PREC_MIXED if args.precision == "mixed" else rb.PREC_FP64
+    cfgd = headline_config(args.lmax, args.nr, prec)
+    cfg = rb.Config(**cfgd, use_graph=True, device=local)
+    ctx = rb.Rayleigh(cfg)
+    rng = np.random.Generator(np.random.PCG64(SEED + rank))
+    wpt, z = initial_state(ctx, args.lmax, args.nr, rng)
+    ctx.put_state(wpt, z, None, iteration=1)
+    peaks, peak_kind = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
+    # warm-up (includes the Euler first step)
+    ctx.time_steps(max(1, args.warmup))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total_ms, per_kernel = ctx.time_steps(args.steps)
+    launches = ctx.launch_count()
+    torch.cuda.synchronize()
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms * 1e-3)
+
+    # end to end through the C ABI with host buffers: H2D of the full state, one
+    # step, D2H of the new state and its CFL cargo, every step
+    n_lm = ctx.n_lm
+    nr = args.nr
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    h_wpt, h_z, h_ab = pin(n_lm * 2 * 3 * nr), pin(n_lm * 2 * nr), pin(4 * n_lm * 2 * nr)
+    o_wpt, o_z, o_ab = pin(n_lm * 2 * 3 * nr), pin(n_lm * 2 * nr), pin(4 * n_lm * 2 * nr)
+    w0, z0, ab0 = ctx.get_state()
+    h_wpt[:] = w0.ravel()
+    h_z[:] = z0.ravel()
+    h_ab[:] = ab0.ravel()
+    import ctypes
+    lib = ctx.lib
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    e2e_steps = max(1, min(args.steps, 5))
+    cfl = ctypes.c_double()
+    it = 1000
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx._check(lib.ra_put_state(ctx.h, P(h_wpt), P(h_z), P(h_ab), it))
+        ctx._check(lib.ra_step(ctx.h, 1, ctypes.byref(cfl)))
+        ctx._check(lib.ra_get_state(ctx.h, P(o_wpt), P(o_z), P(o_ab)))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    h2d = (h_wpt.nbytes + h_z.nbytes + h_ab.nbytes)
+    d2h = (o_wpt.nbytes + o_z.nbytes + o_ab.nbytes + 8)
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world / float(e2e_t.item())
+    if rank != 0:
+        return
+    # roofline of the dominant kernel
+    work = kernel_work(args.lmax, args.nr, ctx.n_theta)
+    dom = max(per_kernel, key=lambda k: per_kernel[k])
+    bound, amount = work[dom]
+    avg_s = per_kernel[dom] / args.steps * 1e-3
+    traffic = None
+    tpath = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"{dom}_{args.precision}_lmax{args.lmax}_nr{args.nr}")
+        except Exception:
+            traffic = None
+    if bound == "tensor":
+        achieved = amount / avg_s / 1e12
+        peak, unit = fp64_peak, "TFLOP/s"
+        peak_note = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"
+    else:
+        achieved = amount / avg_s / 1e9
+        peak, unit = peaks["hbm_gbs"], "GB/s"
+        peak_note = f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json)"
+    kernels = {}
+    for k, ms in per_kernel.items():
+        b, amt = work[k]
+        s = ms / args.steps * 1e-3
+        kernels[k] = {"ms_per_step": round(ms / args.steps, 4), "share": round(ms / total_ms, 4),
+                      ("tflops" if b == "tensor" else "gbs"): round(amt / s / (1e12 if b == "tensor" else 1e9), 2)}
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "precision": args.precision, "data": "synthetic (seeded)",
+        "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
+                   "n_r": args.nr, "n_theta": ctx.n_theta, "n_phi": ctx.n_phi, "ekman": cfgd["ekman"],
+                   "dt": cfgd["dt"], "l2": "working set (~35 GB) larger than L2; no flush needed",
+                   "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
+        "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                     "frac": achieved / peak if peak else None, "traffic": traffic, "peak_source": peak_note},
+        "kernels": kernels,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "how": "ra_put_state (pinned host) + ra_step(1) + ra_get_state (pinned host) per step"},
+    }
+    if not args.no_cpu:
+        cs = CpuSample(args.lmax, args.nr)
+        sec, parts = cs.step_seconds()
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": cs.sample, "stage_seconds": {k: round(v, 3) for k, v in parts.items()}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--lmax", type=int, default=511)
+    ap.add_argument("--nr", type=int, default=192)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, torch, dist)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

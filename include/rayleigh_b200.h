@@ -108,6 +108,16 @@ int ra_physical(ra_ctx* ctx, double* cfl);      /* physical_space: FFTs, NL term
 int ra_rlm_b(ra_ctx* ctx);                      /* PtS Legendre + rlm_spaceb + Transpose_2b1b */
 int ra_advance(ra_ctx* ctx);                    /* AdvanceTime: AB term, BCs, Implicit_Solve */
 
+/* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
+ * replay, so that CUDA events on the context's stream bracket every kernel)
+ * and returns the elapsed device time of the whole region in *total_ms and,
+ * if kernel_ms is not NULL, the summed time of each kernel of the step in
+ * kernel_ms[0..nk) in the order of ra_kernel_name(). */
+int ra_time_steps(ra_ctx* ctx, int nsteps, double* total_ms, double* kernel_ms, int nk);
+/* Number of kernels one step launches and their names (static strings). */
+int ra_kernels_per_step(void);
+const char* ra_kernel_name(int i);
+
 /* Blocks until the context's stream is idle; returns the first device error. */
 int ra_sync(ra_ctx* ctx);
 

@@ -193,11 +193,13 @@ class Horizontal:
             self.sdcoef.append(((ls + 1) * c1, -ls * c2))
 
     # ----- Legendre transforms (Legendre_Transforms.F90:968-1175) -----
-    def s2p(self, s2):
-        """StP_4d_dgp2: spectral s2[m] (nf,2,nr,nl) -> p2 [m][nf][2][nr][theta]."""
+    def s2p(self, s2, ms=None):
+        """StP_4d_dgp2: spectral s2[m] (nf,2,nr,nl) -> p2 [m][nf][2][nr][theta].
+
+        ``ms`` restricts the work to a subset of m (returns that many arrays)."""
         nth, nth2 = self.n_theta, self.n_theta // 2
         out = []
-        for m in range(self.n_m):
+        for m in (range(self.n_m) if ms is None else ms):
             a = s2[m]
             nf, _, nr, nl = a.shape
             a2 = a.reshape(-1, nl).T           # (nl, nrhs)
@@ -213,11 +215,11 @@ class Horizontal:
             out.append(o.T.reshape(nf, 2, nr, nth))
         return out
 
-    def p2s(self, p2):
-        """PtS_4d_dgpv3: p2 [m](nf,2,nr,theta) -> s2[m] (nf,2,nr,nl)."""
+    def p2s(self, p2, ms=None):
+        """PtS_4d_dgpv3: p2 [m](nf,2,nr,theta) -> s2[m] (nf,2,nr,nl); ``ms`` as in s2p."""
         nth, nth2 = self.n_theta, self.n_theta // 2
         out = []
-        for m in range(self.n_m):
+        for m in (range(self.n_m) if ms is None else ms):
             d = p2[m]
             nf, _, nr, _ = d.shape
             d2 = d.reshape(-1, nth).T          # (nth, nrhs)
@@ -670,7 +672,7 @@ class Oracle:
             p1[:, idx] = s2[m].transpose(0, 3, 1, 2)
         return p1
 
-    def rlm_spacea(self, s2):
+    def rlm_spacea(self, s2, ms=None):
         """Sphere_Hybrid_Space.F90:64-125 (hydro): 8 fields -> 12 fields, then StP."""
         h, L = self.h, self.cfg.l_max
         r = self.radius
@@ -679,7 +681,7 @@ class Oracle:
         drho = (self.dlnrho + 1.0 / r)[:, None]
         two_over_r = (2.0 / r)[:, None]
         out = []
-        for m in range(L + 1):
+        for m in (range(L + 1) if ms is None else ms):
             a = s2[m].copy()
             a[..., -1] = 0.0                                          # zero l_max (:73-75)
             ls = np.arange(m, L + 1, dtype=np.float64)
@@ -716,9 +718,12 @@ class Oracle:
             out.append(b)
         return out
 
-    def physical_space(self, p3):
-        """Sphere_Physical_Space.F90:98-224 (hydro): p3a (18 fields) -> p3b (4 fields) + CFL."""
+    def physical_space(self, p3, thetas=None):
+        """Sphere_Physical_Space.F90:98-224 (hydro): p3a (18 fields) -> p3b (4 fields) + CFL.
+
+        ``thetas`` (index array) says which theta rows p3 holds (all when None)."""
         cfg, h = self.cfg, self.h
+        th = slice(None) if thetas is None else np.asarray(thetas)
         nphi = cfg.n_phi
         L = cfg.l_max
         # Phi_Derivatives (:745-759) in packed m-space
@@ -738,10 +743,10 @@ class Oracle:
         f["dtdp"] = dphi(f["t"])
         for k in list(f.keys()):
             f[k] = fft_c2r(f[k], nphi)[..., :nphi]
-        csc = h.csctheta[:, None, None]
-        cot = h.cottheta[:, None, None]
-        sin = h.sintheta[:, None, None]
-        cos = h.costheta[:, None, None]
+        csc = h.csctheta[th][:, None, None]
+        cot = h.cottheta[th][:, None, None]
+        sin = h.sintheta[th][:, None, None]
+        cos = h.costheta[th][:, None, None]
         for k in ("vt", "vp", "dvtdr", "dvpdr", "dtdt", "dvrdt", "dvpdp", "dvtdp"):
             f[k] = f[k] * csc                                          # sintheta_div (:119-126)
         r = self.radius[None, :, None]
@@ -798,11 +803,11 @@ class Oracle:
         P = np.stack([re, im], axis=0).transpose(4, 1, 0, 3, 2)   # (m, f, 2, r, th)
         return [np.ascontiguousarray(P[m]) for m in range(M)]
 
-    def rlm_spaceb(self, s2):
+    def rlm_spaceb(self, s2, ms=None):
         """Sphere_Hybrid_Space.F90:127-222 (hydro): curl algebra on the NL terms."""
         h, L = self.h, self.cfg.l_max
         out = []
-        for m in range(L + 1):
+        for m in (range(L + 1) if ms is None else ms):
             a = s2[m].copy()
             ls = np.arange(m, L + 1, dtype=np.float64)
             ollp1 = np.zeros_like(ls)
@@ -824,8 +829,8 @@ class Oracle:
             out.append(a)
         return out
 
-    def advance_time(self, p1b_new):
-        """AdvanceTime (Sphere_Spectral_Space.F90:415-435): add AB term, BCs, solve."""
+    def advance_time(self, p1b_new, ls=None):
+        """AdvanceTime (Sphere_Spectral_Space.F90:415-435): add AB term, BCs, solve (``ls``: subset of l)."""
         nr = self.cfg.n_r
         self.ab = p1b_new
         nab = self.new_ab
@@ -842,7 +847,7 @@ class Oracle:
         self.rhs_wpt[0, 0, 2 * nr] = self.bc_t[0]          # l=0, m=0, real, top
         self.rhs_wpt[0, 0, 3 * nr - 1] = self.bc_t[1]
         # Implicit_Solve -> DGETRS (Linear_Solve.F90:423-457,1088-1110)
-        for l in range(self.cfg.l_max + 1):
+        for l in (range(self.cfg.l_max + 1) if ls is None else ls):
             s, e = self.l_start[l], self.l_start[l] + l + 1
             b = self.rhs_wpt[s:e].reshape(-1, 3 * nr).T
             x = sla.lu_solve(self.lu_wpt[l], b, check_finite=False)

@@ -133,6 +133,9 @@ def load_library(path: str | None = None):
         "ra_radius": ([_VP, _VP], ctypes.c_int),
         "ra_costheta": ([_VP, _VP], ctypes.c_int),
         "ra_launch_count": ([_VP], ctypes.c_long),
+        "ra_time_steps": ([_VP, ctypes.c_int, _DP, _DP, ctypes.c_int], ctypes.c_int),
+        "ra_kernels_per_step": ([], ctypes.c_int),
+        "ra_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -219,6 +222,15 @@ class Rayleigh:
         cfl = ctypes.c_double()
         self._check(self.lib.ra_step(self.h, int(nsteps), ctypes.byref(cfl)))
         return cfl.value
+
+    def time_steps(self, nsteps):
+        """Device-timed steps (CUDA events on the context's stream): (total_ms, {kernel: ms})."""
+        nk = self.lib.ra_kernels_per_step()
+        total = ctypes.c_double()
+        per = (ctypes.c_double * nk)()
+        self._check(self.lib.ra_time_steps(self.h, int(nsteps), ctypes.byref(total), per, nk))
+        names = [self.lib.ra_kernel_name(i).decode() for i in range(nk)]
+        return total.value, dict(zip(names, list(per)))
 
     def set_dt(self, dt):
         self._check(self.lib.ra_set_dt(self.h, float(dt)))

@@ -686,6 +686,69 @@ int ra_advance(ra_ctx* ctx) {
     });
 }
 
+static const char* kKernelNames[] = {"cheb_synthesis", "post_assemble", "rlm_a",  "lt_inverse",
+                                     "physics",        "lt_forward",    "rlm_b",  "solve"};
+constexpr int kNK = 8;
+
+int ra_kernels_per_step(void) { return kNK; }
+const char* ra_kernel_name(int i) { return (i >= 0 && i < kNK) ? kKernelNames[i] : nullptr; }
+
+int ra_time_steps(ra_ctx* ctx, int nsteps, double* total_ms, double* kernel_ms, int nk) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (nsteps <= 0 || !total_ms) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        c.launches = 0;
+        std::vector<cudaEvent_t> ev((size_t)nsteps * (kNK + 1));
+        for (auto& e : ev) RA_CUDA(cudaEventCreate(&e));
+        try {
+            for (int s = 0; s < nsteps; ++s) {
+                double new_ab, old_ab;
+                ab_factors(c, new_ab, old_ab);
+                cudaEvent_t* E = ev.data() + (size_t)s * (kNK + 1);
+                RA_CUDA(cudaEventRecord(E[0], c.stream));
+                launch_cheb_synthesis(c);
+                RA_CUDA(cudaEventRecord(E[1], c.stream));
+                launch_post_assemble(c, old_ab);
+                RA_CUDA(cudaEventRecord(E[2], c.stream));
+                launch_rlm_a(c);
+                RA_CUDA(cudaEventRecord(E[3], c.stream));
+                launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
+                RA_CUDA(cudaEventRecord(E[4], c.stream));
+                RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
+                launch_physics(c);
+                RA_CUDA(cudaEventRecord(E[5], c.stream));
+                launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+                RA_CUDA(cudaEventRecord(E[6], c.stream));
+                launch_rlm_b(c);
+                RA_CUDA(cudaEventRecord(E[7], c.stream));
+                launch_solve(c, new_ab);
+                RA_CUDA(cudaEventRecord(E[8], c.stream));
+                c.old_dt = c.dt;
+                ++c.iteration;
+            }
+            RA_CUDA(cudaStreamSynchronize(c.stream));
+            float ms = 0.f;
+            RA_CUDA(cudaEventElapsedTime(&ms, ev.front(), ev.back()));
+            *total_ms = ms;
+            if (kernel_ms) {
+                for (int k = 0; k < nk && k < kNK; ++k) kernel_ms[k] = 0.0;
+                for (int s = 0; s < nsteps; ++s) {
+                    cudaEvent_t* E = ev.data() + (size_t)s * (kNK + 1);
+                    for (int k = 0; k < nk && k < kNK; ++k) {
+                        RA_CUDA(cudaEventElapsedTime(&ms, E[k], E[k + 1]));
+                        kernel_ms[k] += ms;
+                    }
+                }
+            }
+        } catch (...) {
+            for (auto& e : ev) cudaEventDestroy(e);
+            throw;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+    });
+}
+
 int ra_sync(ra_ctx* ctx) {
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
     return guarded(ctx, [&] { RA_CUDA(cudaStreamSynchronize(ctx->c.stream)); });

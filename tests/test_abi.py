@@ -15,7 +15,7 @@ def declared_symbols():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"^\s*(?:int|long|void)\s+\**\s*(ra_\w+)\s*\(", src, flags=re.M):
+        for m in re.finditer(r"^\s*(?:const\s+)?(?:int|long|void|char)\s*\**\s*(ra_\w+)\s*\(", src, flags=re.M):
             names.add(m.group(1))
     return sorted(names)
 

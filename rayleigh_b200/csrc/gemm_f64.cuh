@@ -12,13 +12,25 @@
 
 namespace ra {
 
-constexpr int BM = 64, BN = 64, BK = 16, GEMM_THREADS = 128;
+constexpr int BK = 16, GEMM_THREADS = 128;
 constexpr int SPAD = 4;  // row padding (doubles): conflict-free fragment reads
 
-struct GemmSmem {
-    double A[2][BK][BM + SPAD];
-    double B[2][BK][BN + SPAD];
+// Tile shape: WM x WN warps of 32x32 (WM * WN == 4), CTA tile BM x BN.
+template <int WM, int WN>
+struct Shape {
+    static constexpr int BM = 32 * WM, BN = 32 * WN;
+    static constexpr int NA = BK * BM / GEMM_THREADS, NB = BK * BN / GEMM_THREADS;
 };
+using Sq = Shape<2, 2>;     // 64 x 64
+using Wide = Shape<1, 4>;   // 32 x 128
+constexpr int BM = Sq::BM, BN = Sq::BN;
+
+template <int WM, int WN>
+struct GemmSmemT {
+    double A[2][BK][32 * WM + SPAD];
+    double B[2][BK][32 * WN + SPAD];
+};
+using GemmSmem = GemmSmemT<2, 2>;
 
 struct Acc {
     double v[4][4][2];
@@ -36,8 +48,8 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-// Element (k, m) of the 1024-element tile handled by thread t in slot i.
-// MC = true: consecutive threads walk m (A stored m-contiguous in memory);
+// Element (k, x) of a BK x BX tile handled by thread t in slot i.
+// MC = true: consecutive threads walk x (operand stored x-contiguous in memory);
 // MC = false: consecutive threads walk k.
 template <bool MC, int BX>
 __device__ __forceinline__ void tile_coord(int t, int i, int& k, int& x) {
@@ -51,34 +63,43 @@ __device__ __forceinline__ void tile_coord(int t, int i, int& k, int& x) {
     }
 }
 
-// acc += sum_{k < K} A(k, m) B(k, n) for the CTA's 64x64 tile.
+// acc += sum_{k < K} A(k, m) B(k, n) for the CTA's BM x BN tile.
 // fa(k, m) and fb(k, n) must return 0 outside the problem.
-template <bool AMC, bool BNC, class FA, class FB>
-__device__ __forceinline__ void gemm_tile(Acc& acc, const FA& fa, const FB& fb, int K, GemmSmem& sm) {
+template <bool AMC, bool BNC, int WM = 2, int WN = 2, class FA, class FB>
+__device__ __forceinline__ void gemm_tile(Acc& acc, const FA& fa, const FB& fb, int K, GemmSmemT<WM, WN>& sm) {
+    using S = Shape<WM, WN>;
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = warp & 1, wn = warp >> 1;
-    double ra[8], rb[8];
+    const int wm = warp % WM, wn = warp / WM;
+    double ra[S::NA], rb[S::NB];
     const int nk = (K + BK - 1) / BK;
     if (nk == 0) return;
     auto fetch = [&](int kt) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < S::NA; ++i) {
             int k, x;
-            tile_coord<AMC, BM>(t, i, k, x);
+            tile_coord<AMC, S::BM>(t, i, k, x);
             ra[i] = fa(kt * BK + k, x);
-            tile_coord<BNC, BN>(t, i, k, x);
+        }
+#pragma unroll
+        for (int i = 0; i < S::NB; ++i) {
+            int k, x;
+            tile_coord<BNC, S::BN>(t, i, k, x);
             rb[i] = fb(kt * BK + k, x);
         }
     };
     auto stash = [&](int buf) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < S::NA; ++i) {
             int k, x;
-            tile_coord<AMC, BM>(t, i, k, x);
+            tile_coord<AMC, S::BM>(t, i, k, x);
             sm.A[buf][k][x] = ra[i];
-            tile_coord<BNC, BN>(t, i, k, x);
+        }
+#pragma unroll
+        for (int i = 0; i < S::NB; ++i) {
+            int k, x;
+            tile_coord<BNC, S::BN>(t, i, k, x);
             sm.B[buf][k][x] = rb[i];
         }
     };
@@ -105,13 +126,13 @@ __device__ __forceinline__ void gemm_tile(Acc& acc, const FA& fa, const FB& fb, 
     }
 }
 
-// Visit the accumulator: f(m, n, value) with (m, n) local to the 64x64 tile.
-template <class F>
+// Visit the accumulator: f(m, n, value) with (m, n) local to the CTA tile.
+template <int WM = 2, int WN = 2, class F>
 __device__ __forceinline__ void acc_foreach(const Acc& acc, const F& f) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = warp & 1, wn = warp >> 1;
+    const int wm = warp % WM, wn = warp / WM;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -120,12 +141,12 @@ __device__ __forceinline__ void acc_foreach(const Acc& acc, const F& f) {
             for (int q = 0; q < 2; ++q) f(wm * 32 + i * 8 + g, wn * 32 + j * 8 + 2 * tig + q, acc.v[i][j][q]);
 }
 
-template <class F>
+template <int WM = 2, int WN = 2, class F>
 __device__ __forceinline__ void acc_foreach2(const Acc& a, const Acc& b, const F& f) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = warp & 1, wn = warp >> 1;
+    const int wm = warp % WM, wn = warp / WM;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll

@@ -158,7 +158,6 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* 
     const int ne = n_even(m, L);
     const int nl = par ? n_odd(m, L) : ne;
     const long roff = m_off(m, L) + (par ? ne : 0) + l0;
-    const double sgn = par ? -1.0 : 1.0;
     const double* pa = iPtab + roff * nth2;
     const double* pm = p2 + (long)m * nth * ncol;
     Acc acc;
@@ -173,7 +172,6 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* 
         const double n = __ldg(pm + (long)(nth - 1 - k) * ncol + col);
         return par ? (s - n) : (s + n);
     };
-    (void)sgn;
     gemm_tile<false, true>(acc, fa, fb, nth2, sm);
     double* out = s2 + roff * ncol;
     acc_foreach(acc, [&](int x, int y, double v) {

@@ -40,20 +40,36 @@ __device__ __forceinline__ double2 twiddle(const double2* wr, int N, int e, int 
     return w;
 }
 
+__device__ __forceinline__ void dft4(double2& u0, double2& u1, double2& u2, double2& u3, int sign) {
+    const double2 t0 = cadd(u0, u2), t1 = csub(u0, u2);
+    const double2 t2 = cadd(u1, u3), d = csub(u1, u3);
+    // w = sign * i : w * (x + i y) = sign * (-y + i x)
+    const double2 wd = make_double2(-sign * d.y, sign * d.x);
+    u0 = cadd(t0, t2);
+    u2 = csub(t0, t2);
+    u1 = cadd(t1, wd);
+    u3 = csub(t1, wd);
+}
+
 __device__ __forceinline__ void dft_small(int R, double2* u, int sign) {
     if (R == 2) {
         const double2 a = u[0], b = u[1];
         u[0] = cadd(a, b);
         u[1] = csub(a, b);
     } else if (R == 4) {
-        const double2 t0 = cadd(u[0], u[2]), t1 = csub(u[0], u[2]);
-        const double2 t2 = cadd(u[1], u[3]), d = csub(u[1], u[3]);
-        // w = sign * i : w * (x + i y) = sign * (-y + i x)
-        const double2 wd = make_double2(-sign * d.y, sign * d.x);
-        u[0] = cadd(t0, t2);
-        u[2] = csub(t0, t2);
-        u[1] = cadd(t1, wd);
-        u[3] = csub(t1, wd);
+        dft4(u[0], u[1], u[2], u[3], sign);
+    } else if (R == 8) {
+        const double H = 0.70710678118654752440;   // sqrt(2)/2
+        double2 a0 = cadd(u[0], u[4]), a1 = cadd(u[1], u[5]), a2 = cadd(u[2], u[6]), a3 = cadd(u[3], u[7]);
+        double2 b0 = csub(u[0], u[4]), b1 = csub(u[1], u[5]), b2 = csub(u[2], u[6]), b3 = csub(u[3], u[7]);
+        // b_j *= exp(sign i pi j / 4)
+        b1 = make_double2(H * (b1.x - sign * b1.y), H * (b1.y + sign * b1.x));
+        b2 = make_double2(-sign * b2.y, sign * b2.x);
+        b3 = make_double2(H * (-b3.x - sign * b3.y), H * (-b3.y + sign * b3.x));
+        dft4(a0, a1, a2, a3, sign);
+        dft4(b0, b1, b2, b3, sign);
+        u[0] = a0; u[2] = a1; u[4] = a2; u[6] = a3;
+        u[1] = b0; u[3] = b1; u[5] = b2; u[7] = b3;
     } else {  // R == 3
         const double S3 = 0.86602540378443864676;
         const double2 t = cadd(u[1], u[2]), d = csub(u[1], u[2]);
@@ -65,25 +81,35 @@ __device__ __forceinline__ void dft_small(int R, double2* u, int sign) {
     }
 }
 
-// Runs the FFT on the data in a (b is scratch); returns the buffer holding the result.
-// Must be entered with a synchronised input; leaves the result synchronised.
-__device__ double2* fft_run(double2* a, double2* b, const FFTPlan& pl, const double2* wr, int sign) {
+// Runs nb independent FFTs of length N stored at a + b*N (b < nb), scratch at
+// bb + b*N; returns the buffer base holding the results.  Must be entered with
+// a synchronised input; leaves the result synchronised.
+__device__ double2* fft_run(double2* a, double2* bb, int nb, const FFTPlan& pl, const double2* wr, int sign) {
     const int N = pl.n;
     int p = 1;
     double2* src = a;
-    double2* dst = b;
+    double2* dst = bb;
     for (int ps = 0; ps < pl.npass; ++ps) {
         const int R = pl.radix[ps];
         const int T = N / R;
         const int stride = N / (p * R);
-        for (int bi = threadIdx.x; bi < T; bi += blockDim.x) {
+        for (int g = threadIdx.x; g < T * nb; g += blockDim.x) {
+            const int b = g / T, bi = g - b * T;
+            const double2* sb = src + b * N;
+            double2* db = dst + b * N;
             const int k = bi % p;
-            double2 u[4];
-            for (int r = 0; r < R; ++r) u[r] = src[bi + r * T];
-            for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle(wr, N, r * k * stride, sign));
+            double2 u[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < R) u[r] = sb[bi + r * T];
+#pragma unroll
+            for (int r = 1; r < 8; ++r)
+                if (r < R) u[r] = cmul(u[r], twiddle(wr, N, r * k * stride, sign));
             dft_small(R, u, sign);
             const int j = (bi - k) * R + k;
-            for (int r = 0; r < R; ++r) dst[j + r * p] = u[r];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < R) db[j + r * p] = u[r];
         }
         __syncthreads();
         double2* t = src;
@@ -92,6 +118,64 @@ __device__ double2* fft_run(double2* a, double2* b, const FFTPlan& pl, const dou
         p *= R;
     }
     return src;
+}
+
+// ---- compile-time plans: the same greedy radix order as make_plan (8, 4, 2, 3) ----
+__host__ __device__ constexpr int radix_at(int n, int i) {
+    int m = n, k = 0;
+    while (m % 8 == 0) { if (k == i) return 8; m /= 8; ++k; }
+    while (m % 4 == 0) { if (k == i) return 4; m /= 4; ++k; }
+    while (m % 2 == 0) { if (k == i) return 2; m /= 2; ++k; }
+    while (m % 3 == 0) { if (k == i) return 3; m /= 3; ++k; }
+    return 0;
+}
+__host__ __device__ constexpr int npass_of(int n) {
+    int k = 0;
+    while (radix_at(n, k) != 0) ++k;
+    return k;
+}
+__host__ __device__ constexpr int pprod(int n, int i) {
+    int p = 1;
+    for (int j = 0; j < i; ++j) p *= radix_at(n, j);
+    return p;
+}
+
+template <int N, int NB, int NT, int PS>
+__device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, double2* __restrict__ dst,
+                                           const double2* __restrict__ wr, int sign) {
+    constexpr int R = radix_at(N, PS);
+    constexpr int P = pprod(N, PS);
+    constexpr int T = N / R;
+    constexpr int STRIDE = N / (P * R);
+#pragma unroll 1
+    for (int g = threadIdx.x; g < T * NB; g += NT) {
+        const int b = g / T, bi = g - b * T;
+        const double2* sb = src + b * N;
+        double2* db = dst + b * N;
+        const int k = bi % P;
+        double2 u[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = sb[bi + r * T];
+        if (P > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle(wr, N, r * k * STRIDE, sign));
+        }
+        dft_small(R, u, sign);
+        const int j = (bi - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) db[j + r * P] = u[r];
+    }
+}
+
+template <int N, int NB, int NT, int PS = 0>
+__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* wr, int sign) {
+    if constexpr (PS < npass_of(N)) {
+        fft_pass_t<N, NB, NT, PS>(a, b, wr, sign);
+        __syncthreads();
+        return fft_run_t<N, NB, NT, PS + 1>(b, a, wr, sign);
+    } else {
+        return a;
+    }
 }
 
 struct PhysParams {
@@ -108,75 +192,55 @@ struct PhysParams {
     FFTPlan plan;
 };
 
-// c2r of one field of the row into a (real pairs y[2n], y[2n+1] at index n).
-template <int ZPT>
-__device__ __forceinline__ void row_c2r(const PhysParams& P, int th, int r, int f, bool dphi, double2* bufA,
-                                        double2* bufB, const double2* wr, double2 (&out)[ZPT]) {
-    const int N = P.nth, L = P.L;
+constexpr int FB = 4;   // fields per batched FFT pass
+
+// Batched c2r of up to FB fields of one (r, theta) row.  fields[b] >= 0 is the
+// p2a field index, dphi[b] selects d/dphi (i m X_m).  Result: y[2n], y[2n+1]
+// of field b at res[b*N + n].
+template <int NTH, int NB>
+__device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int* fields, const bool* dphi,
+                                  double2* bufA, double2* bufB, const double2* wr) {
+    constexpr int N = NTH, nb = NB;
+    const int L = P.L;
     const long mstride = (long)P.nth * P.ncola;
-    const double* base = P.p2a + (long)th * P.ncola + ((long)f * P.nr + r) * 2;
-    for (int q = 0; q < ZPT; ++q) {
-        const int k = threadIdx.x + q * PHYS_THREADS;
-        if (k >= N) break;
-        double2 xk = make_double2(0.0, 0.0), xn = make_double2(0.0, 0.0);
-        if (k < L) xk = *reinterpret_cast<const double2*>(base + k * mstride);
-        const int kn = N - k;   // X_{N-k}; X_N (Nyquist) is zero since L <= N
-        if (kn < L) xn = *reinterpret_cast<const double2*>(base + kn * mstride);
-        if (dphi) {
-            xk = make_double2(-k * xk.y, k * xk.x);
-            xn = make_double2(-kn * xn.y, kn * xn.x);
+    // stage the spectra X_m (m < L) in bufB
+#pragma unroll
+    for (int b = 0; b < nb; ++b) {
+        const double* base = P.p2a + (long)th * P.ncola + ((long)fields[b] * P.nr + r) * 2;
+        const bool dp = dphi[b];
+        for (int m = threadIdx.x; m < L; m += PHYS_THREADS) {
+            double2 x = *reinterpret_cast<const double2*>(base + m * mstride);
+            if (dp) x = make_double2(-m * x.y, m * x.x);
+            if (m == 0) x.y = 0.0;   // c2r ignores Im X_0 (FFTW's Hermitian convention)
+            bufB[b * N + m] = x;
         }
-        if (k == 0) xk.y = 0.0;   // c2r ignores Im X_0 (FFTW's Hermitian convention)
-        // Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N)
-        const double2 e = cadd(xk, cconj(xn));
-        const double2 d = csub(xk, cconj(xn));
-        const double2 wd = cmul(wr[k], d);
-        bufA[k] = make_double2(e.x - wd.y, e.y + wd.x);
     }
     __syncthreads();
-    double2* res = fft_run(bufA, bufB, P.plan, wr, +1);
-    for (int q = 0; q < ZPT; ++q) {
-        const int n = threadIdx.x + q * PHYS_THREADS;
-        out[q] = (n < N) ? res[n] : make_double2(0.0, 0.0);
+    // Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N); X_m = 0 for m >= L
+#pragma unroll
+    for (int b = 0; b < nb; ++b) {
+        for (int k = threadIdx.x; k < N; k += PHYS_THREADS) {
+            const double2 xk = (k < L) ? bufB[b * N + k] : make_double2(0.0, 0.0);
+            const int kn = N - k;
+            const double2 xn = (kn < L) ? bufB[b * N + kn] : make_double2(0.0, 0.0);
+            const double2 e = cadd(xk, cconj(xn));
+            const double2 d = csub(xk, cconj(xn));
+            const double2 wd = cmul(wr[k], d);
+            bufA[b * N + k] = make_double2(e.x - wd.y, e.y + wd.x);
+        }
     }
     __syncthreads();
+    return fft_run_t<N, NB, PHYS_THREADS>(bufA, bufB, wr, +1);
 }
 
-// r2c of one output row (values in regs as (y[2n], y[2n+1])) -> p2b for m < L.
-template <int ZPT>
-__device__ __forceinline__ void row_r2c(const PhysParams& P, int th, int r, int f, const double2 (&v)[ZPT],
-                                        double2* bufA, double2* bufB, const double2* wr) {
-    const int N = P.nth, L = P.L;
-    for (int q = 0; q < ZPT; ++q) {
-        const int n = threadIdx.x + q * PHYS_THREADS;
-        if (n < N) bufA[n] = v[q];
-    }
-    __syncthreads();
-    double2* Z = fft_run(bufA, bufB, P.plan, wr, -1);
-    const long mstride = (long)P.nth * P.ncolb;
-    double* base = P.p2b + (long)th * P.ncolb + ((long)f * P.nr + r) * 2;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) {
-        const double2 zk = Z[k];
-        const double2 zn = cconj(Z[(N - k) % N]);
-        const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
-        const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
-        // X_k = e - i conj(w^k) d
-        const double2 wc = cconj(wr[k]);
-        const double2 wd = cmul(wc, d);
-        double2 X = make_double2(e.x + wd.y, e.y - wd.x);
-        if (k == 0) X.y = 0.0;
-        *reinterpret_cast<double2*>(base + k * mstride) = X;
-    }
-    __syncthreads();
-}
-
-template <int ZPT>
-__global__ void __launch_bounds__(PHYS_THREADS) physics_kernel(PhysParams P) {
+template <int NTH>
+__global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) {
+    constexpr int ZPT = (NTH + PHYS_THREADS - 1) / PHYS_THREADS;
+    constexpr int N = NTH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N = P.nth;
     double2* bufA = reinterpret_cast<double2*>(smem_raw);
-    double2* bufB = bufA + N;
-    double2* wr = bufB + N;
+    double2* bufB = bufA + FB * N;
+    double2* wr = bufB + FB * N;
     __shared__ double red[PHYS_THREADS / 32];
     for (int k = threadIdx.x; k < N; k += blockDim.x) wr[k] = P.wr[k];
     const int r = blockIdx.x % P.nr;
@@ -191,108 +255,131 @@ __global__ void __launch_bounds__(PHYS_THREADS) physics_kernel(PhysParams P) {
     const double cor = P.rotation ? P.coriolis : 0.0;
     __syncthreads();
 
-    double2 vr[ZPT], vt[ZPT], vp[ZPT], x[ZPT];
+    double2 vr[ZPT], vt[ZPT], vp[ZPT];
     double2 oW[ZPT], oP[ZPT], oT[ZPT], oZ[ZPT];
-    row_c2r<ZPT>(P, th, r, A_VR, false, bufA, bufB, wr, vr);
-    row_c2r<ZPT>(P, th, r, A_VT, false, bufA, bufB, wr, vt);
-    row_c2r<ZPT>(P, th, r, A_VP, false, bufA, bufB, wr, vp);
+    auto val = [&](const double2* res, int b, int q) -> double2 {
+        const int n = threadIdx.x + q * PHYS_THREADS;
+        return (n < N) ? res[b * N + n] : make_double2(0.0, 0.0);
+    };
+    // batch 1: vr, vt, vp, dvrdr
+    {
+        const int f[FB] = {A_VR, A_VT, A_VP, A_DVRDR};
+        const bool dp[FB] = {false, false, false, false};
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            vr[q] = val(res, 0, q);
+            vt[q] = val(res, 1, q);
+            vp[q] = val(res, 2, q);
+            const double2 x = val(res, 3, q);
+            vt[q].x *= csc; vt[q].y *= csc;
+            vp[q].x *= csc; vp[q].y *= csc;
+            auto w0 = [&](double a, double b, double c, double xx) {
+                return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
+            };
+            auto p0 = [&](double a, double b, double c, double xx) {
+                return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
+            };
+            auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+            oW[q] = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
+            oP[q] = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
+            oZ[q] = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+            oT[q] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+    }
+    // batch 2: dvrdt, dvrdp, dvtdr, dvtdp
+    {
+        const int f[FB] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
+        const bool dp[FB] = {false, true, false, true};
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+        const double c2r = csc * csc * orad;
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            const double2 a = val(res, 0, q), b = val(res, 1, q), c = val(res, 2, q), d = val(res, 3, q);
+            oW[q].x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
+            oW[q].y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
+            oP[q].x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
+            oP[q].y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
+            oZ[q].x += vt[q].x * d.x * c2r;
+            oZ[q].y += vt[q].y * d.y * c2r;
+        }
+        __syncthreads();
+    }
+    // batch 3: dvpdr, dvpdp, omega_r, dTdr
+    {
+        const int f[FB] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
+        const bool dp[FB] = {false, true, false, false};
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+        const double c2r = csc * csc * orad;
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            const double2 a = val(res, 0, q), b = val(res, 1, q), c = val(res, 2, q), d = val(res, 3, q);
+            oZ[q].x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
+            oZ[q].y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
+            oP[q].x += -vt[q].x * b.x * c2r;
+            oP[q].y += -vt[q].y * b.y * c2r;
+            oT[q].x += -vr[q].x * d.x;
+            oT[q].y += -vr[q].y * d.y;
+        }
+        __syncthreads();
+    }
+    // batch 4: dTdt, dTdp
+    {
+        const int f[FB] = {A_DTDT, A_T, 0, 0};
+        const bool dp[FB] = {false, true, false, false};
+        const double2* res = row_c2r_batch<NTH, 2>(P, th, r, f, dp, bufA, bufB, wr);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            const double2 a = val(res, 0, q), b = val(res, 1, q);
+            oT[q].x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+            oT[q].y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+        }
+        __syncthreads();
+    }
+    // CFL (Find_MyMinDT)
     double cmax = 0.0;
     const double hfac = P.llmax * orad * orad, rfac = 1.0 / (dr * dr);
+    const double sfac = rho * rad * csc;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
-        vt[q].x *= csc; vt[q].y *= csc;
-        vp[q].x *= csc; vp[q].y *= csc;
-        const bool live = (threadIdx.x + q * PHYS_THREADS) < N;
-        if (live) {
+        if ((threadIdx.x + q * PHYS_THREADS) < N) {
             cmax = fmax(cmax, (vt[q].x * vt[q].x + vp[q].x * vp[q].x) * hfac);
             cmax = fmax(cmax, (vt[q].y * vt[q].y + vp[q].y * vp[q].y) * hfac);
             cmax = fmax(cmax, vr[q].x * vr[q].x * rfac);
             cmax = fmax(cmax, vr[q].y * vr[q].y * rfac);
         }
-        // velocity-only terms
-        auto w0 = [&](double a, double b, double c) {   // vr, vt, vp
-            return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c);
-        };
-        auto p0 = [&](double a, double b, double c) {
-            return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c;
-        };
-        auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
-        oW[q] = make_double2(w0(vr[q].x, vt[q].x, vp[q].x), w0(vr[q].y, vt[q].y, vp[q].y));
-        oP[q] = make_double2(p0(vr[q].x, vt[q].x, vp[q].x), p0(vr[q].y, vt[q].y, vp[q].y));
-        oZ[q] = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
-        oT[q] = make_double2(0.0, 0.0);
-    }
-#define RA_ACC(dst, expr_x, expr_y)   \
-    {                                 \
-        dst[q].x += (expr_x);         \
-        dst[q].y += (expr_y);         \
-    }
-    // dvrdr
-    row_c2r<ZPT>(P, th, r, A_DVRDR, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        RA_ACC(oW, -rho * rad * rad * vr[q].x * x[q].x, -rho * rad * rad * vr[q].y * x[q].y);
-        RA_ACC(oP, -vt[q].x * x[q].x, -vt[q].y * x[q].y);
-    }
-    // dvrdt (sin theta d vr / d theta)
-    row_c2r<ZPT>(P, th, r, A_DVRDT, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oW, -rho * rad * vt[q].x * x[q].x * csc, -rho * rad * vt[q].y * x[q].y * csc);
-    // dvrdp
-    row_c2r<ZPT>(P, th, r, A_VR, true, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oW, -rho * rad * csc * vp[q].x * x[q].x, -rho * rad * csc * vp[q].y * x[q].y);
-    // dvtdr
-    row_c2r<ZPT>(P, th, r, A_DVTDR, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oP, vr[q].x * x[q].x * csc, vr[q].y * x[q].y * csc);
-    // dvtdp
-    row_c2r<ZPT>(P, th, r, A_VT, true, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        const double sx = x[q].x * csc * csc * orad, sy = x[q].y * csc * csc * orad;
-        RA_ACC(oP, vp[q].x * sx, vp[q].y * sy);
-        RA_ACC(oZ, vt[q].x * sx, vt[q].y * sy);
-    }
-    // dvpdr
-    row_c2r<ZPT>(P, th, r, A_DVPDR, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oZ, vr[q].x * x[q].x * csc, vr[q].y * x[q].y * csc);
-    // dvpdp
-    row_c2r<ZPT>(P, th, r, A_VP, true, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        const double sx = x[q].x * csc * csc * orad, sy = x[q].y * csc * csc * orad;
-        RA_ACC(oP, -vt[q].x * sx, -vt[q].y * sy);
-        RA_ACC(oZ, vp[q].x * sx, vp[q].y * sy);
-    }
-    // omega_r
-    row_c2r<ZPT>(P, th, r, A_OMR, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oZ, vt[q].x * x[q].x, vt[q].y * x[q].y);
-    // dTdr
-    row_c2r<ZPT>(P, th, r, A_DTDR, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oT, -vr[q].x * x[q].x, -vr[q].y * x[q].y);
-    // dTdt (sin theta dT/dtheta)
-    row_c2r<ZPT>(P, th, r, A_DTDT, false, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oT, -x[q].x * csc * vt[q].x * orad, -x[q].y * csc * vt[q].y * orad);
-    // dTdp
-    row_c2r<ZPT>(P, th, r, A_T, true, bufA, bufB, wr, x);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) RA_ACC(oT, -vp[q].x * x[q].x * csc * orad, -vp[q].y * x[q].y * csc * orad);
-#undef RA_ACC
-    const double sfac = rho * rad * csc;
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
         oP[q].x *= sfac; oP[q].y *= sfac;
         oZ[q].x *= sfac; oZ[q].y *= sfac;
     }
-    row_r2c<ZPT>(P, th, r, 0, oW, bufA, bufB, wr);
-    row_r2c<ZPT>(P, th, r, 1, oP, bufA, bufB, wr);
-    row_r2c<ZPT>(P, th, r, 2, oT, bufA, bufB, wr);
-    row_r2c<ZPT>(P, th, r, 3, oZ, bufA, bufB, wr);
+    // batched r2c of W, P, T, Z
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {
+        const int n = threadIdx.x + q * PHYS_THREADS;
+        if (n < N) {
+            bufA[0 * N + n] = oW[q];
+            bufA[1 * N + n] = oP[q];
+            bufA[2 * N + n] = oT[q];
+            bufA[3 * N + n] = oZ[q];
+        }
+    }
+    __syncthreads();
+    double2* Z = fft_run_t<N, 4, PHYS_THREADS>(bufA, bufB, wr, -1);
+    const int L = P.L;
+    const long mstride = (long)P.nth * P.ncolb;
+    for (int g = threadIdx.x; g < 4 * L; g += blockDim.x) {
+        const int f = g / L, k = g - f * L;
+        const double2 zk = Z[f * N + k];
+        const double2 zn = cconj(Z[f * N + (N - k) % N]);
+        const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
+        const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
+        // X_k = e - i conj(w^k) d
+        const double2 wd = cmul(cconj(wr[k]), d);
+        double2 X = make_double2(e.x + wd.y, e.y - wd.x);
+        if (k == 0) X.y = 0.0;
+        double* base = P.p2b + (long)th * P.ncolb + ((long)f * P.nr + r) * 2;
+        *reinterpret_cast<double2*>(base + k * mstride) = X;
+    }
     // CFL max over the row
     for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cmax;
@@ -308,6 +395,7 @@ FFTPlan make_plan(int n) {
     FFTPlan p{};
     p.n = n;
     int m = n;
+    while (m % 8 == 0) { p.radix[p.npass++] = 8; m /= 8; }
     while (m % 4 == 0) { p.radix[p.npass++] = 4; m /= 4; }
     while (m % 2 == 0) { p.radix[p.npass++] = 2; m /= 2; }
     while (m % 3 == 0) { p.radix[p.npass++] = 3; m /= 3; }
@@ -332,20 +420,27 @@ void launch_physics(Ctx& c) {
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
     P.plan = make_plan(c.d.nth);
-    const size_t smem = 3 * (size_t)c.d.nth * sizeof(double2);
+    const size_t smem = (2 * FB + 1) * (size_t)c.d.nth * sizeof(double2);
     const unsigned grid = (unsigned)c.d.nth * c.d.nr;
-    const int zpt = (c.d.nth + PHYS_THREADS - 1) / PHYS_THREADS;
     auto go = [&](auto kern) {
         RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, PHYS_THREADS, smem, c.stream>>>(P);
     };
-    switch (zpt) {
-        case 1: go(physics_kernel<1>); break;
-        case 2: go(physics_kernel<2>); break;
-        case 3: go(physics_kernel<3>); break;
-        case 4: go(physics_kernel<4>); break;
-        case 6: go(physics_kernel<6>); break;
-        default: throw ArgError("unsupported n_theta for the physical-space kernel");
+    switch (c.d.nth) {
+        case 24: go(physics_kernel<24>); break;
+        case 32: go(physics_kernel<32>); break;
+        case 48: go(physics_kernel<48>); break;
+        case 64: go(physics_kernel<64>); break;
+        case 96: go(physics_kernel<96>); break;
+        case 128: go(physics_kernel<128>); break;
+        case 192: go(physics_kernel<192>); break;
+        case 256: go(physics_kernel<256>); break;
+        case 384: go(physics_kernel<384>); break;
+        case 512: go(physics_kernel<512>); break;
+        case 768: go(physics_kernel<768>); break;
+        case 1536: go(physics_kernel<1536>); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) +
+                                " has no physical-space kernel instance (24..1536 of the form 2^a or 3*2^a)");
     }
     RA_CUDA(cudaGetLastError());
     ++c.launches;
@@ -375,7 +470,7 @@ __global__ void fft_rows_kernel(double* x, long howmany, const double2* wrg, FFT
             a[k] = make_double2(e.x - wd.y, e.y + wd.x);
         }
         __syncthreads();
-        double2* res = fft_run(a, b, plan, wr, +1);
+        double2* res = fft_run(a, b, 1, plan, wr, +1);
         for (int n = threadIdx.x; n < N; n += blockDim.x) {
             row[2 * n] = res[n].x;
             row[2 * n + 1] = res[n].y;
@@ -385,7 +480,7 @@ __global__ void fft_rows_kernel(double* x, long howmany, const double2* wrg, FFT
     } else {
         for (int n = threadIdx.x; n < N; n += blockDim.x) a[n] = make_double2(row[2 * n], row[2 * n + 1]);
         __syncthreads();
-        double2* Z = fft_run(a, b, plan, wr, -1);
+        double2* Z = fft_run(a, b, 1, plan, wr, -1);
         for (int k = threadIdx.x; k <= N; k += blockDim.x) {
             const double2 zk = Z[k % N];
             const double2 zn = cconj(Z[(N - k) % N]);

@@ -250,7 +250,9 @@ void launch_rlm_a(Ctx& c) {
 // ---------------------------------------------------------------------------
 // rlm_spaceb: curl algebra on the transformed NL terms, written l-major (p1b)
 // ---------------------------------------------------------------------------
-__global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict__ ab, long nlm, int nr, int L) {
+__global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict__ ab, double* __restrict__ rhs_wpt,
+                             double* __restrict__ rhs_z, long nlm, int nr, int L, double new_ab, double bc_top,
+                             double bc_bot) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
     if (idx >= nlm * nr) return;
     const int r = (int)(idx % nr);
@@ -266,6 +268,7 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
     const double ollp1 = (l > 0) ? 1.0 / ((double)l * (l + 1)) : 1.0;
     const double c1 = sdth_c1(l, m), c2 = sdth_c2(l, m);
     const long plane = nlm * 2 * nr;
+    const bool edge = (r == 0 || r == nr - 1);
 #pragma unroll
     for (int ri = 0; ri < 2; ++ri) {
         const double sg = ri ? (double)m : -(double)m;
@@ -287,17 +290,43 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
         if (l == lmax) {   // :205-208
             W = P = Tt = Z = 0.0;
         }
-        const long o = (lm * 2 + ri) * nr + r;
+        const long col = lm * 2 + ri;
+        const long o = col * nr + r;
         ab[0 * plane + o] = W;
         ab[1 * plane + o] = P;
         ab[2 * plane + o] = Tt;
         ab[3 * plane + o] = Z;
+        // AdvanceTime: Add_To_All_RHS(p1b, new_ab) then Apply_Boundary_Mask
+        // (Sphere_Spectral_Space.F90:427-428, Linear_Solve.F90:401-418, 733-754)
+        double* rw = rhs_wpt + col * 3L * nr + r;
+        if (edge) {
+            const double tb = (col == 0) ? (r == 0 ? bc_top : bc_bot) : 0.0;   // only l = 0 T carries a value
+            rw[0] = 0.0;
+            rw[nr] = 0.0;
+            rw[2 * nr] = tb;
+            rhs_z[o] = 0.0;
+        } else {
+            rw[0] += new_ab * W;
+            rw[nr] += new_ab * P;
+            rw[2 * nr] += new_ab * Tt;
+            rhs_z[o] += new_ab * Z;
+        }
     }
 }
 
-void launch_rlm_b(Ctx& c) {
+static void bc_values(const Ctx& c, double& top, double& bot) {
+    // bc_values for l = 0 T (BoundaryConditions.F90:383-418): sqrt(4 pi) x value
+    const double s4pi = std::sqrt(4.0 * M_PI);
+    top = (c.cfg.fix_tvar_top ? c.cfg.t_top : c.cfg.dtdr_top) * s4pi;
+    bot = (c.cfg.fix_tvar_bottom ? c.cfg.t_bottom : c.cfg.dtdr_bottom) * s4pi;
+}
+
+void launch_rlm_b(Ctx& c, double new_ab) {
     const long total = c.d.nlm * c.d.nr;
-    rlm_b_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2b, c.d_ab, c.d.nlm, c.d.nr, c.d.L);
+    double top, bot;
+    bc_values(c, top, bot);
+    rlm_b_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2b, c.d_ab, c.d_rhs_wpt, c.d_rhs_z,
+                                                                        c.d.nlm, c.d.nr, c.d.L, new_ab, top, bot);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -311,10 +340,8 @@ __global__ void __launch_bounds__(GEMM_THREADS) solve_kernel(const int4* __restr
                                                              const double* __restrict__ Az,
                                                              const double* __restrict__ rhs_wpt,
                                                              const double* __restrict__ rhs_z,
-                                                             const double* __restrict__ ab,
                                                              double* __restrict__ sol_wpt,
-                                                             double* __restrict__ sol_z, long nlm, int nr,
-                                                             double new_ab, double bc_top, double bc_bot) {
+                                                             double* __restrict__ sol_z, int nr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
     const int4 tl = tiles[blockIdx.x];
@@ -323,9 +350,8 @@ __global__ void __launch_bounds__(GEMM_THREADS) solve_kernel(const int4* __restr
     const int ncol = 2 * (l + 1);
     const long lstart = (long)l * (l + 1) / 2;
     const double* A = (sys ? Az : Awpt) + (long)l * n * n;
-    const double* rhs = sys ? rhs_z : rhs_wpt;
-    double* sol = sys ? sol_z : sol_wpt;
-    const long plane = nlm * 2 * nr;
+    const double* rhs = (sys ? rhs_z : rhs_wpt) + lstart * 2 * n;
+    double* sol = (sys ? sol_z : sol_wpt) + lstart * 2 * n;
     Acc acc;
     acc.zero();
     auto fa = [&](int k, int x) -> double {
@@ -334,20 +360,12 @@ __global__ void __launch_bounds__(GEMM_THREADS) solve_kernel(const int4* __restr
     };
     auto fb = [&](int k, int y) -> double {
         const int cc = n0 + y;
-        if (k >= n || cc >= ncol) return 0.0;
-        const long col = lstart * 2 + cc;     // (lm, ri)
-        const int eq = sys ? 3 : k / nr;
-        const int r = sys ? k : k % nr;
-        if (r == 0 || r == nr - 1) {          // Apply_Boundary_Mask: only l = 0 T carries values
-            if (eq == 2 && col == 0) return (r == 0) ? bc_top : bc_bot;
-            return 0.0;
-        }
-        return rhs[col * n + k] + new_ab * ab[eq * plane + col * nr + r];
+        return (k < n && cc < ncol) ? __ldg(rhs + (long)cc * n + k) : 0.0;
     };
     gemm_tile<false, false>(acc, fa, fb, n, sm);
     acc_foreach(acc, [&](int x, int y, double v) {
         const int i = i0 + x, cc = n0 + y;
-        if (i < n && cc < ncol) sol[(lstart * 2 + cc) * n + i] = v;
+        if (i < n && cc < ncol) sol[(long)cc * n + i] = v;
     });
 }
 
@@ -369,19 +387,16 @@ static std::vector<int> solve_tiles(int L, int nr) {
     return t;
 }
 
-void launch_solve(Ctx& c, double new_ab) {
+void launch_solve(Ctx& c) {
     if (!c.d_solve_tiles) {
         std::vector<int> t = solve_tiles(c.d.L, c.d.nr);
         c.n_solve_tiles = (int)(t.size() / 4);
         RA_CUDA(cudaMalloc(&c.d_solve_tiles, t.size() * sizeof(int)));
         RA_CUDA(cudaMemcpy(c.d_solve_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
-    const double s4pi = std::sqrt(4.0 * M_PI);
-    const double bc_top = (c.cfg.fix_tvar_top ? c.cfg.t_top : c.cfg.dtdr_top) * s4pi;
-    const double bc_bot = (c.cfg.fix_tvar_bottom ? c.cfg.t_bottom : c.cfg.dtdr_bottom) * s4pi;
     solve_kernel<<<c.n_solve_tiles, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
-        reinterpret_cast<const int4*>(c.d_solve_tiles), c.d_Awpt, c.d_Az, c.d_rhs_wpt, c.d_rhs_z, c.d_ab,
-        c.d_sol_wpt, c.d_sol_z, c.d.nlm, c.d.nr, new_ab, bc_top, bc_bot);
+        reinterpret_cast<const int4*>(c.d_solve_tiles), c.d_Awpt, c.d_Az, c.d_rhs_wpt, c.d_rhs_z, c.d_sol_wpt,
+        c.d_sol_z, c.d.nr);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }

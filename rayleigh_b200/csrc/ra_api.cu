@@ -445,8 +445,8 @@ static void enqueue_step(Ctx& c, double new_ab, double old_ab) {
     RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
     launch_physics(c);
     launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
-    launch_rlm_b(c);
-    launch_solve(c, new_ab);
+    launch_rlm_b(c, new_ab);
+    launch_solve(c);
 }
 
 static void run_steps(Ctx& c, int nsteps, double* cfl) {
@@ -670,17 +670,17 @@ int ra_physical(ra_ctx* ctx, double* cfl) {
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {
+        double n, o;
+        ab_factors(ctx->c, n, o);
         launch_lt_forward(ctx->c, ctx->c.d_p2b, ctx->c.d_s2b, NP2B * ctx->c.d.nr * 2);
-        launch_rlm_b(ctx->c);
+        launch_rlm_b(ctx->c, n);
     });
 }
 
 int ra_advance(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {
-        double n, o;
-        ab_factors(ctx->c, n, o);
-        launch_solve(ctx->c, n);
+        launch_solve(ctx->c);
         ctx->c.old_dt = ctx->c.dt;
         ++ctx->c.iteration;
     });
@@ -720,9 +720,9 @@ int ra_time_steps(ra_ctx* ctx, int nsteps, double* total_ms, double* kernel_ms, 
                 RA_CUDA(cudaEventRecord(E[5], c.stream));
                 launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
                 RA_CUDA(cudaEventRecord(E[6], c.stream));
-                launch_rlm_b(c);
+                launch_rlm_b(c, new_ab);
                 RA_CUDA(cudaEventRecord(E[7], c.stream));
-                launch_solve(c, new_ab);
+                launch_solve(c);
                 RA_CUDA(cudaEventRecord(E[8], c.stream));
                 c.old_dt = c.dt;
                 ++c.iteration;

@@ -121,8 +121,8 @@ void launch_cheb_synthesis(Ctx& c);
 void launch_post_assemble(Ctx& c, double old_ab);
 void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
-void launch_rlm_b(Ctx& c);
-void launch_solve(Ctx& c, double new_ab);
+void launch_rlm_b(Ctx& c, double new_ab);
+void launch_solve(Ctx& c);
 int  invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip);
 void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse);
 void launch_cheb_columns(Ctx& c, const double* d_in, double* d_out, long ncols, int mode, int order);

@@ -140,39 +140,69 @@ __host__ __device__ constexpr int pprod(int n, int i) {
     return p;
 }
 
+// Shared-memory index swizzle for the FFT buffers: permutes the 8 complex
+// values of each aligned group by XOR with the next 3 index bits, which makes the
+// stride-R writes of the first Stockham passes bank-conflict free.
+__device__ __forceinline__ int SW(int i) { return i ^ ((i >> 3) & 7); }
+
+// Offsets of the per-pass twiddle tables tw[(r-1) P + k] = exp(2 pi i r k STRIDE / N).
+__host__ __device__ constexpr int tw_off(int n, int ps) {
+    int o = 0;
+    for (int j = 0; j < ps; ++j) o += (radix_at(n, j) - 1) * pprod(n, j);
+    return o;
+}
+__host__ __device__ constexpr int tw_size(int n) { return tw_off(n, npass_of(n)); }
+
+// Builds the per-pass tables from the global table wr[k] = exp(2 pi i k / 2N).
+template <int N, int NT, int PS = 0>
+__device__ __forceinline__ void build_twiddles(double2* tw, const double2* __restrict__ wrg) {
+    if constexpr (PS < npass_of(N)) {
+        constexpr int R = radix_at(N, PS), P = pprod(N, PS), STRIDE = N / (P * R);
+        for (int idx = threadIdx.x; idx < (R - 1) * P; idx += NT) {
+            const int r = idx / P + 1, k = idx - (r - 1) * P;
+            const int e = (r * k * STRIDE) % N;
+            tw[tw_off(N, PS) + idx] = (2 * e < N) ? wrg[2 * e] : make_double2(-wrg[2 * e - N].x, -wrg[2 * e - N].y);
+        }
+        build_twiddles<N, NT, PS + 1>(tw, wrg);
+    }
+}
+
 template <int N, int NB, int NT, int PS>
 __device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, double2* __restrict__ dst,
-                                           const double2* __restrict__ wr, int sign) {
+                                           const double2* __restrict__ tw, int sign) {
     constexpr int R = radix_at(N, PS);
     constexpr int P = pprod(N, PS);
     constexpr int T = N / R;
-    constexpr int STRIDE = N / (P * R);
+    constexpr int TO = tw_off(N, PS);
 #pragma unroll 1
     for (int g = threadIdx.x; g < T * NB; g += NT) {
         const int b = g / T, bi = g - b * T;
-        const double2* sb = src + b * N;
-        double2* db = dst + b * N;
+        const int base = b * N;
         const int k = bi % P;
         double2 u[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) u[r] = sb[bi + r * T];
+        for (int r = 0; r < R; ++r) u[r] = src[SW(base + bi + r * T)];
         if (P > 1) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle(wr, N, r * k * STRIDE, sign));
+            for (int r = 1; r < R; ++r) {
+                double2 w = tw[TO + (r - 1) * P + k];
+                if (sign < 0) w.y = -w.y;
+                u[r] = cmul(u[r], w);
+            }
         }
         dft_small(R, u, sign);
         const int j = (bi - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) db[j + r * P] = u[r];
+        for (int r = 0; r < R; ++r) dst[SW(base + j + r * P)] = u[r];
     }
 }
 
 template <int N, int NB, int NT, int PS = 0>
-__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* wr, int sign) {
+__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* tw, int sign) {
     if constexpr (PS < npass_of(N)) {
-        fft_pass_t<N, NB, NT, PS>(a, b, wr, sign);
+        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign);
         __syncthreads();
-        return fft_run_t<N, NB, NT, PS + 1>(b, a, wr, sign);
+        return fft_run_t<N, NB, NT, PS + 1>(b, a, tw, sign);
     } else {
         return a;
     }
@@ -199,20 +229,34 @@ constexpr int FB = 4;   // fields per batched FFT pass
 // of field b at res[b*N + n].
 template <int NTH, int NB>
 __device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int* fields, const bool* dphi,
-                                  double2* bufA, double2* bufB, const double2* wr) {
+                                  double2* bufA, double2* bufB, const double2* tw) {
     constexpr int N = NTH, nb = NB;
+    constexpr int QL = (NTH + PHYS_THREADS - 1) / PHYS_THREADS;   // L <= N
     const int L = P.L;
     const long mstride = (long)P.nth * P.ncola;
-    // stage the spectra X_m (m < L) in bufB
+    // stage the spectra X_m (m < L) in bufB: all loads of the batch issued first
+    double2 xs[NB][QL];
 #pragma unroll
     for (int b = 0; b < nb; ++b) {
         const double* base = P.p2a + (long)th * P.ncola + ((long)fields[b] * P.nr + r) * 2;
+#pragma unroll
+        for (int q = 0; q < QL; ++q) {
+            const int m = threadIdx.x + q * PHYS_THREADS;
+            xs[b][q] = (m < L) ? __ldg(reinterpret_cast<const double2*>(base + m * mstride)) : make_double2(0.0, 0.0);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < nb; ++b) {
         const bool dp = dphi[b];
-        for (int m = threadIdx.x; m < L; m += PHYS_THREADS) {
-            double2 x = *reinterpret_cast<const double2*>(base + m * mstride);
-            if (dp) x = make_double2(-m * x.y, m * x.x);
-            if (m == 0) x.y = 0.0;   // c2r ignores Im X_0 (FFTW's Hermitian convention)
-            bufB[b * N + m] = x;
+#pragma unroll
+        for (int q = 0; q < QL; ++q) {
+            const int m = threadIdx.x + q * PHYS_THREADS;
+            if (m < N) {
+                double2 x = xs[b][q];
+                if (dp) x = make_double2(-m * x.y, m * x.x);
+                if (m == 0) x.y = 0.0;   // c2r ignores Im X_0 (FFTW's Hermitian convention)
+                bufB[SW(b * N + m)] = x;
+            }
         }
     }
     __syncthreads();
@@ -220,17 +264,17 @@ __device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int*
 #pragma unroll
     for (int b = 0; b < nb; ++b) {
         for (int k = threadIdx.x; k < N; k += PHYS_THREADS) {
-            const double2 xk = (k < L) ? bufB[b * N + k] : make_double2(0.0, 0.0);
+            const double2 xk = (k < L) ? bufB[SW(b * N + k)] : make_double2(0.0, 0.0);
             const int kn = N - k;
-            const double2 xn = (kn < L) ? bufB[b * N + kn] : make_double2(0.0, 0.0);
+            const double2 xn = (kn < L) ? bufB[SW(b * N + kn)] : make_double2(0.0, 0.0);
             const double2 e = cadd(xk, cconj(xn));
             const double2 d = csub(xk, cconj(xn));
-            const double2 wd = cmul(wr[k], d);
-            bufA[b * N + k] = make_double2(e.x - wd.y, e.y + wd.x);
+            const double2 wd = cmul(__ldg(P.wr + k), d);
+            bufA[SW(b * N + k)] = make_double2(e.x - wd.y, e.y + wd.x);
         }
     }
     __syncthreads();
-    return fft_run_t<N, NB, PHYS_THREADS>(bufA, bufB, wr, +1);
+    return fft_run_t<N, NB, PHYS_THREADS>(bufA, bufB, tw, +1);
 }
 
 template <int NTH>
@@ -240,9 +284,9 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* bufA = reinterpret_cast<double2*>(smem_raw);
     double2* bufB = bufA + FB * N;
-    double2* wr = bufB + FB * N;
+    double2* tw = bufB + FB * N;
     __shared__ double red[PHYS_THREADS / 32];
-    for (int k = threadIdx.x; k < N; k += blockDim.x) wr[k] = P.wr[k];
+    build_twiddles<N, PHYS_THREADS>(tw, P.wr);
     const int r = blockIdx.x % P.nr;
     const int th = blockIdx.x / P.nr;
     const int nr = P.nr;
@@ -259,13 +303,13 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     double2 oW[ZPT], oP[ZPT], oT[ZPT], oZ[ZPT];
     auto val = [&](const double2* res, int b, int q) -> double2 {
         const int n = threadIdx.x + q * PHYS_THREADS;
-        return (n < N) ? res[b * N + n] : make_double2(0.0, 0.0);
+        return (n < N) ? res[SW(b * N + n)] : make_double2(0.0, 0.0);
     };
     // batch 1: vr, vt, vp, dvrdr
     {
         const int f[FB] = {A_VR, A_VT, A_VP, A_DVRDR};
         const bool dp[FB] = {false, false, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             vr[q] = val(res, 0, q);
@@ -292,7 +336,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
         const bool dp[FB] = {false, true, false, true};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
         const double c2r = csc * csc * orad;
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
@@ -310,7 +354,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
         const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, wr);
+        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
         const double c2r = csc * csc * orad;
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
@@ -328,7 +372,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DTDT, A_T, 0, 0};
         const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 2>(P, th, r, f, dp, bufA, bufB, wr);
+        const double2* res = row_c2r_batch<NTH, 2>(P, th, r, f, dp, bufA, bufB, tw);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             const double2 a = val(res, 0, q), b = val(res, 1, q);
@@ -357,24 +401,24 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     for (int q = 0; q < ZPT; ++q) {
         const int n = threadIdx.x + q * PHYS_THREADS;
         if (n < N) {
-            bufA[0 * N + n] = oW[q];
-            bufA[1 * N + n] = oP[q];
-            bufA[2 * N + n] = oT[q];
-            bufA[3 * N + n] = oZ[q];
+            bufA[SW(0 * N + n)] = oW[q];
+            bufA[SW(1 * N + n)] = oP[q];
+            bufA[SW(2 * N + n)] = oT[q];
+            bufA[SW(3 * N + n)] = oZ[q];
         }
     }
     __syncthreads();
-    double2* Z = fft_run_t<N, 4, PHYS_THREADS>(bufA, bufB, wr, -1);
+    double2* Z = fft_run_t<N, 4, PHYS_THREADS>(bufA, bufB, tw, -1);
     const int L = P.L;
     const long mstride = (long)P.nth * P.ncolb;
     for (int g = threadIdx.x; g < 4 * L; g += blockDim.x) {
         const int f = g / L, k = g - f * L;
-        const double2 zk = Z[f * N + k];
-        const double2 zn = cconj(Z[f * N + (N - k) % N]);
+        const double2 zk = Z[SW(f * N + k)];
+        const double2 zn = cconj(Z[SW(f * N + (N - k) % N)]);
         const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
         const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
         // X_k = e - i conj(w^k) d
-        const double2 wd = cmul(cconj(wr[k]), d);
+        const double2 wd = cmul(cconj(__ldg(P.wr + k)), d);
         double2 X = make_double2(e.x + wd.y, e.y - wd.x);
         if (k == 0) X.y = 0.0;
         double* base = P.p2b + (long)th * P.ncolb + ((long)f * P.nr + r) * 2;
@@ -420,25 +464,25 @@ void launch_physics(Ctx& c) {
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
     P.plan = make_plan(c.d.nth);
-    const size_t smem = (2 * FB + 1) * (size_t)c.d.nth * sizeof(double2);
     const unsigned grid = (unsigned)c.d.nth * c.d.nr;
-    auto go = [&](auto kern) {
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (2 * FB * (size_t)n + tw_size(n)) * sizeof(double2);
         RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, PHYS_THREADS, smem, c.stream>>>(P);
     };
     switch (c.d.nth) {
-        case 24: go(physics_kernel<24>); break;
-        case 32: go(physics_kernel<32>); break;
-        case 48: go(physics_kernel<48>); break;
-        case 64: go(physics_kernel<64>); break;
-        case 96: go(physics_kernel<96>); break;
-        case 128: go(physics_kernel<128>); break;
-        case 192: go(physics_kernel<192>); break;
-        case 256: go(physics_kernel<256>); break;
-        case 384: go(physics_kernel<384>); break;
-        case 512: go(physics_kernel<512>); break;
-        case 768: go(physics_kernel<768>); break;
-        case 1536: go(physics_kernel<1536>); break;
+        case 24: go(physics_kernel<24>, 24); break;
+        case 32: go(physics_kernel<32>, 32); break;
+        case 48: go(physics_kernel<48>, 48); break;
+        case 64: go(physics_kernel<64>, 64); break;
+        case 96: go(physics_kernel<96>, 96); break;
+        case 128: go(physics_kernel<128>, 128); break;
+        case 192: go(physics_kernel<192>, 192); break;
+        case 256: go(physics_kernel<256>, 256); break;
+        case 384: go(physics_kernel<384>, 384); break;
+        case 512: go(physics_kernel<512>, 512); break;
+        case 768: go(physics_kernel<768>, 768); break;
+        case 1536: go(physics_kernel<1536>, 1536); break;
         default: throw ArgError("n_theta " + std::to_string(c.d.nth) +
                                 " has no physical-space kernel instance (24..1536 of the form 2^a or 3*2^a)");
     }

@@ -80,7 +80,9 @@ void launch_plm(Ctx& c, const double* d_x, const double* d_w) {
 }
 
 // ---------------------------------------------------------------------------
-// Inverse transform: p2[m][theta][col] = sum_l P(l, theta) s2[row(m, l)][col]
+// Inverse transform, per (m, parity):
+//   p2[m][par][theta_h][col] = sum_l P_par(l, theta_h) s2[row(m, l)][col]
+// (E for par = 0, O for par = 1; the physical-space kernel forms E +- O)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(GEMM_THREADS) lt_inverse_kernel(const double* __restrict__ Ptab,
                                                                   const double* __restrict__ s2,
@@ -88,60 +90,44 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_inverse_kernel(const double* 
                                                                   int ncol) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
-    const int m = blockIdx.z;
+    const int m = blockIdx.z >> 1, par = blockIdx.z & 1;
     const int th0 = blockIdx.y * BM;
     const int c0 = blockIdx.x * BN;
     const int nth2 = nth / 2;
-    const long off = m_off(m, L);
-    const int ne = n_even(m, L), no = n_odd(m, L);
-    Acc ae, ao;
-    ae.zero();
-    ao.zero();
-    {
-        const double* pa = Ptab + off * nth2;
-        const double* pb = s2 + off * ncol;
-        auto fa = [&](int k, int x) -> double {
-            const int th = th0 + x;
-            return (k < ne && th < nth2) ? __ldg(pa + (long)k * nth2 + th) : 0.0;
-        };
-        auto fb = [&](int k, int y) -> double {
-            const int col = c0 + y;
-            return (k < ne && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
-        };
-        gemm_tile<true, true>(ae, fa, fb, ne, sm);
-    }
-    {
-        const double* pa = Ptab + (off + ne) * nth2;
-        const double* pb = s2 + (off + ne) * ncol;
-        auto fa = [&](int k, int x) -> double {
-            const int th = th0 + x;
-            return (k < no && th < nth2) ? __ldg(pa + (long)k * nth2 + th) : 0.0;
-        };
-        auto fb = [&](int k, int y) -> double {
-            const int col = c0 + y;
-            return (k < no && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
-        };
-        gemm_tile<true, true>(ao, fa, fb, no, sm);
-    }
-    double* out = p2 + (long)m * nth * ncol;
-    acc_foreach2(ae, ao, [&](int x, int y, double e, double o) {
+    const int ne = n_even(m, L);
+    const int nl = par ? n_odd(m, L) : ne;
+    const long roff = m_off(m, L) + (par ? ne : 0);
+    const double* pa = Ptab + roff * nth2;
+    const double* pb = s2 + roff * ncol;
+    Acc acc;
+    acc.zero();
+    auto fa = [&](int k, int x) -> double {
+        const int th = th0 + x;
+        return (k < nl && th < nth2) ? __ldg(pa + (long)k * nth2 + th) : 0.0;
+    };
+    auto fb = [&](int k, int y) -> double {
+        const int col = c0 + y;
+        return (k < nl && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
+    };
+    gemm_tile<true, true>(acc, fa, fb, nl, sm);
+    double* out = p2 + (long)blockIdx.z * nth2 * ncol;
+    acc_foreach(acc, [&](int x, int y, double v) {
         const int th = th0 + x, col = c0 + y;
-        if (th < nth2 && col < ncol) {
-            out[(long)th * ncol + col] = e + o;
-            out[(long)(nth - 1 - th) * ncol + col] = e - o;
-        }
+        if (th < nth2 && col < ncol) out[(long)th * ncol + col] = v;
     });
 }
 
 void launch_lt_inverse(Ctx& c, const double* s2, double* p2, int ncol) {
-    dim3 grid((ncol + BN - 1) / BN, (c.d.nth2 + BM - 1) / BM, c.d.L);
+    dim3 grid((ncol + BN - 1) / BN, (c.d.nth2 + BM - 1) / BM, 2 * c.d.L);
     lt_inverse_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(c.d_Ptab, s2, p2, c.d.L, c.d.nth, ncol);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
 
 // ---------------------------------------------------------------------------
-// Forward transform: s2[row(m, l)][col] = sum_th iP(l, th) fold_par(p2[m])[th][col]
+// Forward transform, per (m, parity), on the equatorially folded input
+// p2[m][par][theta_h][col] (f_even, f_odd):
+//   s2[row(m, l)][col] = sum_th iP_par(l, th) p2[m][par][th][col]
 // tiles: (m, parity, l-tile) in descending-K order
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* __restrict__ iPtab,
@@ -159,7 +145,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* 
     const int nl = par ? n_odd(m, L) : ne;
     const long roff = m_off(m, L) + (par ? ne : 0) + l0;
     const double* pa = iPtab + roff * nth2;
-    const double* pm = p2 + (long)m * nth * ncol;
+    const double* pm = p2 + ((long)m * 2 + par) * nth2 * ncol;
     Acc acc;
     acc.zero();
     auto fa = [&](int k, int x) -> double {
@@ -167,10 +153,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_forward_kernel(const double* 
     };
     auto fb = [&](int k, int y) -> double {
         const int col = c0 + y;
-        if (k >= nth2 || col >= ncol) return 0.0;
-        const double s = __ldg(pm + (long)k * ncol + col);
-        const double n = __ldg(pm + (long)(nth - 1 - k) * ncol + col);
-        return par ? (s - n) : (s + n);
+        return (k < nth2 && col < ncol) ? __ldg(pm + (long)k * ncol + col) : 0.0;
     };
     gemm_tile<false, true>(acc, fa, fb, nth2, sm);
     double* out = s2 + roff * ncol;

@@ -169,13 +169,13 @@ __device__ __forceinline__ void build_twiddles(double2* tw, const double2* __res
 
 template <int N, int NB, int NT, int PS>
 __device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, double2* __restrict__ dst,
-                                           const double2* __restrict__ tw, int sign) {
+                                           const double2* __restrict__ tw, int sign, int tid) {
     constexpr int R = radix_at(N, PS);
     constexpr int P = pprod(N, PS);
     constexpr int T = N / R;
     constexpr int TO = tw_off(N, PS);
 #pragma unroll 1
-    for (int g = threadIdx.x; g < T * NB; g += NT) {
+    for (int g = tid; g < T * NB; g += NT) {
         const int b = g / T, bi = g - b * T;
         const int base = b * N;
         const int k = bi % P;
@@ -198,11 +198,11 @@ __device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, doub
 }
 
 template <int N, int NB, int NT, int PS = 0>
-__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* tw, int sign) {
+__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* tw, int sign, int tid) {
     if constexpr (PS < npass_of(N)) {
-        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign);
+        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign, tid);
         __syncthreads();
-        return fft_run_t<N, NB, NT, PS + 1>(b, a, tw, sign);
+        return fft_run_t<N, NB, NT, PS + 1>(b, a, tw, sign, tid);
     } else {
         return a;
     }
@@ -222,27 +222,39 @@ struct PhysParams {
     FFTPlan plan;
 };
 
-constexpr int FB = 4;   // fields per batched FFT pass
+constexpr int FB = 4;                       // fields per batched FFT pass
+constexpr int HALF = PHYS_THREADS;          // threads per row
+constexpr int PAIR_THREADS = 2 * HALF;      // one CTA = rows theta and pi - theta
 
-// Batched c2r of up to FB fields of one (r, theta) row.  fields[b] >= 0 is the
-// p2a field index, dphi[b] selects d/dphi (i m X_m).  Result: y[2n], y[2n+1]
-// of field b at res[b*N + n].
+// Batched c2r of up to FB fields of one row.  The inverse Legendre transform
+// stores its even-l and odd-l products E, O separately (theta in the southern
+// half); the row's spectrum is X = E + O (h = 0, theta) or E - O (h = 1, the
+// mirrored row), as StP_4d_dgp2 reflects them (Legendre_Transforms.F90:1030-1064).
+// fields[b] is the p2a field index, dphi[b] selects d/dphi (i m X_m).  Result:
+// y[2n], y[2n+1] of field b at res[SW(b*N + n)].
 template <int NTH, int NB>
-__device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int* fields, const bool* dphi,
-                                  double2* bufA, double2* bufB, const double2* tw) {
+__device__ double2* row_c2r_batch(const PhysParams& P, int thh, int h, int r, const int* fields, const bool* dphi,
+                                  double2* bufA, double2* bufB, const double2* tw, int t) {
     constexpr int N = NTH, nb = NB;
-    constexpr int QL = (NTH + PHYS_THREADS - 1) / PHYS_THREADS;   // L <= N
+    constexpr int QL = (NTH + HALF - 1) / HALF;   // L <= N
     const int L = P.L;
-    const long mstride = (long)P.nth * P.ncola;
-    // stage the spectra X_m (m < L) in bufB: all loads of the batch issued first
+    const int nth2 = P.nth / 2;
+    const long mstride = 2L * nth2 * P.ncola;     // p2a[m][par][theta_h][col]
+    const long ostride = (long)nth2 * P.ncola;    // E -> O
     double2 xs[NB][QL];
 #pragma unroll
     for (int b = 0; b < nb; ++b) {
-        const double* base = P.p2a + (long)th * P.ncola + ((long)fields[b] * P.nr + r) * 2;
+        const double* base = P.p2a + (long)thh * P.ncola + ((long)fields[b] * P.nr + r) * 2;
 #pragma unroll
         for (int q = 0; q < QL; ++q) {
-            const int m = threadIdx.x + q * PHYS_THREADS;
-            xs[b][q] = (m < L) ? __ldg(reinterpret_cast<const double2*>(base + m * mstride)) : make_double2(0.0, 0.0);
+            const int m = t + q * HALF;
+            if (m < L) {
+                const double2 e = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
+                const double2 o = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
+                xs[b][q] = h ? csub(e, o) : cadd(e, o);
+            } else {
+                xs[b][q] = make_double2(0.0, 0.0);
+            }
         }
     }
 #pragma unroll
@@ -250,7 +262,7 @@ __device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int*
         const bool dp = dphi[b];
 #pragma unroll
         for (int q = 0; q < QL; ++q) {
-            const int m = threadIdx.x + q * PHYS_THREADS;
+            const int m = t + q * HALF;
             if (m < N) {
                 double2 x = xs[b][q];
                 if (dp) x = make_double2(-m * x.y, m * x.x);
@@ -263,7 +275,7 @@ __device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int*
     // Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N); X_m = 0 for m >= L
 #pragma unroll
     for (int b = 0; b < nb; ++b) {
-        for (int k = threadIdx.x; k < N; k += PHYS_THREADS) {
+        for (int k = t; k < N; k += HALF) {
             const double2 xk = (k < L) ? bufB[SW(b * N + k)] : make_double2(0.0, 0.0);
             const int kn = N - k;
             const double2 xn = (kn < L) ? bufB[SW(b * N + kn)] : make_double2(0.0, 0.0);
@@ -274,22 +286,25 @@ __device__ double2* row_c2r_batch(const PhysParams& P, int th, int r, const int*
         }
     }
     __syncthreads();
-    return fft_run_t<N, NB, PHYS_THREADS>(bufA, bufB, tw, +1);
+    return fft_run_t<N, NB, HALF>(bufA, bufB, tw, +1, t);
 }
 
 template <int NTH>
-__global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) {
-    constexpr int ZPT = (NTH + PHYS_THREADS - 1) / PHYS_THREADS;
+__global__ void __launch_bounds__(PAIR_THREADS, 1) physics_kernel(PhysParams P) {
+    constexpr int ZPT = (NTH + HALF - 1) / HALF;
     constexpr int N = NTH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* bufA = reinterpret_cast<double2*>(smem_raw);
+    const int h = threadIdx.x / HALF, t = threadIdx.x % HALF;
+    double2* base0 = reinterpret_cast<double2*>(smem_raw);
+    double2* bufA = base0 + h * (2 * FB * N);
     double2* bufB = bufA + FB * N;
-    double2* tw = bufB + FB * N;
-    __shared__ double red[PHYS_THREADS / 32];
-    build_twiddles<N, PHYS_THREADS>(tw, P.wr);
-    const int r = blockIdx.x % P.nr;
-    const int th = blockIdx.x / P.nr;
+    double2* tw = base0 + 2 * (2 * FB * N);
+    __shared__ double red[PAIR_THREADS / 32];
+    build_twiddles<N, PAIR_THREADS>(tw, P.wr);
     const int nr = P.nr;
+    const int r = blockIdx.x % nr;
+    const int thh = blockIdx.x / nr;                // southern-half theta index
+    const int th = h ? (N - 1 - thh) : thh;         // this half's row
     const double rad = P.radial[R_RADIUS * nr + r];
     const double orad = P.radial[R_OVER_R * nr + r];
     const double rho = P.radial[R_DENSITY * nr + r];
@@ -302,14 +317,14 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
     double2 oW[ZPT], oP[ZPT], oT[ZPT], oZ[ZPT];
     auto val = [&](const double2* res, int b, int q) -> double2 {
-        const int n = threadIdx.x + q * PHYS_THREADS;
+        const int n = t + q * HALF;
         return (n < N) ? res[SW(b * N + n)] : make_double2(0.0, 0.0);
     };
     // batch 1: vr, vt, vp, dvrdr
     {
         const int f[FB] = {A_VR, A_VT, A_VP, A_DVRDR};
         const bool dp[FB] = {false, false, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
+        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             vr[q] = val(res, 0, q);
@@ -336,7 +351,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
         const bool dp[FB] = {false, true, false, true};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
+        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
         const double c2r = csc * csc * orad;
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
@@ -354,7 +369,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
         const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, th, r, f, dp, bufA, bufB, tw);
+        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
         const double c2r = csc * csc * orad;
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
@@ -372,7 +387,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     {
         const int f[FB] = {A_DTDT, A_T, 0, 0};
         const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 2>(P, th, r, f, dp, bufA, bufB, tw);
+        const double2* res = row_c2r_batch<NTH, 2>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             const double2 a = val(res, 0, q), b = val(res, 1, q);
@@ -387,7 +402,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     const double sfac = rho * rad * csc;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
-        if ((threadIdx.x + q * PHYS_THREADS) < N) {
+        if ((t + q * HALF) < N) {
             cmax = fmax(cmax, (vt[q].x * vt[q].x + vp[q].x * vp[q].x) * hfac);
             cmax = fmax(cmax, (vt[q].y * vt[q].y + vp[q].y * vp[q].y) * hfac);
             cmax = fmax(cmax, vr[q].x * vr[q].x * rfac);
@@ -399,7 +414,7 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
     // batched r2c of W, P, T, Z
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
-        const int n = threadIdx.x + q * PHYS_THREADS;
+        const int n = t + q * HALF;
         if (n < N) {
             bufA[SW(0 * N + n)] = oW[q];
             bufA[SW(1 * N + n)] = oP[q];
@@ -408,10 +423,10 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
         }
     }
     __syncthreads();
-    double2* Z = fft_run_t<N, 4, PHYS_THREADS>(bufA, bufB, tw, -1);
+    double2* Z = fft_run_t<N, 4, HALF>(bufA, bufB, tw, -1, t);
+    double2* X = (Z == bufA) ? bufB : bufA;   // this half's spectra X_k, k < L
     const int L = P.L;
-    const long mstride = (long)P.nth * P.ncolb;
-    for (int g = threadIdx.x; g < 4 * L; g += blockDim.x) {
+    for (int g = t; g < 4 * L; g += HALF) {
         const int f = g / L, k = g - f * L;
         const double2 zk = Z[SW(f * N + k)];
         const double2 zn = cconj(Z[SW(f * N + (N - k) % N)]);
@@ -419,18 +434,35 @@ __global__ void __launch_bounds__(PHYS_THREADS, 2) physics_kernel(PhysParams P) 
         const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
         // X_k = e - i conj(w^k) d
         const double2 wd = cmul(cconj(__ldg(P.wr + k)), d);
-        double2 X = make_double2(e.x + wd.y, e.y - wd.x);
-        if (k == 0) X.y = 0.0;
-        double* base = P.p2b + (long)th * P.ncolb + ((long)f * P.nr + r) * 2;
-        *reinterpret_cast<double2*>(base + k * mstride) = X;
+        double2 Xk = make_double2(e.x + wd.y, e.y - wd.x);
+        if (k == 0) Xk.y = 0.0;
+        X[SW(f * N + k)] = Xk;
     }
-    // CFL max over the row
+    __syncthreads();
+    // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122):
+    // f_even = X(theta) + X(pi - theta), f_odd = X(theta) - X(pi - theta)
+    {
+        constexpr bool ZA = (npass_of(N) % 2) == 0;   // the FFT result sits in bufA when the pass count is even
+        const double2* Xs = base0 + (ZA ? FB * N : 0);
+        const double2* Xn = base0 + 2 * FB * N + (ZA ? FB * N : 0);
+        const int nth2 = P.nth / 2;
+        const long mstride = 2L * nth2 * P.ncolb;
+        const long ostride = (long)nth2 * P.ncolb;
+        for (int g = threadIdx.x; g < 4 * L; g += PAIR_THREADS) {
+            const int f = g / L, k = g - f * L;
+            const double2 a = Xs[SW(f * N + k)], b = Xn[SW(f * N + k)];
+            double* o = P.p2b + k * mstride + (long)thh * P.ncolb + ((long)f * P.nr + r) * 2;
+            *reinterpret_cast<double2*>(o) = cadd(a, b);
+            *reinterpret_cast<double2*>(o + ostride) = csub(a, b);
+        }
+    }
+    // CFL max over the two rows
     for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cmax;
     __syncthreads();
     if (threadIdx.x == 0) {
         double v = red[0];
-        for (int i = 1; i < PHYS_THREADS / 32; ++i) v = fmax(v, red[i]);
+        for (int i = 1; i < PAIR_THREADS / 32; ++i) v = fmax(v, red[i]);
         atomicMax(P.cfl, (unsigned long long)__double_as_longlong(v));
     }
 }
@@ -464,11 +496,11 @@ void launch_physics(Ctx& c) {
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
     P.plan = make_plan(c.d.nth);
-    const unsigned grid = (unsigned)c.d.nth * c.d.nr;
+    const unsigned grid = (unsigned)c.d.nth2 * c.d.nr;
     auto go = [&](auto kern, int n) {
-        const size_t smem = (2 * FB * (size_t)n + tw_size(n)) * sizeof(double2);
+        const size_t smem = (4 * FB * (size_t)n + tw_size(n)) * sizeof(double2);
         RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, PHYS_THREADS, smem, c.stream>>>(P);
+        kern<<<grid, PAIR_THREADS, smem, c.stream>>>(P);
     };
     switch (c.d.nth) {
         case 24: go(physics_kernel<24>, 24); break;
@@ -482,9 +514,8 @@ void launch_physics(Ctx& c) {
         case 384: go(physics_kernel<384>, 384); break;
         case 512: go(physics_kernel<512>, 512); break;
         case 768: go(physics_kernel<768>, 768); break;
-        case 1536: go(physics_kernel<1536>, 1536); break;
         default: throw ArgError("n_theta " + std::to_string(c.d.nth) +
-                                " has no physical-space kernel instance (24..1536 of the form 2^a or 3*2^a)");
+                                " has no physical-space kernel instance (24..768 of the form 2^a or 3*2^a)");
     }
     RA_CUDA(cudaGetLastError());
     ++c.launches;

@@ -827,14 +827,21 @@ int ra_legendre_s2p(ra_ctx* ctx, const double* s, double* p, int nf, int nr) {
         RA_CUDA(cudaStreamSynchronize(c.stream));
         cudaFree(ds);
         cudaFree(dp);
-        // device p2[m][th][f][r][ri] -> host p2a(th, (r, ri, f), m)
+        // device p2[m][par][th_h][f][r][ri] (E, O) -> host p2a(th, (r, ri, f), m):
+        // south th_h: E + O, north nth-1-th_h: E - O (Legendre_Transforms.F90:1030-1064)
+        const int nth2 = nth / 2;
         for (int m = 0; m < L; ++m)
             for (int f = 0; f < nf; ++f)
                 for (int ri = 0; ri < 2; ++ri)
                     for (int r = 0; r < nr; ++r)
-                        for (int th = 0; th < nth; ++th)
-                            p[((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth + th] =
-                                hp[((size_t)m * nth + th) * ncol + ((size_t)f * nr + r) * 2 + ri];
+                        for (int th = 0; th < nth2; ++th) {
+                            const size_t cidx = ((size_t)f * nr + r) * 2 + ri;
+                            const double e = hp[(((size_t)m * 2 + 0) * nth2 + th) * ncol + cidx];
+                            const double o = hp[(((size_t)m * 2 + 1) * nth2 + th) * ncol + cidx];
+                            double* dst = p + ((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth;
+                            dst[th] = e + o;
+                            dst[nth - 1 - th] = e - o;
+                        }
     });
 }
 
@@ -846,13 +853,18 @@ int ra_legendre_p2s(ra_ctx* ctx, const double* p, double* s, int nf, int nr) {
         const int L = c.d.L, nth = c.d.nth;
         const int ncol = nf * nr * 2;
         std::vector<double> hs((size_t)c.d.nlm * ncol), hp((size_t)L * nth * ncol);
+        // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122) into p2[m][par][th_h][col]
+        const int nth2 = nth / 2;
         for (int m = 0; m < L; ++m)
             for (int f = 0; f < nf; ++f)
                 for (int ri = 0; ri < 2; ++ri)
                     for (int r = 0; r < nr; ++r)
-                        for (int th = 0; th < nth; ++th)
-                            hp[((size_t)m * nth + th) * ncol + ((size_t)f * nr + r) * 2 + ri] =
-                                p[((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth + th];
+                        for (int th = 0; th < nth2; ++th) {
+                            const size_t cidx = ((size_t)f * nr + r) * 2 + ri;
+                            const double* src = p + ((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth;
+                            hp[(((size_t)m * 2 + 0) * nth2 + th) * ncol + cidx] = src[th] + src[nth - 1 - th];
+                            hp[(((size_t)m * 2 + 1) * nth2 + th) * ncol + cidx] = src[th] - src[nth - 1 - th];
+                        }
         double *ds = nullptr, *dp = nullptr;
         dalloc(ds, hs.size());
         dalloc(dp, hp.size());

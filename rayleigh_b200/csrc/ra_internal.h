@@ -99,8 +99,8 @@ struct Ctx {
     double *d_g = nullptr;                            // [NG][lm][2][nr]
     double *d_s2a = nullptr;                          // [row][NS2A][nr][2]
     double *d_s2a11 = nullptr;                        // [row][NP2A][nr][2]
-    double *d_p2a = nullptr;                          // [m][nth][NP2A][nr][2]
-    double *d_p2b = nullptr;                          // [m][nth][4][nr][2]
+    double *d_p2a = nullptr;                          // [m][par][nth2][NP2A][nr][2]  E, O
+    double *d_p2b = nullptr;                          // [m][par][nth2][4][nr][2]     f_even, f_odd
     double *d_s2b = nullptr;                          // [row][4][nr][2]
     unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
     int *d_status = nullptr;                          // device error word

@@ -40,3 +40,21 @@ def rel_err(a, b):
     if den == 0:
         return float(np.linalg.norm(a.ravel()))
     return float(np.linalg.norm((a - b).ravel()) / den)
+
+
+def p2_eo_to_full(dev, L, nth, F, nr):
+    """device [m][par][nth/2][F][nr][2] (E, O) -> [m][nth][F][nr][2] with south E+O, north E-O."""
+    d = dev.reshape(L, 2, nth // 2, F, nr, 2)
+    e, o = d[:, 0], d[:, 1]
+    full = np.empty((L, nth, F, nr, 2))
+    full[:, :nth // 2] = e + o
+    full[:, nth - 1:nth // 2 - 1:-1] = e - o
+    return full
+
+
+def p2_fold(full):
+    """[m][nth][F][nr][2] -> [m][2][nth/2][F][nr][2] folded (s + n, s - n)."""
+    nth = full.shape[1]
+    s = full[:, :nth // 2]
+    n = full[:, nth - 1:nth // 2 - 1:-1]
+    return np.stack([s + n, s - n], axis=1)

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from layouts import p2_to_dev, rel_err, row_index, s2_to_rows
+from layouts import p2_eo_to_full, p2_fold, p2_to_dev, rel_err, row_index, s2_to_rows
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -133,10 +133,11 @@ def _stage_compare(cfg, steps_before=0, amp=1e-2):
     g.rlm_spacea()
     a_fields = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]
     errs["s2a11"] = rel_err(g.debug_buffer("s2a11"), s2_to_rows(s2a12, a_fields).ravel())
-    errs["p2a"] = rel_err(g.debug_buffer("p2a"), p2_to_dev(p2a, a_fields).ravel())
+    errs["p2a"] = rel_err(p2_eo_to_full(g.debug_buffer("p2a"), L, nth, len(a_fields), nr),
+                          p2_to_dev(p2a, a_fields))
     cfl = g.physical_space()
     errs["cfl"] = abs(cfl - cfl_ref) / max(cfl_ref, 1e-300)
-    errs["p2b"] = rel_err(g.debug_buffer("p2b"), p2_to_dev(p2b, [0, 1, 2, 3]).ravel())
+    errs["p2b"] = rel_err(g.debug_buffer("p2b"), p2_fold(p2_to_dev(p2b, [0, 1, 2, 3])).ravel())
     g.rlm_spaceb()
     errs["s2b"] = rel_err(g.debug_buffer("s2b"), s2_to_rows(s2b, [0, 1, 2, 3]).ravel())
     errs["ab"] = rel_err(g.debug_buffer("ab"), ab.ravel())

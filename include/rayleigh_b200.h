@@ -141,6 +141,14 @@ int ra_cheby_to_spectral(ra_ctx* ctx, const double* f, double* c, long ncols);
 int ra_cheby_from_spectral(ra_ctx* ctx, const double* c, double* f, long ncols);
 int ra_cheby_deriv(ra_ctx* ctx, const double* c, double* dc, int order, long ncols);
 
+/* Split-precision product on the tensor cores, the engine of RA_PREC_MIXED:
+ * C = A B with A (m x k) and B (k x n) row-major host arrays, C (m x n)
+ * row-major; each operand is cut into 6 int8 digits per element (rows of A,
+ * columns of B scaled by powers of two) and the 21 leading digit products are
+ * accumulated exactly in int32 by tcgen05 before an FP64 recombination.
+ * Replaces, for the parity tests, the DGEMM calls of Legendre_Transforms.F90:1028-1150. */
+int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* c, int m, int n, int k);
+
 /* Radial grid of the context: radius(n_r), r(1) = r_max (Chebyshev_Polynomials.F90:168-200). */
 int ra_radius(const ra_ctx* ctx, double* radius);
 /* Gauss-Legendre nodes cos(theta) (n_theta) as used by the context. */

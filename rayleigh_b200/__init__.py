@@ -136,6 +136,7 @@ def load_library(path: str | None = None):
         "ra_time_steps": ([_VP, ctypes.c_int, _DP, _DP, ctypes.c_int], ctypes.c_int),
         "ra_kernels_per_step": ([], ctypes.c_int),
         "ra_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
+        "ra_mixed_gemm": ([_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -312,6 +313,18 @@ class Rayleigh:
         x = _f64(x).copy()
         self._check(self.lib.ra_fft_r2c(self.h, _ptr(x), x.size // (self.n_phi + 2)))
         return x
+
+    def mixed_gemm(self, a, b):
+        """Split-precision tensor-core product a @ b (FP64 in and out)."""
+        a = _f64(a)
+        b = _f64(b)
+        m, k = a.shape
+        k2, n = b.shape
+        if k != k2:
+            raise ValueError("inner dimensions differ")
+        out = np.empty((m, n))
+        self._check(self.lib.ra_mixed_gemm(self.h, _ptr(a), _ptr(b), _ptr(out), m, n, k))
+        return out
 
     def cheby_to_spectral(self, f):
         f = _f64(f)

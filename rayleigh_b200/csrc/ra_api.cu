@@ -14,6 +14,7 @@
 #include <new>
 
 #include "ra_internal.h"
+#include "ozaki.h"
 
 using namespace ra;
 
@@ -923,6 +924,48 @@ static int cheb_op(ra_ctx* ctx, const double* in, double* out, long ncols, int m
         RA_CUDA(cudaStreamSynchronize(c.stream));
         cudaFree(di);
         cudaFree(dout);
+    });
+}
+
+int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* cc, int m, int n, int k) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!a || !b || !cc || m <= 0 || n <= 0 || k <= 0) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (k > OZ_MAX_K) throw ArgError("ra_mixed_gemm: k exceeds the exact int32 accumulation limit");
+        Ctx& c = ctx->c;
+        const int mp = oz_round_m(m), np = oz_round_n(n), kp = oz_round_k(k);
+        double *da = nullptr, *db = nullptr, *dc = nullptr;
+        int8_t *sa = nullptr, *sb = nullptr;
+        int *ea = nullptr, *eb = nullptr, *dst = nullptr, *dtiles = nullptr;
+        OzProblem* dprob = nullptr;
+        dalloc(da, (size_t)m * k);
+        dalloc(db, (size_t)k * n);
+        dalloc(dc, (size_t)m * n);
+        RA_CUDA(cudaMalloc(&sa, (size_t)OZ_S * mp * kp));
+        RA_CUDA(cudaMalloc(&sb, (size_t)OZ_S * np * kp));
+        RA_CUDA(cudaMalloc(&ea, (size_t)mp * sizeof(int)));
+        RA_CUDA(cudaMalloc(&eb, (size_t)np * sizeof(int)));
+        RA_CUDA(cudaMalloc(&dst, sizeof(int)));
+        RA_CUDA(cudaMemsetAsync(dst, 0, sizeof(int), c.stream));
+        RA_CUDA(cudaMemcpyAsync(da, a, (size_t)m * k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(db, b, (size_t)k * n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        ozaki_split(c, da, k, 1, m, k, mp, kp, sa, (long)mp * kp, ea);   // rows of A
+        ozaki_split(c, db, 1, n, n, k, np, kp, sb, (long)np * kp, eb);   // columns of B
+        OzProblem pr{sa, sb, (long)mp * kp, (long)np * kp, ea, eb, m, n, kp, dc, n, 1};
+        std::vector<OzProblem> probs{pr};
+        std::vector<int> tiles = ozaki_tiles(probs);
+        RA_CUDA(cudaMalloc(&dprob, sizeof(OzProblem)));
+        RA_CUDA(cudaMalloc(&dtiles, tiles.size() * sizeof(int)));
+        RA_CUDA(cudaMemcpyAsync(dprob, probs.data(), sizeof(OzProblem), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(dtiles, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        ozaki_gemm(c, dprob, dtiles, (int)(tiles.size() / 4), dst);
+        int status = 0;
+        RA_CUDA(cudaMemcpyAsync(cc, dc, (size_t)m * n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaMemcpyAsync(&status, dst, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        cudaFree(da); cudaFree(db); cudaFree(dc); cudaFree(sa); cudaFree(sb);
+        cudaFree(ea); cudaFree(eb); cudaFree(dst); cudaFree(dprob); cudaFree(dtiles);
+        if (status) throw ArgError("tensor-core product timed out waiting on its pipeline barrier");
     });
 }
 

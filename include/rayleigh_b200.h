@@ -149,6 +149,20 @@ int ra_cheby_deriv(ra_ctx* ctx, const double* c, double* dc, int order, long nco
  * Replaces, for the parity tests, the DGEMM calls of Legendre_Transforms.F90:1028-1150. */
 int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* c, int m, int n, int k);
 
+/* Allocation-free form of ra_mixed_gemm, for callers that cannot allocate
+ * device memory.  No counterpart in the reference.  a (m x k), b (k x n) and
+ * c (m x n) are row-major DEVICE arrays on the current device; the work is
+ * enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) and the
+ * call returns after it finished.  Scratch comes from one fixed 16 MiB
+ * device array inside the library (about 6 (m + n) k bytes are needed;
+ * larger products return RA_ERR_ARG with the needed size in msg).  The
+ * first call on each device looks up that array's address: make it before
+ * any stream capture.  Calls that overlap in time on one device race on the
+ * shared scratch.  msg (may be NULL) receives an error message of at most
+ * msg_len bytes. */
+int ra_mixed_gemm_noalloc(const double* a, const double* b, double* c, int m, int n, int k, void* stream,
+                          char* msg, int msg_len);
+
 /* Radial grid of the context: radius(n_r), r(1) = r_max (Chebyshev_Polynomials.F90:168-200). */
 int ra_radius(const ra_ctx* ctx, double* radius);
 /* Gauss-Legendre nodes cos(theta) (n_theta) as used by the context. */

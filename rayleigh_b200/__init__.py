@@ -137,6 +137,8 @@ def load_library(path: str | None = None):
         "ra_kernels_per_step": ([], ctypes.c_int),
         "ra_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "ra_mixed_gemm": ([_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "ra_mixed_gemm_noalloc": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p,
+                                   ctypes.c_int], ctypes.c_int),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():

@@ -20,6 +20,7 @@
 // commits them to the stage's mbarrier; the accumulators (6 x 64 columns of
 // int32) live in tensor memory and are read back with tcgen05.ld.
 #include <cstdint>
+#include <cstdio>
 
 #include "ra_internal.h"
 #include "ozaki.h"
@@ -310,4 +311,123 @@ int oz_round_m(int m) { return (m + OZ_BM - 1) / OZ_BM * OZ_BM; }
 int oz_round_n(int n) { return (n + OZ_BN - 1) / OZ_BN * OZ_BN; }
 int oz_round_k(int k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
 
+// ---------------------------------------------------------------------------
+// Allocation-free form of the split-precision product (ra_mixed_gemm_noalloc).
+//
+// All scratch lives in one file-scope device array of fixed size; its device
+// address is looked up once per device (cudaGetSymbolAddress, with that device
+// current) on the first call made on that device.  Scratch layout, every piece
+// 256-byte aligned:
+//   [0]        int   status word      (set to zero by oz_static_prepare_kernel)
+//   [256]      OzProblem              (written by oz_static_prepare_kernel)
+//   [512]      int4  tiles[ntiles]    (written by oz_static_prepare_kernel)
+//   then       int   ea[mp], eb[np]   (written by the split kernel)
+//   then       int8  A digits [S][mp][kp], B digits [S][np][kp] (split kernel)
+// Nothing else needs to start at zero: the split kernel writes every padded
+// digit and every exponent the product reads.  Calls on one device share the
+// array, so calls that overlap in time (two host threads, or two streams)
+// race on it.
+// ---------------------------------------------------------------------------
+constexpr size_t OZ_STATIC_BYTES = (size_t)16 << 20;   // 16 MiB
+static __device__ __align__(256) unsigned char oz_static_scratch[OZ_STATIC_BYTES];
+
+constexpr int OZ_MAX_DEVICES = 64;
+static unsigned char* oz_static_ptr[OZ_MAX_DEVICES] = {};
+
+static size_t oz_align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+__global__ void oz_static_prepare_kernel(OzProblem pr, OzProblem* __restrict__ dprob, int4* __restrict__ tiles,
+                                         int ntm, int ntn, int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *dprob = pr;
+        *status = 0;
+    }
+    if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, 0);
+}
+
 }  // namespace ra
+
+static void oz_set_msg(char* msg, int len, const char* text) {
+    if (!msg || len <= 0) return;
+    int i = 0;
+    for (; text[i] && i < len - 1; ++i) msg[i] = text[i];
+    msg[i] = 0;
+}
+
+extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, double* d_c, int m, int n, int k,
+                                     void* stream, char* msg, int msg_len) {
+    using namespace ra;
+    oz_set_msg(msg, msg_len, "");
+    if (!d_a || !d_b || !d_c || m <= 0 || n <= 0 || k <= 0) {
+        oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: null pointer or non-positive size");
+        return RA_ERR_ARG;
+    }
+    if (k > OZ_MAX_K) {
+        oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: k exceeds the exact int32 accumulation limit (20000)");
+        return RA_ERR_ARG;
+    }
+    const int mp = oz_round_m(m), np = oz_round_n(n), kp = oz_round_k(k);
+    const int ntm = mp / 128, ntn = np / 64, ntiles = ntm * ntn;
+    const size_t off_prob = 256, off_tiles = 512;
+    const size_t off_ea = off_tiles + oz_align256((size_t)ntiles * sizeof(int4));
+    const size_t off_eb = off_ea + oz_align256((size_t)mp * sizeof(int));
+    const size_t off_sa = off_eb + oz_align256((size_t)np * sizeof(int));
+    const size_t off_sb = off_sa + oz_align256((size_t)OZ_S * mp * kp);
+    const size_t need = off_sb + oz_align256((size_t)OZ_S * np * kp);
+    if (need > OZ_STATIC_BYTES) {
+        char text[200];
+        snprintf(text, sizeof(text),
+                 "ra_mixed_gemm_noalloc: m=%d n=%d k=%d needs %zu bytes of scratch; the static limit is %zu bytes (16 MiB)",
+                 m, n, k, need, OZ_STATIC_BYTES);
+        oz_set_msg(msg, msg_len, text);
+        return RA_ERR_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= OZ_MAX_DEVICES) {
+        oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: no usable current device");
+        return RA_ERR_CUDA;
+    }
+    if (!oz_static_ptr[dev]) {   // first call on this device: resolve the scratch address
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, oz_static_scratch);
+        if (e != cudaSuccess || !p) {
+            oz_set_msg(msg, msg_len, cudaGetErrorString(e));
+            return RA_ERR_CUDA;
+        }
+        oz_static_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    unsigned char* base = oz_static_ptr[dev];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int* d_status = reinterpret_cast<int*>(base);
+    OzProblem* d_prob = reinterpret_cast<OzProblem*>(base + off_prob);
+    int4* d_tiles = reinterpret_cast<int4*>(base + off_tiles);
+    int* ea = reinterpret_cast<int*>(base + off_ea);
+    int* eb = reinterpret_cast<int*>(base + off_eb);
+    int8_t* sa = reinterpret_cast<int8_t*>(base + off_sa);
+    int8_t* sb = reinterpret_cast<int8_t*>(base + off_sb);
+
+    OzProblem pr{sa, sb, (long)mp * kp, (long)np * kp, ea, eb, m, n, kp, d_c, n, 1};
+    oz_static_prepare_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(pr, d_prob, d_tiles, ntm, ntn, d_status);
+    ozaki_split_kernel<<<(mp + 7) / 8, 256, 0, st>>>(d_a, k, 1, m, k, mp, kp, sa, (long)mp * kp, ea);
+    ozaki_split_kernel<<<(np + 7) / 8, 256, 0, st>>>(d_b, 1, n, n, k, np, kp, sb, (long)np * kp, eb);
+    e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem));
+    if (e == cudaSuccess) {
+        ozaki_gemm_kernel<<<ntiles, OZ_THREADS, sizeof(OzSmem), st>>>(d_prob, d_tiles, d_status);
+        e = cudaGetLastError();
+    }
+    int status = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        oz_set_msg(msg, msg_len, cudaGetErrorString(e));
+        return RA_ERR_CUDA;
+    }
+    if (status) {
+        oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: tensor-core product timed out waiting on its pipeline barrier");
+        return RA_ERR_CUDA;
+    }
+    return RA_OK;
+}
+

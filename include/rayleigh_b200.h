@@ -143,9 +143,10 @@ int ra_cheby_deriv(ra_ctx* ctx, const double* c, double* dc, int order, long nco
 
 /* Split-precision product on the tensor cores, the engine of RA_PREC_MIXED:
  * C = A B with A (m x k) and B (k x n) row-major host arrays, C (m x n)
- * row-major; each operand is cut into 6 int8 digits per element (rows of A,
- * columns of B scaled by powers of two) and the 21 leading digit products are
- * accumulated exactly in int32 by tcgen05 before an FP64 recombination.
+ * row-major; each operand is cut into 5 balanced base-256 int8 digits per
+ * element (rows of A, columns of B scaled by powers of two) and the 15
+ * leading digit products are accumulated exactly in int32 by tcgen05 before
+ * an FP64 recombination (k <= 20000).
  * Replaces, for the parity tests, the DGEMM calls of Legendre_Transforms.F90:1028-1150. */
 int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* c, int m, int n, int k);
 
@@ -154,7 +155,7 @@ int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* c, int 
  * c (m x n) are row-major DEVICE arrays on the current device; the work is
  * enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) and the
  * call returns after it finished.  Scratch comes from one fixed 16 MiB
- * device array inside the library (about 6 (m + n) k bytes are needed;
+ * device array inside the library (about 5 (m + n) k bytes are needed;
  * larger products return RA_ERR_ARG with the needed size in msg).  The
  * first call on each device looks up that array's address: make it before
  * any stream capture.  Calls that overlap in time on one device race on the

@@ -1,0 +1,190 @@
+// RA_PREC_MIXED: the Legendre transforms as batched split-precision products
+// on the int8 tensor cores (k_ozaki.cu).
+//
+// Both transforms are computed transposed, with the long, contiguous column
+// index (field, r, re/im) as the product's M: the tensor-memory lanes, and so
+// the epilogue threads, then walk contiguous output addresses.
+// Inverse transform (StP_4d_dgp2, Legendre_Transforms.F90:968-1074), one
+// product per (m, parity):  p2[m][par][theta_h][col] = sum_l P(l, theta_h) s2[row(m,l)][col]
+//   A = s2^T (M = 11 fields x N_r x re/im, K = number of l of that parity):
+//            digits made every step (exponent per column of s2, over l);
+//   B = P    (N = N_theta/2): digits of the FP64 tables made once at set-up.
+// Forward transform (PtS_4d_dgpv3, Legendre_Transforms.F90:1077-1175), per (m, parity):
+//   s2[row(m,l)][col] = sum_theta iP(l, theta) p2b[m][par][theta][col]
+//   A = p2b^T (M = 4 fields x N_r x re/im, K = N_theta/2): split every step;
+//   B = iP^T  (N = number of l): digits of the iP rows, made once at set-up.
+// Every product of a transform goes out in ONE launch (tile list ordered by K).
+#include <algorithm>
+#include <vector>
+
+#include "ra_internal.h"
+#include "ozaki.h"
+
+namespace ra {
+
+template <class T>
+static void malloc_dev(T*& p, size_t count) {
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc", __FILE__, __LINE__);
+}
+
+template <class T>
+static T* upload(Ctx& c, const std::vector<T>& v) {
+    T* d = nullptr;
+    malloc_dev(d, v.size());
+    RA_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return d;
+}
+
+static void plan_launch(Ctx& c, MixedPlan& p, const std::vector<OzProblem>& probs) {
+    std::vector<int> tiles = ozaki_tiles(probs);
+    p.d_probs = upload(c, probs);
+    p.d_tiles = upload(c, tiles);
+    p.ntiles = (int)(tiles.size() / 4);
+}
+
+static void run_split_once(Ctx& c, const std::vector<OzSplitJob>& jobs, int max_rows) {
+    if (jobs.empty()) return;
+    OzSplitJob* d = upload(c, jobs);
+    ozaki_split(c, d, (int)jobs.size(), max_rows);
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(d);
+}
+
+// ---------------------------------------------------------------------------
+// Inverse Legendre transform
+// ---------------------------------------------------------------------------
+static void setup_lt_inverse(Ctx& c) {
+    const Dims& d = c.d;
+    const int L = d.L, nth2 = d.nth2;
+    const int ncol = NP2A * d.nr * 2;
+    const int nta = oz_tiles_of(ncol, OZ_HA), ntb = oz_tiles_of(nth2, OZ_HB);
+    MixedPlan& p = c.mx_inv;
+    std::vector<long> aoff(2 * L + 1, 0), boff(2 * L + 1, 0);
+    std::vector<int> nks(2 * L), nl(2 * L);
+    for (int q = 0; q < 2 * L; ++q) {
+        const int m = q >> 1, par = q & 1;
+        nl[q] = par ? n_odd(m, L) : n_even(m, L);
+        nks[q] = oz_ksteps(nl[q]);
+        aoff[q + 1] = aoff[q] + (long)nta * nks[q] * OZ_ABLK;
+        boff[q + 1] = boff[q] + (long)ntb * nks[q] * OZ_BBLK;
+    }
+    malloc_dev(p.d_adig, (size_t)aoff[2 * L]);
+    malloc_dev(p.d_bdig, (size_t)boff[2 * L]);
+    malloc_dev(p.d_ea, (size_t)2 * L * ncol);
+    malloc_dev(p.d_eb, (size_t)2 * L * nth2);
+    std::vector<OzSplitJob> ajobs, bjobs;
+    std::vector<OzProblem> probs;
+    for (int q = 0; q < 2 * L; ++q) {
+        const int m = q >> 1, par = q & 1;
+        const long roff = m_off(m, L) + (par ? n_even(m, L) : 0);
+        double* out = c.d_p2a + (size_t)q * nth2 * ncol;
+        if (nks[q] == 0) {   // no l of this parity: the E/O block stays zero
+            RA_CUDA(cudaMemsetAsync(out, 0, (size_t)nth2 * ncol * sizeof(double), c.stream));
+            continue;
+        }
+        int8_t* adig = p.d_adig + aoff[q];
+        int8_t* bdig = p.d_bdig + boff[q];
+        int* ea = p.d_ea + (size_t)q * ncol;
+        int* eb = p.d_eb + (size_t)q * nth2;
+        // A = s2^T: rows = columns of the s2 block (contiguous), K = l; split every step
+        ajobs.push_back({c.d_s2a11 + roff * ncol, 1L, (long)ncol, ncol, nl[q], OZ_HA, nta, nks[q], adig, ea});
+        // B^T = P^T: rows theta_h (contiguous in the table), K = l; split once
+        bjobs.push_back({c.d_Ptab + roff * nth2, 1L, (long)nth2, nth2, nl[q], OZ_HB, ntb, nks[q], bdig, eb});
+        probs.push_back({adig, bdig, (long)nks[q] * OZ_ABLK, (long)nks[q] * OZ_BBLK, ea, eb, ncol, nth2, nks[q], out,
+                         1L, (long)ncol});
+    }
+    run_split_once(c, bjobs, ntb * OZ_HB);
+    p.d_jobs = upload(c, ajobs);
+    p.njobs = (int)ajobs.size();
+    p.max_rows = nta * OZ_HA;
+    plan_launch(c, p, probs);
+}
+
+void launch_lt_inverse_mixed(Ctx& c) {
+    MixedPlan& p = c.mx_inv;
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
+}
+
+// ---------------------------------------------------------------------------
+// Forward Legendre transform
+// ---------------------------------------------------------------------------
+static void setup_lt_forward(Ctx& c) {
+    const Dims& d = c.d;
+    const int L = d.L, nth2 = d.nth2;
+    const int ncol = NP2B * d.nr * 2;
+    const int nta = oz_tiles_of(ncol, OZ_HA), nks = oz_ksteps(nth2);
+    const long ablk = (long)nta * nks * OZ_ABLK;
+    MixedPlan& p = c.mx_fwd;
+    std::vector<long> boff(2 * L + 1, 0);
+    for (int q = 0; q < 2 * L; ++q) {
+        const int m = q >> 1, par = q & 1;
+        const int nl = par ? n_odd(m, L) : n_even(m, L);
+        boff[q + 1] = boff[q] + (long)oz_tiles_of(nl, OZ_HB) * nks * OZ_BBLK;
+    }
+    malloc_dev(p.d_adig, (size_t)ablk * 2 * L);
+    malloc_dev(p.d_bdig, (size_t)boff[2 * L]);
+    malloc_dev(p.d_ea, (size_t)2 * L * ncol);
+    malloc_dev(p.d_eb, (size_t)d.nlm);
+    std::vector<OzSplitJob> ajobs, bjobs;
+    std::vector<OzProblem> probs;
+    int max_b = 0;
+    for (int q = 0; q < 2 * L; ++q) {
+        const int m = q >> 1, par = q & 1;
+        const int nl = par ? n_odd(m, L) : n_even(m, L);
+        if (nl == 0) continue;
+        const long roff = m_off(m, L) + (par ? n_even(m, L) : 0);
+        const int ntb = oz_tiles_of(nl, OZ_HB);
+        max_b = std::max(max_b, ntb * OZ_HB);
+        int8_t* adig = p.d_adig + (size_t)q * ablk;
+        int8_t* bdig = p.d_bdig + boff[q];
+        int* ea = p.d_ea + (size_t)q * ncol;
+        int* eb = p.d_eb + roff;
+        // A = p2b^T: rows = columns of the folded block (contiguous), K = theta_h
+        ajobs.push_back({c.d_p2b + (size_t)q * nth2 * ncol, 1L, (long)ncol, ncol, nth2, OZ_HA, nta, nks, adig, ea});
+        // B^T = iP rows (theta_h contiguous)
+        bjobs.push_back({c.d_iPtab + roff * nth2, (long)nth2, 1L, nl, nth2, OZ_HB, ntb, nks, bdig, eb});
+        probs.push_back({adig, bdig, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, ncol, nl, nks,
+                         c.d_s2b + roff * ncol, 1L, (long)ncol});
+    }
+    run_split_once(c, bjobs, max_b);
+    p.d_jobs = upload(c, ajobs);
+    p.njobs = (int)ajobs.size();
+    p.max_rows = nta * OZ_HA;
+    plan_launch(c, p, probs);
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void launch_lt_forward_mixed(Ctx& c) {
+    MixedPlan& p = c.mx_fwd;
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
+}
+
+void mixed_setup(Ctx& c) {
+    if (!c.d_status) {
+        malloc_dev(c.d_status, 1);
+        RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+    }
+    setup_lt_inverse(c);
+    setup_lt_forward(c);
+}
+
+static void free_plan(MixedPlan& p) {
+    if (p.d_adig) cudaFree(p.d_adig);
+    if (p.d_bdig) cudaFree(p.d_bdig);
+    if (p.d_ea) cudaFree(p.d_ea);
+    if (p.d_eb) cudaFree(p.d_eb);
+    if (p.d_probs) cudaFree(p.d_probs);
+    if (p.d_tiles) cudaFree(p.d_tiles);
+    if (p.d_jobs) cudaFree(p.d_jobs);
+    p = MixedPlan{};
+}
+
+void mixed_release(Ctx& c) {
+    free_plan(c.mx_inv);
+    free_plan(c.mx_fwd);
+}
+
+}  // namespace ra

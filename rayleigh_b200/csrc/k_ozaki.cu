@@ -2,39 +2,59 @@
 //
 // A double-precision product C = A B (A: M x K, B: K x N) is evaluated as an
 // Ozaki-type sum of exact integer products.  Every row of A and every column
-// of B is scaled by a power of two so that its largest entry lies in [1/2, 1),
-// then cut into S signed 7-bit digits (int8):
-//     a_ik = 2^{ea_i} sum_{s<S} qa_s[i,k] 2^{-7(s+1)},  b_kj = 2^{eb_j} sum_{t<S} qb_t[j,k] 2^{-7(t+1)}.
-// The products qa_s qb_t with s + t <= S-1 are accumulated over K in int32 by
-// tcgen05.mma.kind::i8, one TMEM accumulator per diagonal d = s + t (exact: no
-// rounding at all until the epilogue), and the epilogue forms
-//     c_ij = 2^{ea_i + eb_j} sum_d D_d[i,j] 2^{-7(d+2)}
-// in FP64.  With S = 6 (21 products) the relative error of a Legendre
-// transform is ~1e-11 (measured against the FP64 product), against ~1e-6 for
-// a single FP32-accumulated product.
+// of B is scaled by a power of two 2^e so that its largest entry lies in
+// [1/4, 1/2), rounded to a 39-bit integer v = rint(x 2^{39-e}) and cut into
+// S = 5 balanced base-256 digits (int8, the low bytes taken as signed):
+//     x = 2^e sum_{s<S} q_s 2^{-(8s+7)} + r,   |r| <= 2^{e-40}.
+// The digit products qa_s qb_t with s + t <= S-1 (15 of them) are accumulated
+// over K in int32 by tcgen05.mma.kind::i8, one TMEM accumulator per diagonal
+// d = s + t (exact for K < 20000), and the epilogue forms
+//     c_ij = 2^{ea_i + eb_j} sum_d D_d[i,j] 2^{-(8d+14)}
+// in FP64 (all scalings are exact powers of two).  The relative error of a
+// Legendre transform is ~1e-11 (vs ~1e-6 for one FP32-accumulated product).
 //
-// Kernel layout: one CTA (4 warps) per 128 x 64 output tile; operand tiles of
-// 32 int8 columns (one MMA K-step) per slice are staged in shared memory in
-// the K-major "core matrix" layout (8 rows x 16 bytes contiguous, no swizzle)
-// by cp.async, 4 stages deep; thread 0 issues the 21 MMAs of a stage and
-// commits them to the stage's mbarrier; the accumulators (6 x 64 columns of
-// int32) live in tensor memory and are read back with tcgen05.ld.
+// The product kernel is persistent (one CTA per SM, tiles dealt round-robin
+// from a list ordered longest-K first) and warp-specialised:
+//   warp 0      producer: one bulk copy (cp.async.bulk, no multicast) per
+//               operand per K-step into a 6-stage shared-memory ring;
+//   warp 1      MMA issuer: 15 tcgen05.mma per K-step, committed to the
+//               stage's "empty" barrier and, after the last K-step, to the
+//               accumulator's "full" barrier;
+//   warps 2-9   epilogue: two warps per TMEM lane quadrant, each taking half
+//               of the tile's columns: tcgen05.ld of the 5 diagonals (one
+//               wait per 8 columns), FP64 recombination, scaled stores.
+// Output tiles are 128 x 48, so two accumulator sets (2 x 5 x 48 columns)
+// fit in tensor memory and the epilogue of one tile overlaps the MMAs of the
+// next.  Every wait is bounded: when a limit runs out the CTA raises the
+// device error word, drains its own copies and MMAs (bounded again), frees
+// its tensor memory and returns.
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 
 #include "ra_internal.h"
 #include "ozaki.h"
 
 namespace ra {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32, OZ_NST = 4, OZ_THREADS = 128;
+constexpr int OZ_NST = 6;
+constexpr int OZ_EPI_WARPS = 8;                            // two per TMEM lane quadrant
+constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
+constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (24)
+constexpr int OZ_ACC_STRIDE = 256;           // TMEM columns between the two accumulator sets
 constexpr int OZ_TMEM_COLS = 512;
-constexpr long OZ_SPIN_LIMIT = 1L << 26;   // bounded waits: ~seconds, then the error word is set
+constexpr int OZ_STAGE = OZ_ABLK + OZ_BBLK;  // 28160 bytes
+constexpr long OZ_SPIN_LIMIT = 1L << 25;     // bounded waits: ~seconds, then the error word is set
+static_assert(OZ_S * OZ_HB <= OZ_ACC_STRIDE, "accumulator set exceeds its tensor-memory half");
+static_assert(OZ_STAGE % 128 == 0, "stage size");
 
 struct OzSmem {
-    alignas(128) int8_t A[OZ_NST][OZ_S][OZ_BM * OZ_BK];
-    alignas(128) int8_t B[OZ_NST][OZ_S][OZ_BN * OZ_BK];
-    alignas(8) uint64_t mbar[OZ_NST];
+    alignas(128) int8_t stage[OZ_NST][OZ_STAGE];
+    alignas(8) uint64_t full[OZ_NST];
+    uint64_t empty[OZ_NST];
+    uint64_t acc_full[2];
+    uint64_t acc_empty[2];
+    uint64_t drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -43,7 +63,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// K-major, no-swizzle matrix descriptor (sm_100 version 1)
+// K-major, no-swizzle matrix descriptor (sm_100 version 1): start address,
+// leading byte offset (between 16-byte K chunks), stride byte offset (between
+// 8-row groups), all in 16-byte units.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
@@ -65,8 +87,22 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
 }
 
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)));
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(smem_u32(bar)));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(
+                     smem_u32(bar)),
+                 "r"(bytes));
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -78,45 +114,60 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait; returns false when the limit ran out
+// bounded wait for the completion of the phase with the given parity;
+// false when the limit ran out
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     for (long i = 0; i < OZ_SPIN_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(32);
+        if (i > 16) __nanosleep(64);
     }
     return false;
 }
 
-__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc));
+// global -> shared bulk copy (no multicast), completion counted on bar
+__device__ __forceinline__ void bulk_g2s(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(sdst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
-// core-matrix offset of (row, 16-byte chunk kc) in a tile of R rows x 32 bytes
-__device__ __forceinline__ int cm_off(int row, int kc, int R) { return kc * (R / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16; }
+// 2^e as a double (exact; ldexp outside the normal exponent range)
+__device__ __forceinline__ double pow2(int e) {
+    return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+}
+
+__device__ __forceinline__ int vload(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// the 5 balanced base-256 digits of an integer v (|v| <= 2^38), most
+// significant first in q[0]
+__device__ __forceinline__ void oz_digits(long long v, int8_t (&q)[OZ_S]) {
+#pragma unroll
+    for (int s = OZ_S - 1; s > 0; --s) {
+        const int8_t lo = (int8_t)(v & 0xFF);
+        q[s] = lo;
+        v = (v - lo) >> 8;
+    }
+    q[0] = (int8_t)v;
+}
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProblem* __restrict__ probs,
-                                                                   const int4* __restrict__ tiles,
+                                                                   const int4* __restrict__ tiles, int ntiles,
                                                                    int* __restrict__ status) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     OzSmem& sm = *reinterpret_cast<OzSmem*>(smem_raw);
-    const int4 tl = tiles[blockIdx.x];
-    const OzProblem pb = probs[tl.x];
-    const int m0 = tl.y * OZ_BM, n0 = tl.z * OZ_BN;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nk = pb.kpad / OZ_BK;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    if (nk == 0) {   // empty product: the tile is zero
-        for (int e = tid; e < OZ_BM * OZ_BN; e += OZ_THREADS) {
-            const int i = m0 + e / OZ_BN, j = n0 + e % OZ_BN;
-            if (i < pb.M && j < pb.N) pb.C[(long)i * pb.c_m + (long)j * pb.c_n] = 0.0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < OZ_NST; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
         }
-        return;
-    }
-    if (tid == 0) {
-        for (int s = 0; s < OZ_NST; ++s) mbar_init(&sm.mbar[s], 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.acc_full[b], 1);
+            mbar_init(&sm.acc_empty[b], 32 * OZ_EPI_WARPS);
+        }
+        mbar_init(&sm.drain, 1);
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
@@ -130,175 +181,263 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = sm.tmem_base;
 
-    auto load_stage = [&](int kstep, int st) {
-        const long k0 = (long)kstep * OZ_BK;
-        // A: S slices x 128 rows x 2 chunks
-        for (int e = tid; e < OZ_S * OZ_BM * 2; e += OZ_THREADS) {
-            const int s = e / (OZ_BM * 2), rem = e % (OZ_BM * 2);
-            const int row = rem >> 1, kc = rem & 1;
-            const int8_t* src = pb.A + s * pb.a_slice + (long)(m0 + row) * pb.kpad + k0 + kc * 16;
-            cp_async16(&sm.A[st][s][cm_off(row, kc, OZ_BM)], src);
-        }
-        for (int e = tid; e < OZ_S * OZ_BN * 2; e += OZ_THREADS) {
-            const int s = e / (OZ_BN * 2), rem = e % (OZ_BN * 2);
-            const int row = rem >> 1, kc = rem & 1;
-            const int8_t* src = pb.B + s * pb.b_slice + (long)(n0 + row) * pb.kpad + k0 + kc * 16;
-            cp_async16(&sm.B[st][s][cm_off(row, kc, OZ_BN)], src);
-        }
-    };
-
-    const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN);
-    bool ok = true;
-    int issued = 0;   // steps whose MMAs were issued and committed
-    // prologue: stages 0 .. NST-2
-    for (int p = 0; p < OZ_NST - 1; ++p) {
-        if (p < nk) load_stage(p, p);
-        cp_async_commit();
-    }
-    for (int k = 0; k < nk; ++k) {
-        const int st = k % OZ_NST;
-        cp_async_wait<OZ_NST - 2>();
-        asm volatile("fence.proxy.async.shared::cta;");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-#pragma unroll
-            for (int d = 0; d < OZ_S; ++d) {
-#pragma unroll
-                for (int s = 0; s <= d; ++s) {
-                    const int t = d - s;
-                    const uint64_t ad = umma_desc(smem_u32(&sm.A[st][s][0]), (OZ_BM / 8) * 128, 128);
-                    const uint64_t bd = umma_desc(smem_u32(&sm.B[st][t][0]), (OZ_BN / 8) * 128, 128);
-                    mma_i8(tmem + (uint32_t)(d * OZ_BN), ad, bd, idesc, (k > 0 || s > 0) ? 1u : 0u);
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                smem_u32(&sm.mbar[st])));
-        }
-        ++issued;
-        // refill the buffer that the MMAs of step k-1 read
-        const int kn = k + OZ_NST - 1;
-        if (kn < nk) {
-            if (k >= 1) {
-                const int pb_ = (k - 1) % OZ_NST;
-                if (!mbar_wait(&sm.mbar[pb_], (uint32_t)(((k - 1) / OZ_NST) & 1))) {
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            if (vload(&sm.abort)) break;
+            const int4 tl = tiles[t];
+            const OzProblem& pb = probs[tl.x];
+            const int8_t* a = pb.A + (long)tl.y * pb.a_tile;
+            const int8_t* b = pb.B + (long)tl.z * pb.b_tile;
+            const int nks = pb.nks;
+            bool ok = true;
+            for (int ks = 0; ks < nks; ++ks, ++it) {
+                const int st = it % OZ_NST;
+                const uint32_t ph = (uint32_t)(it / OZ_NST) & 1u;
+                if (!__all_sync(0xffffffffu, mbar_wait(&sm.empty[st], ph ^ 1u))) {
                     ok = false;
+                    break;
                 }
+                if (lane == 0) {
+                    mbar_expect_tx(&sm.full[st], (uint32_t)OZ_STAGE);
+                    bulk_g2s(&sm.stage[st][0], a + (long)ks * OZ_ABLK, OZ_ABLK, &sm.full[st]);
+                    bulk_g2s(&sm.stage[st][OZ_ABLK], b + (long)ks * OZ_BBLK, OZ_BBLK, &sm.full[st]);
+                }
+                __syncwarp();
             }
-            if (ok) load_stage(kn, kn % OZ_NST);
+            if (!ok) {
+                sm.abort = 1;
+                break;
+            }
         }
-        cp_async_commit();
-        if (!ok) {
-            sm.abort = 1;
+        // copies still in flight after an abort: wait (bounded) for the last ones
+        if (vload(&sm.abort)) {
+            for (int j = (it > OZ_NST ? it - OZ_NST : 0); j < it; ++j)
+                mbar_wait(&sm.full[j % OZ_NST], (uint32_t)(j / OZ_NST) & 1u);
         }
-        __syncthreads();
-        if (sm.abort) break;
-    }
-    cp_async_wait<0>();
-    // wait (bounded) for the last committed MMAs, on the normal and the abort path alike
-    if (issued > 0) {
-        const int kl = issued - 1;
-        if (!mbar_wait(&sm.mbar[kl % OZ_NST], (uint32_t)((kl / OZ_NST) & 1))) sm.abort = 1;
-    }
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (!sm.abort) {
-        // epilogue: warp w owns tile rows 32w .. 32w+31 (TMEM lanes)
-        const int row = m0 + warp * 32 + lane;
-        const int ea = (row < pb.M) ? pb.ea[row] : 0;
-        for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
-            double acc[16];
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        const uint32_t idesc = idesc_i8(OZ_HA, OZ_HB);
+        int it = 0, tl_i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
+            if (vload(&sm.abort)) break;
+            const int nks = probs[tiles[t].x].nks;
+            const int buf = tl_i & 1;
+            const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+            bool ok = __all_sync(0xffffffffu, mbar_wait(&sm.acc_empty[buf], aph ^ 1u));
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t dacc = tmem + (uint32_t)(buf * OZ_ACC_STRIDE);
+            for (int ks = 0; ks < nks && ok; ++ks, ++it) {
+                const int st = it % OZ_NST;
+                const uint32_t ph = (uint32_t)(it / OZ_NST) & 1u;
+                if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[st], ph))) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                if (lane == 0) {
+                    const uint32_t sa = smem_u32(&sm.stage[st][0]);
+                    const uint32_t sb = smem_u32(&sm.stage[st][OZ_ABLK]);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) acc[j] = 0.0;
+                    for (int d = 0; d < OZ_S; ++d) {
 #pragma unroll
-            for (int d = 0; d < OZ_S; ++d) {
-                uint32_t v[16];
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * OZ_BN + c0);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                      "=r"(v[15])
-                    : "r"(taddr));
+                        for (int s = 0; s <= d; ++s) {
+                            const uint64_t ad = umma_desc(sa + s * (OZ_HA * OZ_BK), OZ_HA * 16, 128);
+                            const uint64_t bd = umma_desc(sb + (d - s) * (OZ_HB * OZ_BK), OZ_HB * 16, 128);
+                            mma_i8(dacc + (uint32_t)(d * OZ_HB), ad, bd, idesc, (ks > 0 || s > 0) ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(&sm.empty[st]);
+                }
+                __syncwarp();
+            }
+            if (!ok) {
+                sm.abort = 1;
+                break;
+            }
+            if (lane == 0) umma_commit(&sm.acc_full[buf]);
+            __syncwarp();
+        }
+        // all MMAs of this CTA finished before the tensor memory is released
+        if (lane == 0) umma_commit(&sm.drain);
+        __syncwarp();
+        if (!__all_sync(0xffffffffu, mbar_wait(&sm.drain, 0))) sm.abort = 1;
+    } else {
+        // ---------------- epilogue (warps 2..9): lane quadrant warp % 4, column half (warp - 2) / 4 ----------------
+        const int q = warp & 3;
+        const int cbeg = ((warp - 2) >> 2) * OZ_EPI_COLS;
+        int tl_i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
+            if (vload(&sm.abort)) break;
+            const int4 tl = tiles[t];
+            const OzProblem pb = probs[tl.x];   // by value: stores to C cannot alias it
+            const int buf = tl_i & 1;
+            const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+            if (!mbar_wait(&sm.acc_full[buf], aph)) {
+                sm.abort = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int row = tl.y * OZ_HA + q * 32 + lane;
+            const bool rok = row < pb.M;
+            // row scale with the digit weight 2^-14 folded in
+            const double sa = rok ? pow2(pb.ea[row] - 14) : 0.0;
+            double* crow = pb.C + (long)row * pb.c_m;
+            const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * OZ_ACC_STRIDE);
+#pragma unroll 1
+            for (int c0 = cbeg; c0 < cbeg + OZ_EPI_COLS; c0 += 8) {
+                uint32_t v[OZ_S][8];
+#pragma unroll
+                for (int d = 0; d < OZ_S; ++d)
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                                 : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]),
+                                   "=r"(v[d][5]), "=r"(v[d][6]), "=r"(v[d][7])
+                                 : "r"(tbase + (uint32_t)(d * OZ_HB + c0)));
                 asm volatile("tcgen05.wait::ld.sync.aligned;");
-                const double sc = ldexp(1.0, -7 * (d + 2));
+                const int cb = tl.z * OZ_HB + c0;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] += (double)(int32_t)v[j] * sc;
-            }
-            if (row < pb.M) {
+                for (int j = 0; j < 8; ++j) {
+                    // int32 -> double as (2^52 + 2^31 + x) - (2^52 + 2^31): exact, no conversion unit
+                    double acc = 0.0, w = 1.0;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + c0 + j;
-                    if (col < pb.N) pb.C[(long)row * pb.c_m + (long)col * pb.c_n] = ldexp(acc[j], ea + pb.eb[col]);
+                    for (int d = 0; d < OZ_S; ++d) {
+                        const double x = __hiloint2double(0x43300000, (int)(v[d][j] ^ 0x80000000u)) - 4503601774854144.0;
+                        acc = fma(x, w, acc);
+                        w *= 0x1p-8;
+                    }
+                    const int col = cb + j;
+                    if (rok && col < pb.N) crow[(long)col * pb.c_n] = (acc * sa) * pow2(__ldg(pb.eb + col));
                 }
             }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            mbar_arrive(&sm.acc_empty[buf]);
         }
-    } else if (tid == 0) {
-        atomicExch(status, 1);
     }
+
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(OZ_TMEM_COLS));
+    if (threadIdx.x == 0 && sm.abort) atomicExch(status, 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(OZ_TMEM_COLS));
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Splitting: rows of X (element (i, k) at X[i*si + k*sk], i < R, k < K) into
-// S int8 digit slices out[s][i][kpad] (rows padded to rpad, columns to kpad)
-// and exponents e[i] (e = 0 for an all-zero row).  One warp per row.
+// Splitting into tiled digits (a batch of jobs).  Block = 16 rows of one job:
+// a max pass over K, then per K-step a 16 x 32 tile of X through shared
+// memory (read along whichever index is contiguous), digits transposed into
+// the [s][kc][row][16] block layout and written as 16-byte rows.
 // ---------------------------------------------------------------------------
-__global__ void ozaki_split_kernel(const double* __restrict__ X, long si, long sk, int R, int K, int rpad, int kpad,
-                                   int8_t* __restrict__ out, long slice, int* __restrict__ e) {
-    const int warps = blockDim.x / 32;
-    const int row = blockIdx.x * warps + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
-    if (row >= rpad) return;
+__global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __restrict__ jobs) {
+    const OzSplitJob& jb = jobs[blockIdx.y];
+    const int r0 = blockIdx.x * 16;
+    if (r0 >= jb.nrt * jb.H) return;
+    __shared__ double xs[16][33];
+    __shared__ double red[16][17];
+    __shared__ int ex_s[16];
+    __shared__ __align__(16) int8_t dig[OZ_S][2][16][16];
+    const int tid = threadIdx.x;
+    const bool kmajor = (jb.sk == 1);
+    // pass 1: row maxima (thread: row lr, K offset lk, stride 16) and the row
+    // shifts 39 - e: the digits are those of the integer rint(x 2^(39-e))
+    const int lr = kmajor ? (tid >> 4) : (tid & 15);
+    const int lk = kmajor ? (tid & 15) : (tid >> 4);
+    const int r = r0 + lr;
     double mx = 0.0;
-    if (row < R)
-        for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(X[(long)row * si + (long)k * sk]));
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    const int ex = (mx > 0.0) ? ilogb(mx) + 1 : 0;
-    if (lane == 0 && row < R) e[row] = ex;
-    const double scale = ldexp(1.0, -ex);
-    for (int k = lane; k < kpad; k += 32) {
-        double a = (row < R && k < K) ? X[(long)row * si + (long)k * sk] * scale : 0.0;
-        int8_t* o = out + (long)row * kpad + k;
+    if (r < jb.R)
+        for (int k = lk; k < jb.K; k += 16) mx = fmax(mx, fabs(jb.X[(long)r * jb.sr + (long)k * jb.sk]));
+    red[lr][lk] = mx;
+    __syncthreads();
+    if (tid < 16) {
+        double m = red[tid][0];
 #pragma unroll
-        for (int s = 0; s < OZ_S; ++s) {
-            a *= 128.0;
-            const double q = trunc(a);
-            a -= q;
-            o[s * slice] = (int8_t)(int)q;
+        for (int i = 1; i < 16; ++i) m = fmax(m, red[tid][i]);
+        const int ex = (m > 0.0) ? ilogb(m) + 2 : 0;
+        ex_s[tid] = 39 - ex;
+        if (r0 + tid < jb.R) jb.e[r0 + tid] = ex;
+    }
+    const int rt = r0 / jb.H, rin = r0 - rt * jb.H;
+    const long blk = (long)OZ_S * jb.H * OZ_BK;
+    for (int ks = 0; ks < jb.nks; ++ks) {
+        const int k0 = ks * OZ_BK;
+        __syncthreads();   // ex_s ready / previous tile consumed
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int idx = tid + 256 * i;
+            const int row = kmajor ? (idx >> 5) : (idx & 15);
+            const int kk = kmajor ? (idx & 31) : (idx >> 4);
+            const int rr = r0 + row, k = k0 + kk;
+            xs[row][kk] = (rr < jb.R && k < jb.K) ? jb.X[(long)rr * jb.sr + (long)k * jb.sk] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int idx = tid + 256 * i;
+            const int row = idx >> 5, kk = idx & 31;
+            const int sh = ex_s[row];
+            const double a = (sh <= 1023 && sh >= -1022) ? xs[row][kk] * pow2(sh) : ldexp(xs[row][kk], sh);
+            int8_t qd[OZ_S];
+            oz_digits(__double2ll_rn(a), qd);
+#pragma unroll
+            for (int s = 0; s < OZ_S; ++s) dig[s][kk >> 4][row][kk & 15] = qd[s];
+        }
+        __syncthreads();
+        if (tid < OZ_S * 32) {
+            const int s = tid >> 5, kc = (tid >> 4) & 1, row = tid & 15;
+            int8_t* dst = jb.out + ((long)rt * jb.nks + ks) * blk + (long)s * jb.H * OZ_BK + (long)kc * jb.H * 16 +
+                          (long)(rin + row) * 16;
+            *reinterpret_cast<int4*>(dst) = *reinterpret_cast<const int4*>(&dig[s][kc][row][0]);
         }
     }
 }
 
-void ozaki_split(Ctx& c, const double* X, long si, long sk, int R, int K, int rpad, int kpad, int8_t* out, long slice,
-                 int* e) {
-    const int warps = 8;
-    ozaki_split_kernel<<<(rpad + warps - 1) / warps, warps * 32, 0, c.stream>>>(X, si, sk, R, K, rpad, kpad, out, slice, e);
+void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows) {
+    if (njobs == 0 || max_rows == 0) return;
+    dim3 grid((max_rows + 15) / 16, njobs);
+    ozaki_split_kernel<<<grid, 256, 0, c.stream>>>(d_jobs);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
 
+static int oz_sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        RA_CUDA(cudaGetDevice(&dev));
+        RA_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return n;
+}
+
 void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles, int* d_status) {
+    if (ntiles == 0) return;
     static bool attr = false;
     if (!attr) {
         RA_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem)));
         attr = true;
     }
-    ozaki_gemm_kernel<<<ntiles, OZ_THREADS, sizeof(OzSmem), c.stream>>>(d_probs, reinterpret_cast<const int4*>(d_tiles),
-                                                                         d_status);
+    const int grid = std::min(ntiles, oz_sm_count());
+    ozaki_gemm_kernel<<<grid, OZ_THREADS, sizeof(OzSmem), c.stream>>>(
+        d_probs, reinterpret_cast<const int4*>(d_tiles), ntiles, d_status);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
 
+// Tile list (problem, m-tile, n-tile, 0), longest K first so that the ragged
+// products finish together; products with K = 0 get no tiles.
 std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
+    std::vector<int> order(probs.size());
+    for (size_t p = 0; p < probs.size(); ++p) order[p] = (int)p;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return probs[a].nks > probs[b].nks; });
     std::vector<int> t;
-    for (size_t p = 0; p < probs.size(); ++p) {
+    for (int p : order) {
         const OzProblem& q = probs[p];
-        for (int mt = 0; mt * OZ_BM < q.M; ++mt)
-            for (int nt = 0; nt * OZ_BN < q.N; ++nt) {
-                t.push_back((int)p);
+        if (q.nks == 0) continue;
+        for (int mt = 0; mt * OZ_HA < q.M; ++mt)
+            for (int nt = 0; nt * OZ_HB < q.N; ++nt) {
+                t.push_back(p);
                 t.push_back(mt);
                 t.push_back(nt);
                 t.push_back(0);
@@ -307,10 +446,6 @@ std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
     return t;
 }
 
-int oz_round_m(int m) { return (m + OZ_BM - 1) / OZ_BM * OZ_BM; }
-int oz_round_n(int n) { return (n + OZ_BN - 1) / OZ_BN * OZ_BN; }
-int oz_round_k(int k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
-
 // ---------------------------------------------------------------------------
 // Allocation-free form of the split-precision product (ra_mixed_gemm_noalloc).
 //
@@ -318,11 +453,12 @@ int oz_round_k(int k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
 // address is looked up once per device (cudaGetSymbolAddress, with that device
 // current) on the first call made on that device.  Scratch layout, every piece
 // 256-byte aligned:
-//   [0]        int   status word      (set to zero by oz_static_prepare_kernel)
-//   [256]      OzProblem              (written by oz_static_prepare_kernel)
-//   [512]      int4  tiles[ntiles]    (written by oz_static_prepare_kernel)
-//   then       int   ea[mp], eb[np]   (written by the split kernel)
-//   then       int8  A digits [S][mp][kp], B digits [S][np][kp] (split kernel)
+//   [0]        int        status word    (set to zero by oz_static_prepare_kernel)
+//   [256]      OzProblem                 (written by oz_static_prepare_kernel)
+//   [512]      OzSplitJob[2]             (written by oz_static_prepare_kernel)
+//   [1024]     int4       tiles[ntiles]  (written by oz_static_prepare_kernel)
+//   then       int        ea[mp], eb[np] (written by the split kernel)
+//   then       int8       A digits (mp x kp x 5), B digits (np x kp x 5) (split kernel)
 // Nothing else needs to start at zero: the split kernel writes every padded
 // digit and every exponent the product reads.  Calls on one device share the
 // array, so calls that overlap in time (two host threads, or two streams)
@@ -336,11 +472,14 @@ static unsigned char* oz_static_ptr[OZ_MAX_DEVICES] = {};
 
 static size_t oz_align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-__global__ void oz_static_prepare_kernel(OzProblem pr, OzProblem* __restrict__ dprob, int4* __restrict__ tiles,
-                                         int ntm, int ntn, int* __restrict__ status) {
+__global__ void oz_static_prepare_kernel(OzProblem pr, OzSplitJob ja, OzSplitJob jb, OzProblem* __restrict__ dprob,
+                                         OzSplitJob* __restrict__ djobs, int4* __restrict__ tiles, int ntm, int ntn,
+                                         int* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         *dprob = pr;
+        djobs[0] = ja;
+        djobs[1] = jb;
         *status = 0;
     }
     if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, 0);
@@ -367,9 +506,9 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
         oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: k exceeds the exact int32 accumulation limit (20000)");
         return RA_ERR_ARG;
     }
-    const int mp = oz_round_m(m), np = oz_round_n(n), kp = oz_round_k(k);
-    const int ntm = mp / 128, ntn = np / 64, ntiles = ntm * ntn;
-    const size_t off_prob = 256, off_tiles = 512;
+    const int ntm = oz_tiles_of(m, OZ_HA), ntn = oz_tiles_of(n, OZ_HB), ntiles = ntm * ntn;
+    const int mp = ntm * OZ_HA, np = ntn * OZ_HB, nks = oz_ksteps(k), kp = nks * OZ_BK;
+    const size_t off_prob = 256, off_jobs = 512, off_tiles = 1024;
     const size_t off_ea = off_tiles + oz_align256((size_t)ntiles * sizeof(int4));
     const size_t off_eb = off_ea + oz_align256((size_t)mp * sizeof(int));
     const size_t off_sa = off_eb + oz_align256((size_t)np * sizeof(int));
@@ -398,23 +537,32 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
         }
         oz_static_ptr[dev] = static_cast<unsigned char*>(p);
     }
+    int nsm = 0;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || nsm <= 0) {
+        oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: cannot read the SM count");
+        return RA_ERR_CUDA;
+    }
     unsigned char* base = oz_static_ptr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int* d_status = reinterpret_cast<int*>(base);
     OzProblem* d_prob = reinterpret_cast<OzProblem*>(base + off_prob);
+    OzSplitJob* d_jobs = reinterpret_cast<OzSplitJob*>(base + off_jobs);
     int4* d_tiles = reinterpret_cast<int4*>(base + off_tiles);
     int* ea = reinterpret_cast<int*>(base + off_ea);
     int* eb = reinterpret_cast<int*>(base + off_eb);
     int8_t* sa = reinterpret_cast<int8_t*>(base + off_sa);
     int8_t* sb = reinterpret_cast<int8_t*>(base + off_sb);
 
-    OzProblem pr{sa, sb, (long)mp * kp, (long)np * kp, ea, eb, m, n, kp, d_c, n, 1};
-    oz_static_prepare_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(pr, d_prob, d_tiles, ntm, ntn, d_status);
-    ozaki_split_kernel<<<(mp + 7) / 8, 256, 0, st>>>(d_a, k, 1, m, k, mp, kp, sa, (long)mp * kp, ea);
-    ozaki_split_kernel<<<(np + 7) / 8, 256, 0, st>>>(d_b, 1, n, n, k, np, kp, sb, (long)np * kp, eb);
+    const OzSplitJob ja{d_a, (long)k, 1L, m, k, OZ_HA, ntm, nks, sa, ea};
+    const OzSplitJob jbj{d_b, 1L, (long)n, n, k, OZ_HB, ntn, nks, sb, eb};
+    const OzProblem pr{sa, sb, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, m, n, nks, d_c, (long)n, 1L};
+    oz_static_prepare_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(pr, ja, jbj, d_prob, d_jobs, d_tiles, ntm, ntn,
+                                                                     d_status);
+    ozaki_split_kernel<<<dim3((std::max(mp, np) + 15) / 16, 2), 256, 0, st>>>(d_jobs);
     e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem));
     if (e == cudaSuccess) {
-        ozaki_gemm_kernel<<<ntiles, OZ_THREADS, sizeof(OzSmem), st>>>(d_prob, d_tiles, d_status);
+        ozaki_gemm_kernel<<<std::min(ntiles, nsm), OZ_THREADS, sizeof(OzSmem), st>>>(d_prob, d_tiles, ntiles, d_status);
         e = cudaGetLastError();
     }
     int status = 0;
@@ -430,4 +578,3 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
     }
     return RA_OK;
 }
-

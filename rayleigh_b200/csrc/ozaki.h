@@ -8,31 +8,49 @@ namespace ra {
 
 struct Ctx;
 
-constexpr int OZ_S = 6;   // int8 digits per operand (21 digit products)
-// int32 accumulators stay exact while K * 127^2 * OZ_S < 2^31
+constexpr int OZ_S = 5;   // balanced base-256 int8 digits per operand (15 digit products)
+// int32 accumulators stay exact while K * 128^2 * OZ_S < 2^31
 constexpr int OZ_MAX_K = 20000;
+constexpr int OZ_HA = 128;   // rows of an A tile (output rows, TMEM lanes)
+constexpr int OZ_HB = 48;    // rows of a B^T tile (output columns)
+constexpr int OZ_BK = 32;    // K per MMA step (int8)
+constexpr int OZ_ABLK = OZ_S * OZ_HA * OZ_BK;   // bytes of one K-step of an A row tile, all digits
+constexpr int OZ_BBLK = OZ_S * OZ_HB * OZ_BK;   // same for B
 
-// One product C = A B of a batch.  A is given as OZ_S int8 digit slices
-// A + s*a_slice, each [rows padded to 128][kpad] (K-major), with row exponents
-// ea[M]; B likewise as slices of B^T, [cols padded to 64][kpad], exponents eb[N].
-// C(i, j) is written to C[i*c_m + j*c_n] in FP64.
+// Digit operands are stored TILED: row tile rt (H rows) and K-step ks form one
+// contiguous block of OZ_S*H*32 bytes at (rt*nks + ks) * OZ_S*H*32, laid out
+// [digit s][16-byte K chunk kc][row][16 bytes] -- the tensor cores' K-major
+// no-swizzle "core matrix" layout, so one bulk copy stages a whole K-step.
+//
+// One product C = A B of a batch: A as digit row tiles (rows = output rows,
+// exponents ea[M]), B as digit row tiles of B^T (rows = output columns,
+// exponents eb[N]); C(i, j) is written to C[i*c_m + j*c_n] in FP64.
 struct OzProblem {
     const int8_t* A;
     const int8_t* B;
-    long a_slice, b_slice;
+    long a_tile, b_tile;   // bytes between consecutive row tiles (nks * block)
     const int* ea;
     const int* eb;
-    int M, N, kpad;
+    int M, N, nks;
     double* C;
     long c_m, c_n;
 };
 
-void ozaki_split(Ctx& c, const double* X, long si, long sk, int R, int K, int rpad, int kpad, int8_t* out, long slice,
-                 int* e);
+// One split job: rows i < R of X (element (i, k) at X[i*sr + k*sk], k < K)
+// become tiled digit rows with tile height H (nrt row tiles, nks K-steps;
+// zero digits past R and K) and exponents e[i] (0 for an all-zero row).
+struct OzSplitJob {
+    const double* X;
+    long sr, sk;
+    int R, K, H, nrt, nks;
+    int8_t* out;
+    int* e;
+};
+
+void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows);
 void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles, int* d_status);
 std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs);
-int oz_round_m(int m);
-int oz_round_n(int n);
-int oz_round_k(int k);
+inline int oz_tiles_of(int rows, int h) { return (rows + h - 1) / h; }
+inline int oz_ksteps(int k) { return (k + OZ_BK - 1) / OZ_BK; }
 
 }  // namespace ra

@@ -410,9 +410,11 @@ static void setup(Ctx& c) {
     cudaFree(d_w);
     // kernels that need more than 48 KB of dynamic shared memory
     linear_setup(c);
+    if (c.cfg.precision == RA_PREC_MIXED) mixed_setup(c);
 }
 
 static void release(Ctx& c) {
+    mixed_release(c);
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
     double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_Awpt, c.d_Az,
@@ -438,16 +440,47 @@ static void ab_factors(const Ctx& c, double& new_ab, double& old_ab) {
     }
 }
 
+// The eight stages of one step, in launch order (their names: kKernelNames).
+constexpr int kNK = 8;
+static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
+    const bool mixed = c.cfg.precision == RA_PREC_MIXED;
+    switch (k) {
+        case 0: launch_cheb_synthesis(c); break;
+        case 1: launch_post_assemble(c, old_ab); break;
+        case 2: launch_rlm_a(c); break;
+        case 3:
+            if (mixed)
+                launch_lt_inverse_mixed(c);
+            else
+                launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
+            break;
+        case 4:
+            RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
+            launch_physics(c);
+            break;
+        case 5:
+            if (mixed)
+                launch_lt_forward_mixed(c);
+            else
+                launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+            break;
+        case 6: launch_rlm_b(c, new_ab); break;
+        default: launch_solve(c); break;
+    }
+}
+
 static void enqueue_step(Ctx& c, double new_ab, double old_ab) {
-    launch_cheb_synthesis(c);
-    launch_post_assemble(c, old_ab);
-    launch_rlm_a(c);
-    launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
-    RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
-    launch_physics(c);
-    launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
-    launch_rlm_b(c, new_ab);
-    launch_solve(c);
+    for (int k = 0; k < kNK; ++k) run_stage(c, k, new_ab, old_ab);
+}
+
+// the device error word of the bounded tensor-core waits (split-precision products)
+static void check_status(Ctx& c) {
+    if (!c.d_status) return;
+    int st = 0;
+    RA_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+    if (st) throw CudaError(cudaErrorLaunchTimeout, "split-precision product (pipeline barrier wait timed out)",
+                            __FILE__, __LINE__);
 }
 
 static void run_steps(Ctx& c, int nsteps, double* cfl) {
@@ -471,10 +504,11 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
                 RA_CUDA(cudaGraphInstantiate(&c.graph_exec, c.graph, 0));
                 c.graph_new_ab = new_ab;
                 c.graph_old_ab = old_ab;
+                c.graph_launches = c.launches - before;
                 c.launches = before;
             }
             RA_CUDA(cudaGraphLaunch(c.graph_exec, c.stream));
-            c.launches += 8;
+            c.launches += c.graph_launches;
         } else {
             enqueue_step(c, new_ab, old_ab);
         }
@@ -482,6 +516,7 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
         ++c.iteration;
     }
     if (cfl) {
+        check_status(c);
         unsigned long long bits = 0;
         RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
@@ -640,16 +675,16 @@ int ra_post_solve(ra_ctx* ctx) {
     return guarded(ctx, [&] {
         double n, o;
         ab_factors(ctx->c, n, o);
-        launch_cheb_synthesis(ctx->c);
-        launch_post_assemble(ctx->c, o);
+        run_stage(ctx->c, 0, n, o);
+        run_stage(ctx->c, 1, n, o);
     });
 }
 
 int ra_rlm_a(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {
-        launch_rlm_a(ctx->c);
-        launch_lt_inverse(ctx->c, ctx->c.d_s2a11, ctx->c.d_p2a, NP2A * ctx->c.d.nr * 2);
+        run_stage(ctx->c, 2, 0.0, 0.0);
+        run_stage(ctx->c, 3, 0.0, 0.0);
     });
 }
 
@@ -657,8 +692,7 @@ int ra_physical(ra_ctx* ctx, double* cfl) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
-        launch_physics(c);
+        run_stage(c, 4, 0.0, 0.0);
         if (cfl) {
             unsigned long long bits = 0;
             RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
@@ -673,15 +707,15 @@ int ra_rlm_b(ra_ctx* ctx) {
     return guarded(ctx, [&] {
         double n, o;
         ab_factors(ctx->c, n, o);
-        launch_lt_forward(ctx->c, ctx->c.d_p2b, ctx->c.d_s2b, NP2B * ctx->c.d.nr * 2);
-        launch_rlm_b(ctx->c, n);
+        run_stage(ctx->c, 5, n, o);
+        run_stage(ctx->c, 6, n, o);
     });
 }
 
 int ra_advance(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {
-        launch_solve(ctx->c);
+        run_stage(ctx->c, 7, 0.0, 0.0);
         ctx->c.old_dt = ctx->c.dt;
         ++ctx->c.iteration;
     });
@@ -689,7 +723,6 @@ int ra_advance(ra_ctx* ctx) {
 
 static const char* kKernelNames[] = {"cheb_synthesis", "post_assemble", "rlm_a",  "lt_inverse",
                                      "physics",        "lt_forward",    "rlm_b",  "solve"};
-constexpr int kNK = 8;
 
 int ra_kernels_per_step(void) { return kNK; }
 const char* ra_kernel_name(int i) { return (i >= 0 && i < kNK) ? kKernelNames[i] : nullptr; }
@@ -707,28 +740,16 @@ int ra_time_steps(ra_ctx* ctx, int nsteps, double* total_ms, double* kernel_ms, 
                 double new_ab, old_ab;
                 ab_factors(c, new_ab, old_ab);
                 cudaEvent_t* E = ev.data() + (size_t)s * (kNK + 1);
-                RA_CUDA(cudaEventRecord(E[0], c.stream));
-                launch_cheb_synthesis(c);
-                RA_CUDA(cudaEventRecord(E[1], c.stream));
-                launch_post_assemble(c, old_ab);
-                RA_CUDA(cudaEventRecord(E[2], c.stream));
-                launch_rlm_a(c);
-                RA_CUDA(cudaEventRecord(E[3], c.stream));
-                launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
-                RA_CUDA(cudaEventRecord(E[4], c.stream));
-                RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
-                launch_physics(c);
-                RA_CUDA(cudaEventRecord(E[5], c.stream));
-                launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
-                RA_CUDA(cudaEventRecord(E[6], c.stream));
-                launch_rlm_b(c, new_ab);
-                RA_CUDA(cudaEventRecord(E[7], c.stream));
-                launch_solve(c);
-                RA_CUDA(cudaEventRecord(E[8], c.stream));
+                for (int k = 0; k < kNK; ++k) {
+                    RA_CUDA(cudaEventRecord(E[k], c.stream));
+                    run_stage(c, k, new_ab, old_ab);
+                }
+                RA_CUDA(cudaEventRecord(E[kNK], c.stream));
                 c.old_dt = c.dt;
                 ++c.iteration;
             }
             RA_CUDA(cudaStreamSynchronize(c.stream));
+            check_status(c);
             float ms = 0.f;
             RA_CUDA(cudaEventElapsedTime(&ms, ev.front(), ev.back()));
             *total_ms = ms;
@@ -933,29 +954,34 @@ int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* cc, int
     return guarded(ctx, [&] {
         if (k > OZ_MAX_K) throw ArgError("ra_mixed_gemm: k exceeds the exact int32 accumulation limit");
         Ctx& c = ctx->c;
-        const int mp = oz_round_m(m), np = oz_round_n(n), kp = oz_round_k(k);
+        const int ntm = oz_tiles_of(m, OZ_HA), ntn = oz_tiles_of(n, OZ_HB), nks = oz_ksteps(k);
         double *da = nullptr, *db = nullptr, *dc = nullptr;
         int8_t *sa = nullptr, *sb = nullptr;
         int *ea = nullptr, *eb = nullptr, *dst = nullptr, *dtiles = nullptr;
         OzProblem* dprob = nullptr;
+        OzSplitJob* djobs = nullptr;
         dalloc(da, (size_t)m * k);
         dalloc(db, (size_t)k * n);
         dalloc(dc, (size_t)m * n);
-        RA_CUDA(cudaMalloc(&sa, (size_t)OZ_S * mp * kp));
-        RA_CUDA(cudaMalloc(&sb, (size_t)OZ_S * np * kp));
-        RA_CUDA(cudaMalloc(&ea, (size_t)mp * sizeof(int)));
-        RA_CUDA(cudaMalloc(&eb, (size_t)np * sizeof(int)));
-        RA_CUDA(cudaMalloc(&dst, sizeof(int)));
+        dalloc(sa, (size_t)ntm * nks * OZ_ABLK);
+        dalloc(sb, (size_t)ntn * nks * OZ_BBLK);
+        dalloc(ea, (size_t)m);
+        dalloc(eb, (size_t)n);
+        dalloc(dst, 1);
         RA_CUDA(cudaMemsetAsync(dst, 0, sizeof(int), c.stream));
         RA_CUDA(cudaMemcpyAsync(da, a, (size_t)m * k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaMemcpyAsync(db, b, (size_t)k * n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-        ozaki_split(c, da, k, 1, m, k, mp, kp, sa, (long)mp * kp, ea);   // rows of A
-        ozaki_split(c, db, 1, n, n, k, np, kp, sb, (long)np * kp, eb);   // columns of B
-        OzProblem pr{sa, sb, (long)mp * kp, (long)np * kp, ea, eb, m, n, kp, dc, n, 1};
+        // rows of A (k contiguous) and columns of B (rows of B^T, n apart)
+        OzSplitJob jobs[2] = {{da, (long)k, 1L, m, k, OZ_HA, ntm, nks, sa, ea},
+                              {db, 1L, (long)n, n, k, OZ_HB, ntn, nks, sb, eb}};
+        dalloc(djobs, 2);
+        RA_CUDA(cudaMemcpyAsync(djobs, jobs, sizeof(jobs), cudaMemcpyHostToDevice, c.stream));
+        ozaki_split(c, djobs, 2, std::max(ntm * OZ_HA, ntn * OZ_HB));
+        OzProblem pr{sa, sb, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, m, n, nks, dc, (long)n, 1L};
         std::vector<OzProblem> probs{pr};
         std::vector<int> tiles = ozaki_tiles(probs);
-        RA_CUDA(cudaMalloc(&dprob, sizeof(OzProblem)));
-        RA_CUDA(cudaMalloc(&dtiles, tiles.size() * sizeof(int)));
+        dalloc(dprob, 1);
+        dalloc(dtiles, tiles.size());
         RA_CUDA(cudaMemcpyAsync(dprob, probs.data(), sizeof(OzProblem), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaMemcpyAsync(dtiles, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream));
         ozaki_gemm(c, dprob, dtiles, (int)(tiles.size() / 4), dst);
@@ -964,7 +990,7 @@ int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* cc, int
         RA_CUDA(cudaMemcpyAsync(&status, dst, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
         cudaFree(da); cudaFree(db); cudaFree(dc); cudaFree(sa); cudaFree(sb);
-        cudaFree(ea); cudaFree(eb); cudaFree(dst); cudaFree(dprob); cudaFree(dtiles);
+        cudaFree(ea); cudaFree(eb); cudaFree(dst); cudaFree(dprob); cudaFree(dtiles); cudaFree(djobs);
         if (status) throw ArgError("tensor-core product timed out waiting on its pipeline barrier");
     });
 }

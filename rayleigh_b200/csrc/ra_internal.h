@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/rayleigh_b200.h"
+#include "ozaki.h"
 
 namespace ra {
 
@@ -64,6 +65,19 @@ struct Radial {
 
 struct GemmTile { int item, mt, nt, par; };
 
+// One batched split-precision product of the step (RA_PREC_MIXED): digit
+// buffers of its operands, the per-product descriptors, the tile list and the
+// per-step split jobs.
+struct MixedPlan {
+    int8_t *d_adig = nullptr, *d_bdig = nullptr;
+    int *d_ea = nullptr, *d_eb = nullptr;
+    OzProblem* d_probs = nullptr;
+    int* d_tiles = nullptr;
+    int ntiles = 0;
+    OzSplitJob* d_jobs = nullptr;
+    int njobs = 0, max_rows = 0;
+};
+
 struct Ctx {
     ra_config cfg;
     Dims d;
@@ -105,8 +119,11 @@ struct Ctx {
     unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
     int *d_status = nullptr;                          // device error word
 
+    MixedPlan mx_inv, mx_fwd;                         // RA_PREC_MIXED Legendre transforms
+
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    long graph_launches = 0;                          // kernels in one replay of the step graph
     double graph_old_ab = 0, graph_new_ab = 0;
 };
 
@@ -126,6 +143,10 @@ void launch_solve(Ctx& c);
 int  invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip);
 void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse);
 void launch_cheb_columns(Ctx& c, const double* d_in, double* d_out, long ncols, int mode, int order);
+void mixed_setup(Ctx& c);
+void mixed_release(Ctx& c);
+void launch_lt_inverse_mixed(Ctx& c);
+void launch_lt_forward_mixed(Ctx& c);
 
 #define RA_CUDA(call)                                                             \
     do {                                                                          \

@@ -1,9 +1,10 @@
 """Split-precision (int8 digit) tensor-core products against exact products.
 
-Each operand element is cut into six 7-bit digits after a power-of-two scaling
-of its row (A) or column (B); the 21 leading digit products are exact in int32.
-The error of entry (i, j) is therefore bounded by a small multiple of
-2^-40 K max_k|a_ik| max_k|b_kj|, which the tests check entry by entry."""
+Each operand element is rounded to a 39-bit integer after a power-of-two
+scaling of its row (A) or column (B) and cut into five balanced base-256 digits;
+the 15 leading digit products are exact in int32.  The error of entry (i, j) is
+therefore bounded by 2^-33 K max_k|a_ik| max_k|b_kj|, which the tests check entry
+by entry (measured errors are far below it)."""
 import numpy as np
 import pytest
 
@@ -26,7 +27,8 @@ def _check(ctx, a, b):
     c = ctx.mixed_gemm(a, b)
     exact = (a.astype(np.longdouble) @ b.astype(np.longdouble)).astype(np.float64)
     k = a.shape[1]
-    bound = 2.0**-36 * k * np.abs(a).max(axis=1)[:, None] * np.abs(b).max(axis=0)[None, :]
+    # per term: digit truncation <= 2^-37 and dropped digit products <= 2^-34 of max|a_i.| max|b_.j|
+    bound = 2.0**-33 * k * np.abs(a).max(axis=1)[:, None] * np.abs(b).max(axis=0)[None, :]
     err = np.abs(c - exact)
     assert np.all(err <= bound + 1e-300), (err / np.maximum(bound, 1e-300)).max()
     scale = np.abs(exact).max()
@@ -77,3 +79,66 @@ def test_legendre_table_product(ctx):
         s = rng.standard_normal((p.shape[0], 96))
         rel = _check(ctx, np.ascontiguousarray(p.T), s)
         assert rel < 1e-10, (m, rel)
+
+
+# ---------------------------------------------------------------------------
+# The mixed-precision step (RA_PREC_MIXED) against the oracle and the FP64 step
+# ---------------------------------------------------------------------------
+MIXED_TOL = 1e-9
+
+
+def _fields(wpt, z, nr):
+    return {"W": wpt[:, :, :nr], "P": wpt[:, :, nr:2 * nr], "T": wpt[:, :, 2 * nr:], "Z": z}
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _run(cfg, precision, wpt, z, steps):
+    import rayleigh_b200 as rb
+    g = rb.Rayleigh(rb.Config(**dict(cfg, precision=precision, use_graph=True)))
+    g.put_state(wpt, z, None, iteration=1)
+    g.step(steps)
+    w, zz, _ = g.get_state()
+    g.close()
+    return w, zz
+
+
+@pytest.mark.parametrize("cfg,steps", [
+    (dict(n_r=24, l_max=15, dt=2e-4), 20),
+    (dict(n_r=48, l_max=63, dt=1e-4), 10),
+])
+def test_mixed_step_vs_oracle(cfg, steps):
+    import oracle as O
+    import rayleigh_b200 as rb
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    oc = O.Config(**{k: v for k, v in cfg.items() if k in O.Config.__dataclass_fields__})
+    o = O.Oracle(oc)
+    wpt, z = O.seeded_state(oc, amp=1e-3, lmax_pert=min(20, oc.l_max))
+    o.init_state(wpt, z)
+    for _ in range(steps):
+        o.step()
+    w, zz = _run(cfg, rb.PREC_MIXED, wpt, z, steps)
+    ref = _fields(o.rhs_wpt, o.rhs_z, oc.n_r)
+    errs = {k: _rel(v, ref[k]) for k, v in _fields(w, zz, oc.n_r).items()}
+    print(cfg, {k: f"{v:.2e}" for k, v in errs.items()})
+    assert max(errs.values()) < MIXED_TOL, errs
+
+
+def test_mixed_step_vs_fp64_large():
+    # l_max = 255: the GPU FP64 form against the GPU mixed form, 5 steps
+    import oracle as O
+    import rayleigh_b200 as rb
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    cfg = dict(n_r=64, l_max=255, dt=1e-5, ekman=1e-4, rayleigh=1e7)
+    oc = O.Config(**{k: v for k, v in cfg.items() if k in O.Config.__dataclass_fields__})
+    wpt, z = O.seeded_state(oc, amp=1e-3, lmax_pert=20)
+    w64, z64 = _run(cfg, rb.PREC_FP64, wpt, z, 5)
+    wmx, zmx = _run(cfg, rb.PREC_MIXED, wpt, z, 5)
+    ref = _fields(w64, z64, oc.n_r)
+    errs = {k: _rel(v, ref[k]) for k, v in _fields(wmx, zmx, oc.n_r).items()}
+    print(cfg, {k: f"{v:.2e}" for k, v in errs.items()})
+    assert max(errs.values()) < MIXED_TOL, errs

@@ -81,8 +81,10 @@ void launch_plm(Ctx& c, const double* d_x, const double* d_w) {
 
 // ---------------------------------------------------------------------------
 // Inverse transform, per (m, parity):
-//   p2[m][par][theta_h][col] = sum_l P_par(l, theta_h) s2[row(m, l)][col]
-// (E for par = 0, O for par = 1; the physical-space kernel forms E +- O)
+//   p2[theta_h][m][par][col] = sum_l P_par(l, theta_h) s2[row(m, l)][col]
+// (E for par = 0, O for par = 1; the physical-space kernel forms E +- O).
+// theta_h is the slowest index so that the physical-space kernel, which reads
+// every (m, parity) of one theta_h, touches one contiguous block.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(GEMM_THREADS) lt_inverse_kernel(const double* __restrict__ Ptab,
                                                                   const double* __restrict__ s2,
@@ -110,10 +112,11 @@ __global__ void __launch_bounds__(GEMM_THREADS) lt_inverse_kernel(const double* 
         return (k < nl && col < ncol) ? __ldg(pb + (long)k * ncol + col) : 0.0;
     };
     gemm_tile<true, true>(acc, fa, fb, nl, sm);
-    double* out = p2 + (long)blockIdx.z * nth2 * ncol;
+    double* out = p2 + (long)blockIdx.z * ncol;
+    const long th_stride = 2L * L * ncol;
     acc_foreach(acc, [&](int x, int y, double v) {
         const int th = th0 + x, col = c0 + y;
-        if (th < nth2 && col < ncol) out[(long)th * ncol + col] = v;
+        if (th < nth2 && col < ncol) out[(long)th * th_stride + col] = v;
     });
 }
 

@@ -5,7 +5,7 @@
 // index (field, r, re/im) as the product's M: the tensor-memory lanes, and so
 // the epilogue threads, then walk contiguous output addresses.
 // Inverse transform (StP_4d_dgp2, Legendre_Transforms.F90:968-1074), one
-// product per (m, parity):  p2[m][par][theta_h][col] = sum_l P(l, theta_h) s2[row(m,l)][col]
+// product per (m, parity):  p2[theta_h][m][par][col] = sum_l P(l, theta_h) s2[row(m,l)][col]
 //   A = s2^T (M = 11 fields x N_r x re/im, K = number of l of that parity):
 //            digits made every step (exponent per column of s2, over l);
 //   B = P    (N = N_theta/2): digits of the FP64 tables made once at set-up.
@@ -78,9 +78,10 @@ static void setup_lt_inverse(Ctx& c) {
     for (int q = 0; q < 2 * L; ++q) {
         const int m = q >> 1, par = q & 1;
         const long roff = m_off(m, L) + (par ? n_even(m, L) : 0);
-        double* out = c.d_p2a + (size_t)q * nth2 * ncol;
+        double* out = c.d_p2a + (size_t)q * ncol;   // p2a[theta_h][m][par][col]
+        const long th_stride = 2L * L * ncol;
         if (nks[q] == 0) {   // no l of this parity: the E/O block stays zero
-            RA_CUDA(cudaMemsetAsync(out, 0, (size_t)nth2 * ncol * sizeof(double), c.stream));
+            RA_CUDA(cudaMemset2DAsync(out, th_stride * sizeof(double), 0, ncol * sizeof(double), nth2, c.stream));
             continue;
         }
         int8_t* adig = p.d_adig + aoff[q];
@@ -92,7 +93,7 @@ static void setup_lt_inverse(Ctx& c) {
         // B^T = P^T: rows theta_h (contiguous in the table), K = l; split once
         bjobs.push_back({c.d_Ptab + roff * nth2, 1L, (long)nth2, nth2, nl[q], OZ_HB, ntb, nks[q], bdig, eb});
         probs.push_back({adig, bdig, (long)nks[q] * OZ_ABLK, (long)nks[q] * OZ_BBLK, ea, eb, ncol, nth2, nks[q], out,
-                         1L, (long)ncol});
+                         1L, th_stride});
     }
     run_split_once(c, bjobs, ntb * OZ_HB);
     p.d_jobs = upload(c, ajobs);

@@ -4,21 +4,29 @@
 //   sintheta_div + NL terms   (Sphere_Physical_Space.F90:98-224, 303-700),
 //   Find_MyMinDT (CFL max)    (:784-813),
 //   fft_to_spectral (r2c)     (Fourier_Transform.F90:100-140), 4 fields,
-// reading the inverse Legendre output p2a[m][theta][f][r][re/im] and writing
-// p2b[m][theta][f][r][re/im] for m <= l_max.  The reference materialises the
-// packed (n_phi+2, r, theta, f) buffers p3a/p3b between these steps; here the
-// 18 phi rows of one (r, theta) point never leave the SM.
+//   equatorial fold of PtS    (Legendre_Transforms.F90:1109-1122),
+// reading the inverse Legendre output p2a[theta_h][m][par][f][r][re/im] (E, O) and
+// writing the folded p2b[m][par][theta_h][f][r][re/im] for m <= l_max.  The
+// reference materialises the packed (n_phi+2, r, theta, f) buffers p3a/p3b
+// between these steps; here the 18 phi rows of one (r, theta) point never
+// leave the SM.
+//
+// One CTA (256 threads, two per SM) handles one row; the rows theta and
+// pi - theta are the two CTAs of a cluster, which fold their spectra through
+// distributed shared memory.  The 14 input fields go through the FFT two at a
+// time; the four nonlinear outputs accumulate in shared memory (each thread
+// owns its points), the velocity in registers.
 //
 // FFT: a real length-2N transform through one complex length-N transform
-// (N = n_theta = 2^a 3^b), Stockham autosort, radix 4/2/3, in shared memory;
+// (N = n_theta = 2^a 3^b), Stockham autosort, radix 8/4/2/3, in shared memory;
 // unnormalised like FFTW (the normalisation lives in the Legendre tables).
 #include <cmath>
+
+#include <cooperative_groups.h>
 
 #include "ra_internal.h"
 
 namespace ra {
-
-constexpr int PHYS_THREADS = 256;
 
 struct FFTPlan {
     int n;
@@ -145,6 +153,10 @@ __host__ __device__ constexpr int pprod(int n, int i) {
 // stride-R writes of the first Stockham passes bank-conflict free.
 __device__ __forceinline__ int SW(int i) { return i ^ ((i >> 3) & 7); }
 
+// Stride between the fields of a batched buffer: a multiple of 64, so that a
+// field's swizzled indices stay inside the field whatever buffer it sits in.
+__host__ __device__ constexpr int fstride(int n) { return (n + 63) / 64 * 64; }
+
 // Offsets of the per-pass twiddle tables tw[(r-1) P + k] = exp(2 pi i r k STRIDE / N).
 __host__ __device__ constexpr int tw_off(int n, int ps) {
     int o = 0;
@@ -177,7 +189,7 @@ __device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, doub
 #pragma unroll 1
     for (int g = tid; g < T * NB; g += NT) {
         const int b = g / T, bi = g - b * T;
-        const int base = b * N;
+        const int base = b * fstride(N);
         const int k = bi % P;
         double2 u[R];
 #pragma unroll
@@ -219,92 +231,134 @@ struct PhysParams {
     double coriolis;
     int rotation;
     double llmax;
-    FFTPlan plan;
 };
 
-constexpr int FB = 4;                       // fields per batched FFT pass
-constexpr int HALF = PHYS_THREADS;          // threads per row
-constexpr int PAIR_THREADS = 2 * HALF;      // one CTA = rows theta and pi - theta
+// One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
+// 2-CTA cluster that folds its spectra through distributed shared memory.
+constexpr int ROW_THREADS = 256;
+constexpr int FB = 2;   // fields per batched FFT
 
-// Batched c2r of up to FB fields of one row.  The inverse Legendre transform
-// stores its even-l and odd-l products E, O separately (theta in the southern
-// half); the row's spectrum is X = E + O (h = 0, theta) or E - O (h = 1, the
-// mirrored row), as StP_4d_dgp2 reflects them (Legendre_Transforms.F90:1030-1064).
-// fields[b] is the p2a field index, dphi[b] selects d/dphi (i m X_m).  Result:
-// y[2n], y[2n+1] of field b at res[SW(b*N + n)].
-template <int NTH, int NB>
-__device__ double2* row_c2r_batch(const PhysParams& P, int thh, int h, int r, const int* fields, const bool* dphi,
-                                  double2* bufA, double2* bufB, const double2* tw, int t) {
-    constexpr int N = NTH, nb = NB;
-    constexpr int QL = (NTH + HALF - 1) / HALF;   // L <= N
+// Shared memory of a row CTA (double2 units): two FFT ping-pong buffers of FB
+// fields, the four nonlinear outputs (W, P, T, Z; each thread owns its points),
+// the per-pass twiddle tables.
+template <int N>
+struct RowSmem {
+    static constexpr int FS = fstride(N);
+    static constexpr int A = 0, B = FB * FS, ACC = 2 * FB * FS, TW = ACC + 4 * FS;
+    static constexpr int SIZE = TW + tw_size(N);
+};
+
+// Loads FB fields of this row's spectrum: X = E + O (south, h = 0) or E - O
+// (north, h = 1), as StP_4d_dgp2 reflects the even-l / odd-l products
+// (Legendre_Transforms.F90:1030-1064); d/dphi (i m X) where dphi[b]; Im X_0 = 0
+// as FFTW's c2r ignores it.  Then forms the half-length complex input
+//   Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N),
+// X_m = 0 for m >= L, and runs the complex FFT.  Returns the buffer holding
+// y[2n] + i y[2n+1] of field b at [SW(b*N + n)].
+template <int N>
+__device__ __forceinline__ double2* row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h,
+                                            int f0, bool d0, int f1, bool d1, double2* sm, const double2* tw,
+                                            int t) {
+    constexpr int QL = (N + ROW_THREADS - 1) / ROW_THREADS;
+    constexpr int FS = fstride(N);
     const int L = P.L;
-    const int nth2 = P.nth / 2;
-    const long mstride = 2L * nth2 * P.ncola;     // p2a[m][par][theta_h][col]
-    const long ostride = (long)nth2 * P.ncola;    // E -> O
-    double2 xs[NB][QL];
+    const long ostride = (long)P.ncola;   // E -> O within p2a[theta_h][m][par][col]
+    const long mstride = 2L * P.ncola;
+    double2* bA = sm + RowSmem<N>::A;
+    double2* bB = sm + RowSmem<N>::B;
+    {
+        double2 e[FB][QL], o[FB][QL];
+        const int fo[FB] = {f0, f1};
 #pragma unroll
-    for (int b = 0; b < nb; ++b) {
-        const double* base = P.p2a + (long)thh * P.ncola + ((long)fields[b] * P.nr + r) * 2;
+        for (int b = 0; b < FB; ++b) {
+            const double* base = rowbase + (long)fo[b] * P.nr * 2;
 #pragma unroll
-        for (int q = 0; q < QL; ++q) {
-            const int m = t + q * HALF;
-            if (m < L) {
-                const double2 e = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
-                const double2 o = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
-                xs[b][q] = h ? csub(e, o) : cadd(e, o);
-            } else {
-                xs[b][q] = make_double2(0.0, 0.0);
+            for (int q = 0; q < QL; ++q) {
+                const int m = t + q * ROW_THREADS;
+                if (m < L) {
+                    e[b][q] = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
+                    o[b][q] = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
+                }
             }
         }
-    }
+        const bool dp[FB] = {d0, d1};
 #pragma unroll
-    for (int b = 0; b < nb; ++b) {
-        const bool dp = dphi[b];
+        for (int b = 0; b < FB; ++b)
 #pragma unroll
-        for (int q = 0; q < QL; ++q) {
-            const int m = t + q * HALF;
-            if (m < N) {
-                double2 x = xs[b][q];
-                if (dp) x = make_double2(-m * x.y, m * x.x);
-                if (m == 0) x.y = 0.0;   // c2r ignores Im X_0 (FFTW's Hermitian convention)
-                bufB[SW(b * N + m)] = x;
+            for (int q = 0; q < QL; ++q) {
+                const int m = t + q * ROW_THREADS;
+                if (m < L) {
+                    double2 x = h ? csub(e[b][q], o[b][q]) : cadd(e[b][q], o[b][q]);
+                    if (dp[b]) x = make_double2(-m * x.y, m * x.x);
+                    if (m == 0) x.y = 0.0;
+                    bB[SW(b * FS + m)] = x;
+                }
             }
-        }
     }
     __syncthreads();
-    // Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N); X_m = 0 for m >= L
 #pragma unroll
-    for (int b = 0; b < nb; ++b) {
-        for (int k = t; k < N; k += HALF) {
-            const double2 xk = (k < L) ? bufB[SW(b * N + k)] : make_double2(0.0, 0.0);
+    for (int b = 0; b < FB; ++b) {
+        for (int k = t; k < N; k += ROW_THREADS) {
+            const double2 xk = (k < L) ? bB[SW(b * FS + k)] : make_double2(0.0, 0.0);
             const int kn = N - k;
-            const double2 xn = (kn < L) ? bufB[SW(b * N + kn)] : make_double2(0.0, 0.0);
-            const double2 e = cadd(xk, cconj(xn));
+            const double2 xn = (kn < L) ? bB[SW(b * FS + kn)] : make_double2(0.0, 0.0);
+            const double2 ee = cadd(xk, cconj(xn));
             const double2 d = csub(xk, cconj(xn));
             const double2 wd = cmul(__ldg(P.wr + k), d);
-            bufA[SW(b * N + k)] = make_double2(e.x - wd.y, e.y + wd.x);
+            bA[SW(b * FS + k)] = make_double2(ee.x - wd.y, ee.y + wd.x);
         }
     }
     __syncthreads();
-    return fft_run_t<N, NB, HALF>(bufA, bufB, tw, +1, t);
+    return fft_run_t<N, FB, ROW_THREADS>(bA, bB, tw, +1, t);
+}
+
+// r2c of two of the accumulated outputs (acc fields a0, a0+1): Z = FFT(y[2n] + i y[2n+1]),
+// X_k = e - i conj(w^k) d with e, d the half sums/differences of Z_k, conj Z_{N-k};
+// X_k (k < L) is written back over the two acc fields.
+template <int N>
+__device__ __forceinline__ void row_r2c_pair(const PhysParams& P, int a0, double2* sm, const double2* tw, int t) {
+    constexpr int FS = fstride(N);
+    double2* acc = sm + RowSmem<N>::ACC + a0 * FS;
+    double2* bA = sm + RowSmem<N>::A;
+    double2* bB = sm + RowSmem<N>::B;
+    fft_pass_t<N, FB, ROW_THREADS, 0>(acc, bA, tw, -1, t);
+    __syncthreads();
+    const double2* Z = fft_run_t<N, FB, ROW_THREADS, 1>(bA, bB, tw, -1, t);
+    const int L = P.L;
+    for (int g = t; g < FB * L; g += ROW_THREADS) {
+        const int f = g / L, k = g - f * L;
+        const double2 zk = Z[SW(f * FS + k)];
+        const double2 zn = cconj(Z[SW(f * FS + (N - k) % N)]);
+        const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
+        const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
+        const double2 wd = cmul(cconj(__ldg(P.wr + k)), d);
+        double2 Xk = make_double2(e.x + wd.y, e.y - wd.x);
+        if (k == 0) Xk.y = 0.0;
+        acc[SW(f * FS + k)] = Xk;
+    }
+    __syncthreads();
 }
 
 template <int NTH>
-__global__ void __launch_bounds__(PAIR_THREADS, 1) physics_kernel(PhysParams P) {
-    constexpr int ZPT = (NTH + HALF - 1) / HALF;
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) physics_kernel(PhysParams P) {
     constexpr int N = NTH;
+    constexpr int FS = fstride(N);
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int h = threadIdx.x / HALF, t = threadIdx.x % HALF;
-    double2* base0 = reinterpret_cast<double2*>(smem_raw);
-    double2* bufA = base0 + h * (2 * FB * N);
-    double2* bufB = bufA + FB * N;
-    double2* tw = base0 + 2 * (2 * FB * N);
-    __shared__ double red[PAIR_THREADS / 32];
-    build_twiddles<N, PAIR_THREADS>(tw, P.wr);
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    double2* tw = sm + RowSmem<N>::TW;
+    double2* acc = sm + RowSmem<N>::ACC;
+    __shared__ double red[ROW_THREADS / 32];
+    const int t = threadIdx.x;
+    const int h = (int)cluster.block_rank();        // 0: theta (south half), 1: pi - theta
+    build_twiddles<N, ROW_THREADS>(tw, P.wr);
     const int nr = P.nr;
-    const int r = blockIdx.x % nr;
-    const int thh = blockIdx.x / nr;                // southern-half theta index
-    const int th = h ? (N - 1 - thh) : thh;         // this half's row
+    const int pair = blockIdx.x >> 1;
+    const int r = pair % nr;
+    const int thh = pair / nr;
+    const int th = h ? (N - 1 - thh) : thh;
     const double rad = P.radial[R_RADIUS * nr + r];
     const double orad = P.radial[R_OVER_R * nr + r];
     const double rho = P.radial[R_DENSITY * nr + r];
@@ -312,27 +366,37 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1) physics_kernel(PhysParams P) 
     const double dr = P.radial[R_DELTA_R * nr + r];
     const double cs = P.trig[th], sn = P.trig[N + th], csc = P.trig[2 * N + th], cot = P.trig[3 * N + th];
     const double cor = P.rotation ? P.coriolis : 0.0;
+    const double c2r = csc * csc * orad;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * 2;
     __syncthreads();
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
-    double2 oW[ZPT], oP[ZPT], oT[ZPT], oZ[ZPT];
     auto val = [&](const double2* res, int b, int q) -> double2 {
-        const int n = t + q * HALF;
-        return (n < N) ? res[SW(b * N + n)] : make_double2(0.0, 0.0);
+        const int n = t + q * ROW_THREADS;
+        return (n < N) ? res[SW(b * FS + n)] : make_double2(0.0, 0.0);
     };
-    // batch 1: vr, vt, vp, dvrdr
+    auto acc_at = [&](int f, int q) -> double2& { return acc[SW(f * FS + t + q * ROW_THREADS)]; };
+    // B1: v_r, v_theta
     {
-        const int f[FB] = {A_VR, A_VT, A_VP, A_DVRDR};
-        const bool dp[FB] = {false, false, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
+        const double2* res = row_c2r<N>(P, rowbase, h, A_VR, false, A_VT, false, sm, tw, t);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             vr[q] = val(res, 0, q);
             vt[q] = val(res, 1, q);
-            vp[q] = val(res, 2, q);
-            const double2 x = val(res, 3, q);
-            vt[q].x *= csc; vt[q].y *= csc;
-            vp[q].x *= csc; vp[q].y *= csc;
+            vt[q].x *= csc;
+            vt[q].y *= csc;
+        }
+        __syncthreads();
+    }
+    // B2: v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
+    {
+        const double2* res = row_c2r<N>(P, rowbase, h, A_VP, false, A_DVRDR, false, sm, tw, t);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            vp[q] = val(res, 0, q);
+            vp[q].x *= csc;
+            vp[q].y *= csc;
+            const double2 x = val(res, 1, q);
             auto w0 = [&](double a, double b, double c, double xx) {
                 return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
             };
@@ -340,129 +404,133 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1) physics_kernel(PhysParams P) 
                 return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
             };
             auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
-            oW[q] = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
-            oP[q] = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
-            oZ[q] = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
-            oT[q] = make_double2(0.0, 0.0);
+            if (t + q * ROW_THREADS < N) {
+                acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                acc_at(2, q) = make_double2(0.0, 0.0);
+                acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+            }
         }
         __syncthreads();
     }
-    // batch 2: dvrdt, dvrdp, dvtdr, dvtdp
+    // B3: dv_r/dtheta, dv_r/dphi
     {
-        const int f[FB] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
-        const bool dp[FB] = {false, true, false, true};
-        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
-        const double c2r = csc * csc * orad;
+        const double2* res = row_c2r<N>(P, rowbase, h, A_DVRDT, false, A_VR, true, sm, tw, t);
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
-            const double2 a = val(res, 0, q), b = val(res, 1, q), c = val(res, 2, q), d = val(res, 3, q);
-            oW[q].x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
-            oW[q].y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
-            oP[q].x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
-            oP[q].y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
-            oZ[q].x += vt[q].x * d.x * c2r;
-            oZ[q].y += vt[q].y * d.y * c2r;
-        }
-        __syncthreads();
-    }
-    // batch 3: dvpdr, dvpdp, omega_r, dTdr
-    {
-        const int f[FB] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
-        const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 4>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
-        const double c2r = csc * csc * orad;
-#pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            const double2 a = val(res, 0, q), b = val(res, 1, q), c = val(res, 2, q), d = val(res, 3, q);
-            oZ[q].x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
-            oZ[q].y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
-            oP[q].x += -vt[q].x * b.x * c2r;
-            oP[q].y += -vt[q].y * b.y * c2r;
-            oT[q].x += -vr[q].x * d.x;
-            oT[q].y += -vr[q].y * d.y;
-        }
-        __syncthreads();
-    }
-    // batch 4: dTdt, dTdp
-    {
-        const int f[FB] = {A_DTDT, A_T, 0, 0};
-        const bool dp[FB] = {false, true, false, false};
-        const double2* res = row_c2r_batch<NTH, 2>(P, thh, h, r, f, dp, bufA, bufB, tw, t);
-#pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
+            if (t + q * ROW_THREADS >= N) continue;
             const double2 a = val(res, 0, q), b = val(res, 1, q);
-            oT[q].x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
-            oT[q].y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+            double2& w = acc_at(0, q);
+            w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
+            w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
         }
         __syncthreads();
     }
-    // CFL (Find_MyMinDT)
+    // B4: dv_theta/dr, dv_theta/dphi
+    {
+        const double2* res = row_c2r<N>(P, rowbase, h, A_DVTDR, false, A_VT, true, sm, tw, t);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            if (t + q * ROW_THREADS >= N) continue;
+            const double2 c = val(res, 0, q), d = val(res, 1, q);
+            double2& pp = acc_at(1, q);
+            double2& z = acc_at(3, q);
+            pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
+            pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
+            z.x += vt[q].x * d.x * c2r;
+            z.y += vt[q].y * d.y * c2r;
+        }
+        __syncthreads();
+    }
+    // B5: dv_phi/dr, dv_phi/dphi
+    {
+        const double2* res = row_c2r<N>(P, rowbase, h, A_DVPDR, false, A_VP, true, sm, tw, t);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            if (t + q * ROW_THREADS >= N) continue;
+            const double2 a = val(res, 0, q), b = val(res, 1, q);
+            double2& pp = acc_at(1, q);
+            double2& z = acc_at(3, q);
+            z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r;
+            z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r;
+            pp.x += -vt[q].x * b.x * c2r;
+            pp.y += -vt[q].y * b.y * c2r;
+        }
+        __syncthreads();
+    }
+    // B6: omega_r, dT/dr
+    {
+        const double2* res = row_c2r<N>(P, rowbase, h, A_OMR, false, A_DTDR, false, sm, tw, t);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            if (t + q * ROW_THREADS >= N) continue;
+            const double2 c = val(res, 0, q), d = val(res, 1, q);
+            double2& z = acc_at(3, q);
+            double2& tt = acc_at(2, q);
+            z.x += vt[q].x * c.x;
+            z.y += vt[q].y * c.y;
+            tt.x += -vr[q].x * d.x;
+            tt.y += -vr[q].y * d.y;
+        }
+        __syncthreads();
+    }
+    // B7: dT/dtheta, dT/dphi
+    {
+        const double2* res = row_c2r<N>(P, rowbase, h, A_DTDT, false, A_T, true, sm, tw, t);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            if (t + q * ROW_THREADS >= N) continue;
+            const double2 a = val(res, 0, q), b = val(res, 1, q);
+            double2& tt = acc_at(2, q);
+            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+        }
+    }
+    // CFL (Find_MyMinDT) and the rho r sin(theta) factor of the P and Z terms
     double cmax = 0.0;
     const double hfac = P.llmax * orad * orad, rfac = 1.0 / (dr * dr);
     const double sfac = rho * rad * csc;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
-        if ((t + q * HALF) < N) {
+        if ((t + q * ROW_THREADS) < N) {
             cmax = fmax(cmax, (vt[q].x * vt[q].x + vp[q].x * vp[q].x) * hfac);
             cmax = fmax(cmax, (vt[q].y * vt[q].y + vp[q].y * vp[q].y) * hfac);
             cmax = fmax(cmax, vr[q].x * vr[q].x * rfac);
             cmax = fmax(cmax, vr[q].y * vr[q].y * rfac);
-        }
-        oP[q].x *= sfac; oP[q].y *= sfac;
-        oZ[q].x *= sfac; oZ[q].y *= sfac;
-    }
-    // batched r2c of W, P, T, Z
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        const int n = t + q * HALF;
-        if (n < N) {
-            bufA[SW(0 * N + n)] = oW[q];
-            bufA[SW(1 * N + n)] = oP[q];
-            bufA[SW(2 * N + n)] = oT[q];
-            bufA[SW(3 * N + n)] = oZ[q];
+            double2& pp = acc_at(1, q);
+            double2& z = acc_at(3, q);
+            pp.x *= sfac; pp.y *= sfac;
+            z.x *= sfac; z.y *= sfac;
         }
     }
     __syncthreads();
-    double2* Z = fft_run_t<N, 4, HALF>(bufA, bufB, tw, -1, t);
-    double2* X = (Z == bufA) ? bufB : bufA;   // this half's spectra X_k, k < L
-    const int L = P.L;
-    for (int g = t; g < 4 * L; g += HALF) {
-        const int f = g / L, k = g - f * L;
-        const double2 zk = Z[SW(f * N + k)];
-        const double2 zn = cconj(Z[SW(f * N + (N - k) % N)]);
-        const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
-        const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
-        // X_k = e - i conj(w^k) d
-        const double2 wd = cmul(cconj(__ldg(P.wr + k)), d);
-        double2 Xk = make_double2(e.x + wd.y, e.y - wd.x);
-        if (k == 0) Xk.y = 0.0;
-        X[SW(f * N + k)] = Xk;
-    }
-    __syncthreads();
-    // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122):
-    // f_even = X(theta) + X(pi - theta), f_odd = X(theta) - X(pi - theta)
+    // r2c of W, P and of T, Z; the spectra X_k (k < L) replace the accumulators
+    row_r2c_pair<N>(P, 0, sm, tw, t);
+    row_r2c_pair<N>(P, 2, sm, tw, t);
+    // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122) with the
+    // partner row: f_even = X(theta) + X(pi - theta) (written by rank 0),
+    // f_odd = X(theta) - X(pi - theta) (written by rank 1)
+    cluster.sync();
     {
-        constexpr bool ZA = (npass_of(N) % 2) == 0;   // the FFT result sits in bufA when the pass count is even
-        const double2* Xs = base0 + (ZA ? FB * N : 0);
-        const double2* Xn = base0 + 2 * FB * N + (ZA ? FB * N : 0);
-        const int nth2 = P.nth / 2;
-        const long mstride = 2L * nth2 * P.ncolb;
-        const long ostride = (long)nth2 * P.ncolb;
-        for (int g = threadIdx.x; g < 4 * L; g += PAIR_THREADS) {
+        const double2* mine = acc;
+        const double2* peer = cluster.map_shared_rank(acc, h ^ 1);
+        const int L = P.L;
+        const long mstride = 2L * (P.nth / 2) * P.ncolb;   // p2b[m][par][theta_h][col]
+        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * 2;
+        for (int g = t; g < 4 * L; g += ROW_THREADS) {
             const int f = g / L, k = g - f * L;
-            const double2 a = Xs[SW(f * N + k)], b = Xn[SW(f * N + k)];
-            double* o = P.p2b + k * mstride + (long)thh * P.ncolb + ((long)f * P.nr + r) * 2;
-            *reinterpret_cast<double2*>(o) = cadd(a, b);
-            *reinterpret_cast<double2*>(o + ostride) = csub(a, b);
+            const double2 a = mine[SW(f * FS + k)], b = peer[SW(f * FS + k)];
+            const double2 v = h ? csub(b, a) : cadd(a, b);
+            *reinterpret_cast<double2*>(obase + k * mstride + (long)f * P.nr * 2) = v;
         }
     }
-    // CFL max over the two rows
+    // CFL max over the row
     for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cmax;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    if ((t & 31) == 0) red[t >> 5] = cmax;
+    cluster.sync();   // the partner has finished reading this CTA's spectra
+    if (t == 0) {
         double v = red[0];
-        for (int i = 1; i < PAIR_THREADS / 32; ++i) v = fmax(v, red[i]);
+        for (int i = 1; i < ROW_THREADS / 32; ++i) v = fmax(v, red[i]);
         atomicMax(P.cfl, (unsigned long long)__double_as_longlong(v));
     }
 }
@@ -495,25 +563,26 @@ void launch_physics(Ctx& c) {
     P.coriolis = c.rad.coriolis;
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
-    P.plan = make_plan(c.d.nth);
-    const unsigned grid = (unsigned)c.d.nth2 * c.d.nr;
-    auto go = [&](auto kern, int n) {
-        const size_t smem = (4 * FB * (size_t)n + tw_size(n)) * sizeof(double2);
+    make_plan(c.d.nth);   // validates n_theta = 2^a 3^b
+    const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;   // clusters of 2 rows
+    auto go = [&](auto kern, int n, size_t smem_units) {
+        const size_t smem = smem_units * sizeof(double2);
         RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, PAIR_THREADS, smem, c.stream>>>(P);
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P);
+        (void)n;
     };
     switch (c.d.nth) {
-        case 24: go(physics_kernel<24>, 24); break;
-        case 32: go(physics_kernel<32>, 32); break;
-        case 48: go(physics_kernel<48>, 48); break;
-        case 64: go(physics_kernel<64>, 64); break;
-        case 96: go(physics_kernel<96>, 96); break;
-        case 128: go(physics_kernel<128>, 128); break;
-        case 192: go(physics_kernel<192>, 192); break;
-        case 256: go(physics_kernel<256>, 256); break;
-        case 384: go(physics_kernel<384>, 384); break;
-        case 512: go(physics_kernel<512>, 512); break;
-        case 768: go(physics_kernel<768>, 768); break;
+        case 24: go(physics_kernel<24>, 24, RowSmem<24>::SIZE); break;
+        case 32: go(physics_kernel<32>, 32, RowSmem<32>::SIZE); break;
+        case 48: go(physics_kernel<48>, 48, RowSmem<48>::SIZE); break;
+        case 64: go(physics_kernel<64>, 64, RowSmem<64>::SIZE); break;
+        case 96: go(physics_kernel<96>, 96, RowSmem<96>::SIZE); break;
+        case 128: go(physics_kernel<128>, 128, RowSmem<128>::SIZE); break;
+        case 192: go(physics_kernel<192>, 192, RowSmem<192>::SIZE); break;
+        case 256: go(physics_kernel<256>, 256, RowSmem<256>::SIZE); break;
+        case 384: go(physics_kernel<384>, 384, RowSmem<384>::SIZE); break;
+        case 512: go(physics_kernel<512>, 512, RowSmem<512>::SIZE); break;
+        case 768: go(physics_kernel<768>, 768, RowSmem<768>::SIZE); break;
         default: throw ArgError("n_theta " + std::to_string(c.d.nth) +
                                 " has no physical-space kernel instance (24..768 of the form 2^a or 3*2^a)");
     }
@@ -521,9 +590,6 @@ void launch_physics(Ctx& c) {
     ++c.launches;
 }
 
-// ---------------------------------------------------------------------------
-// Standalone in-place row FFTs on x(n_phi+2, howmany) (unit-level operator)
-// ---------------------------------------------------------------------------
 __global__ void fft_rows_kernel(double* x, long howmany, const double2* wrg, FFTPlan plan, int inverse) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N = plan.n;

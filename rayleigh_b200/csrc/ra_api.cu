@@ -849,7 +849,7 @@ int ra_legendre_s2p(ra_ctx* ctx, const double* s, double* p, int nf, int nr) {
         RA_CUDA(cudaStreamSynchronize(c.stream));
         cudaFree(ds);
         cudaFree(dp);
-        // device p2[m][par][th_h][f][r][ri] (E, O) -> host p2a(th, (r, ri, f), m):
+        // device p2[th_h][m][par][f][r][ri] (E, O) -> host p2a(th, (r, ri, f), m):
         // south th_h: E + O, north nth-1-th_h: E - O (Legendre_Transforms.F90:1030-1064)
         const int nth2 = nth / 2;
         for (int m = 0; m < L; ++m)
@@ -858,8 +858,8 @@ int ra_legendre_s2p(ra_ctx* ctx, const double* s, double* p, int nf, int nr) {
                     for (int r = 0; r < nr; ++r)
                         for (int th = 0; th < nth2; ++th) {
                             const size_t cidx = ((size_t)f * nr + r) * 2 + ri;
-                            const double e = hp[(((size_t)m * 2 + 0) * nth2 + th) * ncol + cidx];
-                            const double o = hp[(((size_t)m * 2 + 1) * nth2 + th) * ncol + cidx];
+                            const double e = hp[(((size_t)th * L + m) * 2 + 0) * ncol + cidx];
+                            const double o = hp[(((size_t)th * L + m) * 2 + 1) * ncol + cidx];
                             double* dst = p + ((((size_t)m * nf + f) * 2 + ri) * nr + r) * nth;
                             dst[th] = e + o;
                             dst[nth - 1 - th] = e - o;

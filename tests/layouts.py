@@ -43,8 +43,8 @@ def rel_err(a, b):
 
 
 def p2_eo_to_full(dev, L, nth, F, nr):
-    """device [m][par][nth/2][F][nr][2] (E, O) -> [m][nth][F][nr][2] with south E+O, north E-O."""
-    d = dev.reshape(L, 2, nth // 2, F, nr, 2)
+    """device [nth/2][m][par][F][nr][2] (E, O) -> [m][nth][F][nr][2] with south E+O, north E-O."""
+    d = dev.reshape(nth // 2, L, 2, F, nr, 2).transpose(1, 2, 0, 3, 4, 5)
     e, o = d[:, 0], d[:, 1]
     full = np.empty((L, nth, F, nr, 2))
     full[:, :nth // 2] = e + o

@@ -248,68 +248,123 @@ struct RowSmem {
     static constexpr int SIZE = TW + tw_size(N);
 };
 
-// Loads FB fields of this row's spectrum: X = E + O (south, h = 0) or E - O
-// (north, h = 1), as StP_4d_dgp2 reflects the even-l / odd-l products
-// (Legendre_Transforms.F90:1030-1064); d/dphi (i m X) where dphi[b]; Im X_0 = 0
-// as FFTW's c2r ignores it.  Then forms the half-length complex input
-//   Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N),
-// X_m = 0 for m >= L, and runs the complex FFT.  Returns the buffer holding
-// y[2n] + i y[2n+1] of field b at [SW(b*N + n)].
+// Runs the Stockham passes PS .. PE-1 (ping-pong a -> b -> a ...); returns the
+// buffer holding the result.
+template <int N, int NB, int NT, int PS, int PE>
+__device__ __forceinline__ double2* fft_range(double2* a, double2* b, const double2* tw, int sign, int tid) {
+    if constexpr (PS < PE) {
+        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign, tid);
+        __syncthreads();
+        return fft_range<N, NB, NT, PS + 1, PE>(b, a, tw, sign, tid);
+    } else {
+        return a;
+    }
+}
+
+// One spectrum value of this row: X = E + O (south, h = 0) or E - O (north,
+// h = 1), as StP_4d_dgp2 reflects the even-l / odd-l products
+// (Legendre_Transforms.F90:1030-1064); d/dphi (i m X) when dp; Im X_0 = 0 as
+// FFTW's c2r ignores it; X_m = 0 for m >= L.
+__device__ __forceinline__ double2 spec_value(const double* __restrict__ base, long mstride, long ostride, int m,
+                                              int L, int h, bool dp) {
+    if (m >= L) return make_double2(0.0, 0.0);
+    const double2 e = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
+    const double2 o = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
+    double2 x = h ? csub(e, o) : cadd(e, o);
+    if (dp) x = make_double2(-m * x.y, m * x.x);
+    if (m == 0) x.y = 0.0;
+    return x;
+}
+
+// Half-length complex input of the real transform:
+//   Z_k = (X_k + conj X_{N-k}) + i w^k (X_k - conj X_{N-k}),  w = exp(2 pi i / 2N).
+__device__ __forceinline__ double2 zform(double2 xk, double2 xn, double2 wk) {
+    const double2 e = cadd(xk, cconj(xn));
+    const double2 d = csub(xk, cconj(xn));
+    const double2 wd = cmul(wk, d);
+    return make_double2(e.x - wd.y, e.y + wd.x);
+}
+
+// Whether the last Stockham pass leaves, per thread t, the outputs n = t + q*ROW_THREADS
+// of every field (then it is run straight into registers).
 template <int N>
-__device__ __forceinline__ double2* row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h,
-                                            int f0, bool d0, int f1, bool d1, double2* sm, const double2* tw,
-                                            int t) {
-    constexpr int QL = (N + ROW_THREADS - 1) / ROW_THREADS;
+__host__ __device__ constexpr bool last_pass_in_regs() {
+    return N / radix_at(N, npass_of(N) - 1) == ROW_THREADS;
+}
+
+// Forms the half-length complex FFT input Z_k (zform) of FB fields of this row
+// in buffer A straight from the spectra in p2a (spec_value): one work item is
+// the pair (k, N-k), whose two Z values need the same two spectrum values.
+template <int N>
+__device__ __forceinline__ void c2r_stage(const PhysParams& P, const double* __restrict__ rowbase, int h, int f0,
+                                          bool d0, int f1, bool d1, double2* bA, int t) {
     constexpr int FS = fstride(N);
+    constexpr int NI = N / 2 + 1;                                   // k = 0 .. N/2
+    constexpr int QI = (FB * NI + ROW_THREADS - 1) / ROW_THREADS;   // items per thread
     const int L = P.L;
     const long ostride = (long)P.ncola;   // E -> O within p2a[theta_h][m][par][col]
     const long mstride = 2L * P.ncola;
+    double2 xk[QI], xn[QI];
+#pragma unroll
+    for (int q = 0; q < QI; ++q) {
+        const int g = t + q * ROW_THREADS;
+        xk[q] = xn[q] = make_double2(0.0, 0.0);
+        if (g < FB * NI) {
+            const int b = g / NI, k = g - b * NI;
+            const double* base = rowbase + (long)(b ? f1 : f0) * P.nr * 2;
+            const bool dp = b ? d1 : d0;
+            xk[q] = spec_value(base, mstride, ostride, k, L, h, dp);
+            xn[q] = spec_value(base, mstride, ostride, N - k, L, h, dp);   // N - k >= L for k = 0
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < QI; ++q) {
+        const int g = t + q * ROW_THREADS;
+        if (g < FB * NI) {
+            const int b = g / NI, k = g - b * NI;
+            bA[SW(b * FS + k)] = zform(xk[q], xn[q], __ldg(P.wr + k));
+            if (k != 0 && 2 * k != N) bA[SW(b * FS + N - k)] = zform(xn[q], xk[q], __ldg(P.wr + N - k));
+        }
+    }
+    __syncthreads();
+}
+
+// c2r of FB fields of this row: y[b][q] = (y[2n], y[2n+1]) of field b at n = t + q*ROW_THREADS.
+template <int N, int ZPT>
+__device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h, int f0,
+                                        bool d0, int f1, bool d1, double2* sm, const double2* tw, int t,
+                                        double2 (&y)[FB][ZPT]) {
+    constexpr int FS = fstride(N), NP = npass_of(N);
     double2* bA = sm + RowSmem<N>::A;
     double2* bB = sm + RowSmem<N>::B;
-    {
-        double2 e[FB][QL], o[FB][QL];
-        const int fo[FB] = {f0, f1};
+    c2r_stage<N>(P, rowbase, h, f0, d0, f1, d1, bA, t);
+    if constexpr (last_pass_in_regs<N>()) {
+        const double2* src = fft_range<N, FB, ROW_THREADS, 0, NP - 1>(bA, bB, tw, +1, t);
+        constexpr int PS = NP - 1, R = radix_at(N, PS), PP = pprod(N, PS), TO = tw_off(N, PS);
+        static_assert(R == ZPT, "last radix must equal the points per thread");
 #pragma unroll
         for (int b = 0; b < FB; ++b) {
-            const double* base = rowbase + (long)fo[b] * P.nr * 2;
+            double2 u[R];
 #pragma unroll
-            for (int q = 0; q < QL; ++q) {
-                const int m = t + q * ROW_THREADS;
-                if (m < L) {
-                    e[b][q] = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
-                    o[b][q] = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
-                }
+            for (int r = 0; r < R; ++r) u[r] = src[SW(b * FS + t + r * ROW_THREADS)];
+            if (PP > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], tw[TO + (r - 1) * PP + t]);
             }
+            dft_small(R, u, +1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) y[b][r] = u[r];
         }
-        const bool dp[FB] = {d0, d1};
+    } else {
+        const double2* res = fft_range<N, FB, ROW_THREADS, 0, NP>(bA, bB, tw, +1, t);
 #pragma unroll
         for (int b = 0; b < FB; ++b)
 #pragma unroll
-            for (int q = 0; q < QL; ++q) {
-                const int m = t + q * ROW_THREADS;
-                if (m < L) {
-                    double2 x = h ? csub(e[b][q], o[b][q]) : cadd(e[b][q], o[b][q]);
-                    if (dp[b]) x = make_double2(-m * x.y, m * x.x);
-                    if (m == 0) x.y = 0.0;
-                    bB[SW(b * FS + m)] = x;
-                }
+            for (int q = 0; q < ZPT; ++q) {
+                const int n = t + q * ROW_THREADS;
+                y[b][q] = (n < N) ? res[SW(b * FS + n)] : make_double2(0.0, 0.0);
             }
     }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < FB; ++b) {
-        for (int k = t; k < N; k += ROW_THREADS) {
-            const double2 xk = (k < L) ? bB[SW(b * FS + k)] : make_double2(0.0, 0.0);
-            const int kn = N - k;
-            const double2 xn = (kn < L) ? bB[SW(b * FS + kn)] : make_double2(0.0, 0.0);
-            const double2 ee = cadd(xk, cconj(xn));
-            const double2 d = csub(xk, cconj(xn));
-            const double2 wd = cmul(__ldg(P.wr + k), d);
-            bA[SW(b * FS + k)] = make_double2(ee.x - wd.y, ee.y + wd.x);
-        }
-    }
-    __syncthreads();
-    return fft_run_t<N, FB, ROW_THREADS>(bA, bB, tw, +1, t);
 }
 
 // r2c of two of the accumulated outputs (acc fields a0, a0+1): Z = FFT(y[2n] + i y[2n+1]),
@@ -371,120 +426,104 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     __syncthreads();
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
-    auto val = [&](const double2* res, int b, int q) -> double2 {
-        const int n = t + q * ROW_THREADS;
-        return (n < N) ? res[SW(b * FS + n)] : make_double2(0.0, 0.0);
-    };
+    double2 y[FB][ZPT];
     auto acc_at = [&](int f, int q) -> double2& { return acc[SW(f * FS + t + q * ROW_THREADS)]; };
+    auto live = [&](int q) { return t + q * ROW_THREADS < N; };
     // B1: v_r, v_theta
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_VR, false, A_VT, false, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_VR, false, A_VT, false, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            vr[q] = val(res, 0, q);
-            vt[q] = val(res, 1, q);
-            vt[q].x *= csc;
-            vt[q].y *= csc;
-        }
-        __syncthreads();
+    for (int q = 0; q < ZPT; ++q) {
+        vr[q] = y[0][q];
+        vt[q] = y[1][q];
+        vt[q].x *= csc;
+        vt[q].y *= csc;
     }
+    __syncthreads();
     // B2: v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_VP, false, A_DVRDR, false, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_VP, false, A_DVRDR, false, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            vp[q] = val(res, 0, q);
-            vp[q].x *= csc;
-            vp[q].y *= csc;
-            const double2 x = val(res, 1, q);
-            auto w0 = [&](double a, double b, double c, double xx) {
-                return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
-            };
-            auto p0 = [&](double a, double b, double c, double xx) {
-                return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
-            };
-            auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
-            if (t + q * ROW_THREADS < N) {
-                acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
-                acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
-                acc_at(2, q) = make_double2(0.0, 0.0);
-                acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
-            }
+    for (int q = 0; q < ZPT; ++q) {
+        vp[q] = y[0][q];
+        vp[q].x *= csc;
+        vp[q].y *= csc;
+        const double2 x = y[1][q];
+        auto w0 = [&](double a, double b, double c, double xx) {
+            return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
+        };
+        auto p0 = [&](double a, double b, double c, double xx) {
+            return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
+        };
+        auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+        if (live(q)) {
+            acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
+            acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
+            acc_at(2, q) = make_double2(0.0, 0.0);
+            acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
         }
-        __syncthreads();
     }
+    __syncthreads();
     // B3: dv_r/dtheta, dv_r/dphi
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_DVRDT, false, A_VR, true, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_DVRDT, false, A_VR, true, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (t + q * ROW_THREADS >= N) continue;
-            const double2 a = val(res, 0, q), b = val(res, 1, q);
-            double2& w = acc_at(0, q);
-            w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
-            w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
-        }
-        __syncthreads();
+    for (int q = 0; q < ZPT; ++q) {
+        if (!live(q)) continue;
+        const double2 a = y[0][q], b = y[1][q];
+        double2& w = acc_at(0, q);
+        w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
+        w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
     }
+    __syncthreads();
     // B4: dv_theta/dr, dv_theta/dphi
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_DVTDR, false, A_VT, true, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_DVTDR, false, A_VT, true, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (t + q * ROW_THREADS >= N) continue;
-            const double2 c = val(res, 0, q), d = val(res, 1, q);
-            double2& pp = acc_at(1, q);
-            double2& z = acc_at(3, q);
-            pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
-            pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
-            z.x += vt[q].x * d.x * c2r;
-            z.y += vt[q].y * d.y * c2r;
-        }
-        __syncthreads();
+    for (int q = 0; q < ZPT; ++q) {
+        if (!live(q)) continue;
+        const double2 c = y[0][q], d = y[1][q];
+        double2& pp = acc_at(1, q);
+        double2& z = acc_at(3, q);
+        pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
+        pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
+        z.x += vt[q].x * d.x * c2r;
+        z.y += vt[q].y * d.y * c2r;
     }
+    __syncthreads();
     // B5: dv_phi/dr, dv_phi/dphi
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_DVPDR, false, A_VP, true, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_DVPDR, false, A_VP, true, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (t + q * ROW_THREADS >= N) continue;
-            const double2 a = val(res, 0, q), b = val(res, 1, q);
-            double2& pp = acc_at(1, q);
-            double2& z = acc_at(3, q);
-            z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r;
-            z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r;
-            pp.x += -vt[q].x * b.x * c2r;
-            pp.y += -vt[q].y * b.y * c2r;
-        }
-        __syncthreads();
+    for (int q = 0; q < ZPT; ++q) {
+        if (!live(q)) continue;
+        const double2 a = y[0][q], b = y[1][q];
+        double2& pp = acc_at(1, q);
+        double2& z = acc_at(3, q);
+        z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r;
+        z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r;
+        pp.x += -vt[q].x * b.x * c2r;
+        pp.y += -vt[q].y * b.y * c2r;
     }
+    __syncthreads();
     // B6: omega_r, dT/dr
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_OMR, false, A_DTDR, false, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_OMR, false, A_DTDR, false, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (t + q * ROW_THREADS >= N) continue;
-            const double2 c = val(res, 0, q), d = val(res, 1, q);
-            double2& z = acc_at(3, q);
-            double2& tt = acc_at(2, q);
-            z.x += vt[q].x * c.x;
-            z.y += vt[q].y * c.y;
-            tt.x += -vr[q].x * d.x;
-            tt.y += -vr[q].y * d.y;
-        }
-        __syncthreads();
+    for (int q = 0; q < ZPT; ++q) {
+        if (!live(q)) continue;
+        const double2 c = y[0][q], d = y[1][q];
+        double2& z = acc_at(3, q);
+        double2& tt = acc_at(2, q);
+        z.x += vt[q].x * c.x;
+        z.y += vt[q].y * c.y;
+        tt.x += -vr[q].x * d.x;
+        tt.y += -vr[q].y * d.y;
     }
+    __syncthreads();
     // B7: dT/dtheta, dT/dphi
-    {
-        const double2* res = row_c2r<N>(P, rowbase, h, A_DTDT, false, A_T, true, sm, tw, t);
+    row_c2r<N, ZPT>(P, rowbase, h, A_DTDT, false, A_T, true, sm, tw, t, y);
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (t + q * ROW_THREADS >= N) continue;
-            const double2 a = val(res, 0, q), b = val(res, 1, q);
-            double2& tt = acc_at(2, q);
-            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
-            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
-        }
+    for (int q = 0; q < ZPT; ++q) {
+        if (!live(q)) continue;
+        const double2 a = y[0][q], b = y[1][q];
+        double2& tt = acc_at(2, q);
+        tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+        tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
     }
     // CFL (Find_MyMinDT) and the rho r sin(theta) factor of the P and Z terms
     double cmax = 0.0;

@@ -1,5 +1,5 @@
-// RA_PREC_MIXED: the Legendre transforms as batched split-precision products
-// on the int8 tensor cores (k_ozaki.cu).
+// RA_PREC_MIXED: the Legendre transforms and the implicit solve as batched
+// split-precision products on the int8 tensor cores (k_ozaki.cu).
 //
 // Both transforms are computed transposed, with the long, contiguous column
 // index (field, r, re/im) as the product's M: the tensor-memory lanes, and so
@@ -163,6 +163,83 @@ void launch_lt_forward_mixed(Ctx& c) {
     ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
 }
 
+// ---------------------------------------------------------------------------
+// Implicit solve (Implicit_Solve, Linear_Solve.F90:423-457): x = A_l^{-1} b per
+// (system, l), the inverses' digits made at set-up and after every dt change,
+// the right-hand sides' digits every step.  The K index of b runs over the
+// whole coupled block (W, P, T for the linked system), so a column's scaling
+// is set by its largest block.
+// ---------------------------------------------------------------------------
+static void setup_solve(Ctx& c) {
+    const Dims& d = c.d;
+    const int L = d.L, nr = d.nr;
+    MixedPlan& p = c.mx_solve;
+    long asize = 0, bsize = 0;
+    for (int sys = 0; sys < 2; ++sys) {
+        const int n = sys ? nr : 3 * nr;
+        const int nta = oz_tiles_of(n, OZ_HA), nks = oz_ksteps(n);
+        asize += (long)L * nta * nks * OZ_ABLK;
+        for (int l = 0; l < L; ++l) bsize += (long)oz_tiles_of(2 * (l + 1), OZ_HB) * nks * OZ_BBLK;
+    }
+    malloc_dev(p.d_adig, (size_t)asize);
+    malloc_dev(p.d_bdig, (size_t)bsize);
+    malloc_dev(p.d_ea, (size_t)L * 4 * nr);           // 3 nr + nr rows per l
+    malloc_dev(p.d_eb, (size_t)2 * 2 * d.nlm);        // (lm, re/im) columns of both systems
+    std::vector<OzSplitJob> ajobs, bjobs;
+    std::vector<OzProblem> probs;
+    long ao = 0, bo = 0;
+    int max_a = 0, max_b = 0;
+    for (int sys = 0; sys < 2; ++sys) {
+        const int n = sys ? nr : 3 * nr;
+        const int nta = oz_tiles_of(n, OZ_HA), nks = oz_ksteps(n);
+        const double* Ainv = sys ? c.d_Az : c.d_Awpt;
+        const double* rhs = sys ? c.d_rhs_z : c.d_rhs_wpt;
+        double* sol = sys ? c.d_sol_z : c.d_sol_wpt;
+        int* ea_sys = p.d_ea + (sys ? (size_t)L * 3 * nr : 0);
+        int* eb_sys = p.d_eb + (size_t)sys * 2 * d.nlm;
+        max_a = std::max(max_a, nta * OZ_HA);
+        for (int l = 0; l < L; ++l) {
+            const long lstart = (long)l * (l + 1) / 2;
+            const int ncol = 2 * (l + 1);
+            const int ntb = oz_tiles_of(ncol, OZ_HB);
+            max_b = std::max(max_b, ntb * OZ_HB);
+            int8_t* adig = p.d_adig + ao;
+            int8_t* bdig = p.d_bdig + bo;
+            ao += (long)nta * nks * OZ_ABLK;
+            bo += (long)ntb * nks * OZ_BBLK;
+            int* ea = ea_sys + (size_t)l * n;
+            int* eb = eb_sys + 2 * lstart;
+            // rows of A_l^{-1} (K contiguous); right-hand-side columns (lm, re/im), K contiguous
+            ajobs.push_back({Ainv + (size_t)l * n * n, (long)n, 1L, n, n, OZ_HA, nta, nks, adig, ea});
+            bjobs.push_back({rhs + 2 * lstart * n, (long)n, 1L, ncol, n, OZ_HB, ntb, nks, bdig, eb});
+            probs.push_back({adig, bdig, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, n, ncol, nks,
+                             sol + 2 * lstart * n, 1L, (long)n});
+        }
+    }
+    p.d_setup_jobs = upload(c, ajobs);
+    p.nsetup_jobs = (int)ajobs.size();
+    p.setup_max_rows = max_a;
+    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows);
+    p.d_jobs = upload(c, bjobs);
+    p.njobs = (int)bjobs.size();
+    p.max_rows = max_b;
+    plan_launch(c, p, probs);
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void mixed_resplit_solve(Ctx& c) {
+    MixedPlan& p = c.mx_solve;
+    if (!p.d_setup_jobs) return;
+    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows);
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void launch_solve_mixed(Ctx& c) {
+    MixedPlan& p = c.mx_solve;
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
+}
+
 void mixed_setup(Ctx& c) {
     if (!c.d_status) {
         malloc_dev(c.d_status, 1);
@@ -170,6 +247,7 @@ void mixed_setup(Ctx& c) {
     }
     setup_lt_inverse(c);
     setup_lt_forward(c);
+    setup_solve(c);
 }
 
 static void free_plan(MixedPlan& p) {
@@ -180,12 +258,14 @@ static void free_plan(MixedPlan& p) {
     if (p.d_probs) cudaFree(p.d_probs);
     if (p.d_tiles) cudaFree(p.d_tiles);
     if (p.d_jobs) cudaFree(p.d_jobs);
+    if (p.d_setup_jobs) cudaFree(p.d_setup_jobs);
     p = MixedPlan{};
 }
 
 void mixed_release(Ctx& c) {
     free_plan(c.mx_inv);
     free_plan(c.mx_fwd);
+    free_plan(c.mx_solve);
 }
 
 }  // namespace ra

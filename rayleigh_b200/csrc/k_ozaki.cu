@@ -10,7 +10,7 @@
 // over K in int32 by tcgen05.mma.kind::i8, one TMEM accumulator per diagonal
 // d = s + t (exact for K < 20000), and the epilogue forms
 //     c_ij = 2^{ea_i + eb_j} sum_d D_d[i,j] 2^{-(8d+14)}
-// in FP64 (all scalings are exact powers of two).  The relative error of a
+// exactly in int64 and rounds it once to FP64 (all scalings are powers of two).  The relative error of a
 // Legendre transform is ~1e-11 (vs ~1e-6 for one FP32-accumulated product).
 //
 // The product kernel is persistent (one CTA per SM, tiles dealt round-robin
@@ -20,9 +20,9 @@
 //   warp 1      MMA issuer: 15 tcgen05.mma per K-step, committed to the
 //               stage's "empty" barrier and, after the last K-step, to the
 //               accumulator's "full" barrier;
-//   warps 2-9   epilogue: two warps per TMEM lane quadrant, each taking half
-//               of the tile's columns: tcgen05.ld of the 5 diagonals (one
-//               wait per 8 columns), FP64 recombination, scaled stores.
+//   warps 2-13  epilogue: three warps per TMEM lane quadrant, each taking a
+//               third of the tile's columns: tcgen05.ld of the 5 diagonals (one
+//               wait per 8 columns), exact int64 recombination, scaled stores.
 // Output tiles are 128 x 48, so two accumulator sets (2 x 5 x 48 columns)
 // fit in tensor memory and the epilogue of one tile overlaps the MMAs of the
 // next.  Every wait is bounded: when a limit runs out the CTA raises the
@@ -38,9 +38,10 @@
 namespace ra {
 
 constexpr int OZ_NST = 6;
-constexpr int OZ_EPI_WARPS = 8;                            // two per TMEM lane quadrant
+constexpr int OZ_EPI_WARPS = 12;                           // three per TMEM lane quadrant
 constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
-constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (24)
+constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (16)
+static_assert(OZ_EPI_COLS % 8 == 0 && OZ_EPI_COLS <= 32, "epilogue column split");
 constexpr int OZ_ACC_STRIDE = 256;           // TMEM columns between the two accumulator sets
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_STAGE = OZ_ABLK + OZ_BBLK;  // 28160 bytes
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&sm.acc_full[b], 1);
-            mbar_init(&sm.acc_empty[b], 32 * OZ_EPI_WARPS);
+            mbar_init(&sm.acc_empty[b], OZ_EPI_WARPS);
         }
         mbar_init(&sm.drain, 1);
         sm.abort = 0;
@@ -183,14 +184,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
 
     if (warp == 0) {
         // ---------------- producer ----------------
+        // the next tile's descriptor is loaded while the current one streams
         int it = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int t = blockIdx.x;
+        int4 tl = (t < ntiles) ? tiles[t] : make_int4(0, 0, 0, 0);
+        OzProblem pb = probs[tl.x];
+        for (; t < ntiles; t += gridDim.x) {
             if (vload(&sm.abort)) break;
-            const int4 tl = tiles[t];
-            const OzProblem& pb = probs[tl.x];
+            const int tn = t + gridDim.x;
+            const int4 tl_n = (tn < ntiles) ? tiles[tn] : tl;
             const int8_t* a = pb.A + (long)tl.y * pb.a_tile;
             const int8_t* b = pb.B + (long)tl.z * pb.b_tile;
-            const int nks = pb.nks;
+            const int nks = tl.w;
             bool ok = true;
             for (int ks = 0; ks < nks; ++ks, ++it) {
                 const int st = it % OZ_NST;
@@ -210,6 +215,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
                 sm.abort = 1;
                 break;
             }
+            tl = tl_n;
+            pb = probs[tl.x];
         }
         // copies still in flight after an abort: wait (bounded) for the last ones
         if (vload(&sm.abort)) {
@@ -219,10 +226,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         const uint32_t idesc = idesc_i8(OZ_HA, OZ_HB);
+        // stage-0 descriptors; every stage and digit slice is an offset from these
+        // (shared addresses stay below 2^18, so the 14-bit start field cannot overflow)
+        const uint64_t adesc0 = umma_desc(smem_u32(&sm.stage[0][0]), OZ_HA * 16, 128);
+        const uint64_t bdesc0 = umma_desc(smem_u32(&sm.stage[0][OZ_ABLK]), OZ_HB * 16, 128);
         int it = 0, tl_i = 0;
+        int nks_n = (blockIdx.x < ntiles) ? tiles[blockIdx.x].w : 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
             if (vload(&sm.abort)) break;
-            const int nks = probs[tiles[t].x].nks;
+            const int nks = nks_n;
+            if (t + (int)gridDim.x < ntiles) nks_n = tiles[t + gridDim.x].w;
             const int buf = tl_i & 1;
             const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
             bool ok = __all_sync(0xffffffffu, mbar_wait(&sm.acc_empty[buf], aph ^ 1u));
@@ -237,15 +250,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 if (lane == 0) {
-                    const uint32_t sa = smem_u32(&sm.stage[st][0]);
-                    const uint32_t sb = smem_u32(&sm.stage[st][OZ_ABLK]);
+                    // descriptors of this stage: the start-address field (16-byte units) advanced
+                    const uint64_t ast = adesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
+                    const uint64_t bst = bdesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
 #pragma unroll
                     for (int d = 0; d < OZ_S; ++d) {
 #pragma unroll
                         for (int s = 0; s <= d; ++s) {
-                            const uint64_t ad = umma_desc(sa + s * (OZ_HA * OZ_BK), OZ_HA * 16, 128);
-                            const uint64_t bd = umma_desc(sb + (d - s) * (OZ_HB * OZ_BK), OZ_HB * 16, 128);
-                            mma_i8(dacc + (uint32_t)(d * OZ_HB), ad, bd, idesc, (ks > 0 || s > 0) ? 1u : 0u);
+                            mma_i8(dacc + (uint32_t)(d * OZ_HB), ast + (uint64_t)((s * OZ_HA * OZ_BK) >> 4),
+                                   bst + (uint64_t)(((d - s) * OZ_HB * OZ_BK) >> 4), idesc,
+                                   (ks > 0 || s > 0) ? 1u : 0u);
                         }
                     }
                     umma_commit(&sm.empty[st]);
@@ -264,14 +278,20 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
         __syncwarp();
         if (!__all_sync(0xffffffffu, mbar_wait(&sm.drain, 0))) sm.abort = 1;
     } else {
-        // ---------------- epilogue (warps 2..9): lane quadrant warp % 4, column half (warp - 2) / 4 ----------------
+        // ---------------- epilogue (warps 2..13): lane quadrant warp % 4, column third (warp - 2) / 4 ----------------
         const int q = warp & 3;
         const int cbeg = ((warp - 2) >> 2) * OZ_EPI_COLS;
         int tl_i = 0;
+        int4 tl_n = (blockIdx.x < ntiles) ? tiles[blockIdx.x] : make_int4(0, 0, 0, 0);
+        OzProblem pb_n = probs[tl_n.x];
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
             if (vload(&sm.abort)) break;
-            const int4 tl = tiles[t];
-            const OzProblem pb = probs[tl.x];   // by value: stores to C cannot alias it
+            const int4 tl = tl_n;
+            const OzProblem pb = pb_n;   // by value: stores to C cannot alias it
+            if (t + (int)gridDim.x < ntiles) {
+                tl_n = tiles[t + gridDim.x];
+                pb_n = probs[tl_n.x];
+            }
             const int buf = tl_i & 1;
             const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
             if (!mbar_wait(&sm.acc_full[buf], aph)) {
@@ -281,8 +301,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
             asm volatile("tcgen05.fence::after_thread_sync;");
             const int row = tl.y * OZ_HA + q * 32 + lane;
             const bool rok = row < pb.M;
-            // row scale with the digit weight 2^-14 folded in
-            const double sa = rok ? pow2(pb.ea[row] - 14) : 0.0;
+            // row scale with the combined weight 2^-46 of S below folded in
+            const double sa = rok ? pow2(pb.ea[row] - 46) : 0.0;
+            // column scales of this warp's columns, one per lane, shared by shuffle
+            const int colw = tl.z * OZ_HB + cbeg + lane;
+            const double sbl = (lane < OZ_EPI_COLS && colw < pb.N) ? pow2(__ldg(pb.eb + colw)) : 0.0;
             double* crow = pb.C + (long)row * pb.c_m;
             const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * OZ_ACC_STRIDE);
 #pragma unroll 1
@@ -298,20 +321,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
                 const int cb = tl.z * OZ_HB + c0;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    // int32 -> double as (2^52 + 2^31 + x) - (2^52 + 2^31): exact, no conversion unit
-                    double acc = 0.0, w = 1.0;
+                    // S = sum_d D_d 2^(8(4-d)) is exact in int64 (|S| < 2^59 for K <= 20000);
+                    // the value is S 2^-46 2^(ea + eb), rounded once
+                    long long S = (long long)(int)v[0][j];
 #pragma unroll
-                    for (int d = 0; d < OZ_S; ++d) {
-                        const double x = __hiloint2double(0x43300000, (int)(v[d][j] ^ 0x80000000u)) - 4503601774854144.0;
-                        acc = fma(x, w, acc);
-                        w *= 0x1p-8;
-                    }
+                    for (int d = 1; d < OZ_S; ++d) S = S * 256 + (long long)(int)v[d][j];
+                    const double sb = __shfl_sync(0xffffffffu, sbl, c0 - cbeg + j);
                     const int col = cb + j;
-                    if (rok && col < pb.N) crow[(long)col * pb.c_n] = (acc * sa) * pow2(__ldg(pb.eb + col));
+                    if (rok && col < pb.N) crow[(long)col * pb.c_n] = (__ll2double_rn(S) * sa) * sb;
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
-            mbar_arrive(&sm.acc_empty[buf]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.acc_empty[buf]);
         }
     }
 
@@ -425,8 +447,8 @@ void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles
     ++c.launches;
 }
 
-// Tile list (problem, m-tile, n-tile, 0), longest K first so that the ragged
-// products finish together; products with K = 0 get no tiles.
+// Tile list (problem, m-tile, n-tile, K-steps), longest K first so that the
+// ragged products finish together; products with K = 0 get no tiles.
 std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
     std::vector<int> order(probs.size());
     for (size_t p = 0; p < probs.size(); ++p) order[p] = (int)p;
@@ -440,7 +462,7 @@ std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
                 t.push_back(p);
                 t.push_back(mt);
                 t.push_back(nt);
-                t.push_back(0);
+                t.push_back(q.nks);
             }
     }
     return t;
@@ -482,7 +504,7 @@ __global__ void oz_static_prepare_kernel(OzProblem pr, OzSplitJob ja, OzSplitJob
         djobs[1] = jb;
         *status = 0;
     }
-    if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, 0);
+    if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, pr.nks);
 }
 
 }  // namespace ra

@@ -465,7 +465,12 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
                 launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
             break;
         case 6: launch_rlm_b(c, new_ab); break;
-        default: launch_solve(c); break;
+        default:
+            if (mixed)
+                launch_solve_mixed(c);
+            else
+                launch_solve(c);
+            break;
     }
 }
 
@@ -628,6 +633,7 @@ int ra_set_dt(ra_ctx* ctx, double dt) {
         if (!(dt > 0)) throw ArgError("dt must be positive");
         ctx->c.dt = dt;
         linear_setup(ctx->c);
+        if (ctx->c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(ctx->c);
     });
 }
 

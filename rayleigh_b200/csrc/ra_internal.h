@@ -76,6 +76,8 @@ struct MixedPlan {
     int ntiles = 0;
     OzSplitJob* d_jobs = nullptr;
     int njobs = 0, max_rows = 0;
+    OzSplitJob* d_setup_jobs = nullptr;   // splits of the constant operand, rerun when it changes
+    int nsetup_jobs = 0, setup_max_rows = 0;
 };
 
 struct Ctx {
@@ -119,7 +121,7 @@ struct Ctx {
     unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
     int *d_status = nullptr;                          // device error word
 
-    MixedPlan mx_inv, mx_fwd;                         // RA_PREC_MIXED Legendre transforms
+    MixedPlan mx_inv, mx_fwd, mx_solve;               // RA_PREC_MIXED Legendre transforms, implicit solve
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -147,6 +149,8 @@ void mixed_setup(Ctx& c);
 void mixed_release(Ctx& c);
 void launch_lt_inverse_mixed(Ctx& c);
 void launch_lt_forward_mixed(Ctx& c);
+void launch_solve_mixed(Ctx& c);
+void mixed_resplit_solve(Ctx& c);
 
 #define RA_CUDA(call)                                                             \
     do {                                                                          \

@@ -1,11 +1,15 @@
 """Benchmark: Rayleigh timesteps/s at l_max = 511, N_r = 192 on one B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-                    [--impl ours|reference] [--lmax 511] [--nr 192]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
+                    [--impl ours|reference] [--lmax 511] [--nr 192] [--err-steps 100]
 
 One JSON line on rank 0.  A step is one pass of the hot path (Post_Solve,
 rlm_spacea, physical_space, rlm_spaceb, AdvanceTime) over the whole state;
 the state (~35 GB of buffers) stays resident in HBM and is far larger than L2.
+By default both forms run from the same seeded state: the line reports the
+mixed-precision step, with the FP64 step and the per-field relative error of
+the mixed state against the FP64 state after --err-steps steps beside it (the
+FP64 form is reported instead if that error exceeds 1e-9).
 ``--impl reference`` times the reference algorithm on the host cores: the
 NumPy restatement under ``oracle/`` (the Fortran reference cannot be built in
 this image), sampled per stage and scaled to one full step.
@@ -276,21 +280,17 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, torch, dist):
+def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, peak_kind):
+    """Times one precision form on this rank; returns (line fields or None off rank 0, state at step err_steps)."""
+    import ctypes
     import rayleigh_b200 as rb
-    from rayleigh_b200 import build as rbuild
-    rbuild.build()
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    prec = rb.PREC_MIXED if args.precision == "mixed" else rb.PREC_FP64
+    prec = rb.PREC_MIXED if prec_name == "mixed" else rb.PREC_FP64
     cfgd = headline_config(args.lmax, args.nr, prec)
-    cfg = rb.Config(**cfgd, use_graph=True, device=local)
-    ctx = rb.Rayleigh(cfg)
+    ctx = rb.Rayleigh(rb.Config(**cfgd, use_graph=True, device=local))
     rng = np.random.Generator(np.random.PCG64(SEED + rank))
     wpt, z = initial_state(ctx, args.lmax, args.nr, rng)
     ctx.put_state(wpt, z, None, iteration=1)
-    peaks, peak_kind = measured_peaks()
-    fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
     # warm-up (includes the Euler first step)
     ctx.time_steps(max(1, args.warmup))
     if world > 1:
@@ -306,6 +306,11 @@ def run_ours(args, rank, world, torch, dist):
         dist.barrier()
     max_ms = float(t.item())
     value = world * args.steps / (max_ms * 1e-3)
+    # continue (untimed) to err_steps for the mixed-vs-FP64 comparison
+    done = max(1, args.warmup) + args.steps
+    if args.err_steps > done:
+        ctx.step(args.err_steps - done)
+    state = ctx.get_state()[:2] if rank == 0 else None
 
     # end to end through the C ABI with host buffers: H2D of the full state, one
     # step, D2H of the new state and its CFL cargo, every step
@@ -318,7 +323,6 @@ def run_ours(args, rank, world, torch, dist):
     h_wpt[:] = w0.ravel()
     h_z[:] = z0.ravel()
     h_ab[:] = ab0.ravel()
-    import ctypes
     lib = ctx.lib
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     e2e_steps = max(1, min(args.steps, 5))
@@ -336,10 +340,13 @@ def run_ours(args, rank, world, torch, dist):
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = world / float(e2e_t.item())
+    n_theta, n_phi = ctx.n_theta, ctx.n_phi
+    ctx.close()
+    del h_wpt, h_z, h_ab, o_wpt, o_z, o_ab
     if rank != 0:
-        return
+        return None, None
     # roofline of the dominant kernel
-    work = kernel_work(args.lmax, args.nr, ctx.n_theta)
+    work = kernel_work(args.lmax, args.nr, n_theta)
     dom = max(per_kernel, key=lambda k: per_kernel[k])
     bound, amount = work[dom]
     avg_s = per_kernel[dom] / args.steps * 1e-3
@@ -347,7 +354,7 @@ def run_ours(args, rank, world, torch, dist):
     tpath = os.path.join(HERE, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"{dom}_{args.precision}_lmax{args.lmax}_nr{args.nr}")
+            traffic = json.load(open(tpath)).get(f"{dom}_{prec_name}_lmax{args.lmax}_nr{args.nr}")
         except Exception:
             traffic = None
     if bound == "tensor":
@@ -361,15 +368,13 @@ def run_ours(args, rank, world, torch, dist):
     kernels = {}
     for k, ms in per_kernel.items():
         b, amt = work[k]
-        s = ms / args.steps * 1e-3
+        sec = ms / args.steps * 1e-3
         kernels[k] = {"ms_per_step": round(ms / args.steps, 4), "share": round(ms / total_ms, 4),
-                      ("tflops" if b == "tensor" else "gbs"): round(amt / s / (1e12 if b == "tensor" else 1e9), 2)}
-    line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "precision": args.precision, "data": "synthetic (seeded)",
+                      ("tflops" if b == "tensor" else "gbs"): round(amt / sec / (1e12 if b == "tensor" else 1e9), 2)}
+    fields = {
+        "value": value, "ms_per_step": max_ms / args.steps, "precision": prec_name,
         "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
-                   "n_r": args.nr, "n_theta": ctx.n_theta, "n_phi": ctx.n_phi, "ekman": cfgd["ekman"],
+                   "n_r": args.nr, "n_theta": n_theta, "n_phi": n_phi, "ekman": cfgd["ekman"],
                    "dt": cfgd["dt"], "l2": "working set (~35 GB) larger than L2; no flush needed",
                    "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
@@ -380,6 +385,58 @@ def run_ours(args, rank, world, torch, dist):
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "how": "ra_put_state (pinned host) + ra_step(1) + ra_get_state (pinned host) per step"},
     }
+    return fields, state
+
+
+def _field_errors(mixed_state, fp64_state, nr):
+    (wm, zm), (wf, zf) = mixed_state, fp64_state
+    out = {}
+    for name, a, b in (("W", wm[:, :, :nr], wf[:, :, :nr]), ("P", wm[:, :, nr:2 * nr], wf[:, :, nr:2 * nr]),
+                       ("T", wm[:, :, 2 * nr:], wf[:, :, 2 * nr:]), ("Z", zm, zf)):
+        den = float(np.linalg.norm(b))
+        out[name] = float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a))
+    return out
+
+
+def run_ours(args, rank, world, torch, dist):
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    peaks, peak_kind = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    res = {}
+    for f in forms:
+        res[f] = run_precision(args, f, rank, world, torch, dist, fp64_peak, peaks, peak_kind)
+    if rank != 0:
+        return
+    head_form = "mixed" if "mixed" in res else "fp64"
+    head, _ = res[head_form]
+    line = {"metric": METRIC, "value": head["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "precision": head_form,
+            "data": "synthetic (seeded)"}
+    for k in ("config", "roofline", "kernels", "gpu_launches", "clocks", "e2e"):
+        line[k] = head[k]
+    if len(res) == 2:
+        f64, _ = res["fp64"]
+        errs = _field_errors(res["mixed"][1], res["fp64"][1], args.nr)
+        worst = max(errs.values())
+        line["fp64"] = {k: f64[k] for k in ("value", "ms_per_step", "roofline", "kernels", "gpu_launches",
+                                            "clocks", "e2e")}
+        line["mixed_vs_fp64"] = {"speedup": head["value"] / f64["value"],
+                                 "rel_err_per_field": errs, "max_rel_err": worst, "tolerance": 1e-9,
+                                 "within_tolerance": worst <= 1e-9, "steps_compared": args.err_steps,
+                                 "how": "relative L2 norm per field of the state after the same steps from the "
+                                        "same seeded initial state"}
+        if worst > 1e-9:
+            # the mixed number does not meet the accuracy bound: report the FP64 form as the headline
+            line["value"] = f64["value"]
+            line["ms_per_step"] = f64["ms_per_step"]
+            line["precision"] = "fp64"
+            for k in ("roofline", "kernels", "gpu_launches", "clocks", "e2e"):
+                line[k] = f64[k]
     if not args.no_cpu:
         cs = CpuSample(args.lmax, args.nr)
         sec, parts = cs.step_seconds()
@@ -394,7 +451,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: time the FP64 and the mixed form, report the mixed one with its error vs FP64")
+    ap.add_argument("--err-steps", type=int, default=100,
+                    help="steps after which the mixed and FP64 states are compared")
     ap.add_argument("--lmax", type=int, default=511)
     ap.add_argument("--nr", type=int, default=192)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")

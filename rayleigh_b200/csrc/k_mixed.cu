@@ -166,37 +166,41 @@ void launch_lt_forward_mixed(Ctx& c) {
 // ---------------------------------------------------------------------------
 // Implicit solve (Implicit_Solve, Linear_Solve.F90:423-457): x = A_l^{-1} b per
 // (system, l), the inverses' digits made at set-up and after every dt change,
-// the right-hand sides' digits every step.  The K index of b runs over the
-// whole coupled block (W, P, T for the linked system), so a column's scaling
-// is set by its largest block.
+// the right-hand sides' digits every step.  The K index of the linked W-P-T
+// system runs over three blocks of very different size (the W, P and T
+// coefficients); each block is a K segment with its own exponents, so the
+// small W part keeps its relative accuracy.
 // ---------------------------------------------------------------------------
 static void setup_solve(Ctx& c) {
     const Dims& d = c.d;
     const int L = d.L, nr = d.nr;
     MixedPlan& p = c.mx_solve;
-    long asize = 0, bsize = 0;
+    const int kseg = oz_ksteps(nr);   // K-steps of one radial block
+    long asize = 0, bsize = 0, esize_a = 0, esize_b = 0;
     for (int sys = 0; sys < 2; ++sys) {
-        const int n = sys ? nr : 3 * nr;
-        const int nta = oz_tiles_of(n, OZ_HA), nks = oz_ksteps(n);
+        const int n = sys ? nr : 3 * nr, nseg = sys ? 1 : 3;
+        const int nta = oz_tiles_of(n, OZ_HA), nks = nseg * kseg;
         asize += (long)L * nta * nks * OZ_ABLK;
-        for (int l = 0; l < L; ++l) bsize += (long)oz_tiles_of(2 * (l + 1), OZ_HB) * nks * OZ_BBLK;
+        esize_a += (long)L * nseg * n;
+        for (int l = 0; l < L; ++l) {
+            bsize += (long)oz_tiles_of(2 * (l + 1), OZ_HB) * nks * OZ_BBLK;
+            esize_b += (long)nseg * 2 * (l + 1);
+        }
     }
     malloc_dev(p.d_adig, (size_t)asize);
     malloc_dev(p.d_bdig, (size_t)bsize);
-    malloc_dev(p.d_ea, (size_t)L * 4 * nr);           // 3 nr + nr rows per l
-    malloc_dev(p.d_eb, (size_t)2 * 2 * d.nlm);        // (lm, re/im) columns of both systems
+    malloc_dev(p.d_ea, (size_t)esize_a);
+    malloc_dev(p.d_eb, (size_t)esize_b);
     std::vector<OzSplitJob> ajobs, bjobs;
     std::vector<OzProblem> probs;
-    long ao = 0, bo = 0;
+    long ao = 0, bo = 0, eao = 0, ebo = 0;
     int max_a = 0, max_b = 0;
     for (int sys = 0; sys < 2; ++sys) {
-        const int n = sys ? nr : 3 * nr;
-        const int nta = oz_tiles_of(n, OZ_HA), nks = oz_ksteps(n);
+        const int n = sys ? nr : 3 * nr, nseg = sys ? 1 : 3;
+        const int nta = oz_tiles_of(n, OZ_HA), nks = nseg * kseg;
         const double* Ainv = sys ? c.d_Az : c.d_Awpt;
         const double* rhs = sys ? c.d_rhs_z : c.d_rhs_wpt;
         double* sol = sys ? c.d_sol_z : c.d_sol_wpt;
-        int* ea_sys = p.d_ea + (sys ? (size_t)L * 3 * nr : 0);
-        int* eb_sys = p.d_eb + (size_t)sys * 2 * d.nlm;
         max_a = std::max(max_a, nta * OZ_HA);
         for (int l = 0; l < L; ++l) {
             const long lstart = (long)l * (l + 1) / 2;
@@ -205,15 +209,22 @@ static void setup_solve(Ctx& c) {
             max_b = std::max(max_b, ntb * OZ_HB);
             int8_t* adig = p.d_adig + ao;
             int8_t* bdig = p.d_bdig + bo;
+            int* ea = p.d_ea + eao;   // [segment][n]
+            int* eb = p.d_eb + ebo;   // [segment][ncol]
             ao += (long)nta * nks * OZ_ABLK;
             bo += (long)ntb * nks * OZ_BBLK;
-            int* ea = ea_sys + (size_t)l * n;
-            int* eb = eb_sys + 2 * lstart;
-            // rows of A_l^{-1} (K contiguous); right-hand-side columns (lm, re/im), K contiguous
-            ajobs.push_back({Ainv + (size_t)l * n * n, (long)n, 1L, n, n, OZ_HA, nta, nks, adig, ea});
-            bjobs.push_back({rhs + 2 * lstart * n, (long)n, 1L, ncol, n, OZ_HB, ntb, nks, bdig, eb});
+            eao += (long)nseg * n;
+            ebo += (long)nseg * ncol;
+            for (int sg = 0; sg < nseg; ++sg) {
+                // rows of A_l^{-1} restricted to the columns of block sg (K contiguous);
+                // right-hand-side columns (lm, re/im) restricted to the rows of block sg
+                ajobs.push_back({Ainv + (size_t)l * n * n + sg * nr, (long)n, 1L, n, nr, OZ_HA, nta, kseg, adig,
+                                 ea + (long)sg * n, nks, sg * kseg});
+                bjobs.push_back({rhs + 2 * lstart * n + sg * nr, (long)n, 1L, ncol, nr, OZ_HB, ntb, kseg, bdig,
+                                 eb + (long)sg * ncol, nks, sg * kseg});
+            }
             probs.push_back({adig, bdig, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, n, ncol, nks,
-                             sol + 2 * lstart * n, 1L, (long)n});
+                             sol + 2 * lstart * n, 1L, (long)n, nseg, (long)n, (long)ncol});
         }
     }
     p.d_setup_jobs = upload(c, ajobs);

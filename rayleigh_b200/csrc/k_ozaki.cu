@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
             const int4 tl_n = (tn < ntiles) ? tiles[tn] : tl;
             const int8_t* a = pb.A + (long)tl.y * pb.a_tile;
             const int8_t* b = pb.B + (long)tl.z * pb.b_tile;
-            const int nks = tl.w;
+            const int nks = tl.w & 0xFFFF;
             bool ok = true;
             for (int ks = 0; ks < nks; ++ks, ++it) {
                 const int st = it % OZ_NST;
@@ -230,49 +230,51 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
         // (shared addresses stay below 2^18, so the 14-bit start field cannot overflow)
         const uint64_t adesc0 = umma_desc(smem_u32(&sm.stage[0][0]), OZ_HA * 16, 128);
         const uint64_t bdesc0 = umma_desc(smem_u32(&sm.stage[0][OZ_ABLK]), OZ_HB * 16, 128);
-        int it = 0, tl_i = 0;
-        int nks_n = (blockIdx.x < ntiles) ? tiles[blockIdx.x].w : 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
+        int it = 0, tl_i = 0;   // tl_i counts accumulator uses (segments)
+        int tw_n = (blockIdx.x < ntiles) ? tiles[blockIdx.x].w : 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             if (vload(&sm.abort)) break;
-            const int nks = nks_n;
-            if (t + (int)gridDim.x < ntiles) nks_n = tiles[t + gridDim.x].w;
-            const int buf = tl_i & 1;
-            const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
-            bool ok = __all_sync(0xffffffffu, mbar_wait(&sm.acc_empty[buf], aph ^ 1u));
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t dacc = tmem + (uint32_t)(buf * OZ_ACC_STRIDE);
-            for (int ks = 0; ks < nks && ok; ++ks, ++it) {
-                const int st = it % OZ_NST;
-                const uint32_t ph = (uint32_t)(it / OZ_NST) & 1u;
-                if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[st], ph))) {
-                    ok = false;
-                    break;
-                }
+            const int nks = tw_n & 0xFFFF, nseg = tw_n >> 16;
+            if (t + (int)gridDim.x < ntiles) tw_n = tiles[t + gridDim.x].w;
+            const int kseg = nks / nseg;
+            for (int sg = 0; sg < nseg && ok; ++sg, ++tl_i) {
+                const int buf = tl_i & 1;
+                const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+                ok = __all_sync(0xffffffffu, mbar_wait(&sm.acc_empty[buf], aph ^ 1u));
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                if (lane == 0) {
-                    // descriptors of this stage: the start-address field (16-byte units) advanced
-                    const uint64_t ast = adesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
-                    const uint64_t bst = bdesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
-#pragma unroll
-                    for (int d = 0; d < OZ_S; ++d) {
-#pragma unroll
-                        for (int s = 0; s <= d; ++s) {
-                            mma_i8(dacc + (uint32_t)(d * OZ_HB), ast + (uint64_t)((s * OZ_HA * OZ_BK) >> 4),
-                                   bst + (uint64_t)(((d - s) * OZ_HB * OZ_BK) >> 4), idesc,
-                                   (ks > 0 || s > 0) ? 1u : 0u);
-                        }
+                const uint32_t dacc = tmem + (uint32_t)(buf * OZ_ACC_STRIDE);
+                for (int ks = 0; ks < kseg && ok; ++ks, ++it) {
+                    const int st = it % OZ_NST;
+                    const uint32_t ph = (uint32_t)(it / OZ_NST) & 1u;
+                    if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[st], ph))) {
+                        ok = false;
+                        break;
                     }
-                    umma_commit(&sm.empty[st]);
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    if (lane == 0) {
+                        // descriptors of this stage: the start-address field (16-byte units) advanced
+                        const uint64_t ast = adesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
+                        const uint64_t bst = bdesc0 + (uint64_t)((st * OZ_STAGE) >> 4);
+#pragma unroll
+                        for (int d = 0; d < OZ_S; ++d) {
+#pragma unroll
+                            for (int s = 0; s <= d; ++s) {
+                                mma_i8(dacc + (uint32_t)(d * OZ_HB), ast + (uint64_t)((s * OZ_HA * OZ_BK) >> 4),
+                                       bst + (uint64_t)(((d - s) * OZ_HB * OZ_BK) >> 4), idesc,
+                                       (ks > 0 || s > 0) ? 1u : 0u);
+                            }
+                        }
+                        umma_commit(&sm.empty[st]);
+                    }
+                    __syncwarp();
                 }
+                if (!ok) break;
+                if (lane == 0) umma_commit(&sm.acc_full[buf]);
                 __syncwarp();
             }
-            if (!ok) {
-                sm.abort = 1;
-                break;
-            }
-            if (lane == 0) umma_commit(&sm.acc_full[buf]);
-            __syncwarp();
         }
+        if (!ok) sm.abort = 1;
         // all MMAs of this CTA finished before the tensor memory is released
         if (lane == 0) umma_commit(&sm.drain);
         __syncwarp();
@@ -281,10 +283,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
         // ---------------- epilogue (warps 2..13): lane quadrant warp % 4, column third (warp - 2) / 4 ----------------
         const int q = warp & 3;
         const int cbeg = ((warp - 2) >> 2) * OZ_EPI_COLS;
-        int tl_i = 0;
+        int tl_i = 0;   // accumulator uses (segments), as the MMA warp counts them
         int4 tl_n = (blockIdx.x < ntiles) ? tiles[blockIdx.x] : make_int4(0, 0, 0, 0);
         OzProblem pb_n = probs[tl_n.x];
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl_i) {
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             if (vload(&sm.abort)) break;
             const int4 tl = tl_n;
             const OzProblem pb = pb_n;   // by value: stores to C cannot alias it
@@ -292,49 +295,62 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
                 tl_n = tiles[t + gridDim.x];
                 pb_n = probs[tl_n.x];
             }
-            const int buf = tl_i & 1;
-            const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
-            if (!mbar_wait(&sm.acc_full[buf], aph)) {
-                sm.abort = 1;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int nseg = tl.w >> 16;
             const int row = tl.y * OZ_HA + q * 32 + lane;
             const bool rok = row < pb.M;
-            // row scale with the combined weight 2^-46 of S below folded in
-            const double sa = rok ? pow2(pb.ea[row] - 46) : 0.0;
-            // column scales of this warp's columns, one per lane, shared by shuffle
             const int colw = tl.z * OZ_HB + cbeg + lane;
-            const double sbl = (lane < OZ_EPI_COLS && colw < pb.N) ? pow2(__ldg(pb.eb + colw)) : 0.0;
-            double* crow = pb.C + (long)row * pb.c_m;
-            const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * OZ_ACC_STRIDE);
-#pragma unroll 1
-            for (int c0 = cbeg; c0 < cbeg + OZ_EPI_COLS; c0 += 8) {
-                uint32_t v[OZ_S][8];
+            const bool cok = lane < OZ_EPI_COLS && colw < pb.N;
+            double part[OZ_EPI_COLS];   // FP64 sum over the segments
 #pragma unroll
-                for (int d = 0; d < OZ_S; ++d)
-                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                                 : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]),
-                                   "=r"(v[d][5]), "=r"(v[d][6]), "=r"(v[d][7])
-                                 : "r"(tbase + (uint32_t)(d * OZ_HB + c0)));
-                asm volatile("tcgen05.wait::ld.sync.aligned;");
-                const int cb = tl.z * OZ_HB + c0;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    // S = sum_d D_d 2^(8(4-d)) is exact in int64 (|S| < 2^59 for K <= 20000);
-                    // the value is S 2^-46 2^(ea + eb), rounded once
-                    long long S = (long long)(int)v[0][j];
-#pragma unroll
-                    for (int d = 1; d < OZ_S; ++d) S = S * 256 + (long long)(int)v[d][j];
-                    const double sb = __shfl_sync(0xffffffffu, sbl, c0 - cbeg + j);
-                    const int col = cb + j;
-                    if (rok && col < pb.N) crow[(long)col * pb.c_n] = (__ll2double_rn(S) * sa) * sb;
+            for (int j = 0; j < OZ_EPI_COLS; ++j) part[j] = 0.0;
+            for (int sg = 0; sg < nseg; ++sg, ++tl_i) {
+                const int buf = tl_i & 1;
+                const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+                if (!mbar_wait(&sm.acc_full[buf], aph)) {
+                    ok = false;
+                    break;
                 }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                // row scale with the combined weight 2^-46 of S below folded in; the
+                // column scales of this warp's columns, one per lane, shared by shuffle
+                const double sa = rok ? pow2(pb.ea[sg * pb.ea_seg + row] - 46) : 0.0;
+                const double sbl = cok ? pow2(__ldg(pb.eb + sg * pb.eb_seg + colw)) : 0.0;
+                const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * OZ_ACC_STRIDE);
+#pragma unroll
+                for (int c8 = 0; c8 < OZ_EPI_COLS; c8 += 8) {
+                    uint32_t v[OZ_S][8];
+#pragma unroll
+                    for (int d = 0; d < OZ_S; ++d)
+                        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                                     : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]),
+                                       "=r"(v[d][5]), "=r"(v[d][6]), "=r"(v[d][7])
+                                     : "r"(tbase + (uint32_t)(d * OZ_HB + cbeg + c8)));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        // S = sum_d D_d 2^(8(4-d)) is exact in int64 (|S| < 2^59 for K <= 20000);
+                        // the value is S 2^-46 2^(ea + eb), rounded once per segment
+                        long long S = (long long)(int)v[0][j];
+#pragma unroll
+                        for (int d = 1; d < OZ_S; ++d) S = S * 256 + (long long)(int)v[d][j];
+                        const double sb = __shfl_sync(0xffffffffu, sbl, c8 + j);
+                        part[c8 + j] += (__ll2double_rn(S) * sa) * sb;
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.acc_empty[buf]);
             }
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&sm.acc_empty[buf]);
+            if (!ok) break;
+            if (rok) {
+                double* crow = pb.C + (long)row * pb.c_m;
+                const int cb = tl.z * OZ_HB + cbeg;
+#pragma unroll
+                for (int j = 0; j < OZ_EPI_COLS; ++j)
+                    if (cb + j < pb.N) crow[(long)(cb + j) * pb.c_n] = part[j];
+            }
         }
+        if (!ok) sm.abort = 1;
     }
 
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -382,6 +398,7 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __re
     }
     const int rt = r0 / jb.H, rin = r0 - rt * jb.H;
     const long blk = (long)OZ_S * jb.H * OZ_BK;
+    const int kstride = jb.kstride > 0 ? jb.kstride : jb.nks;
     for (int ks = 0; ks < jb.nks; ++ks) {
         const int k0 = ks * OZ_BK;
         __syncthreads();   // ex_s ready / previous tile consumed
@@ -408,7 +425,7 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __re
         __syncthreads();
         if (tid < OZ_S * 32) {
             const int s = tid >> 5, kc = (tid >> 4) & 1, row = tid & 15;
-            int8_t* dst = jb.out + ((long)rt * jb.nks + ks) * blk + (long)s * jb.H * OZ_BK + (long)kc * jb.H * 16 +
+            int8_t* dst = jb.out + ((long)rt * kstride + jb.ks0 + ks) * blk + (long)s * jb.H * OZ_BK + (long)kc * jb.H * 16 +
                           (long)(rin + row) * 16;
             *reinterpret_cast<int4*>(dst) = *reinterpret_cast<const int4*>(&dig[s][kc][row][0]);
         }
@@ -447,8 +464,9 @@ void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles
     ++c.launches;
 }
 
-// Tile list (problem, m-tile, n-tile, K-steps), longest K first so that the
-// ragged products finish together; products with K = 0 get no tiles.
+// Tile list (problem, m-tile, n-tile, K-steps | segments << 16), longest K
+// first so that the ragged products finish together; products with K = 0 get
+// no tiles.
 std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
     std::vector<int> order(probs.size());
     for (size_t p = 0; p < probs.size(); ++p) order[p] = (int)p;
@@ -462,7 +480,7 @@ std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
                 t.push_back(p);
                 t.push_back(mt);
                 t.push_back(nt);
-                t.push_back(q.nks);
+                t.push_back(q.nks | ((q.nseg > 0 ? q.nseg : 1) << 16));
             }
     }
     return t;
@@ -504,7 +522,7 @@ __global__ void oz_static_prepare_kernel(OzProblem pr, OzSplitJob ja, OzSplitJob
         djobs[1] = jb;
         *status = 0;
     }
-    if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, pr.nks);
+    if (i < ntm * ntn) tiles[i] = make_int4(0, i / ntn, i % ntn, pr.nks | (1 << 16));
 }
 
 }  // namespace ra

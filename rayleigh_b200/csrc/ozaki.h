@@ -25,6 +25,11 @@ constexpr int OZ_BBLK = OZ_S * OZ_HB * OZ_BK;   // same for B
 // One product C = A B of a batch: A as digit row tiles (rows = output rows,
 // exponents ea[M]), B as digit row tiles of B^T (rows = output columns,
 // exponents eb[N]); C(i, j) is written to C[i*c_m + j*c_n] in FP64.
+// K may be cut into nseg equal segments of nks/nseg K-steps, each with its
+// own exponents (ea + s*ea_seg, eb + s*eb_seg): their products are
+// accumulated separately and summed in FP64, so that operands whose K range
+// joins blocks of very different size keep each block's relative accuracy.
+// nseg = 0 means one segment.
 struct OzProblem {
     const int8_t* A;
     const int8_t* B;
@@ -34,17 +39,23 @@ struct OzProblem {
     int M, N, nks;
     double* C;
     long c_m, c_n;
+    int nseg;
+    long ea_seg, eb_seg;
 };
 
 // One split job: rows i < R of X (element (i, k) at X[i*sr + k*sk], k < K)
 // become tiled digit rows with tile height H (nrt row tiles, nks K-steps;
 // zero digits past R and K) and exponents e[i] (0 for an all-zero row).
+// The job's K-steps land at K-step ks0 + ks of row tiles that hold kstride
+// K-steps each (kstride = 0: the job's own nks), so that the segments of one
+// operand can be split separately.
 struct OzSplitJob {
     const double* X;
     long sr, sk;
     int R, K, H, nrt, nks;
     int8_t* out;
     int* e;
+    int kstride, ks0;
 };
 
 void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows);

@@ -31,65 +31,90 @@ __device__ __forceinline__ int ell_of_lm(long lm) {
 // ---------------------------------------------------------------------------
 // Chebyshev synthesis of the 12 grid outputs (W W' W'' W''' P P' T T' T'' Z Z' Z'')
 // ---------------------------------------------------------------------------
-struct ChebOut { int var, d; };
-__constant__ ChebOut kChebOut[NG] = {{0, 0}, {0, 1}, {0, 2}, {0, 3}, {1, 0}, {1, 1},
-                                     {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {3, 2}};
 
-__global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const double* __restrict__ D,
+// One CTA per (field, 64-column tile): the tile's retained Chebyshev
+// coefficients are staged in shared memory once, split by parity, and every
+// derivative order of the field is synthesised from them.  D(n_r - 1 - r, k) =
+// (-1)^(k+d) D(r, k), so rows r < n_r/2 give both halves of the grid:
+//   g(r) = E + O,  g(n_r - 1 - r) = (-1)^d (E - O),
+// E / O the products over even / odd k.  Dpar[d][par][r][k'] = D_d(r, 2k' + par).
+struct ChebField { int o0, nd, var; };
+__constant__ ChebField kChebField[4] = {{G_W0, 4, 0}, {G_P0, 2, 1}, {G_T0, 3, 2}, {G_Z0, 3, 3}};
+
+__global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const double* __restrict__ Dpar,
                                                                       const double* __restrict__ sol_wpt,
                                                                       const double* __restrict__ sol_z,
                                                                       double* __restrict__ g, int nr, int kc,
                                                                       long ncols) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
-    const int o = blockIdx.z;
-    const int var = kChebOut[o].var, d = kChebOut[o].d;
-    const int r0 = blockIdx.y * BM;
+    const int kh = (kc + 1) / 2;                                         // coefficients per parity
+    constexpr int BS = BN + 1;                                           // padded row: conflict-free staging
+    double* Bs = reinterpret_cast<double*>(smem_raw + sizeof(GemmSmem));   // [par][kh][BS]
+    const ChebField cf = kChebField[blockIdx.y];
     const long c0 = (long)blockIdx.x * BN;
     const int nr2 = nr / 2;
-    const int ke = (kc + 1) / 2, ko = kc / 2;
-    const double* Dd = D + (long)d * nr * nr;
     const double* src;
     long cstride;
-    if (var < 3) {
-        src = sol_wpt + (long)var * nr;
+    if (cf.var < 3) {
+        src = sol_wpt + (long)cf.var * nr;
         cstride = 3L * nr;
     } else {
         src = sol_z;
         cstride = nr;
     }
-    Acc ae, ao;
-    ae.zero();
-    ao.zero();
-    for (int par = 0; par < 2; ++par) {
-        const int kk = par ? ko : ke;
-        auto fa = [&](int k, int x) -> double {
-            const int r = r0 + x;
-            return (k < kk && r < nr2) ? __ldg(Dd + (long)r * nr + 2 * k + par) : 0.0;
-        };
-        auto fb = [&](int k, int y) -> double {
-            const long col = c0 + y;
-            return (k < kk && col < ncols) ? __ldg(src + col * cstride + 2 * k + par) : 0.0;
-        };
-        gemm_tile<false, false>(par ? ao : ae, fa, fb, kk, sm);
-    }
-    const double sgn = (d & 1) ? -1.0 : 1.0;
-    double* out = g + (long)o * ncols * nr;
-    acc_foreach2(ae, ao, [&](int x, int y, double e, double od) {
-        const int r = r0 + x;
+    // stage the coefficients (k < kc) of the 64 columns, coalesced along k
+    for (int e = threadIdx.x; e < BN * kc; e += GEMM_THREADS) {
+        const int y = e / kc, k = e - y * kc;
         const long col = c0 + y;
-        if (r < nr2 && col < ncols) {
-            out[col * nr + r] = e + od;
-            out[col * nr + (nr - 1 - r)] = sgn * (e - od);
+        Bs[((k & 1) * kh + (k >> 1)) * BS + y] = (col < ncols) ? __ldg(src + col * cstride + k) : 0.0;
+    }
+    if (kc & 1)   // the odd-parity plane has one coefficient fewer
+        for (int y = threadIdx.x; y < BN; y += GEMM_THREADS) Bs[(kh + kh - 1) * BS + y] = 0.0;
+    __syncthreads();
+    for (int dd = 0; dd < cf.nd; ++dd) {
+        const int o = cf.o0 + dd;
+        const double sgn = (dd & 1) ? -1.0 : 1.0;
+        double* out = g + (long)o * ncols * nr;
+        for (int r0 = 0; r0 < nr2; r0 += BM) {
+            Acc ae, ao;
+            ae.zero();
+            ao.zero();
+#pragma unroll 1
+            for (int par = 0; par < 2; ++par) {
+                const double* Dp = Dpar + (((long)dd * 2 + par) * nr2) * kh;
+                const double* Bp = Bs + (long)par * kh * BS;
+                auto fa = [&](int k, int x) -> double {
+                    const int r = r0 + x;
+                    return (k < kh && r < nr2) ? __ldg(Dp + (long)r * kh + k) : 0.0;
+                };
+                auto fb = [&](int k, int y) -> double { return (k < kh) ? Bp[k * BS + y] : 0.0; };
+                gemm_tile<false, true>(par ? ao : ae, fa, fb, kh, sm);
+            }
+            acc_foreach2(ae, ao, [&](int x, int y, double e, double od) {
+                const int r = r0 + x;
+                const long col = c0 + y;
+                if (r < nr2 && col < ncols) {
+                    out[col * nr + r] = e + od;
+                    out[col * nr + (nr - 1 - r)] = sgn * (e - od);
+                }
+            });
         }
-    });
+    }
 }
 
 void launch_cheb_synthesis(Ctx& c) {
     const long ncols = 2 * c.d.nlm;
-    dim3 grid((unsigned)((ncols + BN - 1) / BN), (c.d.nr / 2 + BM - 1) / BM, NG);
-    cheb_synthesis_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(c.d_D, c.d_sol_wpt, c.d_sol_z, c.d_g,
-                                                                               c.d.nr, c.d.kc, ncols);
+    const int kh = (c.d.kc + 1) / 2;
+    const size_t smem = sizeof(GemmSmem) + (size_t)2 * kh * (BN + 1) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    dim3 grid((unsigned)((ncols + BN - 1) / BN), 4);
+    cheb_synthesis_kernel<<<grid, GEMM_THREADS, smem, c.stream>>>(c.d_Dpar, c.d_sol_wpt, c.d_sol_z, c.d_g, c.d.nr,
+                                                                   c.d.kc, ncols);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }

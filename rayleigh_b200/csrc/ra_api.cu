@@ -396,6 +396,21 @@ static void setup(Ctx& c) {
     RA_CUDA(cudaMemsetAsync(c.d_sol_wpt, 0, (size_t)nlm * 2 * 3 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_sol_z, 0, (size_t)nlm * 2 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_D, c.cheb_D.data(), c.cheb_D.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    {
+        // parity planes of the synthesis matrices: Dpar[d][par][r][k'] = D_d(r, 2k' + par), r < nr/2, 2k'+par < kc
+        const int nr2 = nr / 2, kh = (d.kc + 1) / 2;
+        std::vector<double> dp((size_t)4 * 2 * nr2 * kh, 0.0);
+        for (int dd = 0; dd < 4; ++dd)
+            for (int par = 0; par < 2; ++par)
+                for (int r = 0; r < nr2; ++r)
+                    for (int k = 0; k < kh; ++k)
+                        if (2 * k + par < d.kc)
+                            dp[(((size_t)dd * 2 + par) * nr2 + r) * kh + k] =
+                                c.cheb_D[((size_t)dd * nr + r) * nr + 2 * k + par];
+        dalloc(c.d_Dpar, dp.size());
+        RA_CUDA(cudaMemcpyAsync(c.d_Dpar, dp.data(), dp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    }
     RA_CUDA(cudaMemcpyAsync(c.d_radial, rp.data(), rp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_costh, trig.data(), trig.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_twid, twid.data(), twid.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
@@ -417,7 +432,7 @@ static void release(Ctx& c) {
     mixed_release(c);
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
-    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_Awpt, c.d_Az,
+    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_Awpt, c.d_Az,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
                       c.d_p2a, c.d_p2b, c.d_s2b};
     for (double* b : bufs)

@@ -99,6 +99,7 @@ struct Ctx {
     // device constants
     double *d_Ptab = nullptr, *d_iPtab = nullptr;     // [row][nth2]
     double *d_D = nullptr;                            // [4][nr][nr]
+    double *d_Dpar = nullptr;                         // [4][2][nr/2][(kc+1)/2] parity planes of D, r < nr/2
     double *d_coef = nullptr;                         // [L][NSLOT][nr]
     double *d_radial = nullptr;                       // packed radial profiles (see kRadial*)
     double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot

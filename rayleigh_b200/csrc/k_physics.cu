@@ -21,6 +21,8 @@
 // (N = n_theta = 2^a 3^b), Stockham autosort, radix 8/4/2/3, in shared memory;
 // unnormalised like FFTW (the normalisation lives in the Legendre tables).
 #include <cmath>
+#include <vector>
+#include <algorithm>
 
 #include <cooperative_groups.h>
 
@@ -44,6 +46,19 @@ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -
 // exp(sign * 2 pi i e / N) from wr[k] = exp(2 pi i k / (2N)), k < N
 __device__ __forceinline__ double2 twiddle(const double2* wr, int N, int e, int sign) {
     double2 w = (2 * e < N) ? wr[2 * e] : make_double2(-wr[2 * e - N].x, -wr[2 * e - N].y);
+    if (sign < 0) w.y = -w.y;
+    return w;
+}
+
+// The same from a table in global memory (read-only path).
+__device__ __forceinline__ double2 twiddle_g(const double2* __restrict__ wr, int N, int e, int sign) {
+    double2 w;
+    if (2 * e < N) {
+        w = __ldg(wr + 2 * e);
+    } else {
+        const double2 v = __ldg(wr + 2 * e - N);
+        w = make_double2(-v.x, -v.y);
+    }
     if (sign < 0) w.y = -w.y;
     return w;
 }
@@ -157,75 +172,13 @@ __device__ __forceinline__ int SW(int i) { return i ^ ((i >> 3) & 7); }
 // field's swizzled indices stay inside the field whatever buffer it sits in.
 __host__ __device__ constexpr int fstride(int n) { return (n + 63) / 64 * 64; }
 
-// Offsets of the per-pass twiddle tables tw[(r-1) P + k] = exp(2 pi i r k STRIDE / N).
-__host__ __device__ constexpr int tw_off(int n, int ps) {
-    int o = 0;
-    for (int j = 0; j < ps; ++j) o += (radix_at(n, j) - 1) * pprod(n, j);
-    return o;
-}
-__host__ __device__ constexpr int tw_size(int n) { return tw_off(n, npass_of(n)); }
-
-// Builds the per-pass tables from the global table wr[k] = exp(2 pi i k / 2N).
-template <int N, int NT, int PS = 0>
-__device__ __forceinline__ void build_twiddles(double2* tw, const double2* __restrict__ wrg) {
-    if constexpr (PS < npass_of(N)) {
-        constexpr int R = radix_at(N, PS), P = pprod(N, PS), STRIDE = N / (P * R);
-        for (int idx = threadIdx.x; idx < (R - 1) * P; idx += NT) {
-            const int r = idx / P + 1, k = idx - (r - 1) * P;
-            const int e = (r * k * STRIDE) % N;
-            tw[tw_off(N, PS) + idx] = (2 * e < N) ? wrg[2 * e] : make_double2(-wrg[2 * e - N].x, -wrg[2 * e - N].y);
-        }
-        build_twiddles<N, NT, PS + 1>(tw, wrg);
-    }
-}
-
-template <int N, int NB, int NT, int PS>
-__device__ __forceinline__ void fft_pass_t(const double2* __restrict__ src, double2* __restrict__ dst,
-                                           const double2* __restrict__ tw, int sign, int tid) {
-    constexpr int R = radix_at(N, PS);
-    constexpr int P = pprod(N, PS);
-    constexpr int T = N / R;
-    constexpr int TO = tw_off(N, PS);
-#pragma unroll 1
-    for (int g = tid; g < T * NB; g += NT) {
-        const int b = g / T, bi = g - b * T;
-        const int base = b * fstride(N);
-        const int k = bi % P;
-        double2 u[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) u[r] = src[SW(base + bi + r * T)];
-        if (P > 1) {
-#pragma unroll
-            for (int r = 1; r < R; ++r) {
-                double2 w = tw[TO + (r - 1) * P + k];
-                if (sign < 0) w.y = -w.y;
-                u[r] = cmul(u[r], w);
-            }
-        }
-        dft_small(R, u, sign);
-        const int j = (bi - k) * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) dst[SW(base + j + r * P)] = u[r];
-    }
-}
-
-template <int N, int NB, int NT, int PS = 0>
-__device__ __forceinline__ double2* fft_run_t(double2* a, double2* b, const double2* tw, int sign, int tid) {
-    if constexpr (PS < npass_of(N)) {
-        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign, tid);
-        __syncthreads();
-        return fft_run_t<N, NB, NT, PS + 1>(b, a, tw, sign, tid);
-    } else {
-        return a;
-    }
-}
-
 struct PhysParams {
     const double* p2a;
     double* p2b;
     const double* radial;   // packed radial profiles
     const double* trig;     // [4][nth]: cos, sin, csc, cot
     const double2* wr;      // [nth] exp(2 pi i k / n_phi)
+    const double2* twp;     // per-pass FFT twiddles (tw_table_off / pass_twiddles)
     unsigned long long* cfl;
     int L, nth, nr, ncola, ncolb;
     double coriolis;
@@ -236,28 +189,88 @@ struct PhysParams {
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
 // 2-CTA cluster that folds its spectra through distributed shared memory.
 constexpr int ROW_THREADS = 256;
-constexpr int FB = 2;   // fields per batched FFT
+constexpr int FB = 4;   // fields per batched FFT
 
-// Shared memory of a row CTA (double2 units): two FFT ping-pong buffers of FB
-// fields, the four nonlinear outputs (W, P, T, Z; each thread owns its points),
-// the per-pass twiddle tables.
+// Shared memory of a row CTA (double2 units): one in-place FFT buffer of FB
+// fields and the four nonlinear outputs (W, P, T, Z; each thread owns its
+// points; the r2c runs in place on them).
 template <int N>
 struct RowSmem {
     static constexpr int FS = fstride(N);
-    static constexpr int A = 0, B = FB * FS, ACC = 2 * FB * FS, TW = ACC + 4 * FS;
-    static constexpr int SIZE = TW + tw_size(N);
+    static constexpr int BUF = 0, ACC = FB * FS;
+    static constexpr int SIZE = ACC + 4 * FS;
 };
 
-// Runs the Stockham passes PS .. PE-1 (ping-pong a -> b -> a ...); returns the
-// buffer holding the result.
-template <int N, int NB, int NT, int PS, int PE>
-__device__ __forceinline__ double2* fft_range(double2* a, double2* b, const double2* tw, int sign, int tid) {
-    if constexpr (PS < PE) {
-        fft_pass_t<N, NB, NT, PS>(a, b, tw, sign, tid);
+// In-place mixed-radix FFT passes (field f at f*FS, swizzled).  Pass s:
+// sub-transform length LS = N / (R_0 ... R_{s-1}), radix R = R_s, stride
+// SS = LS / R; butterfly (b, j) takes the elements b*LS + j + m*SS.
+// Decimation in frequency (c2r, sign +1): DFT_R, then twiddle w_LS^{jk}; after
+// all passes position p holds the output of a fixed digit-reversed index.
+// Decimation in time (r2c, sign -1, passes in reverse order): twiddle
+// w_LS^{-jm}, then DFT_R; it takes the digit-reversed arrangement back to
+// natural order.  The nonlinear terms are pointwise in phi, so the physical
+// points may stay digit-reversed between the two.
+// The twiddles of pass s are the table entries tw[off(s) + (k-1)*SS + j] =
+// exp(2 pi i j k / LS), k = 1 .. R-1, j < SS (conjugated for sign -1).
+__host__ __device__ constexpr int ip_ls(int n, int ps) { return n / pprod(n, ps); }
+__host__ __device__ constexpr int ip_tw_off(int n, int ps) {
+    int o = 0;
+    for (int j = 0; j < ps; ++j) o += (radix_at(n, j) - 1) * (ip_ls(n, j) / radix_at(n, j));
+    return o;
+}
+__host__ __device__ constexpr int ip_tw_size(int n) { return ip_tw_off(n, npass_of(n)); }
+
+template <int N, int NB, int NT, int PS, bool DIT>
+__device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const double2* __restrict__ twp, int sign,
+                                            int tid) {
+    constexpr int R = radix_at(N, PS), LS = ip_ls(N, PS), SS = LS / R, T = N / R, FS = fstride(N);
+    const double2* __restrict__ tw = twp + ip_tw_off(N, PS);
+    auto butterfly = [&](int g) {
+        const int f = g / T, bi = g - f * T;
+        const int b = bi / SS, j = bi - b * SS;
+        const int base = f * FS + b * LS + j;
+        double2 u[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) u[m] = buf[SW(base + m * SS)];
+        if (SS > 1 && DIT) {
+#pragma unroll
+            for (int m = 1; m < R; ++m) {
+                double2 w = __ldg(tw + (m - 1) * SS + j);
+                w.y = -w.y;
+                u[m] = cmul(u[m], w);
+            }
+        }
+        dft_small(R, u, sign);
+        if (SS > 1 && !DIT) {
+#pragma unroll
+            for (int k = 1; k < R; ++k) u[k] = cmul(u[k], __ldg(tw + (k - 1) * SS + j));
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) buf[SW(base + m * SS)] = u[m];
+    };
+    // two independent butterflies per iteration for instruction-level parallelism
+#pragma unroll 1
+    for (int g = tid; g < T * NB; g += 2 * NT) {
+        butterfly(g);
+        if (g + NT < T * NB) butterfly(g + NT);
+    }
+}
+
+template <int N, int NB, int NT, int PS = 0>
+__device__ __forceinline__ void fft_dif(double2* buf, const double2* twp, int tid) {
+    if constexpr (PS < npass_of(N)) {
+        fft_pass_ip<N, NB, NT, PS, false>(buf, twp, +1, tid);
         __syncthreads();
-        return fft_range<N, NB, NT, PS + 1, PE>(b, a, tw, sign, tid);
-    } else {
-        return a;
+        fft_dif<N, NB, NT, PS + 1>(buf, twp, tid);
+    }
+}
+
+template <int N, int NB, int NT, int PS = npass_of(N) - 1>
+__device__ __forceinline__ void fft_dit(double2* buf, const double2* twp, int tid) {
+    if constexpr (PS >= 0) {
+        fft_pass_ip<N, NB, NT, PS, true>(buf, twp, -1, tid);
+        __syncthreads();
+        fft_dit<N, NB, NT, PS - 1>(buf, twp, tid);
     }
 }
 
@@ -285,113 +298,67 @@ __device__ __forceinline__ double2 zform(double2 xk, double2 xn, double2 wk) {
     return make_double2(e.x - wd.y, e.y + wd.x);
 }
 
-// Whether the last Stockham pass leaves, per thread t, the outputs n = t + q*ROW_THREADS
-// of every field (then it is run straight into registers).
-template <int N>
-__host__ __device__ constexpr bool last_pass_in_regs() {
-    return N / radix_at(N, npass_of(N) - 1) == ROW_THREADS;
+// a[b] for a runtime b without a local-memory array
+template <class T, int NB>
+__device__ __forceinline__ T pick(const T (&a)[NB], int b) {
+    T v = a[0];
+#pragma unroll
+    for (int i = 1; i < NB; ++i)
+        if (b == i) v = a[i];
+    return v;
 }
 
-// Forms the half-length complex FFT input Z_k (zform) of FB fields of this row
-// in buffer A straight from the spectra in p2a (spec_value): one work item is
-// the pair (k, N-k), whose two Z values need the same two spectrum values.
-template <int N>
-__device__ __forceinline__ void c2r_stage(const PhysParams& P, const double* __restrict__ rowbase, int h, int f0,
-                                          bool d0, int f1, bool d1, double2* bA, int t) {
+// c2r of NB fields of this row (fields fo[b], d/dphi where dp[b]): the input
+// Z is formed straight from the spectrum loads (one (k, N-k) pair per work
+// item), then the DIF passes.  On return y[b][q] holds the physical pair
+// (y[2n], y[2n+1]) of field b at the buffer position t + q*ROW_THREADS.
+template <int N, int NB, int ZPT>
+__device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h,
+                                        const int (&fo)[NB], const bool (&dp)[NB], double2* sm, int t,
+                                        double2 (&y)[FB][ZPT]) {
     constexpr int FS = fstride(N);
     constexpr int NI = N / 2 + 1;                                   // k = 0 .. N/2
-    constexpr int QI = (FB * NI + ROW_THREADS - 1) / ROW_THREADS;   // items per thread
+    constexpr int QI = (NB * NI + ROW_THREADS - 1) / ROW_THREADS;   // items per thread
+    double2* buf = sm + RowSmem<N>::BUF;
     const int L = P.L;
     const long ostride = (long)P.ncola;   // E -> O within p2a[theta_h][m][par][col]
     const long mstride = 2L * P.ncola;
-    double2 xk[QI], xn[QI];
+    __syncthreads();   // the buffer is free (previous batch read)
+    constexpr int QC = 3;   // items whose loads are in flight together
+#pragma unroll 1
+    for (int q0 = 0; q0 < QI; q0 += QC) {
+        double2 xk[QC], xn[QC];
 #pragma unroll
-    for (int q = 0; q < QI; ++q) {
-        const int g = t + q * ROW_THREADS;
-        xk[q] = xn[q] = make_double2(0.0, 0.0);
-        if (g < FB * NI) {
-            const int b = g / NI, k = g - b * NI;
-            const double* base = rowbase + (long)(b ? f1 : f0) * P.nr * 2;
-            const bool dp = b ? d1 : d0;
-            xk[q] = spec_value(base, mstride, ostride, k, L, h, dp);
-            xn[q] = spec_value(base, mstride, ostride, N - k, L, h, dp);   // N - k >= L for k = 0
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < QI; ++q) {
-        const int g = t + q * ROW_THREADS;
-        if (g < FB * NI) {
-            const int b = g / NI, k = g - b * NI;
-            bA[SW(b * FS + k)] = zform(xk[q], xn[q], __ldg(P.wr + k));
-            if (k != 0 && 2 * k != N) bA[SW(b * FS + N - k)] = zform(xn[q], xk[q], __ldg(P.wr + N - k));
-        }
-    }
-    __syncthreads();
-}
-
-// c2r of FB fields of this row: y[b][q] = (y[2n], y[2n+1]) of field b at n = t + q*ROW_THREADS.
-template <int N, int ZPT>
-__device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h, int f0,
-                                        bool d0, int f1, bool d1, double2* sm, const double2* tw, int t,
-                                        double2 (&y)[FB][ZPT]) {
-    constexpr int FS = fstride(N), NP = npass_of(N);
-    double2* bA = sm + RowSmem<N>::A;
-    double2* bB = sm + RowSmem<N>::B;
-    c2r_stage<N>(P, rowbase, h, f0, d0, f1, d1, bA, t);
-    if constexpr (last_pass_in_regs<N>()) {
-        const double2* src = fft_range<N, FB, ROW_THREADS, 0, NP - 1>(bA, bB, tw, +1, t);
-        constexpr int PS = NP - 1, R = radix_at(N, PS), PP = pprod(N, PS), TO = tw_off(N, PS);
-        static_assert(R == ZPT, "last radix must equal the points per thread");
-#pragma unroll
-        for (int b = 0; b < FB; ++b) {
-            double2 u[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) u[r] = src[SW(b * FS + t + r * ROW_THREADS)];
-            if (PP > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], tw[TO + (r - 1) * PP + t]);
+        for (int qq = 0; qq < QC; ++qq) {
+            const int g = t + (q0 + qq) * ROW_THREADS;
+            xk[qq] = xn[qq] = make_double2(0.0, 0.0);
+            if (q0 + qq < QI && g < NB * NI) {
+                const int b = g / NI, k = g - b * NI;
+                const double* base = rowbase + (long)pick(fo, b) * P.nr * 2;
+                const bool d = pick(dp, b);
+                xk[qq] = spec_value(base, mstride, ostride, k, L, h, d);
+                xn[qq] = spec_value(base, mstride, ostride, N - k, L, h, d);   // N - k >= L for k = 0
             }
-            dft_small(R, u, +1);
-#pragma unroll
-            for (int r = 0; r < R; ++r) y[b][r] = u[r];
         }
-    } else {
-        const double2* res = fft_range<N, FB, ROW_THREADS, 0, NP>(bA, bB, tw, +1, t);
 #pragma unroll
-        for (int b = 0; b < FB; ++b)
-#pragma unroll
-            for (int q = 0; q < ZPT; ++q) {
-                const int n = t + q * ROW_THREADS;
-                y[b][q] = (n < N) ? res[SW(b * FS + n)] : make_double2(0.0, 0.0);
+        for (int qq = 0; qq < QC; ++qq) {
+            const int g = t + (q0 + qq) * ROW_THREADS;
+            if (q0 + qq < QI && g < NB * NI) {
+                const int b = g / NI, k = g - b * NI;
+                buf[SW(b * FS + k)] = zform(xk[qq], xn[qq], __ldg(P.wr + k));
+                if (k != 0 && 2 * k != N) buf[SW(b * FS + N - k)] = zform(xn[qq], xk[qq], __ldg(P.wr + N - k));
             }
-    }
-}
-
-// r2c of two of the accumulated outputs (acc fields a0, a0+1): Z = FFT(y[2n] + i y[2n+1]),
-// X_k = e - i conj(w^k) d with e, d the half sums/differences of Z_k, conj Z_{N-k};
-// X_k (k < L) is written back over the two acc fields.
-template <int N>
-__device__ __forceinline__ void row_r2c_pair(const PhysParams& P, int a0, double2* sm, const double2* tw, int t) {
-    constexpr int FS = fstride(N);
-    double2* acc = sm + RowSmem<N>::ACC + a0 * FS;
-    double2* bA = sm + RowSmem<N>::A;
-    double2* bB = sm + RowSmem<N>::B;
-    fft_pass_t<N, FB, ROW_THREADS, 0>(acc, bA, tw, -1, t);
-    __syncthreads();
-    const double2* Z = fft_run_t<N, FB, ROW_THREADS, 1>(bA, bB, tw, -1, t);
-    const int L = P.L;
-    for (int g = t; g < FB * L; g += ROW_THREADS) {
-        const int f = g / L, k = g - f * L;
-        const double2 zk = Z[SW(f * FS + k)];
-        const double2 zn = cconj(Z[SW(f * FS + (N - k) % N)]);
-        const double2 e = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y + zn.y));
-        const double2 d = make_double2(0.5 * (zk.x - zn.x), 0.5 * (zk.y - zn.y));
-        const double2 wd = cmul(cconj(__ldg(P.wr + k)), d);
-        double2 Xk = make_double2(e.x + wd.y, e.y - wd.x);
-        if (k == 0) Xk.y = 0.0;
-        acc[SW(f * FS + k)] = Xk;
+        }
     }
     __syncthreads();
+    fft_dif<N, NB, ROW_THREADS>(buf, P.twp, t);
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            const int n = t + q * ROW_THREADS;
+            y[b][q] = (n < N) ? buf[SW(b * FS + n)] : make_double2(0.0, 0.0);
+        }
 }
 
 template <int NTH>
@@ -403,17 +370,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
-    double2* tw = sm + RowSmem<N>::TW;
     double2* acc = sm + RowSmem<N>::ACC;
     __shared__ double red[ROW_THREADS / 32];
     const int t = threadIdx.x;
     const int h = (int)cluster.block_rank();        // 0: theta (south half), 1: pi - theta
-    build_twiddles<N, ROW_THREADS>(tw, P.wr);
     const int nr = P.nr;
     const int pair = blockIdx.x >> 1;
     const int r = pair % nr;
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * 2;
     const double rad = P.radial[R_RADIUS * nr + r];
     const double orad = P.radial[R_OVER_R * nr + r];
     const double rho = P.radial[R_DENSITY * nr + r];
@@ -422,108 +388,94 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     const double cs = P.trig[th], sn = P.trig[N + th], csc = P.trig[2 * N + th], cot = P.trig[3 * N + th];
     const double cor = P.rotation ? P.coriolis : 0.0;
     const double c2r = csc * csc * orad;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * 2;
-    __syncthreads();
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
     double2 y[FB][ZPT];
     auto acc_at = [&](int f, int q) -> double2& { return acc[SW(f * FS + t + q * ROW_THREADS)]; };
     auto live = [&](int q) { return t + q * ROW_THREADS < N; };
-    // B1: v_r, v_theta
-    row_c2r<N, ZPT>(P, rowbase, h, A_VR, false, A_VT, false, sm, tw, t, y);
+    // B1: v_r, v_theta, v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
+    {
+        const int fo[4] = {A_VR, A_VT, A_VP, A_DVRDR};
+        const bool dp[4] = {false, false, false, false};
+        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
 #pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        vr[q] = y[0][q];
-        vt[q] = y[1][q];
-        vt[q].x *= csc;
-        vt[q].y *= csc;
-    }
-    __syncthreads();
-    // B2: v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
-    row_c2r<N, ZPT>(P, rowbase, h, A_VP, false, A_DVRDR, false, sm, tw, t, y);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        vp[q] = y[0][q];
-        vp[q].x *= csc;
-        vp[q].y *= csc;
-        const double2 x = y[1][q];
-        auto w0 = [&](double a, double b, double c, double xx) {
-            return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
-        };
-        auto p0 = [&](double a, double b, double c, double xx) {
-            return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
-        };
-        auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
-        if (live(q)) {
-            acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
-            acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
-            acc_at(2, q) = make_double2(0.0, 0.0);
-            acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+        for (int q = 0; q < ZPT; ++q) {
+            vr[q] = y[0][q];
+            vt[q] = y[1][q];
+            vp[q] = y[2][q];
+            vt[q].x *= csc;
+            vt[q].y *= csc;
+            vp[q].x *= csc;
+            vp[q].y *= csc;
+            const double2 x = y[3][q];
+            auto w0 = [&](double a, double b, double c, double xx) {
+                return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
+            };
+            auto p0 = [&](double a, double b, double c, double xx) {
+                return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
+            };
+            auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+            if (live(q)) {
+                acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                acc_at(2, q) = make_double2(0.0, 0.0);
+                acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+            }
         }
     }
-    __syncthreads();
-    // B3: dv_r/dtheta, dv_r/dphi
-    row_c2r<N, ZPT>(P, rowbase, h, A_DVRDT, false, A_VR, true, sm, tw, t, y);
+    // B2: dv_r/dtheta, dv_r/dphi, dv_theta/dr, dv_theta/dphi
+    {
+        const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
+        const bool dp[4] = {false, true, false, true};
+        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
 #pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        if (!live(q)) continue;
-        const double2 a = y[0][q], b = y[1][q];
-        double2& w = acc_at(0, q);
-        w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
-        w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
+        for (int q = 0; q < ZPT; ++q) {
+            if (!live(q)) continue;
+            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
+            double2& w = acc_at(0, q);
+            double2& pp = acc_at(1, q);
+            double2& z = acc_at(3, q);
+            w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
+            w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
+            pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
+            pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
+            z.x += vt[q].x * d.x * c2r;
+            z.y += vt[q].y * d.y * c2r;
+        }
     }
-    __syncthreads();
-    // B4: dv_theta/dr, dv_theta/dphi
-    row_c2r<N, ZPT>(P, rowbase, h, A_DVTDR, false, A_VT, true, sm, tw, t, y);
+    // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr
+    {
+        const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
+        const bool dp[4] = {false, true, false, false};
+        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
 #pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        if (!live(q)) continue;
-        const double2 c = y[0][q], d = y[1][q];
-        double2& pp = acc_at(1, q);
-        double2& z = acc_at(3, q);
-        pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
-        pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
-        z.x += vt[q].x * d.x * c2r;
-        z.y += vt[q].y * d.y * c2r;
+        for (int q = 0; q < ZPT; ++q) {
+            if (!live(q)) continue;
+            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
+            double2& pp = acc_at(1, q);
+            double2& tt = acc_at(2, q);
+            double2& z = acc_at(3, q);
+            z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
+            z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
+            pp.x += -vt[q].x * b.x * c2r;
+            pp.y += -vt[q].y * b.y * c2r;
+            tt.x += -vr[q].x * d.x;
+            tt.y += -vr[q].y * d.y;
+        }
     }
-    __syncthreads();
-    // B5: dv_phi/dr, dv_phi/dphi
-    row_c2r<N, ZPT>(P, rowbase, h, A_DVPDR, false, A_VP, true, sm, tw, t, y);
+    // B4: dT/dtheta, dT/dphi
+    {
+        const int fo[2] = {A_DTDT, A_T};
+        const bool dp[2] = {false, true};
+        row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
 #pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        if (!live(q)) continue;
-        const double2 a = y[0][q], b = y[1][q];
-        double2& pp = acc_at(1, q);
-        double2& z = acc_at(3, q);
-        z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r;
-        z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r;
-        pp.x += -vt[q].x * b.x * c2r;
-        pp.y += -vt[q].y * b.y * c2r;
-    }
-    __syncthreads();
-    // B6: omega_r, dT/dr
-    row_c2r<N, ZPT>(P, rowbase, h, A_OMR, false, A_DTDR, false, sm, tw, t, y);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        if (!live(q)) continue;
-        const double2 c = y[0][q], d = y[1][q];
-        double2& z = acc_at(3, q);
-        double2& tt = acc_at(2, q);
-        z.x += vt[q].x * c.x;
-        z.y += vt[q].y * c.y;
-        tt.x += -vr[q].x * d.x;
-        tt.y += -vr[q].y * d.y;
-    }
-    __syncthreads();
-    // B7: dT/dtheta, dT/dphi
-    row_c2r<N, ZPT>(P, rowbase, h, A_DTDT, false, A_T, true, sm, tw, t, y);
-#pragma unroll
-    for (int q = 0; q < ZPT; ++q) {
-        if (!live(q)) continue;
-        const double2 a = y[0][q], b = y[1][q];
-        double2& tt = acc_at(2, q);
-        tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
-        tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+        for (int q = 0; q < ZPT; ++q) {
+            if (!live(q)) continue;
+            const double2 a = y[0][q], b = y[1][q];
+            double2& tt = acc_at(2, q);
+            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+        }
     }
     // CFL (Find_MyMinDT) and the rho r sin(theta) factor of the P and Z terms
     double cmax = 0.0;
@@ -531,7 +483,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     const double sfac = rho * rad * csc;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
-        if ((t + q * ROW_THREADS) < N) {
+        if (live(q)) {
             cmax = fmax(cmax, (vt[q].x * vt[q].x + vp[q].x * vp[q].x) * hfac);
             cmax = fmax(cmax, (vt[q].y * vt[q].y + vp[q].y * vp[q].y) * hfac);
             cmax = fmax(cmax, vr[q].x * vr[q].x * rfac);
@@ -543,9 +495,30 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         }
     }
     __syncthreads();
-    // r2c of W, P and of T, Z; the spectra X_k (k < L) replace the accumulators
-    row_r2c_pair<N>(P, 0, sm, tw, t);
-    row_r2c_pair<N>(P, 2, sm, tw, t);
+    // r2c of W, P, T, Z in place on the accumulators: Z = FFT(y[2n] + i y[2n+1]), then
+    // X_k = e - i conj(w^k) d with e, d the half sums/differences of Z_k, conj Z_{N-k},
+    // one (k, N-k) pair per work item, in place
+    fft_dit<N, 4, ROW_THREADS>(acc, P.twp, t);
+    {
+        constexpr int NI = N / 2 + 1;
+        const int L = P.L;
+        for (int g = t; g < 4 * NI; g += ROW_THREADS) {
+            const int f = g / NI, k = g - f * NI;
+            const double2 zk = acc[SW(f * FS + k)];
+            const double2 zn = acc[SW(f * FS + (N - k) % N)];
+            auto xval = [&](double2 a, double2 b, int kk) {   // X_kk from Z_kk = a, Z_{N-kk} = b
+                const double2 bn = cconj(b);
+                const double2 e = make_double2(0.5 * (a.x + bn.x), 0.5 * (a.y + bn.y));
+                const double2 d = make_double2(0.5 * (a.x - bn.x), 0.5 * (a.y - bn.y));
+                const double2 wd = cmul(cconj(__ldg(P.wr + kk)), d);
+                double2 X = make_double2(e.x + wd.y, e.y - wd.x);
+                if (kk == 0) X.y = 0.0;
+                return X;
+            };
+            if (k < L) acc[SW(f * FS + k)] = xval(zk, zn, k);
+            if (k != 0 && 2 * k != N && N - k < L) acc[SW(f * FS + N - k)] = xval(zn, zk, N - k);
+        }
+    }
     // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122) with the
     // partner row: f_even = X(theta) + X(pi - theta) (written by rank 0),
     // f_odd = X(theta) - X(pi - theta) (written by rank 1)
@@ -593,6 +566,23 @@ void launch_physics(Ctx& c) {
     P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    if (!c.d_twp) {   // per-pass twiddles exp(2 pi i j k / LS) of the in-place FFT (long double)
+        const int n = c.d.nth;
+        std::vector<double> tw(2 * (size_t)ip_tw_size(n));
+        const long double PI = 3.141592653589793238462643383279502884L;
+        for (int ps = 0; ps < npass_of(n); ++ps) {
+            const int R = radix_at(n, ps), LS = ip_ls(n, ps), SS = LS / R, off = ip_tw_off(n, ps);
+            for (int k = 1; k < R; ++k)
+                for (int j = 0; j < SS; ++j) {
+                    const long double a = 2.0L * PI * (long double)j * k / LS;
+                    tw[2 * (off + (k - 1) * SS + j)] = (double)cosl(a);
+                    tw[2 * (off + (k - 1) * SS + j) + 1] = (double)sinl(a);
+                }
+        }
+        RA_CUDA(cudaMalloc(&c.d_twp, std::max<size_t>(tw.size(), 2) * sizeof(double)));
+        RA_CUDA(cudaMemcpy(c.d_twp, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
     P.cfl = c.d_cfl;
     P.L = c.d.L;
     P.nth = c.d.nth;
@@ -603,6 +593,8 @@ void launch_physics(Ctx& c) {
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
     make_plan(c.d.nth);   // validates n_theta = 2^a 3^b
+    if (c.d.L > (2 * c.d.nth) / 3 + 1)
+        throw ArgError("n_theta must be at least 3 (l_max + 1) / 2 for the physical-space kernel");
     const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;   // clusters of 2 rows
     auto go = [&](auto kern, int n, size_t smem_units) {
         const size_t smem = smem_units * sizeof(double2);

@@ -432,7 +432,7 @@ static void release(Ctx& c) {
     mixed_release(c);
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
-    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_Awpt, c.d_Az,
+    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp, c.d_Awpt, c.d_Az,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
                       c.d_p2a, c.d_p2b, c.d_s2b};
     for (double* b : bufs)

@@ -104,6 +104,7 @@ struct Ctx {
     double *d_radial = nullptr;                       // packed radial profiles (see kRadial*)
     double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot
     double *d_twid = nullptr;                         // [nth] complex exp(2 pi i k / nphi)
+    double *d_twp = nullptr;                          // per-pass twiddles of the in-place phi FFT
     double *d_Awpt = nullptr, *d_Az = nullptr;        // inverses [L][3nr][3nr], [L][nr][nr]
     int *d_ltiles = nullptr;                          // LT tile lists
     int n_inv_tiles = 0, n_fwd_tiles = 0, n_cheb_tiles = 0, n_solve_tiles = 0;

@@ -81,6 +81,44 @@ __device__ __forceinline__ void dft_small(int R, double2* u, int sign) {
         u[1] = csub(a, b);
     } else if (R == 4) {
         dft4(u[0], u[1], u[2], u[3], sign);
+    } else if (R == 16) {
+        // 16 = 4 x 4: DFT-4 over the elements q + 4p, twiddle w16^(q k1), DFT-4 over q;
+        // output k1 + 4 k2
+        const double C1 = 0.92387953251128675613, S1 = 0.38268343236508977173;   // cos, sin pi/8
+        const double H = 0.70710678118654752440;                                  // cos pi/4
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dft4(u[q], u[q + 4], u[q + 8], u[q + 12], sign);
+        // element (q, k1) sits at u[q + 4 k1]; w16^e = (cos, sign sin)(2 pi e / 16)
+        auto tw16 = [&](double2 a, int e) -> double2 {
+            double c, sn;
+            switch (e) {
+                case 1: c = C1; sn = S1; break;
+                case 2: c = H; sn = H; break;
+                case 3: c = S1; sn = C1; break;
+                case 4: c = 0.0; sn = 1.0; break;
+                case 6: c = -H; sn = H; break;
+                case 9: c = -C1; sn = -S1; break;
+                default: c = 1.0; sn = 0.0; break;
+            }
+            sn *= sign;
+            return make_double2(a.x * c - a.y * sn, a.x * sn + a.y * c);
+        };
+#pragma unroll
+        for (int q = 1; q < 4; ++q)
+#pragma unroll
+            for (int k1 = 1; k1 < 4; ++k1) u[q + 4 * k1] = tw16(u[q + 4 * k1], q * k1);
+        double2 v[16];
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            double2 a0 = u[0 + 4 * k1], a1 = u[1 + 4 * k1], a2 = u[2 + 4 * k1], a3 = u[3 + 4 * k1];
+            dft4(a0, a1, a2, a3, sign);
+            v[k1 + 0] = a0;
+            v[k1 + 4] = a1;
+            v[k1 + 8] = a2;
+            v[k1 + 12] = a3;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) u[k] = v[k];
     } else if (R == 8) {
         const double H = 0.70710678118654752440;   // sqrt(2)/2
         double2 a0 = cadd(u[0], u[4]), a1 = cadd(u[1], u[5]), a2 = cadd(u[2], u[6]), a3 = cadd(u[3], u[7]);
@@ -143,9 +181,10 @@ __device__ double2* fft_run(double2* a, double2* bb, int nb, const FFTPlan& pl, 
     return src;
 }
 
-// ---- compile-time plans: the same greedy radix order as make_plan (8, 4, 2, 3) ----
+// ---- compile-time plans of the in-place FFT: greedy radix order 16, 8, 4, 2, 3 ----
 __host__ __device__ constexpr int radix_at(int n, int i) {
     int m = n, k = 0;
+    while (m % 16 == 0) { if (k == i) return 16; m /= 16; ++k; }
     while (m % 8 == 0) { if (k == i) return 8; m /= 8; ++k; }
     while (m % 4 == 0) { if (k == i) return 4; m /= 4; ++k; }
     while (m % 2 == 0) { if (k == i) return 2; m /= 2; ++k; }
@@ -249,10 +288,16 @@ __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const dou
         for (int m = 0; m < R; ++m) buf[SW(base + m * SS)] = u[m];
     };
     // two independent butterflies per iteration for instruction-level parallelism
+    // (one for radix 16, whose butterfly alone fills the registers)
+    if constexpr (R >= 16) {
 #pragma unroll 1
-    for (int g = tid; g < T * NB; g += 2 * NT) {
-        butterfly(g);
-        if (g + NT < T * NB) butterfly(g + NT);
+        for (int g = tid; g < T * NB; g += NT) butterfly(g);
+    } else {
+#pragma unroll 1
+        for (int g = tid; g < T * NB; g += 2 * NT) {
+            butterfly(g);
+            if (g + NT < T * NB) butterfly(g + NT);
+        }
     }
 }
 

@@ -184,7 +184,6 @@ __device__ double2* fft_run(double2* a, double2* bb, int nb, const FFTPlan& pl, 
 // ---- compile-time plans of the in-place FFT: greedy radix order 16, 8, 4, 2, 3 ----
 __host__ __device__ constexpr int radix_at(int n, int i) {
     int m = n, k = 0;
-    while (m % 16 == 0) { if (k == i) return 16; m /= 16; ++k; }
     while (m % 8 == 0) { if (k == i) return 8; m /= 8; ++k; }
     while (m % 4 == 0) { if (k == i) return 4; m /= 4; ++k; }
     while (m % 2 == 0) { if (k == i) return 2; m /= 2; ++k; }
@@ -227,7 +226,7 @@ struct PhysParams {
 
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
 // 2-CTA cluster that folds its spectra through distributed shared memory.
-constexpr int ROW_THREADS = 256;
+constexpr int ROW_THREADS = 384;
 constexpr int FB = 4;   // fields per batched FFT
 
 // Shared memory of a row CTA (double2 units): one in-place FFT buffer of FB
@@ -289,7 +288,7 @@ __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const dou
     };
     // two independent butterflies per iteration for instruction-level parallelism
     // (one for radix 16, whose butterfly alone fills the registers)
-    if constexpr (R >= 16) {
+    if constexpr (R >= 16 || NT > 256) {
 #pragma unroll 1
         for (int g = tid; g < T * NB; g += NT) butterfly(g);
     } else {

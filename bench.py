@@ -280,6 +280,19 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def max_over_ranks(value, world, dist, torch, device):
+    """The largest value over all ranks (a device-timed duration: the job's time is its slowest rank's)."""
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def ensemble_rate(steps_per_rank, max_ms, world):
+    """Whole-job steps/s of `world` independent replicas that each ran `steps_per_rank` steps."""
+    return world * steps_per_rank / (max_ms * 1e-3)
+
+
 def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, peak_kind):
     """Times one precision form on this rank; returns (line fields or None off rank 0, state at step err_steps)."""
     import ctypes
@@ -300,12 +313,10 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
         total_ms, per_kernel = ctx.time_steps(args.steps)
     launches = ctx.launch_count()
     torch.cuda.synchronize()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    max_ms = max_over_ranks(total_ms, world, dist, torch, "cuda")
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms * 1e-3)
+    value = ensemble_rate(args.steps, max_ms, world)
     # continue (untimed) to err_steps for the mixed-vs-FP64 comparison
     done = max(1, args.warmup) + args.steps
     if args.err_steps > done:
@@ -336,10 +347,7 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     h2d = (h_wpt.nbytes + h_z.nbytes + h_ab.nbytes)
     d2h = (o_wpt.nbytes + o_z.nbytes + o_ab.nbytes + 8)
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world / float(e2e_t.item())
+    e2e_value = world / max_over_ranks(e2e_s, world, dist, torch, "cuda")
     n_theta, n_phi = ctx.n_theta, ctx.n_phi
     ctx.close()
     del h_wpt, h_z, h_ab, o_wpt, o_z, o_ab

@@ -201,10 +201,11 @@ __host__ __device__ constexpr int pprod(int n, int i) {
     return p;
 }
 
-// Shared-memory index swizzle for the FFT buffers: permutes the 8 complex
-// values of each aligned group by XOR with the next 3 index bits, which makes the
-// stride-R writes of the first Stockham passes bank-conflict free.
-__device__ __forceinline__ int SW(int i) { return i ^ ((i >> 3) & 7); }
+// Shared-memory index of a buffer position.  The in-place passes' strides
+// (96, 12, 3, 1 at N = 768) conflict least with the identity map: an XOR
+// swizzle of bits 3-5 cost 1.67 wavefronts per ideal one over all passes
+// (the stride-1 radix-3 pass 2.5), the identity 1.33.
+__device__ __forceinline__ int SW(int i) { return i; }
 
 // Stride between the fields of a batched buffer: a multiple of 64, so that a
 // field's swizzled indices stay inside the field whatever buffer it sits in.

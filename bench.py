@@ -80,7 +80,7 @@ def kernel_work(lmax, nr, nth):
     plane = n_lm * 2 * nr * 8.0
     w["post_assemble"] = ("hbm", (12 + 4 + 4 + 7) * plane)
     w["rlm_a"] = ("hbm", (7 + 11) * plane)
-    w["rlm_b"] = ("hbm", (4 + 4) * plane)
+    w["rlm_b"] = ("hbm", (4 + 4 + 8) * plane)   # s2b in, ab out, rhs read and written
     w["physics"] = ("hbm", L * nth * (11 + 4) * nr * 2 * 8.0)
     return w
 

@@ -122,55 +122,71 @@ void launch_cheb_synthesis(Ctx& c) {
 // ---------------------------------------------------------------------------
 // RHS assembly + transpose to the m-major spectral layout
 // ---------------------------------------------------------------------------
-__constant__ Slot kSlotsDev[NSLOT] = {
-    {EQ_W, G_W0}, {EQ_W, G_W1}, {EQ_W, G_W2}, {EQ_W, G_P1}, {EQ_W, G_T0},
-    {EQ_P, G_W0}, {EQ_P, G_W1}, {EQ_P, G_W2}, {EQ_P, G_W3}, {EQ_P, G_P0},
-    {EQ_T, G_T0}, {EQ_T, G_T1}, {EQ_T, G_T2},
-    {EQ_Z, G_Z0}, {EQ_Z, G_Z1}, {EQ_Z, G_Z2}};
+// the RHS terms (equation, grid source) as compile-time functions, so that
+// unrolled loops index register arrays with constants (same table as kSlots)
+__host__ __device__ constexpr int slot_eq(int s) {
+    constexpr int e[NSLOT] = {EQ_W, EQ_W, EQ_W, EQ_W, EQ_W, EQ_P, EQ_P, EQ_P,
+                              EQ_P, EQ_P, EQ_T, EQ_T, EQ_T, EQ_Z, EQ_Z, EQ_Z};
+    return e[s];
+}
+__host__ __device__ constexpr int slot_g(int s) {
+    constexpr int g[NSLOT] = {G_W0, G_W1, G_W2, G_P1, G_T0, G_W0, G_W1, G_W2,
+                              G_W3, G_P0, G_T0, G_T1, G_T2, G_Z0, G_Z1, G_Z2};
+    return g[s];
+}
+static_assert(slot_eq(3) == kSlots[3].eq && slot_g(8) == kSlots[8].g && slot_g(15) == kSlots[15].g, "slot table");
 
 __global__ void post_assemble_kernel(const double* __restrict__ g, const double* __restrict__ ab,
                                      const double* __restrict__ coef, double* __restrict__ rhs_wpt,
                                      double* __restrict__ rhs_z, double* __restrict__ s2a, long nlm, int nr,
                                      int L, double old_ab) {
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, ri, r), r fastest
-    const long total = nlm * 2 * nr;
-    if (idx >= total) return;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r), r fastest; both re/im
+    if (idx >= nlm * nr) return;
     const int r = (int)(idx % nr);
-    const long col = idx / nr;          // lm * 2 + ri
-    const int ri = (int)(col & 1);
-    const long lm = col >> 1;
+    const long lm = idx / nr;
     const int l = ell_of_lm(lm);
     const int m = (int)(lm - (long)l * (l + 1) / 2);
     const long plane = nlm * 2 * nr;    // one field of g / ab
-    double gv[NG];
+    const long i0 = lm * 2 * nr + r;    // (lm, re, r); (lm, im, r) is nr further
+    double gv[NG][2];
 #pragma unroll
-    for (int o = 0; o < NG; ++o) gv[o] = g[o * plane + idx];
-    double acc[4];
+    for (int o = 0; o < NG; ++o) {
+        gv[o][0] = g[o * plane + i0];
+        gv[o][1] = g[o * plane + i0 + nr];
+    }
+    double acc[4][2];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) acc[e] = ab[e * plane + idx] * old_ab;
+    for (int e = 0; e < 4; ++e) {
+        acc[e][0] = ab[e * plane + i0] * old_ab;
+        acc[e][1] = ab[e * plane + i0 + nr] * old_ab;
+    }
     const double* cf = coef + (long)l * NSLOT * nr + r;
 #pragma unroll
-    for (int s = 0; s < NSLOT; ++s) acc[kSlotsDev[s].eq] += cf[s * nr] * gv[kSlotsDev[s].g];
-    const long base = col * 3L * nr;
-    rhs_wpt[base + r] = acc[EQ_W];
-    rhs_wpt[base + nr + r] = acc[EQ_P];
-    rhs_wpt[base + 2 * nr + r] = acc[EQ_T];
-    rhs_z[col * nr + r] = acc[EQ_Z];
+    for (int s = 0; s < NSLOT; ++s) {
+        const double c = cf[s * nr];
+        acc[slot_eq(s)][0] += c * gv[slot_g(s)][0];   // compile-time indices (unrolled)
+        acc[slot_eq(s)][1] += c * gv[slot_g(s)][1];
+    }
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const long base = (lm * 2 + ri) * 3L * nr;
+        rhs_wpt[base + r] = acc[EQ_W][ri];
+        rhs_wpt[base + nr + r] = acc[EQ_P][ri];
+        rhs_wpt[base + 2 * nr + r] = acc[EQ_T][ri];
+        rhs_z[(lm * 2 + ri) * nr + r] = acc[EQ_Z][ri];
+    }
     // s2a[row][f][r][ri] with f = W T Z W' T' Z' W''
     const long row = row_index(m, l, L);
-    double* o = s2a + row * (long)NS2A * nr * 2 + (long)r * 2 + ri;
+    double* o = s2a + row * (long)NS2A * nr * 2 + (long)r * 2;
     const long fs = 2L * nr;
-    o[S_W * fs] = gv[G_W0];
-    o[S_T * fs] = gv[G_T0];
-    o[S_Z * fs] = gv[G_Z0];
-    o[S_W1 * fs] = gv[G_W1];
-    o[S_T1 * fs] = gv[G_T1];
-    o[S_Z1 * fs] = gv[G_Z1];
-    o[S_W2 * fs] = gv[G_W2];
+    constexpr int kOut[NS2A] = {G_W0, G_T0, G_Z0, G_W1, G_T1, G_Z1, G_W2};
+#pragma unroll
+    for (int f = 0; f < NS2A; ++f)
+        *reinterpret_cast<double2*>(o + f * fs) = make_double2(gv[kOut[f]][0], gv[kOut[f]][1]);
 }
 
 void launch_post_assemble(Ctx& c, double old_ab) {
-    const long total = c.d.nlm * 2 * c.d.nr;
+    const long total = c.d.nlm * c.d.nr;
     post_assemble_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
         c.d_g, c.d_ab, c.d_coef, c.d_rhs_wpt, c.d_rhs_z, c.d_s2a, c.d.nlm, c.d.nr, c.d.L, old_ab);
     RA_CUDA(cudaGetLastError());
@@ -208,9 +224,28 @@ __global__ void rlm_a_kernel(const double* __restrict__ s2a, double* __restrict_
     const int lmax = L - 1;
     const long fsz = 2L * nr;   // one field of one row
     const long rsz = (long)NS2A * fsz;
+    // (re, im) of field f at (ll, m, r) in one load
+    auto get2 = [&](int f, int ll) -> double2 {
+        if (ll < m || ll >= lmax) return make_double2(0.0, 0.0);   // l_max zeroed on entry (Sphere_Hybrid_Space.F90:73-75)
+        return __ldg(reinterpret_cast<const double2*>(s2a + row_index(m, ll, L) * rsz + f * fsz + r * 2));
+    };
+    const double2 cW = get2(S_W, l), cT = get2(S_T, l), cZ = get2(S_Z, l), cW1 = get2(S_W1, l);
+    const double2 cT1 = get2(S_T1, l), cZ1 = get2(S_Z1, l), cW2 = get2(S_W2, l);
+    const double2 mW = get2(S_W, l - 1), pW = get2(S_W, l + 1), mW1 = get2(S_W1, l - 1), pW1 = get2(S_W1, l + 1);
+    const double2 mZ = get2(S_Z, l - 1), pZ = get2(S_Z, l + 1), mW2 = get2(S_W2, l - 1), pW2 = get2(S_W2, l + 1);
+    const double2 mZ1 = get2(S_Z1, l - 1), pZ1 = get2(S_Z1, l + 1), mT = get2(S_T, l - 1), pT = get2(S_T, l + 1);
+    auto c = [](double2 v, int ri) { return ri ? v.y : v.x; };
     auto get = [&](int f, int ll, int ri) -> double {
-        if (ll < m || ll >= lmax) return 0.0;   // l_max zeroed on entry (Sphere_Hybrid_Space.F90:73-75)
-        return s2a[row_index(m, ll, L) * rsz + f * fsz + r * 2 + ri];
+        const int dl = ll - l;
+        switch (f) {
+            case S_W: return c(dl < 0 ? mW : (dl > 0 ? pW : cW), ri);
+            case S_T: return c(dl < 0 ? mT : (dl > 0 ? pT : cT), ri);
+            case S_Z: return c(dl < 0 ? mZ : (dl > 0 ? pZ : cZ), ri);
+            case S_W1: return c(dl < 0 ? mW1 : (dl > 0 ? pW1 : cW1), ri);
+            case S_T1: return c(cT1, ri);
+            case S_Z1: return c(dl < 0 ? mZ1 : (dl > 0 ? pZ1 : cZ1), ri);
+            default: return c(dl < 0 ? mW2 : (dl > 0 ? pW2 : cW2), ri);
+        }
     };
     const double orsq = radial[R_OVER_RHORSQ * nr + r];
     const double orr = radial[R_OVER_RHOR * nr + r];

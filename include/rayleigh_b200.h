@@ -179,10 +179,11 @@ long ra_launch_count(const ra_ctx* ctx);
  * exposes the same data as its Spherical_Buffer configurations. */
 #define RA_BUF_GRID    0   /* [12][n_lm][2][n_r]  W, dW, d2W, d3W, P, dP, T, dT, d2T, Z, dZ, d2Z on the grid */
 #define RA_BUF_S2A     1   /* [row][7][n_r][2]    after Post_Solve: W, T, Z, dW, dT, dZ, d2W */
-#define RA_BUF_S2A11   2   /* [row][11][n_r][2]   after rlm_spacea */
-#define RA_BUF_P2A     3   /* [n_theta/2][m][2][11][n_r][2]  even-l / odd-l products E, O */
-#define RA_BUF_P2B     4   /* [m][2][n_theta/2][4][n_r][2]   folded f_even, f_odd */
-#define RA_BUF_S2B     5   /* [row][4][n_r][2]    */
+#define RA_BUF_S2A11   2   /* [row][n_r][11][2]   after rlm_spacea; fields DVRDT, DVTDR, VR, VT, VP,
+                                 DVRDR, DVPDR, OMR, DTDR, DTDT, T */
+#define RA_BUF_P2A     3   /* [n_theta/2][m][2][n_r][11][2]  even-l / odd-l products E, O */
+#define RA_BUF_P2B     4   /* [m][2][n_theta/2][n_r][4][2]   folded f_even, f_odd */
+#define RA_BUF_S2B     5   /* [row][n_r][4][2]    */
 #define RA_BUF_AB      6   /* [4][n_lm][2][n_r]   */
 #define RA_BUF_RHS_WPT 7   /* [n_lm][2][3 n_r]    */
 #define RA_BUF_RHS_Z   8   /* [n_lm][2][n_r]      */

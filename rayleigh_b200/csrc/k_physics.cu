@@ -5,8 +5,8 @@
 //   Find_MyMinDT (CFL max)    (:784-813),
 //   fft_to_spectral (r2c)     (Fourier_Transform.F90:100-140), 4 fields,
 //   equatorial fold of PtS    (Legendre_Transforms.F90:1109-1122),
-// reading the inverse Legendre output p2a[theta_h][m][par][f][r][re/im] (E, O) and
-// writing the folded p2b[m][par][theta_h][f][r][re/im] for m <= l_max.  The
+// reading the inverse Legendre output p2a[theta_h][m][par][r][f][re/im] (E, O) and
+// writing the folded p2b[m][par][theta_h][r][f][re/im] for m <= l_max.  The
 // reference materialises the packed (n_phi+2, r, theta, f) buffers p3a/p3b
 // between these steps; here the 18 phi rows of one (r, theta) point never
 // leave the SM.
@@ -207,9 +207,10 @@ __host__ __device__ constexpr int pprod(int n, int i) {
 // (the stride-1 radix-3 pass 2.5), the identity 1.33.
 __device__ __forceinline__ int SW(int i) { return i; }
 
-// Stride between the fields of a batched buffer: a multiple of 64, so that a
-// field's swizzled indices stay inside the field whatever buffer it sits in.
-__host__ __device__ constexpr int fstride(int n) { return (n + 63) / 64 * 64; }
+// Stride between the fields of a batched buffer (16-byte slots): 2 mod 8, so
+// that the spectrum writes, whose lanes run over the batch's fields first, hit
+// eight different bank groups per quarter warp (n is a multiple of 8).
+__host__ __device__ constexpr int fstride(int n) { return n + 2; }
 
 struct PhysParams {
     const double* p2a;
@@ -366,10 +367,12 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
     constexpr int QI = (NB * NI + ROW_THREADS - 1) / ROW_THREADS;   // items per thread
     double2* buf = sm + RowSmem<N>::BUF;
     const int L = P.L;
-    const long ostride = (long)P.ncola;   // E -> O within p2a[theta_h][m][par][col]
+    const long ostride = (long)P.ncola;   // E -> O within p2a[theta_h][m][par][r][field][2]
     const long mstride = 2L * P.ncola;
     __syncthreads();   // the buffer is free (previous batch read)
     constexpr int QC = 3;   // items whose loads are in flight together
+    // item g = (k, b), b fastest: a quarter warp reads the batch's adjacent
+    // fields of two wavenumbers
 #pragma unroll 1
     for (int q0 = 0; q0 < QI; q0 += QC) {
         double2 xk[QC], xn[QC];
@@ -378,8 +381,8 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
             const int g = t + (q0 + qq) * ROW_THREADS;
             xk[qq] = xn[qq] = make_double2(0.0, 0.0);
             if (q0 + qq < QI && g < NB * NI) {
-                const int b = g / NI, k = g - b * NI;
-                const double* base = rowbase + (long)pick(fo, b) * P.nr * 2;
+                const int k = g / NB, b = g - k * NB;
+                const double* base = rowbase + (long)pick(fo, b) * 2;
                 const bool d = pick(dp, b);
                 xk[qq] = spec_value(base, mstride, ostride, k, L, h, d);
                 xn[qq] = spec_value(base, mstride, ostride, N - k, L, h, d);   // N - k >= L for k = 0
@@ -389,7 +392,7 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
         for (int qq = 0; qq < QC; ++qq) {
             const int g = t + (q0 + qq) * ROW_THREADS;
             if (q0 + qq < QI && g < NB * NI) {
-                const int b = g / NI, k = g - b * NI;
+                const int k = g / NB, b = g - k * NB;
                 buf[SW(b * FS + k)] = zform(xk[qq], xn[qq], __ldg(P.wr + k));
                 if (k != 0 && 2 * k != N) buf[SW(b * FS + N - k)] = zform(xn[qq], xk[qq], __ldg(P.wr + N - k));
             }
@@ -424,7 +427,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     const int r = pair % nr;
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * 2;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
     const double rad = P.radial[R_RADIUS * nr + r];
     const double orad = P.radial[R_OVER_R * nr + r];
     const double rho = P.radial[R_DENSITY * nr + r];
@@ -572,13 +575,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const double2* mine = acc;
         const double2* peer = cluster.map_shared_rank(acc, h ^ 1);
         const int L = P.L;
-        const long mstride = 2L * (P.nth / 2) * P.ncolb;   // p2b[m][par][theta_h][col]
-        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * 2;
-        for (int g = t; g < 4 * L; g += ROW_THREADS) {
-            const int f = g / L, k = g - f * L;
+        const long mstride = 2L * (P.nth / 2) * P.ncolb;   // p2b[m][par][theta_h][r][field][2]
+        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * NP2B);
+        for (int g = t; g < 4 * L; g += ROW_THREADS) {   // g = (k, f), f fastest: 64 contiguous bytes per k
+            const int k = g >> 2, f = g & 3;
             const double2 a = mine[SW(f * FS + k)], b = peer[SW(f * FS + k)];
             const double2 v = h ? csub(b, a) : cadd(a, b);
-            *reinterpret_cast<double2*>(obase + k * mstride + (long)f * P.nr * 2) = v;
+            *reinterpret_cast<double2*>(obase + k * mstride + f * 2) = v;
         }
     }
     // CFL max over the row

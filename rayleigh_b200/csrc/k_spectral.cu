@@ -213,10 +213,17 @@ __device__ __forceinline__ double sdth_c2(int l, int m) {
     return -l * sqrt(num / den);
 }
 
-__global__ void rlm_a_kernel(const double* __restrict__ s2a, double* __restrict__ s2o,
-                             const double* __restrict__ radial, long nlm, int nr, int L) {
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
-    if (idx >= nlm * nr) return;
+constexpr int RLM_A_THREADS = 256;
+
+__global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __restrict__ s2a,
+                                                             double* __restrict__ s2o,
+                                                             const double* __restrict__ radial, long nlm, int nr,
+                                                             int L) {
+    __shared__ double2 stage[RLM_A_THREADS * NP2A];   // the block's outputs, re-read for coalesced stores
+    const long total = nlm * nr;
+    const long idx0 = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    const bool valid = idx0 < total;
+    const long idx = valid ? idx0 : total - 1;   // tail lanes compute a copy, store nothing
     const int r = (int)(idx % nr);
     const long lm = idx / nr;
     const int l = ell_of_lm(lm);
@@ -255,7 +262,6 @@ __global__ void rlm_a_kernel(const double* __restrict__ s2a, double* __restrict_
     const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
     const double llp1 = (double)l * (l + 1);
     const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
-    const long orow = row_index(m, l, L) * (long)NP2A * fsz + r * 2;
     double out[NP2A][2];
 #pragma unroll
     for (int ri = 0; ri < 2; ++ri) {
@@ -292,17 +298,30 @@ __global__ void rlm_a_kernel(const double* __restrict__ s2a, double* __restrict_
         out[A_DVPDR][ri] = dvpdr;
     }
     const bool zero = (l == lmax);   // Sphere_Hybrid_Space.F90:100-102
+    // s2a11[row][r][field][re, im]: a thread's 11 fields are 176 contiguous
+    // bytes, and a warp's lanes of one row are contiguous in r.  The warp
+    // stages its outputs in shared memory and stores them as consecutive
+    // 16-byte chunks, so each store instruction covers a few whole lines.
+    const int lane = threadIdx.x & 31;
+    double2* st = stage + (threadIdx.x - lane) * NP2A;
 #pragma unroll
-    for (int f = 0; f < NP2A; ++f) {
-        double2 v = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
-        *reinterpret_cast<double2*>(s2o + orow + f * fsz) = v;
+    for (int f = 0; f < NP2A; ++f)
+        st[lane * NP2A + f] = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
+    __syncwarp();
+    const long obase = row_index(m, l, L) * (long)NP2A * fsz + (long)r * (2 * NP2A);
+#pragma unroll
+    for (int i = 0; i < NP2A; ++i) {
+        const int ci = i * 32 + lane, sl = ci / NP2A, f = ci - sl * NP2A;
+        const long b = __shfl_sync(0xffffffffu, obase, sl);
+        const int ok = __shfl_sync(0xffffffffu, (int)valid, sl);
+        if (ok) *reinterpret_cast<double2*>(s2o + b + f * 2) = st[ci];
     }
 }
 
 void launch_rlm_a(Ctx& c) {
     const long total = c.d.nlm * c.d.nr;
-    rlm_a_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm,
-                                                                        c.d.nr, c.d.L);
+    rlm_a_kernel<<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
+        c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -320,10 +339,19 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
     const int l = ell_of_lm(lm);
     const int m = (int)(lm - (long)l * (l + 1) / 2);
     const int lmax = L - 1;
-    const long fsz = 2L * nr, rsz = 4L * fsz;
-    auto get = [&](int f, int ll, int ri) -> double {
-        if (ll < m || ll > lmax) return 0.0;
-        return s2b[row_index(m, ll, L) * rsz + f * fsz + r * 2 + ri];
+    const long rsz = 2L * NP2B * nr;   // s2b[row][r][field][re, im]
+    auto get2 = [&](int f, int ll) -> double2 {
+        if (ll < m || ll > lmax) return make_double2(0.0, 0.0);
+        return __ldg(reinterpret_cast<const double2*>(s2b + row_index(m, ll, L) * rsz + r * (2 * NP2B) + f * 2));
+    };
+    const double2 cW = get2(0, l), cP = get2(1, l), cT = get2(2, l), cZ = get2(3, l);
+    const double2 mP = get2(1, l - 1), pP = get2(1, l + 1), mZ = get2(3, l - 1), pZ = get2(3, l + 1);
+    auto get = [&](int f, int ll, int ri) -> double {   // f, ll - l are compile-time after unrolling
+        const int dl = ll - l;
+        const double2 v = f == 0 ? cW : f == 2 ? cT
+                        : f == 1 ? (dl < 0 ? mP : (dl > 0 ? pP : cP))
+                                 : (dl < 0 ? mZ : (dl > 0 ? pZ : cZ));
+        return ri ? v.y : v.x;
     };
     const double ollp1 = (l > 0) ? 1.0 / ((double)l * (l + 1)) : 1.0;
     const double c1 = sdth_c1(l, m), c2 = sdth_c2(l, m);

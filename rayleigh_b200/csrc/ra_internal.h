@@ -53,9 +53,12 @@ constexpr Slot kSlots[NSLOT] = {
 // Spectral forward-leg fields after Post_Solve (s2a, 7 fields; P is not carried
 // because the hydrodynamic non-output step never transforms it):
 enum { S_W, S_T, S_Z, S_W1, S_T1, S_Z1, S_W2, NS2A };
-// Fields of the inverse Legendre transform (p2a, 11 fields):
-enum { A_VR, A_T, A_OMR, A_DVRDR, A_DTDR, A_DVRDT, A_DTDT, A_VT, A_VP, A_DVTDR, A_DVPDR, NP2A };
-// Return-leg fields (p2b / s2b / ab): W P T Z
+// Fields of the inverse Legendre transform (p2a, 11 fields).  s2a11 and p2a
+// keep the fields of one radius together ([..][r][field][re, im]), in an order
+// that puts the fields each physical-space FFT batch reads next to each other:
+// {DVRDT, DVTDR, VR, VT}, {VR, VT, VP, DVRDR}, {VP, DVPDR, OMR, DTDR}, {DTDT, T}.
+enum { A_DVRDT, A_DVTDR, A_VR, A_VT, A_VP, A_DVRDR, A_DVPDR, A_OMR, A_DTDR, A_DTDT, A_T, NP2A };
+// Return-leg fields (p2b / s2b / ab): W P T Z; p2b and s2b are [..][r][field][re, im]
 constexpr int NP2B = 4;
 
 struct Radial {

@@ -14,23 +14,24 @@ def row_index(m, l, L):
     return m_off(m, L) + ((ne + (d - 1) // 2) if (d & 1) else d // 2)
 
 
-def s2_to_rows(s2, fields):
-    """list over m of (nf, 2, nr, nl) -> [row][len(fields)][nr][2]."""
+def s2_to_rows(s2, fields, r_major=False):
+    """list over m of (nf, 2, nr, nl) -> [row][F][nr][2], or [row][nr][F][2] when r_major."""
     L = len(s2)
     nr = s2[0].shape[2]
     nlm = L * (L + 1) // 2
-    out = np.zeros((nlm, len(fields), nr, 2))
+    F = len(fields)
+    out = np.zeros((nlm, nr, F, 2) if r_major else (nlm, F, nr, 2))
     for m in range(L):
         a = s2[m][list(fields)]                      # (F, 2, nr, nl)
         rows = [row_index(m, m + j, L) for j in range(L - m)]
-        out[rows] = a.transpose(3, 0, 2, 1)
+        out[rows] = a.transpose(3, 2, 0, 1) if r_major else a.transpose(3, 0, 2, 1)
     return out
 
 
 def p2_to_dev(p2, fields):
-    """list over m of (nf, 2, nr, nth) -> [m][nth][F][nr][2]."""
+    """list over m of (nf, 2, nr, nth) -> [m][nth][nr][F][2]."""
     P = np.stack([p[list(fields)] for p in p2])     # (m, F, 2, nr, nth)
-    return P.transpose(0, 4, 1, 3, 2).copy()
+    return P.transpose(0, 4, 3, 1, 2).copy()
 
 
 def rel_err(a, b):
@@ -43,17 +44,17 @@ def rel_err(a, b):
 
 
 def p2_eo_to_full(dev, L, nth, F, nr):
-    """device [nth/2][m][par][F][nr][2] (E, O) -> [m][nth][F][nr][2] with south E+O, north E-O."""
-    d = dev.reshape(nth // 2, L, 2, F, nr, 2).transpose(1, 2, 0, 3, 4, 5)
+    """device [nth/2][m][par][nr][F][2] (E, O) -> [m][nth][nr][F][2] with south E+O, north E-O."""
+    d = dev.reshape(nth // 2, L, 2, nr, F, 2).transpose(1, 2, 0, 3, 4, 5)
     e, o = d[:, 0], d[:, 1]
-    full = np.empty((L, nth, F, nr, 2))
+    full = np.empty((L, nth, nr, F, 2))
     full[:, :nth // 2] = e + o
     full[:, nth - 1:nth // 2 - 1:-1] = e - o
     return full
 
 
 def p2_fold(full):
-    """[m][nth][F][nr][2] -> [m][2][nth/2][F][nr][2] folded (s + n, s - n)."""
+    """[m][nth][nr][F][2] -> [m][2][nth/2][nr][F][2] folded (s + n, s - n)."""
     nth = full.shape[1]
     s = full[:, :nth // 2]
     n = full[:, nth - 1:nth // 2 - 1:-1]

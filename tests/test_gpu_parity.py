@@ -131,15 +131,16 @@ def _stage_compare(cfg, steps_before=0, amp=1e-2):
     errs["rhs_z"] = rel_err(g.debug_buffer("rhs_z"), rhs_z.ravel())
     errs["s2a"] = rel_err(g.debug_buffer("s2a"), s2_to_rows(s2a, [0, 2, 3, 4, 5, 6, 7]).ravel())
     g.rlm_spacea()
-    a_fields = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]
-    errs["s2a11"] = rel_err(g.debug_buffer("s2a11"), s2_to_rows(s2a12, a_fields).ravel())
+    # device field order DVRDT, DVTDR, VR, VT, VP, DVRDR, DVPDR, OMR, DTDR, DTDT, T as oracle indexes
+    a_fields = [6, 10, 0, 8, 9, 4, 11, 3, 5, 7, 2]
+    errs["s2a11"] = rel_err(g.debug_buffer("s2a11"), s2_to_rows(s2a12, a_fields, r_major=True).ravel())
     errs["p2a"] = rel_err(p2_eo_to_full(g.debug_buffer("p2a"), L, nth, len(a_fields), nr),
                           p2_to_dev(p2a, a_fields))
     cfl = g.physical_space()
     errs["cfl"] = abs(cfl - cfl_ref) / max(cfl_ref, 1e-300)
     errs["p2b"] = rel_err(g.debug_buffer("p2b"), p2_fold(p2_to_dev(p2b, [0, 1, 2, 3])).ravel())
     g.rlm_spaceb()
-    errs["s2b"] = rel_err(g.debug_buffer("s2b"), s2_to_rows(s2b, [0, 1, 2, 3]).ravel())
+    errs["s2b"] = rel_err(g.debug_buffer("s2b"), s2_to_rows(s2b, [0, 1, 2, 3], r_major=True).ravel())
     errs["ab"] = rel_err(g.debug_buffer("ab"), ab.ravel())
     g.advance_time()
     wg, zg, _ = g.get_state()

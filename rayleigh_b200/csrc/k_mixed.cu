@@ -46,7 +46,7 @@ static void plan_launch(Ctx& c, MixedPlan& p, const std::vector<OzProblem>& prob
 static void run_split_once(Ctx& c, const std::vector<OzSplitJob>& jobs, int max_rows) {
     if (jobs.empty()) return;
     OzSplitJob* d = upload(c, jobs);
-    ozaki_split(c, d, (int)jobs.size(), max_rows);
+    ozaki_split(c, d, (int)jobs.size(), max_rows, oz_split_kinds(jobs.data(), (int)jobs.size()));
     RA_CUDA(cudaStreamSynchronize(c.stream));
     cudaFree(d);
 }
@@ -99,12 +99,13 @@ static void setup_lt_inverse(Ctx& c) {
     p.d_jobs = upload(c, ajobs);
     p.njobs = (int)ajobs.size();
     p.max_rows = nta * OZ_HA;
+    p.kinds = oz_split_kinds(ajobs.data(), p.njobs);
     plan_launch(c, p, probs);
 }
 
 void launch_lt_inverse_mixed(Ctx& c) {
     MixedPlan& p = c.mx_inv;
-    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows, p.kinds);
     ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
 }
 
@@ -153,13 +154,14 @@ static void setup_lt_forward(Ctx& c) {
     p.d_jobs = upload(c, ajobs);
     p.njobs = (int)ajobs.size();
     p.max_rows = nta * OZ_HA;
+    p.kinds = oz_split_kinds(ajobs.data(), p.njobs);
     plan_launch(c, p, probs);
     RA_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 void launch_lt_forward_mixed(Ctx& c) {
     MixedPlan& p = c.mx_fwd;
-    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows, p.kinds);
     ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
 }
 
@@ -230,10 +232,12 @@ static void setup_solve(Ctx& c) {
     p.d_setup_jobs = upload(c, ajobs);
     p.nsetup_jobs = (int)ajobs.size();
     p.setup_max_rows = max_a;
-    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows);
+    p.setup_kinds = oz_split_kinds(ajobs.data(), p.nsetup_jobs);
+    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows, p.setup_kinds);
     p.d_jobs = upload(c, bjobs);
     p.njobs = (int)bjobs.size();
     p.max_rows = max_b;
+    p.kinds = oz_split_kinds(bjobs.data(), p.njobs);
     plan_launch(c, p, probs);
     RA_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -241,13 +245,13 @@ static void setup_solve(Ctx& c) {
 void mixed_resplit_solve(Ctx& c) {
     MixedPlan& p = c.mx_solve;
     if (!p.d_setup_jobs) return;
-    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows);
+    ozaki_split(c, p.d_setup_jobs, p.nsetup_jobs, p.setup_max_rows, p.setup_kinds);
     RA_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 void launch_solve_mixed(Ctx& c) {
     MixedPlan& p = c.mx_solve;
-    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows);
+    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows, p.kinds);
     ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
 }
 

@@ -368,8 +368,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
 // memory (read along whichever index is contiguous), digits transposed into
 // the [s][kc][row][16] block layout and written as 16-byte rows.
 // ---------------------------------------------------------------------------
+// Split of a job whose K runs are contiguous (sk == 1): 16 rows per CTA,
+// staged through shared memory so that each store is 16 rows x 16 bytes.
 __global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __restrict__ jobs) {
     const OzSplitJob& jb = jobs[blockIdx.y];
+    if (jb.sk != 1) return;   // ozaki_split_rows_kernel
     const int r0 = blockIdx.x * 16;
     if (r0 >= jb.nrt * jb.H) return;
     __shared__ double xs[16][33];
@@ -432,12 +435,91 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __re
     }
 }
 
-void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows) {
+// Split of a job whose rows are contiguous (sk != 1; the transposed operands
+// s2a11^T, p2b^T): one thread per row.  A warp's loads cover 32 consecutive
+// rows of one k; each thread packs the digits of 16 consecutive k into one
+// 16-byte chunk per digit plane, and a warp's chunks are 512 contiguous bytes
+// of the tiled layout.  No shared memory and no barriers: every thread keeps
+// 16 loads in flight.
+constexpr int OZ_ROWS_THREADS = 256;
+
+__global__ void __launch_bounds__(OZ_ROWS_THREADS) ozaki_split_rows_kernel(const OzSplitJob* __restrict__ jobs) {
+    const OzSplitJob& jb = jobs[blockIdx.y];
+    if (jb.sk == 1) return;   // ozaki_split_kernel
+    const int r = blockIdx.x * OZ_ROWS_THREADS + threadIdx.x;
+    if (r >= jb.nrt * jb.H) return;
+    const bool live = r < jb.R;   // rows R .. nrt*H - 1 are padding: zero digits
+    const long sk = jb.sk;
+    const int K = jb.K;
+    const double* __restrict__ xr = jb.X + (long)(live ? r : 0) * jb.sr;
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    if (live) {
+        int k = 0;
+        for (; k + 3 < K; k += 4) {
+            m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
+            m1 = fmax(m1, fabs(__ldg(xr + (k + 1) * sk)));
+            m2 = fmax(m2, fabs(__ldg(xr + (k + 2) * sk)));
+            m3 = fmax(m3, fabs(__ldg(xr + (k + 3) * sk)));
+        }
+        for (; k < K; ++k) m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
+    }
+    const double mx = fmax(fmax(m0, m1), fmax(m2, m3));
+    const int ex = (mx > 0.0) ? ilogb(mx) + 2 : 0;   // digits of the integer rint(x 2^(39-e))
+    if (live) jb.e[r] = ex;
+    const int sh = 39 - ex;
+    const bool direct = (sh <= 1023 && sh >= -1022);
+    const double sc = direct ? pow2(sh) : 1.0;
+    const int rt = r / jb.H, rin = r - rt * jb.H;
+    const long blk = (long)OZ_S * jb.H * OZ_BK;
+    const int kstride = jb.kstride > 0 ? jb.kstride : jb.nks;
+#pragma unroll 1
+    for (int ks = 0; ks < jb.nks; ++ks) {
+        int8_t* base = jb.out + ((long)rt * kstride + jb.ks0 + ks) * blk + (long)rin * 16;
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+            const int k0 = ks * OZ_BK + kc * 16;
+            double v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = (live && k0 + i < K) ? __ldg(xr + (long)(k0 + i) * sk) : 0.0;
+            unsigned w[OZ_S][4];
+#pragma unroll
+            for (int s = 0; s < OZ_S; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const double a = direct ? v[i] * sc : ldexp(v[i], sh);
+                int8_t qd[OZ_S];
+                oz_digits(__double2ll_rn(a), qd);
+#pragma unroll
+                for (int s = 0; s < OZ_S; ++s) w[s][i >> 2] |= (unsigned)(uint8_t)qd[s] << (8 * (i & 3));
+            }
+#pragma unroll
+            for (int s = 0; s < OZ_S; ++s)
+                *reinterpret_cast<int4*>(base + (long)s * jb.H * OZ_BK + (long)kc * jb.H * 16) =
+                    make_int4((int)w[s][0], (int)w[s][1], (int)w[s][2], (int)w[s][3]);
+        }
+    }
+}
+
+int oz_split_kinds(const OzSplitJob* jobs, int njobs) {
+    int kinds = 0;
+    for (int i = 0; i < njobs; ++i) kinds |= (jobs[i].sk == 1) ? OZ_SPLIT_KMAJOR : OZ_SPLIT_ROWS;
+    return kinds;
+}
+
+void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows, int kinds) {
     if (njobs == 0 || max_rows == 0) return;
-    dim3 grid((max_rows + 15) / 16, njobs);
-    ozaki_split_kernel<<<grid, 256, 0, c.stream>>>(d_jobs);
-    RA_CUDA(cudaGetLastError());
-    ++c.launches;
+    if (kinds & OZ_SPLIT_KMAJOR) {
+        dim3 grid((max_rows + 15) / 16, njobs);
+        ozaki_split_kernel<<<grid, 256, 0, c.stream>>>(d_jobs);
+        RA_CUDA(cudaGetLastError());
+        ++c.launches;
+    }
+    if (kinds & OZ_SPLIT_ROWS) {
+        dim3 grid((max_rows + OZ_ROWS_THREADS - 1) / OZ_ROWS_THREADS, njobs);
+        ozaki_split_rows_kernel<<<grid, OZ_ROWS_THREADS, 0, c.stream>>>(d_jobs);
+        RA_CUDA(cudaGetLastError());
+        ++c.launches;
+    }
 }
 
 static int oz_sm_count() {
@@ -600,6 +682,8 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
     oz_static_prepare_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(pr, ja, jbj, d_prob, d_jobs, d_tiles, ntm, ntn,
                                                                      d_status);
     ozaki_split_kernel<<<dim3((std::max(mp, np) + 15) / 16, 2), 256, 0, st>>>(d_jobs);
+    ozaki_split_rows_kernel<<<dim3((std::max(mp, np) + OZ_ROWS_THREADS - 1) / OZ_ROWS_THREADS, 2), OZ_ROWS_THREADS, 0,
+                              st>>>(d_jobs);
     e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem));
     if (e == cudaSuccess) {
         ozaki_gemm_kernel<<<std::min(ntiles, nsm), OZ_THREADS, sizeof(OzSmem), st>>>(d_prob, d_tiles, ntiles, d_status);

@@ -229,6 +229,7 @@ struct PhysParams {
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
 // 2-CTA cluster that folds its spectra through distributed shared memory.
 constexpr int ROW_THREADS = 384;
+enum { RC_RAD, RC_ORAD, RC_RHO, RC_DLNRHO, RC_DR, RC_CS, RC_SN, RC_CSC, RC_COT, RC_COR, RC_C2R, RC_COUNT };
 constexpr int FB = 4;   // fields per batched FFT
 
 // Shared memory of a row CTA (double2 units): one in-place FFT buffer of FB
@@ -428,14 +429,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
-    const double rad = P.radial[R_RADIUS * nr + r];
-    const double orad = P.radial[R_OVER_R * nr + r];
-    const double rho = P.radial[R_DENSITY * nr + r];
-    const double dlnrho = P.radial[R_DLNRHO * nr + r];
-    const double dr = P.radial[R_DELTA_R * nr + r];
-    const double cs = P.trig[th], sn = P.trig[N + th], csc = P.trig[2 * N + th], cot = P.trig[3 * N + th];
-    const double cor = P.rotation ? P.coriolis : 0.0;
-    const double c2r = csc * csc * orad;
+    // The row's radial and colatitude factors live in shared memory and are read
+    // where they are used, so that they hold no registers across the FFTs.
+    __shared__ double rowc[RC_COUNT];
+    if (t == 0) {
+        const double csc = P.trig[2 * N + th], orad = P.radial[R_OVER_R * nr + r];
+        rowc[RC_RAD] = P.radial[R_RADIUS * nr + r];
+        rowc[RC_ORAD] = orad;
+        rowc[RC_RHO] = P.radial[R_DENSITY * nr + r];
+        rowc[RC_DLNRHO] = P.radial[R_DLNRHO * nr + r];
+        rowc[RC_DR] = P.radial[R_DELTA_R * nr + r];
+        rowc[RC_CS] = P.trig[th];
+        rowc[RC_SN] = P.trig[N + th];
+        rowc[RC_CSC] = csc;
+        rowc[RC_COT] = P.trig[3 * N + th];
+        rowc[RC_COR] = P.rotation ? P.coriolis : 0.0;
+        rowc[RC_C2R] = csc * csc * orad;
+    }   // read after row_c2r's first barrier
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
     double2 y[FB][ZPT];
@@ -446,6 +456,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const int fo[4] = {A_VR, A_VT, A_VP, A_DVRDR};
         const bool dp[4] = {false, false, false, false};
         row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], dlnrho = rowc[RC_DLNRHO];
+        const double cs = rowc[RC_CS], sn = rowc[RC_SN], csc = rowc[RC_CSC], cot = rowc[RC_COT], cor = rowc[RC_COR];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             vr[q] = y[0][q];
@@ -476,6 +488,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
         const bool dp[4] = {false, true, false, true};
         row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const double rad = rowc[RC_RAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
@@ -496,6 +509,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
         const bool dp[4] = {false, true, false, false};
         row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
@@ -516,6 +530,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const int fo[2] = {A_DTDT, A_T};
         const bool dp[2] = {false, true};
         row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
@@ -527,8 +542,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     }
     // CFL (Find_MyMinDT) and the rho r sin(theta) factor of the P and Z terms
     double cmax = 0.0;
+    const double orad = rowc[RC_ORAD], dr = rowc[RC_DR];
     const double hfac = P.llmax * orad * orad, rfac = 1.0 / (dr * dr);
-    const double sfac = rho * rad * csc;
+    const double sfac = rowc[RC_RHO] * rowc[RC_RAD] * rowc[RC_CSC];
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
         if (live(q)) {

@@ -58,7 +58,12 @@ struct OzSplitJob {
     int kstride, ks0;
 };
 
-void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows);
+// Jobs with contiguous K runs (sk == 1) and jobs with contiguous rows go to two
+// kernels; kinds says which of the two a job list holds.
+constexpr int OZ_SPLIT_KMAJOR = 1, OZ_SPLIT_ROWS = 2;
+int oz_split_kinds(const OzSplitJob* jobs, int njobs);
+void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows,
+                 int kinds = OZ_SPLIT_KMAJOR | OZ_SPLIT_ROWS);
 void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles, int* d_status);
 std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs);
 inline int oz_tiles_of(int rows, int h) { return (rows + h - 1) / h; }

@@ -78,9 +78,9 @@ struct MixedPlan {
     int* d_tiles = nullptr;
     int ntiles = 0;
     OzSplitJob* d_jobs = nullptr;
-    int njobs = 0, max_rows = 0;
+    int njobs = 0, max_rows = 0, kinds = 0;
     OzSplitJob* d_setup_jobs = nullptr;   // splits of the constant operand, rerun when it changes
-    int nsetup_jobs = 0, setup_max_rows = 0;
+    int nsetup_jobs = 0, setup_max_rows = 0, setup_kinds = 0;
 };
 
 struct Ctx {

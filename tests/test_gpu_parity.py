@@ -163,6 +163,16 @@ def test_step_stages_ab2_step():
     assert not bad, errs
 
 
+def test_step_stages_768_point_phi_transform():
+    """l_max = 511, n_theta = 768 (the headline grid's angular size, few radii):
+    the physical-space kernel runs its 768-point plan, with its own
+    shared-memory layouts and the radix-12 register pass, only at this size."""
+    errs = _stage_compare(dict(n_r=8, l_max=511, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1)
+    print({k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if v > TOL}
+    assert not bad, errs
+
+
 def _fields(wpt, z, nr):
     return {"W": wpt[:, :, :nr], "P": wpt[:, :, nr:2 * nr], "T": wpt[:, :, 2 * nr:], "Z": z}
 

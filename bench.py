@@ -37,7 +37,9 @@ SEED = 0x5241594C
 
 
 def headline_config(lmax, nr, precision):
-    """Boussinesq rotating convection at the headline grid (BASELINE config 5 sizes, hydrodynamic)."""
+    """Boussinesq rotating convection (hydrodynamic) on an l_max x N_r grid; the
+    default l_max = 511, N_r = 192 is the size the reference's largest
+    benchmark case runs at."""
     return dict(n_r=nr, l_max=lmax, aspect_ratio=0.35, shell_depth=1.0, rayleigh=2.0e8, ekman=1.0e-5,
                 prandtl=1.0, gravity_power=1.0, rotation=True, no_slip_top=True, no_slip_bottom=True,
                 fix_tvar_top=True, fix_tvar_bottom=True, t_top=0.0, t_bottom=1.0, dt=1.0e-6,

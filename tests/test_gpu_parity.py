@@ -164,9 +164,9 @@ def test_step_stages_ab2_step():
 
 
 def test_step_stages_768_point_phi_transform():
-    """l_max = 511, n_theta = 768 (the headline grid's angular size, few radii):
-    the physical-space kernel runs its 768-point plan, with its own
-    shared-memory layouts and the radix-12 register pass, only at this size."""
+    """l_max = 511, n_theta = 768 (the l_max = 511 grid's angular size, few
+    radii): the largest phi transform, and the only size here at which each
+    physical-space thread owns two points of a row."""
     errs = _stage_compare(dict(n_r=8, l_max=511, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1)
     print({k: f"{v:.2e}" for k, v in errs.items()})
     bad = {k: v for k, v in errs.items() if v > TOL}
@@ -179,7 +179,7 @@ def _fields(wpt, z, nr):
 
 @pytest.mark.parametrize("cfg,steps", [
     (dict(n_r=24, l_max=15, dt=2e-4), 20),
-    (dict(n_r=48, l_max=63, dt=1e-4), 10),          # BASELINE config 1 grid (C1)
+    (dict(n_r=48, l_max=63, dt=1e-4), 10),          # the l_max = 63, N_r = 48 grid
     (dict(n_r=32, l_max=31, dt=1e-4, no_slip_top=False, no_slip_bottom=False, fix_tvar_bottom=False,
           dtdr_bottom=-1.0, rotation=False), 10),
 ])

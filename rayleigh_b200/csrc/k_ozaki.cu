@@ -37,7 +37,7 @@
 
 namespace ra {
 
-constexpr int OZ_NST = 6;
+constexpr int OZ_NST = 8;   // operand ring stages: about 1.8 tiles of the longest-K products ahead of the MMAs
 constexpr int OZ_EPI_WARPS = 12;                           // three per TMEM lane quadrant
 constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
 constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (16)
@@ -59,6 +59,7 @@ struct OzSmem {
     uint32_t tmem_base;
     int abort;
 };
+static_assert(sizeof(OzSmem) <= 232448, "operand ring exceeds the 227 KB of shared memory per block");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -306,15 +307,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
             for (int sg = 0; sg < nseg; ++sg, ++tl_i) {
                 const int buf = tl_i & 1;
                 const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+                // row scale with the combined weight 2^-46 of S below folded in; the
+                // column scales of this warp's columns, one per lane, shared by shuffle
+                // (loaded before the wait for the accumulator, which hides their latency)
+                const int ea_v = rok ? pb.ea[sg * pb.ea_seg + row] : 0;
+                const int eb_v = cok ? __ldg(pb.eb + sg * pb.eb_seg + colw) : 0;
                 if (!mbar_wait(&sm.acc_full[buf], aph)) {
                     ok = false;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                // row scale with the combined weight 2^-46 of S below folded in; the
-                // column scales of this warp's columns, one per lane, shared by shuffle
-                const double sa = rok ? pow2(pb.ea[sg * pb.ea_seg + row] - 46) : 0.0;
-                const double sbl = cok ? pow2(__ldg(pb.eb + sg * pb.eb_seg + colw)) : 0.0;
+                const double sa = rok ? pow2(ea_v - 46) : 0.0;
+                const double sbl = cok ? pow2(eb_v) : 0.0;
                 const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * OZ_ACC_STRIDE);
 #pragma unroll
                 for (int c8 = 0; c8 < OZ_EPI_COLS; c8 += 8) {
@@ -436,36 +440,49 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(const OzSplitJob* __re
 }
 
 // Split of a job whose rows are contiguous (sk != 1; the transposed operands
-// s2a11^T, p2b^T): one thread per row.  A warp's loads cover 32 consecutive
-// rows of one k; each thread packs the digits of 16 consecutive k into one
-// 16-byte chunk per digit plane, and a warp's chunks are 512 contiguous bytes
-// of the tiled layout.  No shared memory and no barriers: every thread keeps
-// 16 loads in flight.
+// s2a11^T, p2b^T): 64 rows per CTA, four threads per row taking every fourth
+// k (pass 1) and every fourth 16-wide K chunk (pass 2).  A warp is 32
+// consecutive rows of one K lane, so its loads cover 256 contiguous bytes; each
+// thread packs the digits of 16 consecutive k into one 16-byte chunk per digit
+// plane, and a warp's chunks are 512 contiguous bytes of the tiled layout.  A
+// CTA reads its 64 x K block twice (maxima, then digits); the blocks of all
+// resident CTAs fit in L2, so the second pass does not go back to HBM.
 constexpr int OZ_ROWS_THREADS = 256;
+constexpr int OZ_ROWS_PER_CTA = 64;
+constexpr int OZ_KLANES = OZ_ROWS_THREADS / OZ_ROWS_PER_CTA;
 
 __global__ void __launch_bounds__(OZ_ROWS_THREADS) ozaki_split_rows_kernel(const OzSplitJob* __restrict__ jobs) {
     const OzSplitJob& jb = jobs[blockIdx.y];
     if (jb.sk == 1) return;   // ozaki_split_kernel
-    const int r = blockIdx.x * OZ_ROWS_THREADS + threadIdx.x;
-    if (r >= jb.nrt * jb.H) return;
-    const bool live = r < jb.R;   // rows R .. nrt*H - 1 are padding: zero digits
+    const int r0 = blockIdx.x * OZ_ROWS_PER_CTA;
+    if (r0 >= jb.nrt * jb.H) return;
+    __shared__ double red[OZ_KLANES][OZ_ROWS_PER_CTA];
+    const int lrow = threadIdx.x % OZ_ROWS_PER_CTA, kl = threadIdx.x / OZ_ROWS_PER_CTA;
+    const int r = r0 + lrow;
+    const bool pad = r >= jb.nrt * jb.H;   // past the last row tile: no work
+    const bool live = r < jb.R;            // rows R .. nrt*H - 1 are padding: zero digits
     const long sk = jb.sk;
     const int K = jb.K;
     const double* __restrict__ xr = jb.X + (long)(live ? r : 0) * jb.sr;
     double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
     if (live) {
-        int k = 0;
-        for (; k + 3 < K; k += 4) {
+        int k = kl;
+        for (; k + 3 * OZ_KLANES < K; k += 4 * OZ_KLANES) {
             m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
-            m1 = fmax(m1, fabs(__ldg(xr + (k + 1) * sk)));
-            m2 = fmax(m2, fabs(__ldg(xr + (k + 2) * sk)));
-            m3 = fmax(m3, fabs(__ldg(xr + (k + 3) * sk)));
+            m1 = fmax(m1, fabs(__ldg(xr + (k + OZ_KLANES) * sk)));
+            m2 = fmax(m2, fabs(__ldg(xr + (k + 2 * OZ_KLANES) * sk)));
+            m3 = fmax(m3, fabs(__ldg(xr + (k + 3 * OZ_KLANES) * sk)));
         }
-        for (; k < K; ++k) m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
+        for (; k < K; k += OZ_KLANES) m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
     }
-    const double mx = fmax(fmax(m0, m1), fmax(m2, m3));
+    red[kl][lrow] = fmax(fmax(m0, m1), fmax(m2, m3));
+    __syncthreads();
+    double mx = red[0][lrow];
+#pragma unroll
+    for (int i = 1; i < OZ_KLANES; ++i) mx = fmax(mx, red[i][lrow]);
+    if (pad) return;
     const int ex = (mx > 0.0) ? ilogb(mx) + 2 : 0;   // digits of the integer rint(x 2^(39-e))
-    if (live) jb.e[r] = ex;
+    if (live && kl == 0) jb.e[r] = ex;
     const int sh = 39 - ex;
     const bool direct = (sh <= 1023 && sh >= -1022);
     const double sc = direct ? pow2(sh) : 1.0;
@@ -473,30 +490,28 @@ __global__ void __launch_bounds__(OZ_ROWS_THREADS) ozaki_split_rows_kernel(const
     const long blk = (long)OZ_S * jb.H * OZ_BK;
     const int kstride = jb.kstride > 0 ? jb.kstride : jb.nks;
 #pragma unroll 1
-    for (int ks = 0; ks < jb.nks; ++ks) {
-        int8_t* base = jb.out + ((long)rt * kstride + jb.ks0 + ks) * blk + (long)rin * 16;
+    for (int ch = kl; ch < 2 * jb.nks; ch += OZ_KLANES) {   // 16-wide K chunk ch = (K-step, half)
+        const int ks = ch >> 1, kc = ch & 1;
+        const int k0 = ch * 16;
+        double v[16];
 #pragma unroll
-        for (int kc = 0; kc < 2; ++kc) {
-            const int k0 = ks * OZ_BK + kc * 16;
-            double v[16];
+        for (int i = 0; i < 16; ++i) v[i] = (live && k0 + i < K) ? __ldg(xr + (long)(k0 + i) * sk) : 0.0;
+        unsigned w[OZ_S][4];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = (live && k0 + i < K) ? __ldg(xr + (long)(k0 + i) * sk) : 0.0;
-            unsigned w[OZ_S][4];
+        for (int s = 0; s < OZ_S; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
 #pragma unroll
-            for (int s = 0; s < OZ_S; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
+        for (int i = 0; i < 16; ++i) {
+            const double a = direct ? v[i] * sc : ldexp(v[i], sh);
+            int8_t qd[OZ_S];
+            oz_digits(__double2ll_rn(a), qd);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const double a = direct ? v[i] * sc : ldexp(v[i], sh);
-                int8_t qd[OZ_S];
-                oz_digits(__double2ll_rn(a), qd);
-#pragma unroll
-                for (int s = 0; s < OZ_S; ++s) w[s][i >> 2] |= (unsigned)(uint8_t)qd[s] << (8 * (i & 3));
-            }
-#pragma unroll
-            for (int s = 0; s < OZ_S; ++s)
-                *reinterpret_cast<int4*>(base + (long)s * jb.H * OZ_BK + (long)kc * jb.H * 16) =
-                    make_int4((int)w[s][0], (int)w[s][1], (int)w[s][2], (int)w[s][3]);
+            for (int s = 0; s < OZ_S; ++s) w[s][i >> 2] |= (unsigned)(uint8_t)qd[s] << (8 * (i & 3));
         }
+        int8_t* base = jb.out + ((long)rt * kstride + jb.ks0 + ks) * blk + (long)kc * jb.H * 16 + (long)rin * 16;
+#pragma unroll
+        for (int s = 0; s < OZ_S; ++s)
+            *reinterpret_cast<int4*>(base + (long)s * jb.H * OZ_BK) =
+                make_int4((int)w[s][0], (int)w[s][1], (int)w[s][2], (int)w[s][3]);
     }
 }
 
@@ -515,7 +530,7 @@ void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows, int 
         ++c.launches;
     }
     if (kinds & OZ_SPLIT_ROWS) {
-        dim3 grid((max_rows + OZ_ROWS_THREADS - 1) / OZ_ROWS_THREADS, njobs);
+        dim3 grid((max_rows + OZ_ROWS_PER_CTA - 1) / OZ_ROWS_PER_CTA, njobs);
         ozaki_split_rows_kernel<<<grid, OZ_ROWS_THREADS, 0, c.stream>>>(d_jobs);
         RA_CUDA(cudaGetLastError());
         ++c.launches;
@@ -682,8 +697,8 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
     oz_static_prepare_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(pr, ja, jbj, d_prob, d_jobs, d_tiles, ntm, ntn,
                                                                      d_status);
     ozaki_split_kernel<<<dim3((std::max(mp, np) + 15) / 16, 2), 256, 0, st>>>(d_jobs);
-    ozaki_split_rows_kernel<<<dim3((std::max(mp, np) + OZ_ROWS_THREADS - 1) / OZ_ROWS_THREADS, 2), OZ_ROWS_THREADS, 0,
-                              st>>>(d_jobs);
+    ozaki_split_rows_kernel<<<dim3((std::max(mp, np) + OZ_ROWS_PER_CTA - 1) / OZ_ROWS_PER_CTA, 2), OZ_ROWS_THREADS,
+                              0, st>>>(d_jobs);
     e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem));
     if (e == cudaSuccess) {
         ozaki_gemm_kernel<<<std::min(ntiles, nsm), OZ_THREADS, sizeof(OzSmem), st>>>(d_prob, d_tiles, ntiles, d_status);

@@ -32,25 +32,32 @@ __device__ __forceinline__ int ell_of_lm(long lm) {
 // Chebyshev synthesis of the 12 grid outputs (W W' W'' W''' P P' T T' T'' Z Z' Z'')
 // ---------------------------------------------------------------------------
 
-// One CTA per (field, 64-column tile): the tile's retained Chebyshev
-// coefficients are staged in shared memory once, split by parity, and every
-// derivative order of the field is synthesised from them.  D(n_r - 1 - r, k) =
-// (-1)^(k+d) D(r, k), so rows r < n_r/2 give both halves of the grid:
+// One CTA per (field, 64-column tile).  D(n_r - 1 - r, k) = (-1)^(k+d) D(r, k),
+// so rows r < n_r/2 give both halves of the grid:
 //   g(r) = E + O,  g(n_r - 1 - r) = (-1)^d (E - O),
 // E / O the products over even / odd k.  Dpar[d][par][r][k'] = D_d(r, 2k' + par).
+// Per (derivative order, 64-row block) the CTA computes E, parks it in shared
+// memory (each thread its own accumulator slots, so no barrier), computes O in
+// the same registers and writes both halves.  The coefficients stream through
+// the tile engine's own double-buffered stage from L2: one accumulator and no
+// coefficient stage keep a CTA at about 67 KB of shared memory and under 128
+// registers, three CTAs per SM.
 struct ChebField { int o0, nd, var; };
 __constant__ ChebField kChebField[4] = {{G_W0, 4, 0}, {G_P0, 2, 1}, {G_T0, 3, 2}, {G_Z0, 3, 3}};
 
-__global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const double* __restrict__ Dpar,
-                                                                      const double* __restrict__ sol_wpt,
-                                                                      const double* __restrict__ sol_z,
-                                                                      double* __restrict__ g, int nr, int kc,
-                                                                      long ncols) {
+struct ChebSmem {
+    GemmSmem g;
+    double park[32][GEMM_THREADS];   // E of the thread's 32 accumulator slots
+};
+
+__global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const double* __restrict__ Dpar,
+                                                                         const double* __restrict__ sol_wpt,
+                                                                         const double* __restrict__ sol_z,
+                                                                         double* __restrict__ g, int nr, int kc,
+                                                                         long ncols) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
-    const int kh = (kc + 1) / 2;                                         // coefficients per parity
-    constexpr int BS = BN + 1;                                           // padded row: conflict-free staging
-    double* Bs = reinterpret_cast<double*>(smem_raw + sizeof(GemmSmem));   // [par][kh][BS]
+    ChebSmem& sm = *reinterpret_cast<ChebSmem*>(smem_raw);
+    const int kh = (kc + 1) / 2;   // coefficients per parity (the odd plane has one fewer when kc is odd)
     const ChebField cf = kChebField[blockIdx.y];
     const long c0 = (long)blockIdx.x * BN;
     const int nr2 = nr / 2;
@@ -63,35 +70,39 @@ __global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const doub
         src = sol_z;
         cstride = nr;
     }
-    // stage the coefficients (k < kc) of the 64 columns, coalesced along k
-    for (int e = threadIdx.x; e < BN * kc; e += GEMM_THREADS) {
-        const int y = e / kc, k = e - y * kc;
-        const long col = c0 + y;
-        Bs[((k & 1) * kh + (k >> 1)) * BS + y] = (col < ncols) ? __ldg(src + col * cstride + k) : 0.0;
-    }
-    if (kc & 1)   // the odd-parity plane has one coefficient fewer
-        for (int y = threadIdx.x; y < BN; y += GEMM_THREADS) Bs[(kh + kh - 1) * BS + y] = 0.0;
-    __syncthreads();
+    const int t = threadIdx.x;
     for (int dd = 0; dd < cf.nd; ++dd) {
         const int o = cf.o0 + dd;
         const double sgn = (dd & 1) ? -1.0 : 1.0;
         double* out = g + (long)o * ncols * nr;
         for (int r0 = 0; r0 < nr2; r0 += BM) {
-            Acc ae, ao;
-            ae.zero();
-            ao.zero();
+            Acc acc;
 #pragma unroll 1
             for (int par = 0; par < 2; ++par) {
                 const double* Dp = Dpar + (((long)dd * 2 + par) * nr2) * kh;
-                const double* Bp = Bs + (long)par * kh * BS;
                 auto fa = [&](int k, int x) -> double {
                     const int r = r0 + x;
                     return (k < kh && r < nr2) ? __ldg(Dp + (long)r * kh + k) : 0.0;
                 };
-                auto fb = [&](int k, int y) -> double { return (k < kh) ? Bp[k * BS + y] : 0.0; };
-                gemm_tile<false, true>(par ? ao : ae, fa, fb, kh, sm);
+                auto fb = [&](int k, int y) -> double {   // coefficient 2k + par of column c0 + y
+                    const long col = c0 + y;
+                    const int kk = 2 * k + par;
+                    return (kk < kc && col < ncols) ? __ldg(src + col * cstride + kk) : 0.0;
+                };
+                acc.zero();
+                gemm_tile<false, false>(acc, fa, fb, kh, sm.g);
+                if (par == 0) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+#pragma unroll
+                            for (int q = 0; q < 2; ++q) sm.park[(i * 4 + j) * 2 + q][t] = acc.v[i][j][q];
+                }
             }
-            acc_foreach2(ae, ao, [&](int x, int y, double e, double od) {
+            int slot = 0;
+            acc_foreach(acc, [&](int x, int y, double od) {
+                const double e = sm.park[slot++][t];
                 const int r = r0 + x;
                 const long col = c0 + y;
                 if (r < nr2 && col < ncols) {
@@ -105,11 +116,10 @@ __global__ void __launch_bounds__(GEMM_THREADS) cheb_synthesis_kernel(const doub
 
 void launch_cheb_synthesis(Ctx& c) {
     const long ncols = 2 * c.d.nlm;
-    const int kh = (c.d.kc + 1) / 2;
-    const size_t smem = sizeof(GemmSmem) + (size_t)2 * kh * (BN + 1) * sizeof(double);
+    const size_t smem = sizeof(ChebSmem);
     static bool attr = false;
     if (!attr) {
-        RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     dim3 grid((unsigned)((ncols + BN - 1) / BN), 4);

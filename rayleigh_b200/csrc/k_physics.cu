@@ -261,6 +261,30 @@ __host__ __device__ constexpr int ip_tw_off(int n, int ps) {
 }
 __host__ __device__ constexpr int ip_tw_size(int n) { return ip_tw_off(n, npass_of(n)); }
 
+// Twiddles w[k] = exp(2 pi i j k / LS), k = 1 .. R-1, of butterfly j: the
+// table's w^j, the others by complex products (at most three deep, a few
+// units in the last place), so a butterfly makes one table load.
+template <int R, int SS>
+__device__ __forceinline__ void pass_twiddles(const double2* __restrict__ tw, int j, double2 (&w)[R]) {
+    w[0] = make_double2(1.0, 0.0);
+    w[1] = __ldg(tw + j);
+    if constexpr (R == 8) {
+        w[2] = cmul(w[1], w[1]);
+        w[4] = cmul(w[2], w[2]);
+        w[3] = cmul(w[2], w[1]);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    } else if constexpr (R == 4) {
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+    } else if constexpr (R == 3) {
+        w[2] = cmul(w[1], w[1]);
+    } else {
+        static_assert(R == 2, "radix");
+    }
+}
+
 template <int N, int NB, int NT, int PS, bool DIT>
 __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const double2* __restrict__ twp, int sign,
                                             int tid) {
@@ -273,18 +297,22 @@ __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const dou
         double2 u[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) u[m] = buf[SW(base + m * SS)];
+        double2 w[R];   // w[k] = exp(2 pi i j k / LS), conjugated for the r2c
+        if constexpr (SS > 1) {
+            pass_twiddles<R, SS>(tw, j, w);
+            if (DIT) {
+#pragma unroll
+                for (int k = 1; k < R; ++k) w[k].y = -w[k].y;
+            }
+        }
         if (SS > 1 && DIT) {
 #pragma unroll
-            for (int m = 1; m < R; ++m) {
-                double2 w = __ldg(tw + (m - 1) * SS + j);
-                w.y = -w.y;
-                u[m] = cmul(u[m], w);
-            }
+            for (int m = 1; m < R; ++m) u[m] = cmul(u[m], w[m]);
         }
         dft_small(R, u, sign);
         if (SS > 1 && !DIT) {
 #pragma unroll
-            for (int k = 1; k < R; ++k) u[k] = cmul(u[k], __ldg(tw + (k - 1) * SS + j));
+            for (int k = 1; k < R; ++k) u[k] = cmul(u[k], w[k]);
         }
 #pragma unroll
         for (int m = 0; m < R; ++m) buf[SW(base + m * SS)] = u[m];
@@ -394,8 +422,9 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
             const int g = t + (q0 + qq) * ROW_THREADS;
             if (q0 + qq < QI && g < NB * NI) {
                 const int k = g / NB, b = g - k * NB;
-                buf[SW(b * FS + k)] = zform(xk[qq], xn[qq], __ldg(P.wr + k));
-                if (k != 0 && 2 * k != N) buf[SW(b * FS + N - k)] = zform(xn[qq], xk[qq], __ldg(P.wr + N - k));
+                const double2 wk = __ldg(P.wr + k);   // w^(N-k) = -conj(w^k), w = exp(2 pi i / 2N)
+                buf[SW(b * FS + k)] = zform(xk[qq], xn[qq], wk);
+                if (k != 0 && 2 * k != N) buf[SW(b * FS + N - k)] = zform(xn[qq], xk[qq], make_double2(-wk.x, wk.y));
             }
         }
     }
@@ -570,17 +599,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             const int f = g / NI, k = g - f * NI;
             const double2 zk = acc[SW(f * FS + k)];
             const double2 zn = acc[SW(f * FS + (N - k) % N)];
-            auto xval = [&](double2 a, double2 b, int kk) {   // X_kk from Z_kk = a, Z_{N-kk} = b
+            const double2 wk = __ldg(P.wr + k);   // w^(N-k) = -conj(w^k)
+            auto xval = [&](double2 a, double2 b, double2 w, bool zero_im) {   // X from Z_kk = a, Z_{N-kk} = b
                 const double2 bn = cconj(b);
                 const double2 e = make_double2(0.5 * (a.x + bn.x), 0.5 * (a.y + bn.y));
                 const double2 d = make_double2(0.5 * (a.x - bn.x), 0.5 * (a.y - bn.y));
-                const double2 wd = cmul(cconj(__ldg(P.wr + kk)), d);
+                const double2 wd = cmul(cconj(w), d);
                 double2 X = make_double2(e.x + wd.y, e.y - wd.x);
-                if (kk == 0) X.y = 0.0;
+                if (zero_im) X.y = 0.0;
                 return X;
             };
-            if (k < L) acc[SW(f * FS + k)] = xval(zk, zn, k);
-            if (k != 0 && 2 * k != N && N - k < L) acc[SW(f * FS + N - k)] = xval(zn, zk, N - k);
+            if (k < L) acc[SW(f * FS + k)] = xval(zk, zn, wk, k == 0);
+            if (k != 0 && 2 * k != N && N - k < L)
+                acc[SW(f * FS + N - k)] = xval(zn, zk, make_double2(-wk.x, wk.y), false);
         }
     }
     // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122) with the

@@ -379,8 +379,15 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     for k, ms in per_kernel.items():
         b, amt = work[k]
         sec = ms / args.steps * 1e-3
+        rate = amt / sec / (1e12 if b == "tensor" else 1e9)
         kernels[k] = {"ms_per_step": round(ms / args.steps, 4), "share": round(ms / total_ms, 4),
-                      ("tflops" if b == "tensor" else "gbs"): round(amt / sec / (1e12 if b == "tensor" else 1e9), 2)}
+                      ("tflops" if b == "tensor" else "gbs"): round(rate, 2)}
+        # fraction of the measured peak: HBM copy for byte-bound kernels; for the FP64
+        # form's products, the cuBLAS DGEMM rate (FP64 tensor pipe) of this run
+        if b != "tensor":
+            kernels[k]["frac_of_hbm"] = round(rate / peaks["hbm_gbs"], 3)
+        elif prec_name == "fp64" and fp64_peak:
+            kernels[k]["frac_of_dgemm"] = round(rate / fp64_peak, 3)
     fields = {
         "value": value, "ms_per_step": max_ms / args.steps, "precision": prec_name,
         "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
@@ -426,7 +433,7 @@ def run_ours(args, rank, world, torch, dist):
     line = {"metric": METRIC, "value": head["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "precision": head_form,
-            "data": "synthetic (seeded)"}
+            "data": "synthetic (seeded)", "fp64_dgemm_tflops": fp64_peak}
     for k in ("config", "roofline", "kernels", "gpu_launches", "clocks", "e2e"):
         line[k] = head[k]
     if len(res) == 2:

@@ -16,16 +16,19 @@
 // The product kernel is persistent (one CTA per SM, tiles dealt round-robin
 // from a list ordered longest-K first) and warp-specialised:
 //   warp 0      producer: one bulk copy (cp.async.bulk, no multicast) per
-//               operand per K-step into a 6-stage shared-memory ring;
+//               operand per K-step into a shared-memory ring of OZ_NST stages;
 //   warp 1      MMA issuer: 15 tcgen05.mma per K-step, committed to the
 //               stage's "empty" barrier and, after the last K-step, to the
 //               accumulator's "full" barrier;
 //   warps 2-13  epilogue: three warps per TMEM lane quadrant, each taking a
 //               third of the tile's columns: tcgen05.ld of the 5 diagonals (one
 //               wait per 8 columns), exact int64 recombination, scaled stores.
-// Output tiles are 128 x 48, so two accumulator sets (2 x 5 x 48 columns)
-// fit in tensor memory and the epilogue of one tile overlaps the MMAs of the
-// next.  Every wait is bounded: when a limit runs out the CTA raises the
+// Output tiles are 128 x 96: one accumulator set of 5 x 96 of the 512
+// tensor-memory columns.  A 96-wide tile reads each A K-step once for 96
+// output columns (the operands stream from L2 and bound the kernel), at the
+// price of the next tile's MMAs waiting while the epilogue reads the set out
+// of tensor memory (the stores and the FP64 sum over segments come after the
+// set is released).  Every wait is bounded: when a limit runs out the CTA raises the
 // device error word, drains its own copies and MMAs (bounded again), frees
 // its tensor memory and returns.
 #include <cstdint>
@@ -37,24 +40,27 @@
 
 namespace ra {
 
-constexpr int OZ_NST = 8;   // operand ring stages: about 1.8 tiles of the longest-K products ahead of the MMAs
+constexpr int OZ_STAGE = OZ_ABLK + OZ_BBLK;  // 35840 bytes
+constexpr int OZ_NST = (232448 - 1024) / OZ_STAGE;   // operand ring stages that fit in 227 KB (6)
 constexpr int OZ_EPI_WARPS = 12;                           // three per TMEM lane quadrant
 constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
-constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (16)
+constexpr int OZ_EPI_COLS = OZ_HB / (OZ_EPI_WARPS / 4);   // columns per epilogue warp (32)
 static_assert(OZ_EPI_COLS % 8 == 0 && OZ_EPI_COLS <= 32, "epilogue column split");
-constexpr int OZ_ACC_STRIDE = 256;           // TMEM columns between the two accumulator sets
 constexpr int OZ_TMEM_COLS = 512;
-constexpr int OZ_STAGE = OZ_ABLK + OZ_BBLK;  // 28160 bytes
+// accumulator sets in tensor memory (two when 2 x 5 x HB columns fit, at a 256-column stride)
+constexpr int OZ_NACC = (2 * OZ_S * OZ_HB <= OZ_TMEM_COLS) ? 2 : 1;
+constexpr int OZ_ACC_STRIDE = 256;
+static_assert(OZ_NACC == 2 ? OZ_S * OZ_HB <= OZ_ACC_STRIDE : OZ_S * OZ_HB <= OZ_TMEM_COLS,
+              "accumulator sets exceed tensor memory");
 constexpr long OZ_SPIN_LIMIT = 1L << 25;     // bounded waits: ~seconds, then the error word is set
-static_assert(OZ_S * OZ_HB <= OZ_ACC_STRIDE, "accumulator set exceeds its tensor-memory half");
 static_assert(OZ_STAGE % 128 == 0, "stage size");
 
 struct OzSmem {
     alignas(128) int8_t stage[OZ_NST][OZ_STAGE];
     alignas(8) uint64_t full[OZ_NST];
     uint64_t empty[OZ_NST];
-    uint64_t acc_full[2];
-    uint64_t acc_empty[2];
+    uint64_t acc_full[OZ_NACC];
+    uint64_t acc_empty[OZ_NACC];
     uint64_t drain;
     uint32_t tmem_base;
     int abort;
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
             mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < OZ_NACC; ++b) {
             mbar_init(&sm.acc_full[b], 1);
             mbar_init(&sm.acc_empty[b], OZ_EPI_WARPS);
         }
@@ -240,8 +246,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
             if (t + (int)gridDim.x < ntiles) tw_n = tiles[t + gridDim.x].w;
             const int kseg = nks / nseg;
             for (int sg = 0; sg < nseg && ok; ++sg, ++tl_i) {
-                const int buf = tl_i & 1;
-                const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+                const int buf = tl_i % OZ_NACC;
+                const uint32_t aph = (uint32_t)(tl_i / OZ_NACC) & 1u;
                 ok = __all_sync(0xffffffffu, mbar_wait(&sm.acc_empty[buf], aph ^ 1u));
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t dacc = tmem + (uint32_t)(buf * OZ_ACC_STRIDE);
@@ -305,8 +311,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
 #pragma unroll
             for (int j = 0; j < OZ_EPI_COLS; ++j) part[j] = 0.0;
             for (int sg = 0; sg < nseg; ++sg, ++tl_i) {
-                const int buf = tl_i & 1;
-                const uint32_t aph = (uint32_t)(tl_i >> 1) & 1u;
+                const int buf = tl_i % OZ_NACC;
+                const uint32_t aph = (uint32_t)(tl_i / OZ_NACC) & 1u;
                 // row scale with the combined weight 2^-46 of S below folded in; the
                 // column scales of this warp's columns, one per lane, shared by shuffle
                 // (loaded before the wait for the accumulator, which hides their latency)

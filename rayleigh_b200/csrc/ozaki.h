@@ -12,7 +12,7 @@ constexpr int OZ_S = 5;   // balanced base-256 int8 digits per operand (15 digit
 // int32 accumulators stay exact while K * 128^2 * OZ_S < 2^31
 constexpr int OZ_MAX_K = 20000;
 constexpr int OZ_HA = 128;   // rows of an A tile (output rows, TMEM lanes)
-constexpr int OZ_HB = 48;    // rows of a B^T tile (output columns)
+constexpr int OZ_HB = 96;    // rows of a B^T tile (output columns)
 constexpr int OZ_BK = 32;    // K per MMA step (int8)
 constexpr int OZ_ABLK = OZ_S * OZ_HA * OZ_BK;   // bytes of one K-step of an A row tile, all digits
 constexpr int OZ_BBLK = OZ_S * OZ_HB * OZ_BK;   // same for B

@@ -393,6 +393,8 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
         "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
                    "n_r": args.nr, "n_theta": n_theta, "n_phi": n_phi, "ekman": cfgd["ekman"],
                    "dt": cfgd["dt"], "l2": "working set (~35 GB) larger than L2; no flush needed",
+                   "equation_set": "hydrodynamic (W, P, T, Z) on the dynamo case's grid; the magnetic "
+                                   "fields C, A of the dynamo case are not built",
                    "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                      "frac": achieved / peak if peak else None, "traffic": traffic, "peak_source": peak_note},

@@ -32,21 +32,22 @@ __device__ __forceinline__ int ell_of_lm(long lm) {
 // Chebyshev synthesis of the 12 grid outputs (W W' W'' W''' P P' T T' T'' Z Z' Z'')
 // ---------------------------------------------------------------------------
 
-// One CTA per (field, 64-column tile).  D(n_r - 1 - r, k) = (-1)^(k+d) D(r, k),
+// One CTA per (field, 128-column tile).  D(n_r - 1 - r, k) = (-1)^(k+d) D(r, k),
 // so rows r < n_r/2 give both halves of the grid:
 //   g(r) = E + O,  g(n_r - 1 - r) = (-1)^d (E - O),
 // E / O the products over even / odd k.  Dpar[d][par][r][k'] = D_d(r, 2k' + par).
-// Per (derivative order, 64-row block) the CTA computes E, parks it in shared
-// memory (each thread its own accumulator slots, so no barrier), computes O in
-// the same registers and writes both halves.  The coefficients stream through
-// the tile engine's own double-buffered stage from L2: one accumulator and no
-// coefficient stage keep a CTA at about 67 KB of shared memory and under 128
-// registers, three CTAs per SM.
+// Per (derivative order, 32-row block: the n_r/2 = 96 half-grid rows in three
+// full blocks) the CTA computes E, parks it in shared memory (each thread its
+// own accumulator slots, so no barrier), computes O in the same registers and
+// writes both halves.  The coefficients stream through the tile engine's own
+// double-buffered stage from L2: one accumulator and no coefficient stage keep
+// a CTA at about 75 KB of shared memory and 168 registers, three CTAs per SM.
 struct ChebField { int o0, nd, var; };
 __constant__ ChebField kChebField[4] = {{G_W0, 4, 0}, {G_P0, 2, 1}, {G_T0, 3, 2}, {G_Z0, 3, 3}};
 
+using ChebShape = Wide;   // 32 x 128 tiles: 32-row blocks cover the n_r/2 = 96 half-grid rows exactly
 struct ChebSmem {
-    GemmSmem g;
+    GemmSmemT<1, 4> g;
     double park[32][GEMM_THREADS];   // E of the thread's 32 accumulator slots
 };
 
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
     ChebSmem& sm = *reinterpret_cast<ChebSmem*>(smem_raw);
     const int kh = (kc + 1) / 2;   // coefficients per parity (the odd plane has one fewer when kc is odd)
     const ChebField cf = kChebField[blockIdx.y];
-    const long c0 = (long)blockIdx.x * BN;
+    const long c0 = (long)blockIdx.x * ChebShape::BN;
     const int nr2 = nr / 2;
     const double* src;
     long cstride;
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
         const int o = cf.o0 + dd;
         const double sgn = (dd & 1) ? -1.0 : 1.0;
         double* out = g + (long)o * ncols * nr;
-        for (int r0 = 0; r0 < nr2; r0 += BM) {
+        for (int r0 = 0; r0 < nr2; r0 += ChebShape::BM) {
             Acc acc;
 #pragma unroll 1
             for (int par = 0; par < 2; ++par) {
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
                     return (kk < kc && col < ncols) ? __ldg(src + col * cstride + kk) : 0.0;
                 };
                 acc.zero();
-                gemm_tile<false, false>(acc, fa, fb, kh, sm.g);
+                gemm_tile<false, false, 1, 4>(acc, fa, fb, kh, sm.g);
                 if (par == 0) {
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
                 }
             }
             int slot = 0;
-            acc_foreach(acc, [&](int x, int y, double od) {
+            acc_foreach<1, 4>(acc, [&](int x, int y, double od) {
                 const double e = sm.park[slot++][t];
                 const int r = r0 + x;
                 const long col = c0 + y;
@@ -122,7 +123,7 @@ void launch_cheb_synthesis(Ctx& c) {
         RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    dim3 grid((unsigned)((ncols + BN - 1) / BN), 4);
+    dim3 grid((unsigned)((ncols + ChebShape::BN - 1) / ChebShape::BN), 4);
     cheb_synthesis_kernel<<<grid, GEMM_THREADS, smem, c.stream>>>(c.d_Dpar, c.d_sol_wpt, c.d_sol_z, c.d_g, c.d.nr,
                                                                    c.d.kc, ncols);
     RA_CUDA(cudaGetLastError());

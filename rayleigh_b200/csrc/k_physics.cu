@@ -11,15 +11,21 @@
 // between these steps; here the 18 phi rows of one (r, theta) point never
 // leave the SM.
 //
-// One CTA (256 threads, two per SM) handles one row; the rows theta and
+// One CTA (384 threads, two per SM) handles one row; the rows theta and
 // pi - theta are the two CTAs of a cluster, which fold their spectra through
-// distributed shared memory.  The 14 input fields go through the FFT two at a
+// distributed shared memory.  The 14 input fields go through the FFT four at a
 // time; the four nonlinear outputs accumulate in shared memory (each thread
-// owns its points), the velocity in registers.
+// owns its points), the velocity in registers, the row's radial and
+// colatitude factors in shared memory.
 //
 // FFT: a real length-2N transform through one complex length-N transform
-// (N = n_theta = 2^a 3^b), Stockham autosort, radix 8/4/2/3, in shared memory;
-// unnormalised like FFTW (the normalisation lives in the Legendre tables).
+// (N = n_theta = 2^a 3^b), in place in shared memory: decimation in frequency
+// (radix 8, 4, 2, 3 passes) for the c2r, which leaves the physical points in
+// a digit-reversed order; the nonlinear terms are pointwise in phi, so they
+// are formed in that order, and the r2c runs the passes in reverse
+// (decimation in time) back to natural order.  One twiddle table load per
+// butterfly, the other powers by complex products.  Unnormalised like FFTW
+// (the normalisation lives in the Legendre tables).
 #include <cmath>
 #include <vector>
 #include <algorithm>
@@ -242,7 +248,7 @@ struct RowSmem {
     static constexpr int SIZE = ACC + 4 * FS;
 };
 
-// In-place mixed-radix FFT passes (field f at f*FS, swizzled).  Pass s:
+// In-place mixed-radix FFT passes (field f at f*FS).  Pass s:
 // sub-transform length LS = N / (R_0 ... R_{s-1}), radix R = R_s, stride
 // SS = LS / R; butterfly (b, j) takes the elements b*LS + j + m*SS.
 // Decimation in frequency (c2r, sign +1): DFT_R, then twiddle w_LS^{jk}; after

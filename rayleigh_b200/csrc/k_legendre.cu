@@ -182,13 +182,19 @@ static std::vector<int> forward_tiles(int L) {
     return t;
 }
 
-void launch_lt_forward(Ctx& c, const double* p2, double* s2, int ncol) {
+// The forward transform's tile list, built once at set-up (no allocation may
+// run while the step is captured into a graph).
+void lt_forward_prepare(Ctx& c) {
     if (!c.d_fwd_tiles) {
         std::vector<int> t = forward_tiles(c.d.L);
         c.n_fwd_tiles = (int)(t.size() / 4);
         RA_CUDA(cudaMalloc(&c.d_fwd_tiles, t.size() * sizeof(int)));
         RA_CUDA(cudaMemcpy(c.d_fwd_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
+}
+
+void launch_lt_forward(Ctx& c, const double* p2, double* s2, int ncol) {
+    if (!c.d_fwd_tiles) throw ArgError("forward-transform tiles not prepared (lt_forward_prepare runs at set-up)");
     dim3 grid((ncol + BN - 1) / BN, c.n_fwd_tiles);
     lt_forward_kernel<<<grid, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
         c.d_iPtab, p2, s2, reinterpret_cast<const int4*>(c.d_fwd_tiles), c.d.L, c.d.nth, ncol);

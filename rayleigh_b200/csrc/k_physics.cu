@@ -660,14 +660,12 @@ FFTPlan make_plan(int n) {
     return p;
 }
 
-void launch_physics(Ctx& c) {
-    PhysParams P{};
-    P.p2a = c.d_p2a;
-    P.p2b = c.d_p2b;
-    P.radial = c.d_radial;
-    P.trig = c.d_costh;
-    P.wr = reinterpret_cast<const double2*>(c.d_twid);
-    if (!c.d_twp) {   // per-pass twiddles exp(2 pi i j k / LS) of the in-place FFT (long double)
+// Per-pass twiddles exp(2 pi i j k / LS) of the in-place FFT, in long
+// double, built once at set-up: the step may be captured into a CUDA graph on
+// its first launch (a context restored at a later iteration), where no
+// allocation or blocking copy may run.
+void physics_prepare(Ctx& c) {
+    if (!c.d_twp) {
         const int n = c.d.nth;
         std::vector<double> tw(2 * (size_t)ip_tw_size(n));
         const long double PI = 3.141592653589793238462643383279502884L;
@@ -683,6 +681,16 @@ void launch_physics(Ctx& c) {
         RA_CUDA(cudaMalloc(&c.d_twp, std::max<size_t>(tw.size(), 2) * sizeof(double)));
         RA_CUDA(cudaMemcpy(c.d_twp, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
+}
+
+void launch_physics(Ctx& c) {
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.p2b = c.d_p2b;
+    P.radial = c.d_radial;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
     P.cfl = c.d_cfl;
     P.L = c.d.L;

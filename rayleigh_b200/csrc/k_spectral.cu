@@ -486,13 +486,19 @@ static std::vector<int> solve_tiles(int L, int nr) {
     return t;
 }
 
-void launch_solve(Ctx& c) {
+// The solve's tile list, built once at set-up (no allocation may run while
+// the step is captured into a graph).
+void solve_prepare(Ctx& c) {
     if (!c.d_solve_tiles) {
         std::vector<int> t = solve_tiles(c.d.L, c.d.nr);
         c.n_solve_tiles = (int)(t.size() / 4);
         RA_CUDA(cudaMalloc(&c.d_solve_tiles, t.size() * sizeof(int)));
         RA_CUDA(cudaMemcpy(c.d_solve_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
+}
+
+void launch_solve(Ctx& c) {
+    if (!c.d_solve_tiles) throw ArgError("solve tiles not prepared (solve_prepare runs at set-up)");
     solve_kernel<<<c.n_solve_tiles, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
         reinterpret_cast<const int4*>(c.d_solve_tiles), c.d_Awpt, c.d_Az, c.d_rhs_wpt, c.d_rhs_z, c.d_sol_wpt,
         c.d_sol_z, c.d.nr);

@@ -425,6 +425,9 @@ static void setup(Ctx& c) {
     cudaFree(d_w);
     // kernels that need more than 48 KB of dynamic shared memory
     linear_setup(c);
+    physics_prepare(c);
+    lt_forward_prepare(c);
+    solve_prepare(c);
     if (c.cfg.precision == RA_PREC_MIXED) mixed_setup(c);
 }
 

@@ -145,6 +145,10 @@ void launch_cheb_synthesis(Ctx& c);
 void launch_post_assemble(Ctx& c, double old_ab);
 void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
+// tables the launches read, built at set-up (never inside a graph capture)
+void physics_prepare(Ctx& c);
+void lt_forward_prepare(Ctx& c);
+void solve_prepare(Ctx& c);
 void launch_rlm_b(Ctx& c, double new_ab);
 void launch_solve(Ctx& c);
 int  invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip);

@@ -198,3 +198,32 @@ def test_multi_step_parity(cfg, steps):
     errs = {k: rel_err(v, _fields(o.rhs_wpt, o.rhs_z, nr)[k]) for k, v in _fields(wg, zg, nr).items()}
     print(cfg, {k: f"{v:.2e}" for k, v in errs.items()})
     assert max(errs.values()) < TOL, errs
+
+
+@pytest.mark.parametrize("precision,tol", [(0, TOL), (1, 1e-9)])
+def test_timestep_change(precision, tol):
+    """Reset_Linear_Equations on a dt change (Sphere_Linear_Terms.F90:67-76):
+    the implicit matrices are rebuilt and inverted again (and their digits
+    split again in the mixed form), the AB2 factors of the first step after
+    the change use the unequal steps, and the replayed step graph is captured
+    again; the state then follows the oracle as before."""
+    cfg = dict(n_r=24, l_max=15, dt=2e-4, rayleigh=1e5, ekman=1e-3)
+    oc = _ocfg(cfg)
+    o = O.Oracle(oc)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    o.init_state(wpt, z)
+    g = _ctx(dict(cfg, precision=precision, use_graph=True))
+    g.put_state(wpt, z, None, iteration=1)
+    for _ in range(4):
+        o.step()
+    g.step(4)
+    o.set_dt(1.3e-4)
+    g.set_dt(1.3e-4)
+    for _ in range(4):
+        o.step()
+    g.step(4)
+    wg, zg, _ = g.get_state()
+    nr = oc.n_r
+    errs = {k: rel_err(v, _fields(o.rhs_wpt, o.rhs_z, nr)[k]) for k, v in _fields(wg, zg, nr).items()}
+    print(precision, {k: f"{v:.2e}" for k, v in errs.items()})
+    assert max(errs.values()) < tol, errs

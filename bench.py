@@ -397,7 +397,11 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
                                    "fields C, A of the dynamo case are not built",
                    "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                     "frac": achieved / peak if peak else None, "traffic": traffic, "peak_source": peak_note},
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "traffic_unit": "GB per launch (ncu dram bytes read + written)" if traffic is not None else None,
+                     "algorithmic": amount / (1e12 if bound == "tensor" else 1e9),
+                     "algorithmic_unit": "TFLOP per launch" if bound == "tensor" else "GB per launch",
+                     "peak_source": peak_note},
         "kernels": kernels,
         "gpu_launches": launches,
         "clocks": clk.summary(),

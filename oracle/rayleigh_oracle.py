@@ -749,6 +749,8 @@ class Oracle:
         cos = h.costheta[th][:, None, None]
         for k in ("vt", "vp", "dvtdr", "dvpdr", "dtdt", "dvrdt", "dvpdp", "dvtdp"):
             f[k] = f[k] * csc                                          # sintheta_div (:119-126)
+        # the velocity Benchmark_Checkup reads at this point of the step (:158-159)
+        self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
         r = self.radius[None, :, None]
         dlnrho = self.dlnrho[None, :, None]
         one_over_r = 1.0 / r
@@ -857,6 +859,50 @@ class Oracle:
                 xz = sla.lu_solve(self.lu_z[l], bz, check_finite=False)
                 self.rhs_z[s:e] = xz.T.reshape(e - s, 2, nr)
 
+    # ----- the reference's accuracy benchmark (Christensen et al. 2001, case 0) -----
+    def benchmark_init_hydro(self):
+        """Benchmark_Init_Hydro (Initial_Conditions.F90:731-787): W = P = Z = 0;
+        T(l=0) = sqrt(4 pi) (r_o r_i / r - r_i) and the real part of T(l=4, m=4) =
+        0.2 (1 - 3x^2 + 3x^4 - x^6), x = 2r - r_i - r_o, on the collocation grid,
+        then To_Spectral.  Returns (wpt, z) in the init_state layout."""
+        nr, L = self.cfg.n_r, self.cfg.l_max
+        r = self.radius
+        ri, ro = self.rmin, self.rmax
+        x = 2.0 * r - ri - ro
+        grid = np.zeros((self.n_lm, 2, nr))
+        grid[0, 0, :] = (ro * ri / r - ri) * math.sqrt(4.0 * math.pi)
+        if L >= 4:
+            grid[4 * 5 // 2 + 4, 0, :] = 0.2 * (1.0 - 3.0 * x * x + 3.0 * x ** 4 - x ** 6)
+        wpt = np.zeros((self.n_lm, 2, 3 * nr))
+        wpt[:, :, 2 * nr:] = self.cg.to_spectral(grid)
+        return wpt, np.zeros((self.n_lm, 2, nr))
+
+    def radial_integration_weights(self):
+        """Initialize_Cheby_Grid's integration_weights (Chebyshev_Polynomials.F90:165-194):
+        3 pi scaling / ((r_o^3 - r_i^3) N) r^2 sqrt(1 - x^2), halved at the two end
+        points; they sum to ~1 (a volume average over the shell)."""
+        cg, n = self.cg, self.cfg.n_r
+        scaling = (self.rmax - self.rmin) / (cg.x[0] - cg.x[n - 1])
+        int_scale = 3.0 * math.pi * scaling / ((self.rmax ** 3 - self.rmin ** 3) * n)
+        w = int_scale * self.radius ** 2 * np.sqrt(1.0 - cg.x * cg.x)
+        w[0] *= 0.5
+        w[n - 1] *= 0.5
+        return w
+
+    def benchmark_kinetic_energy(self):
+        """Benchmark_Checkup's kinetic energy (Benchmarking.F90:645-656, 733-736) of the
+        velocity the last step's physical-space stage formed: 0.5 rho |u|^2 averaged
+        over phi, over theta with the Gauss-Legendre weights / 2 (ComputeEll0,
+        Spherical_IO.F90:1350-1391) and over radius with the radial integration
+        weights (Compute_Radial_Average, :1436-1470)."""
+        vr, vt, vp, th = self.last_velocity
+        if not (isinstance(th, slice) and th == slice(None)):
+            raise ValueError("the last physical-space stage did not cover every theta row")
+        q = 0.5 * self.density[None, :, None] * (vr * vr + vt * vt + vp * vp)   # [theta, r, phi]
+        tw = (self.h.wq / 2.0).astype(np.float64)
+        ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
+        return float(np.dot(self.radial_integration_weights(), ell0))
+
     def step(self):
         """One pass of Main_Loop_Sphere (Sphere_Driver.F90:305-328) at fixed dt."""
         g = self.post_solve()
@@ -873,6 +919,16 @@ class Oracle:
         self.old_dt = self.dt
         self.iteration += 1
         return self.last_cfl
+
+
+def c2001_case0_config(n_r=48, n_theta=64):
+    """The settings benchmark_mode = 1 imposes (Benchmarking.F90:107-149: Christensen
+    et al. 2001, hydrodynamic case 0) on an n_r x n_theta grid; l_max from n_theta as
+    ProblemSize.F90:431-436 derives it (2 n_theta / 3 - 1)."""
+    return Config(n_r=n_r, l_max=(2 * n_theta) // 3 - 1, n_theta=n_theta, aspect_ratio=0.35, shell_depth=1.0,
+                  rayleigh=1.0e5, ekman=1.0e-3, prandtl=1.0, gravity_power=1.0, rotation=True,
+                  no_slip_top=True, no_slip_bottom=True, fix_tvar_top=True, fix_tvar_bottom=True,
+                  t_top=0.0, t_bottom=1.0, dt=1.0e-4, alpha_implicit=0.50001)
 
 
 def seeded_state(cfg: Config, seed=0x5241594C, amp=1.0e-3, lmin=1, lmax_pert=20, cheby=None):

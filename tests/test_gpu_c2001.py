@@ -1,0 +1,52 @@
+"""The reference's regression run of its accuracy benchmark, on the GPU.
+
+tests/c2001_case0 of the reference (Christensen et al. 2001 case 0 from
+Benchmark_Init_Hydro, N_r = 48, N_theta = 64, 400 steps of dt = 1e-4) reports
+the mean and standard deviation of the volume-averaged kinetic energy at
+iterations 100, 200, 300 and 400.  The CUDA path runs those steps through the
+C ABI; at each sample iteration k its state after k - 1 steps goes through one
+oracle step, whose physical-space stage forms the velocity Benchmark_Checkup
+reads, and the oracle's restatement of the benchmark's averaging gives the
+sample.  Both precision forms must reproduce the reference's report to its 6
+printed decimals."""
+import dataclasses
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_c2001_case0_reproduces_the_reference_report(precision):
+    import rayleigh_b200 as rb
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c2001_case0.json")))
+    ocfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"])
+    o = O.Oracle(ocfg)
+    wpt, z = o.benchmark_init_hydro()
+    names = {f.name for f in dataclasses.fields(rb.Config)}
+    cfg = {k: v for k, v in dataclasses.asdict(ocfg).items() if k in names}
+    ke = []
+    with rb.Rayleigh(rb.Config(**cfg, precision=precision, use_graph=True)) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        done = 0
+        every = gold["integration_interval"]
+        for k in range(every, gold["max_iterations"] + 1, every):
+            g.step(k - 1 - done)
+            done = k - 1
+            sw, sz, sab = g.get_state()
+            o.init_state(sw, sz, sab)
+            o.step()                                   # its physical-space stage sees iteration k's velocity
+            ke.append(o.benchmark_kinetic_energy())
+    ke = np.array(ke)
+    ref = gold["observables"]["Kinetic Energy"]
+    print(precision, ke, ke.mean(), ke.std())
+    assert len(ke) == gold["samples"]
+    assert abs(ke.mean() - ref["measured"]) < 5e-6, (ke.mean(), ref)
+    assert abs(ke.std() - ref["sdev"]) < 5e-6, (ke.std(), ref)

@@ -163,3 +163,29 @@ def test_perturbation_evolves_and_stays_finite():
     assert np.isfinite(o.rhs_wpt).all() and np.isfinite(o.rhs_z).all()
     assert np.abs(o.rhs_wpt[:, :, :cfg.n_r]).max() > 0.0      # buoyancy drives W
     assert cfl > 0.0
+
+
+def test_c2001_case0_matches_the_reference_regression_report():
+    """The reference's own regression run of its accuracy benchmark
+    (tests/c2001_case0: Christensen et al. 2001 case 0 from Benchmark_Init_Hydro,
+    N_r = 48, N_theta = 64, 400 steps of dt = 1e-4, alpha = 0.50001): mean and
+    standard deviation of the volume-averaged kinetic energy at iterations 100,
+    200, 300, 400, as its Benchmark_Reports/00000400 prints them (6 decimals).
+    This pins the oracle's whole time step, not only its transforms."""
+    import json
+    import os
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c2001_case0.json")))
+    cfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"])
+    o = O.Oracle(cfg)
+    wpt, z = o.benchmark_init_hydro()
+    o.init_state(wpt, z)
+    ke = []
+    for it in range(1, gold["max_iterations"] + 1):
+        o.step()
+        if it % gold["integration_interval"] == 0:
+            ke.append(o.benchmark_kinetic_energy())
+    ke = np.array(ke)
+    ref = gold["observables"]["Kinetic Energy"]
+    assert len(ke) == gold["samples"]
+    assert abs(ke.mean() - ref["measured"]) < 1e-6 * 5, (ke.mean(), ref)
+    assert abs(ke.std() - ref["sdev"]) < 1e-6 * 5, (ke.std(), ref)

@@ -749,8 +749,9 @@ class Oracle:
         cos = h.costheta[th][:, None, None]
         for k in ("vt", "vp", "dvtdr", "dvpdr", "dtdt", "dvrdt", "dvpdp", "dvtdp"):
             f[k] = f[k] * csc                                          # sintheta_div (:119-126)
-        # the velocity Benchmark_Checkup reads at this point of the step (:158-159)
+        # the velocity and temperature Benchmark_Checkup reads at this point of the step (:158-159)
         self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
+        self.last_temperature = f["t"]
         r = self.radius[None, :, None]
         dlnrho = self.dlnrho[None, :, None]
         one_over_r = 1.0 / r
@@ -902,6 +903,43 @@ class Oracle:
         tw = (self.h.wq / 2.0).astype(np.float64)
         ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
         return float(np.dot(self.radial_integration_weights(), ell0))
+
+    def benchmark_point_observations(self, msymm=4):
+        """Assemble_Strips and Point_Observations (Benchmarking.F90:934-1063) on the last
+        physical-space stage: the phi strips of v_r, v_phi and T at the two radii that
+        straddle mid-depth (n_r/2, n_r/2 + 1) and the two colatitudes that straddle the
+        equator, averaged; at the first msymm points (in phi order, starting across the
+        wrap) where v_r changes sign upwards, v_phi and T are interpolated linearly and
+        averaged.  Returns (v_phi, T)."""
+        vr, vt, vp, th = self.last_velocity
+        if not (isinstance(th, slice) and th == slice(None)):
+            raise ValueError("the last physical-space stage did not cover every theta row")
+        nth, nr, nphi = self.cfg.n_theta, self.cfg.n_r, self.cfg.n_phi
+        t1, t2 = nth // 2 - 1, nth // 2
+        r1, r2 = nr // 2 - 1, nr // 2
+
+        def strip(a):   # strips 1..4 = (r_one, th_one), (r_one, th_two), (r_two, th_one), (r_two, th_two)
+            s = np.zeros(nphi)
+            for rr, tt in ((r1, t1), (r1, t2), (r2, t1), (r2, t2)):
+                s = s + a[tt, rr, :]
+            return s * (1.0 / 4)
+
+        strips = [strip(vr), strip(vp), strip(self.last_temperature)]
+        vsave = np.zeros((msymm, 3))
+        xind = 0
+        im1 = nphi - 1
+        for i in range(nphi):
+            vrnext, vrlast = strips[0][i], strips[0][im1]
+            dvr = vrnext - vrlast
+            if vrnext * vrlast < 0 and xind < msymm and dvr > 0:
+                x = -vrlast / dvr
+                for j in range(3):
+                    y1, y2 = strips[j][im1], strips[j][i]
+                    vsave[xind, j] = (y2 - y1) * x + y1
+                xind += 1
+            im1 = i
+        obs = vsave.sum(axis=0) / msymm
+        return float(obs[1]), float(obs[2])
 
     def step(self):
         """One pass of Main_Loop_Sphere (Sphere_Driver.F90:305-328) at fixed dt."""

@@ -108,6 +108,16 @@ int ra_physical(ra_ctx* ctx, double* cfl);      /* physical_space: FFTs, NL term
 int ra_rlm_b(ra_ctx* ctx);                      /* PtS Legendre + rlm_spaceb + Transpose_2b1b */
 int ra_advance(ra_ctx* ctx);                    /* AdvanceTime: AB term, BCs, Implicit_Solve */
 
+/* Benchmark_Checkup's volume-averaged kinetic energy of the current state
+ * (Benchmarking.F90:645-656, 733-736): 0.5 rho |u|^2 on the physical grid,
+ * averaged over phi, over theta with the Gauss-Legendre weights / 2
+ * (Spherical_IO.F90:1350-1391) and over radius with the Chebyshev integration
+ * weights (Spherical_IO.F90:1436-1470, Chebyshev_Polynomials.F90:165-194).
+ * Runs the stages that form the velocity on the grid (Post_Solve through the
+ * inverse Legendre transform; they only assign their outputs, so the next
+ * ra_step is unchanged) and a reduction on the device; *ke receives the sum. */
+int ra_kinetic_energy(ra_ctx* ctx, double* ke);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

@@ -122,6 +122,7 @@ def load_library(path: str | None = None):
         "ra_physical": ([_VP, _DP], ctypes.c_int),
         "ra_rlm_b": ([_VP], ctypes.c_int),
         "ra_advance": ([_VP], ctypes.c_int),
+        "ra_kinetic_energy": ([_VP, _DP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -261,6 +262,13 @@ class Rayleigh:
 
     def advance_time(self):
         self._check(self.lib.ra_advance(self.h))
+
+    def kinetic_energy(self):
+        """Benchmark_Checkup's volume-averaged kinetic energy of the current state
+        (Benchmarking.F90:645-656, 733-736), reduced on the device."""
+        ke = ctypes.c_double()
+        self._check(self.lib.ra_kinetic_energy(self.h, ctypes.byref(ke)))
+        return ke.value
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,
                "rhs_wpt": 7, "rhs_z": 8, "ptab": 9, "iptab": 10}

@@ -787,4 +787,108 @@ void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse) {
     ++c.launches;
 }
 
+
+// Benchmark_Checkup's volume-averaged kinetic energy (Benchmarking.F90:645-656,
+// 733-736) of the velocity in p2a.  One CTA per (theta, r) row forms v_r,
+// v_theta, v_phi on the phi grid with the physics kernel's c2r and writes the
+// row's share w_theta w_r rho / 2 * mean_phi |u|^2; kew holds the theta weights
+// (Gauss-Legendre weight / 2 / n_phi, ComputeEll0) and then the radial
+// integration weights (Compute_Radial_Average).  No cluster: each row reads
+// its own hemisphere's reflection of the even and odd parts.
+template <int N>
+__global__ void __launch_bounds__(ROW_THREADS) kinetic_energy_rows_kernel(PhysParams P, const double* __restrict__ kew,
+                                                                          double* __restrict__ rows) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    __shared__ double red[ROW_THREADS / 32];
+    const int t = threadIdx.x;
+    const int h = (int)(blockIdx.x & 1);
+    const int nr = P.nr;
+    const int pair = (int)(blockIdx.x >> 1);
+    const int r = pair % nr;
+    const int thh = pair / nr;
+    const int th = h ? (N - 1 - thh) : thh;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[3] = {A_VR, A_VT, A_VP};
+    const bool dp[3] = {false, false, false};
+    double2 y[FB][ZPT];
+    row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+    const double csc = P.trig[2 * N + th];
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q)
+        if (t + q * ROW_THREADS < N) {
+            const double2 a = y[0][q];
+            const double2 b = make_double2(y[1][q].x * csc, y[1][q].y * csc);
+            const double2 c = make_double2(y[2][q].x * csc, y[2][q].y * csc);
+            s += (a.x * a.x + b.x * b.x + c.x * c.x) + (a.y * a.y + b.y * b.y + c.y * c.y);
+        }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((t & 31) == 0) red[t >> 5] = s;
+    __syncthreads();
+    if (t == 0) {
+        double v = red[0];
+        for (int i = 1; i < ROW_THREADS / 32; ++i) v += red[i];
+        rows[(long)th * nr + r] = 0.5 * P.radial[R_DENSITY * nr + r] * v * kew[th] * kew[N + r];
+    }
+}
+
+// Sum of the row shares in a fixed order (one CTA): the result is the same on
+// every call for the same state.
+__global__ void __launch_bounds__(1024) kinetic_energy_sum_kernel(const double* __restrict__ rows, long n,
+                                                                  double* __restrict__ out) {
+    __shared__ double red[32];
+    const int t = threadIdx.x;
+    double s = 0.0;
+    for (long i = t; i < n; i += 1024) s += rows[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((t & 31) == 0) red[t >> 5] = s;
+    __syncthreads();
+    if (t == 0) {
+        double v = red[0];
+        for (int i = 1; i < 32; ++i) v += red[i];
+        *out = v;
+    }
+}
+
+void launch_kinetic_energy(Ctx& c) {
+    if (!c.d_twp || !c.d_kew || !c.d_ke_rows) throw ArgError("diagnostic tables not prepared at set-up");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)3 * fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, c.d_kew, c.d_ke_rows);
+    };
+    switch (c.d.nth) {
+        case 24: go(kinetic_energy_rows_kernel<24>, 24); break;
+        case 32: go(kinetic_energy_rows_kernel<32>, 32); break;
+        case 48: go(kinetic_energy_rows_kernel<48>, 48); break;
+        case 64: go(kinetic_energy_rows_kernel<64>, 64); break;
+        case 96: go(kinetic_energy_rows_kernel<96>, 96); break;
+        case 128: go(kinetic_energy_rows_kernel<128>, 128); break;
+        case 192: go(kinetic_energy_rows_kernel<192>, 192); break;
+        case 256: go(kinetic_energy_rows_kernel<256>, 256); break;
+        case 384: go(kinetic_energy_rows_kernel<384>, 384); break;
+        case 512: go(kinetic_energy_rows_kernel<512>, 512); break;
+        case 768: go(kinetic_energy_rows_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no kinetic-energy kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    kinetic_energy_sum_kernel<<<1, 1024, 0, c.stream>>>(c.d_ke_rows, (long)c.d.nth * c.d.nr,
+                                                        c.d_ke_rows + (long)c.d.nth * c.d.nr);
+    RA_CUDA(cudaGetLastError());
+    c.launches += 2;
+}
+
 }  // namespace ra

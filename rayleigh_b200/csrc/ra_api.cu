@@ -115,6 +115,14 @@ static void chebyshev_setup(Ctx& c, double rmin, double rmax) {
     double scaling = (rmax - rmin) / (xmax - xmin);
     c.rad.radius.resize(n);
     for (int i = 0; i < n; ++i) c.rad.radius[i] = (x[i] - xmin) * scaling + rmin;
+    // integration weights 3 pi scaling / ((r_o^3 - r_i^3) N) r^2 sqrt(1 - x^2), halved
+    // at the two end points (Chebyshev_Polynomials.F90:165-194)
+    const double int_scale = 3.0 * M_PI * scaling / ((rmax * rmax * rmax - rmin * rmin * rmin) * n);
+    c.rad.int_w.resize(n);
+    for (int i = 0; i < n; ++i)
+        c.rad.int_w[i] = int_scale * c.rad.radius[i] * c.rad.radius[i] * sqrt(1.0 - x[i] * x[i]);
+    c.rad.int_w[0] *= 0.5;
+    c.rad.int_w[n - 1] *= 0.5;
     scaling = 1.0 / scaling;
     c.deriv_scaling = scaling;
     for (int d = 1; d < 4; ++d) {
@@ -352,6 +360,10 @@ static void setup(Ctx& c) {
         twid[2 * k] = (double)cosl(a);
         twid[2 * k + 1] = (double)sinl(a);
     }
+    // weights of the kinetic-energy diagnostic: theta (Gauss-Legendre / 2 / n_phi), then radius
+    std::vector<double> kew((size_t)d.nth + d.nr);
+    for (int i = 0; i < d.nth; ++i) kew[i] = (double)(wq[i] / 2.0L) / d.nphi;
+    for (int i = 0; i < d.nr; ++i) kew[d.nth + i] = c.rad.int_w[i];
     // radial profiles
     const int nr = d.nr;
     std::vector<double> rp((size_t)R_COUNT * nr);
@@ -392,6 +404,9 @@ static void setup(Ctx& c) {
     dalloc(c.d_p2b, (size_t)d.L * d.nth * NP2B * 2 * nr);
     dalloc(c.d_s2b, (size_t)nlm * NP2B * 2 * nr);
     dalloc(c.d_cfl, 1);
+    dalloc(c.d_kew, kew.size());
+    dalloc(c.d_ke_rows, (size_t)d.nth * nr + 1);
+    RA_CUDA(cudaMemcpyAsync(c.d_kew, kew.data(), kew.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_ab, 0, (size_t)4 * nlm * 2 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_sol_wpt, 0, (size_t)nlm * 2 * 3 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_sol_z, 0, (size_t)nlm * 2 * nr * sizeof(double), c.stream));
@@ -437,7 +452,7 @@ static void release(Ctx& c) {
     if (c.graph) cudaGraphDestroy(c.graph);
     double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp, c.d_Awpt, c.d_Az,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
-                      c.d_p2a, c.d_p2b, c.d_s2b};
+                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows};
     for (double* b : bufs)
         if (b) cudaFree(b);
     int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status};
@@ -723,6 +738,22 @@ int ra_physical(ra_ctx* ctx, double* cfl) {
             RA_CUDA(cudaStreamSynchronize(c.stream));
             std::memcpy(cfl, &bits, sizeof(double));
         }
+    });
+}
+
+int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!ke) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        launch_kinetic_energy(c);
+        RA_CUDA(cudaMemcpyAsync(ke, c.d_ke_rows + (size_t)c.d.nth * c.d.nr, sizeof(double), cudaMemcpyDeviceToHost,
+                                c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
     });
 }
 

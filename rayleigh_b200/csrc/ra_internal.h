@@ -63,6 +63,7 @@ constexpr int NP2B = 4;
 
 struct Radial {
     std::vector<double> radius, delta_r, density, dlnrho, buoy, dpdr_w, pdwdr, nu, kappa;
+    std::vector<double> int_w;   // radial integration weights (a volume average over the shell)
     double coriolis;
 };
 
@@ -125,6 +126,8 @@ struct Ctx {
     double *d_s2b = nullptr;                          // [row][4][nr][2]
     unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
     int *d_status = nullptr;                          // device error word
+    double *d_kew = nullptr;                          // [nth] theta weights / n_phi, then [nr] radial weights
+    double *d_ke_rows = nullptr;                      // [nth][nr] kinetic-energy shares, then the sum
 
     MixedPlan mx_inv, mx_fwd, mx_solve;               // RA_PREC_MIXED Legendre transforms, implicit solve
 
@@ -145,6 +148,7 @@ void launch_cheb_synthesis(Ctx& c);
 void launch_post_assemble(Ctx& c, double old_ab);
 void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
+void launch_kinetic_energy(Ctx& c);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

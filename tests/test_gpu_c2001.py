@@ -7,9 +7,10 @@ the point observations T and v_phi at iterations 100, 200, 300 and 400.  The
 CUDA path runs those steps through the C ABI; at each sample iteration k its
 state after k - 1 steps goes through one oracle step, whose physical-space
 stage forms the fields Benchmark_Checkup reads, and the oracle's restatement
-of the benchmark's averaging and point observations gives the sample.  Both
-precision forms must reproduce the reference's report to its 6 printed
-decimals."""
+of the point observations gives their sample; the kinetic energy is the
+device's own reduction (ra_kinetic_energy), checked against the oracle's
+restatement of the benchmark's averaging on the way.  Both precision forms
+must reproduce the reference's report to its 6 printed decimals."""
 import dataclasses
 import json
 import os
@@ -41,11 +42,14 @@ def test_c2001_case0_reproduces_the_reference_report(precision):
         for k in range(every, gold["max_iterations"] + 1, every):
             g.step(k - 1 - done)
             done = k - 1
+            ke_dev = g.kinetic_energy()                # reduced on the device
             sw, sz, sab = g.get_state()
             o.init_state(sw, sz, sab)
             o.step()                                   # its physical-space stage sees iteration k's velocity
             vphi, temp = o.benchmark_point_observations()
-            ke.append((o.benchmark_kinetic_energy(), vphi, temp))
+            ke_o = o.benchmark_kinetic_energy()
+            assert abs(ke_dev - ke_o) <= (1e-12 if precision == 0 else 1e-9) * ke_o, (k, ke_dev, ke_o)
+            ke.append((ke_dev, vphi, temp))
     ke = np.array(ke)
     print(precision, ke)
     assert len(ke) == gold["samples"]

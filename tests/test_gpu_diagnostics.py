@@ -1,0 +1,66 @@
+"""The device-side kinetic-energy diagnostic (ra_kinetic_energy).
+
+Benchmark_Checkup (Benchmarking.F90:645-656, 733-736) volume-averages
+0.5 rho |u|^2 of the velocity the physical-space stage forms.  The CUDA entry
+forms that velocity from the current state with the step's own stages and
+reduces on the device; the oracle forms it in its step's physical-space stage
+and averages it with its restatement of the same weights.  The two must agree
+to the path's tolerance (1e-12 relative for the FP64 form, 1e-9 for the mixed
+form), and calling the diagnostic between steps must leave the run unchanged
+bit for bit."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(cfg):
+    import rayleigh_b200 as rb
+    from rayleigh_b200 import build as rbuild
+    rbuild.build()
+    return rb.Rayleigh(rb.Config(**cfg))
+
+
+def _ocfg(cfg):
+    return O.Config(**{k: v for k, v in cfg.items() if k in O.Config.__dataclass_fields__})
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+@pytest.mark.parametrize("n_r,l_max", [(24, 31), (32, 127)])
+def test_kinetic_energy_matches_the_oracle(precision, tol, n_r, l_max):
+    cfg = dict(n_r=n_r, l_max=l_max, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=min(10, l_max))
+    o = O.Oracle(oc)
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        for steps in (1, 4):   # the seeded state starts at rest: the first step makes the flow
+            g.step(steps)
+            ke = g.kinetic_energy()
+            sw, sz, sab = g.get_state()
+            o.init_state(sw, sz, sab)
+            o.step()
+            ref = o.benchmark_kinetic_energy()
+            assert ref > 0.0
+            print(precision, n_r, l_max, steps, ke, ref, abs(ke - ref) / ref)
+            assert abs(ke - ref) <= tol * ref, (steps, ke, ref)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_kinetic_energy_leaves_the_run_unchanged(precision):
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    wpt, z = O.seeded_state(_ocfg(cfg), amp=1e-2, lmax_pert=10)
+    plain = _ctx(cfg)
+    plain.put_state(wpt, z, None, iteration=1)
+    plain.step(6)
+    probed = _ctx(cfg)
+    probed.put_state(wpt, z, None, iteration=1)
+    kes = []
+    for _ in range(3):
+        probed.step(2)
+        kes.append(probed.kinetic_energy())
+    for a, b in zip(plain.get_state(), probed.get_state()):
+        assert np.array_equal(a, b)
+    assert kes[-1] == probed.kinetic_energy()   # deterministic: a fixed-order device reduction

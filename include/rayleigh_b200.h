@@ -118,6 +118,31 @@ int ra_advance(ra_ctx* ctx);                    /* AdvanceTime: AB term, BCs, Im
  * ra_step is unchanged) and a reduction on the device; *ke receives the sum. */
 int ra_kinetic_energy(ra_ctx* ctx, double* ke);
 
+/* Shell slices of the current state (Shell_Slices output, Spherical_IO.F90):
+ * each quantity of quantities[0..nq) on the full theta-phi grid at the radial
+ * indices levels[0..nlev) (0-based grid indices, 0 = outer boundary), into
+ * out(n_phi, n_theta, nlev, nq) (Fortran order; phi fastest, theta in the
+ * grid's order).  Quantity codes are the reference's output codes
+ * (velocity_field_codes.F, thermal_field_codes.F) of values the
+ * physical-space buffer holds: */
+#define RA_Q_V_R            1
+#define RA_Q_V_THETA        2
+#define RA_Q_V_PHI          3
+#define RA_Q_DV_R_DR       10
+#define RA_Q_DV_THETA_DR   11
+#define RA_Q_DV_PHI_DR     12
+#define RA_Q_DV_R_DT       19
+#define RA_Q_DV_R_DP       28
+#define RA_Q_DV_THETA_DP   29
+#define RA_Q_DV_PHI_DP     30
+#define RA_Q_ENTROPY      501
+#define RA_Q_ENTROPY_DR   507
+#define RA_Q_ENTROPY_DTHETA 513
+#define RA_Q_ENTROPY_DPHI 519
+/* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
+ * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
+int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

@@ -752,6 +752,7 @@ class Oracle:
         # the velocity and temperature Benchmark_Checkup reads at this point of the step (:158-159)
         self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
         self.last_temperature = f["t"]
+        self.last_fields = dict(f)   # every physical-space field, [theta, r, phi]: the diagnostics' buffer
         r = self.radius[None, :, None]
         dlnrho = self.dlnrho[None, :, None]
         one_over_r = 1.0 / r

@@ -123,6 +123,7 @@ def load_library(path: str | None = None):
         "ra_rlm_b": ([_VP], ctypes.c_int),
         "ra_advance": ([_VP], ctypes.c_int),
         "ra_kinetic_energy": ([_VP, _DP], ctypes.c_int),
+        "ra_shell_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -269,6 +270,21 @@ class Rayleigh:
         ke = ctypes.c_double()
         self._check(self.lib.ra_kinetic_energy(self.h, ctypes.byref(ke)))
         return ke.value
+
+    # the reference's output codes of the quantities ra_shell_slices provides
+    QUANTITIES = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
+                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "entropy": 501,
+                  "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519}
+
+    def shell_slices(self, quantities, levels):
+        """Shell slices of the current state: array [quantity][level][theta][phi] of the
+        quantities (output codes or names of QUANTITIES) at the radial grid indices."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        out = np.empty((len(q), len(lv), self.n_theta, self.n_phi))
+        self._check(self.lib.ra_shell_slices(self.h, q.ctypes.data, len(q), lv.ctypes.data, len(lv),
+                                             out.ctypes.data))
+        return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,
                "rhs_wpt": 7, "rhs_z": 8, "ptab": 9, "iptab": 10}

@@ -891,4 +891,84 @@ void launch_kinetic_energy(Ctx& c) {
     c.launches += 2;
 }
 
+// Natural phi index of buffer position p after the in-place DIF passes: with
+// p = sum_s d_s SS_s (SS_s the stride of pass s), n = d_0 + R_0 (d_1 + R_1 (d_2 + ...)).
+template <int N>
+__device__ __forceinline__ int natural_index(int p) {
+    int n = 0, mul = 1;
+#pragma unroll
+    for (int s = 0; s < npass_of(N); ++s) {
+        const int R = radix_at(N, s), SS = ip_ls(N, s) / R;
+        n += ((p / SS) % R) * mul;
+        mul *= R;
+    }
+    return n;
+}
+
+// Shell slices (Spherical_IO.F90 Shell_Slices) of one diagnostic quantity: one
+// CTA per (theta, level) row forms the quantity on the phi grid from p2a with
+// the physics kernel's c2r (d/dphi in the spectrum, 1/sin(theta) where the
+// physical-space stage divides by it) and writes the row in natural phi order:
+// out[level][theta][phi].
+template <int N>
+__global__ void __launch_bounds__(ROW_THREADS) shell_slice_kernel(PhysParams P, SliceSpec S, double* __restrict__ out) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    const int t = threadIdx.x;
+    const int h = (int)(blockIdx.x & 1);
+    const int thh = (int)(blockIdx.x >> 1);
+    const int th = h ? (N - 1 - thh) : thh;
+    const int lv = (int)blockIdx.y;
+    const int r = S.level[lv];
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    double2* row = reinterpret_cast<double2*>(out + ((long)lv * N + th) * (2L * N));
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {
+        const int p = t + q * ROW_THREADS;
+        if (p < N) row[natural_index<N>(p)] = make_double2(y[0][q].x * scale, y[0][q].y * scale);
+    }
+}
+
+void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out) {
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
+    if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("shell slice: 1 .. 64 levels per launch");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)S.nl);
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, out);
+    };
+    switch (c.d.nth) {
+        case 24: go(shell_slice_kernel<24>, 24); break;
+        case 32: go(shell_slice_kernel<32>, 32); break;
+        case 48: go(shell_slice_kernel<48>, 48); break;
+        case 64: go(shell_slice_kernel<64>, 64); break;
+        case 96: go(shell_slice_kernel<96>, 96); break;
+        case 128: go(shell_slice_kernel<128>, 128); break;
+        case 192: go(shell_slice_kernel<192>, 192); break;
+        case 256: go(shell_slice_kernel<256>, 256); break;
+        case 384: go(shell_slice_kernel<384>, 384); break;
+        case 512: go(shell_slice_kernel<512>, 512); break;
+        case 768: go(shell_slice_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no shell-slice kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

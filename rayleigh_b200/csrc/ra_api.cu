@@ -757,6 +757,56 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
     });
 }
 
+// Diagnostic quantity codes of the reference's output system (velocity_field_codes.F,
+// thermal_field_codes.F: voffset = 0, pt_off = 500) that are values of the
+// physical-space buffer, and where each comes from in p2a.
+struct QuantitySource { int code, field, dphi, csc; };
+static const QuantitySource kQuantities[] = {
+    {1, A_VR, 0, 0},      {2, A_VT, 0, 1},      {3, A_VP, 0, 1},      {10, A_DVRDR, 0, 0}, {11, A_DVTDR, 0, 1},
+    {12, A_DVPDR, 0, 1},  {19, A_DVRDT, 0, 1},  {28, A_VR, 1, 0},     {29, A_VT, 1, 1},    {30, A_VP, 1, 1},
+    {501, A_T, 0, 0},     {507, A_DTDR, 0, 0},  {513, A_DTDT, 0, 1},  {519, A_T, 1, 0},
+};
+
+int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !levels || !out || nq < 1 || nlev < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        std::vector<SliceSpec> spec(nq);
+        for (int q = 0; q < nq; ++q) {
+            const QuantitySource* src = nullptr;
+            for (const QuantitySource& k : kQuantities)
+                if (k.code == quantities[q]) src = &k;
+            if (!src) throw ArgError("shell slice: quantity code " + std::to_string(quantities[q]) + " is not provided");
+            spec[q] = SliceSpec{};
+            spec[q].field = src->field;
+            spec[q].dphi = src->dphi;
+            spec[q].csc = src->csc;
+        }
+        for (int l = 0; l < nlev; ++l)
+            if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell slice: radial index out of range");
+        // the slices go through p2b, which the step rewrites before reading
+        const long per = (long)c.d.nth * c.d.nphi;
+        const long room = (long)c.d.L * c.d.nth * NP2B * 2 * c.d.nr;
+        if (room < per) throw ArgError("shell slice: no room for one slice");
+        const int chunk = (int)std::min<long>(SliceSpec::MAXL, room / per);
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q)
+            for (int l0 = 0; l0 < nlev; l0 += chunk) {
+                SliceSpec S = spec[q];
+                S.nl = std::min(chunk, nlev - l0);
+                for (int i = 0; i < S.nl; ++i) S.level[i] = levels[l0 + i];
+                launch_shell_slice(c, S, c.d_p2b);
+                RA_CUDA(cudaMemcpyAsync(out + ((long)q * nlev + l0) * per, c.d_p2b, (size_t)S.nl * per * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c.stream));
+            }
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
+    });
+}
+
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {

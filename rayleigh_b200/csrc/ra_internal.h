@@ -149,6 +149,13 @@ void launch_post_assemble(Ctx& c, double old_ab);
 void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
 void launch_kinetic_energy(Ctx& c);
+// one diagnostic quantity on the phi grid at up to MAXL radial levels
+struct SliceSpec {
+    static constexpr int MAXL = 64;
+    int field, dphi, csc, nl;   // p2a field, d/dphi, times 1/sin(theta), levels in this launch
+    int level[MAXL];            // radial indices
+};
+void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

@@ -64,3 +64,43 @@ def test_kinetic_energy_leaves_the_run_unchanged(precision):
     for a, b in zip(plain.get_state(), probed.get_state()):
         assert np.array_equal(a, b)
     assert kes[-1] == probed.kinetic_energy()   # deterministic: a fixed-order device reduction
+
+
+# the oracle's physical-space buffer names of the quantities ra_shell_slices provides
+_ORACLE_NAME = {"v_r": "vr", "v_theta": "vt", "v_phi": "vp", "dv_r_dr": "dvrdr", "dv_theta_dr": "dvtdr",
+                "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp",
+                "dv_phi_dp": "dvpdp", "entropy": "t", "entropy_dr": "dtdr", "entropy_dtheta": "dtdt",
+                "entropy_dphi": "dtdp"}
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+def test_shell_slices_match_the_oracle(precision, tol):
+    """Every provided quantity at 70 levels (repeats included, so that the slices
+    take two launches through the scratch buffer) against the oracle's
+    physical-space buffer, relative L2 per quantity."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    levels = [(7 * i) % oc.n_r for i in range(70)]
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        sl = g.shell_slices(names, levels)
+        again = g.shell_slices(["v_r"], [levels[5]])
+        sw, sz, sab = g.get_state()
+        with pytest.raises(rb.RayleighError):
+            g.shell_slices([502], [0])                 # pressure: not a value of this path's buffer
+        with pytest.raises(rb.RayleighError):
+            g.shell_slices(["v_r"], [oc.n_r])
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    assert sl.shape == (len(names), len(levels), o.cfg.n_theta, o.cfg.n_phi)
+    for i, name in enumerate(names):
+        ref = o.last_fields[_ORACLE_NAME[name]][:, levels, :].transpose(1, 0, 2)   # [level, theta, phi]
+        err = np.linalg.norm(sl[i] - ref) / np.linalg.norm(ref)
+        print(precision, name, err)
+        assert err < tol, (name, err)
+    assert np.array_equal(again[0, 0], sl[0, 5])

@@ -905,16 +905,21 @@ class Oracle:
         ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
         return float(np.dot(self.radial_integration_weights(), ell0))
 
-    def benchmark_point_observations(self, msymm=4):
+    def benchmark_point_observations(self, msymm=4, fields=None):
         """Assemble_Strips and Point_Observations (Benchmarking.F90:934-1063) on the last
-        physical-space stage: the phi strips of v_r, v_phi and T at the two radii that
-        straddle mid-depth (n_r/2, n_r/2 + 1) and the two colatitudes that straddle the
-        equator, averaged; at the first msymm points (in phi order, starting across the
-        wrap) where v_r changes sign upwards, v_phi and T are interpolated linearly and
+        physical-space stage, or on ``fields`` = (v_r, v_phi, T) given as [theta, r, phi]
+        arrays: the phi strips of v_r, v_phi and T at the two radii that straddle
+        mid-depth (n_r/2, n_r/2 + 1) and the two colatitudes that straddle the equator,
+        averaged; at the first msymm points (in phi order, starting across the wrap)
+        where v_r changes sign upwards, v_phi and T are interpolated linearly and
         averaged.  Returns (v_phi, T)."""
-        vr, vt, vp, th = self.last_velocity
-        if not (isinstance(th, slice) and th == slice(None)):
-            raise ValueError("the last physical-space stage did not cover every theta row")
+        if fields is None:
+            vr, vt, vp, th = self.last_velocity
+            if not (isinstance(th, slice) and th == slice(None)):
+                raise ValueError("the last physical-space stage did not cover every theta row")
+            temperature = self.last_temperature
+        else:
+            vr, vp, temperature = fields
         nth, nr, nphi = self.cfg.n_theta, self.cfg.n_r, self.cfg.n_phi
         t1, t2 = nth // 2 - 1, nth // 2
         r1, r2 = nr // 2 - 1, nr // 2
@@ -925,7 +930,7 @@ class Oracle:
                 s = s + a[tt, rr, :]
             return s * (1.0 / 4)
 
-        strips = [strip(vr), strip(vp), strip(self.last_temperature)]
+        strips = [strip(vr), strip(vp), strip(temperature)]
         vsave = np.zeros((msymm, 3))
         xind = 0
         im1 = nphi - 1

@@ -235,7 +235,7 @@ struct PhysParams {
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
 // 2-CTA cluster that folds its spectra through distributed shared memory.
 constexpr int ROW_THREADS = 384;
-enum { RC_RAD, RC_ORAD, RC_RHO, RC_DLNRHO, RC_DR, RC_CS, RC_SN, RC_CSC, RC_COT, RC_COR, RC_C2R, RC_COUNT };
+enum { RC_RAD, RC_ORAD, RC_RHO, RC_DLNRHO, RC_DR, RC_CS, RC_SN, RC_CSC, RC_COT, RC_COR, RC_C2R, RC_HSF, RC_COUNT };
 constexpr int FB = 4;   // fields per batched FFT
 
 // Shared memory of a row CTA (double2 units): one in-place FFT buffer of FB
@@ -480,6 +480,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         rowc[RC_COT] = P.trig[3 * N + th];
         rowc[RC_COR] = P.rotation ? P.coriolis : 0.0;
         rowc[RC_C2R] = csc * csc * orad;
+        rowc[RC_HSF] = 0.5 * (P.radial[R_DENSITY * nr + r] * P.radial[R_RADIUS * nr + r] * csc);
     }   // read after row_c2r's first barrier
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
@@ -513,7 +514,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             if (live(q)) {
                 acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
                 acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
-                acc_at(2, q) = make_double2(0.0, 0.0);
                 acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
             }
         }
@@ -539,47 +539,43 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             z.y += vt[q].y * d.y * c2r;
         }
     }
-    // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr
+    // B3: dv_phi/dr, dv_phi/dphi, omega_r
     {
-        const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
-        const bool dp[4] = {false, true, false, false};
-        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const int fo[3] = {A_DVPDR, A_VP, A_OMR};
+        const bool dp[3] = {false, true, false};
+        row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
         const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
+            const double2 a = y[0][q], b = y[1][q], c = y[2][q];
             double2& pp = acc_at(1, q);
-            double2& tt = acc_at(2, q);
             double2& z = acc_at(3, q);
             z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
             z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
             pp.x += -vt[q].x * b.x * c2r;
             pp.y += -vt[q].y * b.y * c2r;
-            tt.x += -vr[q].x * d.x;
-            tt.y += -vr[q].y * d.y;
         }
     }
-    // B4: dT/dtheta, dT/dphi
+    // B4: dT/dr, dT/dtheta, dT/dphi: the whole T term, written once
     {
-        const int fo[2] = {A_DTDT, A_T};
-        const bool dp[2] = {false, true};
-        row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const int fo[3] = {A_DTDR, A_DTDT, A_T};
+        const bool dp[3] = {false, false, true};
+        row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
         const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q];
-            double2& tt = acc_at(2, q);
-            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
-            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+            const double2 d = y[0][q], a = y[1][q], b = y[2][q];
+            acc_at(2, q) = make_double2(-vr[q].x * d.x + (-a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad),
+                                        -vr[q].y * d.y + (-a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad));
         }
     }
-    // CFL (Find_MyMinDT) and the rho r sin(theta) factor of the P and Z terms
+    // CFL (Find_MyMinDT); the rho r / sin(theta) factor of the P and Z terms is a
+    // row constant, applied to their spectra after the r2c (RC_HSF)
     double cmax = 0.0;
     const double orad = rowc[RC_ORAD], dr = rowc[RC_DR];
     const double hfac = P.llmax * orad * orad, rfac = 1.0 / (dr * dr);
-    const double sfac = rowc[RC_RHO] * rowc[RC_RAD] * rowc[RC_CSC];
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
         if (live(q)) {
@@ -587,10 +583,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             cmax = fmax(cmax, (vt[q].y * vt[q].y + vp[q].y * vp[q].y) * hfac);
             cmax = fmax(cmax, vr[q].x * vr[q].x * rfac);
             cmax = fmax(cmax, vr[q].y * vr[q].y * rfac);
-            double2& pp = acc_at(1, q);
-            double2& z = acc_at(3, q);
-            pp.x *= sfac; pp.y *= sfac;
-            z.x *= sfac; z.y *= sfac;
         }
     }
     __syncthreads();
@@ -606,10 +598,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             const double2 zk = acc[SW(f * FS + k)];
             const double2 zn = acc[SW(f * FS + (N - k) % N)];
             const double2 wk = __ldg(P.wr + k);   // w^(N-k) = -conj(w^k)
+            const double hs = (f & 1) ? rowc[RC_HSF] : 0.5;   // P and Z (f = 1, 3) take the row factor
             auto xval = [&](double2 a, double2 b, double2 w, bool zero_im) {   // X from Z_kk = a, Z_{N-kk} = b
                 const double2 bn = cconj(b);
-                const double2 e = make_double2(0.5 * (a.x + bn.x), 0.5 * (a.y + bn.y));
-                const double2 d = make_double2(0.5 * (a.x - bn.x), 0.5 * (a.y - bn.y));
+                const double2 e = make_double2(hs * (a.x + bn.x), hs * (a.y + bn.y));
+                const double2 d = make_double2(hs * (a.x - bn.x), hs * (a.y - bn.y));
                 const double2 wd = cmul(cconj(w), d);
                 double2 X = make_double2(e.x + wd.y, e.y - wd.x);
                 if (zero_im) X.y = 0.0;

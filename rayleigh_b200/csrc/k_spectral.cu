@@ -226,19 +226,32 @@ __device__ __forceinline__ double sdth_c2(int l, int m) {
 
 constexpr int RLM_A_THREADS = 256;
 
+// (m, l) of a row of the m-major, parity-split row order (row_index inverted):
+// m_off(m) <= row < m_off(m + 1), then the even-l rows of m before the odd-l ones.
+__device__ __forceinline__ void ml_of_row(long row, int L, int& m, int& l) {
+    const double b = 2.0 * L + 1.0;
+    int mm = (int)floor((b - sqrt(b * b - 8.0 * (double)row)) * 0.5);
+    mm = max(0, min(mm, L - 1));
+    while (mm > 0 && m_off(mm, L) > row) --mm;
+    while (mm + 1 < L && m_off(mm + 1, L) <= row) ++mm;
+    const int p = (int)(row - m_off(mm, L));
+    const int ne = n_even(mm, L);
+    m = mm;
+    l = mm + (p < ne ? 2 * p : 2 * (p - ne) + 1);
+}
+
 __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __restrict__ s2a,
                                                              double* __restrict__ s2o,
                                                              const double* __restrict__ radial, long nlm, int nr,
                                                              int L) {
     __shared__ double2 stage[RLM_A_THREADS * NP2A];   // the block's outputs, re-read for coalesced stores
     const long total = nlm * nr;
-    const long idx0 = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    const long idx0 = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (row, r)
     const bool valid = idx0 < total;
     const long idx = valid ? idx0 : total - 1;   // tail lanes compute a copy, store nothing
     const int r = (int)(idx % nr);
-    const long lm = idx / nr;
-    const int l = ell_of_lm(lm);
-    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    int l, m;   // threads run in row order: input and output rows stream, the l +- 1 rows are near
+    ml_of_row(idx / nr, L, m, l);
     const int lmax = L - 1;
     const long fsz = 2L * nr;   // one field of one row
     const long rsz = (long)NS2A * fsz;

@@ -291,14 +291,83 @@ __device__ __forceinline__ void pass_twiddles(const double2* __restrict__ tw, in
     }
 }
 
+// Butterfly g of a pass -> (field f, block b, offset j).  The plain order runs
+// over (f, b, j).  A 16-byte shared access is served in 8-lane phases, one
+// wavefront per phase when its 8 slots fall in 8 different bank groups
+// (slot mod 8); the field stride (2 mod 8) shifts a field's slots by 2.  In
+// two passes the plain order puts two slots of a phase in one group, and
+// these passes deal their butterflies out over pairs of fields instead:
+//   R = 8, SS = 12 (slot = 2f + j mod 8): fields f and f + 2 together; per b,
+//     j 0-7 of f, j 0-7 of f + 2, then j 8-11 of both: every phase conflict-free;
+//   R = 4, SS = 3 (slot = 2f + 4b + j mod 8): fields f and f + 1 together; per
+//     four b, the six butterflies of (b0, b0+1) of f with the j = 1 ones of
+//     (b0+2, b0+3) of f + 1, the same with the fields swapped, then the
+//     j = 0, 2 ones of (b0+2, b0+3) of both: 4 wavefronts per 24 butterflies
+//     instead of 6 (the fewest: j = 1 gives the only odd slots).
+// The mapping only changes which thread computes which butterfly.
+template <int N, int NB, int R, int LS, int SS, int T>
+__device__ __forceinline__ void butterfly_of(int g, int& f, int& b, int& j) {
+    if constexpr (R == 8 && SS == 12 && NB >= 3) {
+        constexpr int NPAIR = NB == 4 ? 2 : 1;   // fields (0, 2), (1, 3)
+        if (g < NPAIR * 2 * T) {
+            const int p = g / (2 * T), rem = g - p * 2 * T;
+            b = rem / 24;
+            const int w = rem - b * 24, qi = w >> 3, l8 = w & 7;
+            if (qi < 2) {
+                f = p + 2 * qi;
+                j = l8;
+            } else {
+                f = (l8 < 4) ? p : p + 2;
+                j = 8 + (l8 & 3);
+            }
+            return;
+        }
+        const int bi = g - NPAIR * 2 * T;   // NB = 3: field 1 alone
+        f = 1;
+        b = bi / SS;
+        j = bi - b * SS;
+        return;
+    } else if constexpr (R == 4 && SS == 3 && (N / LS) % 4 == 0 && NB >= 2) {
+        constexpr int NPAIR = NB / 2;   // fields (0, 1), (2, 3)
+        if (g < NPAIR * 2 * T) {
+            const int fp = g / (2 * T), rem = g - fp * 2 * T;
+            const int blk = rem / 24, w = rem - blk * 24, qi = w >> 3, l8 = w & 7;
+            const int f0 = 2 * fp, b0 = 4 * blk;
+            if (qi == 2) {
+                f = f0 + (l8 >> 2);
+                b = b0 + 2 + ((l8 & 3) >> 1);
+                j = (l8 & 1) * 2;
+            } else if (l8 < 6) {
+                f = f0 + qi;
+                b = b0 + l8 / 3;
+                j = l8 - (l8 / 3) * 3;
+            } else {
+                f = f0 + 1 - qi;
+                b = b0 + 2 + (l8 - 6);
+                j = 1;
+            }
+            return;
+        }
+        const int bi = g - NPAIR * 2 * T;   // NB = 3: field 2 alone
+        f = 2 * NPAIR;
+        b = bi / SS;
+        j = bi - b * SS;
+        return;
+    }
+    f = g / T;
+    const int bi = g - f * T;
+    b = bi / SS;
+    j = bi - b * SS;
+}
+
 template <int N, int NB, int NT, int PS, bool DIT>
 __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const double2* __restrict__ twp, int sign,
                                             int tid) {
     constexpr int R = radix_at(N, PS), LS = ip_ls(N, PS), SS = LS / R, T = N / R, FS = fstride(N);
     const double2* __restrict__ tw = twp + ip_tw_off(N, PS);
     auto butterfly = [&](int g) {
-        const int f = g / T, bi = g - f * T;
-        const int b = bi / SS, j = bi - b * SS;
+        int f, b, j;
+        butterfly_of<N, NB, R, LS, SS, T>(g, f, b, j);
         const int base = f * FS + b * LS + j;
         double2 u[R];
 #pragma unroll

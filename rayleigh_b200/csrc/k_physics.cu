@@ -476,7 +476,19 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
     __syncthreads();   // the buffer is free (previous batch read)
     constexpr int QC = 3;   // items whose loads are in flight together
     // item g = (k, b), b fastest: a quarter warp reads the batch's adjacent
-    // fields of two wavenumbers
+    // fields of two wavenumbers (NB = 4).  For NB = 2 a quarter warp takes the
+    // wavenumbers k0 + {0, 1, 4, 5} (then k0 + {2, 3, 6, 7}) of both fields, so
+    // that its Z writes (slot 2b + k mod 8) fall in distinct bank groups.
+    auto item = [](int g, int& k, int& b) {
+        if constexpr (NB == 2 && (N / 2) % 8 == 0) {
+            const int l8 = g & 7, kk = l8 >> 1;
+            b = l8 & 1;
+            k = (g >> 4) * 8 + ((g >> 3) & 1) * 2 + (kk & 1) + ((kk >> 1) << 2);
+        } else {
+            k = g / NB;
+            b = g - k * NB;
+        }
+    };
 #pragma unroll 1
     for (int q0 = 0; q0 < QI; q0 += QC) {
         double2 xk[QC], xn[QC];
@@ -485,7 +497,8 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
             const int g = t + (q0 + qq) * ROW_THREADS;
             xk[qq] = xn[qq] = make_double2(0.0, 0.0);
             if (q0 + qq < QI && g < NB * NI) {
-                const int k = g / NB, b = g - k * NB;
+                int k, b;
+                item(g, k, b);
                 const double* base = rowbase + (long)pick(fo, b) * 2;
                 const bool d = pick(dp, b);
                 xk[qq] = spec_value(base, mstride, ostride, k, L, h, d);
@@ -496,7 +509,8 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
         for (int qq = 0; qq < QC; ++qq) {
             const int g = t + (q0 + qq) * ROW_THREADS;
             if (q0 + qq < QI && g < NB * NI) {
-                const int k = g / NB, b = g - k * NB;
+                int k, b;
+                item(g, k, b);
                 const double2 wk = __ldg(P.wr + k);   // w^(N-k) = -conj(w^k), w = exp(2 pi i / 2N)
                 buf[SW(b * FS + k)] = zform(xk[qq], xn[qq], wk);
                 if (k != 0 && 2 * k != N) buf[SW(b * FS + N - k)] = zform(xn[qq], xk[qq], make_double2(-wk.x, wk.y));
@@ -608,36 +622,38 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             z.y += vt[q].y * d.y * c2r;
         }
     }
-    // B3: dv_phi/dr, dv_phi/dphi, omega_r
+    // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr (the T term's first part, written)
     {
-        const int fo[3] = {A_DVPDR, A_VP, A_OMR};
-        const bool dp[3] = {false, true, false};
-        row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
+        const bool dp[4] = {false, true, false, false};
+        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
         const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q], c = y[2][q];
+            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
             double2& pp = acc_at(1, q);
             double2& z = acc_at(3, q);
             z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
             z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
             pp.x += -vt[q].x * b.x * c2r;
             pp.y += -vt[q].y * b.y * c2r;
+            acc_at(2, q) = make_double2(-vr[q].x * d.x, -vr[q].y * d.y);
         }
     }
-    // B4: dT/dr, dT/dtheta, dT/dphi: the whole T term, written once
+    // B4: dT/dtheta, dT/dphi
     {
-        const int fo[3] = {A_DTDR, A_DTDT, A_T};
-        const bool dp[3] = {false, false, true};
-        row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+        const int fo[2] = {A_DTDT, A_T};
+        const bool dp[2] = {false, true};
+        row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
         const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             if (!live(q)) continue;
-            const double2 d = y[0][q], a = y[1][q], b = y[2][q];
-            acc_at(2, q) = make_double2(-vr[q].x * d.x + (-a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad),
-                                        -vr[q].y * d.y + (-a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad));
+            const double2 a = y[0][q], b = y[1][q];
+            double2& tt = acc_at(2, q);
+            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
         }
     }
     // CFL (Find_MyMinDT); the rho r / sin(theta) factor of the P and Z terms is a

@@ -224,7 +224,7 @@ struct PhysParams {
     const double* radial;   // packed radial profiles
     const double* trig;     // [4][nth]: cos, sin, csc, cot
     const double2* wr;      // [nth] exp(2 pi i k / n_phi)
-    const double2* twp;     // per-pass FFT twiddles (tw_table_off / pass_twiddles)
+    const double2* twp;     // per-pass FFT twiddles (ip_tw_off; one load per butterfly, twiddle_apply)
     unsigned long long* cfl;
     int L, nth, nr, ncola, ncolb;
     double coriolis;
@@ -267,27 +267,29 @@ __host__ __device__ constexpr int ip_tw_off(int n, int ps) {
 }
 __host__ __device__ constexpr int ip_tw_size(int n) { return ip_tw_off(n, npass_of(n)); }
 
-// Twiddles w[k] = exp(2 pi i j k / LS), k = 1 .. R-1, of butterfly j: the
-// table's w^j, the others by complex products (at most three deep, a few
-// units in the last place), so a butterfly makes one table load.
-template <int R, int SS>
-__device__ __forceinline__ void pass_twiddles(const double2* __restrict__ tw, int j, double2 (&w)[R]) {
-    w[0] = make_double2(1.0, 0.0);
-    w[1] = __ldg(tw + j);
-    if constexpr (R == 8) {
-        w[2] = cmul(w[1], w[1]);
-        w[4] = cmul(w[2], w[2]);
-        w[3] = cmul(w[2], w[1]);
-        w[5] = cmul(w[4], w[1]);
-        w[6] = cmul(w[4], w[2]);
-        w[7] = cmul(w[4], w[3]);
-    } else if constexpr (R == 4) {
-        w[2] = cmul(w[1], w[1]);
-        w[3] = cmul(w[2], w[1]);
-    } else if constexpr (R == 3) {
-        w[2] = cmul(w[1], w[1]);
-    } else {
-        static_assert(R == 2, "radix");
+// u[k] *= w^k, k = 1 .. R-1, for the butterfly's one table twiddle w: the
+// powers are complex products (at most three deep, a few units in the last
+// place) formed in the order they are used, w^2 = w w, w^3 = w^2 w,
+// w^4 = w^2 w^2, w^5 = w^4 w, w^6 = w^4 w^2, w^7 = w^4 w^3, so that no more
+// than four of them are live next to the butterfly's R values.
+template <int R>
+__device__ __forceinline__ void twiddle_apply(double2 (&u)[R], double2 w1) {
+    static_assert(R == 2 || R == 3 || R == 4 || R == 8, "radix");
+    u[1] = cmul(u[1], w1);
+    if constexpr (R >= 3) {
+        const double2 w2 = cmul(w1, w1);
+        u[2] = cmul(u[2], w2);
+        if constexpr (R >= 4) {
+            const double2 w3 = cmul(w2, w1);
+            u[3] = cmul(u[3], w3);
+            if constexpr (R == 8) {
+                const double2 w4 = cmul(w2, w2);
+                u[4] = cmul(u[4], w4);
+                u[5] = cmul(u[5], cmul(w4, w1));
+                u[6] = cmul(u[6], cmul(w4, w2));
+                u[7] = cmul(u[7], cmul(w4, w3));
+            }
+        }
     }
 }
 
@@ -372,22 +374,18 @@ __device__ __forceinline__ void fft_pass_ip(double2* __restrict__ buf, const dou
         double2 u[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) u[m] = buf[SW(base + m * SS)];
-        double2 w[R];   // w[k] = exp(2 pi i j k / LS), conjugated for the r2c
         if constexpr (SS > 1) {
-            pass_twiddles<R, SS>(tw, j, w);
+            double2 w1 = __ldg(tw + j);   // exp(2 pi i j / LS), conjugated for the r2c
             if (DIT) {
-#pragma unroll
-                for (int k = 1; k < R; ++k) w[k].y = -w[k].y;
+                w1.y = -w1.y;
+                twiddle_apply<R>(u, w1);
+                dft_small(R, u, sign);
+            } else {
+                dft_small(R, u, sign);
+                twiddle_apply<R>(u, w1);
             }
-        }
-        if (SS > 1 && DIT) {
-#pragma unroll
-            for (int m = 1; m < R; ++m) u[m] = cmul(u[m], w[m]);
-        }
-        dft_small(R, u, sign);
-        if (SS > 1 && !DIT) {
-#pragma unroll
-            for (int k = 1; k < R; ++k) u[k] = cmul(u[k], w[k]);
+        } else {
+            dft_small(R, u, sign);
         }
 #pragma unroll
         for (int m = 0; m < R; ++m) buf[SW(base + m * SS)] = u[m];

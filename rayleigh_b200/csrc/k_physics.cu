@@ -13,10 +13,11 @@
 //
 // One CTA (384 threads, two per SM) handles one row; the rows theta and
 // pi - theta are the two CTAs of a cluster, which fold their spectra through
-// distributed shared memory.  The 14 input fields go through the FFT four at a
-// time; the four nonlinear outputs accumulate in shared memory (each thread
-// owns its points), the velocity in registers, the row's radial and
-// colatitude factors in shared memory.
+// distributed shared memory.  The 14 input fields go through the FFT in
+// batches of four, four, four and two; the four nonlinear outputs accumulate
+// in shared memory (each thread owns its points), the velocity in registers,
+// the row's radial and colatitude factors in shared memory.  The same c2r
+// serves the output-iteration diagnostics (kinetic energy, shell slices).
 //
 // FFT: a real length-2N transform through one complex length-N transform
 // (N = n_theta = 2^a 3^b), in place in shared memory: decimation in frequency
@@ -24,8 +25,10 @@
 // a digit-reversed order; the nonlinear terms are pointwise in phi, so they
 // are formed in that order, and the r2c runs the passes in reverse
 // (decimation in time) back to natural order.  One twiddle table load per
-// butterfly, the other powers by complex products.  Unnormalised like FFTW
-// (the normalisation lives in the Legendre tables).
+// butterfly, the other powers by complex products; two passes deal their
+// butterflies over pairs of fields so that shared accesses avoid bank
+// conflicts (butterfly_of).  Unnormalised like FFTW (the normalisation lives
+// in the Legendre tables).
 #include <cmath>
 #include <vector>
 #include <algorithm>

@@ -143,6 +143,15 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);
 
+/* Shell averages of the current state (Shell_Averages output, Spherical_IO.F90
+ * Add_Quantity :548-575 with ComputeEll0 :1350-1391): for each quantity of
+ * quantities[0..nq) (codes as above) and each radius, the mean over the sphere
+ * (phi mean, Gauss-Legendre theta weights / 2) and the same average of
+ * (q - mean)^2, ^3, ^4, into out(n_r, 4, nq) (Fortran order).  Runs the stages
+ * that form the fields on the grid (as ra_kinetic_energy); unknown codes
+ * return RA_ERR_ARG. */
+int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

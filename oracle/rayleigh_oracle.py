@@ -905,6 +905,25 @@ class Oracle:
         ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
         return float(np.dot(self.radial_integration_weights(), ell0))
 
+    def shell_averages(self, names):
+        """Shell_Averages (Spherical_IO.F90 Add_Quantity :548-575 with ComputeEll0
+        :1350-1391) of the last physical-space stage's fields (keys of last_fields): per
+        radius the mean over phi and over theta with the Gauss-Legendre weights / 2, and
+        the same average of (q - mean)^m for m = 2, 3, 4.  Returns [len(names), 4, n_r]."""
+        th = self.last_velocity[3]
+        if not (isinstance(th, slice) and th == slice(None)):
+            raise ValueError("the last physical-space stage did not cover every theta row")
+        tw = (self.h.wq / 2.0).astype(np.float64)
+        out = np.zeros((len(names), 4, self.cfg.n_r))
+        for i, name in enumerate(names):
+            q = self.last_fields[name]                      # [theta, r, phi]
+            mean = np.einsum("t,tr->r", tw, q.mean(axis=2))
+            out[i, 0] = mean
+            d = q - mean[None, :, None]
+            for m in (2, 3, 4):
+                out[i, m - 1] = np.einsum("t,tr->r", tw, (d ** m).mean(axis=2))
+        return out
+
     def benchmark_point_observations(self, msymm=4, fields=None):
         """Assemble_Strips and Point_Observations (Benchmarking.F90:934-1063) on the last
         physical-space stage, or on ``fields`` = (v_r, v_phi, T) given as [theta, r, phi]

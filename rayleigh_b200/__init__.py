@@ -124,6 +124,7 @@ def load_library(path: str | None = None):
         "ra_advance": ([_VP], ctypes.c_int),
         "ra_kinetic_energy": ([_VP, _DP], ctypes.c_int),
         "ra_shell_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_shell_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -284,6 +285,14 @@ class Rayleigh:
         out = np.empty((len(q), len(lv), self.n_theta, self.n_phi))
         self._check(self.lib.ra_shell_slices(self.h, q.ctypes.data, len(q), lv.ctypes.data, len(lv),
                                              out.ctypes.data))
+        return out
+
+    def shell_averages(self, quantities):
+        """Shell averages of the current state: array [quantity][moment][r], moment 0 the
+        mean over the sphere, 1-3 the averages of (q - mean)^2, ^3, ^4."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        out = np.empty((len(q), 4, self.n_r))
+        self._check(self.lib.ra_shell_averages(self.h, q.ctypes.data, len(q), out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

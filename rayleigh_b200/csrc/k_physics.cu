@@ -1050,4 +1050,131 @@ void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out) {
     ++c.launches;
 }
 
+// Shell averages (Spherical_IO.F90 Shell_Averages, ComputeEll0 :1350-1391) of
+// one diagnostic quantity: one CTA per (theta, r) row forms the quantity on the
+// phi grid (as shell_slice_kernel) and writes its theta-weighted phi sum:
+// MOMENTS = false, sum q (the mean's share, slot 0); MOMENTS = true, the sums
+// of (q - mean(r))^m for m = 2, 3, 4 (slots 1-3).  rows[slot][theta][r];
+// kew[theta] = Gauss-Legendre weight / 2 / n_phi.
+template <int N, bool MOMENTS>
+__global__ void __launch_bounds__(ROW_THREADS) shell_moment_rows_kernel(PhysParams P, SliceSpec S,
+                                                                        const double* __restrict__ kew,
+                                                                        const double* __restrict__ mean,
+                                                                        double* __restrict__ rows) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    __shared__ double red[3][ROW_THREADS / 32];
+    const int t = threadIdx.x;
+    const int h = (int)(blockIdx.x & 1);
+    const int thh = (int)(blockIdx.x >> 1);
+    const int th = h ? (N - 1 - thh) : thh;
+    const int r = (int)blockIdx.y;
+    const int nr = P.nr;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double mu = MOMENTS ? mean[r] : 0.0;
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q)
+        if (t + q * ROW_THREADS < N) {
+            const double a = y[0][q].x * scale - mu, b = y[0][q].y * scale - mu;
+            if (MOMENTS) {
+                const double a2 = a * a, b2 = b * b;
+                s1 += a2 + b2;
+                s2 += a2 * a + b2 * b;
+                s3 += a2 * a2 + b2 * b2;
+            } else {
+                s1 += a + b;
+            }
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        if (MOMENTS) {
+            s2 += __shfl_down_sync(0xffffffffu, s2, o);
+            s3 += __shfl_down_sync(0xffffffffu, s3, o);
+        }
+    }
+    if ((t & 31) == 0) {
+        red[0][t >> 5] = s1;
+        red[1][t >> 5] = s2;
+        red[2][t >> 5] = s3;
+    }
+    __syncthreads();
+    if (t < (MOMENTS ? 3 : 1)) {
+        double v = red[t][0];
+        for (int i = 1; i < ROW_THREADS / 32; ++i) v += red[t][i];
+        const int slot = MOMENTS ? 1 + t : 0;
+        rows[((long)slot * N + th) * nr + r] = v * kew[th];
+    }
+}
+
+// out[slot][r] = sum over theta of rows[slot][theta][r], in a fixed order (one
+// CTA per (r, slot)).
+__global__ void __launch_bounds__(256) shell_reduce_kernel(const double* __restrict__ rows, int nth, int nr,
+                                                           int slot0, double* __restrict__ out) {
+    __shared__ double red[8];
+    const int r = (int)blockIdx.x, slot = slot0 + (int)blockIdx.y, t = threadIdx.x;
+    double s = 0.0;
+    for (int th = t; th < nth; th += 256) s += rows[((long)slot * nth + th) * nr + r];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((t & 31) == 0) red[t >> 5] = s;
+    __syncthreads();
+    if (t == 0) {
+        double v = red[0];
+        for (int i = 1; i < 8; ++i) v += red[i];
+        out[(long)slot * nr + r] = v;
+    }
+}
+
+// The four shell moments of one quantity into out[4][nr] (device): mean, then
+// the theta-phi averages of (q - mean)^2, ^3, ^4.  rows: 4 nth nr scratch.
+void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out) {
+    if (!c.d_twp || !c.d_kew) throw ArgError("diagnostic tables not prepared at set-up");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
+    auto go = [&](auto k0, auto k1, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RA_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k0<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, c.d_kew, out, rows);
+        RA_CUDA(cudaGetLastError());
+        shell_reduce_kernel<<<dim3((unsigned)c.d.nr, 1), 256, 0, c.stream>>>(rows, c.d.nth, c.d.nr, 0, out);
+        RA_CUDA(cudaGetLastError());
+        k1<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, c.d_kew, out, rows);   // reads the mean, out[0][r]
+        RA_CUDA(cudaGetLastError());
+        shell_reduce_kernel<<<dim3((unsigned)c.d.nr, 3), 256, 0, c.stream>>>(rows, c.d.nth, c.d.nr, 1, out);
+        RA_CUDA(cudaGetLastError());
+    };
+#define RA_MOM(n) go(shell_moment_rows_kernel<n, false>, shell_moment_rows_kernel<n, true>, n)
+    switch (c.d.nth) {
+        case 24: RA_MOM(24); break;
+        case 32: RA_MOM(32); break;
+        case 48: RA_MOM(48); break;
+        case 64: RA_MOM(64); break;
+        case 96: RA_MOM(96); break;
+        case 128: RA_MOM(128); break;
+        case 192: RA_MOM(192); break;
+        case 256: RA_MOM(256); break;
+        case 384: RA_MOM(384); break;
+        case 512: RA_MOM(512); break;
+        case 768: RA_MOM(768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no shell-average kernel instance");
+    }
+#undef RA_MOM
+    c.launches += 4;
+}
+
 }  // namespace ra

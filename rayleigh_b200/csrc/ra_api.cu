@@ -767,22 +767,27 @@ static const QuantitySource kQuantities[] = {
     {501, A_T, 0, 0},     {507, A_DTDR, 0, 0},  {513, A_DTDT, 0, 1},  {519, A_T, 1, 0},
 };
 
+static std::vector<SliceSpec> quantity_specs(const int* quantities, int nq) {
+    std::vector<SliceSpec> spec(nq);
+    for (int q = 0; q < nq; ++q) {
+        const QuantitySource* src = nullptr;
+        for (const QuantitySource& k : kQuantities)
+            if (k.code == quantities[q]) src = &k;
+        if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " is not provided");
+        spec[q] = SliceSpec{};
+        spec[q].field = src->field;
+        spec[q].dphi = src->dphi;
+        spec[q].csc = src->csc;
+    }
+    return spec;
+}
+
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     if (!quantities || !levels || !out || nq < 1 || nlev < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        std::vector<SliceSpec> spec(nq);
-        for (int q = 0; q < nq; ++q) {
-            const QuantitySource* src = nullptr;
-            for (const QuantitySource& k : kQuantities)
-                if (k.code == quantities[q]) src = &k;
-            if (!src) throw ArgError("shell slice: quantity code " + std::to_string(quantities[q]) + " is not provided");
-            spec[q] = SliceSpec{};
-            spec[q].field = src->field;
-            spec[q].dphi = src->dphi;
-            spec[q].csc = src->csc;
-        }
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
         for (int l = 0; l < nlev; ++l)
             if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell slice: radial index out of range");
         // the slices go through p2b, which the step rewrites before reading
@@ -803,6 +808,29 @@ int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* level
                                         cudaMemcpyDeviceToHost, c.stream));
             }
         RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
+    });
+}
+
+int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !out || nq < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        // row sums and the moments go through p2b, which the step rewrites before reading
+        const long nrows = (long)c.d.nth * c.d.nr;
+        double* rows = c.d_p2b;
+        double* dev_out = c.d_p2b + 4 * nrows;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q) {
+            launch_shell_moments(c, spec[q], rows, dev_out);
+            RA_CUDA(cudaMemcpyAsync(out + (long)q * 4 * c.d.nr, dev_out, 4 * (size_t)c.d.nr * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));   // dev_out is reused by the next quantity
+        }
         check_status(c);
     });
 }

@@ -156,6 +156,7 @@ struct SliceSpec {
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);
+void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

@@ -71,3 +71,4 @@ def test_diagnostic_quantity_codes_are_the_references():
     assert lib.ra_kinetic_energy(None, ctypes.byref(ke)) == rb.RA_ERR_STATE
     q = (ctypes.c_int * 1)(1)
     assert lib.ra_shell_slices(None, q, 1, q, 1, None) == rb.RA_ERR_STATE
+    assert lib.ra_shell_averages(None, q, 1, None) == rb.RA_ERR_STATE

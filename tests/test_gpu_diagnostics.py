@@ -104,3 +104,34 @@ def test_shell_slices_match_the_oracle(precision, tol):
         print(precision, name, err)
         assert err < tol, (name, err)
     assert np.array_equal(again[0, 0], sl[0, 5])
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-8)])
+def test_shell_averages_match_the_oracle(precision, tol):
+    """Mean and central moments 2-4 per radius of every provided quantity against the
+    oracle's restatement of Shell_Averages; each moment m is compared on the scale S^m,
+    S the quantity's largest RMS over the radii (some quantities vanish at the walls)."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        av = g.shell_averages(names)
+        sw, sz, sab = g.get_state()
+        with pytest.raises(rb.RayleighError):
+            g.shell_averages([502])
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    ref = o.shell_averages([_ORACLE_NAME[n] for n in names])
+    assert av.shape == ref.shape == (len(names), 4, oc.n_r)
+    for i, name in enumerate(names):
+        S = np.sqrt((ref[i, 1] + ref[i, 0] ** 2).max())
+        assert S > 0
+        for m in range(4):
+            err = np.abs(av[i, m] - ref[i, m]).max() / S ** (m + 1)
+            print(precision, name, m, err)
+            assert err < tol, (name, m, err)

@@ -152,6 +152,12 @@ int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* level
  * return RA_ERR_ARG. */
 int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
 
+/* Azimuthal averages of the current state (AZ_Avgs output, Spherical_IO.F90
+ * :477-481): the phi mean of each quantity at every (r, theta) point, into
+ * out(n_r, n_theta, nq) (Fortran order; theta in the grid's order).  Codes and
+ * errors as for ra_shell_slices. */
+int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

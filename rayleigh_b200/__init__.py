@@ -125,6 +125,7 @@ def load_library(path: str | None = None):
         "ra_kinetic_energy": ([_VP, _DP], ctypes.c_int),
         "ra_shell_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_shell_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_azimuthal_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -293,6 +294,13 @@ class Rayleigh:
         q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
         out = np.empty((len(q), 4, self.n_r))
         self._check(self.lib.ra_shell_averages(self.h, q.ctypes.data, len(q), out.ctypes.data))
+        return out
+
+    def azimuthal_averages(self, quantities):
+        """Azimuthal (phi) averages of the current state: array [quantity][theta][r]."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        out = np.empty((len(q), self.n_theta, self.n_r))
+        self._check(self.lib.ra_azimuthal_averages(self.h, q.ctypes.data, len(q), out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

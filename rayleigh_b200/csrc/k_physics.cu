@@ -1177,4 +1177,44 @@ void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out)
     c.launches += 4;
 }
 
+// Azimuthal averages (AZ_Avgs) of one quantity: the phi mean of every
+// (theta, r) row into rows[theta][r] (the shell-moment row kernel with the
+// weights 1 / n_phi).
+void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows) {
+    if (!c.d_twp || !c.d_kaz) throw ArgError("diagnostic tables not prepared at set-up");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
+    auto go = [&](auto k0, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k0<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, c.d_kaz, nullptr, rows);
+    };
+#define RA_AZ(n) go(shell_moment_rows_kernel<n, false>, n)
+    switch (c.d.nth) {
+        case 24: RA_AZ(24); break;
+        case 32: RA_AZ(32); break;
+        case 48: RA_AZ(48); break;
+        case 64: RA_AZ(64); break;
+        case 96: RA_AZ(96); break;
+        case 128: RA_AZ(128); break;
+        case 192: RA_AZ(192); break;
+        case 256: RA_AZ(256); break;
+        case 384: RA_AZ(384); break;
+        case 512: RA_AZ(512); break;
+        case 768: RA_AZ(768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no azimuthal-average kernel instance");
+    }
+#undef RA_AZ
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

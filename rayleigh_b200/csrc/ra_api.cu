@@ -405,6 +405,12 @@ static void setup(Ctx& c) {
     dalloc(c.d_s2b, (size_t)nlm * NP2B * 2 * nr);
     dalloc(c.d_cfl, 1);
     dalloc(c.d_kew, kew.size());
+    {
+        const std::vector<double> kaz((size_t)d.nth, 1.0 / d.nphi);
+        dalloc(c.d_kaz, kaz.size());
+        RA_CUDA(cudaMemcpyAsync(c.d_kaz, kaz.data(), kaz.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    }
     dalloc(c.d_ke_rows, (size_t)d.nth * nr + 1);
     RA_CUDA(cudaMemcpyAsync(c.d_kew, kew.data(), kew.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_ab, 0, (size_t)4 * nlm * 2 * nr * sizeof(double), c.stream));
@@ -452,7 +458,7 @@ static void release(Ctx& c) {
     if (c.graph) cudaGraphDestroy(c.graph);
     double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp, c.d_Awpt, c.d_Az,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
-                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows};
+                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz};
     for (double* b : bufs)
         if (b) cudaFree(b);
     int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status};
@@ -830,6 +836,26 @@ int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
             RA_CUDA(cudaMemcpyAsync(out + (long)q * 4 * c.d.nr, dev_out, 4 * (size_t)c.d.nr * sizeof(double),
                                     cudaMemcpyDeviceToHost, c.stream));
             RA_CUDA(cudaStreamSynchronize(c.stream));   // dev_out is reused by the next quantity
+        }
+        check_status(c);
+    });
+}
+
+int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !out || nq < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const long nrows = (long)c.d.nth * c.d.nr;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q) {
+            launch_azimuthal_average(c, spec[q], c.d_p2b);   // p2b: scratch between steps
+            RA_CUDA(cudaMemcpyAsync(out + (long)q * nrows, c.d_p2b, (size_t)nrows * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));
         }
         check_status(c);
     });

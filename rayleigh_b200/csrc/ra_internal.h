@@ -128,6 +128,7 @@ struct Ctx {
     int *d_status = nullptr;                          // device error word
     double *d_kew = nullptr;                          // [nth] theta weights / n_phi, then [nr] radial weights
     double *d_ke_rows = nullptr;                      // [nth][nr] kinetic-energy shares, then the sum
+    double *d_kaz = nullptr;                          // [nth] 1 / n_phi (azimuthal averages)
 
     MixedPlan mx_inv, mx_fwd, mx_solve;               // RA_PREC_MIXED Legendre transforms, implicit solve
 
@@ -157,6 +158,7 @@ struct SliceSpec {
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);
 void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out);
+void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

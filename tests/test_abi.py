@@ -72,3 +72,4 @@ def test_diagnostic_quantity_codes_are_the_references():
     q = (ctypes.c_int * 1)(1)
     assert lib.ra_shell_slices(None, q, 1, q, 1, None) == rb.RA_ERR_STATE
     assert lib.ra_shell_averages(None, q, 1, None) == rb.RA_ERR_STATE
+    assert lib.ra_azimuthal_averages(None, q, 1, None) == rb.RA_ERR_STATE

@@ -135,3 +135,28 @@ def test_shell_averages_match_the_oracle(precision, tol):
             err = np.abs(av[i, m] - ref[i, m]).max() / S ** (m + 1)
             print(precision, name, m, err)
             assert err < tol, (name, m, err)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+def test_azimuthal_averages_match_the_oracle(precision, tol):
+    """The phi mean of every provided quantity at every (theta, r) point against the
+    oracle's physical-space buffer, on the scale of the quantity's largest magnitude."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        az = g.azimuthal_averages(names)
+        sw, sz, sab = g.get_state()
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    for i, name in enumerate(names):
+        q = o.last_fields[_ORACLE_NAME[name]]           # [theta, r, phi]
+        ref = q.mean(axis=2)
+        err = np.abs(az[i] - ref).max() / np.abs(q).max()
+        print(precision, name, err)
+        assert err < tol, (name, err)

@@ -470,18 +470,22 @@ __global__ void __launch_bounds__(OZ_ROWS_THREADS) ozaki_split_rows_kernel(const
     const long sk = jb.sk;
     const int K = jb.K;
     const double* __restrict__ xr = jb.X + (long)(live ? r : 0) * jb.sr;
-    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    // eight loads in flight per thread: this pass streams the operand from HBM
+    double mm[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) mm[i] = 0.0;
     if (live) {
         int k = kl;
-        for (; k + 3 * OZ_KLANES < K; k += 4 * OZ_KLANES) {
-            m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
-            m1 = fmax(m1, fabs(__ldg(xr + (k + OZ_KLANES) * sk)));
-            m2 = fmax(m2, fabs(__ldg(xr + (k + 2 * OZ_KLANES) * sk)));
-            m3 = fmax(m3, fabs(__ldg(xr + (k + 3 * OZ_KLANES) * sk)));
+        for (; k + 7 * OZ_KLANES < K; k += 8 * OZ_KLANES) {
+            double v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = __ldg(xr + (long)(k + i * OZ_KLANES) * sk);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) mm[i] = fmax(mm[i], fabs(v[i]));
         }
-        for (; k < K; k += OZ_KLANES) m0 = fmax(m0, fabs(__ldg(xr + k * sk)));
+        for (; k < K; k += OZ_KLANES) mm[0] = fmax(mm[0], fabs(__ldg(xr + (long)k * sk)));
     }
-    red[kl][lrow] = fmax(fmax(m0, m1), fmax(m2, m3));
+    red[kl][lrow] = fmax(fmax(fmax(mm[0], mm[1]), fmax(mm[2], mm[3])), fmax(fmax(mm[4], mm[5]), fmax(mm[6], mm[7])));
     __syncthreads();
     double mx = red[0][lrow];
 #pragma unroll

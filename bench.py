@@ -361,10 +361,13 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     bound, amount = work[dom]
     avg_s = per_kernel[dom] / args.steps * 1e-3
     traffic = None
+    binding = None
     tpath = os.path.join(HERE, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"{dom}_{prec_name}_lmax{args.lmax}_nr{args.nr}")
+            tj = json.load(open(tpath))
+            traffic = tj.get(f"{dom}_{prec_name}_lmax{args.lmax}_nr{args.nr}")
+            binding = tj.get(f"{dom}_binding_unit")   # the unit ncu shows saturated, when it is not HBM
         except Exception:
             traffic = None
     if bound == "tensor":
@@ -401,7 +404,7 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
                      "traffic_unit": "GB per launch (ncu dram bytes read + written)" if traffic is not None else None,
                      "algorithmic": amount / (1e12 if bound == "tensor" else 1e9),
                      "algorithmic_unit": "TFLOP per launch" if bound == "tensor" else "GB per launch",
-                     "peak_source": peak_note},
+                     "peak_source": peak_note, "binding_unit": binding},
         "kernels": kernels,
         "gpu_launches": launches,
         "clocks": clk.summary(),

@@ -158,6 +158,14 @@ int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
  * errors as for ra_shell_slices. */
 int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
 
+/* Shell spectra of the current state (Shell_Spectra output; Parallel_IO.F90
+ * Spectral_Prep :973-1047): each quantity at the radial indices levels[0..nlev)
+ * taken to (l, m) space by the unnormalised phi FFT and the forward Legendre
+ * transform (FFT_To_Spectral, Legendre_Transform p2b -> s2b), into
+ * out(l_max+1 [l], l_max+1 [m], 2 [re, im], nlev, nq) (Fortran order; zero for
+ * l < m).  Codes, levels and errors as for ra_shell_slices. */
+int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

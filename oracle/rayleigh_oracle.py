@@ -924,6 +924,26 @@ class Oracle:
                 out[i, m - 1] = np.einsum("t,tr->r", tw, (d ** m).mean(axis=2))
         return out
 
+    def shell_spectra(self, names, levels):
+        """Shell_Spectra (Parallel_IO.F90 Spectral_Prep :973-1047) of the last physical-space
+        stage's fields at the radial indices ``levels``: the unnormalised r2c along phi
+        (FFT_To_Spectral) and PtS_4d_dgpv3.  Returns [len(names), len(levels), 2, L, L] as
+        [re/im][m][l], zero for l < m."""
+        th = self.last_velocity[3]
+        if not (isinstance(th, slice) and th == slice(None)):
+            raise ValueError("the last physical-space stage did not cover every theta row")
+        L = self.cfg.l_max + 1
+        lv = list(levels)
+        out = np.zeros((len(names), len(lv), 2, L, L))
+        for i, name in enumerate(names):
+            q = self.last_fields[name][:, lv, :]              # [theta, level, phi]
+            X = np.fft.rfft(q, axis=2)                         # unnormalised, like FFTW's r2c
+            p2 = [np.stack([X[:, :, m].real.T, X[:, :, m].imag.T])[None] for m in range(L)]   # (1, 2, nlev, theta)
+            s2 = self.h.p2s(p2)
+            for m in range(L):
+                out[i, :, :, m, m:] = s2[m][0].transpose(1, 0, 2)   # (2, nlev, nl) -> (nlev, 2, nl)
+        return out
+
     def benchmark_point_observations(self, msymm=4, fields=None):
         """Assemble_Strips and Point_Observations (Benchmarking.F90:934-1063) on the last
         physical-space stage, or on ``fields`` = (v_r, v_phi, T) given as [theta, r, phi]

@@ -126,6 +126,7 @@ def load_library(path: str | None = None):
         "ra_shell_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_shell_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_azimuthal_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_shell_spectra": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -301,6 +302,17 @@ class Rayleigh:
         q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
         out = np.empty((len(q), self.n_theta, self.n_r))
         self._check(self.lib.ra_azimuthal_averages(self.h, q.ctypes.data, len(q), out.ctypes.data))
+        return out
+
+    def shell_spectra(self, quantities, levels):
+        """Shell spectra of the current state: array [quantity][level][re/im][m][l]
+        (l, m = 0 .. l_max; zero for l < m)."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        L = self.l_max + 1
+        out = np.empty((len(q), len(lv), 2, L, L))
+        self._check(self.lib.ra_shell_spectra(self.h, q.ctypes.data, len(q), lv.ctypes.data, len(lv),
+                                              out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

@@ -1217,4 +1217,129 @@ void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows) {
     ++c.launches;
 }
 
+// Shell spectra (Shell_Spectra output; Parallel_IO.F90 Spectral_Prep
+// :973-1047): the quantity on the phi grid (as shell_slice_kernel), its
+// unnormalised r2c (FFT_To_Spectral) and the equatorial fold of PtS with the
+// partner row (theta, pi - theta in one cluster, as physics_kernel), written
+// into the p2b layout at the column slot slot0 + level index; the forward
+// Legendre transform of that buffer then gives the (l, m) coefficients.
+template <int N>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
+    spectra_rows_kernel(PhysParams P, SliceSpec S, int slot0, double* __restrict__ p2b) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    constexpr int NI = N / 2 + 1;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    const int t = threadIdx.x;
+    const int h = (int)cluster.block_rank();
+    const int thh = (int)(blockIdx.x >> 1);
+    const int th = h ? (N - 1 - thh) : thh;
+    const int lv = (int)blockIdx.y;
+    const int r = S.level[lv];
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
+        const int p = t + q * ROW_THREADS;
+        if (p < N) buf[p] = make_double2(y[0][q].x * scale, y[0][q].y * scale);
+    }
+    __syncthreads();
+    fft_dit<N, 1, ROW_THREADS>(buf, P.twp, t);
+    const int L = P.L;
+    for (int k = t; k < NI; k += ROW_THREADS) {   // r2c steps, one (k, N - k) pair per item, in place
+        const double2 zk = buf[k];
+        const double2 zn = buf[(N - k) % N];
+        const double2 wk = __ldg(P.wr + k);
+        auto xval = [&](double2 a, double2 b, double2 w, bool zero_im) {
+            const double2 bn = cconj(b);
+            const double2 e = make_double2(0.5 * (a.x + bn.x), 0.5 * (a.y + bn.y));
+            const double2 d = make_double2(0.5 * (a.x - bn.x), 0.5 * (a.y - bn.y));
+            const double2 wd = cmul(cconj(w), d);
+            double2 X = make_double2(e.x + wd.y, e.y - wd.x);
+            if (zero_im) X.y = 0.0;
+            return X;
+        };
+        if (k < L) buf[k] = xval(zk, zn, wk, k == 0);
+        if (k != 0 && 2 * k != N && N - k < L) buf[N - k] = xval(zn, zk, make_double2(-wk.x, wk.y), false);
+    }
+    cluster.sync();
+    {
+        const double2* peer = cluster.map_shared_rank(buf, h ^ 1);
+        const long ncolb = (long)NP2B * P.nr * 2;
+        const long mstride = 2L * (N / 2) * ncolb;   // p2b[m][par][theta_h][col]
+        double* obase = p2b + (long)h * (N / 2) * ncolb + (long)thh * ncolb + (long)(slot0 + lv) * 2;
+        for (int k = t; k < L; k += ROW_THREADS) {
+            const double2 a = buf[k], b = peer[k];
+            *reinterpret_cast<double2*>(obase + k * mstride) = h ? csub(b, a) : cadd(a, b);
+        }
+    }
+    cluster.sync();   // the partner has finished reading this CTA's spectrum
+}
+
+// (l, m) coefficients of ns consecutive column slots of the forward transform's
+// output s2[row][slot][re/im] into out[slot][re/im][m][l] (zero for l < m).
+__global__ void spectra_gather_kernel(const double* __restrict__ s2, int L, int nslots, long rowlen,
+                                      double* __restrict__ out) {
+    const long total = (long)nslots * 2 * L * L;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int l = (int)(i % L);
+        const long rest = i / L;
+        const int m = (int)(rest % L);
+        const int ri = (int)((rest / L) % 2);
+        const int s = (int)(rest / (2L * L));
+        out[i] = (l >= m) ? s2[row_index(m, l, L) * rowlen + (long)s * 2 + ri] : 0.0;
+    }
+}
+
+void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b) {
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
+    if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("shell spectra: 1 .. 64 levels per launch");
+    if (slot0 < 0 || slot0 + S.nl > NP2B * c.d.nr) throw ArgError("shell spectra: column slots out of range");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)S.nl);
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, slot0, p2b);
+    };
+    switch (c.d.nth) {
+        case 24: go(spectra_rows_kernel<24>, 24); break;
+        case 32: go(spectra_rows_kernel<32>, 32); break;
+        case 48: go(spectra_rows_kernel<48>, 48); break;
+        case 64: go(spectra_rows_kernel<64>, 64); break;
+        case 96: go(spectra_rows_kernel<96>, 96); break;
+        case 128: go(spectra_rows_kernel<128>, 128); break;
+        case 192: go(spectra_rows_kernel<192>, 192); break;
+        case 256: go(spectra_rows_kernel<256>, 256); break;
+        case 384: go(spectra_rows_kernel<384>, 384); break;
+        case 512: go(spectra_rows_kernel<512>, 512); break;
+        case 768: go(spectra_rows_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no shell-spectra kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out) {
+    const long total = (long)nslots * 2 * c.d.L * c.d.L;
+    const unsigned blocks = (unsigned)std::min<long>((total + 255) / 256, 148L * 16);
+    spectra_gather_kernel<<<blocks, 256, 0, c.stream>>>(s2, c.d.L, nslots, (long)NP2B * c.d.nr * 2, out);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

@@ -861,6 +861,42 @@ int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* ou
     });
 }
 
+int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !levels || !out || nq < 1 || nlev < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        for (int l = 0; l < nlev; ++l)
+            if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell spectra: radial index out of range");
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        // (quantity, level) pairs fill the 4 n_r column slots of the p2b / s2b layouts, which the
+        // step rewrites before reading; each batch of slots goes through one forward transform
+        const long total = (long)nq * nlev;
+        const int cap = NP2B * c.d.nr;
+        const long per = 2L * c.d.L * c.d.L;
+        for (long s0 = 0; s0 < total; s0 += cap) {
+            const int ns = (int)std::min<long>(cap, total - s0);
+            for (long s = s0; s < s0 + ns;) {   // runs of one quantity, at most 64 levels each
+                const int q = (int)(s / nlev), l0 = (int)(s % nlev);
+                SliceSpec S = spec[q];
+                S.nl = (int)std::min<long>({(long)SliceSpec::MAXL, (long)(nlev - l0), s0 + ns - s});
+                for (int i = 0; i < S.nl; ++i) S.level[i] = levels[l0 + i];
+                launch_spectra_rows(c, S, (int)(s - s0), c.d_p2b);
+                s += S.nl;
+            }
+            launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+            launch_spectra_gather(c, c.d_s2b, ns, c.d_p2b);
+            RA_CUDA(cudaMemcpyAsync(out + s0 * per, c.d_p2b, (size_t)ns * per * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));
+        }
+        check_status(c);
+    });
+}
+
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {

@@ -160,3 +160,33 @@ def test_azimuthal_averages_match_the_oracle(precision, tol):
         err = np.abs(az[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
         assert err < tol, (name, err)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+def test_shell_spectra_match_the_oracle(precision, tol):
+    """(l, m) coefficients of every provided quantity at 30 levels (two batches of column
+    slots through the forward transform, runs of one quantity split across them) against
+    the oracle's r2c + PtS of its physical-space buffer, on the scale of each quantity's
+    largest coefficient."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    levels = [(5 * i + 1) % oc.n_r for i in range(30)]
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        sp = g.shell_spectra(names, levels)
+        sw, sz, sab = g.get_state()
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    ref = o.shell_spectra([_ORACLE_NAME[n] for n in names], levels)
+    assert sp.shape == ref.shape
+    for i, name in enumerate(names):
+        scale = np.abs(ref[i]).max()
+        assert scale > 0
+        err = np.abs(sp[i] - ref[i]).max() / scale
+        print(precision, name, err)
+        assert err < tol, (name, err)

@@ -166,6 +166,12 @@ int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* ou
  * l < m).  Codes, levels and errors as for ra_shell_slices. */
 int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);
 
+/* Equatorial slices of the current state (Equatorial_Slices output,
+ * Spherical_IO.F90:394-398: the mean of the theta rows n_theta/2 and
+ * n_theta/2 + 1) at every radius, into out(n_phi, n_r, nq) (Fortran order).
+ * Codes and errors as for ra_shell_slices. */
+int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

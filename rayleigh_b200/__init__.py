@@ -127,6 +127,7 @@ def load_library(path: str | None = None):
         "ra_shell_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_azimuthal_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_shell_spectra": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_equatorial_slices": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -313,6 +314,14 @@ class Rayleigh:
         out = np.empty((len(q), len(lv), 2, L, L))
         self._check(self.lib.ra_shell_spectra(self.h, q.ctypes.data, len(q), lv.ctypes.data, len(lv),
                                               out.ctypes.data))
+        return out
+
+    def equatorial_slices(self, quantities):
+        """Equatorial slices of the current state: array [quantity][r][phi], the mean of
+        the two theta rows nearest the equator."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        out = np.empty((len(q), self.n_r, self.n_phi))
+        self._check(self.lib.ra_equatorial_slices(self.h, q.ctypes.data, len(q), out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

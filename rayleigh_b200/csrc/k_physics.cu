@@ -1342,4 +1342,80 @@ void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out) {
     ++c.launches;
 }
 
+// Equatorial slices (Spherical_IO.F90:394-398: the theta rows n_theta/2 and
+// n_theta/2 + 1, weights 1/2 each): the pair of rows nearest the equator is one
+// cluster (theta_h = n_theta/2 - 1); each CTA forms its row on the phi grid (as
+// shell_slice_kernel) and rank 0 averages the two through distributed shared
+// memory into out[r][phi] (natural phi order).  One cluster per radius.
+template <int N>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
+    equatorial_slice_kernel(PhysParams P, SliceSpec S, double* __restrict__ out) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    const int t = threadIdx.x;
+    const int h = (int)cluster.block_rank();
+    const int thh = N / 2 - 1;
+    const int th = h ? (N - 1 - thh) : thh;
+    const int r = (int)blockIdx.y;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
+        const int p = t + q * ROW_THREADS;
+        if (p < N) buf[p] = make_double2(y[0][q].x * scale, y[0][q].y * scale);
+    }
+    cluster.sync();
+    if (h == 0) {
+        const double2* peer = cluster.map_shared_rank(buf, 1);
+        double2* row = reinterpret_cast<double2*>(out + (long)r * (2L * N));
+        for (int p = t; p < N; p += ROW_THREADS) {
+            const double2 a = buf[p], b = peer[p];
+            row[natural_index<N>(p)] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
+        }
+    }
+    cluster.sync();   // the partner has finished reading this CTA's row
+}
+
+void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out) {
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u, (unsigned)c.d.nr);
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, out);
+    };
+    switch (c.d.nth) {
+        case 24: go(equatorial_slice_kernel<24>, 24); break;
+        case 32: go(equatorial_slice_kernel<32>, 32); break;
+        case 48: go(equatorial_slice_kernel<48>, 48); break;
+        case 64: go(equatorial_slice_kernel<64>, 64); break;
+        case 96: go(equatorial_slice_kernel<96>, 96); break;
+        case 128: go(equatorial_slice_kernel<128>, 128); break;
+        case 192: go(equatorial_slice_kernel<192>, 192); break;
+        case 256: go(equatorial_slice_kernel<256>, 256); break;
+        case 384: go(equatorial_slice_kernel<384>, 384); break;
+        case 512: go(equatorial_slice_kernel<512>, 512); break;
+        case 768: go(equatorial_slice_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no equatorial-slice kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

@@ -897,6 +897,26 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
     });
 }
 
+int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !out || nq < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const long per = (long)c.d.nr * c.d.nphi;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q) {
+            launch_equatorial_slice(c, spec[q], c.d_p2b);   // p2b: scratch between steps
+            RA_CUDA(cudaMemcpyAsync(out + (long)q * per, c.d_p2b, (size_t)per * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));
+        }
+        check_status(c);
+    });
+}
+
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {

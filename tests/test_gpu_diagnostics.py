@@ -190,3 +190,29 @@ def test_shell_spectra_match_the_oracle(precision, tol):
         err = np.abs(sp[i] - ref[i]).max() / scale
         print(precision, name, err)
         assert err < tol, (name, err)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+def test_equatorial_slices_match_the_oracle(precision, tol):
+    """The mean of the two theta rows nearest the equator at every radius, against the
+    oracle's physical-space buffer, on the scale of the quantity's largest magnitude."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        eq = g.equatorial_slices(names)
+        sw, sz, sab = g.get_state()
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    nth = o.cfg.n_theta
+    for i, name in enumerate(names):
+        q = o.last_fields[_ORACLE_NAME[name]]           # [theta, r, phi]
+        ref = 0.5 * (q[nth // 2 - 1] + q[nth // 2])
+        err = np.abs(eq[i] - ref).max() / np.abs(q).max()
+        print(precision, name, err)
+        assert err < tol, (name, err)

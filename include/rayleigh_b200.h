@@ -172,6 +172,14 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
  * Codes and errors as for ra_shell_slices. */
 int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out);
 
+/* Meridional slices of the current state (Meridional_Slices output,
+ * Spherical_IO.F90:384-387, 467-473): each quantity at the phi indices
+ * phi_indices[0..nphi_sel) (0-based, 0 .. n_phi-1) at every (r, theta), into
+ * out(n_r, n_theta, nphi_sel, nq) (Fortran order).  Codes and errors as for
+ * ra_shell_slices; an index outside 0 .. n_phi-1 returns RA_ERR_ARG. */
+int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* phi_indices, int nphi_sel,
+                         double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

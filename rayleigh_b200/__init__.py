@@ -128,6 +128,7 @@ def load_library(path: str | None = None):
         "ra_azimuthal_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_shell_spectra": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_equatorial_slices": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_meridional_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -322,6 +323,15 @@ class Rayleigh:
         q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
         out = np.empty((len(q), self.n_r, self.n_phi))
         self._check(self.lib.ra_equatorial_slices(self.h, q.ctypes.data, len(q), out.ctypes.data))
+        return out
+
+    def meridional_slices(self, quantities, phi_indices):
+        """Meridional slices of the current state: array [quantity][phi index][theta][r]."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        ph = np.ascontiguousarray(phi_indices, dtype=np.int32)
+        out = np.empty((len(q), len(ph), self.n_theta, self.n_r))
+        self._check(self.lib.ra_meridional_slices(self.h, q.ctypes.data, len(q), ph.ctypes.data, len(ph),
+                                                  out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

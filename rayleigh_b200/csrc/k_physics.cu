@@ -1418,4 +1418,73 @@ void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out) {
     ++c.launches;
 }
 
+// Meridional slices (Spherical_IO.F90:384-387, 467-473): the quantity at
+// chosen phi indices (S.level[0 .. S.nl) holds them here) at every (theta, r);
+// one CTA per row forms the row on the phi grid, puts it in natural order in
+// shared memory and writes the chosen points to out[j][theta][r].
+template <int N>
+__global__ void __launch_bounds__(ROW_THREADS) meridional_slice_kernel(PhysParams P, SliceSpec S,
+                                                                       double* __restrict__ out) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    const int t = threadIdx.x;
+    const int h = (int)(blockIdx.x & 1);
+    const int thh = (int)(blockIdx.x >> 1);
+    const int th = h ? (N - 1 - thh) : thh;
+    const int r = (int)blockIdx.y;
+    const int nr = P.nr;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    __syncthreads();   // every thread has read its points out of the buffer
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {
+        const int p = t + q * ROW_THREADS;
+        if (p < N) buf[natural_index<N>(p)] = make_double2(y[0][q].x * scale, y[0][q].y * scale);
+    }
+    __syncthreads();
+    const double* row = reinterpret_cast<const double*>(buf);   // natural phi order
+    for (int j = t; j < S.nl; j += ROW_THREADS) out[((long)j * N + th) * nr + r] = row[S.level[j]];
+}
+
+void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out) {
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
+    if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("meridional slices: 1 .. 64 phi indices");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, out);
+    };
+    switch (c.d.nth) {
+        case 24: go(meridional_slice_kernel<24>, 24); break;
+        case 32: go(meridional_slice_kernel<32>, 32); break;
+        case 48: go(meridional_slice_kernel<48>, 48); break;
+        case 64: go(meridional_slice_kernel<64>, 64); break;
+        case 96: go(meridional_slice_kernel<96>, 96); break;
+        case 128: go(meridional_slice_kernel<128>, 128); break;
+        case 192: go(meridional_slice_kernel<192>, 192); break;
+        case 256: go(meridional_slice_kernel<256>, 256); break;
+        case 384: go(meridional_slice_kernel<384>, 384); break;
+        case 512: go(meridional_slice_kernel<512>, 512); break;
+        case 768: go(meridional_slice_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no meridional-slice kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

@@ -917,6 +917,34 @@ int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out
     });
 }
 
+int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* phi_indices, int nphi_sel,
+                         double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !phi_indices || !out || nq < 1 || nphi_sel < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        for (int j = 0; j < nphi_sel; ++j)
+            if (phi_indices[j] < 0 || phi_indices[j] >= c.d.nphi)
+                throw ArgError("meridional slices: phi index out of range");
+        const long per = (long)c.d.nth * c.d.nr;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q)
+            for (int j0 = 0; j0 < nphi_sel; j0 += SliceSpec::MAXL) {
+                SliceSpec S = spec[q];
+                S.nl = std::min(SliceSpec::MAXL, nphi_sel - j0);
+                for (int i = 0; i < S.nl; ++i) S.level[i] = phi_indices[j0 + i];
+                launch_meridional_slice(c, S, c.d_p2b);   // p2b: scratch between steps
+                RA_CUDA(cudaMemcpyAsync(out + ((long)q * nphi_sel + j0) * per, c.d_p2b,
+                                        (size_t)S.nl * per * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+                RA_CUDA(cudaStreamSynchronize(c.stream));
+            }
+        check_status(c);
+    });
+}
+
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {

@@ -162,6 +162,7 @@ void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows);
 void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b);
 void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out);
 void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out);
+void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

@@ -216,3 +216,34 @@ def test_equatorial_slices_match_the_oracle(precision, tol):
         err = np.abs(eq[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
         assert err < tol, (name, err)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-8)])
+def test_meridional_slices_match_the_oracle(precision, tol):
+    """Every provided quantity at 70 phi indices (two launches) at every (theta, r)
+    against the oracle's physical-space buffer, on the scale of its largest magnitude.
+    Pointwise, the mixed form's bound is 1e-8: the quantities divided by sin(theta)
+    carry the split-precision products' error amplified by 1/sin(theta) near the poles
+    (about 20 at N_theta = 48; measured 9e-10)."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    with _ctx(cfg) as g:
+        phis = [(13 * i + 3) % g.n_phi for i in range(70)]
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        me = g.meridional_slices(names, phis)
+        sw, sz, sab = g.get_state()
+        with pytest.raises(rb.RayleighError):
+            g.meridional_slices(["v_r"], [g.n_phi])
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    for i, name in enumerate(names):
+        q = o.last_fields[_ORACLE_NAME[name]]           # [theta, r, phi]
+        ref = q[:, :, phis].transpose(2, 0, 1)           # [j, theta, r]
+        err = np.abs(me[i] - ref).max() / np.abs(q).max()
+        print(precision, name, err)
+        assert err < tol, (name, err)

@@ -123,7 +123,7 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
  * indices levels[0..nlev) (0-based grid indices, 0 = outer boundary), into
  * out(n_phi, n_theta, nlev, nq) (Fortran order; phi fastest, theta in the
  * grid's order).  Quantity codes are the reference's output codes
- * (velocity_field_codes.F, thermal_field_codes.F) of values the
+ * (velocity_field_codes.F, vorticity_field_codes.F, thermal_field_codes.F) of values the
  * physical-space buffer holds: */
 #define RA_Q_V_R            1
 #define RA_Q_V_THETA        2
@@ -135,6 +135,7 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
 #define RA_Q_DV_R_DP       28
 #define RA_Q_DV_THETA_DP   29
 #define RA_Q_DV_PHI_DP     30
+#define RA_Q_VORT_R       301   /* l(l+1) Z / r^2 (Boussinesq radial vorticity) */
 #define RA_Q_ENTROPY      501
 #define RA_Q_ENTROPY_DR   507
 #define RA_Q_ENTROPY_DTHETA 513

@@ -764,13 +764,17 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
 }
 
 // Diagnostic quantity codes of the reference's output system (velocity_field_codes.F,
-// thermal_field_codes.F: voffset = 0, pt_off = 500) that are values of the
-// physical-space buffer, and where each comes from in p2a.
+// vorticity_field_codes.F, thermal_field_codes.F: voffset = 0, vort_off = 300,
+// pt_off = 500) that are values of the physical-space buffer, and where each
+// comes from in p2a.  vort_r, which Diagnostics_Vorticity_Field.F90:89-93 forms
+// as (dv_phi/dtheta + cot v_phi - csc dv_theta/dphi) / r, is the spectral
+// l(l+1) Z / r^2 here: the same band-limited field, equal up to rounding.
 struct QuantitySource { int code, field, dphi, csc; };
 static const QuantitySource kQuantities[] = {
     {1, A_VR, 0, 0},      {2, A_VT, 0, 1},      {3, A_VP, 0, 1},      {10, A_DVRDR, 0, 0}, {11, A_DVTDR, 0, 1},
     {12, A_DVPDR, 0, 1},  {19, A_DVRDT, 0, 1},  {28, A_VR, 1, 0},     {29, A_VT, 1, 1},    {30, A_VP, 1, 1},
     {501, A_T, 0, 0},     {507, A_DTDR, 0, 0},  {513, A_DTDT, 0, 1},  {519, A_T, 1, 0},
+    {301, A_OMR, 0, 0},   // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
 };
 
 static std::vector<SliceSpec> quantity_specs(const int* quantities, int nq) {

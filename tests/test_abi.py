@@ -56,14 +56,15 @@ def test_default_config_and_argument_errors_without_gpu():
 
 def test_diagnostic_quantity_codes_are_the_references():
     """RA_Q_* in the header, the Python names and the reference's output codes
-    (velocity_field_codes.F: voffset = 0; thermal_field_codes.F: pt_off = 500)
+    (velocity_field_codes.F: voffset = 0; vorticity_field_codes.F: vort_off = 300;
+    thermal_field_codes.F: pt_off = 500)
     agree; context-less diagnostic calls report a state error."""
     import rayleigh_b200 as rb
     src = open(os.path.join(ROOT, "include", "rayleigh_b200.h")).read()
     header = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"#define RA_Q_(\w+)\s+(\d+)", src)}
     assert header == rb.Rayleigh.QUANTITIES
     reference = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
-                 "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30,
+                 "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 300 + 1,
                  "entropy": 500 + 1, "entropy_dr": 500 + 7, "entropy_dtheta": 500 + 13, "entropy_dphi": 500 + 19}
     assert header == reference
     lib = rb.load_library()

@@ -68,7 +68,7 @@ def test_kinetic_energy_leaves_the_run_unchanged(precision):
 
 # the oracle's physical-space buffer names of the quantities ra_shell_slices provides
 _ORACLE_NAME = {"v_r": "vr", "v_theta": "vt", "v_phi": "vp", "dv_r_dr": "dvrdr", "dv_theta_dr": "dvtdr",
-                "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp",
+                "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp", "vort_r": "omr",
                 "dv_phi_dp": "dvpdp", "entropy": "t", "entropy_dr": "dtdr", "entropy_dtheta": "dtdt",
                 "entropy_dphi": "dtdp"}
 

@@ -181,6 +181,21 @@ int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out
 int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* phi_indices, int nphi_sel,
                          double* out);
 
+/* Global averages of the current state (G_Avgs output; Compute_Radial_Average,
+ * Spherical_IO.F90:1436-1470): the volume average of each quantity (the
+ * spherical means per radius weighted by the radial integration weights, as
+ * in ra_kinetic_energy), into out[0..nq).  Codes and errors as for
+ * ra_shell_slices. */
+int ra_global_averages(ra_ctx* ctx, const int* quantities, int nq, double* out);
+
+/* Point probes of the current state (Point_Probes output, Spherical_IO.F90:
+ * 379-382): each quantity at the tensor product of the radial, theta and phi
+ * grid indices (0-based; 1 .. 64 of each), into
+ * out(nphi_p, ntheta_p, nr_p, nq) (Fortran order).  Codes as for
+ * ra_shell_slices; an index out of range returns RA_ERR_ARG. */
+int ra_point_probes(ra_ctx* ctx, const int* quantities, int nq, const int* r_idx, int nr_p, const int* theta_idx,
+                    int ntheta_p, const int* phi_idx, int nphi_p, double* out);
+
 /* Timed stepping for benchmarks: runs nsteps like ra_step (without graph
  * replay, so that CUDA events on the context's stream bracket every kernel)
  * and returns the elapsed device time of the whole region in *total_ms and,

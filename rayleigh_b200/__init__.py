@@ -129,6 +129,9 @@ def load_library(path: str | None = None):
         "ra_shell_spectra": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_equatorial_slices": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_meridional_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_global_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_point_probes": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP],
+                            ctypes.c_int),
         "ra_sync": ([_VP], ctypes.c_int),
         "ra_legendre_s2p": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_legendre_p2s": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -332,6 +335,23 @@ class Rayleigh:
         out = np.empty((len(q), len(ph), self.n_theta, self.n_r))
         self._check(self.lib.ra_meridional_slices(self.h, q.ctypes.data, len(q), ph.ctypes.data, len(ph),
                                                   out.ctypes.data))
+        return out
+
+    def global_averages(self, quantities):
+        """Volume averages of the current state: array [quantity]."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        out = np.empty(len(q))
+        self._check(self.lib.ra_global_averages(self.h, q.ctypes.data, len(q), out.ctypes.data))
+        return out
+
+    def point_probes(self, quantities, r_idx, theta_idx, phi_idx):
+        """Point probes of the current state: array [quantity][r][theta][phi] at the
+        tensor product of the grid indices."""
+        q = np.ascontiguousarray([self.QUANTITIES.get(x, x) for x in quantities], dtype=np.int32)
+        ri, ti, pi = (np.ascontiguousarray(a, dtype=np.int32) for a in (r_idx, theta_idx, phi_idx))
+        out = np.empty((len(q), len(ri), len(ti), len(pi)))
+        self._check(self.lib.ra_point_probes(self.h, q.ctypes.data, len(q), ri.ctypes.data, len(ri), ti.ctypes.data,
+                                             len(ti), pi.ctypes.data, len(pi), out.ctypes.data))
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,

@@ -1487,4 +1487,126 @@ void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out) {
     ++c.launches;
 }
 
+// out[0] = sum_r w[r] v[r] in a fixed order (one warp).
+__global__ void radial_dot_kernel(const double* __restrict__ v, const double* __restrict__ w, int nr,
+                                  double* __restrict__ out) {
+    double s = 0.0;
+    for (int r = threadIdx.x; r < nr; r += 32) s += w[r] * v[r];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// Global average (G_Avgs; Compute_Radial_Average, Spherical_IO.F90:1436-1470)
+// of one quantity into out[0]: the spherical means per radius (the shell-moment
+// row kernel and the theta reduction) weighted by the radial integration
+// weights.  rows: nth nr scratch; mean: nr scratch.
+void launch_global_average(Ctx& c, const SliceSpec& S, double* rows, double* mean, double* out) {
+    if (!c.d_twp || !c.d_kew) throw ArgError("diagnostic tables not prepared at set-up");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
+    auto go = [&](auto k0, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k0<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, c.d_kew, nullptr, rows);
+    };
+#define RA_GA(n) go(shell_moment_rows_kernel<n, false>, n)
+    switch (c.d.nth) {
+        case 24: RA_GA(24); break;
+        case 32: RA_GA(32); break;
+        case 48: RA_GA(48); break;
+        case 64: RA_GA(64); break;
+        case 96: RA_GA(96); break;
+        case 128: RA_GA(128); break;
+        case 192: RA_GA(192); break;
+        case 256: RA_GA(256); break;
+        case 384: RA_GA(384); break;
+        case 512: RA_GA(512); break;
+        case 768: RA_GA(768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no global-average kernel instance");
+    }
+#undef RA_GA
+    RA_CUDA(cudaGetLastError());
+    shell_reduce_kernel<<<dim3((unsigned)c.d.nr, 1), 256, 0, c.stream>>>(rows, c.d.nth, c.d.nr, 0, mean);
+    RA_CUDA(cudaGetLastError());
+    radial_dot_kernel<<<1, 32, 0, c.stream>>>(mean, c.d_kew + c.d.nth, c.d.nr, out);
+    RA_CUDA(cudaGetLastError());
+    c.launches += 3;
+}
+
+// Point probes (Spherical_IO.F90:379-382: tensor products of radial, theta and
+// phi index lists): one CTA per chosen (theta, r) row forms the row on the phi
+// grid, in natural order in shared memory, and writes the chosen phi points to
+// out[r_i][theta_j][phi_k].
+template <int N>
+__global__ void __launch_bounds__(ROW_THREADS) point_probe_kernel(PhysParams P, SliceSpec S, ProbeSet Q,
+                                                                  double* __restrict__ out) {
+    constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    const int t = threadIdx.x;
+    const int jt = (int)blockIdx.x, ir = (int)blockIdx.y;
+    const int th = Q.theta[jt], r = Q.r[ir];
+    const int h = th >= N / 2 ? 1 : 0;
+    const int thh = h ? (N - 1 - th) : th;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const int fo[1] = {S.field};
+    const bool dp[1] = {S.dphi != 0};
+    double2 y[FB][ZPT];
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    __syncthreads();   // every thread has read its points out of the buffer
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) {
+        const int p = t + q * ROW_THREADS;
+        if (p < N) buf[natural_index<N>(p)] = make_double2(y[0][q].x * scale, y[0][q].y * scale);
+    }
+    __syncthreads();
+    const double* row = reinterpret_cast<const double*>(buf);
+    for (int k = t; k < Q.nphi; k += ROW_THREADS)
+        out[((long)ir * Q.ntheta + jt) * Q.nphi + k] = row[Q.phi[k]];
+}
+
+void launch_point_probes(Ctx& c, const SliceSpec& S, const ProbeSet& Q, double* out) {
+    if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
+    PhysParams P{};
+    P.p2a = c.d_p2a;
+    P.trig = c.d_costh;
+    P.wr = reinterpret_cast<const double2*>(c.d_twid);
+    P.twp = reinterpret_cast<const double2*>(c.d_twp);
+    P.L = c.d.L;
+    P.nth = c.d.nth;
+    P.nr = c.d.nr;
+    P.ncola = NP2A * c.d.nr * 2;
+    const dim3 grid((unsigned)Q.ntheta, (unsigned)Q.nr);
+    auto go = [&](auto kern, int n) {
+        const size_t smem = (size_t)fstride(n) * sizeof(double2);
+        RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, S, Q, out);
+    };
+    switch (c.d.nth) {
+        case 24: go(point_probe_kernel<24>, 24); break;
+        case 32: go(point_probe_kernel<32>, 32); break;
+        case 48: go(point_probe_kernel<48>, 48); break;
+        case 64: go(point_probe_kernel<64>, 64); break;
+        case 96: go(point_probe_kernel<96>, 96); break;
+        case 128: go(point_probe_kernel<128>, 128); break;
+        case 192: go(point_probe_kernel<192>, 192); break;
+        case 256: go(point_probe_kernel<256>, 256); break;
+        case 384: go(point_probe_kernel<384>, 384); break;
+        case 512: go(point_probe_kernel<512>, 512); break;
+        case 768: go(point_probe_kernel<768>, 768); break;
+        default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no point-probe kernel instance");
+    }
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ra

@@ -949,6 +949,63 @@ int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* 
     });
 }
 
+int ra_global_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !out || nq < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const long nrows = (long)c.d.nth * c.d.nr;
+        double* rows = c.d_p2b;                       // scratch between steps
+        double* mean = c.d_p2b + nrows;
+        double* res = mean + c.d.nr;                  // nq results
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q) launch_global_average(c, spec[q], rows, mean, res + q);
+        RA_CUDA(cudaMemcpyAsync(out, res, (size_t)nq * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
+    });
+}
+
+int ra_point_probes(ra_ctx* ctx, const int* quantities, int nq, const int* r_idx, int nr_p, const int* theta_idx,
+                    int ntheta_p, const int* phi_idx, int nphi_p, double* out) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!quantities || !r_idx || !theta_idx || !phi_idx || !out || nq < 1) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        if (nr_p < 1 || nr_p > ProbeSet::MAXP || ntheta_p < 1 || ntheta_p > ProbeSet::MAXP || nphi_p < 1 ||
+            nphi_p > ProbeSet::MAXP)
+            throw ArgError("point probes: 1 .. 64 indices per direction");
+        ProbeSet Q{};
+        Q.nr = nr_p;
+        Q.ntheta = ntheta_p;
+        Q.nphi = nphi_p;
+        for (int i = 0; i < nr_p; ++i) {
+            if (r_idx[i] < 0 || r_idx[i] >= c.d.nr) throw ArgError("point probes: radial index out of range");
+            Q.r[i] = r_idx[i];
+        }
+        for (int i = 0; i < ntheta_p; ++i) {
+            if (theta_idx[i] < 0 || theta_idx[i] >= c.d.nth) throw ArgError("point probes: theta index out of range");
+            Q.theta[i] = theta_idx[i];
+        }
+        for (int i = 0; i < nphi_p; ++i) {
+            if (phi_idx[i] < 0 || phi_idx[i] >= c.d.nphi) throw ArgError("point probes: phi index out of range");
+            Q.phi[i] = phi_idx[i];
+        }
+        const long per = (long)nr_p * ntheta_p * nphi_p;
+        double n, o;
+        ab_factors(c, n, o);
+        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        for (int q = 0; q < nq; ++q) launch_point_probes(c, spec[q], Q, c.d_p2b + q * per);   // p2b: scratch
+        RA_CUDA(cudaMemcpyAsync(out, c.d_p2b, (size_t)nq * per * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
+    });
+}
+
 int ra_rlm_b(ra_ctx* ctx) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     return guarded(ctx, [&] {

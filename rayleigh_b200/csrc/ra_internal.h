@@ -163,6 +163,14 @@ void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b);
 void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out);
 void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out);
 void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out);
+void launch_global_average(Ctx& c, const SliceSpec& S, double* rows, double* mean, double* out);
+// point-probe index lists (radial, theta, phi grid indices)
+struct ProbeSet {
+    static constexpr int MAXP = 64;
+    int nr, ntheta, nphi;
+    int r[MAXP], theta[MAXP], phi[MAXP];
+};
+void launch_point_probes(Ctx& c, const SliceSpec& S, const ProbeSet& Q, double* out);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
 void lt_forward_prepare(Ctx& c);

@@ -77,3 +77,5 @@ def test_diagnostic_quantity_codes_are_the_references():
     assert lib.ra_shell_spectra(None, q, 1, q, 1, None) == rb.RA_ERR_STATE
     assert lib.ra_equatorial_slices(None, q, 1, None) == rb.RA_ERR_STATE
     assert lib.ra_meridional_slices(None, q, 1, q, 1, None) == rb.RA_ERR_STATE
+    assert lib.ra_global_averages(None, q, 1, None) == rb.RA_ERR_STATE
+    assert lib.ra_point_probes(None, q, 1, q, 1, q, 1, q, 1, None) == rb.RA_ERR_STATE

@@ -247,3 +247,38 @@ def test_meridional_slices_match_the_oracle(precision, tol):
         err = np.abs(me[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
         assert err < tol, (name, err)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-8)])
+def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
+    """Volume averages (the oracle's shell means weighted by its radial integration
+    weights, on the scale of the quantity's largest magnitude) and point probes at a
+    5 x 7 x 9 index product (pointwise on the same scale; the mixed bound as for the
+    meridional slices) against the oracle."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    names = list(rb.Rayleigh.QUANTITIES)
+    ri, ti, pi = [0, 5, 11, 12, 23], [0, 3, 23, 24, 40, 46, 47], [0, 1, 17, 40, 41, 63, 64, 80, 95]
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        ga = g.global_averages(names)
+        pp = g.point_probes(names, ri, ti, pi)
+        sw, sz, sab = g.get_state()
+        with pytest.raises(rb.RayleighError):
+            g.point_probes(["v_r"], [0], [g.n_theta], [0])
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, sab)
+    o.step()
+    sa = o.shell_averages([_ORACLE_NAME[n] for n in names])
+    w = o.radial_integration_weights()
+    for i, name in enumerate(names):
+        q = o.last_fields[_ORACLE_NAME[name]]           # [theta, r, phi]
+        scale = np.abs(q).max()
+        e_ga = abs(ga[i] - float(np.dot(w, sa[i, 0]))) / scale
+        ref = q[np.ix_(ti, ri, pi)].transpose(1, 0, 2)  # [r, theta, phi]
+        e_pp = np.abs(pp[i] - ref).max() / scale
+        print(precision, name, e_ga, e_pp)
+        assert e_ga < tol and e_pp < tol, (name, e_ga, e_pp)

@@ -137,9 +137,11 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
 #define RA_Q_DV_PHI_DP     30
 #define RA_Q_VORT_R       301   /* l(l+1) Z / r^2 (Boussinesq radial vorticity) */
 #define RA_Q_ENTROPY      501
+#define RA_Q_PRESSURE     502   /* formed with the P grid in T's place */
 #define RA_Q_ENTROPY_DR   507
 #define RA_Q_ENTROPY_DTHETA 513
 #define RA_Q_ENTROPY_DPHI 519
+#define RA_Q_PRESSURE_DPHI 520
 /* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);

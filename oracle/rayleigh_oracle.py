@@ -741,6 +741,7 @@ class Oracle:
         f["dvtdp"] = dphi(f["vt"])
         f["dvpdp"] = dphi(f["vp"])
         f["dtdp"] = dphi(f["t"])
+        f["dpdp"] = dphi(f["p"])     # the diagnostics' pressure_dphi (only read by them)
         for k in list(f.keys()):
             f[k] = fft_c2r(f[k], nphi)[..., :nphi]
         csc = h.csctheta[th][:, None, None]

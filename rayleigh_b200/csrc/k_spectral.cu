@@ -433,6 +433,31 @@ static void bc_values(const Ctx& c, double& top, double& bot) {
     bot = (c.cfg.fix_tvar_bottom ? c.cfg.t_bottom : c.cfg.dtdr_bottom) * s4pi;
 }
 
+// Diagnostics of the pressure: the P grid g[G_P0] into the T field of s2a, so
+// that rlm_spacea and the inverse Legendre transform form P on the physical
+// grid in T's place (the T field there is the T grid copied unchanged).
+__global__ void pressure_to_s2a_kernel(const double* __restrict__ g, double* __restrict__ s2a, long nlm, int nr,
+                                       int L) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    const long lm = idx / nr;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const long plane = nlm * 2 * nr;   // g[o][lm][ri][r]
+    double* dst = s2a + row_index(m, l, L) * (NS2A * 2L * nr) + S_T * (2L * nr) + 2L * r;
+    dst[0] = g[G_P0 * plane + (lm * 2) * nr + r];
+    dst[1] = g[G_P0 * plane + (lm * 2 + 1) * nr + r];
+}
+
+void launch_pressure_to_s2a(Ctx& c) {
+    const long total = c.d.nlm * c.d.nr;
+    pressure_to_s2a_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_g, c.d_s2a, c.d.nlm, c.d.nr,
+                                                                                   c.d.L);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 void launch_rlm_b(Ctx& c, double new_ab) {
     const long total = c.d.nlm * c.d.nr;
     double top, bot;

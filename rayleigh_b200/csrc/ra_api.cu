@@ -747,14 +747,33 @@ int ra_physical(ra_ctx* ctx, double* cfl) {
     });
 }
 
+// The stages that form the fields on the physical grid (p2a) from the current
+// state; they only assign their outputs, so the next ra_step is unchanged.
+// With pressure, the P grid takes the place of T before rlm_spacea, so that
+// the T slot of p2a holds P.
+static void form_grid_fields(Ctx& c, bool pressure) {
+    double n, o;
+    ab_factors(c, n, o);
+    run_stage(c, 0, n, o);
+    run_stage(c, 1, n, o);
+    if (pressure) launch_pressure_to_s2a(c);
+    run_stage(c, 2, n, o);
+    run_stage(c, 3, n, o);
+}
+
+static void need_phase(Ctx& c, int& phase, const SliceSpec& S) {
+    if (phase != S.pressure) {
+        form_grid_fields(c, S.pressure != 0);
+        phase = S.pressure;
+    }
+}
+
 int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     if (!ke) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        form_grid_fields(c, false);
         launch_kinetic_energy(c);
         RA_CUDA(cudaMemcpyAsync(ke, c.d_ke_rows + (size_t)c.d.nth * c.d.nr, sizeof(double), cudaMemcpyDeviceToHost,
                                 c.stream));
@@ -769,12 +788,15 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
 // comes from in p2a.  vort_r, which Diagnostics_Vorticity_Field.F90:89-93 forms
 // as (dv_phi/dtheta + cot v_phi - csc dv_theta/dphi) / r, is the spectral
 // l(l+1) Z / r^2 here: the same band-limited field, equal up to rounding.
-struct QuantitySource { int code, field, dphi, csc; };
+struct QuantitySource { int code, field, dphi, csc, pressure; };
 static const QuantitySource kQuantities[] = {
-    {1, A_VR, 0, 0},      {2, A_VT, 0, 1},      {3, A_VP, 0, 1},      {10, A_DVRDR, 0, 0}, {11, A_DVTDR, 0, 1},
-    {12, A_DVPDR, 0, 1},  {19, A_DVRDT, 0, 1},  {28, A_VR, 1, 0},     {29, A_VT, 1, 1},    {30, A_VP, 1, 1},
-    {501, A_T, 0, 0},     {507, A_DTDR, 0, 0},  {513, A_DTDT, 0, 1},  {519, A_T, 1, 0},
-    {301, A_OMR, 0, 0},   // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
+    {1, A_VR, 0, 0, 0},     {2, A_VT, 0, 1, 0},     {3, A_VP, 0, 1, 0},     {10, A_DVRDR, 0, 0, 0},
+    {11, A_DVTDR, 0, 1, 0}, {12, A_DVPDR, 0, 1, 0}, {19, A_DVRDT, 0, 1, 0}, {28, A_VR, 1, 0, 0},
+    {29, A_VT, 1, 1, 0},    {30, A_VP, 1, 1, 0},    {501, A_T, 0, 0, 0},    {507, A_DTDR, 0, 0, 0},
+    {513, A_DTDT, 0, 1, 0}, {519, A_T, 1, 0, 0},
+    {301, A_OMR, 0, 0, 0},  // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
+    {502, A_T, 0, 0, 1},    // pressure, formed in T's place
+    {520, A_T, 1, 0, 1},    // d pressure / d phi
 };
 
 static std::vector<SliceSpec> quantity_specs(const int* quantities, int nq) {
@@ -788,6 +810,7 @@ static std::vector<SliceSpec> quantity_specs(const int* quantities, int nq) {
         spec[q].field = src->field;
         spec[q].dphi = src->dphi;
         spec[q].csc = src->csc;
+        spec[q].pressure = src->pressure;
     }
     return spec;
 }
@@ -805,14 +828,13 @@ int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* level
         const long room = (long)c.d.L * c.d.nth * NP2B * 2 * c.d.nr;
         if (room < per) throw ArgError("shell slice: no room for one slice");
         const int chunk = (int)std::min<long>(SliceSpec::MAXL, room / per);
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q)
             for (int l0 = 0; l0 < nlev; l0 += chunk) {
                 SliceSpec S = spec[q];
                 S.nl = std::min(chunk, nlev - l0);
                 for (int i = 0; i < S.nl; ++i) S.level[i] = levels[l0 + i];
+                need_phase(c, phase, S);
                 launch_shell_slice(c, S, c.d_p2b);
                 RA_CUDA(cudaMemcpyAsync(out + ((long)q * nlev + l0) * per, c.d_p2b, (size_t)S.nl * per * sizeof(double),
                                         cudaMemcpyDeviceToHost, c.stream));
@@ -832,10 +854,9 @@ int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
         const long nrows = (long)c.d.nth * c.d.nr;
         double* rows = c.d_p2b;
         double* dev_out = c.d_p2b + 4 * nrows;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q) {
+            need_phase(c, phase, spec[q]);
             launch_shell_moments(c, spec[q], rows, dev_out);
             RA_CUDA(cudaMemcpyAsync(out + (long)q * 4 * c.d.nr, dev_out, 4 * (size_t)c.d.nr * sizeof(double),
                                     cudaMemcpyDeviceToHost, c.stream));
@@ -852,10 +873,9 @@ int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* ou
         Ctx& c = ctx->c;
         const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
         const long nrows = (long)c.d.nth * c.d.nr;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q) {
+            need_phase(c, phase, spec[q]);
             launch_azimuthal_average(c, spec[q], c.d_p2b);   // p2b: scratch between steps
             RA_CUDA(cudaMemcpyAsync(out + (long)q * nrows, c.d_p2b, (size_t)nrows * sizeof(double),
                                     cudaMemcpyDeviceToHost, c.stream));
@@ -873,9 +893,7 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
         const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
         for (int l = 0; l < nlev; ++l)
             if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell spectra: radial index out of range");
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         // (quantity, level) pairs fill the 4 n_r column slots of the p2b / s2b layouts, which the
         // step rewrites before reading; each batch of slots goes through one forward transform
         const long total = (long)nq * nlev;
@@ -888,6 +906,7 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
                 SliceSpec S = spec[q];
                 S.nl = (int)std::min<long>({(long)SliceSpec::MAXL, (long)(nlev - l0), s0 + ns - s});
                 for (int i = 0; i < S.nl; ++i) S.level[i] = levels[l0 + i];
+                need_phase(c, phase, S);   // the phases' preparations leave p2b alone
                 launch_spectra_rows(c, S, (int)(s - s0), c.d_p2b);
                 s += S.nl;
             }
@@ -908,10 +927,9 @@ int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out
         Ctx& c = ctx->c;
         const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
         const long per = (long)c.d.nr * c.d.nphi;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q) {
+            need_phase(c, phase, spec[q]);
             launch_equatorial_slice(c, spec[q], c.d_p2b);   // p2b: scratch between steps
             RA_CUDA(cudaMemcpyAsync(out + (long)q * per, c.d_p2b, (size_t)per * sizeof(double),
                                     cudaMemcpyDeviceToHost, c.stream));
@@ -932,14 +950,13 @@ int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* 
             if (phi_indices[j] < 0 || phi_indices[j] >= c.d.nphi)
                 throw ArgError("meridional slices: phi index out of range");
         const long per = (long)c.d.nth * c.d.nr;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q)
             for (int j0 = 0; j0 < nphi_sel; j0 += SliceSpec::MAXL) {
                 SliceSpec S = spec[q];
                 S.nl = std::min(SliceSpec::MAXL, nphi_sel - j0);
                 for (int i = 0; i < S.nl; ++i) S.level[i] = phi_indices[j0 + i];
+                need_phase(c, phase, S);
                 launch_meridional_slice(c, S, c.d_p2b);   // p2b: scratch between steps
                 RA_CUDA(cudaMemcpyAsync(out + ((long)q * nphi_sel + j0) * per, c.d_p2b,
                                         (size_t)S.nl * per * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -959,10 +976,11 @@ int ra_global_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) 
         double* rows = c.d_p2b;                       // scratch between steps
         double* mean = c.d_p2b + nrows;
         double* res = mean + c.d.nr;                  // nq results
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
-        for (int q = 0; q < nq; ++q) launch_global_average(c, spec[q], rows, mean, res + q);
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
+        for (int q = 0; q < nq; ++q) {
+            need_phase(c, phase, spec[q]);
+            launch_global_average(c, spec[q], rows, mean, res + q);
+        }
         RA_CUDA(cudaMemcpyAsync(out, res, (size_t)nq * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
         check_status(c);
@@ -996,10 +1014,11 @@ int ra_point_probes(ra_ctx* ctx, const int* quantities, int nq, const int* r_idx
             Q.phi[i] = phi_idx[i];
         }
         const long per = (long)nr_p * ntheta_p * nphi_p;
-        double n, o;
-        ab_factors(c, n, o);
-        for (int k = 0; k < 4; ++k) run_stage(c, k, n, o);   // state -> p2a; the stages only assign
-        for (int q = 0; q < nq; ++q) launch_point_probes(c, spec[q], Q, c.d_p2b + q * per);   // p2b: scratch
+        int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
+        for (int q = 0; q < nq; ++q) {
+            need_phase(c, phase, spec[q]);
+            launch_point_probes(c, spec[q], Q, c.d_p2b + q * per);   // p2b: scratch
+        }
         RA_CUDA(cudaMemcpyAsync(out, c.d_p2b, (size_t)nq * per * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
         check_status(c);

@@ -154,6 +154,7 @@ void launch_kinetic_energy(Ctx& c);
 struct SliceSpec {
     static constexpr int MAXL = 64;
     int field, dphi, csc, nl;   // p2a field, d/dphi, times 1/sin(theta), levels in this launch
+    int pressure;               // formed with the P grid in T's place (pressure quantities)
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);
@@ -163,6 +164,7 @@ void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b);
 void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out);
 void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out);
 void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out);
+void launch_pressure_to_s2a(Ctx& c);
 void launch_global_average(Ctx& c, const SliceSpec& S, double* rows, double* mean, double* out);
 // point-probe index lists (radial, theta, phi grid indices)
 struct ProbeSet {

@@ -70,7 +70,7 @@ def test_kinetic_energy_leaves_the_run_unchanged(precision):
 _ORACLE_NAME = {"v_r": "vr", "v_theta": "vt", "v_phi": "vp", "dv_r_dr": "dvrdr", "dv_theta_dr": "dvtdr",
                 "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp", "vort_r": "omr",
                 "dv_phi_dp": "dvpdp", "entropy": "t", "entropy_dr": "dtdr", "entropy_dtheta": "dtdt",
-                "entropy_dphi": "dtdp"}
+                "entropy_dphi": "dtdp", "pressure": "p", "pressure_dphi": "dpdp"}
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -91,7 +91,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
         again = g.shell_slices(["v_r"], [levels[5]])
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_slices([502], [0])                 # pressure: not a value of this path's buffer
+            g.shell_slices([503], [0])                 # entropy_p (fluctuating part): not provided
         with pytest.raises(rb.RayleighError):
             g.shell_slices(["v_r"], [oc.n_r])
     o = O.Oracle(oc)
@@ -122,7 +122,7 @@ def test_shell_averages_match_the_oracle(precision, tol):
         av = g.shell_averages(names)
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_averages([502])
+            g.shell_averages([503])
     o = O.Oracle(oc)
     o.init_state(sw, sz, sab)
     o.step()

@@ -49,7 +49,7 @@ def test_kinetic_energy_matches_the_oracle(precision, tol, n_r, l_max):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_kinetic_energy_leaves_the_run_unchanged(precision):
+def test_diagnostics_leave_the_run_unchanged(precision):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     wpt, z = O.seeded_state(_ocfg(cfg), amp=1e-2, lmax_pert=10)
     plain = _ctx(cfg)
@@ -61,6 +61,9 @@ def test_kinetic_energy_leaves_the_run_unchanged(precision):
     for _ in range(3):
         probed.step(2)
         kes.append(probed.kinetic_energy())
+        probed.shell_slices(["pressure", "v_r"], [3])    # P takes T's place in the grid buffers
+        probed.shell_spectra(["pressure_dphi", "entropy"], [5, 7])
+        probed.point_probes(["v_phi"], [2], [4], [6])
     for a, b in zip(plain.get_state(), probed.get_state()):
         assert np.array_equal(a, b)
     assert kes[-1] == probed.kinetic_energy()   # deterministic: a fixed-order device reduction

@@ -139,6 +139,7 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
 #define RA_Q_ENTROPY      501
 #define RA_Q_PRESSURE     502   /* formed with the P grid in T's place */
 #define RA_Q_ENTROPY_DR   507
+#define RA_Q_PRESSURE_DR  508
 #define RA_Q_ENTROPY_DTHETA 513
 #define RA_Q_ENTROPY_DPHI 519
 #define RA_Q_PRESSURE_DPHI 520

@@ -630,6 +630,7 @@ class Oracle:
         self._add_derivative(p1b, ZEQ, ZVAR, 2, ctemp[3])
         g = cg.from_spectral(cg.dealias(np.stack([W, P, T, Z, dw, dt_, dz, d2w])))  # :301-309
         Wg, Pg, Tg, Zg, dWg, dTg, dZg, d2Wg = g
+        self.last_pressure_grids = np.stack([Pg, ctemp[1]])   # P and dP/dr, for pressure_fields
         self._add_derivative(p1b, PEQ, WVAR, 0, Wg)
         self._add_derivative(p1b, PEQ, WVAR, 1, dWg)
         self._add_derivative(p1b, PEQ, WVAR, 2, d2Wg)
@@ -905,6 +906,24 @@ class Oracle:
         tw = (self.h.wq / 2.0).astype(np.float64)
         ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
         return float(np.dot(self.radial_integration_weights(), ell0))
+
+    def pressure_fields(self):
+        """dP/dr and dP/dtheta on the physical grid for the state the last step started from
+        (the diagnostics' pressure_dr and pressure_dtheta,
+        Diagnostics_Thermodynamic_Gradients.F90:197-223): Post_Solve's P and dP/dr grids
+        through Transpose_1a2a, l_max zeroed as rlm_spacea does (Sphere_Hybrid_Space.F90:73-75),
+        d/dtheta as for dT/dtheta (sin(theta) d/dtheta in (l, m), then 1/sin(theta)), StP and
+        the c2r.  Returns {"dpdr", "dpdt"} as [theta, r, phi]."""
+        h = self.h
+        b = []
+        for m, a in enumerate(self.transpose_1a2a(self.last_pressure_grids)):   # [m](2, 2, r, l)
+            a = a.copy()
+            a[..., -1] = 0.0
+            b.append(np.stack([a[1], h.d_by_dtheta(a[0], m)]))
+        p3 = self.transpose_2a3a(h.s2p(b))
+        nphi = self.cfg.n_phi
+        return {"dpdr": fft_c2r(p3[0], nphi)[..., :nphi],
+                "dpdt": fft_c2r(p3[1], nphi)[..., :nphi] * h.csctheta[:, None, None]}
 
     def shell_averages(self, names):
         """Shell_Averages (Spherical_IO.F90 Add_Quantity :548-575 with ComputeEll0

@@ -433,9 +433,10 @@ static void bc_values(const Ctx& c, double& top, double& bot) {
     bot = (c.cfg.fix_tvar_bottom ? c.cfg.t_bottom : c.cfg.dtdr_bottom) * s4pi;
 }
 
-// Diagnostics of the pressure: the P grid g[G_P0] into the T field of s2a, so
-// that rlm_spacea and the inverse Legendre transform form P on the physical
-// grid in T's place (the T field there is the T grid copied unchanged).
+// Diagnostics of the pressure: the P and dP/dr grids g[G_P0], g[G_P1] into the
+// T and dT/dr fields of s2a, so that rlm_spacea and the inverse Legendre
+// transform form P and dP/dr on the physical grid in the places of T and dT/dr
+// (those s2a fields are the grids copied unchanged).
 __global__ void pressure_to_s2a_kernel(const double* __restrict__ g, double* __restrict__ s2a, long nlm, int nr,
                                        int L) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
@@ -448,6 +449,9 @@ __global__ void pressure_to_s2a_kernel(const double* __restrict__ g, double* __r
     double* dst = s2a + row_index(m, l, L) * (NS2A * 2L * nr) + S_T * (2L * nr) + 2L * r;
     dst[0] = g[G_P0 * plane + (lm * 2) * nr + r];
     dst[1] = g[G_P0 * plane + (lm * 2 + 1) * nr + r];
+    double* dst1 = dst + (S_T1 - S_T) * (2L * nr);
+    dst1[0] = g[G_P1 * plane + (lm * 2) * nr + r];
+    dst1[1] = g[G_P1 * plane + (lm * 2 + 1) * nr + r];
 }
 
 void launch_pressure_to_s2a(Ctx& c) {

@@ -749,8 +749,8 @@ int ra_physical(ra_ctx* ctx, double* cfl) {
 
 // The stages that form the fields on the physical grid (p2a) from the current
 // state; they only assign their outputs, so the next ra_step is unchanged.
-// With pressure, the P grid takes the place of T before rlm_spacea, so that
-// the T slot of p2a holds P.
+// With pressure, the P and dP/dr grids take the places of T and dT/dr before
+// rlm_spacea, so that the T and dT/dr slots of p2a hold P and dP/dr.
 static void form_grid_fields(Ctx& c, bool pressure) {
     double n, o;
     ab_factors(c, n, o);
@@ -796,6 +796,7 @@ static const QuantitySource kQuantities[] = {
     {513, A_DTDT, 0, 1, 0}, {519, A_T, 1, 0, 0},
     {301, A_OMR, 0, 0, 0},  // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
     {502, A_T, 0, 0, 1},    // pressure, formed in T's place
+    {508, A_DTDR, 0, 0, 1}, // d pressure / dr, in dT/dr's place
     {520, A_T, 1, 0, 1},    // d pressure / d phi
 };
 

@@ -66,7 +66,7 @@ def test_diagnostic_quantity_codes_are_the_references():
     reference = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 300 + 1,
                  "entropy": 500 + 1, "entropy_dr": 500 + 7, "entropy_dtheta": 500 + 13, "entropy_dphi": 500 + 19,
-                 "pressure": 500 + 2, "pressure_dphi": 500 + 20}
+                 "pressure": 500 + 2, "pressure_dr": 500 + 8, "pressure_dphi": 500 + 20}
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()

@@ -33,10 +33,10 @@ extern "C" {
 #define RA_OK               0
 #define RA_ERR_ARG         -1   /* invalid argument or unsupported configuration */
 #define RA_ERR_CUDA        -2   /* a CUDA runtime call failed */
-#define RA_ERR_SINGULAR    -3   /* a zero pivot in a per-l implicit matrix */
+#define RA_ERR_SINGULAR    -3   /* a pivot |u_kk| <= n 2^-53 max|A| in a per-l implicit matrix */
 #define RA_ERR_NOMEM       -4   /* device allocation failed */
 #define RA_ERR_STATE       -5   /* call out of order (e.g. step before put_state) */
-#define RA_ERR_NONFINITE   -6   /* NaN/Inf detected in the state */
+#define RA_ERR_NONFINITE   -6   /* NaN/Inf in an input, or reaching the implicit solve during a step */
 
 #define RA_PREC_FP64   0        /* every product in FP64 */
 #define RA_PREC_MIXED  1        /* split-precision tensor-core products, FP64 state */
@@ -73,8 +73,8 @@ typedef struct ra_config {
 int ra_default_config(ra_config* cfg);
 
 /* Creates a context: builds the grids, the P_l^m tables (on the device),
- * the radial coefficient profiles, the per-l implicit matrices and their
- * inverses (Reset_Linear_Equations).  Replaces Main_Initialization's grid,
+ * the radial coefficient profiles, the per-l implicit matrices and their LU
+ * factors (Reset_Linear_Equations).  A singular matrix returns RA_ERR_SINGULAR.  Replaces Main_Initialization's grid,
  * Legendre and linear-system set-up (src/Physics/Main.F90:71-117). */
 int ra_create(ra_ctx** ctx, const ra_config* cfg);
 int ra_destroy(ra_ctx* ctx);
@@ -84,8 +84,43 @@ int ra_last_error(const ra_ctx* ctx, char* msg, int len);
 int ra_sizes(const ra_ctx* ctx, long* n_lm, int* n_r, int* n_theta, int* n_phi);
 
 /* New time step: Reset_Linear_Equations (Sphere_Linear_Terms.F90:67-76):
- * rebuild LHS = I - alpha dt L with boundary rows and invert it per l. */
+ * rebuild LHS = I - alpha dt L with boundary rows and factor it per l on the
+ * device (LU with partial pivoting, LU_Decompose_full, Linear_Solve.F90:1028-1036).
+ * Replaces any matrices loaded with ra_load_matrices. */
 int ra_set_dt(ra_ctx* ctx, double dt);
+
+/* The driver's own implicit system, for runs whose matrices the library does
+ * not assemble itself (other reference states, custom coefficients):
+ * Load_Linear_Coefficients + Set_Boundary_Conditions output
+ * (Sphere_Linear_Terms.F90:196-1100), replacing the context's matrices of
+ * one system:
+ *   sys 0: the linked W-P-T system, lhs(3 n_r, 3 n_r, l_max + 1)
+ *   sys 1: Z,                       lhs(  n_r,   n_r, l_max + 1)
+ * each lhs(:, :, l) = equation_set(l, eq)%lhs in Fortran (column-major) order,
+ * rows/columns ordered W, P, T blocks of n_r.  coefs (may be NULL) replaces
+ * the explicit Post_Solve coefficients of the system's equations
+ * (equation_set(l, eq)%coefs(var)%data(:, dorder), Linear_Solve.F90:494-539)
+ * as coefs(n_r, 16, l_max + 1), the 16 slots being (eq, var, dorder) =
+ *   (W,W,0) (W,W,1) (W,W,2) (W,P,1) (W,T,0) (P,W,0) (P,W,1) (P,W,2) (P,W,3)
+ *   (P,P,0) (T,T,0) (T,T,1) (T,T,2) (Z,Z,0) (Z,Z,1) (Z,Z,2)
+ * (sys 0 reads the W, P, T slots, sys 1 the Z slots).  Non-finite entries
+ * return RA_ERR_NONFINITE.  The matrices take effect at ra_factor. */
+int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coefs);
+/* The library's own assembly of those matrices for a configuration, on the
+ * host only (no device is used): lhs(n, n, nl) of l = l0 .. l0+nl-1 in the
+ * layout ra_load_matrices takes, and (if coefs is not NULL) coefs(n_r, 16, nl).
+ * Either output may be NULL. */
+int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs, double* coefs);
+/* LU_Decompose_Matrices (Linear_Solve.F90:459-480) of the loaded matrices of
+ * both systems, which belong to time step dt (the AB2 factors use it).
+ * RA_ERR_SINGULAR names the system and l of a negligible pivot. */
+int ra_factor(ra_ctx* ctx, double dt);
+/* bc_values(2 [top, bottom], 2 [re, im], n_lm, 4 [W, P, T, Z]) of
+ * BoundaryConditions.F90:364-531, written into the boundary rows of the
+ * right-hand sides by Apply_Boundary_Mask (Linear_Solve.F90:401-418); (l, m)
+ * in this library's l-major order.  NULL restores the built-in values (zero,
+ * except the fixed T or dT/dr of l = 0). */
+int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values);
 
 /* State exchange in the equation-set RHS layout (Linear_Solve.F90:355-386):
  *   wpt[3 n_r][2][n_lm]  W, P, T Chebyshev coefficients of the linked l-block
@@ -94,6 +129,17 @@ int ra_set_dt(ra_ctx* ctx, double dt);
  * iteration: the reference's iteration counter (1 = Euler first step). */
 int ra_put_state(ra_ctx* ctx, const double* wpt, const double* z, const double* ab, int iteration);
 int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab);
+/* The same for one rank's slice of the modes (the (l, m) pairs a rank of the
+ * reference holds, Load_Balance.F90:357-368): l_of[i], m_of[i] name mode i of
+ * the slice, whose arrays are the rank's own equation-set layout
+ *   wpt[3 n_r][2][nmodes], z[n_r][2][nmodes], ab[n_r][2][nmodes][4]
+ * (Fortran order; ab may be NULL = zero).  A driver that gathers its ranks'
+ * slices puts each one (in any order) before stepping; modes not put keep
+ * their previous values.  Non-finite input returns RA_ERR_NONFINITE. */
+int ra_put_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of, const double* wpt, const double* z,
+                       const double* ab, int iteration);
+int ra_get_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of, double* wpt, double* z,
+                       double* ab);
 
 /* One full step, the five stage calls of Main_Loop_Sphere
  * (Sphere_Driver.F90:305-328) at the current dt, nsteps times.  cfl (may be
@@ -247,13 +293,35 @@ int ra_mixed_gemm(ra_ctx* ctx, const double* a, const double* b, double* c, int 
  * enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) and the
  * call returns after it finished.  Scratch comes from one fixed 16 MiB
  * device array inside the library (about 5 (m + n) k bytes are needed;
- * larger products return RA_ERR_ARG with the needed size in msg).  The
- * first call on each device looks up that array's address: make it before
- * any stream capture.  Calls that overlap in time on one device race on the
- * shared scratch.  msg (may be NULL) receives an error message of at most
+ * larger products return RA_ERR_ARG with the needed size in msg).  Every
+ * call looks up that array's address on the current device.  The call is
+ * synchronous (it reads a status word back and waits for `stream`), so it
+ * cannot be made on a stream that is being captured.  Calls that overlap in
+ * time on one device race on the shared scratch.  msg (may be NULL) receives an error message of at most
  * msg_len bytes. */
 int ra_mixed_gemm_noalloc(const double* a, const double* b, double* c, int m, int n, int k, void* stream,
                           char* msg, int msg_len);
+
+/* ---- batched per-l solves on their own (no transform context) ----
+ * LU_Decompose_full / LU_Solve_full (Linear_Solve.F90:1028-1036, 1088-1110)
+ * for count matrices of order n (even, <= 1152) on one device. */
+typedef struct ra_lu ra_lu;
+#define RA_SOLVE_FP64    0   /* block substitution with the FP64 LU factors */
+#define RA_SOLVE_REFINE  1   /* FP32 substitution + FP64 residuals, refined to FP64 accuracy */
+int ra_lu_create(ra_lu** lu, int n, int count, int device);
+int ra_lu_destroy(ra_lu* lu);
+int ra_lu_last_error(const ra_lu* lu, char* msg, int len);
+/* a(n, n, count): the matrices in Fortran (column-major) order.  Factors them
+ * on the device (partial pivoting); ms (may be NULL) receives the device time
+ * of the factorisation.  RA_ERR_SINGULAR names the first singular matrix,
+ * RA_ERR_NONFINITE refuses NaN/Inf entries. */
+int ra_lu_factor(ra_lu* lu, const double* a, double* ms);
+/* x = A_l^-1 b for b(n, ncols, count) (Fortran order) in one launch.  iters
+ * (may be NULL) receives, per matrix and per tile of columns
+ * (ra_lu_tiles(lu, ncols, mode) entries, matrix-major), the refinement
+ * iterations (1 in the FP64 form); ms the device time of the solve. */
+int ra_lu_solve(ra_lu* lu, const double* b, double* x, int ncols, int mode, int* iters, double* ms);
+int ra_lu_tiles(const ra_lu* lu, int ncols, int mode);
 
 /* Radial grid of the context: radius(n_r), r(1) = r_max (Chebyshev_Polynomials.F90:168-200). */
 int ra_radius(const ra_ctx* ctx, double* radius);

@@ -438,6 +438,7 @@ class Oracle:
         self.iteration = 1
         self._build_linear()
         self.last_cfl = 0.0
+        self.bc_values = None   # None: the built-in boundary values (only l = 0 T carries one)
 
     # ----- linear system (Sphere_Linear_Terms.F90:79-537, Linear_Solve.F90:494-539) -----
     def _build_linear(self):
@@ -850,8 +851,16 @@ class Oracle:
             self.rhs_wpt[:, :, b + nr - 1] = 0.0
         self.rhs_z[:, :, 0] = 0.0
         self.rhs_z[:, :, nr - 1] = 0.0
-        self.rhs_wpt[0, 0, 2 * nr] = self.bc_t[0]          # l=0, m=0, real, top
-        self.rhs_wpt[0, 0, 3 * nr - 1] = self.bc_t[1]
+        if self.bc_values is None:
+            self.rhs_wpt[0, 0, 2 * nr] = self.bc_t[0]          # l=0, m=0, real, top
+            self.rhs_wpt[0, 0, 3 * nr - 1] = self.bc_t[1]
+        else:
+            # bc_values(top/bottom, re/im, lm, eq) (BoundaryConditions.F90:364-531), here [eq][lm][ri][tb]
+            bv = self.bc_values
+            for eq, (arr, b) in enumerate(((self.rhs_wpt, 0), (self.rhs_wpt, nr), (self.rhs_wpt, 2 * nr),
+                                           (self.rhs_z, 0))):
+                arr[:, :, b] = bv[eq, :, :, 0]
+                arr[:, :, b + nr - 1] = bv[eq, :, :, 1]
         # Implicit_Solve -> DGETRS (Linear_Solve.F90:423-457,1088-1110)
         for l in (range(self.cfg.l_max + 1) if ls is None else ls):
             s, e = self.l_start[l], self.l_start[l] + l + 1

@@ -150,6 +150,19 @@ def load_library(path: str | None = None):
         "ra_mixed_gemm_noalloc": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p,
                                    ctypes.c_int], ctypes.c_int),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+        "ra_put_state_modes": ([_VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, ctypes.c_int], ctypes.c_int),
+        "ra_get_state_modes": ([_VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP], ctypes.c_int),
+        "ra_build_matrices": ([ctypes.POINTER(_Config), ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, _VP],
+                              ctypes.c_int),
+        "ra_load_matrices": ([_VP, ctypes.c_int, _VP, _VP], ctypes.c_int),
+        "ra_factor": ([_VP, ctypes.c_double], ctypes.c_int),
+        "ra_set_bc_mask": ([_VP, _VP], ctypes.c_int),
+        "ra_lu_create": ([ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "ra_lu_destroy": ([_VP], ctypes.c_int),
+        "ra_lu_last_error": ([_VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "ra_lu_factor": ([_VP, _VP, _DP], ctypes.c_int),
+        "ra_lu_solve": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _DP], ctypes.c_int),
+        "ra_lu_tiles": ([_VP, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -230,6 +243,41 @@ class Rayleigh:
         ab = np.empty((4, self.n_lm, 2, self.n_r))
         self._check(self.lib.ra_get_state(self.h, _ptr(wpt), _ptr(z), _ptr(ab)))
         return wpt, z, ab
+
+    # ---- one rank's slice of the modes (the reference's per-rank equation-set layout) ----
+    def put_state_modes(self, l_of, m_of, wpt, z, ab=None, iteration=1):
+        """Put the modes (l_of[i], m_of[i]): wpt[mode][ri][3 nr], z[mode][ri][nr], ab[4][mode][ri][nr]."""
+        lo = np.ascontiguousarray(l_of, dtype=np.int32)
+        mo = np.ascontiguousarray(m_of, dtype=np.int32)
+        w, zz = _f64(wpt), _f64(z)
+        a = None if ab is None else _f64(ab)
+        self._check(self.lib.ra_put_state_modes(self.h, len(lo), lo.ctypes.data, mo.ctypes.data, _ptr(w), _ptr(zz),
+                                                _ptr(a), int(iteration)))
+
+    def get_state_modes(self, l_of, m_of):
+        lo = np.ascontiguousarray(l_of, dtype=np.int32)
+        mo = np.ascontiguousarray(m_of, dtype=np.int32)
+        k = len(lo)
+        w = np.empty((k, 2, 3 * self.n_r))
+        z = np.empty((k, 2, self.n_r))
+        ab = np.empty((4, k, 2, self.n_r))
+        self._check(self.lib.ra_get_state_modes(self.h, k, lo.ctypes.data, mo.ctypes.data, _ptr(w), _ptr(z), _ptr(ab)))
+        return w, z, ab
+
+    # ---- the driver's own implicit system ----
+    def load_matrices(self, sys, lhs=None, coefs=None):
+        """lhs[l][col][row] (each matrix column-major, as the reference stores it), coefs[l][slot][r]."""
+        self._lhs_keep = None if lhs is None else _f64(lhs)
+        self._coef_keep = None if coefs is None else _f64(coefs)
+        self._check(self.lib.ra_load_matrices(self.h, int(sys), _ptr(self._lhs_keep), _ptr(self._coef_keep)))
+
+    def factor(self, dt):
+        self._check(self.lib.ra_factor(self.h, float(dt)))
+
+    def set_bc_mask(self, bc_values):
+        """bc_values[eq W/P/T/Z][lm][re/im][top/bottom] (Fortran bc_values(2, 2, n_lm, 4)), or None."""
+        self._bcv = None if bc_values is None else _f64(bc_values)
+        self._check(self.lib.ra_set_bc_mask(self.h, _ptr(self._bcv)))
 
     def step(self, nsteps=1):
         cfl = ctypes.c_double()
@@ -440,4 +488,90 @@ class Rayleigh:
         return out
 
 
-__all__ = ["Config", "Rayleigh", "RayleighError", "load_library", "LIB_PATH", "PREC_FP64", "PREC_MIXED"]
+def build_matrices(cfg: Config, sys, l0, nl, coefs=False):
+    """The library's own assembly of the per-l implicit matrices (host only): lhs[l][col][row]
+    (column-major per l) of system sys (0 = W-P-T, 1 = Z) for l = l0 .. l0+nl-1, and with
+    coefs=True also coefs[l][slot][r]."""
+    lib = load_library()
+    c = cfg.to_c()
+    n = cfg.n_r * (1 if sys else 3)
+    lhs = np.empty((nl, n, n))
+    cf = np.empty((nl, 16, cfg.n_r)) if coefs else None
+    rc = lib.ra_build_matrices(ctypes.byref(c), int(sys), int(l0), int(nl), _ptr(lhs), _ptr(cf))
+    if rc != RA_OK:
+        raise RayleighError(rc, "ra_build_matrices refused the configuration or range")
+    return (lhs, cf) if coefs else lhs
+
+
+SOLVE_FP64 = 0
+SOLVE_REFINE = 1
+
+
+class BatchedLU:
+    """Batched per-l LU factorisation and solves on one device (LU_Decompose_full /
+    LU_Solve_full, Linear_Solve.F90:1028-1036, 1088-1110), independent of a context."""
+
+    def __init__(self, n, count, device=0):
+        self.lib = load_library()
+        h = _VP()
+        rc = self.lib.ra_lu_create(ctypes.byref(h), int(n), int(count), int(device))
+        self.h = h
+        self.n, self.count = n, count
+        if rc != RA_OK:
+            msg = self._err()
+            self.lib.ra_lu_destroy(h)
+            self.h = None
+            raise RayleighError(rc, msg)
+
+    def _err(self):
+        buf = ctypes.create_string_buffer(1024)
+        if self.h:
+            self.lib.ra_lu_last_error(self.h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc):
+        if rc != RA_OK:
+            raise RayleighError(rc, self._err())
+
+    def factor(self, mats_colmajor):
+        """mats[l][col][row] (column-major per matrix); returns the device time in ms."""
+        a = _f64(mats_colmajor)
+        if a.size != self.count * self.n * self.n:
+            raise ValueError("matrices have the wrong size")
+        ms = ctypes.c_double()
+        self._check(self.lib.ra_lu_factor(self.h, _ptr(a), ctypes.byref(ms)))
+        return ms.value
+
+    def solve(self, b, mode=SOLVE_FP64):
+        """b[l][col][row]; returns (x, iterations[l][column tile], device ms)."""
+        b = _f64(b)
+        ncols = b.size // (self.count * self.n)
+        x = np.empty_like(b)
+        nt = self.lib.ra_lu_tiles(self.h, ncols, int(mode))
+        if nt < 0:
+            self._check(nt)
+        it = np.empty(nt, dtype=np.int32)
+        ms = ctypes.c_double()
+        self._check(self.lib.ra_lu_solve(self.h, _ptr(b), _ptr(x), ncols, int(mode), it.ctypes.data, ctypes.byref(ms)))
+        return x, it.reshape(self.count, -1), ms.value
+
+    def close(self):
+        if self.h:
+            self.lib.ra_lu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+__all__ = ["Config", "Rayleigh", "RayleighError", "load_library", "LIB_PATH", "PREC_FP64", "PREC_MIXED",
+           "BatchedLU", "build_matrices", "SOLVE_FP64", "SOLVE_REFINE"]

@@ -200,7 +200,7 @@ static void setup_solve(Ctx& c) {
     for (int sys = 0; sys < 2; ++sys) {
         const int n = sys ? nr : 3 * nr, nseg = sys ? 1 : 3;
         const int nta = oz_tiles_of(n, OZ_HA), nks = nseg * kseg;
-        const double* Ainv = sys ? c.d_Az : c.d_Awpt;
+        const double* Ainv = sys ? c.d_Ainv_z : c.d_Ainv_wpt;   // transposed: (i, k) at [k][i]
         const double* rhs = sys ? c.d_rhs_z : c.d_rhs_wpt;
         double* sol = sys ? c.d_sol_z : c.d_sol_wpt;
         max_a = std::max(max_a, nta * OZ_HA);
@@ -220,8 +220,8 @@ static void setup_solve(Ctx& c) {
             for (int sg = 0; sg < nseg; ++sg) {
                 // rows of A_l^{-1} restricted to the columns of block sg (K contiguous);
                 // right-hand-side columns (lm, re/im) restricted to the rows of block sg
-                ajobs.push_back({Ainv + (size_t)l * n * n + sg * nr, (long)n, 1L, n, nr, OZ_HA, nta, kseg, adig,
-                                 ea + (long)sg * n, nks, sg * kseg});
+                ajobs.push_back({Ainv + (size_t)l * n * n + (size_t)sg * nr * n, 1L, (long)n, n, nr, OZ_HA, nta, kseg,
+                                 adig, ea + (long)sg * n, nks, sg * kseg});
                 bjobs.push_back({rhs + 2 * lstart * n + sg * nr, (long)n, 1L, ncol, nr, OZ_HB, ntb, kseg, bdig,
                                  eb + (long)sg * ncol, nks, sg * kseg});
             }

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_gemm_kernel(const OzProbl
 
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (threadIdx.x == 0 && sm.abort) atomicExch(status, 1);
+    if (threadIdx.x == 0 && sm.abort) atomicOr(status, RA_STATUS_TIMEOUT);
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(OZ_TMEM_COLS));
@@ -547,23 +547,18 @@ void ozaki_split(Ctx& c, const OzSplitJob* d_jobs, int njobs, int max_rows, int 
     }
 }
 
+// SM count of the current device (asked on every call: one process may drive several devices)
 static int oz_sm_count() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
-        RA_CUDA(cudaGetDevice(&dev));
-        RA_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-    }
+    int dev = 0, n = 0;
+    RA_CUDA(cudaGetDevice(&dev));
+    RA_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
     return n;
 }
 
 void ozaki_gemm(Ctx& c, const OzProblem* d_probs, const int* d_tiles, int ntiles, int* d_status) {
     if (ntiles == 0) return;
-    static bool attr = false;
-    if (!attr) {
-        RA_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem)));
-        attr = true;
-    }
+    // the limit is per device: set it on every launch
+    RA_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(OzSmem)));
     const int grid = std::min(ntiles, oz_sm_count());
     ozaki_gemm_kernel<<<grid, OZ_THREADS, sizeof(OzSmem), c.stream>>>(
         d_probs, reinterpret_cast<const int4*>(d_tiles), ntiles, d_status);
@@ -597,8 +592,9 @@ std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
 // Allocation-free form of the split-precision product (ra_mixed_gemm_noalloc).
 //
 // All scratch lives in one file-scope device array of fixed size; its device
-// address is looked up once per device (cudaGetSymbolAddress, with that device
-// current) on the first call made on that device.  Scratch layout, every piece
+// address is looked up on every call (cudaGetSymbolAddress with the caller's
+// device current: one lookup per call, nothing cached between calls, so no
+// host-side state is shared by threads).  Scratch layout, every piece
 // 256-byte aligned:
 //   [0]        int        status word    (set to zero by oz_static_prepare_kernel)
 //   [256]      OzProblem                 (written by oz_static_prepare_kernel)
@@ -613,9 +609,6 @@ std::vector<int> ozaki_tiles(const std::vector<OzProblem>& probs) {
 // ---------------------------------------------------------------------------
 constexpr size_t OZ_STATIC_BYTES = (size_t)16 << 20;   // 16 MiB
 static __device__ __align__(256) unsigned char oz_static_scratch[OZ_STATIC_BYTES];
-
-constexpr int OZ_MAX_DEVICES = 64;
-static unsigned char* oz_static_ptr[OZ_MAX_DEVICES] = {};
 
 static size_t oz_align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -671,18 +664,16 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= OZ_MAX_DEVICES) {
+    if (e != cudaSuccess || dev < 0) {
         oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: no usable current device");
         return RA_ERR_CUDA;
     }
-    if (!oz_static_ptr[dev]) {   // first call on this device: resolve the scratch address
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, oz_static_scratch);
-        if (e != cudaSuccess || !p) {
-            oz_set_msg(msg, msg_len, cudaGetErrorString(e));
-            return RA_ERR_CUDA;
-        }
-        oz_static_ptr[dev] = static_cast<unsigned char*>(p);
+    // the array's device address on the current device (the host-side name is not one)
+    void* scratch = nullptr;
+    e = cudaGetSymbolAddress(&scratch, oz_static_scratch);
+    if (e != cudaSuccess || !scratch) {
+        oz_set_msg(msg, msg_len, cudaGetErrorString(e));
+        return RA_ERR_CUDA;
     }
     int nsm = 0;
     e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -690,7 +681,7 @@ extern "C" int ra_mixed_gemm_noalloc(const double* d_a, const double* d_b, doubl
         oz_set_msg(msg, msg_len, "ra_mixed_gemm_noalloc: cannot read the SM count");
         return RA_ERR_CUDA;
     }
-    unsigned char* base = oz_static_ptr[dev];
+    unsigned char* base = static_cast<unsigned char*>(scratch);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int* d_status = reinterpret_cast<int*>(base);
     OzProblem* d_prob = reinterpret_cast<OzProblem*>(base + off_prob);

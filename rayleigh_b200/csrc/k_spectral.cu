@@ -9,11 +9,8 @@
 //                          (Sphere_Spectral_Space.F90:204-410, Linear_Solve.F90:758-796).
 //   rlm_a_kernel           rlm_spacea algebra (Sphere_Hybrid_Space.F90:64-355).
 //   rlm_b_kernel           rlm_spaceb algebra + Transpose_2b1b (Sphere_Hybrid_Space.F90:127-222).
-//   solve_kernel           AdvanceTime: Add_To_All_RHS, Apply_Boundary_Mask,
-//                          Implicit_Solve (Sphere_Spectral_Space.F90:415-435,
-//                          Linear_Solve.F90:401-457) as x = A^{-1} b per l.
-//   gj_invert_kernel       the per-l inverse used above (LU_Decompose_Matrices,
-//                          Linear_Solve.F90:459-480): Gauss-Jordan, partial pivoting.
+// The per-l implicit solves that follow (Implicit_Solve, LU_Decompose_Matrices)
+// are in k_solve.cu.
 #include <cmath>
 
 #include "ra_internal.h"
@@ -118,11 +115,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
 void launch_cheb_synthesis(Ctx& c) {
     const long ncols = 2 * c.d.nlm;
     const size_t smem = sizeof(ChebSmem);
-    static bool attr = false;
-    if (!attr) {
-        RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    // the limit is per device: set it on every launch (a host-side call, also legal during capture)
+    RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((ncols + ChebShape::BN - 1) / ChebShape::BN), 4);
     cheb_synthesis_kernel<<<grid, GEMM_THREADS, smem, c.stream>>>(c.d_Dpar, c.d_sol_wpt, c.d_sol_z, c.d_g, c.d.nr,
                                                                    c.d.kc, ncols);
@@ -355,7 +349,7 @@ void launch_rlm_a(Ctx& c) {
 // ---------------------------------------------------------------------------
 __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict__ ab, double* __restrict__ rhs_wpt,
                              double* __restrict__ rhs_z, long nlm, int nr, int L, double new_ab, double bc_top,
-                             double bc_bot) {
+                             double bc_bot, const double* __restrict__ bcv, int* __restrict__ status) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
     if (idx >= nlm * nr) return;
     const int r = (int)(idx % nr);
@@ -402,6 +396,7 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
         if (l == lmax) {   // :205-208
             W = P = Tt = Z = 0.0;
         }
+        if (!(isfinite(W) && isfinite(P) && isfinite(Tt) && isfinite(Z))) atomicOr(status, RA_STATUS_NONFINITE);
         const long col = lm * 2 + ri;
         const long o = col * nr + r;
         ab[0 * plane + o] = W;
@@ -412,11 +407,19 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
         // (Sphere_Spectral_Space.F90:427-428, Linear_Solve.F90:401-418, 733-754)
         double* rw = rhs_wpt + col * 3L * nr + r;
         if (edge) {
-            const double tb = (col == 0) ? (r == 0 ? bc_top : bc_bot) : 0.0;   // only l = 0 T carries a value
-            rw[0] = 0.0;
-            rw[nr] = 0.0;
-            rw[2 * nr] = tb;
-            rhs_z[o] = 0.0;
+            if (bcv) {   // the caller's bc_values(top/bottom, re/im, lm, equation)
+                const double* bv = bcv + (lm * 2 + ri) * 2 + (r == 0 ? 0 : 1);
+                rw[0] = bv[0];
+                rw[nr] = bv[4 * nlm];
+                rw[2 * nr] = bv[8 * nlm];
+                rhs_z[o] = bv[12 * nlm];
+            } else {
+                const double tb = (col == 0) ? (r == 0 ? bc_top : bc_bot) : 0.0;   // only l = 0 T carries a value
+                rw[0] = 0.0;
+                rw[nr] = 0.0;
+                rw[2 * nr] = tb;
+                rhs_z[o] = 0.0;
+            }
         } else {
             rw[0] += new_ab * W;
             rw[nr] += new_ab * P;
@@ -467,207 +470,10 @@ void launch_rlm_b(Ctx& c, double new_ab) {
     double top, bot;
     bc_values(c, top, bot);
     rlm_b_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2b, c.d_ab, c.d_rhs_wpt, c.d_rhs_z,
-                                                                        c.d.nlm, c.d.nr, c.d.L, new_ab, top, bot);
+                                                                        c.d.nlm, c.d.nr, c.d.L, new_ab, top, bot,
+                                                                        c.d_bcval, c.d_status);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
-}
-
-// ---------------------------------------------------------------------------
-// AdvanceTime: b = rhs + new_ab * ab with boundary rows, x = A_l^{-1} b
-// tiles: (sys, l, mt, nt); sys 0 = W-P-T block (n = 3 nr), 1 = Z (n = nr)
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(GEMM_THREADS) solve_kernel(const int4* __restrict__ tiles,
-                                                             const double* __restrict__ Awpt,
-                                                             const double* __restrict__ Az,
-                                                             const double* __restrict__ rhs_wpt,
-                                                             const double* __restrict__ rhs_z,
-                                                             double* __restrict__ sol_wpt,
-                                                             double* __restrict__ sol_z, int nr) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw);
-    const int4 tl = tiles[blockIdx.x];
-    const int sys = tl.x, l = tl.y, i0 = tl.z * BM, n0 = tl.w * BN;
-    const int n = sys ? nr : 3 * nr;
-    const int ncol = 2 * (l + 1);
-    const long lstart = (long)l * (l + 1) / 2;
-    const double* A = (sys ? Az : Awpt) + (long)l * n * n;
-    const double* rhs = (sys ? rhs_z : rhs_wpt) + lstart * 2 * n;
-    double* sol = (sys ? sol_z : sol_wpt) + lstart * 2 * n;
-    Acc acc;
-    acc.zero();
-    auto fa = [&](int k, int x) -> double {
-        const int i = i0 + x;
-        return (k < n && i < n) ? __ldg(A + (long)i * n + k) : 0.0;
-    };
-    auto fb = [&](int k, int y) -> double {
-        const int cc = n0 + y;
-        return (k < n && cc < ncol) ? __ldg(rhs + (long)cc * n + k) : 0.0;
-    };
-    gemm_tile<false, false>(acc, fa, fb, n, sm);
-    acc_foreach(acc, [&](int x, int y, double v) {
-        const int i = i0 + x, cc = n0 + y;
-        if (i < n && cc < ncol) sol[(long)cc * n + i] = v;
-    });
-}
-
-static std::vector<int> solve_tiles(int L, int nr) {
-    std::vector<int> t;
-    for (int sys = 0; sys < 2; ++sys) {
-        const int n = sys ? nr : 3 * nr;
-        for (int l = L - 1; l >= 0; --l) {
-            const int ncol = 2 * (l + 1);
-            for (int mt = 0; mt * BM < n; ++mt)
-                for (int nt = 0; nt * BN < ncol; ++nt) {
-                    t.push_back(sys);
-                    t.push_back(l);
-                    t.push_back(mt);
-                    t.push_back(nt);
-                }
-        }
-    }
-    return t;
-}
-
-// The solve's tile list, built once at set-up (no allocation may run while
-// the step is captured into a graph).
-void solve_prepare(Ctx& c) {
-    if (!c.d_solve_tiles) {
-        std::vector<int> t = solve_tiles(c.d.L, c.d.nr);
-        c.n_solve_tiles = (int)(t.size() / 4);
-        RA_CUDA(cudaMalloc(&c.d_solve_tiles, t.size() * sizeof(int)));
-        RA_CUDA(cudaMemcpy(c.d_solve_tiles, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice));
-    }
-}
-
-void launch_solve(Ctx& c) {
-    if (!c.d_solve_tiles) throw ArgError("solve tiles not prepared (solve_prepare runs at set-up)");
-    solve_kernel<<<c.n_solve_tiles, GEMM_THREADS, sizeof(GemmSmem), c.stream>>>(
-        reinterpret_cast<const int4*>(c.d_solve_tiles), c.d_Awpt, c.d_Az, c.d_rhs_wpt, c.d_rhs_z, c.d_sol_wpt,
-        c.d_sol_z, c.d.nr);
-    RA_CUDA(cudaGetLastError());
-    ++c.launches;
-}
-
-// ---------------------------------------------------------------------------
-// In-place Gauss-Jordan inversion with partial (row) pivoting, one CTA per matrix.
-// status[mat] = 0 ok, 1 zero pivot.
-// ---------------------------------------------------------------------------
-constexpr int GJ_THREADS = 512;
-
-__global__ void __launch_bounds__(GJ_THREADS) gj_invert_kernel(double* __restrict__ mats, int n,
-                                                               const int* __restrict__ skip,
-                                                               int* __restrict__ status, int* __restrict__ piv_all) {
-    const int mat = blockIdx.x;
-    double* A = mats + (long)mat * n * n;
-    int* piv = piv_all + (long)mat * n;
-    extern __shared__ double gsm[];
-    double* rowk = gsm;           // n
-    double* colk = gsm + n;       // n
-    __shared__ double red_v[GJ_THREADS / 32];
-    __shared__ int red_i[GJ_THREADS / 32];
-    __shared__ int s_p;
-    __shared__ int s_bad;
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    if (skip && skip[mat]) {      // identity (an equation that is not solved for this l)
-        for (long e = t; e < (long)n * n; e += blockDim.x) A[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
-        if (t == 0) status[mat] = 0;
-        return;
-    }
-    if (t == 0) s_bad = 0;
-    for (int k = 0; k < n; ++k) {
-        // pivot search: max |A[i][k]|, i >= k (first index on ties, as IDAMAX)
-        double bv = -1.0;
-        int bi = n;
-        for (int i = k + t; i < n; i += blockDim.x) {
-            const double v = fabs(A[(long)i * n + k]);
-            if (v > bv) { bv = v; bi = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
-        if (lane == 0) { red_v[w] = bv; red_i[w] = bi; }
-        __syncthreads();
-        if (t == 0) {
-            double v = red_v[0];
-            int ii = red_i[0];
-            for (int q = 1; q < (int)(blockDim.x / 32); ++q)
-                if (red_v[q] > v || (red_v[q] == v && red_i[q] < ii)) { v = red_v[q]; ii = red_i[q]; }
-            s_p = ii;
-            piv[k] = ii;
-            if (!(v > 0.0)) s_bad = 1;
-        }
-        __syncthreads();
-        const int p = s_p;
-        if (s_bad) break;
-        if (p != k) {
-            for (int j = t; j < n; j += blockDim.x) {
-                const double a = A[(long)k * n + j], b = A[(long)p * n + j];
-                A[(long)k * n + j] = b;
-                A[(long)p * n + j] = a;
-            }
-            __syncthreads();
-        }
-        const double inv = 1.0 / A[(long)k * n + k];
-        __syncthreads();
-        for (int j = t; j < n; j += blockDim.x) {
-            const double v = (j == k) ? inv : A[(long)k * n + j] * inv;
-            rowk[j] = v;
-            A[(long)k * n + j] = v;
-            colk[j] = A[(long)j * n + k];
-        }
-        __syncthreads();
-        // eliminate column k from every other row
-        for (long e = t; e < (long)n * n; e += blockDim.x) {
-            const int i = (int)(e / n), j = (int)(e % n);
-            if (i == k) continue;
-            const double f = colk[i];
-            if (j == k) A[e] = -f * rowk[k];
-            else A[e] = A[e] - f * rowk[j];
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-    if (s_bad) {
-        if (t == 0) status[mat] = 1;
-        return;
-    }
-    // undo the row interchanges as column interchanges, in reverse order
-    for (int k = n - 1; k >= 0; --k) {
-        const int p = piv[k];
-        if (p != k) {
-            for (int i = t; i < n; i += blockDim.x) {
-                const double a = A[(long)i * n + k], b = A[(long)i * n + p];
-                A[(long)i * n + k] = b;
-                A[(long)i * n + p] = a;
-            }
-        }
-        __syncthreads();
-    }
-    if (t == 0) status[mat] = 0;
-}
-
-int invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip_h) {
-    int *d_status = nullptr, *d_piv = nullptr, *d_skip = nullptr;
-    RA_CUDA(cudaMalloc(&d_status, count * sizeof(int)));
-    RA_CUDA(cudaMalloc(&d_piv, (long)count * n * sizeof(int)));
-    if (skip_h) {
-        RA_CUDA(cudaMalloc(&d_skip, count * sizeof(int)));
-        RA_CUDA(cudaMemcpyAsync(d_skip, skip_h, count * sizeof(int), cudaMemcpyHostToDevice, c.stream));
-    }
-    gj_invert_kernel<<<count, GJ_THREADS, 2 * n * sizeof(double), c.stream>>>(d_mats, n, d_skip, d_status, d_piv);
-    RA_CUDA(cudaGetLastError());
-    ++c.launches;
-    std::vector<int> st(count);
-    RA_CUDA(cudaMemcpyAsync(st.data(), d_status, count * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    RA_CUDA(cudaStreamSynchronize(c.stream));
-    cudaFree(d_status);
-    cudaFree(d_piv);
-    if (d_skip) cudaFree(d_skip);
-    for (int i = 0; i < count; ++i)
-        if (st[i]) return i + 1;
-    return 0;
 }
 
 }  // namespace ra

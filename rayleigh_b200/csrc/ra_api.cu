@@ -306,13 +306,7 @@ static void linear_setup(Ctx& c) {
     RA_CUDA(cudaMemcpyAsync(c.d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_Awpt, Aall.data(), Aall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_Az, Zall.data(), Zall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    int bad = invert_matrices(c, c.d_Awpt, n3, L, nullptr);
-    if (bad) throw ArgError("singular W-P-T matrix at l = " + std::to_string(bad - 1));
-    std::vector<int> skip(L, 0);
-    skip[0] = 1;   // Z is not solved for at l = 0 (Sphere_Linear_Terms.F90:116-150)
-    bad = invert_matrices(c, c.d_Az, nr, L, skip.data());
-    if (bad) throw ArgError("singular Z matrix at l = " + std::to_string(bad - 1));
-    RA_CUDA(cudaStreamSynchronize(c.stream));
+    factor_matrices(c);
 }
 
 template <class T>
@@ -392,6 +386,19 @@ static void setup(Ctx& c) {
     dalloc(c.d_twid, twid.size());
     dalloc(c.d_Awpt, (size_t)d.L * 9 * nr * nr);
     dalloc(c.d_Az, (size_t)d.L * nr * nr);
+    dalloc(c.d_perm_wpt, (size_t)d.L * 3 * nr);
+    dalloc(c.d_perm_z, (size_t)d.L * nr);
+    dalloc(c.d_skip_z, (size_t)d.L);
+    {
+        std::vector<int> skip(d.L, 0);
+        skip[0] = 1;   // Z is not solved for at l = 0 (Sphere_Linear_Terms.F90:116-150)
+        RA_CUDA(cudaMemcpyAsync(c.d_skip_z, skip.data(), skip.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    if (c.cfg.precision == RA_PREC_MIXED) {
+        dalloc(c.d_Ainv_wpt, (size_t)d.L * 9 * nr * nr);
+        dalloc(c.d_Ainv_z, (size_t)d.L * nr * nr);
+    }
     dalloc(c.d_sol_wpt, (size_t)nlm * 2 * 3 * nr);
     dalloc(c.d_sol_z, (size_t)nlm * 2 * nr);
     dalloc(c.d_rhs_wpt, (size_t)nlm * 2 * 3 * nr);
@@ -404,6 +411,8 @@ static void setup(Ctx& c) {
     dalloc(c.d_p2b, (size_t)d.L * d.nth * NP2B * 2 * nr);
     dalloc(c.d_s2b, (size_t)nlm * NP2B * 2 * nr);
     dalloc(c.d_cfl, 1);
+    dalloc(c.d_status, 1);
+    RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
     dalloc(c.d_kew, kew.size());
     {
         const std::vector<double> kaz((size_t)d.nth, 1.0 / d.nphi);
@@ -444,11 +453,10 @@ static void setup(Ctx& c) {
     RA_CUDA(cudaStreamSynchronize(c.stream));
     cudaFree(d_x);
     cudaFree(d_w);
-    // kernels that need more than 48 KB of dynamic shared memory
+    solve_prepare(c);
     linear_setup(c);
     physics_prepare(c);
     lt_forward_prepare(c);
-    solve_prepare(c);
     if (c.cfg.precision == RA_PREC_MIXED) mixed_setup(c);
 }
 
@@ -456,12 +464,16 @@ static void release(Ctx& c) {
     mixed_release(c);
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
+    lu_workspace_free(c.lu_work);
     double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp, c.d_Awpt, c.d_Az,
+                      c.d_Ainv_wpt, c.d_Ainv_z,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
-                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz};
+                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz, c.d_bcval};
     for (double* b : bufs)
         if (b) cudaFree(b);
-    int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status};
+    int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status,
+                    c.d_perm_wpt, c.d_perm_z, c.d_skip_z, c.d_inv_sol_tiles, c.d_inv_sol_tiles_z,
+                    c.d_solve_tiles_z};
     for (int* b : ibufs)
         if (b) cudaFree(b);
     if (c.d_cfl) cudaFree(c.d_cfl);
@@ -517,14 +529,31 @@ static void enqueue_step(Ctx& c, double new_ab, double old_ab) {
     for (int k = 0; k < kNK; ++k) run_stage(c, k, new_ab, old_ab);
 }
 
-// the device error word of the bounded tensor-core waits (split-precision products)
+// the device error word: bounded tensor-core waits of the split-precision
+// products, and non-finite values reaching the implicit solve's right-hand side
 static void check_status(Ctx& c) {
     if (!c.d_status) return;
     int st = 0;
     RA_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     RA_CUDA(cudaStreamSynchronize(c.stream));
-    if (st) throw CudaError(cudaErrorLaunchTimeout, "split-precision product (pipeline barrier wait timed out)",
-                            __FILE__, __LINE__);
+    if (st & RA_STATUS_TIMEOUT)
+        throw CudaError(cudaErrorLaunchTimeout, "split-precision product (pipeline barrier wait timed out)", __FILE__,
+                        __LINE__);
+    if (st & RA_STATUS_NONFINITE)
+        throw NonFiniteError("a NaN or Inf reached the right-hand side of the implicit solve (iteration " +
+                             std::to_string(c.iteration - 1) + " or earlier); put a finite state to continue");
+}
+
+__global__ void nonfinite_scan_kernel(const double* __restrict__ x, long n, int* __restrict__ flag) {
+    bool bad = false;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        bad |= !isfinite(x[i]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, RA_STATUS_NONFINITE);
+}
+
+static void scan_nonfinite(Ctx& c, const double* d_x, long n) {
+    nonfinite_scan_kernel<<<1184, 256, 0, c.stream>>>(d_x, n, c.d_status);
+    RA_CUDA(cudaGetLastError());
 }
 
 static void run_steps(Ctx& c, int nsteps, double* cfl) {
@@ -559,8 +588,8 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
         c.old_dt = c.dt;
         ++c.iteration;
     }
+    check_status(c);
     if (cfl) {
-        check_status(c);
         unsigned long long bits = 0;
         RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
@@ -568,6 +597,121 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
         std::memcpy(&v, &bits, sizeof(v));
         *cfl = v;
     }
+}
+
+// Rank-local state exchange: the modes of one slice (a rank's (l, m) list,
+// Load_Balance.F90:357-368) between the slice's own arrays (mode index
+// slowest, the reference's equation_set rhs(N_r nlinks, 2, my_num_lm)) and
+// the device state ([lm][re/im][k], lm = l (l + 1) / 2 + m).
+__global__ void modes_scatter_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                     const long* __restrict__ lm_of, int nmodes, int k, long state_plane,
+                                     long slice_plane, int nplanes, int to_device) {
+    const long total = (long)nplanes * nmodes * 2 * k;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % (2L * k));
+        const long rest = e / (2L * k);
+        const int md = (int)(rest % nmodes);
+        const int pl = (int)(rest / nmodes);
+        const long so = pl * slice_plane + (long)md * 2 * k + i;
+        const long dof = pl * state_plane + lm_of[md] * 2 * k + i;
+        if (to_device)
+            dst[dof] = src[so];   // src: the slice, dst: the state
+        else
+            dst[so] = src[dof];   // src: the state, dst: the slice
+    }
+}
+
+// Batched transpose: out[b][i][j] = in[b][j][i] (n x n blocks), for the
+// reference's column-major per-l matrices.
+__global__ void transpose_batch_kernel(const double* __restrict__ in, double* __restrict__ out, int n) {
+    __shared__ double tile[32][33];
+    const size_t b = blockIdx.z;
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    const double* src = in + b * n * n;
+    double* dst = out + b * n * n;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int j = j0 + r, i = i0 + threadIdx.x;
+        if (j < n && i < n) tile[r][threadIdx.x] = src[(size_t)j * n + i];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, j = j0 + threadIdx.x;
+        if (i < n && j < n) dst[(size_t)i * n + j] = tile[threadIdx.x][r];
+    }
+}
+
+static void scatter_launch(Ctx& c, const double* src, double* dst, const long* d_lm, int nmodes, int k,
+                           long state_plane, long slice_plane, int np, bool to_device) {
+    modes_scatter_kernel<<<1184, 256, 0, c.stream>>>(src, dst, d_lm, nmodes, k, state_plane, slice_plane, np,
+                                                     to_device ? 1 : 0);
+    RA_CUDA(cudaGetLastError());
+}
+
+static std::vector<long> mode_indices(const Ctx& c, int nmodes, const int* l_of, const int* m_of) {
+    if (nmodes <= 0 || !l_of || !m_of) throw ArgError("a mode list needs nmodes > 0 and l, m arrays");
+    std::vector<long> lm(nmodes);
+    std::vector<char> seen(c.d.nlm, 0);
+    for (int i = 0; i < nmodes; ++i) {
+        const int l = l_of[i], m = m_of[i];
+        if (l < 0 || l > c.d.lmax || m < 0 || m > l)
+            throw ArgError("mode " + std::to_string(i) + " (l = " + std::to_string(l) + ", m = " + std::to_string(m) +
+                           ") is outside 0 <= m <= l <= l_max");
+        lm[i] = lm_index(l, m);
+        if (seen[lm[i]]) throw ArgError("mode (l = " + std::to_string(l) + ", m = " + std::to_string(m) + ") repeated");
+        seen[lm[i]] = 1;
+    }
+    return lm;
+}
+
+// moves one slice's W-P-T, Z and AB arrays to (to_device) or from the device state
+static void move_modes(Ctx& c, int nmodes, const int* l_of, const int* m_of, const double* wpt_in, const double* z_in,
+                       const double* ab_in, double* wpt_out, double* z_out, double* ab_out, bool to_device) {
+    const std::vector<long> lm = mode_indices(c, nmodes, l_of, m_of);
+    const int nr = c.d.nr;
+    long* d_lm = nullptr;
+    double* d_tmp = nullptr;
+    const size_t nw = (size_t)nmodes * 2 * 3 * nr, nz = (size_t)nmodes * 2 * nr;
+    RA_CUDA(cudaMalloc(&d_lm, lm.size() * sizeof(long)));
+    cudaError_t e = cudaMalloc(&d_tmp, (nw + 5 * nz) * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(d_lm);
+        throw CudaError(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    try {
+        RA_CUDA(cudaMemcpyAsync(d_lm, lm.data(), lm.size() * sizeof(long), cudaMemcpyHostToDevice, c.stream));
+        double* t_w = d_tmp;
+        double* t_z = d_tmp + nw;
+        double* t_ab = d_tmp + nw + nz;
+        const long plane = c.d.nlm * 2L * nr;
+        auto run = [&](const double* src, double* dst, int k, long state_plane, long slice_plane, int np) {
+            scatter_launch(c, src, dst, d_lm, nmodes, k, state_plane, slice_plane, np, to_device);
+        };
+        if (to_device) {
+            RA_CUDA(cudaMemcpyAsync(t_w, wpt_in, nw * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+            RA_CUDA(cudaMemcpyAsync(t_z, z_in, nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+            if (ab_in) RA_CUDA(cudaMemcpyAsync(t_ab, ab_in, 4 * nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+            else RA_CUDA(cudaMemsetAsync(t_ab, 0, 4 * nz * sizeof(double), c.stream));
+            run(t_w, c.d_sol_wpt, 3 * nr, 0, 0, 1);
+            run(t_z, c.d_sol_z, nr, 0, 0, 1);
+            run(t_ab, c.d_ab, nr, plane, (long)nz, 4);
+            RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+            scan_nonfinite(c, t_w, (long)(nw + 5 * nz));
+        } else {
+            run(c.d_sol_wpt, t_w, 3 * nr, 0, 0, 1);
+            run(c.d_sol_z, t_z, nr, 0, 0, 1);
+            run(c.d_ab, t_ab, nr, plane, (long)nz, 4);
+            if (wpt_out) RA_CUDA(cudaMemcpyAsync(wpt_out, t_w, nw * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            if (z_out) RA_CUDA(cudaMemcpyAsync(z_out, t_z, nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            if (ab_out) RA_CUDA(cudaMemcpyAsync(ab_out, t_ab, 4 * nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        }
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    } catch (...) {
+        cudaFree(d_lm);
+        cudaFree(d_tmp);
+        throw;
+    }
+    cudaFree(d_lm);
+    cudaFree(d_tmp);
 }
 
 }  // namespace ra
@@ -578,11 +722,19 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
 template <class F>
 static int guarded(ra_ctx* ctx, F f) {
     try {
+        // one process may hold contexts on several devices: make this context's current
+        if (ctx && ctx->c.stream) RA_CUDA(cudaSetDevice(ctx->c.cfg.device));
         f();
         return RA_OK;
     } catch (const ArgError& e) {
         if (ctx) ctx->c.err = e.what;
         return RA_ERR_ARG;
+    } catch (const SingularError& e) {
+        if (ctx) ctx->c.err = e.what;
+        return RA_ERR_SINGULAR;
+    } catch (const NonFiniteError& e) {
+        if (ctx) ctx->c.err = e.what;
+        return RA_ERR_NONFINITE;
     } catch (const CudaError& e) {
         if (ctx) ctx->c.err = e.what;
         return e.code == cudaErrorMemoryAllocation ? RA_ERR_NOMEM : RA_ERR_CUDA;
@@ -686,7 +838,13 @@ int ra_put_state(ra_ctx* ctx, const double* wpt, const double* z, const double* 
         RA_CUDA(cudaMemcpyAsync(c.d_sol_z, z, nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         if (ab) RA_CUDA(cudaMemcpyAsync(c.d_ab, ab, 4 * nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         else RA_CUDA(cudaMemsetAsync(c.d_ab, 0, 4 * nz * sizeof(double), c.stream));
-        RA_CUDA(cudaStreamSynchronize(c.stream));
+        // a new state clears the error word; non-finite input is refused
+        RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+        scan_nonfinite(c, c.d_sol_wpt, (long)nw);
+        scan_nonfinite(c, c.d_sol_z, (long)nz);
+        if (ab) scan_nonfinite(c, c.d_ab, 4L * (long)nz);
+        c.have_state = false;
+        check_status(c);
         c.iteration = iteration > 0 ? iteration : 1;
         c.have_state = true;
     });
@@ -700,6 +858,139 @@ int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab) {
         if (wpt) RA_CUDA(cudaMemcpyAsync(wpt, c.d_sol_wpt, nw * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         if (z) RA_CUDA(cudaMemcpyAsync(z, c.d_sol_z, nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
         if (ab) RA_CUDA(cudaMemcpyAsync(ab, c.d_ab, 4 * nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int ra_put_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of, const double* wpt, const double* z,
+                       const double* ab, int iteration) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!wpt || !z) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        c.have_state = false;
+        move_modes(c, nmodes, l_of, m_of, wpt, z, ab, nullptr, nullptr, nullptr, true);
+        check_status(c);
+        c.iteration = iteration > 0 ? iteration : 1;
+        c.have_state = true;
+    });
+}
+
+int ra_get_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of, double* wpt, double* z, double* ab) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        move_modes(ctx->c, nmodes, l_of, m_of, nullptr, nullptr, nullptr, wpt, z, ab, false);
+    });
+}
+
+int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs, double* coefs) {
+    if (!cfg || (sys != 0 && sys != 1) || nl < 1 || l0 < 0 || l0 + nl - 1 > cfg->l_max || (!lhs && !coefs))
+        return RA_ERR_ARG;
+    try {   // host only: the library's own Load_Linear_Coefficients + Set_Boundary_Conditions
+        Ctx c;
+        check_config(*cfg);
+        c.cfg = *cfg;
+        c.d = make_dims(*cfg);
+        c.dt = cfg->dt;
+        const double rmax = cfg->shell_depth / (1.0 - cfg->aspect_ratio);
+        chebyshev_setup(c, rmax * cfg->aspect_ratio, rmax);
+        reference_setup(c);
+        const int nr = c.d.nr, n = sys ? nr : 3 * nr;
+        std::vector<double> A, Z, cf((size_t)NSLOT * nr);
+        for (int i = 0; i < nl; ++i) {
+            build_l(c, l0 + i, A, Z, cf.data());
+            const std::vector<double>& M = sys ? Z : A;
+            if (lhs) {
+                double* out = lhs + (size_t)i * n * n;   // column-major
+                for (int r = 0; r < n; ++r)
+                    for (int k = 0; k < n; ++k) out[(size_t)k * n + r] = M[(size_t)r * n + k];
+            }
+            if (coefs) std::copy(cf.begin(), cf.end(), coefs + (size_t)i * NSLOT * nr);
+        }
+        return RA_OK;
+    } catch (const ArgError&) {
+        return RA_ERR_ARG;
+    } catch (const std::bad_alloc&) {
+        return RA_ERR_NOMEM;
+    }
+}
+
+int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coefs) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (sys != 0 && sys != 1) throw ArgError("sys must be 0 (linked W-P-T) or 1 (Z)");
+        if (!lhs && !coefs) throw ArgError("nothing to load");
+        const int L = c.d.L, nr = c.d.nr, n = sys ? nr : 3 * nr;
+        if (lhs) {
+            const size_t cnt = (size_t)L * n * n;
+            for (size_t i = 0; i < cnt; ++i)
+                if (!std::isfinite(lhs[i]))
+                    throw NonFiniteError("lhs entry " + std::to_string(i) + " is not finite");
+            double* tmp = nullptr;
+            RA_CUDA(cudaMalloc(&tmp, cnt * sizeof(double)));
+            cudaError_t e = cudaMemcpyAsync(tmp, lhs, cnt * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+            if (e == cudaSuccess) {
+                dim3 grid((n + 31) / 32, (n + 31) / 32, L);
+                transpose_batch_kernel<<<grid, dim3(32, 8), 0, c.stream>>>(tmp, sys ? c.d_Az : c.d_Awpt, n);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+            cudaFree(tmp);
+            if (e != cudaSuccess) throw CudaError(e, "ra_load_matrices upload", __FILE__, __LINE__);
+            c.matrices_loaded |= (sys ? 2 : 1);
+        }
+        if (coefs) {
+            // coefs(n_r, 16 slots, l) of this system's equations: slots of other equations are kept
+            std::vector<double> h((size_t)L * NSLOT * nr);
+            RA_CUDA(cudaMemcpy(h.data(), c.d_coef, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int l = 0; l < L; ++l)
+                for (int sl = 0; sl < NSLOT; ++sl) {
+                    if ((kSlots[sl].eq == EQ_Z) != (sys == 1)) continue;
+                    for (int r = 0; r < nr; ++r) {
+                        const double v = coefs[((size_t)l * NSLOT + sl) * nr + r];
+                        if (!std::isfinite(v)) throw NonFiniteError("coefs entry is not finite");
+                        h[((size_t)l * NSLOT + sl) * nr + r] = v;
+                    }
+                }
+            RA_CUDA(cudaMemcpy(c.d_coef, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    });
+}
+
+int ra_factor(ra_ctx* ctx, double dt) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (!(dt > 0)) throw ArgError("dt must be positive");
+        if (c.matrices_loaded != 3) throw ArgError("ra_factor needs both systems loaded by ra_load_matrices");
+        c.dt = dt;
+        factor_matrices(c);
+        if (c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(c);
+        c.matrices_loaded = 0;
+    });
+}
+
+int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (c.graph_exec) {   // the captured step holds the old pointer
+            cudaGraphExecDestroy(c.graph_exec);
+            cudaGraphDestroy(c.graph);
+            c.graph_exec = nullptr;
+            c.graph = nullptr;
+        }
+        if (!bc_values) {
+            if (c.d_bcval) cudaFree(c.d_bcval);
+            c.d_bcval = nullptr;
+            return;
+        }
+        const size_t cnt = (size_t)4 * c.d.nlm * 4;
+        for (size_t i = 0; i < cnt; ++i)
+            if (!std::isfinite(bc_values[i])) throw NonFiniteError("bc_values entry is not finite");
+        if (!c.d_bcval) dalloc(c.d_bcval, cnt);
+        RA_CUDA(cudaMemcpyAsync(c.d_bcval, bc_values, cnt * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
     });
 }
@@ -1042,6 +1333,7 @@ int ra_advance(ra_ctx* ctx) {
         run_stage(ctx->c, 7, 0.0, 0.0);
         ctx->c.old_dt = ctx->c.dt;
         ++ctx->c.iteration;
+        check_status(ctx->c);
     });
 }
 

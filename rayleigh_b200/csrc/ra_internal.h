@@ -69,6 +69,26 @@ struct Radial {
 
 struct GemmTile { int item, mt, nt, par; };
 
+// One batch of per-l systems for the block substitution (k_solve.cu): M in
+// block-substitution form [count][n][n], row permutations [count][n],
+// right-hand sides and solutions as columns of n doubles.
+struct LuSys {
+    const double* M;
+    const int* perm;
+    const double* rhs;
+    double* sol;
+    int n;
+};
+// where a tile's right-hand-side columns are: the step's equation-set layout
+// (2 (l+1) columns from l (l+1)/2 on), the identity (explicit inverse), or a
+// fixed number of columns per l ([l][ncols][n])
+enum { LU_MODE_STEP = 0, LU_MODE_INVERSE = 1, LU_MODE_FIXED = 2 };
+struct LuWork {
+    int* d_status = nullptr;
+    double* d_inv = nullptr;   // inverses of the diagonal blocks
+    int cap_n = 0, cap_count = 0;
+};
+
 // One batched split-precision product of the step (RA_PREC_MIXED): digit
 // buffers of its operands, the per-product descriptors, the tile list and the
 // per-step split jobs.
@@ -109,7 +129,14 @@ struct Ctx {
     double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot
     double *d_twid = nullptr;                         // [nth] complex exp(2 pi i k / nphi)
     double *d_twp = nullptr;                          // per-pass twiddles of the in-place phi FFT
-    double *d_Awpt = nullptr, *d_Az = nullptr;        // inverses [L][3nr][3nr], [L][nr][nr]
+    double *d_Awpt = nullptr, *d_Az = nullptr;        // LU factors in block-substitution form [L][3nr][3nr], [L][nr][nr]
+    int *d_perm_wpt = nullptr, *d_perm_z = nullptr;   // row permutations of the factors [L][3nr], [L][nr]
+    int *d_skip_z = nullptr;                          // [L]: 1 where Z is not solved for (l = 0)
+    double *d_Ainv_wpt = nullptr, *d_Ainv_z = nullptr;   // RA_PREC_MIXED: (A_l^-1)^T, rows = columns of A_l^-1
+    int solve_nc = 32, solve_nc_z = 32;               // right-hand-side columns per substitution CTA (W-P-T, Z)
+    int n_inv_sol_tiles = 0, n_inv_sol_tiles_z = 0, n_solve_tiles_z = 0;
+    int *d_inv_sol_tiles = nullptr, *d_inv_sol_tiles_z = nullptr;   // tile lists of the explicit inverses (mixed form)
+    int* d_solve_tiles_z = nullptr;                   // the Z system's substitution tiles
     int *d_ltiles = nullptr;                          // LT tile lists
     int n_inv_tiles = 0, n_fwd_tiles = 0, n_cheb_tiles = 0, n_solve_tiles = 0;
     int *d_inv_tiles = nullptr, *d_fwd_tiles = nullptr, *d_cheb_tiles = nullptr, *d_solve_tiles = nullptr;
@@ -125,18 +152,25 @@ struct Ctx {
     double *d_p2b = nullptr;                          // [m][par][nth2][4][nr][2]     f_even, f_odd
     double *d_s2b = nullptr;                          // [row][4][nr][2]
     unsigned long long *d_cfl = nullptr;              // CFL max (double bits)
-    int *d_status = nullptr;                          // device error word
+    int *d_status = nullptr;                          // device error word (RA_STATUS_* bits)
+    int matrices_loaded = 0;                          // ra_load_matrices: bit 0 W-P-T, bit 1 Z (until ra_factor)
+    double *d_bcval = nullptr;                        // caller's boundary values [eq][lm][re/im][top/bottom], or none
     double *d_kew = nullptr;                          // [nth] theta weights / n_phi, then [nr] radial weights
     double *d_ke_rows = nullptr;                      // [nth][nr] kinetic-energy shares, then the sum
     double *d_kaz = nullptr;                          // [nth] 1 / n_phi (azimuthal averages)
 
     MixedPlan mx_inv, mx_fwd, mx_solve;               // RA_PREC_MIXED Legendre transforms, implicit solve
+    LuWork lu_work;                                   // factorisation scratch
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     long graph_launches = 0;                          // kernels in one replay of the step graph
     double graph_old_ab = 0, graph_new_ab = 0;
 };
+
+// bits of the device error word
+constexpr int RA_STATUS_TIMEOUT = 1;     // a bounded pipeline wait of a split-precision product ran out
+constexpr int RA_STATUS_NONFINITE = 2;   // a NaN/Inf reached the right-hand side of the implicit solve
 
 // radial profile packing in d_radial: index k * nr + r
 enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R, R_COUNT };
@@ -179,7 +213,20 @@ void lt_forward_prepare(Ctx& c);
 void solve_prepare(Ctx& c);
 void launch_rlm_b(Ctx& c, double new_ab);
 void launch_solve(Ctx& c);
-int  invert_matrices(Ctx& c, double* d_mats, int n, int count, const int* skip);
+void factor_matrices(Ctx& c);   // LU of the loaded per-l matrices (+ explicit inverses in the mixed form)
+// k_solve.cu
+int lu_nc_for(int n);
+void lu_workspace(LuWork& w, int n, int count);
+void lu_workspace_free(LuWork& w);
+int lu_factor_batch(cudaStream_t st, LuWork& w, double* d_mats, int* d_perm, int n, int count, const int* d_skip,
+                    long* launches);
+void launch_lu_solve(cudaStream_t st, const int* d_tiles, int ntiles, const LuSys& sys, int mode, int ncols_fixed,
+                     int nc);
+void lu_append_tiles(std::vector<int>& t, int sys, int L, const std::vector<int>& ncols_of_l, int nc);
+void launch_lu_refine(cudaStream_t st, const int* d_tiles, int ntiles, const LuSys& s, const float* d_mf,
+                      const double* d_a, int ncols, int* d_iters);
+void launch_to_float(cudaStream_t st, const double* in, float* out, long count);
+int lu_refine_tile_cols();
 void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse);
 void launch_cheb_columns(Ctx& c, const double* d_in, double* d_out, long ncols, int mode, int order);
 void mixed_setup(Ctx& c);
@@ -203,6 +250,16 @@ struct CudaError {
     CudaError(cudaError_t e, const char* call, const char* file, int line) : code(e) {
         what = std::string(call) + " failed at " + file + ":" + std::to_string(line) + ": " + cudaGetErrorString(e);
     }
+};
+
+struct SingularError {   // a negligible pivot in a per-l matrix: RA_ERR_SINGULAR
+    std::string what;
+    explicit SingularError(std::string w) : what(std::move(w)) {}
+};
+
+struct NonFiniteError {   // RA_ERR_NONFINITE
+    std::string what;
+    explicit NonFiniteError(std::string w) : what(std::move(w)) {}
 };
 
 struct ArgError {

@@ -1,0 +1,54 @@
+"""The library's own assembly of the per-l implicit matrices (ra_build_matrices,
+host only, no GPU) against the oracle's restatement of Load_Linear_Coefficients +
+Set_Boundary_Conditions (Sphere_Linear_Terms.F90:196-1100, Linear_Solve.F90:494-539),
+and the Post_Solve coefficients of the same terms."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def _slots():
+    # (eq, var, dorder) of the 16 coefficient slots, in the order the C ABI documents
+    W, P, T, Z = O.WVAR, O.PVAR, O.TVAR, O.ZVAR
+    WE, PE, TE, ZE = O.WEQ, O.PEQ, O.TEQ, O.ZEQ
+    return [(WE, W, 0), (WE, W, 1), (WE, W, 2), (WE, P, 1), (WE, T, 0), (PE, W, 0), (PE, W, 1), (PE, W, 2),
+            (PE, W, 3), (PE, P, 0), (TE, T, 0), (TE, T, 1), (TE, T, 2), (ZE, Z, 0), (ZE, Z, 1), (ZE, Z, 2)]
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(n_r=24, l_max=7, dt=2e-4, ekman=1e-3, rayleigh=1e5),
+    dict(n_r=32, l_max=7, dt=1e-4, no_slip_top=False, no_slip_bottom=False, fix_tvar_bottom=False, dtdr_bottom=-1.0,
+         rotation=False),
+    dict(n_r=128, l_max=7, dt=1e-5, ekman=1e-4, rayleigh=1e5),   # the batched-solve workload's radial size
+])
+def test_build_matrices_match_oracle(cfg):
+    import rayleigh_b200 as rb
+    oc = O.Config(**cfg)
+    o = O.Oracle(oc)
+    L = oc.l_max + 1
+    rc = rb.Config(**cfg)
+    wpt, cw = rb.build_matrices(rc, 0, 0, L, coefs=True)
+    z = rb.build_matrices(rc, 1, 1, L - 1)
+    for l in range(L):
+        ref = o.mat_wpt[l]
+        got = wpt[l].T                          # column-major per l
+        scale = np.abs(ref).max()
+        assert np.abs(got - ref).max() <= 1e-13 * scale, l
+        if l > 0:
+            assert np.abs(z[l - 1].T - o.mat_z[l]).max() <= 1e-13 * np.abs(o.mat_z[l]).max(), l
+        for s, key in enumerate(_slots()):
+            ref_c = o.coefs[l].get(key)
+            if ref_c is None:
+                assert not np.any(cw[l, s]), (l, key)
+            else:
+                np.testing.assert_allclose(cw[l, s], ref_c, rtol=1e-14, atol=1e-300)
+
+
+def test_build_matrices_argument_errors():
+    import rayleigh_b200 as rb
+    rc = rb.Config(n_r=24, l_max=7)
+    with pytest.raises(rb.RayleighError):
+        rb.build_matrices(rc, 0, 5, 4)       # l beyond l_max
+    with pytest.raises(rb.RayleighError):
+        rb.build_matrices(rb.Config(n_r=7, l_max=7), 0, 0, 1)

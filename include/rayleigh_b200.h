@@ -251,6 +251,11 @@ int ra_point_probes(ra_ctx* ctx, const int* quantities, int nq, const int* r_idx
  * if kernel_ms is not NULL, the summed time of each kernel of the step in
  * kernel_ms[0..nk) in the order of ra_kernel_name(). */
 int ra_time_steps(ra_ctx* ctx, int nsteps, double* total_ms, double* kernel_ms, int nk);
+/* ra_step (graph replays included) bracketed by CUDA events on the context's
+ * stream: *total_ms receives the device time of the nsteps steps.  The
+ * status check that ends ra_step (a host read of the device error word)
+ * follows the closing event, so it is not part of the time. */
+int ra_step_timed(ra_ctx* ctx, int nsteps, double* total_ms);
 /* Number of kernels one step launches and their names (static strings). */
 int ra_kernels_per_step(void);
 const char* ra_kernel_name(int i);

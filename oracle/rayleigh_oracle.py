@@ -269,10 +269,35 @@ class Horizontal:
 # FFT in phi (Fourier_Transform.F90:100-183): unnormalised, packed n+2 layout
 # ---------------------------------------------------------------------------
 
+# Threads of the phi FFTs: 1 (NumPy's FFT) by default; the CPU baseline sets the
+# host's core count (SciPy's FFT with that many workers, the same transform).
+FFT_WORKERS = 1
+
+
+def set_fft_workers(n):
+    """Threads for the phi FFTs (1 = NumPy's single-threaded FFT)."""
+    global FFT_WORKERS
+    FFT_WORKERS = max(1, int(n))
+
+
+def _irfft(c, n):
+    if FFT_WORKERS > 1:
+        import scipy.fft
+        return scipy.fft.irfft(c, n=n, axis=-1, workers=FFT_WORKERS)
+    return np.fft.irfft(c, n=n, axis=-1)
+
+
+def _rfft(x):
+    if FFT_WORKERS > 1:
+        import scipy.fft
+        return scipy.fft.rfft(x, axis=-1, workers=FFT_WORKERS)
+    return np.fft.rfft(x, axis=-1)
+
+
 def fft_c2r(p3, n_phi):
     """c2r_ip4D_fftw: last axis (n_phi+2 packed re/im) -> n_phi real values (unnormalised)."""
     c = p3[..., 0::2] + 1j * p3[..., 1::2]
-    y = np.fft.irfft(c, n=n_phi, axis=-1) * n_phi
+    y = _irfft(c, n_phi) * n_phi
     out = np.zeros_like(p3)
     out[..., :n_phi] = y
     return out
@@ -280,7 +305,7 @@ def fft_c2r(p3, n_phi):
 
 def fft_r2c(p3, n_phi):
     """r2c_ip4D_fftw: first n_phi real values -> packed spectrum (unnormalised)."""
-    c = np.fft.rfft(p3[..., :n_phi], axis=-1)
+    c = _rfft(p3[..., :n_phi])
     out = np.empty(p3.shape[:-1] + (n_phi + 2,))
     out[..., 0::2] = c.real
     out[..., 1::2] = c.imag
@@ -720,10 +745,12 @@ class Oracle:
             out.append(b)
         return out
 
-    def physical_space(self, p3, thetas=None):
+    def physical_space(self, p3, thetas=None, diagnostics=True):
         """Sphere_Physical_Space.F90:98-224 (hydro): p3a (18 fields) -> p3b (4 fields) + CFL.
 
-        ``thetas`` (index array) says which theta rows p3 holds (all when None)."""
+        ``thetas`` (index array) says which theta rows p3 holds (all when None).
+        ``diagnostics=False`` skips what only the diagnostics read (the pressure
+        and its phi derivative on the grid, the copy of every grid field)."""
         cfg, h = self.cfg, self.h
         th = slice(None) if thetas is None else np.asarray(thetas)
         nphi = cfg.n_phi
@@ -743,7 +770,10 @@ class Oracle:
         f["dvtdp"] = dphi(f["vt"])
         f["dvpdp"] = dphi(f["vp"])
         f["dtdp"] = dphi(f["t"])
-        f["dpdp"] = dphi(f["p"])     # the diagnostics' pressure_dphi (only read by them)
+        if diagnostics:
+            f["dpdp"] = dphi(f["p"])     # the diagnostics' pressure_dphi (only read by them)
+        else:
+            del f["p"]
         for k in list(f.keys()):
             f[k] = fft_c2r(f[k], nphi)[..., :nphi]
         csc = h.csctheta[th][:, None, None]
@@ -755,7 +785,8 @@ class Oracle:
         # the velocity and temperature Benchmark_Checkup reads at this point of the step (:158-159)
         self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
         self.last_temperature = f["t"]
-        self.last_fields = dict(f)   # every physical-space field, [theta, r, phi]: the diagnostics' buffer
+        if diagnostics:
+            self.last_fields = dict(f)   # every physical-space field, [theta, r, phi]: the diagnostics' buffer
         r = self.radius[None, :, None]
         dlnrho = self.dlnrho[None, :, None]
         one_over_r = 1.0 / r

@@ -144,6 +144,7 @@ def load_library(path: str | None = None):
         "ra_costheta": ([_VP, _VP], ctypes.c_int),
         "ra_launch_count": ([_VP], ctypes.c_long),
         "ra_time_steps": ([_VP, ctypes.c_int, _DP, _DP, ctypes.c_int], ctypes.c_int),
+        "ra_step_timed": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
         "ra_kernels_per_step": ([], ctypes.c_int),
         "ra_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "ra_mixed_gemm": ([_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -283,6 +284,13 @@ class Rayleigh:
         cfl = ctypes.c_double()
         self._check(self.lib.ra_step(self.h, int(nsteps), ctypes.byref(cfl)))
         return cfl.value
+
+    def step_timed(self, nsteps):
+        """nsteps steps as ra_step runs them (graph replays), device-timed with CUDA events
+        on the context's stream: total milliseconds."""
+        ms = ctypes.c_double()
+        self._check(self.lib.ra_step_timed(self.h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
 
     def time_steps(self, nsteps):
         """Device-timed steps (CUDA events on the context's stream): (total_ms, {kernel: ms})."""

@@ -556,7 +556,7 @@ static void scan_nonfinite(Ctx& c, const double* d_x, long n) {
     RA_CUDA(cudaGetLastError());
 }
 
-static void run_steps(Ctx& c, int nsteps, double* cfl) {
+static void run_steps(Ctx& c, int nsteps, double* cfl, bool check = true) {
     if (!c.have_state) throw ArgError("ra_put_state must be called before stepping");
     for (int s = 0; s < nsteps; ++s) {
         double new_ab, old_ab;
@@ -588,7 +588,7 @@ static void run_steps(Ctx& c, int nsteps, double* cfl) {
         c.old_dt = c.dt;
         ++c.iteration;
     }
-    check_status(c);
+    if (check) check_status(c);
     if (cfl) {
         unsigned long long bits = 0;
         RA_CUDA(cudaMemcpyAsync(&bits, c.d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c.stream));
@@ -993,6 +993,30 @@ int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values) {
         RA_CUDA(cudaMemcpyAsync(c.d_bcval, bc_values, cnt * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
     });
+}
+
+int ra_step_timed(ra_ctx* ctx, int nsteps, double* total_ms) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (nsteps < 1 || !total_ms) return RA_ERR_ARG;
+    int rc = guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        cudaEvent_t e0, e1;
+        RA_CUDA(cudaEventCreate(&e0));
+        RA_CUDA(cudaEventCreate(&e1));
+        c.launches = 0;
+        RA_CUDA(cudaEventRecord(e0, c.stream));
+        run_steps(c, nsteps, nullptr, false);   // graph replays from the second step on (use_graph)
+        RA_CUDA(cudaEventRecord(e1, c.stream));
+        RA_CUDA(cudaEventSynchronize(e1));
+        check_status(c);
+        float ms = 0.f;
+        RA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *total_ms = ms;
+    });
+    if (rc == RA_ERR_ARG && !ctx->c.have_state) return RA_ERR_STATE;
+    return rc;
 }
 
 int ra_step(ra_ctx* ctx, int nsteps, double* cfl) {

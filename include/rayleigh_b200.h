@@ -67,6 +67,8 @@ typedef struct ra_config {
     int    precision;        /* RA_PREC_FP64 or RA_PREC_MIXED */
     int    use_graph;        /* capture the steady AB2 step as a CUDA graph */
     int    device;           /* CUDA device ordinal */
+    int    autotune;         /* 0: built-in kernel choices; 1: time the candidate kernels of each
+                                tunable stage at set-up on this device and keep the fastest */
 } ra_config;
 
 /* Fills *cfg with the defaults of the reference (Controls.F90, PDE_Coefficients.F90). */
@@ -332,6 +334,23 @@ int ra_lu_tiles(const ra_lu* lu, int ncols, int mode);
 int ra_radius(const ra_ctx* ctx, double* radius);
 /* Gauss-Legendre nodes cos(theta) (n_theta) as used by the context. */
 int ra_costheta(const ra_ctx* ctx, double* costheta);
+
+/* Kernel choices of the tunable stages (the autotuner's knobs):
+ *   "physics"   physical-space kernel: 1 every FFT pass in shared memory
+ *               (n_theta <= 768); 0 the last (radix-3) pass and the
+ *               nonlinear terms in registers, two CTAs per SM, 2 the same
+ *               with one CTA per SM (n_theta 384, 768, 1536; the only
+ *               kernel at 1536)
+ *   "solve_nc"  right-hand-side columns per block-substitution CTA of the
+ *               W-P-T system: 32 or 16 (32 only where its column block fits)
+ * ra_get_choice reads a choice, ra_set_choice forces one (RA_ERR_ARG for an
+ * unknown knob or value); the results do not depend on the choice beyond
+ * rounding.  ra_autotune times every candidate on the context's buffers
+ * (nreps launches each, CUDA events) and keeps the fastest; ms_out (may be
+ * NULL) receives, per knob in the order above, the chosen candidate's time. */
+int ra_get_choice(const ra_ctx* ctx, const char* knob, int* value);
+int ra_set_choice(ra_ctx* ctx, const char* knob, int value);
+int ra_autotune(ra_ctx* ctx, int nreps, double* ms_out);
 
 /* Number of kernel launches issued by the last ra_step call (for accounting). */
 long ra_launch_count(const ra_ctx* ctx);

@@ -51,6 +51,7 @@ class _Config(ctypes.Structure):
         ("dtdr_top", ctypes.c_double), ("dtdr_bottom", ctypes.c_double),
         ("dt", ctypes.c_double), ("alpha_implicit", ctypes.c_double),
         ("precision", ctypes.c_int), ("use_graph", ctypes.c_int), ("device", ctypes.c_int),
+        ("autotune", ctypes.c_int),
     ]
 
 
@@ -83,6 +84,7 @@ class Config:
     precision: int = PREC_FP64
     use_graph: bool = True
     device: int = 0
+    autotune: bool = False
 
     def to_c(self):
         c = _Config()
@@ -145,6 +147,9 @@ def load_library(path: str | None = None):
         "ra_launch_count": ([_VP], ctypes.c_long),
         "ra_time_steps": ([_VP, ctypes.c_int, _DP, _DP, ctypes.c_int], ctypes.c_int),
         "ra_step_timed": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
+        "ra_get_choice": ([_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "ra_set_choice": ([_VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "ra_autotune": ([_VP, ctypes.c_int, _DP], ctypes.c_int),
         "ra_kernels_per_step": ([], ctypes.c_int),
         "ra_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "ra_mixed_gemm": ([_VP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -284,6 +289,23 @@ class Rayleigh:
         cfl = ctypes.c_double()
         self._check(self.lib.ra_step(self.h, int(nsteps), ctypes.byref(cfl)))
         return cfl.value
+
+    KNOBS = ("physics", "solve_nc")
+
+    def get_choice(self, knob):
+        v = ctypes.c_int()
+        self._check(self.lib.ra_get_choice(self.h, knob.encode(), ctypes.byref(v)))
+        return v.value
+
+    def set_choice(self, knob, value):
+        self._check(self.lib.ra_set_choice(self.h, knob.encode(), int(value)))
+
+    def autotune(self, nreps=3):
+        """Times every candidate of each knob on this context and keeps the fastest;
+        returns {knob: (choice, ms)}."""
+        ms = (ctypes.c_double * len(self.KNOBS))()
+        self._check(self.lib.ra_autotune(self.h, int(nreps), ms))
+        return {k: (self.get_choice(k), ms[i]) for i, k in enumerate(self.KNOBS)}
 
     def step_timed(self, nsteps):
         """nsteps steps as ra_step runs them (graph replays), device-timed with CUDA events

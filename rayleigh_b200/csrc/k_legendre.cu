@@ -1,9 +1,9 @@
 // Legendre path: P_l^m table generation and the two Legendre transforms.
 //
 //  * plm_kernel  restates Compute_Plms + Parity_Resort
-//    (src/Math_Layer/Legendre_Polynomials.F90:146-331) in FP64 with a carried
-//    binary exponent, so the sin^m(theta) underflow that the reference avoids
-//    with REAL*16 is handled without quad precision.
+//    (src/Math_Layer/Legendre_Polynomials.F90:146-331) in double-double
+//    arithmetic (the reference computes in REAL*16) with a carried binary
+//    exponent for the sin^m(theta) underflow.
 //  * lt_inverse_kernel restates StP_4d_dgp2 (Legendre_Transforms.F90:968-1074):
 //    per m, an even-l and an odd-l product, then the equatorial mirror
 //    (south = e + o, north = e - o).
@@ -17,53 +17,106 @@
 
 namespace ra {
 
-__global__ void plm_kernel(const double* __restrict__ x, const double* __restrict__ s,
-                           const double* __restrict__ w2pi, int L, int nth,
-                           double* __restrict__ Ptab, double* __restrict__ iPtab) {
+// Double-double arithmetic (an unevaluated sum hi + lo, |lo| <= ulp(hi)/2, about
+// 106 significant bits) for the table recurrence, so that the tables come out
+// correctly rounded from a computation at least as precise as the reference's
+// REAL*16 one.  Error-free transformations: Knuth's two-sum, the FMA two-product.
+struct dd {
+    double hi, lo;
+};
+__device__ __forceinline__ dd dd_two_sum(double a, double b) {
+    const double s = a + b, bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ dd dd_fast(double a, double b) {   // |a| >= |b|
+    const double s = a + b;
+    return {s, b - (s - a)};
+}
+__device__ __forceinline__ dd dd_mul(dd a, dd b) {
+    const double p = a.hi * b.hi;
+    const double e = fma(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi);
+    return dd_fast(p, e);
+}
+__device__ __forceinline__ dd dd_mul_d(dd a, double b) {
+    const double p = a.hi * b;
+    return dd_fast(p, fma(a.hi, b, -p) + a.lo * b);
+}
+__device__ __forceinline__ dd dd_sub(dd a, dd b) {
+    dd s = dd_two_sum(a.hi, -b.hi);
+    const dd t = dd_two_sum(a.lo, -b.lo);
+    s = dd_fast(s.hi, s.lo + t.hi);
+    return dd_fast(s.hi, s.lo + t.lo);
+}
+__device__ __forceinline__ dd dd_div(dd a, dd b) {
+    const double q1 = a.hi / b.hi;
+    const dd r = dd_sub(a, dd_mul_d(b, q1));
+    const double q2 = r.hi / b.hi;
+    const dd r2 = dd_sub(r, dd_mul_d(b, q2));
+    return dd_fast(dd_fast(q1, q2).hi, dd_fast(q1, q2).lo + r2.hi / b.hi);
+}
+// n / d for integers exactly representable in double
+__device__ __forceinline__ dd dd_ratio(double n, double d) { return dd_div(dd{n, 0.0}, dd{d, 0.0}); }
+__device__ __forceinline__ dd dd_sqrt(dd a) {
+    const double s = sqrt(a.hi);
+    const double e = fma(-s, s, a.hi);   // a.hi - s^2, exact
+    return dd_fast(s, (e + a.lo) / (2.0 * s));
+}
+
+// Compute_Plms + Parity_Resort in double-double: P_m^m from its closed form
+// (Legendre_Polynomials.F90:190-212), the three-term recurrence in l
+// (:215-226), the normalisations 1 / 1/2 (p_lm) and 2 pi w times the
+// double-precision constants 1/(2 N_theta), 1/N_theta (ip_lm, :270-276); a
+// carried binary exponent keeps sin^m(theta) from underflowing.  x, s = sin,
+// and 2 pi w come as hi/lo pairs made from the host's long-double values.
+__global__ void plm_kernel(const double* __restrict__ xhl, const double* __restrict__ shl,
+                           const double* __restrict__ whl, int L, int nth, double* __restrict__ Ptab,
+                           double* __restrict__ iPtab) {
     const int nth2 = nth / 2;
     const int th = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (th >= nth2 || m >= L) return;
     const int lmax = L - 1;
-    const double xv = x[th], sv = s[th];
-    const double wt = w2pi[th];
+    const dd xv{xhl[th], xhl[nth2 + th]}, sv{shl[th], shl[nth2 + th]}, wt{whl[th], whl[nth2 + th]};
     const double stp = (m == 0) ? 1.0 : 0.5;
-    const double pts = (m == 0) ? 1.0 / (2.0 * nth) : 1.0 / (double)nth;
+    const double pts = (m == 0) ? 1.0 / (2.0 * nth) : 1.0 / (double)nth;   // double-precision constants
     const double TWO600 = 0x1p600, TWOM600 = 0x1p-600;
+    const dd twopi{6.283185307179586232e+00, 2.449293598294706414e-16};
     // P_m^m = (-1)^m sqrt((m+1/2)/(2 pi)) prod_{i<=m} sqrt((i-1/2)/i) sin^m(theta)
-    double p = sqrt((m + 0.5) / (2.0 * 3.14159265358979323846));
+    dd p = dd_sqrt(dd_div(dd{m + 0.5, 0.0}, twopi));
     int e = 0;
     for (int i = 1; i <= m; ++i) {
-        p *= sqrt((i - 0.5) / (double)i) * sv;
-        if (p < TWOM600) {
-            p *= TWO600;
+        p = dd_mul(dd_mul(p, dd_sqrt(dd_ratio(2.0 * i - 1.0, 2.0 * i))), sv);
+        if (fabs(p.hi) < TWOM600) {
+            p.hi *= TWO600;
+            p.lo *= TWO600;
             e -= 600;
         }
     }
-    if (m & 1) p = -p;
-    auto store = [&](int l, double v) {
+    if (m & 1) p = dd{-p.hi, -p.lo};
+    auto store = [&](int l, dd v) {
         const long row = row_index(m, l, L);
-        const double a = ldexp(v, e);
-        Ptab[row * nth2 + th] = a * stp;
-        iPtab[row * nth2 + th] = (a * wt) * pts;
+        Ptab[row * nth2 + th] = ldexp(v.hi, e) * stp;
+        const dd vw = dd_mul_d(dd_mul(v, wt), pts);
+        iPtab[row * nth2 + th] = ldexp(vw.hi, e);
     };
     store(m, p);
     if (m == lmax) return;
-    double p1 = p * xv * sqrt(2.0 * m + 3.0);  // P_{m+1}^m
-    double p0 = p;
+    dd p1 = dd_mul(dd_mul(p, xv), dd_sqrt(dd{2.0 * m + 3.0, 0.0}));   // P_{m+1}^m
+    dd p0 = p;
     store(m + 1, p1);
     for (int l = m + 2; l <= lmax; ++l) {
         const double lm1 = (double)(l - 1);
-        double a = (lm1 * lm1 - (double)m * m) / (4.0 * lm1 * lm1 - 1.0);
-        a = sqrt(a);
-        const double t = p1 * xv - a * p0;
-        const double b = (4.0 * (double)l * l - 1.0) / ((double)l * l - (double)m * m);
-        const double pn = t * sqrt(b);
+        const dd a = dd_sqrt(dd_ratio(lm1 * lm1 - (double)m * m, 4.0 * lm1 * lm1 - 1.0));
+        const dd t = dd_sub(dd_mul(p1, xv), dd_mul(a, p0));
+        const dd b = dd_sqrt(dd_ratio(4.0 * (double)l * l - 1.0, (double)l * l - (double)m * m));
+        const dd pn = dd_mul(t, b);
         p0 = p1;
         p1 = pn;
-        if (e < 0 && fabs(p1) > TWO600) {
-            p1 *= TWOM600;
-            p0 *= TWOM600;
+        if (e < 0 && fabs(p1.hi) > TWO600) {
+            p1.hi *= TWOM600;
+            p1.lo *= TWOM600;
+            p0.hi *= TWOM600;
+            p0.lo *= TWOM600;
             e += 600;
         }
         store(l, p1);
@@ -71,10 +124,10 @@ __global__ void plm_kernel(const double* __restrict__ x, const double* __restric
 }
 
 void launch_plm(Ctx& c, const double* d_x, const double* d_w) {
-    // d_x holds [x | s] (2 * nth2 doubles); d_w holds 2 pi w (nth2 doubles)
+    // d_x holds [x hi | x lo | s hi | s lo] (nth2 each); d_w holds [2 pi w hi | lo]
     const int nth2 = c.d.nth2;
     dim3 grid((nth2 + 127) / 128, c.d.L);
-    plm_kernel<<<grid, 128, 0, c.stream>>>(d_x, d_x + nth2, d_w, c.d.L, c.d.nth, c.d_Ptab, c.d_iPtab);
+    plm_kernel<<<grid, 128, 0, c.stream>>>(d_x, d_x + 2 * nth2, d_w, c.d.L, c.d.nth, c.d_Ptab, c.d_iPtab);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }

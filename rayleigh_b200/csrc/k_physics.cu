@@ -743,6 +743,8 @@ FFTPlan make_plan(int n) {
 // double, built once at set-up: the step may be captured into a CUDA graph on
 // its first launch (a context restored at a later iteration), where no
 // allocation or blocking copy may run.
+static bool p3_supported(int n);
+
 void physics_prepare(Ctx& c) {
     if (!c.d_twp) {
         const int n = c.d.nth;
@@ -759,6 +761,323 @@ void physics_prepare(Ctx& c) {
         }
         RA_CUDA(cudaMalloc(&c.d_twp, std::max<size_t>(tw.size(), 2) * sizeof(double)));
         RA_CUDA(cudaMemcpy(c.d_twp, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    c.physics3_ok = p3_supported(c.d.nth);
+    // default: all passes in shared memory where that kernel exists (20.7 against 21.5 ms at
+    // n_theta = 768, N_r = 192); the autotuner measures both
+    c.physics_form = physics_form1_supported(c.d.nth) ? 1 : 0;
+    if (!c.physics3_ok && !physics_form1_supported(c.d.nth))
+        throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no physical-space kernel instance");
+}
+
+// ---------------------------------------------------------------------------
+// Physical-space kernel with the last FFT pass in registers (N = n_theta with
+// a final radix-3 pass: 384, 768, 1536; N/3 threads per row).
+//
+// The c2r runs the in-place passes of physics_kernel except the last one; the
+// last (radix-3, stride-1) pass is done in registers by thread t on the three
+// points 3t, 3t+1, 3t+2 of every field, the same points in every batch, so
+// the nonlinear terms are formed where the transform leaves them, and the
+// r2c's first (radix-3) pass is done on the same registers.  Per field this
+// saves the last pass's write and the read-back of the physical values in the
+// c2r, and the first pass's read in the r2c; the velocity stays in registers
+// (nine complex values per thread).  Shared layout and butterfly dealing are
+// physics_kernel's.
+// ---------------------------------------------------------------------------
+template <int N>
+struct P3 {
+    static constexpr int NT = N / 3;
+    static constexpr int NP = npass_of(N);     // passes; the last one (radix 3) runs in registers
+    static_assert(radix_at(N, npass_of(N) - 1) == 3, "the last pass must be radix 3");
+    static constexpr int FS = fstride(N);
+    static constexpr int SIZE = 8 * FS;        // 4-field FFT buffer + 4 accumulators (double2)
+    static __host__ __device__ constexpr int slot(int p) { return p; }
+};
+
+template <int N, int NB, int NT, int PS = 0>
+__device__ __forceinline__ void fft_dif_upto_last(double2* buf, const double2* twp, int tid) {
+    if constexpr (PS < npass_of(N) - 1) {
+        fft_pass_ip<N, NB, NT, PS, false>(buf, twp, +1, tid);
+        __syncthreads();
+        fft_dif_upto_last<N, NB, NT, PS + 1>(buf, twp, tid);
+    }
+}
+
+template <int N, int NB, int NT, int PS = npass_of(N) - 2>
+__device__ __forceinline__ void fft_dit_from_second(double2* buf, const double2* twp, int tid) {
+    if constexpr (PS >= 0) {
+        fft_pass_ip<N, NB, NT, PS, true>(buf, twp, -1, tid);
+        __syncthreads();
+        fft_dit_from_second<N, NB, NT, PS - 1>(buf, twp, tid);
+    }
+}
+
+// c2r of NB fields of this row (fo, dp as in row_c2r); on return y[b][m] holds
+// the physical pair at buffer position 3t + m of field b.
+template <int N, int NB>
+__device__ __forceinline__ void p3_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h,
+                                       const int (&fo)[NB], const bool (&dp)[NB], double2* buf, int t,
+                                       double2 (&y)[4][3]) {
+    using S = P3<N>;
+    constexpr int NI = N / 2 + 1;
+    const int L = P.L;
+    const long ostride = (long)P.ncola, mstride = 2L * P.ncola;
+    __syncthreads();   // the buffer is free
+    auto item = [](int g, int& k, int& b) {
+        if constexpr (NB == 2 && (N / 2) % 8 == 0) {
+            const int l8 = g & 7, kk = l8 >> 1;
+            b = l8 & 1;
+            k = (g >> 4) * 8 + ((g >> 3) & 1) * 2 + (kk & 1) + ((kk >> 1) << 2);
+        } else {
+            k = g / NB;
+            b = g - k * NB;
+        }
+    };
+    constexpr int QI = (NB * NI + S::NT - 1) / S::NT;
+    constexpr int QC = 3;
+#pragma unroll 1
+    for (int q0 = 0; q0 < QI; q0 += QC) {
+        double2 xk[QC], xn[QC];
+#pragma unroll
+        for (int qq = 0; qq < QC; ++qq) {
+            const int g = t + (q0 + qq) * S::NT;
+            xk[qq] = xn[qq] = make_double2(0.0, 0.0);
+            if (q0 + qq < QI && g < NB * NI) {
+                int k, b;
+                item(g, k, b);
+                const double* base = rowbase + (long)pick(fo, b) * 2;
+                const bool d = pick(dp, b);
+                xk[qq] = spec_value(base, mstride, ostride, k, L, h, d);
+                xn[qq] = spec_value(base, mstride, ostride, N - k, L, h, d);
+            }
+        }
+#pragma unroll
+        for (int qq = 0; qq < QC; ++qq) {
+            const int g = t + (q0 + qq) * S::NT;
+            if (q0 + qq < QI && g < NB * NI) {
+                int k, b;
+                item(g, k, b);
+                const double2 wk = __ldg(P.wr + k);
+                buf[b * S::FS + k] = zform(xk[qq], xn[qq], wk);
+                if (k != 0 && 2 * k != N) buf[b * S::FS + N - k] = zform(xn[qq], xk[qq], make_double2(-wk.x, wk.y));
+            }
+        }
+    }
+    __syncthreads();
+    fft_dif_upto_last<N, NB, S::NT>(buf, P.twp, t);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        double2 u[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) u[m] = buf[b * S::FS + 3 * t + m];
+        dft_small(3, u, +1);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) y[b][m] = u[m];
+    }
+}
+
+template <int N, int MINB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(P3<N>::NT, MINB) physics3_kernel(PhysParams P) {
+    using S = P3<N>;
+    constexpr int FS = S::FS, NT = S::NT;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);
+    double2* acc = buf + 4 * FS;
+    __shared__ double red[NT / 32];
+    __shared__ double rowc[RC_COUNT];
+    const int t = threadIdx.x;
+    const int h = (int)cluster.block_rank();
+    const int nr = P.nr;
+    const int pair = blockIdx.x >> 1;
+    const int r = pair % nr;
+    const int thh = pair / nr;
+    const int th = h ? (N - 1 - thh) : thh;
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    if (t == 0) {
+        const double csc = P.trig[2 * N + th], orad = P.radial[R_OVER_R * nr + r];
+        rowc[RC_RAD] = P.radial[R_RADIUS * nr + r];
+        rowc[RC_ORAD] = orad;
+        rowc[RC_RHO] = P.radial[R_DENSITY * nr + r];
+        rowc[RC_DLNRHO] = P.radial[R_DLNRHO * nr + r];
+        rowc[RC_DR] = P.radial[R_DELTA_R * nr + r];
+        rowc[RC_CS] = P.trig[th];
+        rowc[RC_SN] = P.trig[N + th];
+        rowc[RC_CSC] = csc;
+        rowc[RC_COT] = P.trig[3 * N + th];
+        rowc[RC_COR] = P.rotation ? P.coriolis : 0.0;
+        rowc[RC_C2R] = csc * csc * orad;
+        rowc[RC_HSF] = 0.5 * (P.radial[R_DENSITY * nr + r] * P.radial[R_RADIUS * nr + r] * csc);
+    }   // read after p3_c2r's first barrier
+    double2 vr[3], vt[3], vp[3];
+    double2 y[4][3];
+    auto acc_at = [&](int f, int m) -> double2& { return acc[f * FS + S::slot(3 * t + m)]; };
+    // B1: v_r, v_theta, v_phi, dv_r/dr
+    {
+        const int fo[4] = {A_VR, A_VT, A_VP, A_DVRDR};
+        const bool dp[4] = {false, false, false, false};
+        p3_c2r<N, 4>(P, rowbase, h, fo, dp, buf, t, y);
+        const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], dlnrho = rowc[RC_DLNRHO];
+        const double cs = rowc[RC_CS], sn = rowc[RC_SN], csc = rowc[RC_CSC], cot = rowc[RC_COT], cor = rowc[RC_COR];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            vr[m] = y[0][m];
+            vt[m] = make_double2(y[1][m].x * csc, y[1][m].y * csc);
+            vp[m] = make_double2(y[2][m].x * csc, y[2][m].y * csc);
+            const double2 x = y[3][m];
+            auto w0 = [&](double a, double b, double c, double xx) {
+                return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
+            };
+            auto p0 = [&](double a, double b, double c, double xx) {
+                return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
+            };
+            auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+            acc_at(0, m) = make_double2(w0(vr[m].x, vt[m].x, vp[m].x, x.x), w0(vr[m].y, vt[m].y, vp[m].y, x.y));
+            acc_at(1, m) = make_double2(p0(vr[m].x, vt[m].x, vp[m].x, x.x), p0(vr[m].y, vt[m].y, vp[m].y, x.y));
+            acc_at(3, m) = make_double2(z0(vr[m].x, vt[m].x, vp[m].x), z0(vr[m].y, vt[m].y, vp[m].y));
+        }
+    }
+    // B2: dv_r/dtheta, dv_r/dphi, dv_theta/dr, dv_theta/dphi
+    {
+        const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
+        const bool dp[4] = {false, true, false, true};
+        p3_c2r<N, 4>(P, rowbase, h, fo, dp, buf, t, y);
+        const double rad = rowc[RC_RAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double2 a = y[0][m], b = y[1][m], c = y[2][m], d = y[3][m];
+            double2& w = acc_at(0, m);
+            double2& pp = acc_at(1, m);
+            double2& z = acc_at(3, m);
+            w.x += -rho * rad * vt[m].x * a.x * csc - rho * rad * csc * vp[m].x * b.x;
+            w.y += -rho * rad * vt[m].y * a.y * csc - rho * rad * csc * vp[m].y * b.y;
+            pp.x += vr[m].x * c.x * csc + vp[m].x * d.x * c2r;
+            pp.y += vr[m].y * c.y * csc + vp[m].y * d.y * c2r;
+            z.x += vt[m].x * d.x * c2r;
+            z.y += vt[m].y * d.y * c2r;
+        }
+    }
+    // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr (the T term's first part, written)
+    {
+        const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
+        const bool dp[4] = {false, true, false, false};
+        p3_c2r<N, 4>(P, rowbase, h, fo, dp, buf, t, y);
+        const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double2 a = y[0][m], b = y[1][m], c = y[2][m], d = y[3][m];
+            double2& pp = acc_at(1, m);
+            double2& z = acc_at(3, m);
+            z.x += vr[m].x * a.x * csc + vp[m].x * b.x * c2r + vt[m].x * c.x;
+            z.y += vr[m].y * a.y * csc + vp[m].y * b.y * c2r + vt[m].y * c.y;
+            pp.x += -vt[m].x * b.x * c2r;
+            pp.y += -vt[m].y * b.y * c2r;
+            acc_at(2, m) = make_double2(-vr[m].x * d.x, -vr[m].y * d.y);
+        }
+    }
+    // B4: dT/dtheta, dT/dphi; then the r2c's first (radix-3, stride-1) pass on the
+    // thread's own points of W, P, T, Z, in registers
+    {
+        const int fo[2] = {A_DTDT, A_T};
+        const bool dp[2] = {false, true};
+        p3_c2r<N, 2>(P, rowbase, h, fo, dp, buf, t, y);
+        const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
+        double2 u[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const double2 a = y[0][m], b = y[1][m];
+            const double2 tt = acc_at(2, m);
+            u[m] = make_double2(tt.x - a.x * csc * vt[m].x * orad - vp[m].x * b.x * csc * orad,
+                                tt.y - a.y * csc * vt[m].y * orad - vp[m].y * b.y * csc * orad);
+        }
+        dft_small(3, u, -1);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) acc_at(2, m) = u[m];
+#pragma unroll
+        for (int f = 0; f < 4; f += (f == 1 ? 2 : 1)) {   // W, P, Z
+#pragma unroll
+            for (int m = 0; m < 3; ++m) u[m] = acc_at(f, m);
+            dft_small(3, u, -1);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) acc_at(f, m) = u[m];
+        }
+    }
+    // CFL (Find_MyMinDT)
+    double cmax = 0.0;
+    {
+        const double orad = rowc[RC_ORAD], dr = rowc[RC_DR];
+        const double hfac = P.llmax * orad * orad, rfac = 1.0 / (dr * dr);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            cmax = fmax(cmax, (vt[m].x * vt[m].x + vp[m].x * vp[m].x) * hfac);
+            cmax = fmax(cmax, (vt[m].y * vt[m].y + vp[m].y * vp[m].y) * hfac);
+            cmax = fmax(cmax, vr[m].x * vr[m].x * rfac);
+            cmax = fmax(cmax, vr[m].y * vr[m].y * rfac);
+        }
+    }
+    __syncthreads();
+    // the r2c's remaining passes (reverse order, decimation in time) in shared memory
+    fft_dit_from_second<N, 4, NT>(acc, P.twp, t);
+    {
+        constexpr int NI = N / 2 + 1;
+        const int L = P.L;
+        for (int g = t; g < 4 * NI; g += NT) {
+            const int f = g / NI, k = g - f * NI;
+            const double2 zk = acc[f * FS + S::slot(k)];
+            const double2 zn = acc[f * FS + S::slot((N - k) % N)];
+            const double2 wk = __ldg(P.wr + k);
+            const double hs = (f & 1) ? rowc[RC_HSF] : 0.5;
+            auto xval = [&](double2 a, double2 b, double2 w, bool zero_im) {
+                const double2 bn = cconj(b);
+                const double2 e = make_double2(hs * (a.x + bn.x), hs * (a.y + bn.y));
+                const double2 d = make_double2(hs * (a.x - bn.x), hs * (a.y - bn.y));
+                const double2 wd = cmul(cconj(w), d);
+                double2 X = make_double2(e.x + wd.y, e.y - wd.x);
+                if (zero_im) X.y = 0.0;
+                return X;
+            };
+            // both values are read before either is written: k and N - k belong to this item only
+            const bool wk_ok = k < L, wn_ok = k != 0 && 2 * k != N && N - k < L;
+            const double2 xk = xval(zk, zn, wk, k == 0);
+            const double2 xn = xval(zn, zk, make_double2(-wk.x, wk.y), false);
+            if (wk_ok) acc[f * FS + S::slot(k)] = xk;
+            if (wn_ok) acc[f * FS + S::slot(N - k)] = xn;
+        }
+    }
+    cluster.sync();
+    {
+        const double2* peer = cluster.map_shared_rank(acc, h ^ 1);
+        const int L = P.L;
+        const long mstride = 2L * (P.nth / 2) * P.ncolb;
+        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * NP2B);
+        for (int g = t; g < 4 * L; g += NT) {
+            const int k = g >> 2, f = g & 3;
+            const double2 a = acc[f * FS + S::slot(k)], b = peer[f * FS + S::slot(k)];
+            const double2 v = h ? csub(b, a) : cadd(a, b);
+            *reinterpret_cast<double2*>(obase + k * mstride + f * 2) = v;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
+    if ((t & 31) == 0) red[t >> 5] = cmax;
+    cluster.sync();
+    if (t == 0) {
+        double v = red[0];
+        for (int i = 1; i < NT / 32; ++i) v = fmax(v, red[i]);
+        atomicMax(P.cfl, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// the register-last-pass kernel serves the n_theta whose plan ends in radix 3
+static bool p3_supported(int n) { return n == 384 || n == 768 || n == 1536; }
+
+// n_theta with an instance of physics_kernel (all passes in shared memory)
+bool physics_form1_supported(int n) {
+    switch (n) {
+        case 24: case 32: case 48: case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768:
+            return true;
+        default:
+            return false;
     }
 }
 
@@ -784,6 +1103,30 @@ void launch_physics(Ctx& c) {
     if (c.d.L > (2 * c.d.nth) / 3 + 1)
         throw ArgError("n_theta must be at least 3 (l_max + 1) / 2 for the physical-space kernel");
     const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;   // clusters of 2 rows
+    if (c.physics3_ok && c.physics_form != 1) {   // last pass in registers (form 0: two CTAs per SM, 2: one)
+        auto go3 = [&](auto kern, int nt, size_t units) {
+            const size_t smem = units * sizeof(double2);
+            RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kern<<<grid, nt, smem, c.stream>>>(P);
+        };
+        const bool two = c.physics_form == 0;
+        switch (c.d.nth) {
+            case 384:
+                if (two) go3(physics3_kernel<384, 2>, P3<384>::NT, P3<384>::SIZE);
+                else go3(physics3_kernel<384, 1>, P3<384>::NT, P3<384>::SIZE);
+                break;
+            case 768:
+                if (two) go3(physics3_kernel<768, 2>, P3<768>::NT, P3<768>::SIZE);
+                else go3(physics3_kernel<768, 1>, P3<768>::NT, P3<768>::SIZE);
+                break;
+            default:   // 1536: 512 threads and 197 KB of shared memory, one CTA per SM
+                go3(physics3_kernel<1536, 1>, P3<1536>::NT, P3<1536>::SIZE);
+                break;
+        }
+        RA_CUDA(cudaGetLastError());
+        ++c.launches;
+        return;
+    }
     auto go = [&](auto kern, int n, size_t smem_units) {
         const size_t smem = smem_units * sizeof(double2);
         RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -361,9 +361,12 @@ __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
 }
 
 // The column block in shared memory, [row][NC] with the columns of row i
-// permuted by XOR with h(i) = 8 (i mod 2) + (i/2 mod 8): a B fragment (rows
-// k..k+3, k = 0 mod 4, 8 columns) and a walk down 32 consecutive rows of one
-// column both touch every 8-byte bank exactly twice (the minimum).
+// permuted by XOR with h(i) = 8 (i mod 2) + (i/2 mod 8): over a warp, a B
+// fragment (rows k..k+3, k = 0 mod 4, 8 columns) and a walk down 32
+// consecutive rows of one column both touch every 8-byte bank exactly twice.
+// (A layout that is also conflict-free per half warp, h(i) = 4 (i mod 4) +
+// (i/4 mod 4), measured 35 % slower: 0.92 against 0.68 ms at l_max = 127,
+// N_r = 192, with a third of the shared wavefronts.)
 template <int NC>
 __device__ __forceinline__ int xs_index(int i, int c) {
     return i * NC + (c ^ (((i & 1) << 3) | ((i >> 1) & 7)));
@@ -413,12 +416,14 @@ __global__ void __launch_bounds__(LS_THREADS) lu_solve_kernel(const int4* __rest
     }
     const int t = threadIdx.x;
     // permuted right-hand sides (P b), zero past n and past the last column; threads walk rows
-    for (int e = t; e < nrow * NC; e += LS_THREADS) {
-        const int c = e / nrow, i = e % nrow, col = c0 + c;
-        double v = 0.0;
-        if (i < n && col < ncol)
-            v = (mode == LU_MODE_INVERSE) ? (perm[i] == col ? 1.0 : 0.0) : rhs[(size_t)col * n + perm[i]];
-        Xs[xs_index<NC>(i, c)] = v;
+    for (int c = 0; c < NC; ++c) {
+        const int col = c0 + c;
+        for (int i = t; i < nrow; i += LS_THREADS) {
+            double v = 0.0;
+            if (i < n && col < ncol)
+                v = (mode == LU_MODE_INVERSE) ? (perm[i] == col ? 1.0 : 0.0) : rhs[(size_t)col * n + perm[i]];
+            Xs[xs_index<NC>(i, c)] = v;
+        }
     }
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
@@ -524,10 +529,8 @@ __global__ void __launch_bounds__(LS_THREADS) lu_solve_kernel(const int4* __rest
         }
     }
     cp_async_wait<0>();
-    for (int e = t; e < n * NC; e += LS_THREADS) {
-        const int c = e / n, i = e % n, col = c0 + c;
-        if (col < ncol) sol[(size_t)col * n + i] = Xs[xs_index<NC>(i, c)];
-    }
+    for (int c = 0; c < NC && c0 + c < ncol; ++c)
+        for (int i = t; i < n; i += LS_THREADS) sol[(size_t)(c0 + c) * n + i] = Xs[xs_index<NC>(i, c)];
 }
 
 // ---------------------------------------------------------------------------
@@ -769,9 +772,14 @@ static T* upload_vec(Ctx& c, const std::vector<T>& v) {
 // mixed form, of the explicit inverses; built once at set-up, since no
 // allocation may run while a step is captured.
 void solve_prepare(Ctx& c) {
+    c.solve_nc = lu_nc_for(3 * c.d.nr);
+    c.solve_nc_z = lu_nc_for(c.d.nr);
+    rebuild_solve_tiles(c);
+}
+
+// (re)builds the missing tile lists for the current column-block choices
+void rebuild_solve_tiles(Ctx& c) {
     const int L = c.d.L, nr = c.d.nr;
-    c.solve_nc = lu_nc_for(3 * nr);
-    c.solve_nc_z = lu_nc_for(nr);
     auto make = [&](int*& d, int& cnt, const std::vector<int>& ncols, int nc) {
         if (d) return;
         std::vector<int> t;

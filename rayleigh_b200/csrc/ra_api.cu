@@ -315,6 +315,8 @@ static void dalloc(T*& p, size_t count) {
     if (e != cudaSuccess) throw CudaError(e, "cudaMalloc", __FILE__, __LINE__);
 }
 
+static void autotune(Ctx& c, int nreps, double* ms_out);
+
 static void setup(Ctx& c) {
     const Dims& d = c.d;
     RA_CUDA(cudaSetDevice(c.cfg.device));
@@ -330,12 +332,17 @@ static void setup(Ctx& c) {
     gauss_legendre(d.nth, xq, wq);
     c.costheta_h.resize(d.nth);
     for (int i = 0; i < d.nth; ++i) c.costheta_h[i] = (double)xq[i];
-    std::vector<double> xs(2 * d.nth2), w2(d.nth2);
+    // [x hi | x lo | s hi | s lo] and [2 pi w hi | lo] for the table recurrence (double-double)
+    std::vector<double> xs(4 * (size_t)d.nth2), w2(2 * (size_t)d.nth2);
     const long double PI = 3.141592653589793238462643383279502884L;
     for (int i = 0; i < d.nth2; ++i) {
-        xs[i] = (double)xq[i];
-        xs[d.nth2 + i] = (double)sqrtl((1.0L - xq[i]) * (1.0L + xq[i]));
-        w2[i] = (double)(2.0L * PI * wq[i]);
+        const long double x = xq[i], sn = sqrtl((1.0L - xq[i]) * (1.0L + xq[i])), w = 2.0L * PI * wq[i];
+        xs[i] = (double)x;
+        xs[d.nth2 + i] = (double)(x - (long double)xs[i]);
+        xs[2 * d.nth2 + i] = (double)sn;
+        xs[3 * d.nth2 + i] = (double)(sn - (long double)xs[2 * d.nth2 + i]);
+        w2[i] = (double)w;
+        w2[d.nth2 + i] = (double)(w - (long double)w2[i]);
     }
     // trig tables as the reference computes them in double (ProblemSize.F90:489-495)
     std::vector<double> trig(4 * (size_t)d.nth);
@@ -458,6 +465,7 @@ static void setup(Ctx& c) {
     physics_prepare(c);
     lt_forward_prepare(c);
     if (c.cfg.precision == RA_PREC_MIXED) mixed_setup(c);
+    if (c.cfg.autotune) autotune(c, 3, nullptr);
 }
 
 static void release(Ctx& c) {
@@ -465,7 +473,8 @@ static void release(Ctx& c) {
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
     lu_workspace_free(c.lu_work);
-    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp, c.d_Awpt, c.d_Az,
+    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp,
+                      c.d_Awpt, c.d_Az,
                       c.d_Ainv_wpt, c.d_Ainv_z,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
                       c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz, c.d_bcval};
@@ -714,6 +723,107 @@ static void move_modes(Ctx& c, int nmodes, const int* l_of, const int* m_of, con
     cudaFree(d_tmp);
 }
 
+// ---- the autotuner: candidate kernels of the tunable stages ----
+static std::vector<int> knob_candidates(const Ctx& c, int knob) {
+    if (knob == 0) {   // physics
+        std::vector<int> v;
+        if (c.physics3_ok) {
+            v.push_back(0);
+            v.push_back(2);
+        }
+        if (physics_form1_supported(c.d.nth)) v.push_back(1);
+        return v;
+    }
+    std::vector<int> v;   // solve_nc
+    if (lu_nc_for(3 * c.d.nr) == 32) v.push_back(32);
+    v.push_back(16);
+    return v;
+}
+
+static int knob_index(const char* knob) {
+    if (!knob) return -1;
+    if (!std::strcmp(knob, "physics")) return 0;
+    if (!std::strcmp(knob, "solve_nc")) return 1;
+    return -1;
+}
+
+static void drop_graph(Ctx& c) {
+    if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    c.graph_exec = nullptr;
+    c.graph = nullptr;
+}
+
+static void set_knob(Ctx& c, int knob, int value) {
+    const std::vector<int> cand = knob_candidates(c, knob);
+    if (std::find(cand.begin(), cand.end(), value) == cand.end())
+        throw ArgError("value " + std::to_string(value) + " is not a candidate of this knob for this configuration");
+    if (knob == 0) {
+        c.physics_form = value;
+    } else if (value != c.solve_nc) {
+        c.solve_nc = value;
+        if (c.d_solve_tiles) cudaFree(c.d_solve_tiles);
+        c.d_solve_tiles = nullptr;
+        if (c.d_inv_sol_tiles) cudaFree(c.d_inv_sol_tiles);
+        c.d_inv_sol_tiles = nullptr;
+        rebuild_solve_tiles(c);
+    }
+    drop_graph(c);
+}
+
+// Times every candidate of each knob on the context's own buffers (the stage's
+// kernel alone, nreps launches after one untimed launch) and keeps the fastest.
+static void autotune(Ctx& c, int nreps, double* ms_out) {
+    const size_t plane = (size_t)c.d.nlm * 2 * c.d.nr;
+    if (!c.have_state) {   // give the stages finite inputs
+        RA_CUDA(cudaMemsetAsync(c.d_p2a, 0, (size_t)c.d.L * c.d.nth * NP2A * 2 * c.d.nr * sizeof(double), c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_rhs_wpt, 0, 3 * plane * sizeof(double), c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_rhs_z, 0, plane * sizeof(double), c.stream));
+    }
+    // the solve overwrites the state: park it in the grid buffer (rebuilt by every step)
+    RA_CUDA(cudaMemcpyAsync(c.d_g, c.d_sol_wpt, 3 * plane * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_g + 3 * plane, c.d_sol_z, plane * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    cudaEvent_t e0, e1;
+    RA_CUDA(cudaEventCreate(&e0));
+    RA_CUDA(cudaEventCreate(&e1));
+    for (int knob = 0; knob < 2; ++knob) {
+        double best = 1e300;
+        int best_v = -1;
+        for (int v : knob_candidates(c, knob)) {
+            set_knob(c, knob, v);
+            auto run = [&] {
+                if (knob == 0) {
+                    RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
+                    launch_physics(c);
+                } else {
+                    if (c.cfg.precision == RA_PREC_MIXED) return;   // the mixed form solves by split products
+                    launch_solve(c);
+                }
+            };
+            run();
+            RA_CUDA(cudaEventRecord(e0, c.stream));
+            for (int i = 0; i < nreps; ++i) run();
+            RA_CUDA(cudaEventRecord(e1, c.stream));
+            RA_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            RA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double per = ms / std::max(1, nreps);
+            if (per < best) {
+                best = per;
+                best_v = v;
+            }
+        }
+        set_knob(c, knob, best_v);
+        if (ms_out) ms_out[knob] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RA_CUDA(cudaMemcpyAsync(c.d_sol_wpt, c.d_g, 3 * plane * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    RA_CUDA(cudaMemcpyAsync(c.d_sol_z, c.d_g + 3 * plane, plane * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+    RA_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 }  // namespace ra
 
 // ---------------------------------------------------------------------------
@@ -770,6 +880,7 @@ int ra_default_config(ra_config* cfg) {
     cfg->precision = RA_PREC_FP64;
     cfg->use_graph = 1;
     cfg->device = 0;
+    cfg->autotune = 0;
     return RA_OK;
 }
 
@@ -1017,6 +1128,28 @@ int ra_step_timed(ra_ctx* ctx, int nsteps, double* total_ms) {
     });
     if (rc == RA_ERR_ARG && !ctx->c.have_state) return RA_ERR_STATE;
     return rc;
+}
+
+int ra_get_choice(const ra_ctx* ctx, const char* knob, int* value) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    const int k = knob_index(knob);
+    if (k < 0 || !value) return RA_ERR_ARG;
+    *value = k == 0 ? ctx->c.physics_form : ctx->c.solve_nc;
+    return RA_OK;
+}
+
+int ra_set_choice(ra_ctx* ctx, const char* knob, int value) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        const int k = knob_index(knob);
+        if (k < 0) throw ArgError(std::string("unknown knob ") + (knob ? knob : "(null)"));
+        set_knob(ctx->c, k, value);
+    });
+}
+
+int ra_autotune(ra_ctx* ctx, int nreps, double* ms_out) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] { autotune(ctx->c, std::max(1, nreps), ms_out); });
 }
 
 int ra_step(ra_ctx* ctx, int nsteps, double* cfl) {

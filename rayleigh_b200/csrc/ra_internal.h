@@ -129,6 +129,8 @@ struct Ctx {
     double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot
     double *d_twid = nullptr;                         // [nth] complex exp(2 pi i k / nphi)
     double *d_twp = nullptr;                          // per-pass twiddles of the in-place phi FFT
+    bool physics3_ok = false;                         // n_theta has a physical-space kernel with the last pass in registers
+    int physics_form = 0;                             // 0/2: that kernel (2 / 1 CTAs per SM), 1: all passes in shared memory
     double *d_Awpt = nullptr, *d_Az = nullptr;        // LU factors in block-substitution form [L][3nr][3nr], [L][nr][nr]
     int *d_perm_wpt = nullptr, *d_perm_z = nullptr;   // row permutations of the factors [L][3nr], [L][nr]
     int *d_skip_z = nullptr;                          // [L]: 1 where Z is not solved for (l = 0)
@@ -209,11 +211,13 @@ struct ProbeSet {
 void launch_point_probes(Ctx& c, const SliceSpec& S, const ProbeSet& Q, double* out);
 // tables the launches read, built at set-up (never inside a graph capture)
 void physics_prepare(Ctx& c);
+bool physics_form1_supported(int n_theta);
 void lt_forward_prepare(Ctx& c);
 void solve_prepare(Ctx& c);
 void launch_rlm_b(Ctx& c, double new_ab);
 void launch_solve(Ctx& c);
-void factor_matrices(Ctx& c);   // LU of the loaded per-l matrices (+ explicit inverses in the mixed form)
+void factor_matrices(Ctx& c);
+void rebuild_solve_tiles(Ctx& c);   // LU of the loaded per-l matrices (+ explicit inverses in the mixed form)
 // k_solve.cu
 int lu_nc_for(int n);
 void lu_workspace(LuWork& w, int n, int count);

@@ -93,13 +93,15 @@ def test_chebyshev_operators():
 SMALL = dict(n_r=24, l_max=15, dt=2e-4, rayleigh=1e5, ekman=1e-3)
 
 
-def _stage_compare(cfg, steps_before=0, amp=1e-2):
+def _stage_compare(cfg, steps_before=0, amp=1e-2, choices=None):
     """Run one step stage by stage on both sides; return {stage: rel err}."""
     oc = _ocfg(cfg)
     o = O.Oracle(oc)
     wpt, z = O.seeded_state(oc, amp=amp, lmax_pert=min(10, oc.l_max))
     o.init_state(wpt, z)
     g = _ctx(dict(cfg, use_graph=False))
+    for knob, v in (choices or {}).items():
+        g.set_choice(knob, v)
     g.put_state(wpt, z, None, iteration=1)
     for _ in range(steps_before):
         o.step()
@@ -163,14 +165,57 @@ def test_step_stages_ab2_step():
     assert not bad, errs
 
 
-def test_step_stages_768_point_phi_transform():
+@pytest.mark.parametrize("physics", [0, 1, 2])
+def test_step_stages_768_point_phi_transform(physics):
     """l_max = 511, n_theta = 768 (the l_max = 511 grid's angular size, few
-    radii): the largest phi transform, and the only size here at which each
-    physical-space thread owns two points of a row."""
-    errs = _stage_compare(dict(n_r=8, l_max=511, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1)
+    radii): the largest phi transform, through each physical-space kernel
+    (0, 2: the three-pass 16 x 16 x 3 FFT at two or one CTA per SM; 1: the
+    four-pass one, where each thread owns two points of a row)."""
+    errs = _stage_compare(dict(n_r=8, l_max=511, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1,
+                          choices={"physics": physics})
+    print(physics, {k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if v > TOL}
+    assert not bad, errs
+
+
+def test_step_stages_1536_point_phi_transform():
+    """l_max = 1023, n_theta = 1536, n_phi = 3072 (the transform sweep's largest
+    size, few radii): the physical-space kernel with 512 threads per row."""
+    errs = _stage_compare(dict(n_r=8, l_max=1023, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1)
     print({k: f"{v:.2e}" for k, v in errs.items()})
     bad = {k: v for k, v in errs.items() if v > TOL}
     assert not bad, errs
+
+
+@pytest.mark.parametrize("physics", [0, 1])
+def test_step_stages_384_point_phi_transform(physics):
+    """l_max = 255, n_theta = 384: the three-pass kernel's 16 x 8 x 3 plan."""
+    errs = _stage_compare(dict(n_r=8, l_max=255, dt=1e-6, rayleigh=1e5, ekman=1e-3), steps_before=1,
+                          choices={"physics": physics})
+    print(physics, {k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if v > TOL}
+    assert not bad, errs
+
+
+def test_autotune_choices():
+    """The set-up autotuner picks a candidate of each knob; every candidate of
+    the solve's column block gives the same state to rounding."""
+    cfg = dict(n_r=96, l_max=63, dt=1e-5, ekman=1e-4, rayleigh=1e6)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-3, lmax_pert=10)
+    g = _ctx(dict(cfg, autotune=True))
+    res = g.autotune(2)
+    assert res["physics"][0] in (0, 1, 2) and res["solve_nc"][0] in (16, 32), res
+    states = []
+    for nc in (16, 32):
+        g.set_choice("solve_nc", nc)
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(4)
+        states.append(g.get_state())
+    for a, b in zip(states[0], states[1]):
+        assert rel_err(a, b) < 1e-14
+    with pytest.raises(Exception):
+        g.set_choice("physics", 7)
 
 
 def _fields(wpt, z, nr):

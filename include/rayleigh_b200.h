@@ -58,7 +58,8 @@ typedef struct ra_config {
     double magnetic_prandtl;
     double gravity_power;
     int    rotation;         /* Coriolis terms on/off */
-    int    magnetism;        /* must be 0: the hydrodynamic equation set */
+    int    magnetism;        /* 1: the dynamo equation set (C, A potentials, Lorentz force, EMF;
+                                insulating boundaries); needs n_theta <= 768 */
     int    no_slip_top, no_slip_bottom;    /* else stress-free */
     int    fix_tvar_top, fix_tvar_bottom;  /* else fixed dT/dr */
     double t_top, t_bottom, dtdr_top, dtdr_bottom;
@@ -98,6 +99,9 @@ int ra_set_dt(ra_ctx* ctx, double dt);
  * one system:
  *   sys 0: the linked W-P-T system, lhs(3 n_r, 3 n_r, l_max + 1)
  *   sys 1: Z,                       lhs(  n_r,   n_r, l_max + 1)
+ *   sys 2: C, sys 3: A (magnetism), lhs(  n_r,   n_r, l_max + 1); their coefs are
+ *          coefs(n_r, 2, l_max + 1) = (C,C,0) (C,C,2) and coefs(n_r, 3, l_max + 1) =
+ *          (A,A,0) (A,A,1) (A,A,2); l = 0 has no magnetic equation (its matrix is ignored)
  * each lhs(:, :, l) = equation_set(l, eq)%lhs in Fortran (column-major) order,
  * rows/columns ordered W, P, T blocks of n_r.  coefs (may be NULL) replaces
  * the explicit Post_Solve coefficients of the system's equations
@@ -114,7 +118,7 @@ int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coef
  * Either output may be NULL. */
 int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs, double* coefs);
 /* LU_Decompose_Matrices (Linear_Solve.F90:459-480) of the loaded matrices of
- * both systems, which belong to time step dt (the AB2 factors use it).
+ * all systems (both, or the four with magnetism), which belong to time step dt (the AB2 factors use it).
  * RA_ERR_SINGULAR names the system and l of a negligible pivot. */
 int ra_factor(ra_ctx* ctx, double dt);
 /* bc_values(2 [top, bottom], 2 [re, im], n_lm, 4 [W, P, T, Z]) of
@@ -131,6 +135,15 @@ int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values);
  * iteration: the reference's iteration counter (1 = Euler first step). */
 int ra_put_state(ra_ctx* ctx, const double* wpt, const double* z, const double* ab, int iteration);
 int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab);
+/* The magnetic part of the state (contexts created with magnetism = 1), in the
+ * same layout: the equation-set RHS of the C (poloidal) and A (toroidal)
+ * equations (ceq, aeq; Fields.F90:86-88, Linear_Solve.F90:355-386)
+ *   c [n_r][2][n_lm], a [n_r][2][n_lm]  Chebyshev coefficients
+ *   ab[n_r][2][n_lm][2]                 their Adams-Bashforth terms (C, A); may be NULL (zero)
+ * Independent of ra_put_state (either order); a magnetic context whose
+ * magnetic state was never put starts from C = A = 0. */
+int ra_put_magnetic_state(ra_ctx* ctx, const double* c, const double* a, const double* ab);
+int ra_get_magnetic_state(ra_ctx* ctx, double* c, double* a, double* ab);
 /* The same for one rank's slice of the modes (the (l, m) pairs a rank of the
  * reference holds, Load_Balance.F90:357-368): l_of[i], m_of[i] name mode i of
  * the slice, whose arrays are the rank's own equation-set layout
@@ -372,6 +385,14 @@ long ra_launch_count(const ra_ctx* ctx);
 #define RA_BUF_RHS_Z   8   /* [n_lm][2][n_r]      */
 #define RA_BUF_PTAB    9   /* [row][n_theta/2]    P_l^m (times 1/2 for m > 0) */
 #define RA_BUF_IPTAB  10   /* [row][n_theta/2]    weighted P_l^m with the FFT normalisation */
+/* with magnetism: RA_BUF_GRID adds C, dC, d2C, A, dA, d2A ([18]); RA_BUF_S2A11 and RA_BUF_P2A add
+ * B_r, (curl B)_r, (curl B)_theta, (curl B)_phi, B_theta, B_phi ([17], the last four times
+ * r sin(theta)); RA_BUF_P2B and RA_BUF_S2B add EMF_theta, EMF_r, EMF_phi ([7]; after rlm_spaceb
+ * the C right-hand side, EMF_r and the term whose radial derivative completes the A one);
+ * RA_BUF_AB holds [6] fields (W P T Z C A) */
+#define RA_BUF_S2AM   11   /* [row][5][n_r][2]    magnetism: C, A, dC, dA, d2C after Post_Solve */
+#define RA_BUF_RHS_C  12   /* [n_lm][2][n_r]      magnetism */
+#define RA_BUF_RHS_A  13   /* [n_lm][2][n_r]      magnetism */
 int ra_debug_buffer(ra_ctx* ctx, int which, double* out, long n, long* n_out);
 
 #ifdef __cplusplus

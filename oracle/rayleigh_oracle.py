@@ -29,8 +29,8 @@ LD = np.longdouble
 PI_LD = LD("3.14159265358979323846264338327950288")
 
 # Field indices of the forward-leg buffers, 0-based restatement of
-# Fields.F90:232-335 (hydro, no scalars).
-WVAR, PVAR, TVAR, ZVAR = 0, 1, 2, 3
+# Fields.F90:232-335 (no scalars); C and A follow Z when magnetism is on (:240-243).
+WVAR, PVAR, TVAR, ZVAR, CVAR, AVAR = 0, 1, 2, 3, 4, 5
 # equation ids (Fields.F90:86-88), 0-based
 WEQ, PEQ, TEQ, ZEQ, CEQ, AEQ = 0, 1, 2, 3, 4, 5
 
@@ -51,6 +51,7 @@ class Config:
     gravity_power: float = 1.0
     rotation: bool = True
     magnetism: bool = False
+    lorentz_forces: bool = True      # Controls.F90:63 (on whenever magnetism is on)
     momentum_advection: bool = True
     no_slip_top: bool = True
     no_slip_bottom: bool = True
@@ -417,15 +418,18 @@ def lm_pairs(l_max):
 
 
 class Oracle:
-    """Boussinesq (reference_type 1) rotating convection, hydro, single Chebyshev domain."""
+    """Boussinesq (reference_type 1) rotating convection, single Chebyshev domain;
+    with ``cfg.magnetism`` the dynamo equation set (poloidal C and toroidal A
+    potentials of B, Lorentz force, induction by the EMF)."""
 
-    NF1A = 8     # W P T Z W' T' Z' W''  (Fields.F90:244-252, aliases :317-335)
-    NF2A = 12
-    NFB = 4
+    NF1A = 8     # W P T Z W' T' Z' W''  (Fields.F90:244-252, aliases :317-335); + C A C' A' C'' with magnetism
+    NF2A = 12    # + Br, (curl B)_r, (curl B)_theta, (curl B)_phi, B_theta, B_phi with magnetism
+    NFB = 4      # + EMF_theta (C slot), EMF_r (A slot), EMF_phi with magnetism (Fields.F90:365-368)
 
     def __init__(self, cfg: Config, horizontal: Horizontal | None = None):
-        if cfg.magnetism:
-            raise NotImplementedError("oracle covers the hydrodynamic equation set")
+        self.mag = bool(cfg.magnetism)
+        if self.mag:
+            self.NF1A, self.NF2A, self.NFB = 13, 18, 7
         self.cfg = cfg
         self.h = horizontal if horizontal is not None else Horizontal(cfg.l_max, cfg.n_theta)
         rmax = cfg.shell_depth / (1.0 - cfg.aspect_ratio)
@@ -450,6 +454,9 @@ class Oracle:
         self.coriolis = 2.0 / cfg.ekman
         self.nu = np.ones(nr)
         self.kappa = np.full(nr, 1.0 / cfg.prandtl)
+        # Constant_Reference, magnetism (PDE_Coefficients.F90:418-427): Lorentz_Coeff, eta
+        self.lorentz = 1.0 / (cfg.magnetic_prandtl * cfg.ekman) if self.mag else 0.0
+        self.eta = np.full(nr, 1.0 / cfg.magnetic_prandtl) if self.mag else np.zeros(nr)
         r_out, r_in = r[0], r[-1]
         pref = r_out * r_in / (r_in - r_out)
         self.s_conductive = pref * (1.0 / r_out - 1.0 / r)
@@ -479,11 +486,14 @@ class Oracle:
         self.lu_z = []
         self.mat_wpt = []
         self.mat_z = []
+        self.mat_c, self.mat_a, self.lu_c, self.lu_a = [], [], [], []
         over_r2 = 1.0 / r ** 2
         for l in range(cfg.l_max + 1):
             coefs = {}
             A = np.zeros((3 * nr, 3 * nr))
             Z = np.zeros((nr, nr))
+            Cm = np.zeros((nr, nr))
+            Am = np.zeros((nr, nr))
             blk = {WEQ: 0, PEQ: nr, TEQ: 2 * nr, WVAR: 0, PVAR: nr, TVAR: 2 * nr}
 
             def add(eq, var, d, amp, static=False, mat=None, rb=None, cb=None):
@@ -531,6 +541,17 @@ class Oracle:
                 add(ZEQ, ZVAR, 2, self.nu, mat=Z, rb=0, cb=0)
                 add(ZEQ, ZVAR, 0, np.zeros(nr), mat=Z, rb=0, cb=0)
                 add(ZEQ, ZVAR, 1, np.zeros(nr), mat=Z, rb=0, cb=0)
+                if self.mag:
+                    # Btor (A) and Bpol (C) equations (Sphere_Linear_Terms.F90:473-499); no eta variation
+                    blk[AEQ] = blk[AVAR] = 0
+                    blk[CEQ] = blk[CVAR] = 0
+                    add(AEQ, AVAR, 0, ones, static=True, mat=Am)
+                    add(AEQ, AVAR, 0, H * self.eta, mat=Am)
+                    add(AEQ, AVAR, 2, self.eta, mat=Am)
+                    add(AEQ, AVAR, 1, np.zeros(nr), mat=Am)    # A_Diffusion_Coefs_1
+                    add(CEQ, CVAR, 0, ones, static=True, mat=Cm)
+                    add(CEQ, CVAR, 0, H * self.eta, mat=Cm)
+                    add(CEQ, CVAR, 2, self.eta, mat=Cm)
             # Set_Boundary_Conditions (Sphere_Linear_Terms.F90:539-1100)
             def bc(mat, row, col0, d, amp):
                 # Load_Single_Row_Cheby (Linear_Solve.F90:1483-1522): dealiased columns only
@@ -584,12 +605,29 @@ class Oracle:
                     bc(A, nr + bot, 0, 1, samp)
                     bc(Z, bot, 0, 1, 1.0)
                     bc(Z, bot, 0, 0, samp)
+                if self.mag:
+                    # insulating boundaries (:1041-1077): A = 0; C matched to a potential field,
+                    # dC/dr + l C / r = 0 at the top, dC/dr - (l + 1) C / r = 0 at the bottom
+                    for mm in (Cm, Am):
+                        mm[top, :] = 0.0
+                        mm[bot, :] = 0.0
+                    bc(Am, top, 0, 0, 1.0)
+                    bc(Am, bot, 0, 0, 1.0)
+                    bc(Cm, top, 0, 1, 1.0)
+                    bc(Cm, top, 0, 0, l / r[top])
+                    bc(Cm, bot, 0, 1, 1.0)
+                    bc(Cm, bot, 0, 0, -(l + 1) / r[bot])
             self.coefs.append(coefs)
             self.mat_wpt.append(A)
             self.mat_z.append(Z)
             # LU_Decompose_full -> DGETRF (Linear_Solve.F90:1028-1036)
             self.lu_wpt.append(sla.lu_factor(A, check_finite=False))
             self.lu_z.append(sla.lu_factor(Z, check_finite=False) if l > 0 else None)
+            if self.mag:
+                self.mat_c.append(Cm)
+                self.mat_a.append(Am)
+                self.lu_c.append(sla.lu_factor(Cm, check_finite=False) if l > 0 else None)
+                self.lu_a.append(sla.lu_factor(Am, check_finite=False) if l > 0 else None)
         # bc_values (BoundaryConditions.F90:364-402): only l=0 T rows carry values
         self.bc_t = (cfg.t_top * math.sqrt(4 * math.pi) if cfg.fix_tvar_top else cfg.dtdr_top * math.sqrt(4 * math.pi),
                      cfg.t_bottom * math.sqrt(4 * math.pi) if cfg.fix_tvar_bottom else cfg.dtdr_bottom * math.sqrt(4 * math.pi))
@@ -600,21 +638,30 @@ class Oracle:
         self._build_linear()
 
     # ----- state -----
-    def init_state(self, wpt_coeffs, z_coeffs, ab=None):
-        """State in the equation-set RHS layout: wpt[lm, ri, 3nr], z[lm, ri, nr] (Chebyshev coefficients)."""
+    def init_state(self, wpt_coeffs, z_coeffs, ab=None, c_coeffs=None, a_coeffs=None):
+        """State in the equation-set RHS layout: wpt[lm, ri, 3nr], z[lm, ri, nr] (Chebyshev coefficients);
+        with magnetism also c[lm, ri, nr], a[lm, ri, nr] (zero when None) and ab[6] (W P T Z C A)."""
         nr = self.cfg.n_r
         self.rhs_wpt = np.array(wpt_coeffs, dtype=np.float64).reshape(self.n_lm, 2, 3 * nr)
         self.rhs_z = np.array(z_coeffs, dtype=np.float64).reshape(self.n_lm, 2, nr)
-        self.ab = np.zeros((self.NFB, self.n_lm, 2, nr)) if ab is None else np.array(ab, dtype=np.float64)
+        nab = 6 if self.mag else 4
+        self.ab = np.zeros((nab, self.n_lm, 2, nr)) if ab is None else np.array(ab, dtype=np.float64)
+        if self.mag:
+            z0 = np.zeros((self.n_lm, 2, nr))
+            self.rhs_c = z0.copy() if c_coeffs is None else np.array(c_coeffs, dtype=np.float64).reshape(z0.shape)
+            self.rhs_a = z0.copy() if a_coeffs is None else np.array(a_coeffs, dtype=np.float64).reshape(z0.shape)
 
     def get_all_rhs(self):
-        """Get_All_RHS (Linear_Solve.F90:691-711) -> p1 [f][lm][ri][r] for W P T Z."""
+        """Get_All_RHS (Linear_Solve.F90:691-711) -> p1 [f][lm][ri][r] for W P T Z (C A)."""
         nr = self.cfg.n_r
-        p = np.empty((4, self.n_lm, 2, nr))
+        p = np.empty((6 if self.mag else 4, self.n_lm, 2, nr))
         p[WVAR] = self.rhs_wpt[:, :, 0:nr]
         p[PVAR] = self.rhs_wpt[:, :, nr:2 * nr]
         p[TVAR] = self.rhs_wpt[:, :, 2 * nr:3 * nr]
         p[ZVAR] = self.rhs_z
+        if self.mag:
+            p[CVAR] = self.rhs_c
+            p[AVAR] = self.rhs_a
         return p
 
     def _coef(self, l, eq, var, d):
@@ -649,13 +696,21 @@ class Oracle:
         dt_ = cg.deriv(T, 1)
         d2z = cg.deriv(Z, 2)
         dz = cg.deriv(Z, 1)
-        ctemp = cg.from_spectral(cg.dealias(np.stack([d3w, dp, d2t, d2z])))   # :277-283
+        ct = [d3w, dp, d2t, d2z]
+        gl = [W, P, T, Z, dw, dt_, dz, d2w]
+        if self.mag:                                           # :268-274
+            C, A = c[CVAR], c[AVAR]
+            ct.append(cg.deriv(A, 2))
+            gl += [C, A, cg.deriv(C, 1), cg.deriv(A, 1), cg.deriv(C, 2)]
+        ctemp = cg.from_spectral(cg.dealias(np.stack(ct)))    # :277-283
         self._add_derivative(p1b, PEQ, WVAR, 3, ctemp[0])
         self._add_derivative(p1b, WEQ, PVAR, 1, ctemp[1])
         self._add_derivative(p1b, TEQ, TVAR, 2, ctemp[2])
         self._add_derivative(p1b, ZEQ, ZVAR, 2, ctemp[3])
-        g = cg.from_spectral(cg.dealias(np.stack([W, P, T, Z, dw, dt_, dz, d2w])))  # :301-309
-        Wg, Pg, Tg, Zg, dWg, dTg, dZg, d2Wg = g
+        if self.mag:
+            self._add_derivative(p1b, AEQ, AVAR, 2, ctemp[4])  # :295-297
+        g = cg.from_spectral(cg.dealias(np.stack(gl)))         # :301-309
+        Wg, Pg, Tg, Zg, dWg, dTg, dZg, d2Wg = g[:8]
         self.last_pressure_grids = np.stack([Pg, ctemp[1]])   # P and dP/dr, for pressure_fields
         self._add_derivative(p1b, PEQ, WVAR, 0, Wg)
         self._add_derivative(p1b, PEQ, WVAR, 1, dWg)
@@ -669,8 +724,14 @@ class Oracle:
         self._add_derivative(p1b, WEQ, TVAR, 0, Tg)
         self._add_derivative(p1b, ZEQ, ZVAR, 0, Zg)
         self._add_derivative(p1b, ZEQ, ZVAR, 1, dZg)
+        if self.mag:                                            # :370-384
+            Cg, Ag, dCg, dAg, d2Cg = g[8:13]
+            self._add_derivative(p1b, AEQ, AVAR, 0, Ag)
+            self._add_derivative(p1b, AEQ, AVAR, 1, dAg)
+            self._add_derivative(p1b, CEQ, CVAR, 2, d2Cg)
+            self._add_derivative(p1b, CEQ, CVAR, 0, Cg)
         self._set_all_rhs(p1b)                                  # :391
-        return g                                                # p1a grid fields (8)
+        return g                                                # p1a grid fields (8; 13 with magnetism)
 
     def _set_all_rhs(self, p1b):
         nr = self.cfg.n_r
@@ -678,6 +739,9 @@ class Oracle:
         self.rhs_wpt[:, :, nr:2 * nr] = p1b[PEQ]
         self.rhs_wpt[:, :, 2 * nr:3 * nr] = p1b[TEQ]
         self.rhs_z[:] = p1b[ZEQ]
+        if self.mag:
+            self.rhs_c[:] = p1b[CEQ]
+            self.rhs_a[:] = p1b[AEQ]
 
     def transpose_1a2a(self, p1):
         """Transpose_1a2a (Spherical_Buffer.F90:849-949): p1[f][lm][ri][r] -> s2[m](f,2,r,l)."""
@@ -715,7 +779,7 @@ class Oracle:
             llp1 = ls * (ls + 1)
             W, P, T, Z = a[0], a[1], a[2], a[3]
             dW, dT, dZ, d2W = a[4], a[5], a[6], a[7]
-            b = np.zeros((12,) + W.shape)
+            b = np.zeros((self.NF2A,) + W.shape)
             vr = llp1 * W * over_rhorsq                               # Velocity_Components :246-248
             vt = (h.d_by_dtheta(dW, m) + h.d_by_dphi(Z[None], m)[0]) * over_rhor
             vp = (h.d_by_dphi(dW[None], m)[0] - h.d_by_dtheta(Z, m)) * over_rhor
@@ -741,6 +805,19 @@ class Oracle:
             b[9] = vp
             b[10] = dvtdr
             b[11] = dvpdr
+            if self.mag:
+                # Compute_BandCurlB (Sphere_Hybrid_Space.F90:357-435), each times r sin(theta)
+                # except B_r and (curl B)_r
+                C, A, dC, dA, d2C = a[8], a[9], a[10], a[11], a[12]
+                over_rsq = (1.0 / r ** 2)[:, None]
+                br = llp1 * C * over_rsq
+                x = d2C - br
+                b[12] = br
+                b[13] = llp1 * A * over_rsq                           # (curl B)_r
+                b[14] = h.d_by_dtheta(dA, m) - h.d_by_dphi(x[None], m)[0]   # (curl B)_theta
+                b[15] = h.d_by_dphi(dA[None], m)[0] + h.d_by_dtheta(x, m)   # (curl B)_phi
+                b[16] = h.d_by_dphi(A[None], m)[0] + h.d_by_dtheta(dC, m)   # B_theta
+                b[17] = h.d_by_dphi(dC[None], m)[0] - h.d_by_dtheta(A, m)   # B_phi
             b[..., -1] = 0.0                                          # :100-102
             out.append(b)
         return out
@@ -764,6 +841,8 @@ class Oracle:
             return o
         f = {}
         names = ["vr", "p", "t", "omr", "dvrdr", "dtdr", "dvrdt", "dtdt", "vt", "vp", "dvtdr", "dvpdr"]
+        if self.mag:
+            names += ["br", "curlbr", "curlbt", "curlbp", "bt", "bp"]
         for i, n in enumerate(names):
             f[n] = p3[i]
         f["dvrdp"] = dphi(f["vr"])
@@ -782,6 +861,10 @@ class Oracle:
         cos = h.costheta[th][:, None, None]
         for k in ("vt", "vp", "dvtdr", "dvpdr", "dtdt", "dvrdt", "dvpdp", "dvtdp"):
             f[k] = f[k] * csc                                          # sintheta_div (:119-126)
+        if self.mag:
+            orad = (1.0 / self.radius)[None, :, None]
+            for k in ("curlbt", "curlbp", "bt", "bp"):
+                f[k] = f[k] * csc * orad                               # rsintheta_div (:142-147)
         # the velocity and temperature Benchmark_Checkup reads at this point of the step (:158-159)
         self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
         self.last_temperature = f["t"]
@@ -796,9 +879,16 @@ class Oracle:
         llp1max = L * (L + 1.0)
         ovht2 = (np.max(f["vt"] ** 2 + f["vp"] ** 2, axis=(0, 2)) / self.radius ** 2 * llp1max)
         ovrt2 = np.max(f["vr"] ** 2, axis=(0, 2)) / self.delta_r ** 2
-        self.last_cfl = float(max(ovht2.max(), ovrt2.max(), 0.0))
+        cfl = max(ovht2.max(), ovrt2.max(), 0.0)
+        if self.mag:   # the Alfven speed (:798-806)
+            ovht2 = (np.max(f["bt"] ** 2 + f["bp"] ** 2, axis=(0, 2)) / self.radius ** 2 * llp1max
+                     / self.density * self.lorentz)
+            ovrt2 = np.max(f["br"] ** 2, axis=(0, 2)) / self.delta_r ** 2 / self.density * self.lorentz
+            cfl = max(cfl, ovht2.max(), ovrt2.max())
+        self.last_cfl = float(cfl)
         vr, vt, vp = f["vr"], f["vt"], f["vp"]
-        out = np.zeros((4,) + vr.shape)
+        out = np.zeros((self.NFB,) + vr.shape)
+        lorentz = self.mag and cfg.lorentz_forces
         # Temperature_Advection (:303-318)
         out[TVAR] = -vr * f["dtdr"] - one_over_r * (f["dtdt"] * vt + vp * f["dtdp"] * csc)
         # Momentum_Advection_Radial (:466-529)
@@ -806,19 +896,31 @@ class Oracle:
         if cfg.rotation:
             w = w + self.coriolis * sin * vp * r2
         out[WVAR] = w * rho
+        if lorentz:   # r^2 [J x B]_r (:512-519)
+            out[WVAR] = out[WVAR] + r2 * self.lorentz * (f["curlbt"] * f["bp"] - f["curlbp"] * f["bt"])
         # Momentum_Advection_Theta (:583-645)
         pth = f["dvrdr"] + (f["dvpdp"] * csc + vt * cot + vr) * one_over_r + vr * dlnrho
         pth = -pth * vt + vr * f["dvtdr"] + vp * (f["dvtdp"] * csc - vp * cot) * one_over_r
         if cfg.rotation:
             pth = pth - self.coriolis * cos * vp
         pth = pth * rho
+        if lorentz:   # -[J x B]_theta (:635-641)
+            pth = pth - self.lorentz * (f["curlbp"] * f["br"] - f["curlbr"] * f["bp"])
         out[PVAR] = pth * r * csc
         # Momentum_Advection_Phi (:648-700)
         z = vt * (f["omr"] + f["dvtdp"] * csc * one_over_r) + vr * f["dvpdr"] + vp * (f["dvpdp"] * csc + vr) * one_over_r
         if cfg.rotation:
             z = z + self.coriolis * cos * vt + self.coriolis * sin * vr
         z = z * rho
+        if lorentz:   # -[J x B]_phi (:712-718)
+            z = z - self.lorentz * (f["curlbr"] * f["bt"] - f["curlbt"] * f["br"])
         out[ZVAR] = z * r * csc
+        if self.mag:
+            # Compute_EMF (:534-581): u x B; the theta and phi parts times r / sin(theta)
+            br, bt, bp = f["br"], f["bt"], f["bp"]
+            out[4] = (-vr * bp + vp * br) * csc * r      # emftheta (C slot)
+            out[5] = vt * bp - vp * bt                   # emfr (A slot)
+            out[6] = (vr * bt - vt * br) * csc * r       # emfphi
         pad = np.zeros(out.shape[:-1] + (nphi + 2,))
         pad[..., :nphi] = out
         return fft_r2c(pad, nphi)
@@ -863,6 +965,17 @@ class Oracle:
                 a[PVAR][..., 0] = 0.0
                 a[WVAR][..., 0] = 0.0
                 a[ZVAR][..., 0] = 0.0
+            if self.mag:
+                # Adjust_Emf (:557-602): C RHS from the radial curl of the EMF in the C slot;
+                # the A slot keeps EMF_r; slot 7 the term Finalize_EMF differentiates in r
+                ft1 = h.d_by_sdtheta(a[6], m)
+                ft2 = h.d_by_dphi(a[4][None], m)[0]
+                ft3 = a[4].copy()
+                a[4] = (ft1 - ft2) * ollp1
+                ft2 = h.d_by_dphi(a[6][None], m)[0]
+                a[6] = ft3
+                ft1 = h.d_by_sdtheta(a[6], m)
+                a[6] = (ft2 + ft1) * ollp1
             a[..., -1] = 0.0
             out.append(a)
         return out
@@ -870,12 +983,25 @@ class Oracle:
     def advance_time(self, p1b_new, ls=None):
         """AdvanceTime (Sphere_Spectral_Space.F90:415-435): add AB term, BCs, solve (``ls``: subset of l)."""
         nr = self.cfg.n_r
+        if self.mag:
+            # Finalize_EMF (:436-488), Chebyshev branch: A RHS += d/dr of slot 7 (grid ->
+            # coefficients -> derivative -> dealias -> grid)
+            cg = self.cg
+            dx = cg.from_spectral(cg.dealias(cg.deriv(cg.to_spectral(p1b_new[6]), 1)))
+            p1b_new = p1b_new[:6].copy()
+            p1b_new[AEQ] = p1b_new[AEQ] + dx
         self.ab = p1b_new
         nab = self.new_ab
         self.rhs_wpt[:, :, 0:nr] += nab * p1b_new[WEQ]
         self.rhs_wpt[:, :, nr:2 * nr] += nab * p1b_new[PEQ]
         self.rhs_wpt[:, :, 2 * nr:3 * nr] += nab * p1b_new[TEQ]
         self.rhs_z += nab * p1b_new[ZEQ]
+        if self.mag:
+            self.rhs_c += nab * p1b_new[CEQ]
+            self.rhs_a += nab * p1b_new[AEQ]
+            for arr in (self.rhs_c, self.rhs_a):     # the magnetic boundary values are zero
+                arr[:, :, 0] = 0.0
+                arr[:, :, nr - 1] = 0.0
         # Apply_Boundary_Mask (Linear_Solve.F90:401-418)
         for b in (0, nr, 2 * nr):
             self.rhs_wpt[:, :, b] = 0.0
@@ -902,6 +1028,10 @@ class Oracle:
                 bz = self.rhs_z[s:e].reshape(-1, nr).T
                 xz = sla.lu_solve(self.lu_z[l], bz, check_finite=False)
                 self.rhs_z[s:e] = xz.T.reshape(e - s, 2, nr)
+                if self.mag:
+                    for arr, lu in ((self.rhs_c, self.lu_c[l]), (self.rhs_a, self.lu_a[l])):
+                        x = sla.lu_solve(lu, arr[s:e].reshape(-1, nr).T, check_finite=False)
+                        arr[s:e] = x.T.reshape(e - s, 2, nr)
 
     # ----- the reference's accuracy benchmark (Christensen et al. 2001, case 0) -----
     def benchmark_init_hydro(self):
@@ -1111,3 +1241,29 @@ def seeded_state(cfg: Config, seed=0x5241594C, amp=1.0e-3, lmin=1, lmax_pert=20,
             tgrid[i, 1] += im * radial * shape
     wpt[:, :, 2 * nr:] = cg.to_spectral(tgrid)
     return wpt, z
+
+
+def seeded_magnetic_state(cfg: Config, seed=0x5241594D, amp=1.0e-3, lmin=1, lmax_pert=20, cheby=None):
+    """Seeded magnetic perturbation: (c[lm,2,nr], a[lm,2,nr]) Chebyshev coefficients of the
+    poloidal (C) and toroidal (A) potentials, complex Gaussian of amplitude amp*(l+1)^-2 on
+    l in [lmin, lmax_pert] (m = 0 imaginary parts zero) times the grid function
+    sin(pi (r - rmin) / (rmax - rmin)), which vanishes at both boundaries."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nr = cfg.n_r
+    rmax = cfg.shell_depth / (1.0 - cfg.aspect_ratio)
+    rmin = rmax * cfg.aspect_ratio
+    cg = cheby if cheby is not None else Chebyshev(nr, rmin, rmax)
+    r = cg.radius
+    ls, ms = lm_pairs(cfg.l_max)
+    radial = np.sin(np.pi * (r - rmin) / (rmax - rmin))
+    grids = np.zeros((2, len(ls), 2, nr))
+    for i in range(len(ls)):
+        l, m = ls[i], ms[i]
+        if lmin <= l <= lmax_pert:
+            for k in range(2):
+                re, im = rng.standard_normal(2) * amp * (l + 1.0) ** -2
+                if m == 0:
+                    im = 0.0
+                grids[k, i, 0] = re * radial
+                grids[k, i, 1] = im * radial
+    return cg.to_spectral(grids[0]), cg.to_spectral(grids[1])

@@ -156,6 +156,8 @@ def load_library(path: str | None = None):
         "ra_mixed_gemm_noalloc": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p,
                                    ctypes.c_int], ctypes.c_int),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+        "ra_put_magnetic_state": ([_VP, _VP, _VP, _VP], ctypes.c_int),
+        "ra_get_magnetic_state": ([_VP, _VP, _VP, _VP], ctypes.c_int),
         "ra_put_state_modes": ([_VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, ctypes.c_int], ctypes.c_int),
         "ra_get_state_modes": ([_VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP], ctypes.c_int),
         "ra_build_matrices": ([ctypes.POINTER(_Config), ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, _VP],
@@ -249,6 +251,22 @@ class Rayleigh:
         ab = np.empty((4, self.n_lm, 2, self.n_r))
         self._check(self.lib.ra_get_state(self.h, _ptr(wpt), _ptr(z), _ptr(ab)))
         return wpt, z, ab
+
+    # ---- magnetic state (magnetism = True): c[lm][ri][nr], a[lm][ri][nr], ab[2][lm][ri][nr] (C, A) ----
+    def put_magnetic_state(self, c, a, ab=None):
+        self._mc = _f64(c)
+        self._ma = _f64(a)
+        self._mab = None if ab is None else _f64(ab)
+        if self._mc.size != self.n_lm * 2 * self.n_r or self._ma.size != self.n_lm * 2 * self.n_r:
+            raise ValueError("magnetic state arrays have the wrong size")
+        self._check(self.lib.ra_put_magnetic_state(self.h, _ptr(self._mc), _ptr(self._ma), _ptr(self._mab)))
+
+    def get_magnetic_state(self):
+        c = np.empty((self.n_lm, 2, self.n_r))
+        a = np.empty((self.n_lm, 2, self.n_r))
+        ab = np.empty((2, self.n_lm, 2, self.n_r))
+        self._check(self.lib.ra_get_magnetic_state(self.h, _ptr(c), _ptr(a), _ptr(ab)))
+        return c, a, ab
 
     # ---- one rank's slice of the modes (the reference's per-rank equation-set layout) ----
     def put_state_modes(self, l_of, m_of, wpt, z, ab=None, iteration=1):
@@ -434,7 +452,7 @@ class Rayleigh:
         return out
 
     BUFFERS = {"grid": 0, "s2a": 1, "s2a11": 2, "p2a": 3, "p2b": 4, "s2b": 5, "ab": 6,
-               "rhs_wpt": 7, "rhs_z": 8, "ptab": 9, "iptab": 10}
+               "rhs_wpt": 7, "rhs_z": 8, "ptab": 9, "iptab": 10, "s2am": 11, "rhs_c": 12, "rhs_a": 13}
 
     def debug_buffer(self, name):
         """Copy of an internal device buffer (diagnostics for the stage-by-stage parity tests)."""
@@ -520,13 +538,14 @@ class Rayleigh:
 
 def build_matrices(cfg: Config, sys, l0, nl, coefs=False):
     """The library's own assembly of the per-l implicit matrices (host only): lhs[l][col][row]
-    (column-major per l) of system sys (0 = W-P-T, 1 = Z) for l = l0 .. l0+nl-1, and with
-    coefs=True also coefs[l][slot][r]."""
+    (column-major per l) of system sys (0 = W-P-T, 1 = Z, 2 = C, 3 = A with magnetism) for
+    l = l0 .. l0+nl-1, and with coefs=True also coefs[l][slot][r] (16 slots for systems 0
+    and 1, 2 for C, 3 for A)."""
     lib = load_library()
     c = cfg.to_c()
     n = cfg.n_r * (1 if sys else 3)
     lhs = np.empty((nl, n, n))
-    cf = np.empty((nl, 16, cfg.n_r)) if coefs else None
+    cf = np.empty((nl, {0: 16, 1: 16, 2: 2, 3: 3}[int(sys)], cfg.n_r)) if coefs else None
     rc = lib.ra_build_matrices(ctypes.byref(c), int(sys), int(l0), int(nl), _ptr(lhs), _ptr(cf))
     if rc != RA_OK:
         raise RayleighError(rc, "ra_build_matrices refused the configuration or range")

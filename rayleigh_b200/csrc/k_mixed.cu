@@ -57,7 +57,7 @@ static void run_split_once(Ctx& c, const std::vector<OzSplitJob>& jobs, int max_
 static void setup_lt_inverse(Ctx& c) {
     const Dims& d = c.d;
     const int L = d.L, nth2 = d.nth2;
-    const int ncol = NP2A * d.nr * 2;
+    const int ncol = c.nfa * d.nr * 2;
     const int nta = oz_tiles_of(ncol, OZ_HA), ntb = oz_tiles_of(nth2, OZ_HB);
     MixedPlan& p = c.mx_inv;
     std::vector<long> aoff(2 * L + 1, 0), boff(2 * L + 1, 0);
@@ -115,7 +115,7 @@ void launch_lt_inverse_mixed(Ctx& c) {
 static void setup_lt_forward(Ctx& c) {
     const Dims& d = c.d;
     const int L = d.L, nth2 = d.nth2;
-    const int ncol = NP2B * d.nr * 2;
+    const int ncol = c.nfb * d.nr * 2;
     const int nta = oz_tiles_of(ncol, OZ_HA), nks = oz_ksteps(nth2);
     const long ablk = (long)nta * nks * OZ_ABLK;
     MixedPlan& p = c.mx_fwd;

@@ -233,6 +233,8 @@ struct PhysParams {
     double coriolis;
     int rotation;
     double llmax;
+    int nfa, nfb;           // fields per radius of p2a / p2b
+    double lorentz;         // Lorentz_Coeff (magnetism)
 };
 
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
@@ -529,7 +531,35 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
         }
 }
 
-template <int NTH>
+// X_k of the real transform from the complex r2c output Z (in place, one (k, N-k) pair per
+// work item): X_k = e - i conj(w^k) d with e, d the half sums / differences of Z_k and
+// conj Z_{N-k}, each times hs(f); Im X_0 = 0; only k < L is kept.
+template <int N, class HS>
+__device__ __forceinline__ void r2c_finish(double2* a, int nf, int L, const double2* __restrict__ wr, int t,
+                                           const HS& hsf) {
+    constexpr int FS = fstride(N);
+    constexpr int NI = N / 2 + 1;
+    for (int g = t; g < nf * NI; g += ROW_THREADS) {
+        const int f = g / NI, k = g - f * NI;
+        const double2 zk = a[SW(f * FS + k)];
+        const double2 zn = a[SW(f * FS + (N - k) % N)];
+        const double2 wk = __ldg(wr + k);   // w^(N-k) = -conj(w^k)
+        const double hs = hsf(f);
+        auto xval = [&](double2 p, double2 q, double2 w, bool zero_im) {   // X from Z_kk = p, Z_{N-kk} = q
+            const double2 qn = cconj(q);
+            const double2 e = make_double2(hs * (p.x + qn.x), hs * (p.y + qn.y));
+            const double2 d = make_double2(hs * (p.x - qn.x), hs * (p.y - qn.y));
+            const double2 wd = cmul(cconj(w), d);
+            double2 X = make_double2(e.x + wd.y, e.y - wd.x);
+            if (zero_im) X.y = 0.0;
+            return X;
+        };
+        if (k < L) a[SW(f * FS + k)] = xval(zk, zn, wk, k == 0);
+        if (k != 0 && 2 * k != N && N - k < L) a[SW(f * FS + N - k)] = xval(zn, zk, make_double2(-wk.x, wk.y), false);
+    }
+}
+
+template <int NTH, bool MAG>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) physics_kernel(PhysParams P) {
     constexpr int N = NTH;
     constexpr int FS = fstride(N);
@@ -547,7 +577,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
     const int r = pair % nr;
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     // The row's radial and colatitude factors live in shared memory and are read
     // where they are used, so that they hold no registers across the FFTs.
     __shared__ double rowc[RC_COUNT];
@@ -671,33 +701,92 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
             cmax = fmax(cmax, vr[q].y * vr[q].y * rfac);
         }
     }
+    if constexpr (MAG) {
+        // M1: B_r, B_theta, B_phi, (curl B)_r.  The EMF u x B (Compute_EMF,
+        // Sphere_Physical_Space.F90:534-581) replaces them in the FFT buffer and goes through
+        // its own r2c and fold into p2b fields B_EMFT, B_EMFR, B_EMFP; B stays in registers
+        // for the Lorentz force, which M2 ((curl B)_theta, (curl B)_phi) completes.
+        double2 br[ZPT], bt[ZPT], bp[ZPT], cbr[ZPT];
+        double2* buf = sm + RowSmem<N>::BUF;
+        {
+            const int fo[4] = {A_BR, A_BT, A_BP, A_CBR};
+            const bool dp[4] = {false, false, false, false};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double csc = rowc[RC_CSC], rad = rowc[RC_RAD], rho = rowc[RC_RHO];
+            // the Alfven speed (:798-806)
+            const double hfb = P.llmax * orad * orad / rho * P.lorentz, rfb = P.lorentz / (dr * dr * rho);
+#pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                br[q] = y[0][q];
+                bt[q] = make_double2(y[1][q].x * csc * orad, y[1][q].y * csc * orad);   // rsintheta_div
+                bp[q] = make_double2(y[2][q].x * csc * orad, y[2][q].y * csc * orad);
+                cbr[q] = y[3][q];
+                if (!live(q)) continue;
+                cmax = fmax(cmax, (bt[q].x * bt[q].x + bp[q].x * bp[q].x) * hfb);
+                cmax = fmax(cmax, (bt[q].y * bt[q].y + bp[q].y * bp[q].y) * hfb);
+                cmax = fmax(cmax, br[q].x * br[q].x * rfb);
+                cmax = fmax(cmax, br[q].y * br[q].y * rfb);
+                auto emft = [&](double a, double c, double b_r, double b_p) { return (-a * b_p + c * b_r) * csc * rad; };
+                auto emfr = [&](double b, double c, double b_t, double b_p) { return b * b_p - c * b_t; };
+                auto emfp = [&](double a, double b, double b_r, double b_t) { return (a * b_t - b * b_r) * csc * rad; };
+                const int n = t + q * ROW_THREADS;
+                buf[SW(0 * FS + n)] = make_double2(emft(vr[q].x, vp[q].x, br[q].x, bp[q].x),
+                                                   emft(vr[q].y, vp[q].y, br[q].y, bp[q].y));
+                buf[SW(1 * FS + n)] = make_double2(emfr(vt[q].x, vp[q].x, bt[q].x, bp[q].x),
+                                                   emfr(vt[q].y, vp[q].y, bt[q].y, bp[q].y));
+                buf[SW(2 * FS + n)] = make_double2(emfp(vr[q].x, vt[q].x, br[q].x, bt[q].x),
+                                                   emfp(vr[q].y, vt[q].y, br[q].y, bt[q].y));
+            }
+        }
+        __syncthreads();
+        fft_dit<N, 3, ROW_THREADS>(buf, P.twp, t);
+        r2c_finish<N>(buf, 3, P.L, P.wr, t, [](int) { return 0.5; });
+        cluster.sync();
+        {
+            const double2* peer = cluster.map_shared_rank(buf, h ^ 1);
+            const int L = P.L;
+            const long mstride = 2L * (P.nth / 2) * P.ncolb;
+            double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * P.nfb) +
+                            2 * B_EMFT;
+            for (int g = t; g < 3 * L; g += ROW_THREADS) {
+                const int k = g / 3, f = g - 3 * k;
+                const double2 a = buf[SW(f * FS + k)], b = peer[SW(f * FS + k)];
+                *reinterpret_cast<double2*>(obase + k * mstride + f * 2) = h ? csub(b, a) : cadd(a, b);
+            }
+        }
+        cluster.sync();   // the partner has read this CTA's EMF spectra
+        // M2: (curl B)_theta, (curl B)_phi -> the Lorentz force (:512-519, 635-641, 712-718)
+        {
+            const int fo[2] = {A_CBT, A_CBP};
+            const bool dp[2] = {false, false};
+            row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double csc = rowc[RC_CSC], rad = rowc[RC_RAD], rho = rowc[RC_RHO];
+            const double lc = P.lorentz, r2lc = rad * rad * lc, lcr = lc / rho;
+#pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                const double2 cbt = make_double2(y[0][q].x * csc * orad, y[0][q].y * csc * orad);
+                const double2 cbp = make_double2(y[1][q].x * csc * orad, y[1][q].y * csc * orad);
+                double2& w = acc_at(0, q);
+                double2& pp = acc_at(1, q);
+                double2& z = acc_at(3, q);
+                w.x += r2lc * (cbt.x * bp[q].x - cbp.x * bt[q].x);
+                w.y += r2lc * (cbt.y * bp[q].y - cbp.y * bt[q].y);
+                pp.x -= lcr * (cbp.x * br[q].x - cbr[q].x * bp[q].x);
+                pp.y -= lcr * (cbp.y * br[q].y - cbr[q].y * bp[q].y);
+                z.x -= lcr * (cbr[q].x * bt[q].x - cbt.x * br[q].x);
+                z.y -= lcr * (cbr[q].y * bt[q].y - cbt.y * br[q].y);
+            }
+        }
+    }
     __syncthreads();
     // r2c of W, P, T, Z in place on the accumulators: Z = FFT(y[2n] + i y[2n+1]), then
     // X_k = e - i conj(w^k) d with e, d the half sums/differences of Z_k, conj Z_{N-k},
     // one (k, N-k) pair per work item, in place
     fft_dit<N, 4, ROW_THREADS>(acc, P.twp, t);
     {
-        constexpr int NI = N / 2 + 1;
-        const int L = P.L;
-        for (int g = t; g < 4 * NI; g += ROW_THREADS) {
-            const int f = g / NI, k = g - f * NI;
-            const double2 zk = acc[SW(f * FS + k)];
-            const double2 zn = acc[SW(f * FS + (N - k) % N)];
-            const double2 wk = __ldg(P.wr + k);   // w^(N-k) = -conj(w^k)
-            const double hs = (f & 1) ? rowc[RC_HSF] : 0.5;   // P and Z (f = 1, 3) take the row factor
-            auto xval = [&](double2 a, double2 b, double2 w, bool zero_im) {   // X from Z_kk = a, Z_{N-kk} = b
-                const double2 bn = cconj(b);
-                const double2 e = make_double2(hs * (a.x + bn.x), hs * (a.y + bn.y));
-                const double2 d = make_double2(hs * (a.x - bn.x), hs * (a.y - bn.y));
-                const double2 wd = cmul(cconj(w), d);
-                double2 X = make_double2(e.x + wd.y, e.y - wd.x);
-                if (zero_im) X.y = 0.0;
-                return X;
-            };
-            if (k < L) acc[SW(f * FS + k)] = xval(zk, zn, wk, k == 0);
-            if (k != 0 && 2 * k != N && N - k < L)
-                acc[SW(f * FS + N - k)] = xval(zn, zk, make_double2(-wk.x, wk.y), false);
-        }
+        const double hsf_pz = rowc[RC_HSF];   // P and Z (f = 1, 3) take the row factor
+        r2c_finish<N>(acc, 4, P.L, P.wr, t, [&](int f) { return (f & 1) ? hsf_pz : 0.5; });
     }
     // equatorial fold of PtS_4d_dgpv3 (Legendre_Transforms.F90:1109-1122) with the
     // partner row: f_even = X(theta) + X(pi - theta) (written by rank 0),
@@ -708,7 +797,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         const double2* peer = cluster.map_shared_rank(acc, h ^ 1);
         const int L = P.L;
         const long mstride = 2L * (P.nth / 2) * P.ncolb;   // p2b[m][par][theta_h][r][field][2]
-        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * NP2B);
+        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * P.nfb);
         for (int g = t; g < 4 * L; g += ROW_THREADS) {   // g = (k, f), f fastest: 64 contiguous bytes per k
             const int k = g >> 2, f = g & 3;
             const double2 a = mine[SW(f * FS + k)], b = peer[SW(f * FS + k)];
@@ -768,6 +857,8 @@ void physics_prepare(Ctx& c) {
     c.physics_form = physics_form1_supported(c.d.nth) ? 1 : 0;
     if (!c.physics3_ok && !physics_form1_supported(c.d.nth))
         throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no physical-space kernel instance");
+    if (c.mag && !physics_form1_supported(c.d.nth))   // the magnetic terms live in that kernel only
+        throw ArgError("magnetism needs n_theta in 24..768 (2^a or 3*2^a); got " + std::to_string(c.d.nth));
 }
 
 // ---------------------------------------------------------------------------
@@ -894,7 +985,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(P3<N>::NT, MINB) phy
     const int r = pair % nr;
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     if (t == 0) {
         const double csc = P.trig[2 * N + th], orad = P.radial[R_OVER_R * nr + r];
         rowc[RC_RAD] = P.radial[R_RADIUS * nr + r];
@@ -1050,7 +1141,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(P3<N>::NT, MINB) phy
         const double2* peer = cluster.map_shared_rank(acc, h ^ 1);
         const int L = P.L;
         const long mstride = 2L * (P.nth / 2) * P.ncolb;
-        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * NP2B);
+        double* obase = P.p2b + (long)h * (P.nth / 2) * P.ncolb + (long)thh * P.ncolb + (long)r * (2 * P.nfb);
         for (int g = t; g < 4 * L; g += NT) {
             const int k = g >> 2, f = g & 3;
             const double2 a = acc[f * FS + S::slot(k)], b = peer[f * FS + S::slot(k)];
@@ -1094,16 +1185,19 @@ void launch_physics(Ctx& c) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
-    P.ncolb = NP2B * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
+    P.ncolb = c.nfb * c.d.nr * 2;
     P.coriolis = c.rad.coriolis;
     P.rotation = c.cfg.rotation;
     P.llmax = (double)c.d.lmax * (c.d.lmax + 1);
+    P.lorentz = c.cfg.magnetism ? c.rad.lorentz : 0.0;
     make_plan(c.d.nth);   // validates n_theta = 2^a 3^b
     if (c.d.L > (2 * c.d.nth) / 3 + 1)
         throw ArgError("n_theta must be at least 3 (l_max + 1) / 2 for the physical-space kernel");
     const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;   // clusters of 2 rows
-    if (c.physics3_ok && c.physics_form != 1) {   // last pass in registers (form 0: two CTAs per SM, 2: one)
+    if (c.physics3_ok && c.physics_form != 1 && !c.mag) {   // last pass in registers (form 0: two CTAs per SM, 2: one)
         auto go3 = [&](auto kern, int nt, size_t units) {
             const size_t smem = units * sizeof(double2);
             RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1133,18 +1227,26 @@ void launch_physics(Ctx& c) {
         kern<<<grid, ROW_THREADS, smem, c.stream>>>(P);
         (void)n;
     };
+#define RA_PHYS_CASE(NN)                                                   \
+    case NN:                                                               \
+        if (c.mag)                                                         \
+            go(physics_kernel<NN, true>, NN, RowSmem<NN>::SIZE);           \
+        else                                                               \
+            go(physics_kernel<NN, false>, NN, RowSmem<NN>::SIZE);          \
+        break;
     switch (c.d.nth) {
-        case 24: go(physics_kernel<24>, 24, RowSmem<24>::SIZE); break;
-        case 32: go(physics_kernel<32>, 32, RowSmem<32>::SIZE); break;
-        case 48: go(physics_kernel<48>, 48, RowSmem<48>::SIZE); break;
-        case 64: go(physics_kernel<64>, 64, RowSmem<64>::SIZE); break;
-        case 96: go(physics_kernel<96>, 96, RowSmem<96>::SIZE); break;
-        case 128: go(physics_kernel<128>, 128, RowSmem<128>::SIZE); break;
-        case 192: go(physics_kernel<192>, 192, RowSmem<192>::SIZE); break;
-        case 256: go(physics_kernel<256>, 256, RowSmem<256>::SIZE); break;
-        case 384: go(physics_kernel<384>, 384, RowSmem<384>::SIZE); break;
-        case 512: go(physics_kernel<512>, 512, RowSmem<512>::SIZE); break;
-        case 768: go(physics_kernel<768>, 768, RowSmem<768>::SIZE); break;
+        RA_PHYS_CASE(24)
+        RA_PHYS_CASE(32)
+        RA_PHYS_CASE(48)
+        RA_PHYS_CASE(64)
+        RA_PHYS_CASE(96)
+        RA_PHYS_CASE(128)
+        RA_PHYS_CASE(192)
+        RA_PHYS_CASE(256)
+        RA_PHYS_CASE(384)
+        RA_PHYS_CASE(512)
+        RA_PHYS_CASE(768)
+#undef RA_PHYS_CASE
         default: throw ArgError("n_theta " + std::to_string(c.d.nth) +
                                 " has no physical-space kernel instance (24..768 of the form 2^a or 3*2^a)");
     }
@@ -1231,7 +1333,7 @@ __global__ void __launch_bounds__(ROW_THREADS) kinetic_energy_rows_kernel(PhysPa
     const int r = pair % nr;
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[3] = {A_VR, A_VT, A_VP};
     const bool dp[3] = {false, false, false};
     double2 y[FB][ZPT];
@@ -1285,7 +1387,9 @@ void launch_kinetic_energy(Ctx& c) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)3 * fstride(n) * sizeof(double2);
@@ -1343,7 +1447,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_slice_kernel(PhysParams P, 
     const int th = h ? (N - 1 - thh) : thh;
     const int lv = (int)blockIdx.y;
     const int r = S.level[lv];
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1368,7 +1472,9 @@ void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)S.nl);
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1414,7 +1520,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_moment_rows_kernel(PhysPara
     const int th = h ? (N - 1 - thh) : thh;
     const int r = (int)blockIdx.y;
     const int nr = P.nr;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1486,7 +1592,9 @@ void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out)
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
     auto go = [&](auto k0, auto k1, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1533,7 +1641,9 @@ void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
     auto go = [&](auto k0, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1581,7 +1691,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int th = h ? (N - 1 - thh) : thh;
     const int lv = (int)blockIdx.y;
     const int r = S.level[lv];
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1614,7 +1724,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     cluster.sync();
     {
         const double2* peer = cluster.map_shared_rank(buf, h ^ 1);
-        const long ncolb = (long)NP2B * P.nr * 2;
+        const long ncolb = (long)P.nfb * P.nr * 2;
         const long mstride = 2L * (N / 2) * ncolb;   // p2b[m][par][theta_h][col]
         double* obase = p2b + (long)h * (N / 2) * ncolb + (long)thh * ncolb + (long)(slot0 + lv) * 2;
         for (int k = t; k < L; k += ROW_THREADS) {
@@ -1643,7 +1753,7 @@ __global__ void spectra_gather_kernel(const double* __restrict__ s2, int L, int 
 void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b) {
     if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
     if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("shell spectra: 1 .. 64 levels per launch");
-    if (slot0 < 0 || slot0 + S.nl > NP2B * c.d.nr) throw ArgError("shell spectra: column slots out of range");
+    if (slot0 < 0 || slot0 + S.nl > c.nfb * c.d.nr) throw ArgError("shell spectra: column slots out of range");
     PhysParams P{};
     P.p2a = c.d_p2a;
     P.trig = c.d_costh;
@@ -1652,7 +1762,9 @@ void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)S.nl);
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1680,7 +1792,7 @@ void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b) {
 void launch_spectra_gather(Ctx& c, const double* s2, int nslots, double* out) {
     const long total = (long)nslots * 2 * c.d.L * c.d.L;
     const unsigned blocks = (unsigned)std::min<long>((total + 255) / 256, 148L * 16);
-    spectra_gather_kernel<<<blocks, 256, 0, c.stream>>>(s2, c.d.L, nslots, (long)NP2B * c.d.nr * 2, out);
+    spectra_gather_kernel<<<blocks, 256, 0, c.stream>>>(s2, c.d.L, nslots, (long)c.nfb * c.d.nr * 2, out);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -1703,7 +1815,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int thh = N / 2 - 1;
     const int th = h ? (N - 1 - thh) : thh;
     const int r = (int)blockIdx.y;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1736,7 +1848,9 @@ void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u, (unsigned)c.d.nr);
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1777,7 +1891,7 @@ __global__ void __launch_bounds__(ROW_THREADS) meridional_slice_kernel(PhysParam
     const int th = h ? (N - 1 - thh) : thh;
     const int r = (int)blockIdx.y;
     const int nr = P.nr;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1805,7 +1919,9 @@ void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out) {
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1853,7 +1969,9 @@ void launch_global_average(Ctx& c, const SliceSpec& S, double* rows, double* mea
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid(2u * (unsigned)c.d.nth2, (unsigned)c.d.nr);
     auto go = [&](auto k0, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);
@@ -1899,7 +2017,7 @@ __global__ void __launch_bounds__(ROW_THREADS) point_probe_kernel(PhysParams P, 
     const int th = Q.theta[jt], r = Q.r[ir];
     const int h = th >= N / 2 ? 1 : 0;
     const int thh = h ? (N - 1 - th) : th;
-    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * NP2A);
+    const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
@@ -1927,7 +2045,9 @@ void launch_point_probes(Ctx& c, const SliceSpec& S, const ProbeSet& Q, double* 
     P.L = c.d.L;
     P.nth = c.d.nth;
     P.nr = c.d.nr;
-    P.ncola = NP2A * c.d.nr * 2;
+    P.ncola = c.nfa * c.d.nr * 2;
+    P.nfa = c.nfa;
+    P.nfb = c.nfb;
     const dim3 grid((unsigned)Q.ntheta, (unsigned)Q.nr);
     auto go = [&](auto kern, int n) {
         const size_t smem = (size_t)fstride(n) * sizeof(double2);

@@ -808,6 +808,12 @@ void factor_matrices(Ctx& c) {
     if (bad) throw SingularError("singular W-P-T matrix at l = " + std::to_string(bad - 1));
     bad = lu_factor_batch(c.stream, c.lu_work, c.d_Az, c.d_perm_z, nr, L, c.d_skip_z, &c.launches);
     if (bad) throw SingularError("singular Z matrix at l = " + std::to_string(bad - 1));
+    if (c.mag) {   // C and A: no equation at l = 0, as for Z
+        bad = lu_factor_batch(c.stream, c.lu_work, c.d_Ac, c.d_perm_c, nr, L, c.d_skip_z, &c.launches);
+        if (bad) throw SingularError("singular C matrix at l = " + std::to_string(bad - 1));
+        bad = lu_factor_batch(c.stream, c.lu_work, c.d_Aa, c.d_perm_a, nr, L, c.d_skip_z, &c.launches);
+        if (bad) throw SingularError("singular A matrix at l = " + std::to_string(bad - 1));
+    }
     if (c.cfg.precision == RA_PREC_MIXED) {
         const LuSys s0{c.d_Awpt, c.d_perm_wpt, nullptr, c.d_Ainv_wpt, 3 * nr};
         const LuSys s1{c.d_Az, c.d_perm_z, nullptr, c.d_Ainv_z, nr};
@@ -826,6 +832,18 @@ void launch_solve(Ctx& c) {
     const LuSys s1{c.d_Az, c.d_perm_z, c.d_rhs_z, c.d_sol_z, nr};
     launch_lu_solve(c.stream, c.d_solve_tiles, c.n_solve_tiles, s0, LU_MODE_STEP, 0, c.solve_nc);
     launch_lu_solve(c.stream, c.d_solve_tiles_z, c.n_solve_tiles_z, s1, LU_MODE_STEP, 0, c.solve_nc_z);
+    c.launches += 2;
+}
+
+// The C and A equations of the magnetic set (both precision forms): FP64 LU substitution
+// with the Z system's tile list (same size, same columns per l; l = 0 is the identity).
+void launch_solve_mag(Ctx& c) {
+    if (!c.d_solve_tiles_z) throw ArgError("solve tiles not prepared (solve_prepare runs at set-up)");
+    const int nr = c.d.nr;
+    const LuSys sc{c.d_Ac, c.d_perm_c, c.d_rhs_c, c.d_sol_c, nr};
+    const LuSys sa{c.d_Aa, c.d_perm_a, c.d_rhs_a, c.d_sol_a, nr};
+    launch_lu_solve(c.stream, c.d_solve_tiles_z, c.n_solve_tiles_z, sc, LU_MODE_STEP, 0, c.solve_nc_z);
+    launch_lu_solve(c.stream, c.d_solve_tiles_z, c.n_solve_tiles_z, sa, LU_MODE_STEP, 0, c.solve_nc_z);
     c.launches += 2;
 }
 

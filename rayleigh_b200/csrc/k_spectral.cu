@@ -40,7 +40,8 @@ __device__ __forceinline__ int ell_of_lm(long lm) {
 // double-buffered stage from L2: one accumulator and no coefficient stage keep
 // a CTA at about 75 KB of shared memory and 168 registers, three CTAs per SM.
 struct ChebField { int o0, nd, var; };
-__constant__ ChebField kChebField[4] = {{G_W0, 4, 0}, {G_P0, 2, 1}, {G_T0, 3, 2}, {G_Z0, 3, 3}};
+__constant__ ChebField kChebField[6] = {{G_W0, 4, 0}, {G_P0, 2, 1}, {G_T0, 3, 2}, {G_Z0, 3, 3},
+                                        {G_C0, 3, 4}, {G_A0, 3, 5}};   // C and A with magnetism
 
 using ChebShape = Wide;   // 32 x 128 tiles: 32-row blocks cover the n_r/2 = 96 half-grid rows exactly
 struct ChebSmem {
@@ -51,6 +52,8 @@ struct ChebSmem {
 __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const double* __restrict__ Dpar,
                                                                          const double* __restrict__ sol_wpt,
                                                                          const double* __restrict__ sol_z,
+                                                                         const double* __restrict__ sol_c,
+                                                                         const double* __restrict__ sol_a,
                                                                          double* __restrict__ g, int nr, int kc,
                                                                          long ncols) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -65,7 +68,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
         src = sol_wpt + (long)cf.var * nr;
         cstride = 3L * nr;
     } else {
-        src = sol_z;
+        src = cf.var == 3 ? sol_z : (cf.var == 4 ? sol_c : sol_a);
         cstride = nr;
     }
     const int t = threadIdx.x;
@@ -117,9 +120,9 @@ void launch_cheb_synthesis(Ctx& c) {
     const size_t smem = sizeof(ChebSmem);
     // the limit is per device: set it on every launch (a host-side call, also legal during capture)
     RA_CUDA(cudaFuncSetAttribute(cheb_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)((ncols + ChebShape::BN - 1) / ChebShape::BN), 4);
-    cheb_synthesis_kernel<<<grid, GEMM_THREADS, smem, c.stream>>>(c.d_Dpar, c.d_sol_wpt, c.d_sol_z, c.d_g, c.d.nr,
-                                                                   c.d.kc, ncols);
+    dim3 grid((unsigned)((ncols + ChebShape::BN - 1) / ChebShape::BN), c.mag ? 6 : 4);
+    cheb_synthesis_kernel<<<grid, GEMM_THREADS, smem, c.stream>>>(c.d_Dpar, c.d_sol_wpt, c.d_sol_z, c.d_sol_c,
+                                                                   c.d_sol_a, c.d_g, c.d.nr, c.d.kc, ncols);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -198,6 +201,61 @@ void launch_post_assemble(Ctx& c, double old_ab) {
     ++c.launches;
 }
 
+// The C and A parts of Post_Solve (Sphere_Spectral_Space.F90:268-297, 370-384): their
+// right-hand sides, and the fields rlm_spacea's magnetic part reads, m-major.
+__global__ void post_assemble_mag_kernel(const double* __restrict__ g, const double* __restrict__ ab,
+                                         const double* __restrict__ coefm, double* __restrict__ rhs_c,
+                                         double* __restrict__ rhs_a, double* __restrict__ s2am, long nlm, int nr,
+                                         int L, double old_ab) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    const long lm = idx / nr;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const long plane = nlm * 2 * nr;
+    const long i0 = lm * 2 * nr + r;
+    const double* cf = coefm + (long)l * NMSLOT * nr + r;
+    const double c0 = cf[MS_C0 * nr], c2 = cf[MS_C2 * nr];
+    const double a0 = cf[MS_A0 * nr], a1 = cf[MS_A1 * nr], a2 = cf[MS_A2 * nr];
+    double gv[6][2];
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        gv[o][0] = g[(G_C0 + o) * plane + i0];
+        gv[o][1] = g[(G_C0 + o) * plane + i0 + nr];
+    }
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const long o = i0 + ri * nr;
+        // p1b = old_ab * p1b, then Add_Derivative in the reference's order: A'' (from the
+        // ctemp buffer), then A, A' and C'', C
+        double ra = ab[5 * plane + o] * old_ab;
+        double rc = ab[4 * plane + o] * old_ab;
+        ra += a2 * gv[G_A2 - G_C0][ri];
+        ra += a0 * gv[G_A0 - G_C0][ri];
+        ra += a1 * gv[G_A1 - G_C0][ri];
+        rc += c2 * gv[G_C2 - G_C0][ri];
+        rc += c0 * gv[G_C0 - G_C0][ri];
+        rhs_a[o] = ra;
+        rhs_c[o] = rc;
+    }
+    const long row = row_index(m, l, L);
+    double* so = s2am + row * (long)NS2AM * nr * 2 + (long)r * 2;
+    const long fs = 2L * nr;
+    constexpr int kOut[NS2AM] = {G_C0, G_A0, G_C1, G_A1, G_C2};
+#pragma unroll
+    for (int f = 0; f < NS2AM; ++f)
+        *reinterpret_cast<double2*>(so + f * fs) = make_double2(gv[kOut[f] - G_C0][0], gv[kOut[f] - G_C0][1]);
+}
+
+void launch_post_assemble_mag(Ctx& c, double old_ab) {
+    const long total = c.d.nlm * c.d.nr;
+    post_assemble_mag_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
+        c.d_g, c.d_ab, c.d_coef_mag, c.d_rhs_c, c.d_rhs_a, c.d_s2am, c.d.nlm, c.d.nr, c.d.L, old_ab);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 // ---------------------------------------------------------------------------
 // rlm_spacea: 7 spectral fields -> the 11 fields the inverse transform carries
 // ---------------------------------------------------------------------------
@@ -237,7 +295,7 @@ __device__ __forceinline__ void ml_of_row(long row, int L, int& m, int& l) {
 __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __restrict__ s2a,
                                                              double* __restrict__ s2o,
                                                              const double* __restrict__ radial, long nlm, int nr,
-                                                             int L) {
+                                                             int L, int nfa) {
     __shared__ double2 stage[RLM_A_THREADS * NP2A];   // the block's outputs, re-read for coalesced stores
     const long total = nlm * nr;
     const long idx0 = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (row, r)
@@ -326,7 +384,7 @@ __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __re
     for (int f = 0; f < NP2A; ++f)
         st[lane * NP2A + f] = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
     __syncwarp();
-    const long obase = row_index(m, l, L) * (long)NP2A * fsz + (long)r * (2 * NP2A);
+    const long obase = row_index(m, l, L) * (long)nfa * fsz + (long)r * (2 * nfa);   // nfa >= NP2A fields per radius
 #pragma unroll
     for (int i = 0; i < NP2A; ++i) {
         const int ci = i * 32 + lane, sl = ci / NP2A, f = ci - sl * NP2A;
@@ -339,7 +397,71 @@ __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __re
 void launch_rlm_a(Ctx& c) {
     const long total = c.d.nlm * c.d.nr;
     rlm_a_kernel<<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
-        c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L);
+        c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
+// Compute_BandCurlB (Sphere_Hybrid_Space.F90:357-435): B and curl B in (l, m) space from
+// C, A, C', A', C'' (the l_max mode zeroed on entry and exit, as for the hydrodynamic fields):
+//   B_r = l(l+1) C / r^2,  (curl B)_r = l(l+1) A / r^2,  X = C'' - B_r,
+//   r sin(theta) (curl B)_theta = d_theta A' - d_phi X,  r sin(theta) (curl B)_phi = d_phi A' + d_theta X,
+//   r sin(theta) B_theta = d_phi A + d_theta C',          r sin(theta) B_phi = d_phi C' - d_theta A,
+// with d_theta = sin(theta) d/dtheta through the l -+ 1 couplings; written into fields
+// A_BR .. A_BP of s2a11.
+__global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_mag_kernel(const double* __restrict__ s2am,
+                                                                 double* __restrict__ s2o,
+                                                                 const double* __restrict__ radial, long nlm,
+                                                                 int nr, int L, int nfa) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (row, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    int l, m;
+    ml_of_row(idx / nr, L, m, l);
+    const int lmax = L - 1;
+    const long fsz = 2L * nr;
+    const long rsz = (long)NS2AM * fsz;
+    auto get2 = [&](int f, int ll) -> double2 {
+        if (ll < m || ll >= lmax) return make_double2(0.0, 0.0);
+        return __ldg(reinterpret_cast<const double2*>(s2am + row_index(m, ll, L) * rsz + f * fsz + r * 2));
+    };
+    const double orsq = radial[R_OVER_RSQ * nr + r];
+    const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
+    const double llp1 = (double)l * (l + 1);
+    const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
+    const double2 C = get2(SM_C, l), A = get2(SM_A, l), C1 = get2(SM_C1, l), A1 = get2(SM_A1, l);
+    const double2 C2 = get2(SM_C2, l);
+    const double2 Cm = get2(SM_C, l - 1), Cp = get2(SM_C, l + 1), C2m = get2(SM_C2, l - 1), C2p = get2(SM_C2, l + 1);
+    const double2 Am = get2(SM_A, l - 1), Ap = get2(SM_A, l + 1), A1m = get2(SM_A1, l - 1), A1p = get2(SM_A1, l + 1);
+    const double2 C1m = get2(SM_C1, l - 1), C1p = get2(SM_C1, l + 1);
+    auto c = [](double2 v, int ri) { return ri ? v.y : v.x; };
+    double out[6][2];
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const double sg = ri ? (double)m : -(double)m;   // d/dphi: (re, im) -> (-m im, m re)
+        const int rj = 1 - ri;
+        const double br = llp1 * c(C, ri) * orsq;
+        const double xj = c(C2, rj) - llp1 * c(C, rj) * orsq;    // X at l, the other part
+        const double xm = c(C2m, ri) - llm * c(Cm, ri) * orsq;   // X at l - 1, l + 1
+        const double xp = c(C2p, ri) - llq * c(Cp, ri) * orsq;
+        out[0][ri] = br;
+        out[1][ri] = llp1 * c(A, ri) * orsq;
+        out[2][ri] = (c(A1m, ri) * c1 + c(A1p, ri) * c2) - sg * xj;
+        out[3][ri] = sg * c(A1, rj) + (xm * c1 + xp * c2);
+        out[4][ri] = sg * c(A, rj) + (c(C1m, ri) * c1 + c(C1p, ri) * c2);
+        out[5][ri] = sg * c(C1, rj) - (c(Am, ri) * c1 + c(Ap, ri) * c2);
+    }
+    const bool zero = (l == lmax);
+    double* o = s2o + row_index(m, l, L) * (long)nfa * fsz + (long)r * (2 * nfa) + 2 * A_BR;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        *reinterpret_cast<double2*>(o + 2 * f) = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
+}
+
+void launch_rlm_a_mag(Ctx& c) {
+    const long total = c.d.nlm * c.d.nr;
+    rlm_a_mag_kernel<<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
+        c.d_s2am, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -349,7 +471,7 @@ void launch_rlm_a(Ctx& c) {
 // ---------------------------------------------------------------------------
 __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict__ ab, double* __restrict__ rhs_wpt,
                              double* __restrict__ rhs_z, long nlm, int nr, int L, double new_ab, double bc_top,
-                             double bc_bot, const double* __restrict__ bcv, int* __restrict__ status) {
+                             double bc_bot, const double* __restrict__ bcv, int* __restrict__ status, int nfb) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
     if (idx >= nlm * nr) return;
     const int r = (int)(idx % nr);
@@ -357,10 +479,10 @@ __global__ void rlm_b_kernel(const double* __restrict__ s2b, double* __restrict_
     const int l = ell_of_lm(lm);
     const int m = (int)(lm - (long)l * (l + 1) / 2);
     const int lmax = L - 1;
-    const long rsz = 2L * NP2B * nr;   // s2b[row][r][field][re, im]
+    const long rsz = 2L * nfb * nr;   // s2b[row][r][field][re, im]
     auto get2 = [&](int f, int ll) -> double2 {
         if (ll < m || ll > lmax) return make_double2(0.0, 0.0);
-        return __ldg(reinterpret_cast<const double2*>(s2b + row_index(m, ll, L) * rsz + r * (2 * NP2B) + f * 2));
+        return __ldg(reinterpret_cast<const double2*>(s2b + row_index(m, ll, L) * rsz + r * (2 * nfb) + f * 2));
     };
     const double2 cW = get2(0, l), cP = get2(1, l), cT = get2(2, l), cZ = get2(3, l);
     const double2 mP = get2(1, l - 1), pP = get2(1, l + 1), mZ = get2(3, l - 1), pZ = get2(3, l + 1);
@@ -471,9 +593,103 @@ void launch_rlm_b(Ctx& c, double new_ab) {
     bc_values(c, top, bot);
     rlm_b_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_s2b, c.d_ab, c.d_rhs_wpt, c.d_rhs_z,
                                                                         c.d.nlm, c.d.nr, c.d.L, new_ab, top, bot,
-                                                                        c.d_bcval, c.d_status);
+                                                                        c.d_bcval, c.d_status, c.nfb);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
+}
+
+// Adjust_Emf (Sphere_Hybrid_Space.F90:557-602) and the first half of Finalize_EMF: the C
+// right-hand side from the radial curl of the EMF,
+//   N_C = (sd_theta EMF_phi - d_phi EMF_theta) / l(l+1),
+// the A one's EMF_r part, and X = (d_phi EMF_phi + sd_theta EMF_theta) / l(l+1), whose
+// radial derivative emf_radial_kernel adds (1 / l(l+1) -> 1 at l = 0, l_max zeroed).
+// Then AB history, Add_To_All_RHS and the (zero) magnetic boundary rows for C.
+__global__ void rlm_b_mag_kernel(const double* __restrict__ s2b, double* __restrict__ ab,
+                                 double* __restrict__ rhs_c, double* __restrict__ xemf, long nlm, int nr, int L,
+                                 double new_ab, int nfb, int* __restrict__ status) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r)
+    if (idx >= nlm * nr) return;
+    const int r = (int)(idx % nr);
+    const long lm = idx / nr;
+    const int l = ell_of_lm(lm);
+    const int m = (int)(lm - (long)l * (l + 1) / 2);
+    const int lmax = L - 1;
+    const long rsz = 2L * nfb * nr;
+    auto get2 = [&](int f, int ll) -> double2 {
+        if (ll < m || ll > lmax) return make_double2(0.0, 0.0);
+        return __ldg(reinterpret_cast<const double2*>(s2b + row_index(m, ll, L) * rsz + r * (2 * nfb) + f * 2));
+    };
+    const double2 et = get2(B_EMFT, l), er = get2(B_EMFR, l), ep = get2(B_EMFP, l);
+    const double2 etm = get2(B_EMFT, l - 1), etp = get2(B_EMFT, l + 1);
+    const double2 epm = get2(B_EMFP, l - 1), epp = get2(B_EMFP, l + 1);
+    auto c = [](double2 v, int ri) { return ri ? v.y : v.x; };
+    const double ollp1 = (l > 0) ? 1.0 / ((double)l * (l + 1)) : 1.0;
+    const double c1 = sdth_c1(l, m), c2 = sdth_c2(l, m);
+    const long plane = nlm * 2 * nr;
+    const bool edge = (r == 0 || r == nr - 1);
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const double sg = ri ? (double)m : -(double)m;
+        const int rj = 1 - ri;
+        double nc = ((c(epm, ri) * c1 + c(epp, ri) * c2) - sg * c(et, rj)) * ollp1;
+        double x = (sg * c(ep, rj) + (c(etm, ri) * c1 + c(etp, ri) * c2)) * ollp1;
+        double na = c(er, ri);
+        if (l == lmax) nc = x = na = 0.0;
+        if (!(isfinite(nc) && isfinite(x) && isfinite(na))) atomicOr(status, RA_STATUS_NONFINITE);
+        const long o = (lm * 2 + ri) * nr + r;
+        ab[4 * plane + o] = nc;
+        ab[5 * plane + o] = na;   // emf_radial_kernel adds d/dr X
+        xemf[o] = x;
+        rhs_c[o] = edge ? 0.0 : rhs_c[o] + new_ab * nc;
+    }
+}
+
+// Finalize_EMF's radial derivative (Sphere_Spectral_Space.F90:436-488) as one product with
+// the grid operator M (to_spectral, d/dr, dealias, from_spectral): N_A = EMF_r + M X per
+// (l, m, re/im) column, on the FP64 tensor-core tile engine; then the A history, the A
+// right-hand side and its (zero) boundary rows.
+__global__ void __launch_bounds__(GEMM_THREADS) emf_radial_kernel(const double* __restrict__ M,
+                                                                  const double* __restrict__ xemf,
+                                                                  double* __restrict__ ab_a,
+                                                                  double* __restrict__ rhs_a, int nr, long ncols,
+                                                                  double new_ab) {
+    __shared__ GemmSmem sm;
+    const int r0 = blockIdx.y * Sq::BM;
+    const long c0 = (long)blockIdx.x * Sq::BN;
+    auto fa = [&](int k, int x) -> double {   // M(r0 + x, k)
+        const int rr = r0 + x;
+        return (k < nr && rr < nr) ? __ldg(M + (long)rr * nr + k) : 0.0;
+    };
+    auto fb = [&](int k, int y) -> double {   // X(k, c0 + y)
+        const long col = c0 + y;
+        return (k < nr && col < ncols) ? __ldg(xemf + col * nr + k) : 0.0;
+    };
+    Acc acc;
+    acc.zero();
+    gemm_tile<false, false>(acc, fa, fb, nr, sm);
+    acc_foreach(acc, [&](int x, int y, double v) {
+        const int rr = r0 + x;
+        const long col = c0 + y;
+        if (rr < nr && col < ncols) {
+            const long o = col * nr + rr;
+            const double na = ab_a[o] + v;
+            ab_a[o] = na;
+            rhs_a[o] = (rr == 0 || rr == nr - 1) ? 0.0 : rhs_a[o] + new_ab * na;
+        }
+    });
+}
+
+void launch_rlm_b_mag(Ctx& c, double new_ab) {
+    const long total = c.d.nlm * c.d.nr;
+    rlm_b_mag_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
+        c.d_s2b, c.d_ab, c.d_rhs_c, c.d_xemf, c.d.nlm, c.d.nr, c.d.L, new_ab, c.nfb, c.d_status);
+    RA_CUDA(cudaGetLastError());
+    const long ncols = 2 * c.d.nlm;
+    dim3 grid((unsigned)((ncols + Sq::BN - 1) / Sq::BN), (unsigned)((c.d.nr + Sq::BM - 1) / Sq::BM));
+    emf_radial_kernel<<<grid, GEMM_THREADS, 0, c.stream>>>(c.d_Memf, c.d_xemf, c.d_ab + 5 * c.d.nlm * 2 * c.d.nr,
+                                                         c.d_rhs_a, c.d.nr, ncols, new_ab);
+    RA_CUDA(cudaGetLastError());
+    c.launches += 2;
 }
 
 }  // namespace ra

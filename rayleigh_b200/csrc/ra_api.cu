@@ -27,7 +27,7 @@ namespace ra {
 static void check_config(const ra_config& cfg) {
     if (cfg.n_r < 8 || (cfg.n_r & 1)) throw ArgError("n_r must be even and >= 8");
     if (cfg.l_max < 3) throw ArgError("l_max must be >= 3");
-    if (cfg.magnetism) throw ArgError("magnetism is not supported: the hydrodynamic equation set only");
+    if (cfg.magnetism && !(cfg.magnetic_prandtl > 0)) throw ArgError("magnetic_prandtl must be positive");
     if (!(cfg.aspect_ratio > 0 && cfg.aspect_ratio < 1)) throw ArgError("aspect_ratio must lie in (0, 1)");
     if (!(cfg.shell_depth > 0)) throw ArgError("shell_depth must be positive");
     if (!(cfg.dt > 0)) throw ArgError("dt must be positive");
@@ -155,6 +155,102 @@ static void reference_setup(Ctx& c) {
     R.coriolis = 2.0 / cfg.ekman;
     R.nu.assign(n, 1.0);
     R.kappa.assign(n, 1.0 / cfg.prandtl);
+    // magnetism (PDE_Coefficients.F90:418-427): Lorentz_Coeff = 1 / (Pm Ek), eta = 1 / Pm
+    R.lorentz = cfg.magnetism ? 1.0 / (cfg.magnetic_prandtl * cfg.ekman) : 0.0;
+    R.eta.assign(n, cfg.magnetism ? 1.0 / cfg.magnetic_prandtl : 0.0);
+}
+
+// The C (poloidal) and A (toroidal) systems of one l > 0 (Sphere_Linear_Terms.F90:473-499)
+// with the insulating boundaries (:1041-1077): A = 0 at both; C matched to a potential
+// field, dC/dr + l C / r = 0 at the top and dC/dr - (l + 1) C / r = 0 at the bottom.
+// coefm[NMSLOT][nr]: the Post_Solve coefficients (C,C,0) (C,C,2) (A,A,0) (A,A,1) (A,A,2).
+static void build_l_mag(const Ctx& c, int l, std::vector<double>& Cm, std::vector<double>& Am, double* coefm) {
+    const int nr = c.d.nr, rda = c.d.rda;
+    const double dt = c.dt, al = c.cfg.alpha_implicit;
+    const double lf = -dt * al, rf = dt * (1.0 - al);
+    const double* D = c.cheb_D.data();
+    const std::vector<double>& r = c.rad.radius;
+    const std::vector<double>& eta = c.rad.eta;
+    Cm.assign((size_t)nr * nr, 0.0);
+    Am.assign((size_t)nr * nr, 0.0);
+    std::fill(coefm, coefm + (size_t)NMSLOT * nr, 0.0);
+    if (l == 0) return;   // no magnetic equation at l = 0 (Sphere_Linear_Terms.F90:160-163)
+    const double llp1 = (double)l * (l + 1);
+    auto add = [&](std::vector<double>& M, int slot, int d, int i, double amp, bool stat) {
+        if (slot >= 0) coefm[(size_t)slot * nr + i] += stat ? amp : amp * rf;
+        const double fac = stat ? 1.0 : lf;
+        const double* Dd = D + (size_t)d * nr * nr;
+        for (int j = 0; j < nr; ++j) M[(size_t)i * nr + j] += amp * fac * Dd[(size_t)i * nr + j];
+    };
+    for (int i = 0; i < nr; ++i) {
+        const double H = -llp1 / (r[i] * r[i]);
+        add(Am, MS_A0, 0, i, 1.0, true);
+        add(Am, MS_A0, 0, i, H * eta[i], false);
+        add(Am, MS_A2, 2, i, 1.0 * eta[i], false);
+        add(Am, MS_A1, 1, i, 0.0, false);   // A_Diffusion_Coefs_1 (constant eta)
+        add(Cm, MS_C0, 0, i, 1.0, true);
+        add(Cm, MS_C0, 0, i, H * eta[i], false);
+        add(Cm, MS_C2, 2, i, 1.0 * eta[i], false);
+    }
+    auto clear = [&](std::vector<double>& M, int row) {
+        std::fill(M.begin() + (size_t)row * nr, M.begin() + (size_t)(row + 1) * nr, 0.0);
+    };
+    auto bc = [&](std::vector<double>& M, int row, int d, double amp) {
+        const double* Dd = D + (size_t)d * nr * nr;
+        for (int j = 0; j < rda - 1; ++j) M[(size_t)row * nr + j] += amp * Dd[(size_t)row * nr + j];
+    };
+    const int top = 0, bot = nr - 1;
+    clear(Cm, top);
+    clear(Cm, bot);
+    clear(Am, top);
+    clear(Am, bot);
+    bc(Am, top, 0, 1.0);
+    bc(Am, bot, 0, 1.0);
+    bc(Cm, top, 1, 1.0);
+    bc(Cm, top, 0, l / r[top]);
+    bc(Cm, bot, 1, 1.0);
+    bc(Cm, bot, 0, -(l + 1) / r[bot]);
+}
+
+// Finalize_EMF's radial operator (Sphere_Spectral_Space.F90:436-488, Chebyshev branch) as one
+// matrix on the collocation grid: grid -> coefficients (To_Spectral4D) -> d/dr
+// (Cheby_Deriv_Buffer_4D) -> dealias -> grid (From_Spectral4D), formed in long double.
+static void emf_matrix(const Ctx& c, std::vector<double>& M) {
+    const int n = c.d.nr, kc = c.d.kc;
+    std::vector<long double> T((size_t)n * n), Dr((size_t)n * n, 0.0L);
+    // To_Spectral4D: c_k = (2/N) sum_r f(r) cos(k theta_r), theta_r accumulated in double as
+    // Gen_Colocation_Points does (Chebyshev_Polynomials.F90:233-244)
+    std::vector<long double> th(n);
+    const double dth = M_PI / n;
+    double a = dth * 0.5;
+    for (int i = 0; i < n; ++i) {
+        th[i] = a;
+        a = a + dth;
+    }
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < n; ++i) T[(size_t)k * n + i] = 2.0L / n * cosl(k * th[i]);
+    // derivative recursion d_{N-1} = 0, d_{N-2} = 2 (N-1) c_{N-1}, d_i = d_{i+2} + 2 (i+1) c_{i+1}
+    for (int k = n - 2; k >= 0; --k) {
+        Dr[(size_t)k * n + k + 1] = 2.0L * (k + 1);
+        if (k + 2 < n)
+            for (int j = 0; j < n; ++j) Dr[(size_t)k * n + j] += Dr[(size_t)(k + 2) * n + j];
+    }
+    // grid value: sum_{k < kc} d_k cos(k theta_r) - d_0 / 2, times the derivative scaling
+    M.assign((size_t)n * n, 0.0);
+    std::vector<long double> DT((size_t)n * n, 0.0L);   // (Dr T)[k][i]
+    for (int k = 0; k < kc; ++k)
+        for (int j = 0; j < n; ++j) {
+            const long double dkj = Dr[(size_t)k * n + j];
+            if (dkj == 0.0L) continue;
+            for (int i = 0; i < n; ++i) DT[(size_t)k * n + i] += dkj * T[(size_t)j * n + i];
+        }
+    const long double sc = (long double)c.deriv_scaling;
+    for (int r = 0; r < n; ++r)
+        for (int i = 0; i < n; ++i) {
+            long double v = -0.5L * DT[i];
+            for (int k = 0; k < kc; ++k) v += DT[(size_t)k * n + i] * cosl(k * th[r]);
+            M[(size_t)r * n + i] = (double)(v * sc);
+        }
 }
 
 // One l of the implicit system: LHS (row-major) and the Post_Solve RHS coefficients.
@@ -306,6 +402,19 @@ static void linear_setup(Ctx& c) {
     RA_CUDA(cudaMemcpyAsync(c.d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_Awpt, Aall.data(), Aall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_Az, Zall.data(), Zall.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (c.mag) {
+        std::vector<double> cm((size_t)L * NMSLOT * nr), Call((size_t)L * nr * nr), Aall2((size_t)L * nr * nr);
+        std::vector<double> Cm, Am;
+        for (int l = 0; l < L; ++l) {
+            build_l_mag(c, l, Cm, Am, cm.data() + (size_t)l * NMSLOT * nr);
+            std::copy(Cm.begin(), Cm.end(), Call.begin() + (size_t)l * nr * nr);
+            std::copy(Am.begin(), Am.end(), Aall2.begin() + (size_t)l * nr * nr);
+        }
+        RA_CUDA(cudaMemcpyAsync(c.d_coef_mag, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(c.d_Ac, Call.data(), Call.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(c.d_Aa, Aall2.data(), Aall2.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));   // the host vectors go out of scope
+    }
     factor_matrices(c);
 }
 
@@ -319,6 +428,10 @@ static void autotune(Ctx& c, int nreps, double* ms_out);
 
 static void setup(Ctx& c) {
     const Dims& d = c.d;
+    c.mag = c.cfg.magnetism != 0;
+    c.nfa = c.mag ? (int)NP2A_MAG : (int)NP2A;
+    c.nfb = c.mag ? (int)NP2B_MAG : (int)NP2B;
+    c.ng = c.mag ? (int)NG_MAG : (int)NG;
     RA_CUDA(cudaSetDevice(c.cfg.device));
     RA_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.dt = c.cfg.dt;
@@ -381,6 +494,7 @@ static void setup(Ctx& c) {
         rp[R_OVER_RHORSQ * nr + i] = oor2 / c.rad.density[i];
         rp[R_DRHO_TERM * nr + i] = c.rad.dlnrho[i] + oor;
         rp[R_TWO_OVER_R * nr + i] = 2.0 / r;
+        rp[R_OVER_RSQ * nr + i] = oor2;
     }
     // device buffers
     const long nlm = d.nlm;
@@ -410,13 +524,35 @@ static void setup(Ctx& c) {
     dalloc(c.d_sol_z, (size_t)nlm * 2 * nr);
     dalloc(c.d_rhs_wpt, (size_t)nlm * 2 * 3 * nr);
     dalloc(c.d_rhs_z, (size_t)nlm * 2 * nr);
-    dalloc(c.d_ab, (size_t)4 * nlm * 2 * nr);
-    dalloc(c.d_g, (size_t)NG * nlm * 2 * nr);
+    const int nab = c.mag ? 6 : 4;   // AB history: W P T Z (C A)
+    dalloc(c.d_ab, (size_t)nab * nlm * 2 * nr);
+    dalloc(c.d_g, (size_t)c.ng * nlm * 2 * nr);
     dalloc(c.d_s2a, (size_t)nlm * NS2A * 2 * nr);
-    dalloc(c.d_s2a11, (size_t)nlm * NP2A * 2 * nr);
-    dalloc(c.d_p2a, (size_t)d.L * d.nth * NP2A * 2 * nr);
-    dalloc(c.d_p2b, (size_t)d.L * d.nth * NP2B * 2 * nr);
-    dalloc(c.d_s2b, (size_t)nlm * NP2B * 2 * nr);
+    dalloc(c.d_s2a11, (size_t)nlm * c.nfa * 2 * nr);
+    dalloc(c.d_p2a, (size_t)d.L * d.nth * c.nfa * 2 * nr);
+    dalloc(c.d_p2b, (size_t)d.L * d.nth * c.nfb * 2 * nr);
+    dalloc(c.d_s2b, (size_t)nlm * c.nfb * 2 * nr);
+    if (c.mag) {
+        const size_t plane = (size_t)nlm * 2 * nr;
+        dalloc(c.d_sol_c, plane);
+        dalloc(c.d_sol_a, plane);
+        dalloc(c.d_rhs_c, plane);
+        dalloc(c.d_rhs_a, plane);
+        dalloc(c.d_xemf, plane);
+        dalloc(c.d_s2am, (size_t)nlm * NS2AM * 2 * nr);
+        dalloc(c.d_Ac, (size_t)d.L * nr * nr);
+        dalloc(c.d_Aa, (size_t)d.L * nr * nr);
+        dalloc(c.d_perm_c, (size_t)d.L * nr);
+        dalloc(c.d_perm_a, (size_t)d.L * nr);
+        dalloc(c.d_coef_mag, (size_t)d.L * NMSLOT * nr);
+        std::vector<double> M;
+        emf_matrix(c, M);
+        dalloc(c.d_Memf, M.size());
+        RA_CUDA(cudaMemcpyAsync(c.d_Memf, M.data(), M.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_sol_c, 0, plane * sizeof(double), c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_sol_a, 0, plane * sizeof(double), c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    }
     dalloc(c.d_cfl, 1);
     dalloc(c.d_status, 1);
     RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
@@ -429,7 +565,7 @@ static void setup(Ctx& c) {
     }
     dalloc(c.d_ke_rows, (size_t)d.nth * nr + 1);
     RA_CUDA(cudaMemcpyAsync(c.d_kew, kew.data(), kew.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    RA_CUDA(cudaMemsetAsync(c.d_ab, 0, (size_t)4 * nlm * 2 * nr * sizeof(double), c.stream));
+    RA_CUDA(cudaMemsetAsync(c.d_ab, 0, (size_t)nab * nlm * 2 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_sol_wpt, 0, (size_t)nlm * 2 * 3 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemsetAsync(c.d_sol_z, 0, (size_t)nlm * 2 * nr * sizeof(double), c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_D, c.cheb_D.data(), c.cheb_D.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
@@ -477,12 +613,14 @@ static void release(Ctx& c) {
                       c.d_Awpt, c.d_Az,
                       c.d_Ainv_wpt, c.d_Ainv_z,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
-                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz, c.d_bcval};
+                      c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz, c.d_bcval,
+                      c.d_sol_c, c.d_sol_a, c.d_rhs_c, c.d_rhs_a, c.d_Ac, c.d_Aa, c.d_coef_mag, c.d_s2am,
+                      c.d_xemf, c.d_Memf};
     for (double* b : bufs)
         if (b) cudaFree(b);
     int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status,
                     c.d_perm_wpt, c.d_perm_z, c.d_skip_z, c.d_inv_sol_tiles, c.d_inv_sol_tiles_z,
-                    c.d_solve_tiles_z};
+                    c.d_solve_tiles_z, c.d_perm_c, c.d_perm_a};
     for (int* b : ibufs)
         if (b) cudaFree(b);
     if (c.d_cfl) cudaFree(c.d_cfl);
@@ -506,13 +644,19 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
     const bool mixed = c.cfg.precision == RA_PREC_MIXED;
     switch (k) {
         case 0: launch_cheb_synthesis(c); break;
-        case 1: launch_post_assemble(c, old_ab); break;
-        case 2: launch_rlm_a(c); break;
+        case 1:
+            launch_post_assemble(c, old_ab);
+            if (c.mag) launch_post_assemble_mag(c, old_ab);
+            break;
+        case 2:
+            launch_rlm_a(c);
+            if (c.mag) launch_rlm_a_mag(c);
+            break;
         case 3:
             if (mixed)
                 launch_lt_inverse_mixed(c);
             else
-                launch_lt_inverse(c, c.d_s2a11, c.d_p2a, NP2A * c.d.nr * 2);
+                launch_lt_inverse(c, c.d_s2a11, c.d_p2a, c.nfa * c.d.nr * 2);
             break;
         case 4:
             RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
@@ -522,14 +666,18 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
             if (mixed)
                 launch_lt_forward_mixed(c);
             else
-                launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+                launch_lt_forward(c, c.d_p2b, c.d_s2b, c.nfb * c.d.nr * 2);
             break;
-        case 6: launch_rlm_b(c, new_ab); break;
+        case 6:
+            launch_rlm_b(c, new_ab);
+            if (c.mag) launch_rlm_b_mag(c, new_ab);
+            break;
         default:
             if (mixed)
                 launch_solve_mixed(c);
             else
                 launch_solve(c);
+            if (c.mag) launch_solve_mag(c);
             break;
     }
 }
@@ -727,7 +875,7 @@ static void move_modes(Ctx& c, int nmodes, const int* l_of, const int* m_of, con
 static std::vector<int> knob_candidates(const Ctx& c, int knob) {
     if (knob == 0) {   // physics
         std::vector<int> v;
-        if (c.physics3_ok) {
+        if (c.physics3_ok && !c.mag) {   // the magnetic terms exist in form 1 only
             v.push_back(0);
             v.push_back(2);
         }
@@ -776,7 +924,7 @@ static void set_knob(Ctx& c, int knob, int value) {
 static void autotune(Ctx& c, int nreps, double* ms_out) {
     const size_t plane = (size_t)c.d.nlm * 2 * c.d.nr;
     if (!c.have_state) {   // give the stages finite inputs
-        RA_CUDA(cudaMemsetAsync(c.d_p2a, 0, (size_t)c.d.L * c.d.nth * NP2A * 2 * c.d.nr * sizeof(double), c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_p2a, 0, (size_t)c.d.L * c.d.nth * c.nfa * 2 * c.d.nr * sizeof(double), c.stream));
         RA_CUDA(cudaMemsetAsync(c.d_rhs_wpt, 0, 3 * plane * sizeof(double), c.stream));
         RA_CUDA(cudaMemsetAsync(c.d_rhs_z, 0, plane * sizeof(double), c.stream));
     }
@@ -973,6 +1121,39 @@ int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab) {
     });
 }
 
+int ra_put_magnetic_state(ra_ctx* ctx, const double* cpol, const double* ator, const double* ab) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!cpol || !ator) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (!c.mag) throw ArgError("the context was created without magnetism");
+        const size_t nz = (size_t)c.d.nlm * 2 * c.d.nr;
+        double* ab_ca = c.d_ab + 4 * nz;   // AB history planes 4, 5: C, A
+        RA_CUDA(cudaMemcpyAsync(c.d_sol_c, cpol, nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaMemcpyAsync(c.d_sol_a, ator, nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        if (ab) RA_CUDA(cudaMemcpyAsync(ab_ca, ab, 2 * nz * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        else RA_CUDA(cudaMemsetAsync(ab_ca, 0, 2 * nz * sizeof(double), c.stream));
+        RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+        scan_nonfinite(c, c.d_sol_c, (long)nz);
+        scan_nonfinite(c, c.d_sol_a, (long)nz);
+        if (ab) scan_nonfinite(c, ab_ca, 2L * (long)nz);
+        check_status(c);
+    });
+}
+
+int ra_get_magnetic_state(ra_ctx* ctx, double* cpol, double* ator, double* ab) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (!c.mag) throw ArgError("the context was created without magnetism");
+        const size_t nz = (size_t)c.d.nlm * 2 * c.d.nr;
+        if (cpol) RA_CUDA(cudaMemcpyAsync(cpol, c.d_sol_c, nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (ator) RA_CUDA(cudaMemcpyAsync(ator, c.d_sol_a, nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (ab) RA_CUDA(cudaMemcpyAsync(ab, c.d_ab + 4 * nz, 2 * nz * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
 int ra_put_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of, const double* wpt, const double* z,
                        const double* ab, int iteration) {
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
@@ -995,8 +1176,9 @@ int ra_get_state_modes(ra_ctx* ctx, int nmodes, const int* l_of, const int* m_of
 }
 
 int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs, double* coefs) {
-    if (!cfg || (sys != 0 && sys != 1) || nl < 1 || l0 < 0 || l0 + nl - 1 > cfg->l_max || (!lhs && !coefs))
+    if (!cfg || sys < 0 || sys > 3 || nl < 1 || l0 < 0 || l0 + nl - 1 > cfg->l_max || (!lhs && !coefs))
         return RA_ERR_ARG;
+    if (sys >= 2 && !cfg->magnetism) return RA_ERR_ARG;
     try {   // host only: the library's own Load_Linear_Coefficients + Set_Boundary_Conditions
         Ctx c;
         check_config(*cfg);
@@ -1007,16 +1189,31 @@ int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs
         chebyshev_setup(c, rmax * cfg->aspect_ratio, rmax);
         reference_setup(c);
         const int nr = c.d.nr, n = sys ? nr : 3 * nr;
-        std::vector<double> A, Z, cf((size_t)NSLOT * nr);
+        std::vector<double> A, Z, cf((size_t)NSLOT * nr), cm((size_t)NMSLOT * nr);
+        // coefficient slots of the magnetic systems: C (C,C,0) (C,C,2); A (A,A,0) (A,A,1) (A,A,2)
+        static const int kMagSlots[2][3] = {{MS_C0, MS_C2, -1}, {MS_A0, MS_A1, MS_A2}};
         for (int i = 0; i < nl; ++i) {
-            build_l(c, l0 + i, A, Z, cf.data());
-            const std::vector<double>& M = sys ? Z : A;
+            const std::vector<double>* M;
+            if (sys < 2) {
+                build_l(c, l0 + i, A, Z, cf.data());
+                M = sys ? &Z : &A;
+            } else {
+                build_l_mag(c, l0 + i, Z, A, cm.data());   // Z: C, A: A
+                M = sys == 2 ? &Z : &A;
+            }
             if (lhs) {
                 double* out = lhs + (size_t)i * n * n;   // column-major
                 for (int r = 0; r < n; ++r)
-                    for (int k = 0; k < n; ++k) out[(size_t)k * n + r] = M[(size_t)r * n + k];
+                    for (int k = 0; k < n; ++k) out[(size_t)k * n + r] = (*M)[(size_t)r * n + k];
             }
-            if (coefs) std::copy(cf.begin(), cf.end(), coefs + (size_t)i * NSLOT * nr);
+            if (coefs && sys < 2) std::copy(cf.begin(), cf.end(), coefs + (size_t)i * NSLOT * nr);
+            if (coefs && sys >= 2) {
+                const int ns = sys == 2 ? 2 : 3;
+                for (int q = 0; q < ns; ++q)
+                    std::copy(cm.begin() + (size_t)kMagSlots[sys - 2][q] * nr,
+                              cm.begin() + (size_t)(kMagSlots[sys - 2][q] + 1) * nr,
+                              coefs + ((size_t)i * ns + q) * nr);
+            }
         }
         return RA_OK;
     } catch (const ArgError&) {
@@ -1030,9 +1227,11 @@ int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coef
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        if (sys != 0 && sys != 1) throw ArgError("sys must be 0 (linked W-P-T) or 1 (Z)");
+        if (sys < 0 || sys > 3) throw ArgError("sys must be 0 (linked W-P-T), 1 (Z), 2 (C) or 3 (A)");
+        if (sys >= 2 && !c.mag) throw ArgError("systems 2 (C) and 3 (A) exist with magnetism only");
         if (!lhs && !coefs) throw ArgError("nothing to load");
         const int L = c.d.L, nr = c.d.nr, n = sys ? nr : 3 * nr;
+        double* const dst = sys == 0 ? c.d_Awpt : sys == 1 ? c.d_Az : sys == 2 ? c.d_Ac : c.d_Aa;
         if (lhs) {
             const size_t cnt = (size_t)L * n * n;
             for (size_t i = 0; i < cnt; ++i)
@@ -1043,15 +1242,29 @@ int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coef
             cudaError_t e = cudaMemcpyAsync(tmp, lhs, cnt * sizeof(double), cudaMemcpyHostToDevice, c.stream);
             if (e == cudaSuccess) {
                 dim3 grid((n + 31) / 32, (n + 31) / 32, L);
-                transpose_batch_kernel<<<grid, dim3(32, 8), 0, c.stream>>>(tmp, sys ? c.d_Az : c.d_Awpt, n);
+                transpose_batch_kernel<<<grid, dim3(32, 8), 0, c.stream>>>(tmp, dst, n);
                 e = cudaGetLastError();
             }
             if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
             cudaFree(tmp);
             if (e != cudaSuccess) throw CudaError(e, "ra_load_matrices upload", __FILE__, __LINE__);
-            c.matrices_loaded |= (sys ? 2 : 1);
+            c.matrices_loaded |= 1 << sys;
         }
-        if (coefs) {
+        if (coefs && sys >= 2) {
+            // coefs(n_r, 2 | 3 slots, l): C (C,C,0) (C,C,2); A (A,A,0) (A,A,1) (A,A,2)
+            static const int kMagSlots[2][3] = {{MS_C0, MS_C2, -1}, {MS_A0, MS_A1, MS_A2}};
+            const int ns = sys == 2 ? 2 : 3;
+            std::vector<double> h((size_t)L * NMSLOT * nr);
+            RA_CUDA(cudaMemcpy(h.data(), c.d_coef_mag, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int l = 0; l < L; ++l)
+                for (int q = 0; q < ns; ++q)
+                    for (int r = 0; r < nr; ++r) {
+                        const double v = coefs[((size_t)l * ns + q) * nr + r];
+                        if (!std::isfinite(v)) throw NonFiniteError("coefs entry is not finite");
+                        h[((size_t)l * NMSLOT + kMagSlots[sys - 2][q]) * nr + r] = v;
+                    }
+            RA_CUDA(cudaMemcpy(c.d_coef_mag, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        } else if (coefs) {
             // coefs(n_r, 16 slots, l) of this system's equations: slots of other equations are kept
             std::vector<double> h((size_t)L * NSLOT * nr);
             RA_CUDA(cudaMemcpy(h.data(), c.d_coef, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1074,7 +1287,10 @@ int ra_factor(ra_ctx* ctx, double dt) {
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
         if (!(dt > 0)) throw ArgError("dt must be positive");
-        if (c.matrices_loaded != 3) throw ArgError("ra_factor needs both systems loaded by ra_load_matrices");
+        const int need = c.mag ? 15 : 3;
+        if (c.matrices_loaded != need)
+            throw ArgError(c.mag ? "ra_factor needs the four systems (W-P-T, Z, C, A) loaded by ra_load_matrices"
+                                 : "ra_factor needs both systems loaded by ra_load_matrices");
         c.dt = dt;
         factor_matrices(c);
         if (c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(c);
@@ -1274,7 +1490,7 @@ int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* level
             if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell slice: radial index out of range");
         // the slices go through p2b, which the step rewrites before reading
         const long per = (long)c.d.nth * c.d.nphi;
-        const long room = (long)c.d.L * c.d.nth * NP2B * 2 * c.d.nr;
+        const long room = (long)c.d.L * c.d.nth * c.nfb * 2 * c.d.nr;
         if (room < per) throw ArgError("shell slice: no room for one slice");
         const int chunk = (int)std::min<long>(SliceSpec::MAXL, room / per);
         int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
@@ -1346,7 +1562,7 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
         // (quantity, level) pairs fill the 4 n_r column slots of the p2b / s2b layouts, which the
         // step rewrites before reading; each batch of slots goes through one forward transform
         const long total = (long)nq * nlev;
-        const int cap = NP2B * c.d.nr;
+        const int cap = c.nfb * c.d.nr;
         const long per = 2L * c.d.L * c.d.L;
         for (long s0 = 0; s0 < total; s0 += cap) {
             const int ns = (int)std::min<long>(cap, total - s0);
@@ -1359,7 +1575,7 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
                 launch_spectra_rows(c, S, (int)(s - s0), c.d_p2b);
                 s += S.nl;
             }
-            launch_lt_forward(c, c.d_p2b, c.d_s2b, NP2B * c.d.nr * 2);
+            launch_lt_forward(c, c.d_p2b, c.d_s2b, c.nfb * c.d.nr * 2);
             launch_spectra_gather(c, c.d_s2b, ns, c.d_p2b);
             RA_CUDA(cudaMemcpyAsync(out + s0 * per, c.d_p2b, (size_t)ns * per * sizeof(double),
                                     cudaMemcpyDeviceToHost, c.stream));
@@ -1559,19 +1775,23 @@ int ra_debug_buffer(ra_ctx* ctx, int which, double* out, long n, long* n_out) {
         const double* src = nullptr;
         long size = 0;
         switch (which) {
-            case RA_BUF_GRID: src = c.d_g; size = NG * nlm * 2 * nr; break;
+            case RA_BUF_GRID: src = c.d_g; size = c.ng * nlm * 2 * nr; break;
             case RA_BUF_S2A: src = c.d_s2a; size = nlm * NS2A * 2 * nr; break;
-            case RA_BUF_S2A11: src = c.d_s2a11; size = nlm * NP2A * 2 * nr; break;
-            case RA_BUF_P2A: src = c.d_p2a; size = L * nth * NP2A * 2 * nr; break;
-            case RA_BUF_P2B: src = c.d_p2b; size = L * nth * NP2B * 2 * nr; break;
-            case RA_BUF_S2B: src = c.d_s2b; size = nlm * NP2B * 2 * nr; break;
-            case RA_BUF_AB: src = c.d_ab; size = 4 * nlm * 2 * nr; break;
+            case RA_BUF_S2A11: src = c.d_s2a11; size = nlm * c.nfa * 2 * nr; break;
+            case RA_BUF_P2A: src = c.d_p2a; size = L * nth * c.nfa * 2 * nr; break;
+            case RA_BUF_P2B: src = c.d_p2b; size = L * nth * c.nfb * 2 * nr; break;
+            case RA_BUF_S2B: src = c.d_s2b; size = nlm * c.nfb * 2 * nr; break;
+            case RA_BUF_AB: src = c.d_ab; size = (c.mag ? 6 : 4) * nlm * 2 * nr; break;
             case RA_BUF_RHS_WPT: src = c.d_rhs_wpt; size = nlm * 2 * 3 * nr; break;
             case RA_BUF_RHS_Z: src = c.d_rhs_z; size = nlm * 2 * nr; break;
             case RA_BUF_PTAB: src = c.d_Ptab; size = nlm * c.d.nth2; break;
             case RA_BUF_IPTAB: src = c.d_iPtab; size = nlm * c.d.nth2; break;
+            case RA_BUF_S2AM: src = c.d_s2am; size = c.mag ? nlm * NS2AM * 2 * nr : 0; break;
+            case RA_BUF_RHS_C: src = c.d_rhs_c; size = c.mag ? nlm * 2 * nr : 0; break;
+            case RA_BUF_RHS_A: src = c.d_rhs_a; size = c.mag ? nlm * 2 * nr : 0; break;
             default: throw ArgError("unknown buffer id");
         }
+        if (!src) throw ArgError("this buffer exists only with magnetism");
         if (n_out) *n_out = size;
         if (!out) return;
         if (n < size) throw ArgError("output capacity too small");

@@ -61,10 +61,26 @@ enum { A_DVRDT, A_DVTDR, A_VR, A_VT, A_VP, A_DVRDR, A_DVPDR, A_OMR, A_DTDR, A_DT
 // Return-leg fields (p2b / s2b / ab): W P T Z; p2b and s2b are [..][r][field][re, im]
 constexpr int NP2B = 4;
 
+// The magnetic (dynamo) equation set adds, behind the hydrodynamic fields:
+//  grids of the Chebyshev synthesis: C C' C'' A A' A'' (g[12..17])
+enum { G_C0 = NG, G_C1, G_C2, G_A0, G_A1, G_A2, NG_MAG };
+//  spectral fields of rlm_spacea's magnetic part, s2am[row][f][r][re, im]
+enum { SM_C, SM_A, SM_C1, SM_A1, SM_C2, NS2AM };
+//  inverse-transform fields (Compute_BandCurlB, Sphere_Hybrid_Space.F90:357-435):
+//  B_r, (curl B)_r, and r sin(theta) times (curl B)_theta, (curl B)_phi, B_theta, B_phi
+enum { A_BR = NP2A, A_CBR, A_CBT, A_CBP, A_BT, A_BP, NP2A_MAG };
+//  return-leg fields in the reference's slots (Fields.F90:365-368): EMF_theta in C's,
+//  EMF_r in A's, EMF_phi after them
+enum { B_EMFT = NP2B, B_EMFR, B_EMFP, NP2B_MAG };
+//  Post_Solve coefficients of the C and A equations, coef_mag[l][slot][r]
+enum { MS_C0, MS_C2, MS_A0, MS_A1, MS_A2, NMSLOT };
+
 struct Radial {
     std::vector<double> radius, delta_r, density, dlnrho, buoy, dpdr_w, pdwdr, nu, kappa;
     std::vector<double> int_w;   // radial integration weights (a volume average over the shell)
     double coriolis;
+    std::vector<double> eta;     // magnetic diffusivity (magnetism)
+    double lorentz = 0.0;        // Lorentz_Coeff
 };
 
 struct GemmTile { int item, mt, nt, par; };
@@ -114,6 +130,8 @@ struct Ctx {
     int iteration = 1;
     bool have_state = false;
     long launches = 0;
+    bool mag = false;                                 // the magnetic equation set (C, A)
+    int nfa = NP2A, nfb = NP2B, ng = NG;              // fields of s2a11/p2a, of p2b/s2b, grids (more with mag)
 
     Radial rad;
     std::vector<double> costheta_h;     // Gauss-Legendre nodes (double)
@@ -160,6 +178,15 @@ struct Ctx {
     double *d_kew = nullptr;                          // [nth] theta weights / n_phi, then [nr] radial weights
     double *d_ke_rows = nullptr;                      // [nth][nr] kinetic-energy shares, then the sum
     double *d_kaz = nullptr;                          // [nth] 1 / n_phi (azimuthal averages)
+    // magnetic equation set
+    double *d_sol_c = nullptr, *d_sol_a = nullptr;    // [lm][2][nr] poloidal / toroidal potentials
+    double *d_rhs_c = nullptr, *d_rhs_a = nullptr;
+    double *d_Ac = nullptr, *d_Aa = nullptr;          // LU factors [L][nr][nr]
+    int *d_perm_c = nullptr, *d_perm_a = nullptr;
+    double *d_coef_mag = nullptr;                     // [L][NMSLOT][nr]
+    double *d_s2am = nullptr;                         // [row][NS2AM][nr][2]
+    double *d_xemf = nullptr;                         // [lm][2][nr] the term Finalize_EMF differentiates
+    double *d_Memf = nullptr;                         // [nr][nr] grid -> d/dr on the grid (dealiased)
 
     MixedPlan mx_inv, mx_fwd, mx_solve;               // RA_PREC_MIXED Legendre transforms, implicit solve
     LuWork lu_work;                                   // factorisation scratch
@@ -175,7 +202,8 @@ constexpr int RA_STATUS_TIMEOUT = 1;     // a bounded pipeline wait of a split-p
 constexpr int RA_STATUS_NONFINITE = 2;   // a NaN/Inf reached the right-hand side of the implicit solve
 
 // radial profile packing in d_radial: index k * nr + r
-enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R, R_COUNT };
+enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R,
+       R_OVER_RSQ, R_COUNT };
 
 // ---- kernels / launchers (defined in the .cu files) ----
 void launch_plm(Ctx& c, const double* d_x, const double* d_w);
@@ -215,6 +243,10 @@ bool physics_form1_supported(int n_theta);
 void lt_forward_prepare(Ctx& c);
 void solve_prepare(Ctx& c);
 void launch_rlm_b(Ctx& c, double new_ab);
+void launch_post_assemble_mag(Ctx& c, double old_ab);
+void launch_rlm_a_mag(Ctx& c);
+void launch_rlm_b_mag(Ctx& c, double new_ab);
+void launch_solve_mag(Ctx& c);
 void launch_solve(Ctx& c);
 void factor_matrices(Ctx& c);
 void rebuild_solve_tiles(Ctx& c);   // LU of the loaded per-l matrices (+ explicit inverses in the mixed form)

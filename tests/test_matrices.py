@@ -52,3 +52,27 @@ def test_build_matrices_argument_errors():
         rb.build_matrices(rc, 0, 5, 4)       # l beyond l_max
     with pytest.raises(rb.RayleighError):
         rb.build_matrices(rb.Config(n_r=7, l_max=7), 0, 0, 1)
+
+
+@pytest.mark.parametrize("n_r", [24, 128])
+def test_build_magnetic_matrices_match_oracle(n_r):
+    """The C (poloidal) and A (toroidal) systems of the dynamo equation set with the
+    insulating (potential-field) boundary rows (Sphere_Linear_Terms.F90:473-499, 1041-1077)
+    and their Post_Solve coefficients."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=n_r, l_max=7, dt=2e-4, ekman=1e-3, rayleigh=1e5, magnetism=True, magnetic_prandtl=5.0)
+    o = O.Oracle(O.Config(**cfg))
+    L = 8
+    rc = rb.Config(**cfg)
+    cm, cc = rb.build_matrices(rc, 2, 1, L - 1, coefs=True)
+    am, ac = rb.build_matrices(rc, 3, 1, L - 1, coefs=True)
+    C, A = O.CVAR, O.AVAR
+    for l in range(1, L):
+        for got, ref in ((cm[l - 1].T, o.mat_c[l]), (am[l - 1].T, o.mat_a[l])):
+            assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), l
+        for s, d in enumerate((0, 2)):
+            np.testing.assert_allclose(cc[l - 1, s], o.coefs[l][(O.CEQ, C, d)], rtol=1e-14, atol=1e-300)
+        for s, d in enumerate((0, 1, 2)):
+            np.testing.assert_allclose(ac[l - 1, s], o.coefs[l][(O.AEQ, A, d)], rtol=1e-14, atol=1e-300)
+    with pytest.raises(rb.RayleighError):   # no magnetic systems without magnetism
+        rb.build_matrices(rb.Config(n_r=24, l_max=7), 2, 1, 2)

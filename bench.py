@@ -2,10 +2,14 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
                     [--impl ours|reference] [--lmax 511] [--nr 192] [--err-steps 100]
+                    [--equation-set dynamo|hydro]
 
-One JSON line on rank 0.  A step is one pass of the hot path (Post_Solve,
-rlm_spacea, physical_space, rlm_spaceb, AdvanceTime) over the whole state;
-the state (~35 GB of buffers) stays resident in HBM and is far larger than L2.
+One JSON line on rank 0.  The workload is the large Boussinesq dynamo (the
+magnetic equation set: W, P, T, Z and the potentials C, A of B; Ek = 1e-5,
+Pr = Pm = 1) with seeded T and B perturbations.  A step is one pass of the hot
+path (Post_Solve, rlm_spacea, physical_space, rlm_spaceb, AdvanceTime) over the
+whole state; the state (~50 GB of buffers) stays resident in HBM and is far
+larger than L2.
 By default both forms run from the same seeded state: the line reports the
 mixed-precision step, with the FP64 step and the per-field relative error of
 the mixed state against the FP64 state after --err-steps steps beside it (the
@@ -38,14 +42,36 @@ METRIC = "steps/s at lmax=511,N_r=192: mixed-prec vs FP64 GPU at rel err≤1e-9;
 SEED = 0x5241594C
 
 
-def headline_config(lmax, nr, precision):
-    """Boussinesq rotating convection (hydrodynamic) on an l_max x N_r grid; the
-    default l_max = 511, N_r = 192 is the size the reference's largest
-    benchmark case runs at."""
+def headline_config(lmax, nr, precision, mag=True):
+    """The large Boussinesq dynamo: rotating convection with the magnetic equation set
+    (C, A potentials; insulating boundaries), radius ratio 0.35, Ek = 1e-5, Pr = Pm = 1,
+    on an l_max x N_r grid (default l_max = 511, N_r = 192).  mag=False gives the same
+    case without the magnetic field (the hydrodynamic equation set)."""
     return dict(n_r=nr, l_max=lmax, aspect_ratio=0.35, shell_depth=1.0, rayleigh=2.0e8, ekman=1.0e-5,
-                prandtl=1.0, gravity_power=1.0, rotation=True, no_slip_top=True, no_slip_bottom=True,
-                fix_tvar_top=True, fix_tvar_bottom=True, t_top=0.0, t_bottom=1.0, dt=1.0e-6,
-                precision=precision)
+                prandtl=1.0, magnetic_prandtl=1.0, gravity_power=1.0, rotation=True, magnetism=mag,
+                no_slip_top=True, no_slip_bottom=True, fix_tvar_top=True, fix_tvar_bottom=True, t_top=0.0,
+                t_bottom=1.0, dt=1.0e-6, precision=precision)
+
+
+def workload_name(lmax, nr, mag):
+    return f"boussinesq_{'dynamo' if mag else 'rotating_convection'}_lmax{lmax}_nr{nr}"
+
+
+def initial_magnetic_state(ctx, lmax, nr, rng):
+    """Seeded B: poloidal and toroidal potentials C, A on l in [1, 20], amplitude 1e-3 (l+1)^-2,
+    as Chebyshev coefficients on the first 16 modes (m = 0 imaginary parts zero)."""
+    n_lm = (lmax + 1) * (lmax + 2) // 2
+    out = []
+    ncoef = min(16, nr // 2)
+    for _ in range(2):
+        a = np.zeros((n_lm, 2, nr))
+        for l in range(1, min(20, lmax) + 1):
+            s = l * (l + 1) // 2
+            block = rng.standard_normal((l + 1, 2, ncoef)) * 1e-3 * (l + 1.0) ** -2 / (1.0 + np.arange(ncoef)) ** 2
+            block[0, 1] = 0.0
+            a[s:s + l + 1, :, :ncoef] = block
+        out.append(a)
+    return out
 
 
 def initial_state(ctx, lmax, nr, rng):
@@ -70,22 +96,31 @@ def initial_state(ctx, lmax, nr, rng):
 # ---------------------------------------------------------------------------
 # algorithmic work per kernel (one launch = one step), FP64
 # ---------------------------------------------------------------------------
-def kernel_work(lmax, nr, nth):
+def kernel_work(lmax, nr, nth, mag=True):
+    """Algorithmic work of each stage per step: FLOPs (2 M N K per product) for the products,
+    bytes (one read of the inputs, one write of the outputs) for the rest.  The magnetic set
+    adds 6 fields to the inverse transform and the physical-space input (17 + 3 d/dphi),
+    3 to the forward transform (7), 6 grids to the synthesis (18) and 2 per-l N_r x N_r solves."""
     L = lmax + 1
     n_lm = L * (L + 1) // 2
     nth2 = nth // 2
     kc = (2 * nr) // 3
     cols = 2 * n_lm
+    nfa, nfb, ng = (17, 7, 18) if mag else (11, 4, 12)
     w = {}
-    w["lt_inverse"] = ("tensor", 2.0 * nth2 * (11 * nr * 2) * n_lm)
-    w["lt_forward"] = ("tensor", 2.0 * nth2 * (4 * nr * 2) * n_lm)
-    w["cheb_synthesis"] = ("tensor", 12 * 2.0 * (nr // 2) * kc * cols)
-    w["solve"] = ("tensor", 2.0 * (9 + 1) * nr * nr * cols)
+    w["lt_inverse"] = ("tensor", 2.0 * nth2 * (nfa * nr * 2) * n_lm)
+    w["lt_forward"] = ("tensor", 2.0 * nth2 * (nfb * nr * 2) * n_lm)
+    w["cheb_synthesis"] = ("tensor", ng * 2.0 * (nr // 2) * kc * cols)
+    w["solve"] = ("tensor", 2.0 * (9 + 1 + (2 if mag else 0)) * nr * nr * cols)
     plane = n_lm * 2 * nr * 8.0
-    w["post_assemble"] = ("hbm", (12 + 4 + 4 + 7) * plane)
-    w["rlm_a"] = ("hbm", (7 + 11) * plane)
-    w["rlm_b"] = ("hbm", (4 + 4 + 8) * plane)   # s2b in, ab out, rhs read and written
-    w["physics"] = ("hbm", L * nth * (11 + 4) * nr * 2 * 8.0)
+    # post_assemble: grids + AB in, RHS + s2a out; magnetism: 6 grids + 2 AB in, 2 RHS + 5 s2am out
+    w["post_assemble"] = ("hbm", ((12 + 4 + 4 + 7) + (15 if mag else 0)) * plane)
+    # rlm_a: s2a in, s2a11 out; magnetism: s2am (5) in, 6 fields out
+    w["rlm_a"] = ("hbm", ((7 + 11) + (11 if mag else 0)) * plane)
+    # rlm_b: s2b in, ab out, rhs read and written; magnetism: 3 EMF fields in, C and A
+    # histories, X written and read, the C and A right-hand sides read and written
+    w["rlm_b"] = ("hbm", ((4 + 4 + 8) + (13 if mag else 0)) * plane)
+    w["physics"] = ("hbm", L * nth * (nfa + nfb) * nr * 2 * 8.0)
     return w
 
 
@@ -180,12 +215,14 @@ class CpuSample:
     seconds of each stage and the factor that scales it to the whole stage are
     reported separately; the full-step estimate is their dot product."""
 
-    def __init__(self, lmax, nr, stride=32, ntheta_rows=4):
+    def __init__(self, lmax, nr, stride=32, ntheta_rows=4, mag=True):
         import oracle as O
         self.O = O
+        self.mag = mag
         self.cores = os.cpu_count()
         O.set_fft_workers(self.cores)
-        cfg = O.Config(**{k: v for k, v in headline_config(lmax, nr, 0).items() if k in O.Config.__dataclass_fields__})
+        cfg = O.Config(**{k: v for k, v in headline_config(lmax, nr, 0, mag).items()
+                          if k in O.Config.__dataclass_fields__})
         t0 = time.perf_counter()
         self.o = O.Oracle(cfg)
         self.init_s = time.perf_counter() - t0
@@ -202,15 +239,17 @@ class CpuSample:
         self.scale = {"post_solve": 1 / f_l, "rlm_a": 1 / f_m, "lt_inverse": 1 / f_m, "physics": 1 / f_t,
                       "lt_forward": 1 / f_m, "rlm_b": 1 / f_m, "solve": 1 / f_l}
         rng = np.random.Generator(np.random.PCG64(SEED))
-        self.s2a = {m: rng.standard_normal((8, 2, nr, L - m)) for m in self.ms}
-        self.s2a12 = {m: rng.standard_normal((12, 2, nr, L - m)) for m in self.ms}
-        self.p2b = {m: rng.standard_normal((4, 2, nr, cfg.n_theta)) for m in self.ms}
-        self.s2b = {m: rng.standard_normal((4, 2, nr, L - m)) for m in self.ms}
-        self.p3a = rng.standard_normal((12, ntheta_rows, nr, cfg.n_phi + 2))
+        o = self.o
+        self.s2a = {m: rng.standard_normal((o.NF1A, 2, nr, L - m)) for m in self.ms}
+        self.s2a12 = {m: rng.standard_normal((o.NF2A, 2, nr, L - m)) for m in self.ms}
+        self.p2b = {m: rng.standard_normal((o.NFB, 2, nr, cfg.n_theta)) for m in self.ms}
+        self.s2b = {m: rng.standard_normal((o.NFB, 2, nr, L - m)) for m in self.ms}
+        self.p3a = rng.standard_normal((o.NF2A, ntheta_rows, nr, cfg.n_phi + 2))
         lm_idx = np.concatenate([np.arange(l * (l + 1) // 2, l * (l + 1) // 2 + l + 1) for l in self.ls])
         self.lm_idx = lm_idx
-        self.c = rng.standard_normal((4, len(lm_idx), 2, nr))
-        self.ab = rng.standard_normal((4, len(lm_idx), 2, nr))
+        nv = 6 if mag else 4
+        self.c = rng.standard_normal((nv, len(lm_idx), 2, nr))
+        self.ab = rng.standard_normal((nv, len(lm_idx), 2, nr))
         self.rhs = {l: rng.standard_normal((3 * nr, 2 * (l + 1))) for l in self.ls}
         self.rhsz = {l: rng.standard_normal((nr, 2 * (l + 1))) for l in self.ls}
         self.sample = (f"per step: Post_Solve on l = {self.ls[0]}::{stride} ({f_l:.3f} of the (l,m) columns), "
@@ -226,13 +265,20 @@ class CpuSample:
         # Post_Solve: radial derivatives, From_Spectral, Add_Derivative on the sampled columns
         t0 = time.perf_counter()
         c = cg.dealias(self.c)
-        W, P, T, Z = c
-        ctemp = cg.from_spectral(cg.dealias(np.stack([cg.deriv(W, 3), cg.deriv(P, 1), cg.deriv(T, 2), cg.deriv(Z, 2)])))
-        g = cg.from_spectral(cg.dealias(np.stack([W, P, T, Z, cg.deriv(W, 1), cg.deriv(T, 1), cg.deriv(Z, 1),
-                                                  cg.deriv(W, 2)])))
+        W, P, T, Z = c[:4]
+        ct = [cg.deriv(W, 3), cg.deriv(P, 1), cg.deriv(T, 2), cg.deriv(Z, 2)]
+        gl = [W, P, T, Z, cg.deriv(W, 1), cg.deriv(T, 1), cg.deriv(Z, 1), cg.deriv(W, 2)]
+        if self.mag:
+            C, A = c[4], c[5]
+            ct.append(cg.deriv(A, 2))
+            gl += [C, A, cg.deriv(C, 1), cg.deriv(A, 1), cg.deriv(C, 2)]
+        ctemp = cg.from_spectral(cg.dealias(np.stack(ct)))
+        g = cg.from_spectral(cg.dealias(np.stack(gl)))
         p1b = self.ab * 0.5
         src = {(0, 0): g[0], (0, 1): g[4], (0, 2): g[7], (0, 3): ctemp[0], (1, 0): g[1], (1, 1): ctemp[1],
                (2, 0): g[2], (2, 1): g[5], (2, 2): ctemp[2], (3, 0): g[3], (3, 1): g[6], (3, 2): ctemp[3]}
+        if self.mag:
+            src.update({(4, 0): g[8], (4, 2): g[12], (5, 0): g[9], (5, 1): g[11], (5, 2): ctemp[4]})
         off = 0
         for l in self.ls:
             sl = slice(off, off + l + 1)
@@ -257,10 +303,15 @@ class CpuSample:
         o.rlm_spaceb(self.s2b, ms=self.ms)
         t["rlm_b"] = time.perf_counter() - t0
         t0 = time.perf_counter()
+        if self.mag:   # Finalize_EMF's radial derivative on the sampled columns (AdvanceTime)
+            cg.from_spectral(cg.dealias(cg.deriv(cg.to_spectral(self.c[5]), 1)))
         for l in self.ls:
             sla.lu_solve(o.lu_wpt[l], self.rhs[l], check_finite=False)
             if l > 0:
                 sla.lu_solve(o.lu_z[l], self.rhsz[l], check_finite=False)
+                if self.mag:
+                    sla.lu_solve(o.lu_c[l], self.rhsz[l], check_finite=False)
+                    sla.lu_solve(o.lu_a[l], self.rhsz[l], check_finite=False)
         t["solve"] = time.perf_counter() - t0
         return t
 
@@ -301,7 +352,8 @@ def run_reference(args, rank):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-    cs = CpuSample(args.lmax, args.nr)
+    mag = args.equation_set == "dynamo"
+    cs = CpuSample(args.lmax, args.nr, mag=mag)
     for _ in range(args.warmup):
         cs.step_seconds()
     timed = [cs.step_seconds() for _ in range(args.steps)]
@@ -314,8 +366,9 @@ def run_reference(args, rank):
         # the time actually spent per timed (sampled) step; value is the full-step estimate
         "ms_per_step": cpu["timed_seconds_per_sampled_step"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
+        "config": {"workload": workload_name(args.lmax, args.nr, mag), "l_max": args.lmax,
                    "n_r": args.nr, "n_theta": cs.cfg.n_theta, "n_phi": cs.cfg.n_phi,
+                   "equation_set": "dynamo (W, P, T, Z, C, A)" if mag else "hydrodynamic (W, P, T, Z)",
                    "l2": "working set larger than L2"},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -345,11 +398,15 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     import rayleigh_b200 as rb
     local = int(os.environ.get("LOCAL_RANK", "0"))
     prec = rb.PREC_MIXED if prec_name == "mixed" else rb.PREC_FP64
-    cfgd = headline_config(args.lmax, args.nr, prec)
+    mag = args.equation_set == "dynamo"
+    cfgd = headline_config(args.lmax, args.nr, prec, mag)
     ctx = rb.Rayleigh(rb.Config(**cfgd, use_graph=True, device=local))
     rng = np.random.Generator(np.random.PCG64(SEED + rank))
     wpt, z = initial_state(ctx, args.lmax, args.nr, rng)
     ctx.put_state(wpt, z, None, iteration=1)
+    if mag:
+        cpol, ator = initial_magnetic_state(ctx, args.lmax, args.nr, rng)
+        ctx.put_magnetic_state(cpol, ator)
     # warm-up (includes the Euler first step and the capture of the step graph)
     ctx.step(max(3, args.warmup))
     if world > 1:
@@ -370,7 +427,7 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     done = max(3, args.warmup) + args.steps + nk_steps
     if args.err_steps > done:
         ctx.step(args.err_steps - done)
-    state = ctx.get_state()[:2] if rank == 0 else None
+    state = (ctx.get_state()[:2] + (ctx.get_magnetic_state()[:2] if mag else ())) if rank == 0 else None
 
     # end to end through the C ABI with host buffers: H2D of the full state, one
     # step, D2H of the new state and its CFL cargo, every step
@@ -383,6 +440,11 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     h_wpt[:] = w0.ravel()
     h_z[:] = z0.ravel()
     h_ab[:] = ab0.ravel()
+    if mag:   # the magnetic part: C, A and their AB terms, both ways
+        hm = [pin(n_lm * 2 * nr), pin(n_lm * 2 * nr), pin(2 * n_lm * 2 * nr)]
+        om = [pin(n_lm * 2 * nr), pin(n_lm * 2 * nr), pin(2 * n_lm * 2 * nr)]
+        for dst, src in zip(hm, ctx.get_magnetic_state()):
+            dst[:] = src.ravel()
     lib = ctx.lib
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     e2e_steps = max(1, min(args.steps, 5))
@@ -391,19 +453,25 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         ctx._check(lib.ra_put_state(ctx.h, P(h_wpt), P(h_z), P(h_ab), it))
+        if mag:
+            ctx._check(lib.ra_put_magnetic_state(ctx.h, P(hm[0]), P(hm[1]), P(hm[2])))
         ctx._check(lib.ra_step(ctx.h, 1, ctypes.byref(cfl)))
         ctx._check(lib.ra_get_state(ctx.h, P(o_wpt), P(o_z), P(o_ab)))
+        if mag:
+            ctx._check(lib.ra_get_magnetic_state(ctx.h, P(om[0]), P(om[1]), P(om[2])))
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    h2d = (h_wpt.nbytes + h_z.nbytes + h_ab.nbytes)
-    d2h = (o_wpt.nbytes + o_z.nbytes + o_ab.nbytes + 8)
+    h2d = (h_wpt.nbytes + h_z.nbytes + h_ab.nbytes) + (sum(a.nbytes for a in hm) if mag else 0)
+    d2h = (o_wpt.nbytes + o_z.nbytes + o_ab.nbytes + 8) + (sum(a.nbytes for a in om) if mag else 0)
     e2e_value = world / max_over_ranks(e2e_s, world, dist, torch, "cuda")
     n_theta, n_phi = ctx.n_theta, ctx.n_phi
     ctx.close()
     del h_wpt, h_z, h_ab, o_wpt, o_z, o_ab
+    if mag:
+        del hm, om
     if rank != 0:
         return None, None
     # roofline of the dominant kernel
-    work = kernel_work(args.lmax, args.nr, n_theta)
+    work = kernel_work(args.lmax, args.nr, n_theta, mag)
     dom = max(per_kernel, key=lambda k: per_kernel[k])
     bound, amount = work[dom]
     avg_s = per_kernel[dom] / nk_steps * 1e-3
@@ -413,7 +481,7 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     if os.path.exists(tpath):
         try:
             tj = json.load(open(tpath))
-            traffic = tj.get(f"{dom}_{prec_name}_lmax{args.lmax}_nr{args.nr}")
+            traffic = tj.get(f"{dom}_{args.equation_set}_{prec_name}_lmax{args.lmax}_nr{args.nr}")
             binding = tj.get(f"{dom}_binding_unit")   # the unit ncu shows saturated, when it is not HBM
         except Exception:
             traffic = None
@@ -442,11 +510,13 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
         "value": value, "ms_per_step": max_ms / args.steps, "precision": prec_name,
         "timing": f"value: {args.steps} steps replayed from the captured step graph, CUDA events on the context "
                   f"stream; kernels: {nk_steps} eager steps with an event around each kernel",
-        "config": {"workload": f"boussinesq_rotating_convection_lmax{args.lmax}_nr{args.nr}", "l_max": args.lmax,
+        "config": {"workload": workload_name(args.lmax, args.nr, mag), "l_max": args.lmax,
                    "n_r": args.nr, "n_theta": n_theta, "n_phi": n_phi, "ekman": cfgd["ekman"],
-                   "dt": cfgd["dt"], "l2": "working set (~35 GB) larger than L2; no flush needed",
-                   "equation_set": "hydrodynamic (W, P, T, Z) on the dynamo case's grid; the magnetic "
-                                   "fields C, A of the dynamo case are not built",
+                   "rayleigh": cfgd["rayleigh"], "prandtl": cfgd["prandtl"],
+                   "magnetic_prandtl": cfgd["magnetic_prandtl"] if mag else None, "dt": cfgd["dt"],
+                   "l2": "working set (~50 GB) larger than L2; no flush needed",
+                   "equation_set": "dynamo (W, P, T, Z, C, A; insulating boundaries)" if mag
+                                   else "hydrodynamic (W, P, T, Z)",
                    "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                      "frac": achieved / peak if peak else None, "traffic": traffic,
@@ -464,10 +534,14 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
 
 
 def _field_errors(mixed_state, fp64_state, nr):
-    (wm, zm), (wf, zf) = mixed_state, fp64_state
+    wm, zm = mixed_state[:2]
+    wf, zf = fp64_state[:2]
+    pairs = [("W", wm[:, :, :nr], wf[:, :, :nr]), ("P", wm[:, :, nr:2 * nr], wf[:, :, nr:2 * nr]),
+             ("T", wm[:, :, 2 * nr:], wf[:, :, 2 * nr:]), ("Z", zm, zf)]
+    if len(mixed_state) == 4:
+        pairs += [("C", mixed_state[2], fp64_state[2]), ("A", mixed_state[3], fp64_state[3])]
     out = {}
-    for name, a, b in (("W", wm[:, :, :nr], wf[:, :, :nr]), ("P", wm[:, :, nr:2 * nr], wf[:, :, nr:2 * nr]),
-                       ("T", wm[:, :, 2 * nr:], wf[:, :, 2 * nr:]), ("Z", zm, zf)):
+    for name, a, b in pairs:
         den = float(np.linalg.norm(b))
         out[name] = float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a))
     return out
@@ -515,7 +589,7 @@ def run_ours(args, rank, world, torch, dist):
     if args.c1:
         line["c1_measured"] = c1_comparison(args, torch)
     if not args.no_cpu:
-        cs = CpuSample(args.lmax, args.nr)
+        cs = CpuSample(args.lmax, args.nr, mag=args.equation_set == "dynamo")
         cs.step_seconds()
         line["cpu_baseline"] = cs.report([cs.step_seconds()])
     print(json.dumps(line), flush=True)
@@ -552,6 +626,8 @@ def main():
                     help="steps after which the mixed and FP64 states are compared")
     ap.add_argument("--lmax", type=int, default=511)
     ap.add_argument("--nr", type=int, default=192)
+    ap.add_argument("--equation-set", default="dynamo", choices=["dynamo", "hydro"],
+                    help="dynamo: the magnetic equation set (the large Boussinesq dynamo); hydro: without B")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-c1", dest="c1", action="store_false",
                     help="skip the whole-step GPU/CPU comparison at the l_max = 63, N_r = 48 size")

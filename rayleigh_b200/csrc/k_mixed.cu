@@ -178,8 +178,9 @@ static void setup_solve(Ctx& c) {
     const int L = d.L, nr = d.nr;
     MixedPlan& p = c.mx_solve;
     const int kseg = oz_ksteps(nr);   // K-steps of one radial block
+    const int nsys = c.mag ? 4 : 2;   // W-P-T, Z (and C, A with magnetism)
     long asize = 0, bsize = 0, esize_a = 0, esize_b = 0;
-    for (int sys = 0; sys < 2; ++sys) {
+    for (int sys = 0; sys < nsys; ++sys) {
         const int n = sys ? nr : 3 * nr, nseg = sys ? 1 : 3;
         const int nta = oz_tiles_of(n, OZ_HA), nks = nseg * kseg;
         asize += (long)L * nta * nks * OZ_ABLK;
@@ -197,12 +198,13 @@ static void setup_solve(Ctx& c) {
     std::vector<OzProblem> probs;
     long ao = 0, bo = 0, eao = 0, ebo = 0;
     int max_a = 0, max_b = 0;
-    for (int sys = 0; sys < 2; ++sys) {
+    for (int sys = 0; sys < nsys; ++sys) {
         const int n = sys ? nr : 3 * nr, nseg = sys ? 1 : 3;
         const int nta = oz_tiles_of(n, OZ_HA), nks = nseg * kseg;
-        const double* Ainv = sys ? c.d_Ainv_z : c.d_Ainv_wpt;   // transposed: (i, k) at [k][i]
-        const double* rhs = sys ? c.d_rhs_z : c.d_rhs_wpt;
-        double* sol = sys ? c.d_sol_z : c.d_sol_wpt;
+        // transposed inverses: (i, k) at [k][i]
+        const double* Ainv = sys == 0 ? c.d_Ainv_wpt : sys == 1 ? c.d_Ainv_z : sys == 2 ? c.d_Ainv_c : c.d_Ainv_a;
+        const double* rhs = sys == 0 ? c.d_rhs_wpt : sys == 1 ? c.d_rhs_z : sys == 2 ? c.d_rhs_c : c.d_rhs_a;
+        double* sol = sys == 0 ? c.d_sol_wpt : sys == 1 ? c.d_sol_z : sys == 2 ? c.d_sol_c : c.d_sol_a;
         max_a = std::max(max_a, nta * OZ_HA);
         for (int l = 0; l < L; ++l) {
             const long lstart = (long)l * (l + 1) / 2;

@@ -820,6 +820,13 @@ void factor_matrices(Ctx& c) {
         launch_lu_solve(c.stream, c.d_inv_sol_tiles, c.n_inv_sol_tiles, s0, LU_MODE_INVERSE, 0, c.solve_nc);
         launch_lu_solve(c.stream, c.d_inv_sol_tiles_z, c.n_inv_sol_tiles_z, s1, LU_MODE_INVERSE, 0, c.solve_nc_z);
         c.launches += 2;
+        if (c.mag) {   // the C and A systems go through the split products too
+            const LuSys sc{c.d_Ac, c.d_perm_c, nullptr, c.d_Ainv_c, nr};
+            const LuSys sa{c.d_Aa, c.d_perm_a, nullptr, c.d_Ainv_a, nr};
+            launch_lu_solve(c.stream, c.d_inv_sol_tiles_z, c.n_inv_sol_tiles_z, sc, LU_MODE_INVERSE, 0, c.solve_nc_z);
+            launch_lu_solve(c.stream, c.d_inv_sol_tiles_z, c.n_inv_sol_tiles_z, sa, LU_MODE_INVERSE, 0, c.solve_nc_z);
+            c.launches += 2;
+        }
     }
     RA_CUDA(cudaStreamSynchronize(c.stream));
 }

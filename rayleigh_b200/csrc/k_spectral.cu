@@ -292,11 +292,59 @@ __device__ __forceinline__ void ml_of_row(long row, int L, int& m, int& l) {
     l = mm + (p < ne ? 2 * p : 2 * (p - ne) + 1);
 }
 
-__global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __restrict__ s2a,
+// Compute_BandCurlB (Sphere_Hybrid_Space.F90:357-435): B and curl B in (l, m) space from
+// C, A, C', A', C'' (the l_max mode zeroed on entry and exit, as for the hydrodynamic fields):
+//   B_r = l(l+1) C / r^2,  (curl B)_r = l(l+1) A / r^2,  X = C'' - B_r,
+//   r sin(theta) (curl B)_theta = d_theta A' - d_phi X,  r sin(theta) (curl B)_phi = d_phi A' + d_theta X,
+//   r sin(theta) B_theta = d_phi A + d_theta C',          r sin(theta) B_phi = d_phi C' - d_theta A,
+// with d_theta = sin(theta) d/dtheta through the l -+ 1 couplings (fields A_BR .. A_BP).
+__device__ __forceinline__ void band_curl_b(const double* __restrict__ s2am, const double* __restrict__ radial,
+                                            int nr, int L, int l, int m, int r, double (*out)[2]) {
+    const int lmax = L - 1;
+    const long fsz = 2L * nr;
+    const long rsz = (long)NS2AM * fsz;
+    auto get2 = [&](int f, int ll) -> double2 {
+        if (ll < m || ll >= lmax) return make_double2(0.0, 0.0);
+        return __ldg(reinterpret_cast<const double2*>(s2am + row_index(m, ll, L) * rsz + f * fsz + r * 2));
+    };
+    const double orsq = radial[R_OVER_RSQ * nr + r];
+    const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
+    const double llp1 = (double)l * (l + 1);
+    const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
+    const double2 C = get2(SM_C, l), A = get2(SM_A, l), C1 = get2(SM_C1, l), A1 = get2(SM_A1, l);
+    const double2 C2 = get2(SM_C2, l);
+    const double2 Cm = get2(SM_C, l - 1), Cp = get2(SM_C, l + 1), C2m = get2(SM_C2, l - 1), C2p = get2(SM_C2, l + 1);
+    const double2 Am = get2(SM_A, l - 1), Ap = get2(SM_A, l + 1), A1m = get2(SM_A1, l - 1), A1p = get2(SM_A1, l + 1);
+    const double2 C1m = get2(SM_C1, l - 1), C1p = get2(SM_C1, l + 1);
+    auto c = [](double2 v, int ri) { return ri ? v.y : v.x; };
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+        const double sg = ri ? (double)m : -(double)m;   // d/dphi: (re, im) -> (-m im, m re)
+        const int rj = 1 - ri;
+        const double br = llp1 * c(C, ri) * orsq;
+        const double xj = c(C2, rj) - llp1 * c(C, rj) * orsq;    // X at l, the other part
+        const double xm = c(C2m, ri) - llm * c(Cm, ri) * orsq;   // X at l - 1, l + 1
+        const double xp = c(C2p, ri) - llq * c(Cp, ri) * orsq;
+        out[0][ri] = br;
+        out[1][ri] = llp1 * c(A, ri) * orsq;
+        out[2][ri] = (c(A1m, ri) * c1 + c(A1p, ri) * c2) - sg * xj;
+        out[3][ri] = sg * c(A1, rj) + (xm * c1 + xp * c2);
+        out[4][ri] = sg * c(A, rj) + (c(C1m, ri) * c1 + c(C1p, ri) * c2);
+        out[5][ri] = sg * c(C1, rj) - (c(Am, ri) * c1 + c(Ap, ri) * c2);
+    }
+}
+
+// MAG: the magnetic fields are formed by the same thread (band_curl_b) and stored with the
+// hydrodynamic ones, the 17 fields of a radius as one contiguous record.
+template <bool MAG>
+__global__ void __launch_bounds__(MAG ? 128 : RLM_A_THREADS, MAG ? 3 : 1) rlm_a_kernel(const double* __restrict__ s2a,
+                                                             const double* __restrict__ s2am,
                                                              double* __restrict__ s2o,
                                                              const double* __restrict__ radial, long nlm, int nr,
                                                              int L, int nfa) {
-    __shared__ double2 stage[RLM_A_THREADS * NP2A];   // the block's outputs, re-read for coalesced stores
+    constexpr int NF = MAG ? (int)NP2A_MAG : (int)NP2A;
+    constexpr int NT = MAG ? 128 : RLM_A_THREADS;
+    __shared__ double2 stage[NT * NF];   // the block's outputs, re-read for coalesced stores
     const long total = nlm * nr;
     const long idx0 = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (row, r)
     const bool valid = idx0 < total;
@@ -338,7 +386,8 @@ __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __re
     const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
     const double llp1 = (double)l * (l + 1);
     const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
-    double out[NP2A][2];
+    double out[NF][2];
+    if constexpr (MAG) band_curl_b(s2am, radial, nr, L, l, m, r, out + NP2A);
 #pragma unroll
     for (int ri = 0; ri < 2; ++ri) {
         const double sg = ri ? (double)m : -(double)m;   // d/dphi: (re, im) -> (-m im, m re)
@@ -379,15 +428,15 @@ __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __re
     // stages its outputs in shared memory and stores them as consecutive
     // 16-byte chunks, so each store instruction covers a few whole lines.
     const int lane = threadIdx.x & 31;
-    double2* st = stage + (threadIdx.x - lane) * NP2A;
+    double2* st = stage + (threadIdx.x - lane) * NF;
 #pragma unroll
-    for (int f = 0; f < NP2A; ++f)
-        st[lane * NP2A + f] = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
+    for (int f = 0; f < NF; ++f)
+        st[lane * NF + f] = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
     __syncwarp();
-    const long obase = row_index(m, l, L) * (long)nfa * fsz + (long)r * (2 * nfa);   // nfa >= NP2A fields per radius
+    const long obase = row_index(m, l, L) * (long)nfa * fsz + (long)r * (2 * nfa);   // nfa == NF fields per radius
 #pragma unroll
-    for (int i = 0; i < NP2A; ++i) {
-        const int ci = i * 32 + lane, sl = ci / NP2A, f = ci - sl * NP2A;
+    for (int i = 0; i < NF; ++i) {
+        const int ci = i * 32 + lane, sl = ci / NF, f = ci - sl * NF;
         const long b = __shfl_sync(0xffffffffu, obase, sl);
         const int ok = __shfl_sync(0xffffffffu, (int)valid, sl);
         if (ok) *reinterpret_cast<double2*>(s2o + b + f * 2) = st[ci];
@@ -396,72 +445,13 @@ __global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_kernel(const double* __re
 
 void launch_rlm_a(Ctx& c) {
     const long total = c.d.nlm * c.d.nr;
-    rlm_a_kernel<<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
-        c.d_s2a, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
-    RA_CUDA(cudaGetLastError());
-    ++c.launches;
-}
-
-// Compute_BandCurlB (Sphere_Hybrid_Space.F90:357-435): B and curl B in (l, m) space from
-// C, A, C', A', C'' (the l_max mode zeroed on entry and exit, as for the hydrodynamic fields):
-//   B_r = l(l+1) C / r^2,  (curl B)_r = l(l+1) A / r^2,  X = C'' - B_r,
-//   r sin(theta) (curl B)_theta = d_theta A' - d_phi X,  r sin(theta) (curl B)_phi = d_phi A' + d_theta X,
-//   r sin(theta) B_theta = d_phi A + d_theta C',          r sin(theta) B_phi = d_phi C' - d_theta A,
-// with d_theta = sin(theta) d/dtheta through the l -+ 1 couplings; written into fields
-// A_BR .. A_BP of s2a11.
-__global__ void __launch_bounds__(RLM_A_THREADS) rlm_a_mag_kernel(const double* __restrict__ s2am,
-                                                                 double* __restrict__ s2o,
-                                                                 const double* __restrict__ radial, long nlm,
-                                                                 int nr, int L, int nfa) {
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (row, r)
-    if (idx >= nlm * nr) return;
-    const int r = (int)(idx % nr);
-    int l, m;
-    ml_of_row(idx / nr, L, m, l);
-    const int lmax = L - 1;
-    const long fsz = 2L * nr;
-    const long rsz = (long)NS2AM * fsz;
-    auto get2 = [&](int f, int ll) -> double2 {
-        if (ll < m || ll >= lmax) return make_double2(0.0, 0.0);
-        return __ldg(reinterpret_cast<const double2*>(s2am + row_index(m, ll, L) * rsz + f * fsz + r * 2));
-    };
-    const double orsq = radial[R_OVER_RSQ * nr + r];
-    const double c1 = dth_c1(l, m), c2 = dth_c2(l, m);
-    const double llp1 = (double)l * (l + 1);
-    const double llm = (double)(l - 1) * l, llq = (double)(l + 1) * (l + 2);
-    const double2 C = get2(SM_C, l), A = get2(SM_A, l), C1 = get2(SM_C1, l), A1 = get2(SM_A1, l);
-    const double2 C2 = get2(SM_C2, l);
-    const double2 Cm = get2(SM_C, l - 1), Cp = get2(SM_C, l + 1), C2m = get2(SM_C2, l - 1), C2p = get2(SM_C2, l + 1);
-    const double2 Am = get2(SM_A, l - 1), Ap = get2(SM_A, l + 1), A1m = get2(SM_A1, l - 1), A1p = get2(SM_A1, l + 1);
-    const double2 C1m = get2(SM_C1, l - 1), C1p = get2(SM_C1, l + 1);
-    auto c = [](double2 v, int ri) { return ri ? v.y : v.x; };
-    double out[6][2];
-#pragma unroll
-    for (int ri = 0; ri < 2; ++ri) {
-        const double sg = ri ? (double)m : -(double)m;   // d/dphi: (re, im) -> (-m im, m re)
-        const int rj = 1 - ri;
-        const double br = llp1 * c(C, ri) * orsq;
-        const double xj = c(C2, rj) - llp1 * c(C, rj) * orsq;    // X at l, the other part
-        const double xm = c(C2m, ri) - llm * c(Cm, ri) * orsq;   // X at l - 1, l + 1
-        const double xp = c(C2p, ri) - llq * c(Cp, ri) * orsq;
-        out[0][ri] = br;
-        out[1][ri] = llp1 * c(A, ri) * orsq;
-        out[2][ri] = (c(A1m, ri) * c1 + c(A1p, ri) * c2) - sg * xj;
-        out[3][ri] = sg * c(A1, rj) + (xm * c1 + xp * c2);
-        out[4][ri] = sg * c(A, rj) + (c(C1m, ri) * c1 + c(C1p, ri) * c2);
-        out[5][ri] = sg * c(C1, rj) - (c(Am, ri) * c1 + c(Ap, ri) * c2);
+    if (c.mag) {
+        rlm_a_kernel<true><<<(unsigned)((total + 127) / 128), 128, 0, c.stream>>>(
+            c.d_s2a, c.d_s2am, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
+    } else {
+        rlm_a_kernel<false><<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
+            c.d_s2a, nullptr, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
     }
-    const bool zero = (l == lmax);
-    double* o = s2o + row_index(m, l, L) * (long)nfa * fsz + (long)r * (2 * nfa) + 2 * A_BR;
-#pragma unroll
-    for (int f = 0; f < 6; ++f)
-        *reinterpret_cast<double2*>(o + 2 * f) = zero ? make_double2(0.0, 0.0) : make_double2(out[f][0], out[f][1]);
-}
-
-void launch_rlm_a_mag(Ctx& c) {
-    const long total = c.d.nlm * c.d.nr;
-    rlm_a_mag_kernel<<<(unsigned)((total + RLM_A_THREADS - 1) / RLM_A_THREADS), RLM_A_THREADS, 0, c.stream>>>(
-        c.d_s2am, c.d_s2a11, c.d_radial, c.d.nlm, c.d.nr, c.d.L, c.nfa);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }
@@ -648,7 +638,7 @@ __global__ void rlm_b_mag_kernel(const double* __restrict__ s2b, double* __restr
 // the grid operator M (to_spectral, d/dr, dealias, from_spectral): N_A = EMF_r + M X per
 // (l, m, re/im) column, on the FP64 tensor-core tile engine; then the A history, the A
 // right-hand side and its (zero) boundary rows.
-__global__ void __launch_bounds__(GEMM_THREADS) emf_radial_kernel(const double* __restrict__ M,
+__global__ void __launch_bounds__(GEMM_THREADS, 4) emf_radial_kernel(const double* __restrict__ M,
                                                                   const double* __restrict__ xemf,
                                                                   double* __restrict__ ab_a,
                                                                   double* __restrict__ rhs_a, int nr, long ncols,

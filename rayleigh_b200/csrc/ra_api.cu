@@ -542,6 +542,10 @@ static void setup(Ctx& c) {
         dalloc(c.d_s2am, (size_t)nlm * NS2AM * 2 * nr);
         dalloc(c.d_Ac, (size_t)d.L * nr * nr);
         dalloc(c.d_Aa, (size_t)d.L * nr * nr);
+        if (c.cfg.precision == RA_PREC_MIXED) {
+            dalloc(c.d_Ainv_c, (size_t)d.L * nr * nr);
+            dalloc(c.d_Ainv_a, (size_t)d.L * nr * nr);
+        }
         dalloc(c.d_perm_c, (size_t)d.L * nr);
         dalloc(c.d_perm_a, (size_t)d.L * nr);
         dalloc(c.d_coef_mag, (size_t)d.L * NMSLOT * nr);
@@ -615,7 +619,7 @@ static void release(Ctx& c) {
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
                       c.d_p2a, c.d_p2b, c.d_s2b, c.d_kew, c.d_ke_rows, c.d_kaz, c.d_bcval,
                       c.d_sol_c, c.d_sol_a, c.d_rhs_c, c.d_rhs_a, c.d_Ac, c.d_Aa, c.d_coef_mag, c.d_s2am,
-                      c.d_xemf, c.d_Memf};
+                      c.d_xemf, c.d_Memf, c.d_Ainv_c, c.d_Ainv_a};
     for (double* b : bufs)
         if (b) cudaFree(b);
     int* ibufs[] = {c.d_ltiles, c.d_inv_tiles, c.d_fwd_tiles, c.d_cheb_tiles, c.d_solve_tiles, c.d_status,
@@ -649,8 +653,7 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
             if (c.mag) launch_post_assemble_mag(c, old_ab);
             break;
         case 2:
-            launch_rlm_a(c);
-            if (c.mag) launch_rlm_a_mag(c);
+            launch_rlm_a(c);   // with the magnetic fields when c.mag
             break;
         case 3:
             if (mixed)
@@ -673,11 +676,12 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
             if (c.mag) launch_rlm_b_mag(c, new_ab);
             break;
         default:
-            if (mixed)
-                launch_solve_mixed(c);
-            else
+            if (mixed) {
+                launch_solve_mixed(c);   // every system, C and A included
+            } else {
                 launch_solve(c);
-            if (c.mag) launch_solve_mag(c);
+                if (c.mag) launch_solve_mag(c);
+            }
             break;
     }
 }

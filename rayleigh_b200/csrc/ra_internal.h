@@ -182,6 +182,7 @@ struct Ctx {
     double *d_sol_c = nullptr, *d_sol_a = nullptr;    // [lm][2][nr] poloidal / toroidal potentials
     double *d_rhs_c = nullptr, *d_rhs_a = nullptr;
     double *d_Ac = nullptr, *d_Aa = nullptr;          // LU factors [L][nr][nr]
+    double *d_Ainv_c = nullptr, *d_Ainv_a = nullptr;  // RA_PREC_MIXED: transposed inverses, as for Z
     int *d_perm_c = nullptr, *d_perm_a = nullptr;
     double *d_coef_mag = nullptr;                     // [L][NMSLOT][nr]
     double *d_s2am = nullptr;                         // [row][NS2AM][nr][2]
@@ -244,7 +245,6 @@ void lt_forward_prepare(Ctx& c);
 void solve_prepare(Ctx& c);
 void launch_rlm_b(Ctx& c, double new_ab);
 void launch_post_assemble_mag(Ctx& c, double old_ab);
-void launch_rlm_a_mag(Ctx& c);
 void launch_rlm_b_mag(Ctx& c, double new_ab);
 void launch_solve_mag(Ctx& c);
 void launch_solve(Ctx& c);

@@ -86,6 +86,25 @@ int ra_last_error(const ra_ctx* ctx, char* msg, int len);
 /* Sizes of the state arrays: n_lm = (l_max+1)(l_max+2)/2 (l-major, m ascending). */
 int ra_sizes(const ra_ctx* ctx, long* n_lm, int* n_r, int* n_theta, int* n_phi);
 
+/* CFL time-step control (Adjust_TimeStep, Sphere_Hybrid_Space.F90:604-649; the
+ * Temporal_Controls namelist values, Controls.F90:113-115, ClockInfo.F90:27). */
+typedef struct ra_dt_controls {
+    double cflmin, cflmax;      /* 0.4, 0.6 */
+    double max_time_step;       /* 1.0 */
+    double min_time_step;       /* 1e-13 */
+    double min_dt_change;       /* 0.1: a decrease is at least this fraction */
+} ra_dt_controls;
+int ra_default_dt_controls(ra_dt_controls* ctl);
+/* The dt Adjust_TimeStep chooses after a step of size dt whose CFL cargo (the
+ * value ra_step returns: the largest squared inverse crossing time) is cfl;
+ * host arithmetic only.  RA_ERR_NONFINITE when it falls below min_time_step. */
+int ra_next_dt(const ra_dt_controls* ctl, double dt, double cfl, double* new_dt);
+/* nsteps steps with that control: after each step the next dt is chosen from
+ * its CFL cargo and, when it changes, the implicit matrices are rebuilt and
+ * factored (Reset_Linear_Equations) before the next step.  *dt_out receives the
+ * dt of the next step, *dt_changes how many changes were made (either may be NULL). */
+int ra_step_adaptive(ra_ctx* ctx, int nsteps, const ra_dt_controls* ctl, double* dt_out, int* dt_changes);
+
 /* New time step: Reset_Linear_Equations (Sphere_Linear_Terms.F90:67-76):
  * rebuild LHS = I - alpha dt L with boundary rows and factor it per l on the
  * device (LU with partial pivoting, LU_Decompose_full, Linear_Solve.F90:1028-1036).
@@ -178,6 +197,9 @@ int ra_advance(ra_ctx* ctx);                    /* AdvanceTime: AB term, BCs, Im
  * inverse Legendre transform; they only assign their outputs, so the next
  * ra_step is unchanged) and a reduction on the device; *ke receives the sum. */
 int ra_kinetic_energy(ra_ctx* ctx, double* ke);
+/* The magnetic energy of the benchmark report (magnetism only; Benchmarking.F90:689-696, 846):
+ * the volume average of |B|^2 (the same weights as the kinetic energy) times 1 / (2 Ek Pm). */
+int ra_magnetic_energy(ra_ctx* ctx, double* me);
 
 /* Shell slices of the current state (Shell_Slices output, Spherical_IO.F90):
  * each quantity of quantities[0..nq) on the full theta-phi grid at the radial
@@ -204,6 +226,9 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke);
 #define RA_Q_ENTROPY_DTHETA 513
 #define RA_Q_ENTROPY_DPHI 519
 #define RA_Q_PRESSURE_DPHI 520
+#define RA_Q_B_R          801   /* magnetism only (magnetic_field_codes.F) */
+#define RA_Q_B_THETA      802
+#define RA_Q_B_PHI        803
 /* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);

@@ -865,6 +865,7 @@ class Oracle:
             orad = (1.0 / self.radius)[None, :, None]
             for k in ("curlbt", "curlbp", "bt", "bp"):
                 f[k] = f[k] * csc * orad                               # rsintheta_div (:142-147)
+            self.last_magnetic = (f["br"], f["bt"], f["bp"], th)
         # the velocity and temperature Benchmark_Checkup reads at this point of the step (:158-159)
         self.last_velocity = (f["vr"], f["vt"], f["vp"], th)
         self.last_temperature = f["t"]
@@ -1051,6 +1052,40 @@ class Oracle:
         wpt[:, :, 2 * nr:] = self.cg.to_spectral(grid)
         return wpt, np.zeros((self.n_lm, 2, nr))
 
+    def benchmark_insulating_init(self):
+        """Benchmark_Insulating_Init (Initial_Conditions.F90:1011-1073): on the collocation grid
+        C(l=1, m=0) = (8 r_o - 6 r - 2 r_i^4 / r^3) (5/8) sqrt(pi/3) r^2 and
+        A(l=2, m=0) = sin(pi (r - r_i)) r sqrt(pi/5) (4/3) 5 (real parts), then To_Spectral.
+        Returns (c, a) in the init_state layout."""
+        nr = self.cfg.n_r
+        r = self.radius
+        ri, ro = self.rmin, self.rmax
+        nrm2 = math.sqrt(math.pi / 5.0) * (4.0 / 3.0) * 5.0
+        nrm1 = (5.0 / 8.0) * math.sqrt(math.pi / 3.0)
+        rf1 = 8.0 * ro - 6.0 * r
+        rf1 = rf1 - 2.0 * (ri ** 4) / (r ** 3)
+        rf1 = rf1 * nrm1 * r ** 2
+        rf2 = np.sin(math.pi * (r - ri)) * r * nrm2
+        gc = np.zeros((self.n_lm, 2, nr))
+        ga = np.zeros((self.n_lm, 2, nr))
+        gc[1, 0, :] = rf1                  # lm(1, 0) = 1
+        if self.cfg.l_max >= 2:
+            ga[3, 0, :] = rf2              # lm(2, 0) = 3
+        return self.cg.to_spectral(gc), self.cg.to_spectral(ga)
+
+    def benchmark_magnetic_energy(self):
+        """Benchmark_Checkup's magnetic energy (Benchmarking.F90:689-696, 846) of the field
+        the last step's physical-space stage formed: |B|^2 averaged as the kinetic energy,
+        times mag_factor = 1 / (2 Ek Pm)."""
+        br, bt, bp, th = self.last_magnetic
+        if not (isinstance(th, slice) and th == slice(None)):
+            raise ValueError("the last physical-space stage did not cover every theta row")
+        q = bp * bp + br * br + bt * bt
+        tw = (self.h.wq / 2.0).astype(np.float64)
+        ell0 = np.einsum("t,tr->r", tw, q.mean(axis=2))
+        return float(np.dot(self.radial_integration_weights(), ell0)) / (2.0 * self.cfg.ekman *
+                                                                           self.cfg.magnetic_prandtl)
+
     def radial_integration_weights(self):
         """Initialize_Cheby_Grid's integration_weights (Chebyshev_Polynomials.F90:165-194):
         3 pi scaling / ((r_o^3 - r_i^3) N) r^2 sqrt(1 - x^2), halved at the two end
@@ -1134,14 +1169,16 @@ class Oracle:
                 out[i, :, :, m, m:] = s2[m][0].transpose(1, 0, 2)   # (2, nlev, nl) -> (nlev, 2, nl)
         return out
 
-    def benchmark_point_observations(self, msymm=4, fields=None):
+    def benchmark_point_observations(self, msymm=4, fields=None, btheta=None):
         """Assemble_Strips and Point_Observations (Benchmarking.F90:934-1063) on the last
         physical-space stage, or on ``fields`` = (v_r, v_phi, T) given as [theta, r, phi]
         arrays: the phi strips of v_r, v_phi and T at the two radii that straddle
         mid-depth (n_r/2, n_r/2 + 1) and the two colatitudes that straddle the equator,
         averaged; at the first msymm points (in phi order, starting across the wrap)
         where v_r changes sign upwards, v_phi and T are interpolated linearly and
-        averaged.  Returns (v_phi, T)."""
+        averaged.  Returns (v_phi, T); with ``btheta`` (True: the last stage's B_theta, or a
+        [theta, r, phi] array) the fourth observation of the magnetic case (Benchmarking.F90:
+        1017-1063, nobs = 4) as well: (v_phi, T, B_theta)."""
         if fields is None:
             vr, vt, vp, th = self.last_velocity
             if not (isinstance(th, slice) and th == slice(None)):
@@ -1160,7 +1197,10 @@ class Oracle:
             return s * (1.0 / 4)
 
         strips = [strip(vr), strip(vp), strip(temperature)]
-        vsave = np.zeros((msymm, 3))
+        if btheta is not None:
+            strips.append(strip(self.last_magnetic[1] if btheta is True else btheta))
+        nobs = len(strips)
+        vsave = np.zeros((msymm, nobs))
         xind = 0
         im1 = nphi - 1
         for i in range(nphi):
@@ -1168,12 +1208,14 @@ class Oracle:
             dvr = vrnext - vrlast
             if vrnext * vrlast < 0 and xind < msymm and dvr > 0:
                 x = -vrlast / dvr
-                for j in range(3):
+                for j in range(nobs):
                     y1, y2 = strips[j][im1], strips[j][i]
                     vsave[xind, j] = (y2 - y1) * x + y1
                 xind += 1
             im1 = i
         obs = vsave.sum(axis=0) / msymm
+        if btheta is not None:
+            return float(obs[1]), float(obs[2]), float(obs[3])
         return float(obs[1]), float(obs[2])
 
     def step(self):
@@ -1202,6 +1244,12 @@ def c2001_case0_config(n_r=48, n_theta=64):
                   rayleigh=1.0e5, ekman=1.0e-3, prandtl=1.0, gravity_power=1.0, rotation=True,
                   no_slip_top=True, no_slip_bottom=True, fix_tvar_top=True, fix_tvar_bottom=True,
                   t_top=0.0, t_bottom=1.0, dt=1.0e-4, alpha_implicit=0.50001)
+
+
+def c2001_case1_config(n_r=64, n_theta=96):
+    """The settings benchmark_mode = 2 imposes (Benchmarking.F90:150-199: Christensen et al.
+    2001, MHD case 1: case 0's settings with magnetism, Pm = 5 and insulating boundaries)."""
+    return replace(c2001_case0_config(n_r, n_theta), magnetism=True, magnetic_prandtl=5.0)
 
 
 def seeded_state(cfg: Config, seed=0x5241594C, amp=1.0e-3, lmin=1, lmax_pert=20, cheby=None):

@@ -55,6 +55,40 @@ class _Config(ctypes.Structure):
     ]
 
 
+class _DtControls(ctypes.Structure):
+    _fields_ = [("cflmin", ctypes.c_double), ("cflmax", ctypes.c_double), ("max_time_step", ctypes.c_double),
+                ("min_time_step", ctypes.c_double), ("min_dt_change", ctypes.c_double)]
+
+
+@dataclass
+class DtControls:
+    """Temporal_Controls of the CFL time-step control (Controls.F90:113-115, ClockInfo.F90:27)."""
+
+    cflmin: float = 0.4
+    cflmax: float = 0.6
+    max_time_step: float = 1.0
+    min_time_step: float = 1.0e-13
+    min_dt_change: float = 0.1
+
+    def to_c(self):
+        c = _DtControls()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+
+def next_dt(ctl: DtControls, dt, cfl):
+    """Adjust_TimeStep (Sphere_Hybrid_Space.F90:604-649) on the host: the next dt after a step of
+    size dt whose CFL cargo is cfl."""
+    lib = load_library()
+    c = ctl.to_c()
+    out = ctypes.c_double()
+    rc = lib.ra_next_dt(ctypes.byref(c), float(dt), float(cfl), ctypes.byref(out))
+    if rc != RA_OK:
+        raise RayleighError(rc, f"time step {out.value} below min_time_step")
+    return out.value
+
+
 @dataclass
 class Config:
     """Namelist values the path reads (defaults follow the reference's Controls/PDE_Coefficients)."""
@@ -125,6 +159,11 @@ def load_library(path: str | None = None):
         "ra_rlm_b": ([_VP], ctypes.c_int),
         "ra_advance": ([_VP], ctypes.c_int),
         "ra_kinetic_energy": ([_VP, _DP], ctypes.c_int),
+        "ra_magnetic_energy": ([_VP, _DP], ctypes.c_int),
+        "ra_default_dt_controls": ([ctypes.POINTER(_DtControls)], ctypes.c_int),
+        "ra_next_dt": ([ctypes.POINTER(_DtControls), ctypes.c_double, ctypes.c_double, _DP], ctypes.c_int),
+        "ra_step_adaptive": ([_VP, ctypes.c_int, ctypes.POINTER(_DtControls), _DP, ctypes.POINTER(ctypes.c_int)],
+                             ctypes.c_int),
         "ra_shell_slices": ([_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_shell_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
         "ra_azimuthal_averages": ([_VP, _VP, ctypes.c_int, _VP], ctypes.c_int),
@@ -376,10 +415,26 @@ class Rayleigh:
         return ke.value
 
     # the reference's output codes of the quantities ra_shell_slices provides
+    def magnetic_energy(self):
+        """The benchmark report's magnetic energy of the current state (magnetism only):
+        the volume average of |B|^2 over 2 Ek Pm (Benchmarking.F90:689-696, 846)."""
+        me = ctypes.c_double()
+        self._check(self.lib.ra_magnetic_energy(self.h, ctypes.byref(me)))
+        return me.value
+
+    def step_adaptive(self, nsteps, ctl: DtControls):
+        """nsteps steps with the CFL time-step control; returns (dt of the next step, dt changes)."""
+        c = ctl.to_c()
+        dt = ctypes.c_double()
+        nch = ctypes.c_int()
+        self._check(self.lib.ra_step_adaptive(self.h, int(nsteps), ctypes.byref(c), ctypes.byref(dt),
+                                              ctypes.byref(nch)))
+        return dt.value, nch.value
+
     QUANTITIES = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
                   "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 301, "entropy": 501,
                   "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519, "pressure": 502,
-                  "pressure_dr": 508, "pressure_dphi": 520}
+                  "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802, "b_phi": 803}
 
     def shell_slices(self, quantities, levels):
         """Shell slices of the current state: array [quantity][level][theta][phi] of the

@@ -1319,9 +1319,10 @@ void launch_fft_rows(Ctx& c, double* d_x, long howmany, int inverse) {
 // (Gauss-Legendre weight / 2 / n_phi, ComputeEll0) and then the radial
 // integration weights (Compute_Radial_Average).  No cluster: each row reads
 // its own hemisphere's reflection of the even and odd parts.
-template <int N>
+template <int N, bool ME>
 __global__ void __launch_bounds__(ROW_THREADS) kinetic_energy_rows_kernel(PhysParams P, const double* __restrict__ kew,
                                                                           double* __restrict__ rows) {
+    // ME: |B|^2 from B_r and r sin(theta) B_theta, B_phi (Benchmarking.F90:689-696), else rho |u|^2 / 2
     constexpr int ZPT = (N + ROW_THREADS - 1) / ROW_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
@@ -1334,11 +1335,16 @@ __global__ void __launch_bounds__(ROW_THREADS) kinetic_energy_rows_kernel(PhysPa
     const int thh = pair / nr;
     const int th = h ? (N - 1 - thh) : thh;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[3] = {A_VR, A_VT, A_VP};
+    int fo[3] = {A_VR, A_VT, A_VP};
+    if (ME) {
+        fo[0] = A_BR;
+        fo[1] = A_BT;
+        fo[2] = A_BP;
+    }
     const bool dp[3] = {false, false, false};
     double2 y[FB][ZPT];
     row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-    const double csc = P.trig[2 * N + th];
+    const double csc = ME ? P.trig[2 * N + th] * P.radial[R_OVER_R * nr + r] : P.trig[2 * N + th];
     double s = 0.0;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q)
@@ -1354,7 +1360,8 @@ __global__ void __launch_bounds__(ROW_THREADS) kinetic_energy_rows_kernel(PhysPa
     if (t == 0) {
         double v = red[0];
         for (int i = 1; i < ROW_THREADS / 32; ++i) v += red[i];
-        rows[(long)th * nr + r] = 0.5 * P.radial[R_DENSITY * nr + r] * v * kew[th] * kew[N + r];
+        const double w = ME ? 1.0 : 0.5 * P.radial[R_DENSITY * nr + r];
+        rows[(long)th * nr + r] = w * v * kew[th] * kew[N + r];
     }
 }
 
@@ -1376,7 +1383,8 @@ __global__ void __launch_bounds__(1024) kinetic_energy_sum_kernel(const double* 
     }
 }
 
-void launch_kinetic_energy(Ctx& c) {
+void launch_kinetic_energy(Ctx& c, bool magnetic) {
+    if (magnetic && !c.mag) throw ArgError("the magnetic energy needs a context created with magnetism");
     if (!c.d_twp || !c.d_kew || !c.d_ke_rows) throw ArgError("diagnostic tables not prepared at set-up");
     PhysParams P{};
     P.p2a = c.d_p2a;
@@ -1397,17 +1405,17 @@ void launch_kinetic_energy(Ctx& c) {
         kern<<<grid, ROW_THREADS, smem, c.stream>>>(P, c.d_kew, c.d_ke_rows);
     };
     switch (c.d.nth) {
-        case 24: go(kinetic_energy_rows_kernel<24>, 24); break;
-        case 32: go(kinetic_energy_rows_kernel<32>, 32); break;
-        case 48: go(kinetic_energy_rows_kernel<48>, 48); break;
-        case 64: go(kinetic_energy_rows_kernel<64>, 64); break;
-        case 96: go(kinetic_energy_rows_kernel<96>, 96); break;
-        case 128: go(kinetic_energy_rows_kernel<128>, 128); break;
-        case 192: go(kinetic_energy_rows_kernel<192>, 192); break;
-        case 256: go(kinetic_energy_rows_kernel<256>, 256); break;
-        case 384: go(kinetic_energy_rows_kernel<384>, 384); break;
-        case 512: go(kinetic_energy_rows_kernel<512>, 512); break;
-        case 768: go(kinetic_energy_rows_kernel<768>, 768); break;
+        case 24: if (magnetic) go(kinetic_energy_rows_kernel<24, true>, 24); else go(kinetic_energy_rows_kernel<24, false>, 24); break;
+        case 32: if (magnetic) go(kinetic_energy_rows_kernel<32, true>, 32); else go(kinetic_energy_rows_kernel<32, false>, 32); break;
+        case 48: if (magnetic) go(kinetic_energy_rows_kernel<48, true>, 48); else go(kinetic_energy_rows_kernel<48, false>, 48); break;
+        case 64: if (magnetic) go(kinetic_energy_rows_kernel<64, true>, 64); else go(kinetic_energy_rows_kernel<64, false>, 64); break;
+        case 96: if (magnetic) go(kinetic_energy_rows_kernel<96, true>, 96); else go(kinetic_energy_rows_kernel<96, false>, 96); break;
+        case 128: if (magnetic) go(kinetic_energy_rows_kernel<128, true>, 128); else go(kinetic_energy_rows_kernel<128, false>, 128); break;
+        case 192: if (magnetic) go(kinetic_energy_rows_kernel<192, true>, 192); else go(kinetic_energy_rows_kernel<192, false>, 192); break;
+        case 256: if (magnetic) go(kinetic_energy_rows_kernel<256, true>, 256); else go(kinetic_energy_rows_kernel<256, false>, 256); break;
+        case 384: if (magnetic) go(kinetic_energy_rows_kernel<384, true>, 384); else go(kinetic_energy_rows_kernel<384, false>, 384); break;
+        case 512: if (magnetic) go(kinetic_energy_rows_kernel<512, true>, 512); else go(kinetic_energy_rows_kernel<512, false>, 512); break;
+        case 768: if (magnetic) go(kinetic_energy_rows_kernel<768, true>, 768); else go(kinetic_energy_rows_kernel<768, false>, 768); break;
         default: throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no kinetic-energy kernel instance");
     }
     RA_CUDA(cudaGetLastError());
@@ -1452,7 +1460,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_slice_kernel(PhysParams P, 
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     double2* row = reinterpret_cast<double2*>(out + ((long)lv * N + th) * (2L * N));
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
@@ -1466,6 +1474,7 @@ void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out) {
     if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("shell slice: 1 .. 64 levels per launch");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1525,7 +1534,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_moment_rows_kernel(PhysPara
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     const double mu = MOMENTS ? mean[r] : 0.0;
     double s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
@@ -1586,6 +1595,7 @@ void launch_shell_moments(Ctx& c, const SliceSpec& S, double* rows, double* out)
     if (!c.d_twp || !c.d_kew) throw ArgError("diagnostic tables not prepared at set-up");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1635,6 +1645,7 @@ void launch_azimuthal_average(Ctx& c, const SliceSpec& S, double* rows) {
     if (!c.d_twp || !c.d_kaz) throw ArgError("diagnostic tables not prepared at set-up");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1696,7 +1707,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
         const int p = t + q * ROW_THREADS;
@@ -1756,6 +1767,7 @@ void launch_spectra_rows(Ctx& c, const SliceSpec& S, int slot0, double* p2b) {
     if (slot0 < 0 || slot0 + S.nl > c.nfb * c.d.nr) throw ArgError("shell spectra: column slots out of range");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1820,7 +1832,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
         const int p = t + q * ROW_THREADS;
@@ -1842,6 +1854,7 @@ void launch_equatorial_slice(Ctx& c, const SliceSpec& S, double* out) {
     if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1896,7 +1909,7 @@ __global__ void __launch_bounds__(ROW_THREADS) meridional_slice_kernel(PhysParam
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
@@ -1913,6 +1926,7 @@ void launch_meridional_slice(Ctx& c, const SliceSpec& S, double* out) {
     if (S.nl < 1 || S.nl > SliceSpec::MAXL) throw ArgError("meridional slices: 1 .. 64 phi indices");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -1963,6 +1977,7 @@ void launch_global_average(Ctx& c, const SliceSpec& S, double* rows, double* mea
     if (!c.d_twp || !c.d_kew) throw ArgError("diagnostic tables not prepared at set-up");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);
@@ -2022,7 +2037,7 @@ __global__ void __launch_bounds__(ROW_THREADS) point_probe_kernel(PhysParams P, 
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
     row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
-    const double scale = S.csc ? P.trig[2 * N + th] : 1.0;
+    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
@@ -2039,6 +2054,7 @@ void launch_point_probes(Ctx& c, const SliceSpec& S, const ProbeSet& Q, double* 
     if (!c.d_twp) throw ArgError("physics tables not prepared (physics_prepare runs at set-up)");
     PhysParams P{};
     P.p2a = c.d_p2a;
+    P.radial = c.d_radial;
     P.trig = c.d_costh;
     P.wr = reinterpret_cast<const double2*>(c.d_twid);
     P.twp = reinterpret_cast<const double2*>(c.d_twp);

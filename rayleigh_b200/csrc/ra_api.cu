@@ -1436,6 +1436,78 @@ static void need_phase(Ctx& c, int& phase, const SliceSpec& S) {
     }
 }
 
+int ra_magnetic_energy(ra_ctx* ctx, double* me) {
+    if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
+    if (!me) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (!c.mag) throw ArgError("the magnetic energy needs a context created with magnetism");
+        form_grid_fields(c, false);
+        launch_kinetic_energy(c, true);
+        double v = 0.0;
+        RA_CUDA(cudaMemcpyAsync(&v, c.d_ke_rows + (size_t)c.d.nth * c.d.nr, sizeof(double), cudaMemcpyDeviceToHost,
+                                c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        check_status(c);
+        // mag_factor of the benchmark report (Benchmarking.F90:392, 846): 1 / (2 Ek Pm)
+        *me = v / (2.0 * c.cfg.ekman * c.cfg.magnetic_prandtl);
+    });
+}
+
+int ra_next_dt(const ra_dt_controls* ctl, double dt, double cfl, double* new_dt) {
+    if (!ctl || !new_dt || !(dt > 0)) return RA_ERR_ARG;
+    // Adjust_TimeStep (Sphere_Hybrid_Space.F90:604-649): cfl = the largest squared inverse
+    // crossing time of the step (the CFL cargo), the new dt applies from the next step
+    double nd = dt;
+    if (cfl > 0.0) {
+        const double maxt = 1.0 / std::sqrt(cfl);
+        if (dt < maxt * ctl->cflmin) {
+            nd = std::min(ctl->cflmax * maxt, ctl->max_time_step);
+        } else if (dt > maxt * ctl->cflmax) {
+            nd = ctl->cflmax * maxt;
+            if (nd > dt * (1.0 - ctl->min_dt_change)) nd = dt * (1.0 - ctl->min_dt_change);
+        }
+    }
+    if (nd > ctl->max_time_step * 1.000001) nd = ctl->max_time_step;
+    *new_dt = nd;
+    return nd < ctl->min_time_step ? RA_ERR_NONFINITE : RA_OK;
+}
+
+int ra_default_dt_controls(ra_dt_controls* ctl) {
+    if (!ctl) return RA_ERR_ARG;
+    ctl->cflmin = 0.4;        // Controls.F90:113-115, ClockInfo.F90:27
+    ctl->cflmax = 0.6;
+    ctl->max_time_step = 1.0;
+    ctl->min_time_step = 1.0e-13;
+    ctl->min_dt_change = 0.1;
+    return RA_OK;
+}
+
+int ra_step_adaptive(ra_ctx* ctx, int nsteps, const ra_dt_controls* ctl, double* dt_out, int* dt_changes) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!ctl || nsteps < 0) return RA_ERR_ARG;
+    int changes = 0;
+    const int rc = guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        for (int s = 0; s < nsteps; ++s) {
+            double cfl = 0.0;
+            run_steps(c, 1, &cfl);
+            double nd = c.dt;
+            if (ra_next_dt(ctl, c.dt, cfl, &nd) != RA_OK)
+                throw NonFiniteError("the time step became smaller than min_time_step (" + std::to_string(nd) + ")");
+            if (nd != c.dt) {   // Reset_Linear_Equations before the next step
+                c.dt = nd;
+                linear_setup(c);
+                if (c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(c);
+                ++changes;
+            }
+        }
+    });
+    if (dt_out) *dt_out = ctx->c.dt;
+    if (dt_changes) *dt_changes = changes;
+    return rc;
+}
+
 int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
     if (!ctx || !ctx->c.have_state) return RA_ERR_STATE;
     if (!ke) return RA_ERR_ARG;
@@ -1456,30 +1528,36 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
 // comes from in p2a.  vort_r, which Diagnostics_Vorticity_Field.F90:89-93 forms
 // as (dv_phi/dtheta + cot v_phi - csc dv_theta/dphi) / r, is the spectral
 // l(l+1) Z / r^2 here: the same band-limited field, equal up to rounding.
-struct QuantitySource { int code, field, dphi, csc, pressure; };
+// With magnetism, magnetic_field_codes.F (boffset = 800): B_r, B_theta, B_phi, the last two
+// formed from the r sin(theta) B_theta, B_phi fields the step transforms (rsintheta_div).
+struct QuantitySource { int code, field, dphi, csc, pressure, orad; };
 static const QuantitySource kQuantities[] = {
-    {1, A_VR, 0, 0, 0},     {2, A_VT, 0, 1, 0},     {3, A_VP, 0, 1, 0},     {10, A_DVRDR, 0, 0, 0},
-    {11, A_DVTDR, 0, 1, 0}, {12, A_DVPDR, 0, 1, 0}, {19, A_DVRDT, 0, 1, 0}, {28, A_VR, 1, 0, 0},
-    {29, A_VT, 1, 1, 0},    {30, A_VP, 1, 1, 0},    {501, A_T, 0, 0, 0},    {507, A_DTDR, 0, 0, 0},
-    {513, A_DTDT, 0, 1, 0}, {519, A_T, 1, 0, 0},
-    {301, A_OMR, 0, 0, 0},  // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
-    {502, A_T, 0, 0, 1},    // pressure, formed in T's place
-    {508, A_DTDR, 0, 0, 1}, // d pressure / dr, in dT/dr's place
-    {520, A_T, 1, 0, 1},    // d pressure / d phi
+    {1, A_VR, 0, 0, 0, 0},     {2, A_VT, 0, 1, 0, 0},     {3, A_VP, 0, 1, 0, 0},     {10, A_DVRDR, 0, 0, 0, 0},
+    {11, A_DVTDR, 0, 1, 0, 0}, {12, A_DVPDR, 0, 1, 0, 0}, {19, A_DVRDT, 0, 1, 0, 0}, {28, A_VR, 1, 0, 0, 0},
+    {29, A_VT, 1, 1, 0, 0},    {30, A_VP, 1, 1, 0, 0},    {501, A_T, 0, 0, 0, 0},    {507, A_DTDR, 0, 0, 0, 0},
+    {513, A_DTDT, 0, 1, 0, 0}, {519, A_T, 1, 0, 0, 0},
+    {301, A_OMR, 0, 0, 0, 0},  // vort_r: l(l+1) Z / r^2, the radial vorticity of the Boussinesq velocity
+    {502, A_T, 0, 0, 1, 0},    // pressure, formed in T's place
+    {508, A_DTDR, 0, 0, 1, 0}, // d pressure / dr, in dT/dr's place
+    {520, A_T, 1, 0, 1, 0},    // d pressure / d phi
+    {801, A_BR, 0, 0, 0, 0},   {802, A_BT, 0, 1, 0, 1},   {803, A_BP, 0, 1, 0, 1},
 };
 
-static std::vector<SliceSpec> quantity_specs(const int* quantities, int nq) {
+static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {
     std::vector<SliceSpec> spec(nq);
     for (int q = 0; q < nq; ++q) {
         const QuantitySource* src = nullptr;
         for (const QuantitySource& k : kQuantities)
             if (k.code == quantities[q]) src = &k;
         if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " is not provided");
+        if (src->field >= c.nfa)
+            throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
         spec[q] = SliceSpec{};
         spec[q].field = src->field;
         spec[q].dphi = src->dphi;
         spec[q].csc = src->csc;
         spec[q].pressure = src->pressure;
+        spec[q].orad = src->orad;
     }
     return spec;
 }
@@ -1489,7 +1567,7 @@ int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* level
     if (!quantities || !levels || !out || nq < 1 || nlev < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         for (int l = 0; l < nlev; ++l)
             if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell slice: radial index out of range");
         // the slices go through p2b, which the step rewrites before reading
@@ -1518,7 +1596,7 @@ int ra_shell_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) {
     if (!quantities || !out || nq < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         // row sums and the moments go through p2b, which the step rewrites before reading
         const long nrows = (long)c.d.nth * c.d.nr;
         double* rows = c.d_p2b;
@@ -1540,7 +1618,7 @@ int ra_azimuthal_averages(ra_ctx* ctx, const int* quantities, int nq, double* ou
     if (!quantities || !out || nq < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         const long nrows = (long)c.d.nth * c.d.nr;
         int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q) {
@@ -1559,7 +1637,7 @@ int ra_shell_spectra(ra_ctx* ctx, const int* quantities, int nq, const int* leve
     if (!quantities || !levels || !out || nq < 1 || nlev < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         for (int l = 0; l < nlev; ++l)
             if (levels[l] < 0 || levels[l] >= c.d.nr) throw ArgError("shell spectra: radial index out of range");
         int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
@@ -1594,7 +1672,7 @@ int ra_equatorial_slices(ra_ctx* ctx, const int* quantities, int nq, double* out
     if (!quantities || !out || nq < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         const long per = (long)c.d.nr * c.d.nphi;
         int phase = -1;   // which fields p2a holds: 0 velocity and T, 1 with P in T's place
         for (int q = 0; q < nq; ++q) {
@@ -1614,7 +1692,7 @@ int ra_meridional_slices(ra_ctx* ctx, const int* quantities, int nq, const int* 
     if (!quantities || !phi_indices || !out || nq < 1 || nphi_sel < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         for (int j = 0; j < nphi_sel; ++j)
             if (phi_indices[j] < 0 || phi_indices[j] >= c.d.nphi)
                 throw ArgError("meridional slices: phi index out of range");
@@ -1640,7 +1718,7 @@ int ra_global_averages(ra_ctx* ctx, const int* quantities, int nq, double* out) 
     if (!quantities || !out || nq < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         const long nrows = (long)c.d.nth * c.d.nr;
         double* rows = c.d_p2b;                       // scratch between steps
         double* mean = c.d_p2b + nrows;
@@ -1662,7 +1740,7 @@ int ra_point_probes(ra_ctx* ctx, const int* quantities, int nq, const int* r_idx
     if (!quantities || !r_idx || !theta_idx || !phi_idx || !out || nq < 1) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        const std::vector<SliceSpec> spec = quantity_specs(quantities, nq);
+        const std::vector<SliceSpec> spec = quantity_specs(c, quantities, nq);
         if (nr_p < 1 || nr_p > ProbeSet::MAXP || ntheta_p < 1 || ntheta_p > ProbeSet::MAXP || nphi_p < 1 ||
             nphi_p > ProbeSet::MAXP)
             throw ArgError("point probes: 1 .. 64 indices per direction");

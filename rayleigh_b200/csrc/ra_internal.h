@@ -214,12 +214,13 @@ void launch_cheb_synthesis(Ctx& c);
 void launch_post_assemble(Ctx& c, double old_ab);
 void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
-void launch_kinetic_energy(Ctx& c);
+void launch_kinetic_energy(Ctx& c, bool magnetic = false);
 // one diagnostic quantity on the phi grid at up to MAXL radial levels
 struct SliceSpec {
     static constexpr int MAXL = 64;
     int field, dphi, csc, nl;   // p2a field, d/dphi, times 1/sin(theta), levels in this launch
     int pressure;               // formed with the P grid in T's place (pressure quantities)
+    int orad;                   // times 1/r (the r sin(theta) B_theta, B_phi fields)
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);

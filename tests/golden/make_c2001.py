@@ -9,7 +9,7 @@ volume-averaged kinetic energy and the point observables.
 
 Run from the repository root in a container that has the reference tree:
 
-    python tests/golden/make_c2001.py [/path/to/reference]
+    python tests/golden/make_c2001.py /path/to/reference
 
 The output ``tests/golden/c2001_case0.json`` is committed; nothing at test
 time reads the reference tree.
@@ -19,7 +19,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python %s /path/to/reference" % os.path.relpath(__file__))
+REF = sys.argv[1]
 CASE = os.path.join(REF, "tests", "c2001_case0")
 HERE = os.path.dirname(os.path.abspath(__file__))
 

@@ -10,7 +10,7 @@ normalisation folding.
 
 Run from the repository root in a container that has the reference tree:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 The output ``tests/golden/sht_golden.npz`` is committed; nothing at test
 time reads the reference tree.
@@ -21,7 +21,9 @@ import warnings
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python %s /path/to/reference" % os.path.relpath(__file__))
+REF = sys.argv[1]
 sys.path.insert(0, os.path.join(REF, "post_processing"))
 warnings.simplefilter("ignore")
 if not hasattr(np, "ComplexWarning"):          # removed from the numpy namespace in 2.x

@@ -57,7 +57,7 @@ def test_default_config_and_argument_errors_without_gpu():
 def test_diagnostic_quantity_codes_are_the_references():
     """RA_Q_* in the header, the Python names and the reference's output codes
     (velocity_field_codes.F: voffset = 0; vorticity_field_codes.F: vort_off = 300;
-    thermal_field_codes.F: pt_off = 500)
+    thermal_field_codes.F: pt_off = 500; magnetic_field_codes.F: boffset = teoffset + 100 = 800)
     agree; context-less diagnostic calls report a state error."""
     import rayleigh_b200 as rb
     src = open(os.path.join(ROOT, "include", "rayleigh_b200.h")).read()
@@ -66,7 +66,8 @@ def test_diagnostic_quantity_codes_are_the_references():
     reference = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 300 + 1,
                  "entropy": 500 + 1, "entropy_dr": 500 + 7, "entropy_dtheta": 500 + 13, "entropy_dphi": 500 + 19,
-                 "pressure": 500 + 2, "pressure_dr": 500 + 8, "pressure_dphi": 500 + 20}
+                 "pressure": 500 + 2, "pressure_dr": 500 + 8, "pressure_dphi": 500 + 20,
+                 "b_r": 800 + 1, "b_theta": 800 + 2, "b_phi": 800 + 3}
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()
@@ -80,3 +81,21 @@ def test_diagnostic_quantity_codes_are_the_references():
     assert lib.ra_meridional_slices(None, q, 1, q, 1, None) == rb.RA_ERR_STATE
     assert lib.ra_global_averages(None, q, 1, None) == rb.RA_ERR_STATE
     assert lib.ra_point_probes(None, q, 1, q, 1, q, 1, q, 1, None) == rb.RA_ERR_STATE
+
+
+def test_cfl_time_step_control_without_gpu():
+    """ra_next_dt restates Adjust_TimeStep (Sphere_Hybrid_Space.F90:604-649): grow to
+    cflmax * t_cross (capped by max_time_step) when dt < cflmin * t_cross, shrink to
+    cflmax * t_cross, by at least min_dt_change, when dt > cflmax * t_cross, else keep dt."""
+    import rayleigh_b200 as rb
+    ctl = rb.DtControls(max_time_step=1e-4)
+    t = 1e-3                                   # crossing time: cfl cargo = 1 / t^2
+    cfl = 1.0 / t ** 2
+    assert rb.next_dt(ctl, 1e-5, cfl) == 1e-4                  # grows, capped by max_time_step
+    assert rb.next_dt(rb.DtControls(), 1e-5, cfl) == 0.6 * t   # grows to cflmax * t
+    assert rb.next_dt(rb.DtControls(), 0.5 * t, cfl) == 0.5 * t   # inside [cflmin, cflmax]: kept
+    assert rb.next_dt(rb.DtControls(), 0.62 * t, cfl) == 0.62 * t * 0.9   # small decrease bumped to 10 %
+    assert abs(rb.next_dt(rb.DtControls(), 2.0 * t, cfl) - 0.6 * t) < 1e-18
+    assert rb.next_dt(ctl, 5e-5, 0.0) == 5e-5                   # no cargo: kept
+    with pytest.raises(rb.RayleighError):
+        rb.next_dt(rb.DtControls(min_time_step=1e-3), 2.0 * t, cfl)

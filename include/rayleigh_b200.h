@@ -163,6 +163,24 @@ int ra_get_state(ra_ctx* ctx, double* wpt, double* z, double* ab);
  * magnetic state was never put starts from C = A = 0. */
 int ra_put_magnetic_state(ra_ctx* ctx, const double* c, const double* a, const double* ab);
 int ra_get_magnetic_state(ra_ctx* ctx, double* c, double* a, double* ab);
+/* Checkpoint files in the reference's format (Write_Checkpoint / Read_Checkpoint,
+ * Checkpointing.F90:143-801, version 2): a directory holding one file per field
+ * (W P T Z, C A with magnetism, their AB terms WAB ..., boundary_conditions) and
+ * grid_etc (endian tag 314, version, n_r, grid type, l_max, dt, new_dt, radius,
+ * elapsed time, iteration).  A field file is n_r (l_max+1)(l_max+2) float64: the
+ * real parts, then the imaginary parts, one chunk per radial index, each chunk
+ * the (l, m) pairs m-major with l fastest.  ra_write_checkpoint writes the
+ * context's state (its last completed iteration, the last and the next dt)
+ * into dir (created if missing); ra_read_checkpoint puts a checkpoint of the
+ * same grid (no interpolation: RA_ERR_ARG otherwise) into the context, rebuilds
+ * the implicit matrices if its next dt differs, and continues from the
+ * following iteration.  The field helpers convert one field between the state
+ * layout (n_r, 2, n_lm) and a file; they use no device. */
+int ra_write_checkpoint(ra_ctx* ctx, const char* dir, double elapsed_time);
+int ra_read_checkpoint(ra_ctx* ctx, const char* dir, int* iteration, double* elapsed_time);
+int ra_checkpoint_write_field(const char* path, int n_r, int l_max, const double* field);
+int ra_checkpoint_read_field(const char* path, int n_r, int l_max, double* field);
+
 /* The same for one rank's slice of the modes (the (l, m) pairs a rank of the
  * reference holds, Load_Balance.F90:357-368): l_of[i], m_of[i] name mode i of
  * the slice, whose arrays are the rank's own equation-set layout

@@ -195,6 +195,10 @@ def load_library(path: str | None = None):
         "ra_mixed_gemm_noalloc": ([_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p,
                                    ctypes.c_int], ctypes.c_int),
         "ra_debug_buffer": ([_VP, ctypes.c_int, _VP, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+        "ra_write_checkpoint": ([_VP, ctypes.c_char_p, ctypes.c_double], ctypes.c_int),
+        "ra_read_checkpoint": ([_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), _DP], ctypes.c_int),
+        "ra_checkpoint_write_field": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+        "ra_checkpoint_read_field": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
         "ra_put_magnetic_state": ([_VP, _VP, _VP, _VP], ctypes.c_int),
         "ra_get_magnetic_state": ([_VP, _VP, _VP, _VP], ctypes.c_int),
         "ra_put_state_modes": ([_VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, ctypes.c_int], ctypes.c_int),
@@ -306,6 +310,17 @@ class Rayleigh:
         ab = np.empty((2, self.n_lm, 2, self.n_r))
         self._check(self.lib.ra_get_magnetic_state(self.h, _ptr(c), _ptr(a), _ptr(ab)))
         return c, a, ab
+
+    # ---- checkpoint files in the reference's format ----
+    def write_checkpoint(self, directory, elapsed_time=0.0):
+        self._check(self.lib.ra_write_checkpoint(self.h, os.fsencode(directory), float(elapsed_time)))
+
+    def read_checkpoint(self, directory):
+        """Returns (iteration of the checkpoint, its elapsed time); the context continues from the next."""
+        it = ctypes.c_int()
+        t = ctypes.c_double()
+        self._check(self.lib.ra_read_checkpoint(self.h, os.fsencode(directory), ctypes.byref(it), ctypes.byref(t)))
+        return it.value, t.value
 
     # ---- one rank's slice of the modes (the reference's per-rank equation-set layout) ----
     def put_state_modes(self, l_of, m_of, wpt, z, ab=None, iteration=1):
@@ -605,6 +620,26 @@ def build_matrices(cfg: Config, sys, l0, nl, coefs=False):
     if rc != RA_OK:
         raise RayleighError(rc, "ra_build_matrices refused the configuration or range")
     return (lhs, cf) if coefs else lhs
+
+
+def checkpoint_write_field(path, field, n_r, l_max):
+    """One checkpoint field file from a state-layout array [lm][re/im][r] (host only)."""
+    f = _f64(field)
+    if f.size != n_r * (l_max + 1) * (l_max + 2):
+        raise ValueError("field has the wrong size")
+    rc = load_library().ra_checkpoint_write_field(os.fsencode(path), int(n_r), int(l_max), _ptr(f))
+    if rc != RA_OK:
+        raise RayleighError(rc, f"cannot write {path}")
+
+
+def checkpoint_read_field(path, n_r, l_max):
+    """A checkpoint field file as a state-layout array [lm][re/im][r] (host only)."""
+    n_lm = (l_max + 1) * (l_max + 2) // 2
+    out = np.empty((n_lm, 2, n_r))
+    rc = load_library().ra_checkpoint_read_field(os.fsencode(path), int(n_r), int(l_max), _ptr(out))
+    if rc != RA_OK:
+        raise RayleighError(rc, f"cannot read {path} (missing, or not a field of this grid)")
+    return out
 
 
 SOLVE_FP64 = 0

@@ -18,9 +18,6 @@
 
 using namespace ra;
 
-struct ra_ctx {
-    Ctx c;
-};
 
 namespace ra {
 

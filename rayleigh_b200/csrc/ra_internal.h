@@ -305,3 +305,8 @@ struct ArgError {
 };
 
 }  // namespace ra
+
+// the opaque handle of the C ABI
+struct ra_ctx {
+    ra::Ctx c;
+};

@@ -33,7 +33,7 @@ extern "C" {
 #define RA_OK               0
 #define RA_ERR_ARG         -1   /* invalid argument or unsupported configuration */
 #define RA_ERR_CUDA        -2   /* a CUDA runtime call failed */
-#define RA_ERR_SINGULAR    -3   /* a pivot |u_kk| <= n 2^-53 max|A| in a per-l implicit matrix */
+#define RA_ERR_SINGULAR    -3   /* a zero or non-finite pivot in a per-l implicit matrix (DGETRF INFO > 0) */
 #define RA_ERR_NOMEM       -4   /* device allocation failed */
 #define RA_ERR_STATE       -5   /* call out of order (e.g. step before put_state) */
 #define RA_ERR_NONFINITE   -6   /* NaN/Inf in an input, or reaching the implicit solve during a step */
@@ -45,7 +45,7 @@ typedef struct ra_ctx ra_ctx;
 
 /* Problem description: the namelist values the path reads
  * (ProblemSize_Namelist, Physical_Controls, Temporal_Controls,
- *  Boundary_Conditions, Reference_Namelist with reference_type = 1). */
+ *  Boundary_Conditions, Reference_Namelist, Transport_Namelist). */
 typedef struct ra_config {
     int    n_r;              /* Chebyshev collocation points (even), one domain */
     int    l_max;            /* maximum spherical-harmonic degree */
@@ -70,6 +70,25 @@ typedef struct ra_config {
     int    device;           /* CUDA device ordinal */
     int    autotune;         /* 0: built-in kernel choices; 1: time the candidate kernels of each
                                 tunable stage at set-up on this device and keep the fastest */
+    /* Reference state (Reference_Namelist, PDE_Coefficients.F90:84-160, 216-257) */
+    int    reference_type;   /* 1: Boussinesq (Constant_Reference, :335-435); 2: dimensional (cgs)
+                                polytrope (Polytropic_Reference, :925-1051); 3: nondimensional
+                                polytrope (Polytropic_ReferenceND, :437-537).  Types 2 and 3 are
+                                anelastic; their heating terms need n_theta <= 768 */
+    double poly_n;           /* polytropic index (types 2, 3) */
+    double poly_nrho;        /* density scale heights across the shell (types 2, 3) */
+    double poly_mass;        /* interior mass, g (type 2; gravity G M / r^2) */
+    double poly_rho_i;       /* density at the inner radius, g/cm^3 (type 2) */
+    double pressure_specific_heat;   /* c_P (type 2) */
+    double angular_velocity; /* frame rotation rate, rad/s (type 2; Coriolis 2 Omega) */
+    double modified_rayleigh;        /* Modified_Rayleigh_Number (type 3) */
+    /* Transport_Namelist (:186-207): type 1 constant, 2 x_top (rho / rho_top)^power.  The tops
+       are read for reference_type 2; types 1 and 3 set them (1, 1/Pr, 1/Pm; Ek, Ek/Pr, Ek/Pm) */
+    int    nu_type, kappa_type, eta_type;
+    double nu_power, kappa_power, eta_power;
+    double nu_top, kappa_top, eta_top;
+    /* Controls.F90:64-65, both on by default; Constant_Reference turns both off */
+    int    viscous_heating, ohmic_heating;
 } ra_config;
 
 /* Fills *cfg with the defaults of the reference (Controls.F90, PDE_Coefficients.F90). */
@@ -138,7 +157,7 @@ int ra_load_matrices(ra_ctx* ctx, int sys, const double* lhs, const double* coef
 int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs, double* coefs);
 /* LU_Decompose_Matrices (Linear_Solve.F90:459-480) of the loaded matrices of
  * all systems (both, or the four with magnetism), which belong to time step dt (the AB2 factors use it).
- * RA_ERR_SINGULAR names the system and l of a negligible pivot. */
+ * RA_ERR_SINGULAR names the system and l of a zero pivot. */
 int ra_factor(ra_ctx* ctx, double dt);
 /* bc_values(2 [top, bottom], 2 [re, im], n_lm, 4 [W, P, T, Z]) of
  * BoundaryConditions.F90:364-531, written into the boundary rows of the

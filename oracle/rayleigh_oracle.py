@@ -63,6 +63,30 @@ class Config:
     dtdr_bottom: float = 0.0
     dt: float = 1.0e-4
     alpha_implicit: float = 0.5
+    # Reference_Namelist (PDE_Coefficients.F90:84-160): 1 Constant_Reference (Boussinesq),
+    # 2 Polytropic_Reference (dimensional, cgs), 3 Polytropic_ReferenceND
+    reference_type: int = 1
+    poly_n: float = 0.0
+    poly_nrho: float = 0.0
+    poly_mass: float = 0.0
+    poly_rho_i: float = 0.0
+    pressure_specific_heat: float = 1.0
+    angular_velocity: float = -1.0
+    modified_rayleigh: float = -1.0
+    # Transport_Namelist (PDE_Coefficients.F90:186-207): type 1 constant, type 2
+    # x_top (rho / rho_top)^power; the tops are read for reference_type 2 only
+    nu_type: int = 1
+    kappa_type: int = 1
+    eta_type: int = 1
+    nu_power: float = 0.0
+    kappa_power: float = 0.0
+    eta_power: float = 0.0
+    nu_top: float = -1.0
+    kappa_top: float = -1.0
+    eta_top: float = -1.0
+    # Controls.F90:64-65 (Constant_Reference turns both off)
+    viscous_heating: bool = True
+    ohmic_heating: bool = True
 
     def __post_init__(self):
         if self.n_theta <= 0:
@@ -418,9 +442,11 @@ def lm_pairs(l_max):
 
 
 class Oracle:
-    """Boussinesq (reference_type 1) rotating convection, single Chebyshev domain;
-    with ``cfg.magnetism`` the dynamo equation set (poloidal C and toroidal A
-    potentials of B, Lorentz force, induction by the EMF)."""
+    """Rotating convection in a spherical shell, single Chebyshev domain, on a
+    Boussinesq (reference_type 1) or anelastic polytropic (2 dimensional, 3
+    nondimensional) reference state; with ``cfg.magnetism`` the dynamo equation
+    set (poloidal C and toroidal A potentials of B, Lorentz force, induction by
+    the EMF)."""
 
     NF1A = 8     # W P T Z W' T' Z' W''  (Fields.F90:244-252, aliases :317-335); + C A C' A' C'' with magnetism
     NF2A = 12    # + Br, (curl B)_r, (curl B)_theta, (curl B)_phi, B_theta, B_phi with magnetism
@@ -444,23 +470,7 @@ class Oracle:
         dr[0] = r[0] - r[1]
         dr[1:] = r[:-1] - r[1:]
         self.delta_r = dr
-        # Constant_Reference (PDE_Coefficients.F90:335-435)
-        self.density = np.ones(nr)
-        self.dlnrho = np.zeros(nr)
-        self.buoy = (cfg.rayleigh / cfg.prandtl) * (r / r[0]) ** cfg.gravity_power
-        pscaling = 1.0 / cfg.ekman if cfg.rotation else 1.0
-        self.dpdr_w_term = self.density * pscaling
-        self.pressure_dwdr_term = -1.0 * self.density * pscaling
-        self.coriolis = 2.0 / cfg.ekman
-        self.nu = np.ones(nr)
-        self.kappa = np.full(nr, 1.0 / cfg.prandtl)
-        # Constant_Reference, magnetism (PDE_Coefficients.F90:418-427): Lorentz_Coeff, eta
-        self.lorentz = 1.0 / (cfg.magnetic_prandtl * cfg.ekman) if self.mag else 0.0
-        self.eta = np.full(nr, 1.0 / cfg.magnetic_prandtl) if self.mag else np.zeros(nr)
-        r_out, r_in = r[0], r[-1]
-        pref = r_out * r_in / (r_in - r_out)
-        self.s_conductive = pref * (1.0 / r_out - 1.0 / r)
-        # transport-derived diffusion coefficients are zero for constant nu, kappa, rho
+        self._reference_state()
         self.ls, self.ms = lm_pairs(cfg.l_max)
         self.n_lm = len(self.ls)
         self.l_start = np.searchsorted(self.ls, np.arange(cfg.l_max + 1))
@@ -471,6 +481,121 @@ class Oracle:
         self._build_linear()
         self.last_cfl = 0.0
         self.bc_values = None   # None: the built-in boundary values (only l = 0 T carries one)
+
+    # ----- reference state and transport coefficients (PDE_Coefficients.F90) -----
+    def _reference_state(self):
+        cfg, r, nr = self.cfg, self.radius, self.cfg.n_r
+        rmin, rmax = self.rmin, self.rmax
+        one = np.ones(nr)
+        self.dsdr = np.zeros(nr)
+        if cfg.reference_type == 1:
+            # Constant_Reference (:335-435)
+            self.density, self.dlnrho, self.d2lnrho = one.copy(), np.zeros(nr), np.zeros(nr)
+            self.temperature, self.dlnT = one.copy(), np.zeros(nr)
+            self.buoy = (cfg.rayleigh / cfg.prandtl) * (r / r[0]) ** cfg.gravity_power
+            pscaling = 1.0 / cfg.ekman if cfg.rotation else 1.0
+            self.coriolis = 2.0 / cfg.ekman
+            nu_top, kappa_top = 1.0, 1.0 / cfg.prandtl
+            self.viscous_amp = np.full(nr, 2.0)
+            self.lorentz = 1.0 / (cfg.magnetic_prandtl * cfg.ekman) if self.mag else 0.0
+            eta_top = 1.0 / cfg.magnetic_prandtl if self.mag else 0.0
+            self.ohmic_amp = np.full(nr, self.lorentz)
+            self.viscous_heating = self.ohmic_heating = False
+        elif cfg.reference_type == 2:
+            # Polytropic_Reference (:925-1051), cgs
+            if cfg.poly_n <= 0 or cfg.poly_nrho <= 0 or cfg.poly_mass <= 0 or cfg.poly_rho_i <= 0:
+                raise ValueError("reference_type 2 needs poly_n, poly_nrho, poly_mass, poly_rho_i > 0")
+            G = 6.67e-8
+            n = cfg.poly_n
+            ri, ro = r[-1], r[0]
+            beta = ri / ro
+            zeta0 = (beta + 1.0) / (beta * math.exp(cfg.poly_nrho / n) + 1.0)
+            c0 = (2.0 * zeta0 - beta - 1.0) / (1.0 - beta)
+            c1 = (1.0 + beta) * (1.0 - zeta0) / (1.0 - beta) ** 2
+            d = ro - ri
+            zeta = c0 + c1 * d / r
+            dlnzeta = -c1 * d / r ** 2 / zeta
+            rho_c = cfg.poly_rho_i / zeta[-1] ** n
+            P_c = G * cfg.poly_mass * rho_c / ((n + 1.0) * d * c1)
+            T_c = (n + 1.0) * P_c / (cfg.pressure_specific_heat * rho_c)
+            gravity = G * cfg.poly_mass / r ** 2
+            self.density = rho_c * zeta ** n
+            self.dlnrho = -n * c1 * d / (zeta * r ** 2)
+            self.d2lnrho = -self.dlnrho * (2.0 / r - c1 * d / zeta / r ** 2)
+            self.temperature = T_c * zeta
+            self.dlnT = dlnzeta
+            self.buoy = gravity / cfg.pressure_specific_heat * self.density
+            pscaling = 1.0
+            self.coriolis = 2.0 * cfg.angular_velocity
+            nu_top, kappa_top, eta_top = cfg.nu_top, cfg.kappa_top, cfg.eta_top
+            self.viscous_amp = 2.0 / self.temperature
+            self.lorentz = 1.0 / (4.0 * math.pi) if self.mag else 0.0
+            self.ohmic_amp = self.lorentz / self.density / self.temperature
+            self.viscous_heating, self.ohmic_heating = cfg.viscous_heating, cfg.ohmic_heating
+        elif cfg.reference_type == 3:
+            # Polytropic_ReferenceND (:437-537)
+            if cfg.poly_n <= 0 or cfg.poly_nrho <= 0:
+                raise ValueError("reference_type 3 needs poly_n, poly_nrho > 0")
+            n = cfg.poly_n
+            beta = cfg.aspect_ratio
+            diss = beta * (math.exp(cfg.poly_nrho / n) - 1.0)
+            dtmp = 1.0 / (1.0 - beta)
+            self.temperature = dtmp * diss * (dtmp / r - 1.0) + 1.0
+            self.density = self.temperature ** n
+            gravity = rmax ** 2 / r ** 2
+            self.buoy = gravity * cfg.modified_rayleigh * self.density
+            self.dlnT = -diss * gravity / self.temperature
+            self.dlnrho = n * self.dlnT
+            self.d2lnrho = -n * self.dlnT ** 2 + (n / self.temperature) * (2.0 * diss * gravity / r)
+            pscaling = 1.0
+            self.coriolis = 2.0
+            nu_top, kappa_top = cfg.ekman, cfg.ekman / cfg.prandtl
+            self.viscous_amp = 2.0 / self.temperature * diss / cfg.modified_rayleigh
+            if self.mag:
+                self.lorentz = cfg.ekman / cfg.magnetic_prandtl
+                eta_top = cfg.ekman / cfg.magnetic_prandtl
+                otmp = diss * cfg.ekman ** 2 / (cfg.modified_rayleigh * cfg.magnetic_prandtl ** 2)
+                self.ohmic_amp = otmp / self.density / self.temperature
+            else:
+                self.lorentz, eta_top, self.ohmic_amp = 0.0, 0.0, np.zeros(nr)
+            self.viscous_heating, self.ohmic_heating = cfg.viscous_heating, cfg.ohmic_heating
+        else:
+            raise ValueError(f"reference_type {cfg.reference_type} is not restated (1, 2, 3)")
+        if not self.mag:
+            eta_top = 0.0
+        self.dpdr_w_term = self.density * pscaling
+        self.pressure_dwdr_term = -1.0 * self.density * pscaling
+
+        # Initialize_Diffusivity / Vary_With_Density (:1906-1981)
+        def diffusivity(top, kind, power):
+            if kind == 1:
+                return np.full(nr, top), np.zeros(nr)
+            if kind == 2:
+                return top * (self.density / self.density[0]) ** power, power * self.dlnrho
+            raise ValueError(f"transport type {kind} is not restated (1, 2)")
+        self.nu, self.dlnu = diffusivity(nu_top, cfg.nu_type, cfg.nu_power)
+        self.kappa, self.dlnkappa = diffusivity(kappa_top, cfg.kappa_type, cfg.kappa_power)
+        if self.mag:
+            self.eta, self.dlneta = diffusivity(eta_top, cfg.eta_type, cfg.eta_power)
+        else:
+            self.eta, self.dlneta = np.zeros(nr), np.zeros(nr)
+        # Initialize_Transport_Coefficients (:1822-1836)
+        self.viscous_heating_coeff = self.viscous_amp * self.nu if self.viscous_heating else None
+        self.ohmic_heating_coeff = (self.ohmic_amp * self.eta if (self.mag and self.ohmic_heating) else None)
+        # Compute_Diffusion_Coefs (:2032-2098)
+        nu, dlnu, dlnrho, d2lnrho = self.nu, self.dlnu, self.dlnrho, self.d2lnrho
+        self.w_diff0 = -nu * (4.0 / 3.0) * (dlnu * dlnrho + d2lnrho + dlnrho / r + 3.0 * dlnu / r)
+        self.w_diff1 = nu * (2.0 * dlnu - dlnrho / 3.0)
+        self.dw_diff2 = (dlnu - dlnrho) * nu
+        self.dw_diff1 = -(d2lnrho + 2.0 / r * dlnrho + 2.0 / r * dlnu + dlnu * dlnrho) * nu
+        self.dw_diff0 = -(2.0 * dlnrho / 3.0 + dlnu) * nu
+        self.s_diff1 = self.kappa * (self.dlnkappa + dlnrho + self.dlnT)
+        self.z_diff0 = -nu * (2.0 * dlnu / r + dlnrho * dlnu + d2lnrho + 2.0 * dlnrho / r)
+        self.z_diff1 = nu * (dlnu - dlnrho)
+        self.a_diff1 = self.eta * self.dlneta
+        r_out, r_in = r[0], r[-1]
+        pref = r_out * r_in / (r_in - r_out)
+        self.s_conductive = pref * (1.0 / r_out - 1.0 / r)
 
     # ----- linear system (Sphere_Linear_Terms.F90:79-537, Linear_Solve.F90:494-539) -----
     def _build_linear(self):
@@ -511,7 +636,7 @@ class Oracle:
                 add(TEQ, TVAR, 0, ones, static=True)
                 add(TEQ, TVAR, 1, 2.0 / r * self.kappa)
                 add(TEQ, TVAR, 2, 1.0 * self.kappa)
-                add(TEQ, TVAR, 1, np.zeros(nr))            # S_Diffusion_Coefs_1 = 0
+                add(TEQ, TVAR, 1, self.s_diff1)            # S_Diffusion_Coefs_1
                 add(PEQ, TVAR, 0, -self.buoy, static=True)
                 add(PEQ, PVAR, 1, self.dpdr_w_term, static=True)
                 add(WEQ, WVAR, 0, ones, static=True)
@@ -521,34 +646,34 @@ class Oracle:
                 add(WEQ, WVAR, 0, ones, static=True)
                 add(WEQ, WVAR, 0, H * self.nu)
                 add(WEQ, WVAR, 2, self.nu)
-                add(WEQ, WVAR, 0, np.zeros(nr))            # W_Diffusion_Coefs_0
-                add(WEQ, WVAR, 1, np.zeros(nr))            # W_Diffusion_Coefs_1
+                add(WEQ, WVAR, 0, self.w_diff0)            # W_Diffusion_Coefs_0
+                add(WEQ, WVAR, 1, self.w_diff1)            # W_Diffusion_Coefs_1
                 add(PEQ, PVAR, 0, self.pressure_dwdr_term)
                 add(PEQ, WVAR, 1, ones, static=True)
                 add(PEQ, WVAR, 0, -self.nu * H * 2.0 / r)
                 add(PEQ, WVAR, 1, H * self.nu)
                 add(PEQ, WVAR, 3, self.nu)
-                add(PEQ, WVAR, 0, np.zeros(nr))            # dW_Diffusion_Coefs_0*H
-                add(PEQ, WVAR, 1, np.zeros(nr))
-                add(PEQ, WVAR, 2, np.zeros(nr))
+                add(PEQ, WVAR, 0, self.dw_diff0 * H)       # dW_Diffusion_Coefs_0*H
+                add(PEQ, WVAR, 1, self.dw_diff1)
+                add(PEQ, WVAR, 2, self.dw_diff2)
                 add(TEQ, TVAR, 0, ones, static=True)
                 add(TEQ, TVAR, 0, H * self.kappa)
                 add(TEQ, TVAR, 1, 2.0 / r * self.kappa)
                 add(TEQ, TVAR, 2, self.kappa)
-                add(TEQ, TVAR, 1, np.zeros(nr))
+                add(TEQ, TVAR, 1, self.s_diff1)
                 add(ZEQ, ZVAR, 0, ones, static=True, mat=Z, rb=0, cb=0)
                 add(ZEQ, ZVAR, 0, H * self.nu, mat=Z, rb=0, cb=0)
                 add(ZEQ, ZVAR, 2, self.nu, mat=Z, rb=0, cb=0)
-                add(ZEQ, ZVAR, 0, np.zeros(nr), mat=Z, rb=0, cb=0)
-                add(ZEQ, ZVAR, 1, np.zeros(nr), mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 0, self.z_diff0, mat=Z, rb=0, cb=0)
+                add(ZEQ, ZVAR, 1, self.z_diff1, mat=Z, rb=0, cb=0)
                 if self.mag:
-                    # Btor (A) and Bpol (C) equations (Sphere_Linear_Terms.F90:473-499); no eta variation
+                    # Btor (A) and Bpol (C) equations (Sphere_Linear_Terms.F90:473-499)
                     blk[AEQ] = blk[AVAR] = 0
                     blk[CEQ] = blk[CVAR] = 0
                     add(AEQ, AVAR, 0, ones, static=True, mat=Am)
                     add(AEQ, AVAR, 0, H * self.eta, mat=Am)
                     add(AEQ, AVAR, 2, self.eta, mat=Am)
-                    add(AEQ, AVAR, 1, np.zeros(nr), mat=Am)    # A_Diffusion_Coefs_1
+                    add(AEQ, AVAR, 1, self.a_diff1, mat=Am)    # A_Diffusion_Coefs_1
                     add(CEQ, CVAR, 0, ones, static=True, mat=Cm)
                     add(CEQ, CVAR, 0, H * self.eta, mat=Cm)
                     add(CEQ, CVAR, 2, self.eta, mat=Cm)
@@ -892,6 +1017,24 @@ class Oracle:
         lorentz = self.mag and cfg.lorentz_forces
         # Temperature_Advection (:303-318)
         out[TVAR] = -vr * f["dtdr"] - one_over_r * (f["dtdt"] * vt + vp * f["dtdp"] * csc)
+        if self.viscous_heating_coeff is not None:
+            # Compute_Viscous_Heating (:337-443) with the colatitude derivatives of
+            # Compute_dvtheta_by_dtheta / Compute_dvphi_by_dtheta (:226-248)
+            dvpdp, dvtdp = f["dvpdp"], f["dvtdp"]
+            dvtdt = -vr * (r * dlnrho + 2.0) - r * f["dvrdr"] - vt * cot - dvpdp * csc
+            dvpdt = r * f["omr"] + dvtdp * csc - vp * cot
+            tmp = (dvpdp * csc + vr + vt * cot) * one_over_r          # e_phi_phi
+            tmp2 = (dvtdt + vr) * one_over_r                          # e_theta_theta
+            ht = f["dvrdr"] * f["dvrdr"] + tmp * tmp + tmp2 * tmp2
+            tmp = (f["dvrdp"] * csc - vp) * one_over_r + f["dvpdr"]   # 2 e_r_phi
+            ht = ht + tmp * tmp * 0.5
+            tmp = (f["dvrdt"] - vt) * one_over_r + f["dvtdr"]         # 2 e_r_theta
+            ht = ht + tmp * tmp * 0.5
+            tmp = (dvpdt + dvtdp * csc - vp * cot) * one_over_r       # 2 e_phi_theta
+            ht = ht + tmp * tmp * 0.5
+            tmp = -vr * dlnrho                                        # div u
+            ht = ht - tmp * tmp * (1.0 / 3.0)
+            out[TVAR] = out[TVAR] + self.viscous_heating_coeff[None, :, None] * ht
         # Momentum_Advection_Radial (:466-529)
         w = -vr * f["dvrdr"] * r2 - vt * (f["dvrdt"] - vt) * r - vp * (f["dvrdp"] * csc - vp) * r
         if cfg.rotation:
@@ -916,6 +1059,9 @@ class Oracle:
         if lorentz:   # -[J x B]_phi (:712-718)
             z = z - self.lorentz * (f["curlbr"] * f["bt"] - f["curlbt"] * f["br"])
         out[ZVAR] = z * r * csc
+        if self.ohmic_heating_coeff is not None:   # Compute_Ohmic_Heating (:446-466)
+            out[TVAR] = out[TVAR] + (f["curlbr"] * f["curlbr"] + f["curlbt"] * f["curlbt"]
+                                     + f["curlbp"] * f["curlbp"]) * self.ohmic_heating_coeff[None, :, None]
         if self.mag:
             # Compute_EMF (:534-581): u x B; the theta and phi parts times r / sin(theta)
             br, bt, bp = f["br"], f["bt"], f["bp"]
@@ -1250,6 +1396,20 @@ def c2001_case1_config(n_r=64, n_theta=96):
     """The settings benchmark_mode = 2 imposes (Benchmarking.F90:150-199: Christensen et al.
     2001, MHD case 1: case 0's settings with magnetism, Pm = 5 and insulating boundaries)."""
     return replace(c2001_case0_config(n_r, n_theta), magnetism=True, magnetic_prandtl=5.0)
+
+
+def anelastic_mhd_config(n_r=128, l_max=255, **kw):
+    """The anelastic MHD step workload: the nondimensional polytrope (reference_type 3,
+    Polytropic_ReferenceND) with 5 density scale heights and polytropic index 2 in a
+    shell of radius ratio 0.35; fields W, Z, P, S (entropy in T's place), C, A;
+    stress-free, fixed-entropy, insulating boundaries; viscous and ohmic heating on
+    (Controls.F90:64-65).  Ek = 1e-3, Pr = 1, Pm = 2, Ra* = 0.5, dt = 1e-4 rotation times."""
+    base = dict(n_r=n_r, l_max=l_max, aspect_ratio=0.35, shell_depth=1.0, reference_type=3, poly_n=2.0,
+                poly_nrho=5.0, modified_rayleigh=0.5, ekman=1.0e-3, prandtl=1.0, magnetic_prandtl=2.0,
+                magnetism=True, rotation=True, no_slip_top=False, no_slip_bottom=False, t_top=0.0,
+                t_bottom=1.0, dt=1.0e-4)
+    base.update(kw)
+    return Config(**base)
 
 
 def seeded_state(cfg: Config, seed=0x5241594C, amp=1.0e-3, lmin=1, lmax_pert=20, cheby=None):

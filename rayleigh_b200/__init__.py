@@ -52,6 +52,14 @@ class _Config(ctypes.Structure):
         ("dt", ctypes.c_double), ("alpha_implicit", ctypes.c_double),
         ("precision", ctypes.c_int), ("use_graph", ctypes.c_int), ("device", ctypes.c_int),
         ("autotune", ctypes.c_int),
+        ("reference_type", ctypes.c_int),
+        ("poly_n", ctypes.c_double), ("poly_nrho", ctypes.c_double), ("poly_mass", ctypes.c_double),
+        ("poly_rho_i", ctypes.c_double), ("pressure_specific_heat", ctypes.c_double),
+        ("angular_velocity", ctypes.c_double), ("modified_rayleigh", ctypes.c_double),
+        ("nu_type", ctypes.c_int), ("kappa_type", ctypes.c_int), ("eta_type", ctypes.c_int),
+        ("nu_power", ctypes.c_double), ("kappa_power", ctypes.c_double), ("eta_power", ctypes.c_double),
+        ("nu_top", ctypes.c_double), ("kappa_top", ctypes.c_double), ("eta_top", ctypes.c_double),
+        ("viscous_heating", ctypes.c_int), ("ohmic_heating", ctypes.c_int),
     ]
 
 
@@ -119,6 +127,26 @@ class Config:
     use_graph: bool = True
     device: int = 0
     autotune: bool = False
+    # reference state: 1 Boussinesq, 2 dimensional polytrope, 3 nondimensional polytrope
+    reference_type: int = 1
+    poly_n: float = 0.0
+    poly_nrho: float = 0.0
+    poly_mass: float = 0.0
+    poly_rho_i: float = 0.0
+    pressure_specific_heat: float = 1.0
+    angular_velocity: float = -1.0
+    modified_rayleigh: float = -1.0
+    nu_type: int = 1
+    kappa_type: int = 1
+    eta_type: int = 1
+    nu_power: float = 0.0
+    kappa_power: float = 0.0
+    eta_power: float = 0.0
+    nu_top: float = -1.0
+    kappa_top: float = -1.0
+    eta_top: float = -1.0
+    viscous_heating: bool = True
+    ohmic_heating: bool = True
 
     def to_c(self):
         c = _Config()

@@ -5,6 +5,7 @@
 The shared library lands next to this file, so it travels with the source
 tree; nothing is installed into site-packages.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -45,14 +46,26 @@ def build(force=False, verbose=False, extra=()):
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    # the translation units compile concurrently; an object is reused while it is newer
+    # than its source, every header and this script (and no extra flags were given)
+    newest_dep = max(os.path.getmtime(p) for p in headers() + [__file__])
+    objs, jobs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+        objs.append(obj)
+        fresh = (not force and not extra and os.path.exists(obj)
+                 and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_dep))
+        if not fresh:
+            jobs.append([nvcc(), *ARCH, *FLAGS, *extra, "-c", src, "-o", obj])
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, cmd) for cmd in jobs]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     if verbose:

@@ -264,7 +264,7 @@ void mixed_setup(Ctx& c) {
     }
     setup_lt_inverse(c);
     setup_lt_forward(c);
-    setup_solve(c);
+    if (c.mixed_solve) setup_solve(c);
 }
 
 static void free_plan(MixedPlan& p) {

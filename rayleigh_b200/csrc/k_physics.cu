@@ -240,7 +240,8 @@ struct PhysParams {
 // One CTA = one (theta, r) row; the rows theta and pi - theta of a pair form a
 // 2-CTA cluster that folds its spectra through distributed shared memory.
 constexpr int ROW_THREADS = 384;
-enum { RC_RAD, RC_ORAD, RC_RHO, RC_DLNRHO, RC_DR, RC_CS, RC_SN, RC_CSC, RC_COT, RC_COR, RC_C2R, RC_HSF, RC_COUNT };
+enum { RC_RAD, RC_ORAD, RC_RHO, RC_DLNRHO, RC_DR, RC_CS, RC_SN, RC_CSC, RC_COT, RC_COR, RC_C2R, RC_HSF, RC_VH, RC_OH,
+       RC_COUNT };
 constexpr int FB = 4;   // fields per batched FFT
 
 // Shared memory of a row CTA (double2 units): one in-place FFT buffer of FB
@@ -559,7 +560,7 @@ __device__ __forceinline__ void r2c_finish(double2* a, int nf, int L, const doub
     }
 }
 
-template <int NTH, bool MAG>
+template <int NTH, bool MAG, bool HEAT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) physics_kernel(PhysParams P) {
     constexpr int N = NTH;
     constexpr int FS = fstride(N);
@@ -595,96 +596,208 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
         rowc[RC_COR] = P.rotation ? P.coriolis : 0.0;
         rowc[RC_C2R] = csc * csc * orad;
         rowc[RC_HSF] = 0.5 * (P.radial[R_DENSITY * nr + r] * P.radial[R_RADIUS * nr + r] * csc);
+        rowc[RC_VH] = P.radial[R_VISC_HEAT * nr + r];
+        rowc[RC_OH] = P.radial[R_OHM_HEAT * nr + r];
     }   // read after row_c2r's first barrier
 
     double2 vr[ZPT], vt[ZPT], vp[ZPT];
     double2 y[FB][ZPT];
     auto acc_at = [&](int f, int q) -> double2& { return acc[SW(f * FS + t + q * ROW_THREADS)]; };
     auto live = [&](int q) { return t + q * ROW_THREADS < N; };
-    // B1: v_r, v_theta, v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
-    {
-        const int fo[4] = {A_VR, A_VT, A_VP, A_DVRDR};
-        const bool dp[4] = {false, false, false, false};
-        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-        const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], dlnrho = rowc[RC_DLNRHO];
-        const double cs = rowc[RC_CS], sn = rowc[RC_SN], csc = rowc[RC_CSC], cot = rowc[RC_COT], cor = rowc[RC_COR];
+    if constexpr (HEAT) {
+        // The anelastic form: the same terms, with the viscous heating
+        // (Compute_Viscous_Heating, Sphere_Physical_Space.F90:337-443) in T's accumulator.
+        // Its strain-rate components are products across fields, so the batches are
+        // regrouped for each component to complete inside one batch:
+        //   H1: v_r, v_theta, v_phi
+        //   H2: dv_r/dtheta, dv_r/dphi, dv_theta/dr, dv_phi/dr  -> 2 e_r_theta, 2 e_r_phi
+        //   H3: dv_phi/dphi, omega_r, dv_theta/dphi, dv_r/dr    -> e_rr, e_theta_theta,
+        //       e_phi_phi, 2 e_phi_theta (dv_theta/dtheta, dv_phi/dtheta as :226-248 form them)
+        //   H4: dT/dr, dT/dtheta, dT/dphi
+        {
+            const int fo[3] = {A_VR, A_VT, A_VP};
+            const bool dp[3] = {false, false, false};
+            row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], dlnrho = rowc[RC_DLNRHO];
+            const double cs = rowc[RC_CS], sn = rowc[RC_SN], csc = rowc[RC_CSC], cot = rowc[RC_COT], cor = rowc[RC_COR];
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            vr[q] = y[0][q];
-            vt[q] = y[1][q];
-            vp[q] = y[2][q];
-            vt[q].x *= csc;
-            vt[q].y *= csc;
-            vp[q].x *= csc;
-            vp[q].y *= csc;
-            const double2 x = y[3][q];
-            auto w0 = [&](double a, double b, double c, double xx) {
-                return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
-            };
-            auto p0 = [&](double a, double b, double c, double xx) {
-                return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
-            };
-            auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
-            if (live(q)) {
-                acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
-                acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
-                acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+            for (int q = 0; q < ZPT; ++q) {
+                vr[q] = y[0][q];
+                vt[q] = make_double2(y[1][q].x * csc, y[1][q].y * csc);
+                vp[q] = make_double2(y[2][q].x * csc, y[2][q].y * csc);
+                auto w0 = [&](double b, double c) { return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c); };
+                auto p0 = [&](double a, double b, double c) {
+                    return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c;
+                };
+                auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+                if (live(q)) {
+                    acc_at(0, q) = make_double2(w0(vt[q].x, vp[q].x), w0(vt[q].y, vp[q].y));
+                    acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x), p0(vr[q].y, vt[q].y, vp[q].y));
+                    acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+                }
             }
         }
-    }
-    // B2: dv_r/dtheta, dv_r/dphi, dv_theta/dr, dv_theta/dphi
-    {
-        const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
-        const bool dp[4] = {false, true, false, true};
-        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-        const double rad = rowc[RC_RAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+        {
+            const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_DVPDR};
+            const bool dp[4] = {false, true, false, false};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC];
+            const double dlnrho = rowc[RC_DLNRHO], vh = rowc[RC_VH];
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
-            double2& w = acc_at(0, q);
-            double2& pp = acc_at(1, q);
-            double2& z = acc_at(3, q);
-            w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
-            w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
-            pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
-            pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
-            z.x += vt[q].x * d.x * c2r;
-            z.y += vt[q].y * d.y * c2r;
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                double2& w = acc_at(0, q);
+                double2& pp = acc_at(1, q);
+                double2& z = acc_at(3, q);
+                // a = sin(theta) dv_r/dtheta, b = dv_r/dphi, c = sin(theta) dv_theta/dr, d = sin(theta) dv_phi/dr
+                auto terms = [&](double a, double b, double c, double d, double vrr, double vtt, double vpp, double& wv,
+                                 double& pv, double& zv) {
+                    wv += -rho * rad * vtt * a * csc - rho * rad * csc * vpp * b;
+                    pv += vrr * c * csc;
+                    zv += vrr * d * csc;
+                    const double erth = (a * csc - vtt) * orad + c * csc;   // 2 e_r_theta
+                    const double erph = (b * csc - vpp) * orad + d * csc;   // 2 e_r_phi
+                    const double dv = -vrr * dlnrho;                        // div u
+                    return vh * (erth * erth * 0.5 + erph * erph * 0.5 - dv * dv * (1.0 / 3.0));
+                };
+                const double hx = terms(y[0][q].x, y[1][q].x, y[2][q].x, y[3][q].x, vr[q].x, vt[q].x, vp[q].x, w.x,
+                                        pp.x, z.x);
+                const double hy = terms(y[0][q].y, y[1][q].y, y[2][q].y, y[3][q].y, vr[q].y, vt[q].y, vp[q].y, w.y,
+                                        pp.y, z.y);
+                acc_at(2, q) = make_double2(hx, hy);
+            }
         }
-    }
-    // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr (the T term's first part, written)
-    {
-        const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
-        const bool dp[4] = {false, true, false, false};
-        row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-        const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+        {
+            const int fo[4] = {A_VP, A_OMR, A_VT, A_DVRDR};
+            const bool dp[4] = {true, false, true, false};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC];
+            const double cot = rowc[RC_COT], c2r = rowc[RC_C2R], dlnrho = rowc[RC_DLNRHO], vh = rowc[RC_VH];
+            const double csc2 = csc * csc;
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
-            double2& pp = acc_at(1, q);
-            double2& z = acc_at(3, q);
-            z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
-            z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
-            pp.x += -vt[q].x * b.x * c2r;
-            pp.y += -vt[q].y * b.y * c2r;
-            acc_at(2, q) = make_double2(-vr[q].x * d.x, -vr[q].y * d.y);
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                double2& w = acc_at(0, q);
+                double2& pp = acc_at(1, q);
+                double2& tt = acc_at(2, q);
+                double2& z = acc_at(3, q);
+                // a = sin(theta) dv_phi/dphi, b = omega_r, c = sin(theta) dv_theta/dphi, x = dv_r/dr
+                auto terms = [&](double a, double b, double c, double x, double vrr, double vtt, double vpp, double& wv,
+                                 double& pv, double& zv) {
+                    wv += -rho * rad * rad * vrr * x;
+                    pv += -vtt * x + vpp * c * c2r - vtt * a * c2r;
+                    zv += vtt * c * c2r + vpp * a * c2r + vtt * b;
+                    const double dvtdt = -vrr * (rad * dlnrho + 2.0) - rad * x - vtt * cot - a * csc2;
+                    const double dvpdt = rad * b + c * csc2 - vpp * cot;
+                    const double eff = (a * csc2 + vrr + vtt * cot) * orad;     // e_phi_phi
+                    const double ett = (dvtdt + vrr) * orad;                    // e_theta_theta
+                    const double eph = (dvpdt + c * csc2 - vpp * cot) * orad;   // 2 e_phi_theta
+                    return vh * (x * x + eff * eff + ett * ett + eph * eph * 0.5);
+                };
+                tt.x += terms(y[0][q].x, y[1][q].x, y[2][q].x, y[3][q].x, vr[q].x, vt[q].x, vp[q].x, w.x, pp.x, z.x);
+                tt.y += terms(y[0][q].y, y[1][q].y, y[2][q].y, y[3][q].y, vr[q].y, vt[q].y, vp[q].y, w.y, pp.y, z.y);
+            }
         }
-    }
-    // B4: dT/dtheta, dT/dphi
-    {
-        const int fo[2] = {A_DTDT, A_T};
-        const bool dp[2] = {false, true};
-        row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
-        const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
+        {
+            const int fo[3] = {A_DTDR, A_DTDT, A_T};
+            const bool dp[3] = {false, false, true};
+            row_c2r<N, 3, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            if (!live(q)) continue;
-            const double2 a = y[0][q], b = y[1][q];
-            double2& tt = acc_at(2, q);
-            tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
-            tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                const double2 d = y[0][q], a = y[1][q], b = y[2][q];
+                double2& tt = acc_at(2, q);
+                tt.x += -vr[q].x * d.x - a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+                tt.y += -vr[q].y * d.y - a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+            }
+        }
+    } else {
+        // B1: v_r, v_theta, v_phi, dv_r/dr: the quadratic, Coriolis and radial-advection terms
+        {
+            const int fo[4] = {A_VR, A_VT, A_VP, A_DVRDR};
+            const bool dp[4] = {false, false, false, false};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double rad = rowc[RC_RAD], orad = rowc[RC_ORAD], rho = rowc[RC_RHO], dlnrho = rowc[RC_DLNRHO];
+            const double cs = rowc[RC_CS], sn = rowc[RC_SN], csc = rowc[RC_CSC], cot = rowc[RC_COT], cor = rowc[RC_COR];
+    #pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                vr[q] = y[0][q];
+                vt[q] = y[1][q];
+                vp[q] = y[2][q];
+                vt[q].x *= csc;
+                vt[q].y *= csc;
+                vp[q].x *= csc;
+                vp[q].y *= csc;
+                const double2 x = y[3][q];
+                auto w0 = [&](double a, double b, double c, double xx) {
+                    return rho * (rad * b * b + rad * c * c + cor * sn * rad * rad * c) - rho * rad * rad * a * xx;
+                };
+                auto p0 = [&](double a, double b, double c, double xx) {
+                    return -b * b * cot * orad - b * a * orad - b * a * dlnrho - c * c * cot * orad - cor * cs * c - b * xx;
+                };
+                auto z0 = [&](double a, double b, double c) { return c * a * orad + cor * (cs * b + sn * a); };
+                if (live(q)) {
+                    acc_at(0, q) = make_double2(w0(vr[q].x, vt[q].x, vp[q].x, x.x), w0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                    acc_at(1, q) = make_double2(p0(vr[q].x, vt[q].x, vp[q].x, x.x), p0(vr[q].y, vt[q].y, vp[q].y, x.y));
+                    acc_at(3, q) = make_double2(z0(vr[q].x, vt[q].x, vp[q].x), z0(vr[q].y, vt[q].y, vp[q].y));
+                }
+            }
+        }
+        // B2: dv_r/dtheta, dv_r/dphi, dv_theta/dr, dv_theta/dphi
+        {
+            const int fo[4] = {A_DVRDT, A_VR, A_DVTDR, A_VT};
+            const bool dp[4] = {false, true, false, true};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double rad = rowc[RC_RAD], rho = rowc[RC_RHO], csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+    #pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
+                double2& w = acc_at(0, q);
+                double2& pp = acc_at(1, q);
+                double2& z = acc_at(3, q);
+                w.x += -rho * rad * vt[q].x * a.x * csc - rho * rad * csc * vp[q].x * b.x;
+                w.y += -rho * rad * vt[q].y * a.y * csc - rho * rad * csc * vp[q].y * b.y;
+                pp.x += vr[q].x * c.x * csc + vp[q].x * d.x * c2r;
+                pp.y += vr[q].y * c.y * csc + vp[q].y * d.y * c2r;
+                z.x += vt[q].x * d.x * c2r;
+                z.y += vt[q].y * d.y * c2r;
+            }
+        }
+        // B3: dv_phi/dr, dv_phi/dphi, omega_r, dT/dr (the T term's first part, written)
+        {
+            const int fo[4] = {A_DVPDR, A_VP, A_OMR, A_DTDR};
+            const bool dp[4] = {false, true, false, false};
+            row_c2r<N, 4, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double csc = rowc[RC_CSC], c2r = rowc[RC_C2R];
+    #pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                const double2 a = y[0][q], b = y[1][q], c = y[2][q], d = y[3][q];
+                double2& pp = acc_at(1, q);
+                double2& z = acc_at(3, q);
+                z.x += vr[q].x * a.x * csc + vp[q].x * b.x * c2r + vt[q].x * c.x;
+                z.y += vr[q].y * a.y * csc + vp[q].y * b.y * c2r + vt[q].y * c.y;
+                pp.x += -vt[q].x * b.x * c2r;
+                pp.y += -vt[q].y * b.y * c2r;
+                acc_at(2, q) = make_double2(-vr[q].x * d.x, -vr[q].y * d.y);
+            }
+        }
+        // B4: dT/dtheta, dT/dphi
+        {
+            const int fo[2] = {A_DTDT, A_T};
+            const bool dp[2] = {false, true};
+            row_c2r<N, 2, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+            const double csc = rowc[RC_CSC], orad = rowc[RC_ORAD];
+    #pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                if (!live(q)) continue;
+                const double2 a = y[0][q], b = y[1][q];
+                double2& tt = acc_at(2, q);
+                tt.x += -a.x * csc * vt[q].x * orad - vp[q].x * b.x * csc * orad;
+                tt.y += -a.y * csc * vt[q].y * orad - vp[q].y * b.y * csc * orad;
+            }
         }
     }
     // CFL (Find_MyMinDT); the rho r / sin(theta) factor of the P and Z terms is a
@@ -722,6 +835,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
                 bp[q] = make_double2(y[2][q].x * csc * orad, y[2][q].y * csc * orad);
                 cbr[q] = y[3][q];
                 if (!live(q)) continue;
+                if constexpr (HEAT) {   // Compute_Ohmic_Heating (:446-466), the (curl B)_r part
+                    const double oh = rowc[RC_OH];
+                    acc_at(2, q).x += cbr[q].x * cbr[q].x * oh;
+                    acc_at(2, q).y += cbr[q].y * cbr[q].y * oh;
+                }
                 cmax = fmax(cmax, (bt[q].x * bt[q].x + bp[q].x * bp[q].x) * hfb);
                 cmax = fmax(cmax, (bt[q].y * bt[q].y + bp[q].y * bp[q].y) * hfb);
                 cmax = fmax(cmax, br[q].x * br[q].x * rfb);
@@ -776,6 +894,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS, 2) phys
                 pp.y -= lcr * (cbp.y * br[q].y - cbr[q].y * bp[q].y);
                 z.x -= lcr * (cbr[q].x * bt[q].x - cbt.x * br[q].x);
                 z.y -= lcr * (cbr[q].y * bt[q].y - cbt.y * br[q].y);
+                if constexpr (HEAT) {   // the (curl B)_theta and (curl B)_phi parts
+                    const double oh = rowc[RC_OH];
+                    acc_at(2, q).x += (cbt.x * cbt.x + cbp.x * cbp.x) * oh;
+                    acc_at(2, q).y += (cbt.y * cbt.y + cbp.y * cbp.y) * oh;
+                }
             }
         }
     }
@@ -859,6 +982,9 @@ void physics_prepare(Ctx& c) {
         throw ArgError("n_theta " + std::to_string(c.d.nth) + " has no physical-space kernel instance");
     if (c.mag && !physics_form1_supported(c.d.nth))   // the magnetic terms live in that kernel only
         throw ArgError("magnetism needs n_theta in 24..768 (2^a or 3*2^a); got " + std::to_string(c.d.nth));
+    if (c.rad.heating && !physics_form1_supported(c.d.nth))   // and so do the heating terms
+        throw ArgError("viscous / ohmic heating needs n_theta in 24..768 (2^a or 3*2^a); got " +
+                       std::to_string(c.d.nth));
 }
 
 // ---------------------------------------------------------------------------
@@ -1197,7 +1323,7 @@ void launch_physics(Ctx& c) {
     if (c.d.L > (2 * c.d.nth) / 3 + 1)
         throw ArgError("n_theta must be at least 3 (l_max + 1) / 2 for the physical-space kernel");
     const unsigned grid = 2u * (unsigned)c.d.nth2 * (unsigned)c.d.nr;   // clusters of 2 rows
-    if (c.physics3_ok && c.physics_form != 1 && !c.mag) {   // last pass in registers (form 0: two CTAs per SM, 2: one)
+    if (c.physics3_ok && c.physics_form != 1 && !c.mag && !c.rad.heating) {   // last pass in registers (form 0: two CTAs per SM, 2: one)
         auto go3 = [&](auto kern, int nt, size_t units) {
             const size_t smem = units * sizeof(double2);
             RA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1229,11 +1355,16 @@ void launch_physics(Ctx& c) {
     };
 #define RA_PHYS_CASE(NN)                                                   \
     case NN:                                                               \
-        if (c.mag)                                                         \
-            go(physics_kernel<NN, true>, NN, RowSmem<NN>::SIZE);           \
+        if (c.mag && heat)                                                 \
+            go(physics_kernel<NN, true, true>, NN, RowSmem<NN>::SIZE);     \
+        else if (c.mag)                                                    \
+            go(physics_kernel<NN, true, false>, NN, RowSmem<NN>::SIZE);    \
+        else if (heat)                                                     \
+            go(physics_kernel<NN, false, true>, NN, RowSmem<NN>::SIZE);    \
         else                                                               \
-            go(physics_kernel<NN, false>, NN, RowSmem<NN>::SIZE);          \
+            go(physics_kernel<NN, false, false>, NN, RowSmem<NN>::SIZE);   \
         break;
+    const bool heat = c.rad.heating;
     switch (c.d.nth) {
         RA_PHYS_CASE(24)
         RA_PHYS_CASE(32)

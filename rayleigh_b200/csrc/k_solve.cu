@@ -7,8 +7,13 @@
 //                       factored in shared memory, the trailing matrix is
 //                       updated in 128-column chunks (FP64 FMA, 8 x 4
 //                       register tiles); pivot ties go to the first row (as
-//                       IDAMAX), a pivot |u_kk| <= n 2^-53 max|A| marks the
-//                       matrix singular.
+//                       IDAMAX), a zero or non-finite pivot marks the
+//                       matrix singular (DGETRF's INFO > 0).  A threshold
+//                       relative to |A| is not used: the anelastic matrices
+//                       in cgs units (the Jones et al. benchmark polytrope)
+//                       have pivots below n 2^-53 of their largest entries,
+//                       even after row and column equilibration, and LAPACK
+//                       factors and solves them.
 //   lu_diag_inv_kernel  the factors rewritten for block substitution with
 //   lu_offdiag_kernel   64-row blocks: M_ij = -L_ii^-1 L_ij (j < i),
 //                       M_ij = -U_ii^-1 U_ij (j > i), M_ii = L_ii^-1 (strictly
@@ -100,11 +105,6 @@ __global__ void __launch_bounds__(LU_THREADS) lu_factor_kernel(double* __restric
         if (t == 0) status[mat] = 0;
         return;
     }
-    double am = 0.0;   // (non-finite entries are refused on the host before a factorisation)
-    int dummy = 0;
-    for (long e = t; e < (long)n * n; e += LU_THREADS) am = fmax(am, fabs(A[e]));
-    block_max_index(am, dummy, red_v, red_i);
-    const double tiny = (double)n * 0x1p-53 * am;
     for (int i = t; i < n; i += LU_THREADS) perm[i] = i;
     if (t == 0) s_bad = 0;
     __syncthreads();
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(LU_THREADS) lu_factor_kernel(double* __restric
                 }
             }
             block_max_index(bv, bi, red_v, red_i);
-            if (!(bv > tiny)) {   // zero, negligible or NaN pivot
+            if (!(bv > 0.0)) {   // zero or NaN pivot
                 if (t == 0) s_bad = 1;
                 break;
             }
@@ -791,7 +791,7 @@ void rebuild_solve_tiles(Ctx& c) {
     for (int l = 0; l < L; ++l) step_cols[l] = 2 * (l + 1);
     make(c.d_solve_tiles, c.n_solve_tiles, step_cols, c.solve_nc);
     make(c.d_solve_tiles_z, c.n_solve_tiles_z, step_cols, c.solve_nc_z);
-    if (c.cfg.precision == RA_PREC_MIXED) {
+    if (c.mixed_solve) {
         make(c.d_inv_sol_tiles, c.n_inv_sol_tiles, std::vector<int>(L, 3 * nr), c.solve_nc);
         make(c.d_inv_sol_tiles_z, c.n_inv_sol_tiles_z, std::vector<int>(L, nr), c.solve_nc_z);
     }
@@ -814,7 +814,7 @@ void factor_matrices(Ctx& c) {
         bad = lu_factor_batch(c.stream, c.lu_work, c.d_Aa, c.d_perm_a, nr, L, c.d_skip_z, &c.launches);
         if (bad) throw SingularError("singular A matrix at l = " + std::to_string(bad - 1));
     }
-    if (c.cfg.precision == RA_PREC_MIXED) {
+    if (c.mixed_solve) {
         const LuSys s0{c.d_Awpt, c.d_perm_wpt, nullptr, c.d_Ainv_wpt, 3 * nr};
         const LuSys s1{c.d_Az, c.d_perm_z, nullptr, c.d_Ainv_z, nr};
         launch_lu_solve(c.stream, c.d_inv_sol_tiles, c.n_inv_sol_tiles, s0, LU_MODE_INVERSE, 0, c.solve_nc);

@@ -29,6 +29,18 @@ static void check_config(const ra_config& cfg) {
     if (!(cfg.shell_depth > 0)) throw ArgError("shell_depth must be positive");
     if (!(cfg.dt > 0)) throw ArgError("dt must be positive");
     if (cfg.precision != RA_PREC_FP64 && cfg.precision != RA_PREC_MIXED) throw ArgError("unknown precision mode");
+    if (cfg.reference_type < 1 || cfg.reference_type > 3)
+        throw ArgError("reference_type must be 1 (Boussinesq), 2 or 3 (polytropes)");
+    if (cfg.reference_type >= 2 && !(cfg.poly_n > 0 && cfg.poly_nrho > 0))
+        throw ArgError("a polytropic reference state needs poly_n > 0 and poly_nrho > 0");
+    if (cfg.reference_type == 2 && !(cfg.poly_mass > 0 && cfg.poly_rho_i > 0 && cfg.pressure_specific_heat > 0 &&
+                                     cfg.nu_top > 0 && cfg.kappa_top > 0 && (!cfg.magnetism || cfg.eta_top > 0)))
+        throw ArgError("reference_type 2 needs poly_mass, poly_rho_i, pressure_specific_heat, nu_top, kappa_top "
+                       "(and eta_top with magnetism) > 0");
+    if (cfg.reference_type == 3 && !(cfg.modified_rayleigh > 0))
+        throw ArgError("reference_type 3 needs modified_rayleigh > 0");
+    for (int t : {cfg.nu_type, cfg.kappa_type, cfg.eta_type})
+        if (t != 1 && t != 2) throw ArgError("transport types 1 (constant) and 2 (density power) are provided");
 }
 
 static Dims make_dims(const ra_config& cfg) {
@@ -79,6 +91,8 @@ static void gauss_legendre(int n, std::vector<long double>& x, std::vector<long 
 // (Chebyshev_Polynomials.F90:65-351; single domain, zeros of T_N).
 static void chebyshev_setup(Ctx& c, double rmin, double rmax) {
     const int n = c.d.nr;
+    c.rad.rmin = rmin;
+    c.rad.rmax = rmax;
     std::vector<double> theta(n), x(n);
     const double dth = M_PI / n;
     double arg = dth * 0.5;
@@ -129,32 +143,137 @@ static void chebyshev_setup(Ctx& c, double rmin, double rmax) {
     }
 }
 
-// Boussinesq reference state and transport coefficients (PDE_Coefficients.F90:335-435, 1766-2098).
+// Reference state and transport coefficients (PDE_Coefficients.F90:216-257, 335-537, 925-1051,
+// 1766-2098): Constant_Reference (Boussinesq), Polytropic_Reference (cgs) or
+// Polytropic_ReferenceND, then Initialize_Diffusivity and Compute_Diffusion_Coefs.
 static void reference_setup(Ctx& c) {
     const ra_config& cfg = c.cfg;
     const int n = c.d.nr;
     Radial& R = c.rad;
     const std::vector<double>& r = R.radius;
+    const bool mag = cfg.magnetism != 0;
     R.delta_r.resize(n);
     R.delta_r[0] = r[0] - r[1];
     for (int i = 1; i < n; ++i) R.delta_r[i] = r[i - 1] - r[i];
     R.density.assign(n, 1.0);
     R.dlnrho.assign(n, 0.0);
+    R.d2lnrho.assign(n, 0.0);
+    R.temperature.assign(n, 1.0);
+    R.dlnT.assign(n, 0.0);
     R.buoy.resize(n);
-    for (int i = 0; i < n; ++i) R.buoy[i] = (cfg.rayleigh / cfg.prandtl) * pow(r[i] / r[0], cfg.gravity_power);
-    const double pscaling = cfg.rotation ? 1.0 / cfg.ekman : 1.0;
+    std::vector<double> visc_amp(n, 2.0), ohm_amp(n, 0.0);
+    double pscaling = 1.0, nu_top, kappa_top, eta_top;
+    bool visc = cfg.viscous_heating != 0, ohm = cfg.ohmic_heating != 0;
+    if (cfg.reference_type == 1) {
+        for (int i = 0; i < n; ++i) R.buoy[i] = (cfg.rayleigh / cfg.prandtl) * pow(r[i] / r[0], cfg.gravity_power);
+        pscaling = cfg.rotation ? 1.0 / cfg.ekman : 1.0;
+        R.coriolis = 2.0 / cfg.ekman;
+        nu_top = 1.0;
+        kappa_top = 1.0 / cfg.prandtl;
+        // magnetism (:418-427): Lorentz_Coeff = 1 / (Pm Ek), eta = 1 / Pm
+        R.lorentz = mag ? 1.0 / (cfg.magnetic_prandtl * cfg.ekman) : 0.0;
+        eta_top = mag ? 1.0 / cfg.magnetic_prandtl : 0.0;
+        std::fill(ohm_amp.begin(), ohm_amp.end(), R.lorentz);
+        visc = ohm = false;   // Constant_Reference turns both heating terms off
+    } else if (cfg.reference_type == 2) {
+        const double G = 6.67e-8, pn = cfg.poly_n;
+        const double ri = r[n - 1], ro = r[0], beta = ri / ro, dd = ro - ri;
+        const double zeta0 = (beta + 1.0) / (beta * exp(cfg.poly_nrho / pn) + 1.0);
+        const double c0 = (2.0 * zeta0 - beta - 1.0) / (1.0 - beta);
+        const double c1 = (1.0 + beta) * (1.0 - zeta0) / ((1.0 - beta) * (1.0 - beta));
+        std::vector<double> zeta(n);
+        for (int i = 0; i < n; ++i) zeta[i] = c0 + c1 * dd / r[i];
+        const double rho_c = cfg.poly_rho_i / pow(zeta[n - 1], pn);
+        const double P_c = G * cfg.poly_mass * rho_c / ((pn + 1.0) * dd * c1);
+        const double T_c = (pn + 1.0) * P_c / (cfg.pressure_specific_heat * rho_c);
+        for (int i = 0; i < n; ++i) {
+            const double gravity = G * cfg.poly_mass / (r[i] * r[i]);
+            R.density[i] = rho_c * pow(zeta[i], pn);
+            R.dlnrho[i] = -pn * c1 * dd / (zeta[i] * r[i] * r[i]);
+            R.d2lnrho[i] = -R.dlnrho[i] * (2.0 / r[i] - c1 * dd / zeta[i] / (r[i] * r[i]));
+            R.temperature[i] = T_c * zeta[i];
+            R.dlnT[i] = -c1 * dd / (r[i] * r[i]) / zeta[i];
+            R.buoy[i] = gravity / cfg.pressure_specific_heat * R.density[i];
+            visc_amp[i] = 2.0 / R.temperature[i];
+        }
+        R.coriolis = 2.0 * cfg.angular_velocity;
+        nu_top = cfg.nu_top;
+        kappa_top = cfg.kappa_top;
+        eta_top = cfg.eta_top;
+        R.lorentz = mag ? 1.0 / (4.0 * M_PI) : 0.0;
+        for (int i = 0; i < n; ++i) ohm_amp[i] = R.lorentz / R.density[i] / R.temperature[i];
+    } else {   // 3: Polytropic_ReferenceND
+        const double pn = cfg.poly_n, beta = cfg.aspect_ratio;
+        const double diss = beta * (exp(cfg.poly_nrho / pn) - 1.0), dtmp = 1.0 / (1.0 - beta);
+        const double rmax = R.rmax;
+        for (int i = 0; i < n; ++i) {
+            const double gravity = rmax * rmax / (r[i] * r[i]);
+            R.temperature[i] = dtmp * diss * (dtmp / r[i] - 1.0) + 1.0;
+            R.density[i] = pow(R.temperature[i], pn);
+            R.buoy[i] = gravity * cfg.modified_rayleigh * R.density[i];
+            R.dlnT[i] = -diss * gravity / R.temperature[i];
+            R.dlnrho[i] = pn * R.dlnT[i];
+            R.d2lnrho[i] = -pn * R.dlnT[i] * R.dlnT[i] + (pn / R.temperature[i]) * (2.0 * diss * gravity / r[i]);
+            visc_amp[i] = 2.0 / R.temperature[i] * diss / cfg.modified_rayleigh;
+        }
+        R.coriolis = 2.0;
+        nu_top = cfg.ekman;
+        kappa_top = cfg.ekman / cfg.prandtl;
+        R.lorentz = mag ? cfg.ekman / cfg.magnetic_prandtl : 0.0;
+        eta_top = mag ? cfg.ekman / cfg.magnetic_prandtl : 0.0;
+        const double otmp = diss * cfg.ekman * cfg.ekman /
+                            (cfg.modified_rayleigh * cfg.magnetic_prandtl * cfg.magnetic_prandtl);
+        for (int i = 0; i < n; ++i) ohm_amp[i] = mag ? otmp / R.density[i] / R.temperature[i] : 0.0;
+    }
     R.dpdr_w.resize(n);
     R.pdwdr.resize(n);
     for (int i = 0; i < n; ++i) {
         R.dpdr_w[i] = R.density[i] * pscaling;
         R.pdwdr[i] = -1.0 * R.density[i] * pscaling;
     }
-    R.coriolis = 2.0 / cfg.ekman;
-    R.nu.assign(n, 1.0);
-    R.kappa.assign(n, 1.0 / cfg.prandtl);
-    // magnetism (PDE_Coefficients.F90:418-427): Lorentz_Coeff = 1 / (Pm Ek), eta = 1 / Pm
-    R.lorentz = cfg.magnetism ? 1.0 / (cfg.magnetic_prandtl * cfg.ekman) : 0.0;
-    R.eta.assign(n, cfg.magnetism ? 1.0 / cfg.magnetic_prandtl : 0.0);
+    // Initialize_Diffusivity / Vary_With_Density (:1906-1981)
+    auto diffusivity = [&](double top, int type, double power, std::vector<double>& x, std::vector<double>& dlnx) {
+        x.assign(n, top);
+        dlnx.assign(n, 0.0);
+        if (type == 2)
+            for (int i = 0; i < n; ++i) {
+                x[i] = top * pow(R.density[i] / R.density[0], power);
+                dlnx[i] = power * R.dlnrho[i];
+            }
+    };
+    diffusivity(nu_top, cfg.nu_type, cfg.nu_power, R.nu, R.dlnu);
+    diffusivity(kappa_top, cfg.kappa_type, cfg.kappa_power, R.kappa, R.dlnkappa);
+    if (mag)
+        diffusivity(eta_top, cfg.eta_type, cfg.eta_power, R.eta, R.dlneta);
+    else {
+        R.eta.assign(n, 0.0);
+        R.dlneta.assign(n, 0.0);
+    }
+    // viscous_heating_coeff = viscous_amp nu, ohmic_heating_coeff = ohmic_amp eta (:1822-1836)
+    R.visc_heat.assign(n, 0.0);
+    R.ohm_heat.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        if (visc) R.visc_heat[i] = visc_amp[i] * R.nu[i];
+        if (mag && ohm) R.ohm_heat[i] = ohm_amp[i] * R.eta[i];
+    }
+    R.heating = visc || (mag && ohm);
+    // Compute_Diffusion_Coefs (:2032-2098)
+    auto sz = [&](std::vector<double>& v) { v.assign(n, 0.0); };
+    for (auto* v : {&R.w_diff0, &R.w_diff1, &R.dw_diff0, &R.dw_diff1, &R.dw_diff2, &R.s_diff1, &R.z_diff0,
+                    &R.z_diff1, &R.a_diff1})
+        sz(*v);
+    for (int i = 0; i < n; ++i) {
+        const double nu = R.nu[i], dlnu = R.dlnu[i], dlnrho = R.dlnrho[i], d2lnrho = R.d2lnrho[i], ri = r[i];
+        R.w_diff0[i] = -nu * (4.0 / 3.0) * (dlnu * dlnrho + d2lnrho + dlnrho / ri + 3.0 * dlnu / ri);
+        R.w_diff1[i] = nu * (2.0 * dlnu - dlnrho / 3.0);
+        R.dw_diff2[i] = (dlnu - dlnrho) * nu;
+        R.dw_diff1[i] = -(d2lnrho + 2.0 / ri * dlnrho + 2.0 / ri * dlnu + dlnu * dlnrho) * nu;
+        R.dw_diff0[i] = -(2.0 * dlnrho / 3.0 + dlnu) * nu;
+        R.s_diff1[i] = R.kappa[i] * (R.dlnkappa[i] + dlnrho + R.dlnT[i]);
+        R.z_diff0[i] = -nu * (2.0 * dlnu / ri + dlnrho * dlnu + d2lnrho + 2.0 * dlnrho / ri);
+        R.z_diff1[i] = nu * (dlnu - dlnrho);
+        R.a_diff1[i] = R.eta[i] * R.dlneta[i];
+    }
 }
 
 // The C (poloidal) and A (toroidal) systems of one l > 0 (Sphere_Linear_Terms.F90:473-499)
@@ -184,7 +303,7 @@ static void build_l_mag(const Ctx& c, int l, std::vector<double>& Cm, std::vecto
         add(Am, MS_A0, 0, i, 1.0, true);
         add(Am, MS_A0, 0, i, H * eta[i], false);
         add(Am, MS_A2, 2, i, 1.0 * eta[i], false);
-        add(Am, MS_A1, 1, i, 0.0, false);   // A_Diffusion_Coefs_1 (constant eta)
+        add(Am, MS_A1, 1, i, c.rad.a_diff1[i], false);   // A_Diffusion_Coefs_1
         add(Cm, MS_C0, 0, i, 1.0, true);
         add(Cm, MS_C0, 0, i, H * eta[i], false);
         add(Cm, MS_C2, 2, i, 1.0 * eta[i], false);
@@ -289,7 +408,7 @@ static void build_l(const Ctx& c, int l, std::vector<double>& A, std::vector<dou
                     A[(size_t)(rb + i) * n3 + cb + j] += amp[i] * fac * Dd[(size_t)i * nr + j];
         }
     };
-    std::vector<double> ones(nr, 1.0), zero(nr, 0.0), v(nr);
+    std::vector<double> ones(nr, 1.0), v(nr);
     const double llp1 = (double)l * (l + 1);
     std::vector<double> H(nr);
     for (int i = 0; i < nr; ++i) H[i] = -llp1 / (r[i] * r[i]);
@@ -302,7 +421,7 @@ static void build_l(const Ctx& c, int l, std::vector<double>& A, std::vector<dou
         add(EQ_T, T_, 0, ones, true);
         add(EQ_T, T_, 1, vec([&](int i) { return 2.0 / r[i] * R.kappa[i]; }), false);
         add(EQ_T, T_, 2, vec([&](int i) { return 1.0 * R.kappa[i]; }), false);
-        add(EQ_T, T_, 1, zero, false);
+        add(EQ_T, T_, 1, R.s_diff1, false);
         add(EQ_P, T_, 0, vec([&](int i) { return -R.buoy[i]; }), true);
         add(EQ_P, P_, 1, R.dpdr_w, true);
         add(EQ_W, W_, 0, ones, true);
@@ -312,26 +431,26 @@ static void build_l(const Ctx& c, int l, std::vector<double>& A, std::vector<dou
         add(EQ_W, W_, 0, ones, true);
         add(EQ_W, W_, 0, vec([&](int i) { return H[i] * R.nu[i]; }), false);
         add(EQ_W, W_, 2, R.nu, false);
-        add(EQ_W, W_, 0, zero, false);
-        add(EQ_W, W_, 1, zero, false);
+        add(EQ_W, W_, 0, R.w_diff0, false);
+        add(EQ_W, W_, 1, R.w_diff1, false);
         add(EQ_P, P_, 0, R.pdwdr, false);
         add(EQ_P, W_, 1, ones, true);
         add(EQ_P, W_, 0, vec([&](int i) { return -R.nu[i] * H[i] * 2.0 / r[i]; }), false);
         add(EQ_P, W_, 1, vec([&](int i) { return H[i] * R.nu[i]; }), false);
         add(EQ_P, W_, 3, R.nu, false);
-        add(EQ_P, W_, 0, zero, false);
-        add(EQ_P, W_, 1, zero, false);
-        add(EQ_P, W_, 2, zero, false);
+        add(EQ_P, W_, 0, vec([&](int i) { return R.dw_diff0[i] * H[i]; }), false);
+        add(EQ_P, W_, 1, R.dw_diff1, false);
+        add(EQ_P, W_, 2, R.dw_diff2, false);
         add(EQ_T, T_, 0, ones, true);
         add(EQ_T, T_, 0, vec([&](int i) { return H[i] * R.kappa[i]; }), false);
         add(EQ_T, T_, 1, vec([&](int i) { return 2.0 / r[i] * R.kappa[i]; }), false);
         add(EQ_T, T_, 2, R.kappa, false);
-        add(EQ_T, T_, 1, zero, false);
+        add(EQ_T, T_, 1, R.s_diff1, false);
         add(EQ_Z, Z_, 0, ones, true);
         add(EQ_Z, Z_, 0, vec([&](int i) { return H[i] * R.nu[i]; }), false);
         add(EQ_Z, Z_, 2, R.nu, false);
-        add(EQ_Z, Z_, 0, zero, false);
-        add(EQ_Z, Z_, 1, zero, false);
+        add(EQ_Z, Z_, 0, R.z_diff0, false);
+        add(EQ_Z, Z_, 1, R.z_diff1, false);
     }
     // Set_Boundary_Conditions (Sphere_Linear_Terms.F90:539-1100):
     // clear boundary rows, then Load_Single_Row_Cheby over the dealiased columns
@@ -426,6 +545,7 @@ static void autotune(Ctx& c, int nreps, double* ms_out);
 static void setup(Ctx& c) {
     const Dims& d = c.d;
     c.mag = c.cfg.magnetism != 0;
+    c.mixed_solve = c.cfg.precision == RA_PREC_MIXED && c.cfg.reference_type != 2;
     c.nfa = c.mag ? (int)NP2A_MAG : (int)NP2A;
     c.nfb = c.mag ? (int)NP2B_MAG : (int)NP2B;
     c.ng = c.mag ? (int)NG_MAG : (int)NG;
@@ -492,6 +612,8 @@ static void setup(Ctx& c) {
         rp[R_DRHO_TERM * nr + i] = c.rad.dlnrho[i] + oor;
         rp[R_TWO_OVER_R * nr + i] = 2.0 / r;
         rp[R_OVER_RSQ * nr + i] = oor2;
+        rp[R_VISC_HEAT * nr + i] = c.rad.visc_heat[i];
+        rp[R_OHM_HEAT * nr + i] = c.rad.ohm_heat[i];
     }
     // device buffers
     const long nlm = d.nlm;
@@ -513,7 +635,7 @@ static void setup(Ctx& c) {
         RA_CUDA(cudaMemcpyAsync(c.d_skip_z, skip.data(), skip.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
     }
-    if (c.cfg.precision == RA_PREC_MIXED) {
+    if (c.mixed_solve) {
         dalloc(c.d_Ainv_wpt, (size_t)d.L * 9 * nr * nr);
         dalloc(c.d_Ainv_z, (size_t)d.L * nr * nr);
     }
@@ -539,7 +661,7 @@ static void setup(Ctx& c) {
         dalloc(c.d_s2am, (size_t)nlm * NS2AM * 2 * nr);
         dalloc(c.d_Ac, (size_t)d.L * nr * nr);
         dalloc(c.d_Aa, (size_t)d.L * nr * nr);
-        if (c.cfg.precision == RA_PREC_MIXED) {
+        if (c.mixed_solve) {
             dalloc(c.d_Ainv_c, (size_t)d.L * nr * nr);
             dalloc(c.d_Ainv_a, (size_t)d.L * nr * nr);
         }
@@ -673,7 +795,7 @@ static void run_stage(Ctx& c, int k, double new_ab, double old_ab) {
             if (c.mag) launch_rlm_b_mag(c, new_ab);
             break;
         default:
-            if (mixed) {
+            if (c.mixed_solve) {
                 launch_solve_mixed(c);   // every system, C and A included
             } else {
                 launch_solve(c);
@@ -876,7 +998,7 @@ static void move_modes(Ctx& c, int nmodes, const int* l_of, const int* m_of, con
 static std::vector<int> knob_candidates(const Ctx& c, int knob) {
     if (knob == 0) {   // physics
         std::vector<int> v;
-        if (c.physics3_ok && !c.mag) {   // the magnetic terms exist in form 1 only
+        if (c.physics3_ok && !c.mag && !c.rad.heating) {   // the magnetic and heating terms exist in form 1 only
             v.push_back(0);
             v.push_back(2);
         }
@@ -945,7 +1067,7 @@ static void autotune(Ctx& c, int nreps, double* ms_out) {
                     RA_CUDA(cudaMemsetAsync(c.d_cfl, 0, sizeof(unsigned long long), c.stream));
                     launch_physics(c);
                 } else {
-                    if (c.cfg.precision == RA_PREC_MIXED) return;   // the mixed form solves by split products
+                    if (c.mixed_solve) return;   // the mixed form solves by split products
                     launch_solve(c);
                 }
             };
@@ -1030,6 +1152,13 @@ int ra_default_config(ra_config* cfg) {
     cfg->use_graph = 1;
     cfg->device = 0;
     cfg->autotune = 0;
+    cfg->reference_type = 1;
+    cfg->pressure_specific_heat = 1.0;
+    cfg->angular_velocity = -1.0;
+    cfg->modified_rayleigh = -1.0;
+    cfg->nu_type = cfg->kappa_type = cfg->eta_type = 1;
+    cfg->nu_top = cfg->kappa_top = cfg->eta_top = -1.0;
+    cfg->viscous_heating = cfg->ohmic_heating = 1;
     return RA_OK;
 }
 
@@ -1084,7 +1213,7 @@ int ra_set_dt(ra_ctx* ctx, double dt) {
         if (!(dt > 0)) throw ArgError("dt must be positive");
         ctx->c.dt = dt;
         linear_setup(ctx->c);
-        if (ctx->c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(ctx->c);
+        if (ctx->c.mixed_solve) mixed_resplit_solve(ctx->c);
     });
 }
 
@@ -1294,7 +1423,7 @@ int ra_factor(ra_ctx* ctx, double dt) {
                                  : "ra_factor needs both systems loaded by ra_load_matrices");
         c.dt = dt;
         factor_matrices(c);
-        if (c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(c);
+        if (c.mixed_solve) mixed_resplit_solve(c);
         c.matrices_loaded = 0;
     });
 }
@@ -1495,7 +1624,7 @@ int ra_step_adaptive(ra_ctx* ctx, int nsteps, const ra_dt_controls* ctl, double*
             if (nd != c.dt) {   // Reset_Linear_Equations before the next step
                 c.dt = nd;
                 linear_setup(c);
-                if (c.cfg.precision == RA_PREC_MIXED) mixed_resplit_solve(c);
+                if (c.mixed_solve) mixed_resplit_solve(c);
                 ++changes;
             }
         }

@@ -81,6 +81,14 @@ struct Radial {
     double coriolis;
     std::vector<double> eta;     // magnetic diffusivity (magnetism)
     double lorentz = 0.0;        // Lorentz_Coeff
+    double rmin = 0.0, rmax = 0.0;
+    // the rest of the reference state and of the transport profiles (anelastic terms)
+    std::vector<double> d2lnrho, temperature, dlnT, dlnu, dlnkappa, dlneta;
+    // Compute_Diffusion_Coefs (PDE_Coefficients.F90:2032-2098)
+    std::vector<double> w_diff0, w_diff1, dw_diff0, dw_diff1, dw_diff2, s_diff1, z_diff0, z_diff1, a_diff1;
+    // viscous_heating_coeff, ohmic_heating_coeff (zero when the term is off)
+    std::vector<double> visc_heat, ohm_heat;
+    bool heating = false;        // either heating term is on
 };
 
 struct GemmTile { int item, mt, nt, par; };
@@ -131,6 +139,10 @@ struct Ctx {
     bool have_state = false;
     long launches = 0;
     bool mag = false;                                 // the magnetic equation set (C, A)
+    // RA_PREC_MIXED solves by split products of the explicit inverses; with the cgs
+    // polytrope (reference_type 2) its matrices are too badly conditioned for an explicit
+    // inverse and the mixed form solves by the FP64 block substitution
+    bool mixed_solve = false;
     int nfa = NP2A, nfb = NP2B, ng = NG;              // fields of s2a11/p2a, of p2b/s2b, grids (more with mag)
 
     Radial rad;
@@ -204,7 +216,7 @@ constexpr int RA_STATUS_NONFINITE = 2;   // a NaN/Inf reached the right-hand sid
 
 // radial profile packing in d_radial: index k * nr + r
 enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R,
-       R_OVER_RSQ, R_COUNT };
+       R_OVER_RSQ, R_VISC_HEAT, R_OHM_HEAT, R_COUNT };
 
 // ---- kernels / launchers (defined in the .cu files) ----
 void launch_plm(Ctx& c, const double* d_x, const double* d_w);

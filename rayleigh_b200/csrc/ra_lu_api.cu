@@ -158,7 +158,7 @@ int ra_lu_factor(ra_lu* lu, const double* a, double* ms) {
         cudaEventDestroy(e1);
         if (ms) *ms = t;
         if (bad) throw SingularError("singular matrix " + std::to_string(bad - 1) +
-                                     " (a pivot |u_kk| <= n 2^-53 max|A|)");
+                                     " (a zero pivot)");
         if (lu->d_mf) {
             cudaFree(lu->d_mf);
             lu->d_mf = nullptr;

@@ -54,6 +54,37 @@ def test_default_config_and_argument_errors_without_gpu():
     lib.ra_destroy(h)
 
 
+def test_config_layout_and_defaults_agree():
+    """The Python dataclass, its ctypes mirror and ra_default_config describe the same
+    struct: every field of the C defaults equals the dataclass default."""
+    import dataclasses
+    import rayleigh_b200 as rb
+    lib = rb.load_library()
+    c = rb._Config()
+    assert lib.ra_default_config(ctypes.byref(c)) == 0
+    names = [f[0] for f in rb._Config._fields_]
+    assert names == [f.name for f in dataclasses.fields(rb.Config)]
+    py = rb.Config().to_c()
+    for n in names:
+        assert getattr(c, n) == getattr(py, n), n
+
+
+def test_reference_state_arguments_are_checked():
+    import rayleigh_b200 as rb
+    lib = rb.load_library()
+    for kw, word in ((dict(reference_type=4), b"reference_type"), (dict(reference_type=3), b"poly"),
+                     (dict(reference_type=3, poly_n=2.0, poly_nrho=5.0), b"modified_rayleigh"),
+                     (dict(reference_type=2, poly_n=2.0, poly_nrho=5.0), b"poly_mass"),
+                     (dict(nu_type=3), b"transport")):
+        cfg = rb.Config(**kw).to_c()
+        h = ctypes.c_void_p()
+        assert lib.ra_create(ctypes.byref(h), ctypes.byref(cfg)) == rb.RA_ERR_ARG, kw
+        buf = ctypes.create_string_buffer(256)
+        lib.ra_last_error(h, buf, 256)
+        assert word in buf.value, (kw, buf.value)
+        lib.ra_destroy(h)
+
+
 def test_diagnostic_quantity_codes_are_the_references():
     """RA_Q_* in the header, the Python names and the reference's output codes
     (velocity_field_codes.F: voffset = 0; vorticity_field_codes.F: vort_off = 300;

@@ -8,6 +8,10 @@ import pytest
 import oracle as O
 
 
+ANEL = dict(n_r=32, l_max=7, dt=1e-4, reference_type=3, poly_n=2.0, poly_nrho=5.0, modified_rayleigh=0.5,
+            ekman=1e-3, no_slip_top=False, no_slip_bottom=False)
+
+
 def _slots():
     # (eq, var, dorder) of the 16 coefficient slots, in the order the C ABI documents
     W, P, T, Z = O.WVAR, O.PVAR, O.TVAR, O.ZVAR
@@ -21,6 +25,15 @@ def _slots():
     dict(n_r=32, l_max=7, dt=1e-4, no_slip_top=False, no_slip_bottom=False, fix_tvar_bottom=False, dtdr_bottom=-1.0,
          rotation=False),
     dict(n_r=128, l_max=7, dt=1e-5, ekman=1e-4, rayleigh=1e5),   # the batched-solve workload's radial size
+    # anelastic: the nondimensional polytrope (5 scale heights, n = 2), constant and
+    # density-dependent diffusivities, and the dimensional (cgs) polytrope of the Jones et al.
+    # hydrodynamic benchmark (Benchmarking.F90:202-247)
+    ANEL,
+    dict(ANEL, nu_type=2, nu_power=-0.5, kappa_type=2, kappa_power=-0.5, no_slip_bottom=True),
+    dict(n_r=32, l_max=7, dt=30.0, reference_type=2, shell_depth=4.55e9, aspect_ratio=0.35, poly_n=2.0,
+         poly_nrho=5.0, poly_mass=1.9e30, poly_rho_i=1.1, pressure_specific_heat=1.0509e8,
+         angular_velocity=1.76e-4, nu_top=3.64364e12, kappa_top=3.64364e12, no_slip_top=False,
+         no_slip_bottom=False, t_bottom=851225.7),
 ])
 def test_build_matrices_match_oracle(cfg):
     import rayleigh_b200 as rb
@@ -42,7 +55,7 @@ def test_build_matrices_match_oracle(cfg):
             if ref_c is None:
                 assert not np.any(cw[l, s]), (l, key)
             else:
-                np.testing.assert_allclose(cw[l, s], ref_c, rtol=1e-14, atol=1e-300)
+                np.testing.assert_allclose(cw[l, s], ref_c, rtol=1e-13, atol=1e-15 * np.abs(ref_c).max())
 
 
 def test_build_matrices_argument_errors():
@@ -54,13 +67,16 @@ def test_build_matrices_argument_errors():
         rb.build_matrices(rb.Config(n_r=7, l_max=7), 0, 0, 1)
 
 
-@pytest.mark.parametrize("n_r", [24, 128])
-def test_build_magnetic_matrices_match_oracle(n_r):
+@pytest.mark.parametrize("n_r,anelastic", [(24, False), (128, False), (32, True)])
+def test_build_magnetic_matrices_match_oracle(n_r, anelastic):
     """The C (poloidal) and A (toroidal) systems of the dynamo equation set with the
     insulating (potential-field) boundary rows (Sphere_Linear_Terms.F90:473-499, 1041-1077)
-    and their Post_Solve coefficients."""
+    and their Post_Solve coefficients; on the polytrope with a density-dependent eta the
+    A equation carries A_Diffusion_Coefs_1 = eta dln(eta)/dr."""
     import rayleigh_b200 as rb
     cfg = dict(n_r=n_r, l_max=7, dt=2e-4, ekman=1e-3, rayleigh=1e5, magnetism=True, magnetic_prandtl=5.0)
+    if anelastic:
+        cfg.update(ANEL, n_r=n_r, magnetism=True, magnetic_prandtl=2.0, eta_type=2, eta_power=-0.5)
     o = O.Oracle(O.Config(**cfg))
     L = 8
     rc = rb.Config(**cfg)
@@ -71,8 +87,10 @@ def test_build_magnetic_matrices_match_oracle(n_r):
         for got, ref in ((cm[l - 1].T, o.mat_c[l]), (am[l - 1].T, o.mat_a[l])):
             assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), l
         for s, d in enumerate((0, 2)):
-            np.testing.assert_allclose(cc[l - 1, s], o.coefs[l][(O.CEQ, C, d)], rtol=1e-14, atol=1e-300)
+            ref_c = o.coefs[l][(O.CEQ, C, d)]
+            np.testing.assert_allclose(cc[l - 1, s], ref_c, rtol=1e-13, atol=1e-15 * np.abs(ref_c).max())
         for s, d in enumerate((0, 1, 2)):
-            np.testing.assert_allclose(ac[l - 1, s], o.coefs[l][(O.AEQ, A, d)], rtol=1e-14, atol=1e-300)
+            ref_c = o.coefs[l][(O.AEQ, A, d)]
+            np.testing.assert_allclose(ac[l - 1, s], ref_c, rtol=1e-13, atol=1e-15 * np.abs(ref_c).max())
     with pytest.raises(rb.RayleighError):   # no magnetic systems without magnetism
         rb.build_matrices(rb.Config(n_r=24, l_max=7), 2, 1, 2)

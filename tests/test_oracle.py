@@ -194,3 +194,80 @@ def test_c2001_case0_matches_the_reference_regression_report():
         assert len(vals) == gold["samples"]
         assert abs(vals.mean() - ref["measured"]) < 5e-6, (name, vals.mean(), ref)
         assert abs(vals.std() - ref["sdev"]) < 5e-6, (name, vals.std(), ref)
+
+
+def _spectral_d(o, f, d):
+    c = o.cg.to_spectral(f[None, None, :])
+    return o.cg.from_spectral(o.cg.deriv(c, d))[0, 0]
+
+
+def test_nondimensional_polytrope_known_answers():
+    """Polytropic_ReferenceND (PDE_Coefficients.F90:437-537): T = rho = 1 at the outer
+    radius, rho(r_i) / rho(r_o) = exp(N_rho), the adiabatic gradient dT/dr = -D g with
+    D = beta (exp(N_rho / n) - 1), and dln(rho)/dr, d2ln(rho)/dr2 the derivatives of ln rho."""
+    o = O.Oracle(O.anelastic_mhd_config(n_r=64, l_max=7))
+    cfg = o.cfg
+    assert abs(o.temperature[0] - 1.0) < 1e-14 and abs(o.density[0] - 1.0) < 1e-14
+    assert abs(o.density[-1] / o.density[0] - math.exp(cfg.poly_nrho)) < 1e-12 * math.exp(cfg.poly_nrho)
+    diss = cfg.aspect_ratio * (math.exp(cfg.poly_nrho / cfg.poly_n) - 1.0)
+    g = o.rmax ** 2 / o.radius ** 2
+    np.testing.assert_allclose(_spectral_d(o, o.temperature, 1), -diss * g, rtol=1e-9)
+    lr = np.log(o.density)
+    np.testing.assert_allclose(_spectral_d(o, lr, 1), o.dlnrho, rtol=1e-9)
+    np.testing.assert_allclose(_spectral_d(o, lr, 2), o.d2lnrho, rtol=1e-7)
+    # Boussinesq limits of the anelastic coefficients vanish; here they do not
+    assert np.abs(o.w_diff0).max() > 0 and np.abs(o.s_diff1).max() > 0
+
+
+def test_dimensional_polytrope_is_hydrostatic():
+    """Polytropic_Reference (PDE_Coefficients.F90:925-1051) on the Jones et al. benchmark's
+    values: rho(r_i) = poly_rho_i, rho(r_i) / rho(r_o) = exp(N_rho), and the ideal-gas
+    pressure P = c_P rho T / (n + 1) is in hydrostatic balance, dP/dr = -rho G M / r^2."""
+    cfg = O.Config(n_r=64, l_max=7, reference_type=2, shell_depth=4.55e9, aspect_ratio=0.35, poly_n=2.0,
+                   poly_nrho=5.0, poly_mass=1.9e30, poly_rho_i=1.1, pressure_specific_heat=1.0509e8,
+                   angular_velocity=1.76e-4, nu_top=3.64364e12, kappa_top=3.64364e12, dt=30.0)
+    o = O.Oracle(cfg)
+    assert abs(o.density[-1] - 1.1) < 1e-13
+    assert abs(o.density[-1] / o.density[0] - math.exp(5.0)) < 1e-11 * math.exp(5.0)
+    P = cfg.pressure_specific_heat * o.density * o.temperature / (cfg.poly_n + 1.0)
+    g = 6.67e-8 * cfg.poly_mass / o.radius ** 2
+    np.testing.assert_allclose(_spectral_d(o, P, 1), -o.density * g, rtol=1e-8)
+    np.testing.assert_allclose(_spectral_d(o, np.log(o.density), 1), o.dlnrho, rtol=1e-9)
+    np.testing.assert_allclose(_spectral_d(o, np.log(o.temperature), 1), o.dlnT, rtol=1e-9)
+    np.testing.assert_allclose(_spectral_d(o, np.log(o.density), 2), o.d2lnrho, rtol=1e-7)
+
+
+def _t_nonlinear(o, wpt, z, c=None, a=None):
+    """T's nonlinear term of one physical-space stage from a state (spectral, per m)."""
+    o.init_state(wpt, z, c_coeffs=c, a_coeffs=a)
+    s2a = o.transpose_1a2a(o.post_solve())
+    p3b = o.physical_space(o.transpose_2a3a(o.h.s2p(o.rlm_spacea(s2a))))
+    return p3b[O.TVAR]
+
+
+def test_anelastic_viscous_heating_of_rotations():
+    """Compute_Viscous_Heating (Sphere_Physical_Space.F90:337-443) on the polytrope: a
+    solid-body rotation about the polar axis (Z_10 proportional to rho r^2, so that
+    v_phi = Omega r sin(theta)) has no strain and heats nothing, while a differential
+    rotation (Z_10 proportional to rho r^3) heats; T has no angular structure and
+    v_r = 0, so advection adds nothing to T's term."""
+    oc = O.anelastic_mhd_config(n_r=64, l_max=15, magnetism=False)
+    o = O.Oracle(oc)
+    assert o.viscous_heating_coeff is not None and np.all(o.viscous_heating_coeff > 0)
+    wpt, _ = O.seeded_state(oc, amp=0.0)
+    r = o.radius
+    out = []
+    for p in (2, 3):
+        z = np.zeros((o.n_lm, 2, oc.n_r))
+        z[1, 0] = o.cg.to_spectral((1e-3 * o.density * r ** p)[None, None, :])[0, 0]   # lm(1, 0) = 1
+        out.append(np.abs(_t_nonlinear(o, wpt, z)).max())
+    assert out[1] > 0 and out[0] < 1e-9 * out[1], out
+
+
+def test_anelastic_heating_coefficients():
+    """Both heating terms are on for the polytropes (Controls.F90:64-65) with positive
+    coefficients, and off for the Boussinesq reference (Constant_Reference)."""
+    o = O.Oracle(O.anelastic_mhd_config(n_r=24, l_max=15))
+    assert np.all(o.viscous_heating_coeff > 0) and np.all(o.ohmic_heating_coeff > 0)
+    b = O.Oracle(O.Config(n_r=24, l_max=15, magnetism=True))
+    assert b.viscous_heating_coeff is None and b.ohmic_heating_coeff is None

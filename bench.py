@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
                     [--impl ours|reference] [--lmax 511] [--nr 192] [--err-steps 100]
-                    [--equation-set dynamo|hydro]
+                    [--equation-set dynamo|hydro|anelastic]
 
 One JSON line on rank 0.  The workload is the large Boussinesq dynamo (the
 magnetic equation set: W, P, T, Z and the potentials C, A of B; Ek = 1e-5,
@@ -21,6 +21,10 @@ factor that scales each stage's sample to the whole stage, and the full-step
 estimate they make, plus whole steps measured at the l_max = 63, N_r = 48 size.
 With N > 1 (torchrun) every rank runs an independent simulation, as the
 reference's multi-run mode does (-nruns); the value sums the ranks' steps.
+``--equation-set anelastic`` runs the anelastic MHD workload instead (the
+nondimensional polytrope with 5 density scale heights and index 2, radius ratio
+0.35, l_max = 255, N_r = 128, W, Z, P, S, C, A with viscous and ohmic heating,
+seeded perturbations of amplitude 1e-4, mixed vs FP64 after 200 steps).
 """
 from __future__ import annotations
 
@@ -53,12 +57,37 @@ def headline_config(lmax, nr, precision, mag=True):
                 t_bottom=1.0, dt=1.0e-6, precision=precision)
 
 
-def workload_name(lmax, nr, mag):
+def anelastic_config(lmax, nr, precision):
+    """The anelastic MHD workload: the nondimensional polytrope (reference_type 3) with 5
+    density scale heights and polytropic index 2 in a shell of radius ratio 0.35; the
+    magnetic equation set with insulating boundaries; stress-free, fixed-entropy boundaries;
+    viscous and ohmic heating on; Ek = 1e-3, Pr = 1, Pm = 2, Ra* = 0.5, dt = 1e-4."""
+    return dict(n_r=nr, l_max=lmax, aspect_ratio=0.35, shell_depth=1.0, reference_type=3, poly_n=2.0,
+                poly_nrho=5.0, modified_rayleigh=0.5, ekman=1.0e-3, prandtl=1.0, magnetic_prandtl=2.0,
+                rotation=True, magnetism=True, no_slip_top=False, no_slip_bottom=False, fix_tvar_top=True,
+                fix_tvar_bottom=True, t_top=0.0, t_bottom=1.0, dt=1.0e-4, precision=precision)
+
+
+def workload_config(equation_set, lmax, nr, precision):
+    if equation_set == "anelastic":
+        return anelastic_config(lmax, nr, precision)
+    return headline_config(lmax, nr, precision, equation_set == "dynamo")
+
+
+SET_LABEL = {"dynamo": "dynamo (W, P, T, Z, C, A; insulating boundaries)",
+             "hydro": "hydrodynamic (W, P, T, Z)",
+             "anelastic": "anelastic dynamo (polytrope, 5 density scale heights; W, P, S, Z, C, A; "
+                          "viscous and ohmic heating)"}
+
+
+def workload_name(lmax, nr, mag, equation_set=None):
+    if equation_set == "anelastic":
+        return f"anelastic_dynamo_polytrope_nrho5_lmax{lmax}_nr{nr}"
     return f"boussinesq_{'dynamo' if mag else 'rotating_convection'}_lmax{lmax}_nr{nr}"
 
 
-def initial_magnetic_state(ctx, lmax, nr, rng):
-    """Seeded B: poloidal and toroidal potentials C, A on l in [1, 20], amplitude 1e-3 (l+1)^-2,
+def initial_magnetic_state(ctx, lmax, nr, rng, amp=1e-3):
+    """Seeded B: poloidal and toroidal potentials C, A on l in [1, 20], amplitude amp (l+1)^-2,
     as Chebyshev coefficients on the first 16 modes (m = 0 imaginary parts zero)."""
     n_lm = (lmax + 1) * (lmax + 2) // 2
     out = []
@@ -67,14 +96,14 @@ def initial_magnetic_state(ctx, lmax, nr, rng):
         a = np.zeros((n_lm, 2, nr))
         for l in range(1, min(20, lmax) + 1):
             s = l * (l + 1) // 2
-            block = rng.standard_normal((l + 1, 2, ncoef)) * 1e-3 * (l + 1.0) ** -2 / (1.0 + np.arange(ncoef)) ** 2
+            block = rng.standard_normal((l + 1, 2, ncoef)) * amp * (l + 1.0) ** -2 / (1.0 + np.arange(ncoef)) ** 2
             block[0, 1] = 0.0
             a[s:s + l + 1, :, :ncoef] = block
         out.append(a)
     return out
 
 
-def initial_state(ctx, lmax, nr, rng):
+def initial_state(ctx, lmax, nr, rng, amp=1e-3):
     """Conductive T plus a seeded perturbation on l in [1, 20] with (l+1)^-2 decay (coefficient space)."""
     n_lm = (lmax + 1) * (lmax + 2) // 2
     wpt = np.zeros((n_lm, 2, 3 * nr))
@@ -86,8 +115,8 @@ def initial_state(ctx, lmax, nr, rng):
     ncoef = min(16, nr // 2)
     for l in range(1, min(20, lmax) + 1):
         s = l * (l + 1) // 2
-        amp = 1e-3 * (l + 1.0) ** -2
-        block = rng.standard_normal((l + 1, 2, ncoef)) * amp / (1.0 + np.arange(ncoef)) ** 2
+        a = amp * (l + 1.0) ** -2
+        block = rng.standard_normal((l + 1, 2, ncoef)) * a / (1.0 + np.arange(ncoef)) ** 2
         block[0, 1] = 0.0
         wpt[s:s + l + 1, :, 2 * nr:2 * nr + ncoef] = block
     return wpt, z
@@ -215,14 +244,14 @@ class CpuSample:
     seconds of each stage and the factor that scales it to the whole stage are
     reported separately; the full-step estimate is their dot product."""
 
-    def __init__(self, lmax, nr, stride=32, ntheta_rows=4, mag=True):
+    def __init__(self, lmax, nr, stride=32, ntheta_rows=4, mag=True, equation_set=None):
         import oracle as O
         self.O = O
         self.mag = mag
         self.cores = os.cpu_count()
         O.set_fft_workers(self.cores)
-        cfg = O.Config(**{k: v for k, v in headline_config(lmax, nr, 0, mag).items()
-                          if k in O.Config.__dataclass_fields__})
+        cfgd = workload_config(equation_set, lmax, nr, 0) if equation_set else headline_config(lmax, nr, 0, mag)
+        cfg = O.Config(**{k: v for k, v in cfgd.items() if k in O.Config.__dataclass_fields__})
         t0 = time.perf_counter()
         self.o = O.Oracle(cfg)
         self.init_s = time.perf_counter() - t0
@@ -352,8 +381,8 @@ def run_reference(args, rank):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-    mag = args.equation_set == "dynamo"
-    cs = CpuSample(args.lmax, args.nr, mag=mag)
+    mag = args.equation_set in ("dynamo", "anelastic")
+    cs = CpuSample(args.lmax, args.nr, mag=mag, equation_set=args.equation_set)
     for _ in range(args.warmup):
         cs.step_seconds()
     timed = [cs.step_seconds() for _ in range(args.steps)]
@@ -366,9 +395,9 @@ def run_reference(args, rank):
         # the time actually spent per timed (sampled) step; value is the full-step estimate
         "ms_per_step": cpu["timed_seconds_per_sampled_step"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": workload_name(args.lmax, args.nr, mag), "l_max": args.lmax,
+        "config": {"workload": workload_name(args.lmax, args.nr, mag, args.equation_set), "l_max": args.lmax,
                    "n_r": args.nr, "n_theta": cs.cfg.n_theta, "n_phi": cs.cfg.n_phi,
-                   "equation_set": "dynamo (W, P, T, Z, C, A)" if mag else "hydrodynamic (W, P, T, Z)",
+                   "equation_set": SET_LABEL[args.equation_set],
                    "l2": "working set larger than L2"},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -398,14 +427,15 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
     import rayleigh_b200 as rb
     local = int(os.environ.get("LOCAL_RANK", "0"))
     prec = rb.PREC_MIXED if prec_name == "mixed" else rb.PREC_FP64
-    mag = args.equation_set == "dynamo"
-    cfgd = headline_config(args.lmax, args.nr, prec, mag)
+    mag = args.equation_set in ("dynamo", "anelastic")
+    cfgd = workload_config(args.equation_set, args.lmax, args.nr, prec)
     ctx = rb.Rayleigh(rb.Config(**cfgd, use_graph=True, device=local))
     rng = np.random.Generator(np.random.PCG64(SEED + rank))
-    wpt, z = initial_state(ctx, args.lmax, args.nr, rng)
+    amp = 1e-4 if args.equation_set == "anelastic" else 1e-3
+    wpt, z = initial_state(ctx, args.lmax, args.nr, rng, amp)
     ctx.put_state(wpt, z, None, iteration=1)
     if mag:
-        cpol, ator = initial_magnetic_state(ctx, args.lmax, args.nr, rng)
+        cpol, ator = initial_magnetic_state(ctx, args.lmax, args.nr, rng, amp)
         ctx.put_magnetic_state(cpol, ator)
     # warm-up (includes the Euler first step and the capture of the step graph)
     ctx.step(max(3, args.warmup))
@@ -510,13 +540,12 @@ def run_precision(args, prec_name, rank, world, torch, dist, fp64_peak, peaks, p
         "value": value, "ms_per_step": max_ms / args.steps, "precision": prec_name,
         "timing": f"value: {args.steps} steps replayed from the captured step graph, CUDA events on the context "
                   f"stream; kernels: {nk_steps} eager steps with an event around each kernel",
-        "config": {"workload": workload_name(args.lmax, args.nr, mag), "l_max": args.lmax,
+        "config": {"workload": workload_name(args.lmax, args.nr, mag, args.equation_set), "l_max": args.lmax,
                    "n_r": args.nr, "n_theta": n_theta, "n_phi": n_phi, "ekman": cfgd["ekman"],
-                   "rayleigh": cfgd["rayleigh"], "prandtl": cfgd["prandtl"],
+                   "rayleigh": cfgd.get("rayleigh", cfgd.get("modified_rayleigh")), "prandtl": cfgd["prandtl"],
                    "magnetic_prandtl": cfgd["magnetic_prandtl"] if mag else None, "dt": cfgd["dt"],
-                   "l2": "working set (~50 GB) larger than L2; no flush needed",
-                   "equation_set": "dynamo (W, P, T, Z, C, A; insulating boundaries)" if mag
-                                   else "hydrodynamic (W, P, T, Z)",
+                   "l2": "working set (GBs of state and buffers) larger than the 126 MB L2; no flush needed",
+                   "equation_set": SET_LABEL[args.equation_set],
                    "parallelism": "replicas (multi-run ensemble)" if world > 1 else "single GPU"},
         "roofline": {"kernel": dom, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                      "frac": achieved / peak if peak else None, "traffic": traffic,
@@ -589,7 +618,8 @@ def run_ours(args, rank, world, torch, dist):
     if args.c1:
         line["c1_measured"] = c1_comparison(args, torch)
     if not args.no_cpu:
-        cs = CpuSample(args.lmax, args.nr, mag=args.equation_set == "dynamo")
+        cs = CpuSample(args.lmax, args.nr, mag=args.equation_set in ("dynamo", "anelastic"),
+                       equation_set=args.equation_set)
         cs.step_seconds()
         line["cpu_baseline"] = cs.report([cs.step_seconds()])
     print(json.dumps(line), flush=True)
@@ -622,16 +652,24 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time the FP64 and the mixed form, report the mixed one with its error vs FP64")
-    ap.add_argument("--err-steps", type=int, default=100,
-                    help="steps after which the mixed and FP64 states are compared")
-    ap.add_argument("--lmax", type=int, default=511)
-    ap.add_argument("--nr", type=int, default=192)
-    ap.add_argument("--equation-set", default="dynamo", choices=["dynamo", "hydro"],
-                    help="dynamo: the magnetic equation set (the large Boussinesq dynamo); hydro: without B")
+    ap.add_argument("--err-steps", type=int, default=None,
+                    help="steps after which the mixed and FP64 states are compared (100; 200 anelastic)")
+    ap.add_argument("--lmax", type=int, default=None, help="511 (255 anelastic)")
+    ap.add_argument("--nr", type=int, default=None, help="192 (128 anelastic)")
+    ap.add_argument("--equation-set", default="dynamo", choices=["dynamo", "hydro", "anelastic"],
+                    help="dynamo: the magnetic equation set (the large Boussinesq dynamo); hydro: without B; "
+                         "anelastic: the anelastic MHD workload (polytrope, l_max 255, N_r 128)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-c1", dest="c1", action="store_false",
                     help="skip the whole-step GPU/CPU comparison at the l_max = 63, N_r = 48 size")
     args = ap.parse_args()
+    anel = args.equation_set == "anelastic"
+    if args.lmax is None:
+        args.lmax = 255 if anel else 511
+    if args.nr is None:
+        args.nr = 128 if anel else 192
+    if args.err_steps is None:
+        args.err_steps = 200 if anel else 100
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -165,6 +165,19 @@ int ra_factor(ra_ctx* ctx, double dt);
  * in this library's l-major order.  NULL restores the built-in values (zero,
  * except the fixed T or dT/dr of l = 0). */
 int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values);
+/* The driver's own reference state for the explicit terms, for reference states the
+ * library does not restate (reference_type 4 and 5, custom files, Augment_Reference;
+ * PDE_Coefficients.F90:216-257): per radius (n_r, the collocation order, outer radius
+ * first) ref%density and ref%dlnrho (the density weights of rlm_spacea's velocity,
+ * Sphere_Hybrid_Space.F90:44-62, 240-350, and of the momentum terms), the
+ * viscous_heating_coeff and ohmic_heating_coeff of the entropy equation
+ * (Sphere_Physical_Space.F90:337-466; NULL: the term is off; ohmic needs magnetism) and
+ * ref%Coriolis_Coeff, ref%Lorentz_Coeff.  The implicit terms are the driver's too: load
+ * its matrices with ra_load_matrices and factor them with ra_factor; ra_set_dt and a dt
+ * change in ra_step_adaptive then return RA_ERR_STATE.  Non-finite entries return
+ * RA_ERR_NONFINITE, a density <= 0 RA_ERR_ARG. */
+int ra_set_reference(ra_ctx* ctx, const double* density, const double* dlnrho, const double* viscous_heating_coeff,
+                     const double* ohmic_heating_coeff, double coriolis_coeff, double lorentz_coeff);
 
 /* State exchange in the equation-set RHS layout (Linear_Solve.F90:355-386):
  *   wpt[3 n_r][2][n_lm]  W, P, T Chebyshev coefficients of the linked l-block
@@ -255,9 +268,9 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_DV_R_DP       28
 #define RA_Q_DV_THETA_DP   29
 #define RA_Q_DV_PHI_DP     30
-#define RA_Q_VORT_R       301   /* l(l+1) Z / r^2 (Boussinesq radial vorticity) */
+#define RA_Q_VORT_R       301   /* l(l+1) Z / (rho r^2), the radial vorticity */
 #define RA_Q_ENTROPY      501
-#define RA_Q_PRESSURE     502   /* formed with the P grid in T's place */
+#define RA_Q_PRESSURE     502   /* formed with the P grid in T's place; the pressure codes need reference_type 1 */
 #define RA_Q_ENTROPY_DR   507
 #define RA_Q_PRESSURE_DR  508
 #define RA_Q_ENTROPY_DTHETA 513

@@ -1198,6 +1198,48 @@ class Oracle:
         wpt[:, :, 2 * nr:] = self.cg.to_spectral(grid)
         return wpt, np.zeros((self.n_lm, 2, nr))
 
+    def abenchmark_init_hydro(self, temp_amp=1.0):
+        """ABenchmark_Init_Hydro (Initial_Conditions.F90:789-879), init_type 6 of the Jones et al.
+        (2011) anelastic benchmark: W = P = Z = 0; on the collocation grid the l = 0 entropy
+        Delta_S (zeta_o^-n - zeta^-n) / (zeta_o^-n - zeta_i^-n) sqrt(4 pi) with Delta_S = t_bottom,
+        zeta = c0 + c1 d / r of the n = 2, N_rho = 5 polytrope, and the real parts of
+        S(19, 19) = temp_amp (1 - cos(2 pi (r - r_i) / d)) and S(1, 1) = 0.1 of that; then
+        To_Spectral.  Returns (wpt, z) in the init_state layout."""
+        nr = self.cfg.n_r
+        r = self.radius
+        d = r[0] - r[-1]
+        beta = r[-1] / r[0]
+        n_rho, bm_n = 5.0, 2.0
+        zeta0 = (beta + 1.0) / (beta * math.exp(n_rho / bm_n) + 1.0)
+        c0 = (2.0 * zeta0 - beta - 1.0) / (1.0 - beta)
+        c1 = (1.0 + beta) * (1.0 - zeta0) / (1.0 - beta) ** 2
+        zeta = c0 + c1 * d / r
+        ee = -bm_n
+        denom = zeta[0] ** ee - zeta[-1] ** ee
+        rfunc2 = self.cfg.t_bottom * (zeta[0] ** ee - zeta ** ee) / denom
+        rfunc1 = (1.0 - np.cos(2.0 * math.pi / d * (r - r[-1]))) * temp_amp
+        grid = np.zeros((self.n_lm, 2, nr))
+        grid[0, 0, :] = rfunc2 * math.sqrt(4.0 * math.pi)
+        if self.cfg.l_max >= 19:
+            grid[19 * 20 // 2 + 19, 0, :] = rfunc1
+        grid[1 * 2 // 2 + 1, 0, :] = rfunc1 * 0.1
+        wpt = np.zeros((self.n_lm, 2, 3 * nr))
+        wpt[:, :, 2 * nr:] = self.cg.to_spectral(grid)
+        return wpt, np.zeros((self.n_lm, 2, nr))
+
+    def benchmark_mean_flow_energies(self, avr, avt, avp):
+        """Benchmark_Checkup's zonal and meridional kinetic energies (Benchmarking.F90:658-687):
+        0.5 rho <v_phi>^2 and 0.5 rho (<v_r>^2 + <v_theta>^2) of the phi means <.>, given as
+        [theta, r] arrays, averaged over theta (Gauss-Legendre weights / 2) and radius (the
+        radial integration weights) as the kinetic energy is."""
+        tw = (self.h.wq / 2.0).astype(np.float64)
+        w = self.radial_integration_weights()
+        rho = self.density[None, :]
+        zonal = 0.5 * rho * avp * avp
+        merid = 0.5 * rho * (avr * avr + avt * avt)
+        return (float(np.dot(w, np.einsum("t,tr->r", tw, zonal))),
+                float(np.dot(w, np.einsum("t,tr->r", tw, merid))))
+
     def benchmark_insulating_init(self):
         """Benchmark_Insulating_Init (Initial_Conditions.F90:1011-1073): on the collocation grid
         C(l=1, m=0) = (8 r_o - 6 r - 2 r_i^4 / r^3) (5/8) sqrt(pi/3) r^2 and
@@ -1396,6 +1438,20 @@ def c2001_case1_config(n_r=64, n_theta=96):
     """The settings benchmark_mode = 2 imposes (Benchmarking.F90:150-199: Christensen et al.
     2001, MHD case 1: case 0's settings with magnetism, Pm = 5 and insulating boundaries)."""
     return replace(c2001_case0_config(n_r, n_theta), magnetism=True, magnetic_prandtl=5.0)
+
+
+def j2011_hydro_config(n_r=128, n_theta=192):
+    """The settings benchmark_mode = 3 imposes (Benchmarking.F90:202-247: Jones et al. 2011,
+    anelastic hydrodynamic case): the cgs polytrope (reference_type 2) with n = 2, N_rho = 5,
+    M = 1.9e30 g, rho_i = 1.1 g/cm^3, c_P = 1.0509e8, Omega = 1.76e-4 rad/s between
+    r_i = 2.45e9 and r_o = 7e9 cm; nu = kappa = 3.64364e12; stress-free; entropy 0 at the
+    top and 851225.7 at the bottom; viscous heating on (Controls.F90:64); dt <= 30 s."""
+    return Config(n_r=n_r, l_max=(2 * n_theta) // 3 - 1, n_theta=n_theta, aspect_ratio=0.35, shell_depth=4.55e9,
+                  reference_type=2, poly_n=2.0, poly_nrho=5.0, poly_mass=1.9e30, poly_rho_i=1.1,
+                  pressure_specific_heat=1.0509e8, angular_velocity=1.76e-4, nu_top=3.64364e12,
+                  kappa_top=3.64364e12, rotation=True, no_slip_top=False, no_slip_bottom=False,
+                  fix_tvar_top=True, fix_tvar_bottom=True, t_top=0.0, t_bottom=851225.7, dt=30.0,
+                  alpha_implicit=0.50001)
 
 
 def anelastic_mhd_config(n_r=128, l_max=255, **kw):

@@ -236,6 +236,7 @@ def load_library(path: str | None = None):
         "ra_load_matrices": ([_VP, ctypes.c_int, _VP, _VP], ctypes.c_int),
         "ra_factor": ([_VP, ctypes.c_double], ctypes.c_int),
         "ra_set_bc_mask": ([_VP, _VP], ctypes.c_int),
+        "ra_set_reference": ([_VP, _VP, _VP, _VP, _VP, ctypes.c_double, ctypes.c_double], ctypes.c_int),
         "ra_lu_create": ([ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_lu_destroy": ([_VP], ctypes.c_int),
         "ra_lu_last_error": ([_VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
@@ -384,6 +385,16 @@ class Rayleigh:
         """bc_values[eq W/P/T/Z][lm][re/im][top/bottom] (Fortran bc_values(2, 2, n_lm, 4)), or None."""
         self._bcv = None if bc_values is None else _f64(bc_values)
         self._check(self.lib.ra_set_bc_mask(self.h, _ptr(self._bcv)))
+
+    def set_reference(self, density, dlnrho, viscous_heating_coeff=None, ohmic_heating_coeff=None,
+                      coriolis_coeff=0.0, lorentz_coeff=0.0):
+        """The driver's reference state for the explicit terms (ra_set_reference): per-radius
+        density, dlnrho and heating coefficients (None: off), the Coriolis and Lorentz coefficients."""
+        arrs = [None if a is None else _f64(a) for a in (density, dlnrho, viscous_heating_coeff,
+                                                          ohmic_heating_coeff)]
+        self._refs = arrs
+        self._check(self.lib.ra_set_reference(self.h, *[_ptr(a) for a in arrs], float(coriolis_coeff),
+                                               float(lorentz_coeff)))
 
     def step(self, nsteps=1):
         cfl = ctypes.c_double()

@@ -534,6 +534,32 @@ static void linear_setup(Ctx& c) {
     factor_matrices(c);
 }
 
+// The packed radial profiles the kernels read (R_* rows of n_r): the grid, the reference
+// density and its log-derivative with rlm_spacea's over_rhor, over_rhorsq and drho_term
+// (Sphere_Hybrid_Space.F90:44-62), and the heating coefficients.
+static std::vector<double> radial_table(const Ctx& c) {
+    const int nr = c.d.nr;
+    std::vector<double> rp((size_t)R_COUNT * nr);
+    for (int i = 0; i < nr; ++i) {
+        const double r = c.rad.radius[i];
+        const double oor = 1.0 / r;
+        const double oor2 = 1.0 / (r * r);
+        rp[R_RADIUS * nr + i] = r;
+        rp[R_OVER_R * nr + i] = oor;
+        rp[R_DELTA_R * nr + i] = c.rad.delta_r[i];
+        rp[R_DENSITY * nr + i] = c.rad.density[i];
+        rp[R_DLNRHO * nr + i] = c.rad.dlnrho[i];
+        rp[R_OVER_RHOR * nr + i] = oor / c.rad.density[i];
+        rp[R_OVER_RHORSQ * nr + i] = oor2 / c.rad.density[i];
+        rp[R_DRHO_TERM * nr + i] = c.rad.dlnrho[i] + oor;
+        rp[R_TWO_OVER_R * nr + i] = 2.0 / r;
+        rp[R_OVER_RSQ * nr + i] = oor2;
+        rp[R_VISC_HEAT * nr + i] = c.rad.visc_heat[i];
+        rp[R_OHM_HEAT * nr + i] = c.rad.ohm_heat[i];
+    }
+    return rp;
+}
+
 template <class T>
 static void dalloc(T*& p, size_t count) {
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
@@ -597,24 +623,7 @@ static void setup(Ctx& c) {
     for (int i = 0; i < d.nr; ++i) kew[d.nth + i] = c.rad.int_w[i];
     // radial profiles
     const int nr = d.nr;
-    std::vector<double> rp((size_t)R_COUNT * nr);
-    for (int i = 0; i < nr; ++i) {
-        const double r = c.rad.radius[i];
-        const double oor = 1.0 / r;
-        const double oor2 = 1.0 / (r * r);
-        rp[R_RADIUS * nr + i] = r;
-        rp[R_OVER_R * nr + i] = oor;
-        rp[R_DELTA_R * nr + i] = c.rad.delta_r[i];
-        rp[R_DENSITY * nr + i] = c.rad.density[i];
-        rp[R_DLNRHO * nr + i] = c.rad.dlnrho[i];
-        rp[R_OVER_RHOR * nr + i] = oor / c.rad.density[i];
-        rp[R_OVER_RHORSQ * nr + i] = oor2 / c.rad.density[i];
-        rp[R_DRHO_TERM * nr + i] = c.rad.dlnrho[i] + oor;
-        rp[R_TWO_OVER_R * nr + i] = 2.0 / r;
-        rp[R_OVER_RSQ * nr + i] = oor2;
-        rp[R_VISC_HEAT * nr + i] = c.rad.visc_heat[i];
-        rp[R_OHM_HEAT * nr + i] = c.rad.ohm_heat[i];
-    }
+    const std::vector<double> rp = radial_table(c);
     // device buffers
     const long nlm = d.nlm;
     dalloc(c.d_Ptab, (size_t)nlm * d.nth2);
@@ -1116,6 +1125,9 @@ static int guarded(ra_ctx* ctx, F f) {
     } catch (const NonFiniteError& e) {
         if (ctx) ctx->c.err = e.what;
         return RA_ERR_NONFINITE;
+    } catch (const StateError& e) {
+        if (ctx) ctx->c.err = e.what;
+        return RA_ERR_STATE;
     } catch (const CudaError& e) {
         if (ctx) ctx->c.err = e.what;
         return e.code == cudaErrorMemoryAllocation ? RA_ERR_NOMEM : RA_ERR_CUDA;
@@ -1211,6 +1223,9 @@ int ra_set_dt(ra_ctx* ctx, double dt) {
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
     return guarded(ctx, [&] {
         if (!(dt > 0)) throw ArgError("dt must be positive");
+        if (ctx->c.custom_reference)
+            throw StateError("the reference state was set by ra_set_reference: load the matrices of the new dt "
+                             "with ra_load_matrices and factor them with ra_factor");
         ctx->c.dt = dt;
         linear_setup(ctx->c);
         if (ctx->c.mixed_solve) mixed_resplit_solve(ctx->c);
@@ -1452,6 +1467,53 @@ int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values) {
     });
 }
 
+int ra_set_reference(ra_ctx* ctx, const double* density, const double* dlnrho, const double* viscous_heating_coeff,
+                     const double* ohmic_heating_coeff, double coriolis_coeff, double lorentz_coeff) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!density || !dlnrho) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        const int n = c.d.nr;
+        auto check = [&](const double* v, const char* what, bool positive) {
+            if (!v) return;
+            for (int i = 0; i < n; ++i) {
+                if (!std::isfinite(v[i])) throw NonFiniteError(std::string(what) + " is not finite");
+                if (positive && !(v[i] > 0)) throw ArgError(std::string(what) + " must be positive");
+            }
+        };
+        check(density, "density", true);
+        check(dlnrho, "dlnrho", false);
+        check(viscous_heating_coeff, "viscous_heating_coeff", false);
+        check(ohmic_heating_coeff, "ohmic_heating_coeff", false);
+        if (!std::isfinite(coriolis_coeff) || !std::isfinite(lorentz_coeff))
+            throw NonFiniteError("coriolis_coeff / lorentz_coeff is not finite");
+        if (ohmic_heating_coeff && !c.mag) throw ArgError("ohmic heating needs magnetism");
+        Radial& R = c.rad;
+        R.density.assign(density, density + n);
+        R.dlnrho.assign(dlnrho, dlnrho + n);
+        R.visc_heat.assign(n, 0.0);
+        R.ohm_heat.assign(n, 0.0);
+        bool heat = false;
+        for (int i = 0; i < n; ++i) {
+            if (viscous_heating_coeff) R.visc_heat[i] = viscous_heating_coeff[i];
+            if (ohmic_heating_coeff) R.ohm_heat[i] = ohmic_heating_coeff[i];
+            heat = heat || R.visc_heat[i] != 0.0 || R.ohm_heat[i] != 0.0;
+        }
+        if (heat && !physics_form1_supported(c.d.nth))
+            throw ArgError("viscous / ohmic heating needs n_theta in 24..768 (2^a or 3*2^a)");
+        R.heating = heat;
+        if (heat || c.mag) c.physics_form = 1;   // the form with the heating and magnetic terms
+        R.coriolis = coriolis_coeff;
+        if (c.mag) R.lorentz = lorentz_coeff;
+        c.custom_reference = true;
+        const std::vector<double> rp = radial_table(c);
+        RA_CUDA(cudaMemcpyAsync(c.d_radial, rp.data(), rp.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        drop_graph(c);   // the captured step holds the old Coriolis and Lorentz coefficients
+    });
+}
+
 int ra_step_timed(ra_ctx* ctx, int nsteps, double* total_ms) {
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
     if (nsteps < 1 || !total_ms) return RA_ERR_ARG;
@@ -1622,6 +1684,8 @@ int ra_step_adaptive(ra_ctx* ctx, int nsteps, const ra_dt_controls* ctl, double*
             if (ra_next_dt(ctl, c.dt, cfl, &nd) != RA_OK)
                 throw NonFiniteError("the time step became smaller than min_time_step (" + std::to_string(nd) + ")");
             if (nd != c.dt) {   // Reset_Linear_Equations before the next step
+                if (c.custom_reference)
+                    throw StateError("a dt change needs the driver's matrices after ra_set_reference");
                 c.dt = nd;
                 linear_setup(c);
                 if (c.mixed_solve) mixed_resplit_solve(c);
@@ -1678,6 +1742,8 @@ static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities
         if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " is not provided");
         if (src->field >= c.nfa)
             throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
+        if (src->pressure && (c.cfg.reference_type != 1 || c.custom_reference))   // the anelastic state holds P / rho
+            throw ArgError("diagnostics: the pressure codes are provided for the Boussinesq reference only");
         spec[q] = SliceSpec{};
         spec[q].field = src->field;
         spec[q].dphi = src->dphi;

@@ -143,6 +143,7 @@ struct Ctx {
     // polytrope (reference_type 2) its matrices are too badly conditioned for an explicit
     // inverse and the mixed form solves by the FP64 block substitution
     bool mixed_solve = false;
+    bool custom_reference = false;                    // radial profiles given by ra_set_reference
     int nfa = NP2A, nfb = NP2B, ng = NG;              // fields of s2a11/p2a, of p2b/s2b, grids (more with mag)
 
     Radial rad;
@@ -301,7 +302,7 @@ struct CudaError {
     }
 };
 
-struct SingularError {   // a negligible pivot in a per-l matrix: RA_ERR_SINGULAR
+struct SingularError {   // a zero pivot in a per-l matrix: RA_ERR_SINGULAR
     std::string what;
     explicit SingularError(std::string w) : what(std::move(w)) {}
 };
@@ -314,6 +315,11 @@ struct NonFiniteError {   // RA_ERR_NONFINITE
 struct ArgError {
     std::string what;
     explicit ArgError(std::string w) : what(std::move(w)) {}
+};
+
+struct StateError {   // a call out of order: RA_ERR_STATE
+    std::string what;
+    explicit StateError(std::string w) : what(std::move(w)) {}
 };
 
 }  // namespace ra

@@ -156,3 +156,37 @@ def test_anelastic_mhd_workload():
           {k: f"{v:.2e}" for k, v in errs.items()})
     assert all(np.isfinite(v) for v in errs.values())
     assert max(errs.values()) < 2e-9, errs
+
+
+def test_driver_reference_state():
+    """ra_set_reference with the polytrope's profiles (density, dlnrho, the heating
+    coefficients, Coriolis and Lorentz coefficients) on a context created with the
+    Boussinesq reference, with the polytrope's matrices loaded through ra_load_matrices and
+    ra_factor, steps as the context that restates the polytrope itself: the route by which
+    reference states the library does not restate (custom files, reference_type 4 and 5)
+    reach the device.  A dt change then needs the driver's matrices (RA_ERR_STATE)."""
+    import rayleigh_b200 as rb
+    oc = M._ocfg(ANEL_MHD)
+    o = O.Oracle(oc)
+    wpt, z, c, a = M._seed(oc, amp_u=1e-3, amp_b=1e-2)
+    ref = M._ctx(dict(ANEL_MHD, use_graph=True))
+    g = M._ctx(dict(ANEL_MHD, reference_type=1, use_graph=True))
+    rc = rb.Config(**ANEL_MHD)
+    L = oc.l_max + 1
+    for sys in range(4):
+        lhs, cf = rb.build_matrices(rc, sys, 0, L, coefs=True)
+        g.load_matrices(sys, lhs, cf)
+    g.factor(ANEL_MHD["dt"])
+    g.set_reference(o.density, o.dlnrho, o.viscous_heating_coeff, o.ohmic_heating_coeff, o.coriolis, o.lorentz)
+    for ctx in (g, ref):
+        ctx.put_state(wpt, z, None, iteration=1)
+        ctx.put_magnetic_state(c, a)
+        ctx.step(5)
+    for x, y in zip(g.get_state()[:2] + g.get_magnetic_state()[:2], ref.get_state()[:2] + ref.get_magnetic_state()[:2]):
+        assert rel_err(x, y) < 1e-13
+    with pytest.raises(rb.RayleighError) as ei:
+        g.set_dt(2e-4)
+    assert ei.value.code == rb.RA_ERR_STATE
+    with pytest.raises(rb.RayleighError) as ei:
+        g.set_reference(-o.density, o.dlnrho)
+    assert ei.value.code == rb.RA_ERR_ARG

@@ -740,6 +740,10 @@ static void release(Ctx& c) {
     mixed_release(c);
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     if (c.graph) cudaGraphDestroy(c.graph);
+    if (c.adapt_exec) cudaGraphExecDestroy(c.adapt_exec);
+    if (c.adapt_graph) cudaGraphDestroy(c.adapt_graph);
+    if (c.d_adapt) cudaFree(c.d_adapt);
+    if (c.d_adapt_dt) cudaFree(c.d_adapt_dt);
     lu_workspace_free(c.lu_work);
     double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp,
                       c.d_Awpt, c.d_Az,
@@ -843,6 +847,85 @@ __global__ void nonfinite_scan_kernel(const double* __restrict__ x, long n, int*
 static void scan_nonfinite(Ctx& c, const double* d_x, long n) {
     nonfinite_scan_kernel<<<1184, 256, 0, c.stream>>>(d_x, n, c.d_status);
     RA_CUDA(cudaGetLastError());
+}
+
+// Adjust_TimeStep (Sphere_Hybrid_Space.F90:604-649): cfl = the largest squared inverse crossing
+// time of the step (the CFL cargo); the new dt applies from the next step.  The same arithmetic
+// on the host (ra_next_dt) and in the adaptive step graph (dt_control_kernel).
+__host__ __device__ inline double next_dt_value(const ra_dt_controls& ctl, double dt, double cfl) {
+    double nd = dt;
+    if (cfl > 0.0) {
+        const double maxt = 1.0 / sqrt(cfl);
+        if (dt < maxt * ctl.cflmin) {
+            nd = fmin(ctl.cflmax * maxt, ctl.max_time_step);
+        } else if (dt > maxt * ctl.cflmax) {
+            nd = ctl.cflmax * maxt;
+            if (nd > dt * (1.0 - ctl.min_dt_change)) nd = dt * (1.0 - ctl.min_dt_change);
+        }
+    }
+    if (nd > ctl.max_time_step * 1.000001) nd = ctl.max_time_step;
+    return nd;
+}
+
+// The last node of the adaptive loop's body: the next dt from this step's CFL cargo; the loop
+// goes on while dt stays, the wanted count is not reached and no error was raised.
+__global__ void dt_control_kernel(const unsigned long long* __restrict__ cfl_bits, int* ad, double* adt,
+                                  const int* __restrict__ status, ra_dt_controls ctl, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    const double cfl = __longlong_as_double((long long)*cfl_bits);
+    const double dt = adt[0];
+    const double nd = next_dt_value(ctl, dt, cfl);
+    const int done = ad[0] + 1;
+    ad[0] = done;
+    adt[1] = nd;
+    adt[2] = cfl;
+    const int changed = nd != dt;
+    ad[2] = changed;
+    const bool go = !changed && done < ad[1] && !(nd < ctl.min_time_step) && *status == 0;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+static void enqueue_step(Ctx& c, double new_ab, double old_ab);
+
+// The adaptive loop's graph for the steady step (AB2 factors of equal dt): a conditional WHILE
+// node whose body is the step's kernels and dt_control_kernel, captured once per (dt, controls).
+static void adaptive_graph(Ctx& c, const ra_dt_controls& ctl, double new_ab, double old_ab) {
+    if (c.adapt_exec && !std::memcmp(&c.adapt_ctl, &ctl, sizeof(ctl)) && c.adapt_new_ab == new_ab &&
+        c.adapt_old_ab == old_ab)
+        return;
+    if (c.adapt_exec) cudaGraphExecDestroy(c.adapt_exec);
+    if (c.adapt_graph) cudaGraphDestroy(c.adapt_graph);
+    c.adapt_exec = nullptr;
+    c.adapt_graph = nullptr;
+    if (!c.d_adapt) {
+        RA_CUDA(cudaMalloc(&c.d_adapt, 4 * sizeof(int)));
+        RA_CUDA(cudaMalloc(&c.d_adapt_dt, 3 * sizeof(double)));
+    }
+    cudaGraph_t g = nullptr;
+    RA_CUDA(cudaGraphCreate(&g, 0));
+    c.adapt_graph = g;
+    cudaGraphConditionalHandle h;
+    RA_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    RA_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    const long before = c.launches;
+    RA_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c, new_ab, old_ab);
+    dt_control_kernel<<<1, 32, 0, c.stream>>>(c.d_cfl, c.d_adapt, c.d_adapt_dt, c.d_status, ctl, h);
+    RA_CUDA(cudaGetLastError());
+    RA_CUDA(cudaStreamEndCapture(c.stream, &body));
+    c.adapt_launches = c.launches - before + 1;
+    c.launches = before;
+    RA_CUDA(cudaGraphInstantiate(&c.adapt_exec, g, 0));
+    c.adapt_ctl = ctl;
+    c.adapt_new_ab = new_ab;
+    c.adapt_old_ab = old_ab;
 }
 
 static void run_steps(Ctx& c, int nsteps, double* cfl, bool check = true) {
@@ -1032,6 +1115,10 @@ static void drop_graph(Ctx& c) {
     if (c.graph) cudaGraphDestroy(c.graph);
     c.graph_exec = nullptr;
     c.graph = nullptr;
+    if (c.adapt_exec) cudaGraphExecDestroy(c.adapt_exec);
+    if (c.adapt_graph) cudaGraphDestroy(c.adapt_graph);
+    c.adapt_exec = nullptr;
+    c.adapt_graph = nullptr;
 }
 
 static void set_knob(Ctx& c, int knob, int value) {
@@ -1447,12 +1534,7 @@ int ra_set_bc_mask(ra_ctx* ctx, const double* bc_values) {
     if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        if (c.graph_exec) {   // the captured step holds the old pointer
-            cudaGraphExecDestroy(c.graph_exec);
-            cudaGraphDestroy(c.graph);
-            c.graph_exec = nullptr;
-            c.graph = nullptr;
-        }
+        drop_graph(c);   // the captured steps hold the old pointer
         if (!bc_values) {
             if (c.d_bcval) cudaFree(c.d_bcval);
             c.d_bcval = nullptr;
@@ -1644,19 +1726,7 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me) {
 
 int ra_next_dt(const ra_dt_controls* ctl, double dt, double cfl, double* new_dt) {
     if (!ctl || !new_dt || !(dt > 0)) return RA_ERR_ARG;
-    // Adjust_TimeStep (Sphere_Hybrid_Space.F90:604-649): cfl = the largest squared inverse
-    // crossing time of the step (the CFL cargo), the new dt applies from the next step
-    double nd = dt;
-    if (cfl > 0.0) {
-        const double maxt = 1.0 / std::sqrt(cfl);
-        if (dt < maxt * ctl->cflmin) {
-            nd = std::min(ctl->cflmax * maxt, ctl->max_time_step);
-        } else if (dt > maxt * ctl->cflmax) {
-            nd = ctl->cflmax * maxt;
-            if (nd > dt * (1.0 - ctl->min_dt_change)) nd = dt * (1.0 - ctl->min_dt_change);
-        }
-    }
-    if (nd > ctl->max_time_step * 1.000001) nd = ctl->max_time_step;
+    const double nd = next_dt_value(*ctl, dt, cfl);
     *new_dt = nd;
     return nd < ctl->min_time_step ? RA_ERR_NONFINITE : RA_OK;
 }
@@ -1677,20 +1747,48 @@ int ra_step_adaptive(ra_ctx* ctx, int nsteps, const ra_dt_controls* ctl, double*
     int changes = 0;
     const int rc = guarded(ctx, [&] {
         Ctx& c = ctx->c;
-        for (int s = 0; s < nsteps; ++s) {
-            double cfl = 0.0;
-            run_steps(c, 1, &cfl);
-            double nd = c.dt;
-            if (ra_next_dt(ctl, c.dt, cfl, &nd) != RA_OK)
+        if (!c.have_state) throw ArgError("ra_put_state must be called before stepping");
+        auto change_dt = [&](double nd) {   // Reset_Linear_Equations before the next step
+            if (nd < ctl->min_time_step)
                 throw NonFiniteError("the time step became smaller than min_time_step (" + std::to_string(nd) + ")");
-            if (nd != c.dt) {   // Reset_Linear_Equations before the next step
-                if (c.custom_reference)
-                    throw StateError("a dt change needs the driver's matrices after ra_set_reference");
-                c.dt = nd;
-                linear_setup(c);
-                if (c.mixed_solve) mixed_resplit_solve(c);
-                ++changes;
+            if (nd == c.dt) return;
+            if (c.custom_reference) throw StateError("a dt change needs the driver's matrices after ra_set_reference");
+            c.dt = nd;
+            linear_setup(c);
+            if (c.mixed_solve) mixed_resplit_solve(c);
+            ++changes;
+        };
+        int s = 0;
+        while (s < nsteps) {
+            double new_ab, old_ab;
+            ab_factors(c, new_ab, old_ab);
+            if (!c.cfg.use_graph || c.iteration == 1 || c.old_dt != c.dt || nsteps - s < 2) {
+                // one step on the host's control: the first (Euler) step, the first after a dt
+                // change (unequal AB2 factors), or a last single step
+                double cfl = 0.0;
+                run_steps(c, 1, &cfl);
+                ++s;
+                change_dt(next_dt_value(*ctl, c.dt, cfl));
+                continue;
             }
+            // the steady steps on the device's control: the loop graph runs until dt changes
+            adaptive_graph(c, *ctl, new_ab, old_ab);
+            int ad[4] = {0, nsteps - s, 0, 0};
+            double adt[3] = {c.dt, c.dt, 0.0};
+            RA_CUDA(cudaMemcpyAsync(c.d_adapt, ad, sizeof(ad), cudaMemcpyHostToDevice, c.stream));
+            RA_CUDA(cudaMemcpyAsync(c.d_adapt_dt, adt, sizeof(adt), cudaMemcpyHostToDevice, c.stream));
+            RA_CUDA(cudaGraphLaunch(c.adapt_exec, c.stream));
+            RA_CUDA(cudaMemcpyAsync(ad, c.d_adapt, sizeof(ad), cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaMemcpyAsync(adt, c.d_adapt_dt, sizeof(adt), cudaMemcpyDeviceToHost, c.stream));
+            RA_CUDA(cudaStreamSynchronize(c.stream));
+            const int done = ad[0];
+            if (done < 1 || done > nsteps - s) throw ArgError("adaptive step loop: bad step count");
+            c.launches += (long)done * c.adapt_launches;
+            c.iteration += done;
+            c.old_dt = c.dt;
+            s += done;
+            check_status(c);
+            change_dt(adt[1]);
         }
     });
     if (dt_out) *dt_out = ctx->c.dt;

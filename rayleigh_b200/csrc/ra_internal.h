@@ -209,6 +209,15 @@ struct Ctx {
     cudaGraphExec_t graph_exec = nullptr;
     long graph_launches = 0;                          // kernels in one replay of the step graph
     double graph_old_ab = 0, graph_new_ab = 0;
+    // ra_step_adaptive's device-side CFL control: a graph whose conditional WHILE node replays
+    // the steady step followed by Adjust_TimeStep until dt changes or the count is reached
+    cudaGraph_t adapt_graph = nullptr;
+    cudaGraphExec_t adapt_exec = nullptr;
+    ra_dt_controls adapt_ctl{};
+    double adapt_new_ab = 0, adapt_old_ab = 0;
+    long adapt_launches = 0;
+    int* d_adapt = nullptr;          // [0] steps done, [1] steps wanted, [2] dt changed
+    double* d_adapt_dt = nullptr;    // [0] the steps' dt, [1] the next dt, [2] the last CFL cargo
 };
 
 // bits of the device error word

@@ -365,6 +365,26 @@ int ra_legendre_p2s(ra_ctx* ctx, const double* p, double* s, int nf, int nr);
 /* c2r_ip4D_fftw / r2c_ip4D_fftw (Fourier_Transform.F90:100-183): in place on
  * x(n_phi+2, howmany), unnormalised, FFTW's packed (re, im) layout. */
 int ra_fft_c2r(ra_ctx* ctx, double* x, long howmany);
+/* Device-resident spherical-harmonic transforms of nfr complex columns (fields x radial
+ * levels), operands in device memory (no host copies): direction 0 (spectral -> physical)
+ * runs StP_4d_dgp2 (Legendre_Transforms.F90:968-1074) from d_spec into d_work, unfolds the
+ * (theta, pi - theta) blocks into phi rows in d_grid and runs FFT_To_Physical's c2r
+ * (Fourier_Transform.F90:142-183) in place; direction 1 (physical -> spectral) runs the r2c
+ * in place on d_grid (overwriting it), folds into d_work and runs PtS_4d_dgpv3 (:1077-1175)
+ * into d_spec.  precision RA_PREC_FP64 (FP64 tensor-core products) or RA_PREC_MIXED
+ * (split int8 products; their plan is built on the first call with given operands).
+ *   d_spec: [n_lm rows][nfr][re, im], rows m-major with the even l - m first (the row order
+ *           of the ra_* device buffers: row(m, l) = off(m) + (l - m even ? (l - m)/2 :
+ *           ne(m) + (l - m - 1)/2), off(m) = m L - m (m - 1)/2, ne(m) = (L - m + 1)/2)
+ *   d_grid: [n_theta][nfr][n_phi + 2] real rows (Gauss-Legendre theta order)
+ *   d_work: l_max + 1 times n_theta times nfr complex entries (the E/O or folded blocks)
+ * stage_ms (may be NULL) receives the device times of [0] the Legendre product (with the
+ * digit split), [1] the relayout and [2] the FFT.  The call first makes the context's stream
+ * wait for the work queued on the legacy default stream (operands written there are
+ * complete) and returns with its own work complete; operands written on other streams must
+ * be complete before the call. */
+int ra_transform_dev(ra_ctx* ctx, int direction, int precision, double* d_spec, double* d_grid, double* d_work,
+                     int nfr, double* stage_ms);
 int ra_fft_r2c(ra_ctx* ctx, double* x, long howmany);
 
 /* Chebyshev_Polynomials.F90: To_Spectral4D (:375), From_Spectral4D (:450) and

@@ -237,6 +237,7 @@ def load_library(path: str | None = None):
         "ra_factor": ([_VP, ctypes.c_double], ctypes.c_int),
         "ra_set_bc_mask": ([_VP, _VP], ctypes.c_int),
         "ra_set_reference": ([_VP, _VP, _VP, _VP, _VP, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "ra_transform_dev": ([_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, ctypes.c_int, _DP], ctypes.c_int),
         "ra_lu_create": ([ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "ra_lu_destroy": ([_VP], ctypes.c_int),
         "ra_lu_last_error": ([_VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
@@ -385,6 +386,15 @@ class Rayleigh:
         """bc_values[eq W/P/T/Z][lm][re/im][top/bottom] (Fortran bc_values(2, 2, n_lm, 4)), or None."""
         self._bcv = None if bc_values is None else _f64(bc_values)
         self._check(self.lib.ra_set_bc_mask(self.h, _ptr(self._bcv)))
+
+    def transform_dev(self, direction, precision, d_spec, d_grid, d_work, nfr):
+        """ra_transform_dev on device buffers given by address (e.g. torch tensors' data_ptr());
+        returns the stage times [Legendre product, relayout, FFT] in ms."""
+        ms = (ctypes.c_double * 3)()
+        self._check(self.lib.ra_transform_dev(self.h, int(direction), int(precision), ctypes.c_void_p(d_spec),
+                                              ctypes.c_void_p(d_grid), ctypes.c_void_p(d_work), int(nfr),
+                                              ctypes.cast(ms, _DP)))
+        return list(ms)
 
     def set_reference(self, density, dlnrho, viscous_heating_coeff=None, ohmic_heating_coeff=None,
                       coriolis_coeff=0.0, lorentz_coeff=0.0):

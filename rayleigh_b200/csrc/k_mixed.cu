@@ -43,6 +43,8 @@ static void plan_launch(Ctx& c, MixedPlan& p, const std::vector<OzProblem>& prob
     p.ntiles = (int)(tiles.size() / 4);
 }
 
+static void free_plan(MixedPlan& p);
+
 static void run_split_once(Ctx& c, const std::vector<OzSplitJob>& jobs, int max_rows) {
     if (jobs.empty()) return;
     OzSplitJob* d = upload(c, jobs);
@@ -54,12 +56,13 @@ static void run_split_once(Ctx& c, const std::vector<OzSplitJob>& jobs, int max_
 // ---------------------------------------------------------------------------
 // Inverse Legendre transform
 // ---------------------------------------------------------------------------
-static void setup_lt_inverse(Ctx& c) {
+// The plan of one batched inverse transform p2 = P s2 over ncol columns (s2 rows in the
+// m-major parity-sorted order, p2[theta_h][m][par][col]): the step's (s2a11 -> p2a) and the
+// device-resident unit transform's.
+static void build_lt_inverse(Ctx& c, MixedPlan& p, const double* s2, double* p2, int ncol) {
     const Dims& d = c.d;
     const int L = d.L, nth2 = d.nth2;
-    const int ncol = c.nfa * d.nr * 2;
     const int nta = oz_tiles_of(ncol, OZ_HA), ntb = oz_tiles_of(nth2, OZ_HB);
-    MixedPlan& p = c.mx_inv;
     std::vector<long> aoff(2 * L + 1, 0), boff(2 * L + 1, 0);
     std::vector<int> nks(2 * L), nl(2 * L);
     for (int q = 0; q < 2 * L; ++q) {
@@ -78,7 +81,7 @@ static void setup_lt_inverse(Ctx& c) {
     for (int q = 0; q < 2 * L; ++q) {
         const int m = q >> 1, par = q & 1;
         const long roff = m_off(m, L) + (par ? n_even(m, L) : 0);
-        double* out = c.d_p2a + (size_t)q * ncol;   // p2a[theta_h][m][par][col]
+        double* out = p2 + (size_t)q * ncol;   // p2[theta_h][m][par][col]
         const long th_stride = 2L * L * ncol;
         if (nks[q] == 0) {   // no l of this parity: the E/O block stays zero
             RA_CUDA(cudaMemset2DAsync(out, th_stride * sizeof(double), 0, ncol * sizeof(double), nth2, c.stream));
@@ -89,7 +92,7 @@ static void setup_lt_inverse(Ctx& c) {
         int* ea = p.d_ea + (size_t)q * ncol;
         int* eb = p.d_eb + (size_t)q * nth2;
         // A = s2^T: rows = columns of the s2 block (contiguous), K = l; split every step
-        ajobs.push_back({c.d_s2a11 + roff * ncol, 1L, (long)ncol, ncol, nl[q], OZ_HA, nta, nks[q], adig, ea});
+        ajobs.push_back({s2 + roff * ncol, 1L, (long)ncol, ncol, nl[q], OZ_HA, nta, nks[q], adig, ea});
         // B^T = P^T: rows theta_h (contiguous in the table), K = l; split once
         bjobs.push_back({c.d_Ptab + roff * nth2, 1L, (long)nth2, nth2, nl[q], OZ_HB, ntb, nks[q], bdig, eb});
         probs.push_back({adig, bdig, (long)nks[q] * OZ_ABLK, (long)nks[q] * OZ_BBLK, ea, eb, ncol, nth2, nks[q], out,
@@ -103,22 +106,25 @@ static void setup_lt_inverse(Ctx& c) {
     plan_launch(c, p, probs);
 }
 
-void launch_lt_inverse_mixed(Ctx& c) {
-    MixedPlan& p = c.mx_inv;
+static void setup_lt_inverse(Ctx& c) { build_lt_inverse(c, c.mx_inv, c.d_s2a11, c.d_p2a, c.nfa * c.d.nr * 2); }
+
+static void run_plan(Ctx& c, MixedPlan& p) {
     ozaki_split(c, p.d_jobs, p.njobs, p.max_rows, p.kinds);
     ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
 }
 
+void launch_lt_inverse_mixed(Ctx& c) { run_plan(c, c.mx_inv); }
+
 // ---------------------------------------------------------------------------
 // Forward Legendre transform
 // ---------------------------------------------------------------------------
-static void setup_lt_forward(Ctx& c) {
+// The plan of one batched forward transform s2 = iP p2 over ncol columns (p2 folded,
+// [m][par][theta_h][col]).
+static void build_lt_forward(Ctx& c, MixedPlan& p, const double* p2, double* s2, int ncol) {
     const Dims& d = c.d;
     const int L = d.L, nth2 = d.nth2;
-    const int ncol = c.nfb * d.nr * 2;
     const int nta = oz_tiles_of(ncol, OZ_HA), nks = oz_ksteps(nth2);
     const long ablk = (long)nta * nks * OZ_ABLK;
-    MixedPlan& p = c.mx_fwd;
     std::vector<long> boff(2 * L + 1, 0);
     for (int q = 0; q < 2 * L; ++q) {
         const int m = q >> 1, par = q & 1;
@@ -144,11 +150,11 @@ static void setup_lt_forward(Ctx& c) {
         int* ea = p.d_ea + (size_t)q * ncol;
         int* eb = p.d_eb + roff;
         // A = p2b^T: rows = columns of the folded block (contiguous), K = theta_h
-        ajobs.push_back({c.d_p2b + (size_t)q * nth2 * ncol, 1L, (long)ncol, ncol, nth2, OZ_HA, nta, nks, adig, ea});
+        ajobs.push_back({p2 + (size_t)q * nth2 * ncol, 1L, (long)ncol, ncol, nth2, OZ_HA, nta, nks, adig, ea});
         // B^T = iP rows (theta_h contiguous)
         bjobs.push_back({c.d_iPtab + roff * nth2, (long)nth2, 1L, nl, nth2, OZ_HB, ntb, nks, bdig, eb});
         probs.push_back({adig, bdig, (long)nks * OZ_ABLK, (long)nks * OZ_BBLK, ea, eb, ncol, nl, nks,
-                         c.d_s2b + roff * ncol, 1L, (long)ncol});
+                         s2 + roff * ncol, 1L, (long)ncol});
     }
     run_split_once(c, bjobs, max_b);
     p.d_jobs = upload(c, ajobs);
@@ -159,10 +165,41 @@ static void setup_lt_forward(Ctx& c) {
     RA_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-void launch_lt_forward_mixed(Ctx& c) {
-    MixedPlan& p = c.mx_fwd;
-    ozaki_split(c, p.d_jobs, p.njobs, p.max_rows, p.kinds);
-    ozaki_gemm(c, p.d_probs, p.d_tiles, p.ntiles, c.d_status);
+static void setup_lt_forward(Ctx& c) { build_lt_forward(c, c.mx_fwd, c.d_p2b, c.d_s2b, c.nfb * c.d.nr * 2); }
+
+void launch_lt_forward_mixed(Ctx& c) { run_plan(c, c.mx_fwd); }
+
+// The device-resident unit transforms' split-product plans, one per direction, rebuilt when
+// the operands or the column count change.
+void launch_lt_unit_mixed(Ctx& c, int inverse, const double* in, double* out, int ncol) {
+    UnitPlan& u = inverse ? c.unit_inv : c.unit_fwd;
+    if (!u.built || u.in != in || u.out != out || u.ncol != ncol) {
+        free_plan(u.plan);
+        if (!c.d_status) {
+            malloc_dev(c.d_status, 1);
+            RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+        }
+        if (inverse)
+            build_lt_inverse(c, u.plan, in, out, ncol);
+        else
+            build_lt_forward(c, u.plan, in, out, ncol);
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+        u.built = true;
+        u.in = in;
+        u.out = out;
+        u.ncol = ncol;
+    } else if (inverse) {
+        // the caller may have reused the output buffer: the (m, parity) blocks without an l
+        // (their zeros were written when the plan was built) are cleared again
+        const int L = c.d.L, nth2 = c.d.nth2;
+        for (int q = 0; q < 2 * L; ++q) {
+            const int m = q >> 1;
+            if (oz_ksteps((q & 1) ? n_odd(m, L) : n_even(m, L)) == 0)
+                RA_CUDA(cudaMemset2DAsync(out + (size_t)q * ncol, 2L * L * ncol * sizeof(double), 0,
+                                          ncol * sizeof(double), nth2, c.stream));
+        }
+    }
+    run_plan(c, u.plan);
 }
 
 // ---------------------------------------------------------------------------
@@ -282,6 +319,8 @@ static void free_plan(MixedPlan& p) {
 void mixed_release(Ctx& c) {
     free_plan(c.mx_inv);
     free_plan(c.mx_fwd);
+    free_plan(c.unit_inv.plan);
+    free_plan(c.unit_fwd.plan);
     free_plan(c.mx_solve);
 }
 

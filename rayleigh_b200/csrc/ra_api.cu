@@ -2292,6 +2292,26 @@ static int fft_op(ra_ctx* ctx, double* x, long howmany, int inverse) {
 }
 
 int ra_fft_c2r(ra_ctx* ctx, double* x, long howmany) { return fft_op(ctx, x, howmany, 1); }
+
+int ra_transform_dev(ra_ctx* ctx, int direction, int precision, double* d_spec, double* d_grid, double* d_work,
+                     int nfr, double* stage_ms) {
+    if (!ctx || ctx->c.d.L == 0) return RA_ERR_STATE;
+    if (!d_spec || !d_grid || !d_work || nfr <= 0 || (direction != 0 && direction != 1)) return RA_ERR_ARG;
+    if (precision != RA_PREC_FP64 && precision != RA_PREC_MIXED) return RA_ERR_ARG;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        // the operands may have been written by work queued on the legacy default stream (where
+        // frameworks queue by default); the context's non-blocking stream waits for it
+        cudaEvent_t ready;
+        RA_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        RA_CUDA(cudaEventRecord(ready, cudaStreamLegacy));
+        RA_CUDA(cudaStreamWaitEvent(c.stream, ready, 0));
+        cudaEventDestroy(ready);
+        RA_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream));
+        transform_dev(c, direction, precision, d_spec, d_grid, d_work, nfr, stage_ms);
+        check_status(c);
+    });
+}
 int ra_fft_r2c(ra_ctx* ctx, double* x, long howmany) { return fft_op(ctx, x, howmany, 0); }
 
 static int cheb_op(ra_ctx* ctx, const double* in, double* out, long ncols, int mode, int order) {

@@ -128,6 +128,16 @@ struct MixedPlan {
     int nsetup_jobs = 0, setup_max_rows = 0, setup_kinds = 0;
 };
 
+// A split-product plan of the device-resident unit transform (ra_transform_dev) for one
+// direction, with the operands it was built for.
+struct UnitPlan {
+    MixedPlan plan;
+    bool built = false;
+    const double* in = nullptr;
+    double* out = nullptr;
+    int ncol = 0;
+};
+
 struct Ctx {
     ra_config cfg;
     Dims d;
@@ -144,6 +154,7 @@ struct Ctx {
     // inverse and the mixed form solves by the FP64 block substitution
     bool mixed_solve = false;
     bool custom_reference = false;                    // radial profiles given by ra_set_reference
+    UnitPlan unit_inv, unit_fwd;                      // ra_transform_dev's split-product plans
     int nfa = NP2A, nfb = NP2B, ng = NG;              // fields of s2a11/p2a, of p2b/s2b, grids (more with mag)
 
     Radial rad;
@@ -291,6 +302,9 @@ void launch_cheb_columns(Ctx& c, const double* d_in, double* d_out, long ncols, 
 void mixed_setup(Ctx& c);
 void mixed_release(Ctx& c);
 void launch_lt_inverse_mixed(Ctx& c);
+void launch_lt_unit_mixed(Ctx& c, int inverse, const double* in, double* out, int ncol);
+void transform_dev(Ctx& c, int direction, int precision, double* spec, double* grid, double* work, int nfr,
+                   double* stage_ms);
 void launch_lt_forward_mixed(Ctx& c);
 void launch_solve_mixed(Ctx& c);
 void mixed_resplit_solve(Ctx& c);

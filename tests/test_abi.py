@@ -69,6 +69,17 @@ def test_config_layout_and_defaults_agree():
         assert getattr(c, n) == getattr(py, n), n
 
 
+def test_contextless_calls_of_the_newer_entry_points():
+    """ra_set_reference, ra_transform_dev and ra_step_adaptive without a context report a state
+    error before touching a device."""
+    import rayleigh_b200 as rb
+    lib = rb.load_library()
+    assert lib.ra_set_reference(None, None, None, None, None, 0.0, 0.0) == rb.RA_ERR_STATE
+    assert lib.ra_transform_dev(None, 0, 0, None, None, None, 1, None) == rb.RA_ERR_STATE
+    ctl = rb.DtControls().to_c()
+    assert lib.ra_step_adaptive(None, 1, ctypes.byref(ctl), None, None) == rb.RA_ERR_STATE
+
+
 def test_reference_state_arguments_are_checked():
     import rayleigh_b200 as rb
     lib = rb.load_library()

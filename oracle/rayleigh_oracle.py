@@ -63,6 +63,7 @@ class Config:
     dtdr_bottom: float = 0.0
     dt: float = 1.0e-4
     alpha_implicit: float = 0.5
+    chebyshev: bool = True           # Numerical_Controls (Controls.F90): False = finite differences, uniform grid
     # Reference_Namelist (PDE_Coefficients.F90:84-160): 1 Constant_Reference (Boussinesq),
     # 2 Polytropic_Reference (dimensional, cgs), 3 Polytropic_ReferenceND
     reference_type: int = 1
@@ -93,7 +94,7 @@ class Config:
             self.n_theta = (3 * (self.l_max + 1)) // 2
         if self.n_theta % 2:
             raise ValueError("n_theta must be even")
-        if self.n_r % 2:
+        if self.n_r % 2 and self.chebyshev:
             raise ValueError("n_r must be even (single Chebyshev domain, parity split)")
 
     @property
@@ -338,6 +339,132 @@ def fft_r2c(p3, n_phi):
 
 
 # ---------------------------------------------------------------------------
+# Finite-difference radial grid (chebyshev = .false.): the uniform grid of
+# Initialize_Radial_Grid (ProblemSize.F90:607-618) and the stencils of
+# Finite_Difference.F90 (Initialize_Derivatives :69-93, Initialize_dcoefs
+# :464-521, Generate_Coefs :525-689, with the default 5-point stencils and
+# boundary accuracy 2).  The state holds grid values, so to_spectral,
+# from_spectral and dealias are identities and a derivative is the banded
+# matrix D_d applied along the radius (d_by_dx3d3 :374-460; the same rows
+# Load_Interior_RowsFD / Load_Single_RowFD put in the implicit matrices, :717-866).
+# ---------------------------------------------------------------------------
+def fd_generate_coefs(grid, n_stencil, deriv_order, boundary_accuracy):
+    """Generate_Coefs (transition type 1): coefs[n_stencil, ngrid] (0-based rows of the
+    Fortran coefs(1:n_stencil, i)).  Interior points use the centred stencil clipped at the
+    ends; the two end points one-sided stencils of deriv_order + boundary_accuracy points.
+    Each stencil's weights are a row of the inverse of the Vandermonde matrix of the
+    point offsets (scaled by their mean, rescaled after), times j!."""
+    ngrid = len(grid)
+    sr = n_stencil // 2
+    sc = sr + 1                                              # stencil centre, 1-based
+    coefs = np.zeros((n_stencil, ngrid))
+
+    def weights(dees, dmean, nxy):
+        temp = np.zeros((nxy, nxy))
+        temp[:, 0] = 1.0
+        for k in range(1, nxy):
+            temp[:, k] = dees ** k
+        inv = np.linalg.inv(temp)                            # dgetrf + dgetri
+        jfact = 1.0
+        for j in range(2, nxy + 1):                          # Fortran rows j = 2 .. nxy
+            jfact = jfact * float(j - 1)
+            inv[j - 1, :] = inv[j - 1, :] * jfact * (1.0 / dmean) ** (j - 1)
+        return inv[deriv_order, :]
+
+    for i in range(2, ngrid):                                # Fortran i = 2 .. ngrid - 1
+        jstart = max(1, sc - i + 1)
+        jend = min(n_stencil, (ngrid - i) + sc)
+        nxy = jend - jstart + 1
+        dees = np.zeros(n_stencil + 1)                       # 1-based
+        dsum = 0.0
+        for j in range(jstart, jend + 1):
+            dees[j] = grid[i + j - sc - 1] - grid[i - 1]
+            dsum = dsum + abs(dees[j])
+        dees[sc] = 0.0
+        dmean = dsum / float(nxy - 1)
+        d = dees[jstart:jend + 1] / dmean
+        coefs[jstart - 1:jend, i - 1] = weights(d, dmean, nxy)
+    nxy = deriv_order + boundary_accuracy
+    for this_pt, diff_dir in ((1, 1), (ngrid, -1)):
+        dees = np.zeros(nxy)
+        dsum = 0.0
+        if diff_dir == 1:
+            for j in range(2, nxy + 1):
+                dees[j - 1] = grid[this_pt + j - 2] - grid[this_pt - 1]
+                dsum = dsum + dees[j - 1]
+        else:
+            for j in range(1, nxy):
+                dees[j - 1] = grid[this_pt + (j - nxy) - 1] - grid[this_pt - 1]
+                dsum = dsum + dees[j - 1]
+        dmean = dsum / float(nxy - 1)
+        w = weights(dees / dmean, dmean, nxy)
+        if diff_dir == 1:
+            coefs[0:nxy, this_pt - 1] = w
+        else:
+            coefs[n_stencil - nxy:n_stencil, this_pt - 1] = w
+    return coefs
+
+
+class FiniteDifference:
+    N_STENCIL = (5, 5, 5)          # n_stencil_1..3 (Finite_Difference.F90:10-12)
+    BOUNDARY_ACCURACY = (2, 2, 2)  # boundary_accuracy_1..3 (:14-16)
+
+    def __init__(self, n, rmin, rmax, dmax=3):
+        self.n = n
+        r = np.zeros(n)
+        r[n - 1] = rmin
+        dr = 1.0 / (n - 1.0) * (rmax - rmin)
+        for i in range(n - 2, -1, -1):
+            r[i] = dr + r[i + 1]
+        self.radius = r
+        self.delta_r = np.full(n, dr)
+        ns = max(self.N_STENCIL)
+        kd = (ns + 1) // 2
+        d = np.zeros((dmax + 1, n, n))
+        d[0] = np.eye(n)
+        for dd in range(1, dmax + 1):
+            st, ba = self.N_STENCIL[dd - 1], self.BOUNDARY_ACCURACY[dd - 1]
+            c = fd_generate_coefs(r, st, dd, ba)
+            off = (ns - st) // 2
+            full = np.zeros((ns, n))
+            full[off:ns - off, 1:n - 1] = c[:, 1:n - 1]
+            full[0:st, 0] = c[:, 0]
+            full[ns - st:ns, n - 1] = c[:, n - 1]
+            nb = dd + ba
+            m = np.zeros((n, n))
+            m[0, 0:nb] = full[0:nb, 0]
+            m[n - 1, n - nb:n] = full[ns - nb:ns, n - 1]
+            for i in range(1, n - 1):                        # Fortran r = i + 1
+                rr = i + 1
+                kstart = max(1, kd - rr + 1)
+                kend = min(st, (n - rr) + kd)
+                for kk in range(kstart, kend + 1):
+                    m[i, rr + kk - kd - 1] = full[kk - 1, i]
+            d[dd] = m
+        self.dcheby = d
+        self.rda = n + 1           # every column of a boundary row (no dealiasing)
+        # Initialize_Derivatives' integration weights: (r_{i-1} - r_{i+1}) / 2 r_i^2, normalised
+        w = np.zeros(n)
+        for i in range(1, n - 1):
+            w[i] = (r[i - 1] - r[i + 1]) / 2.0 * r[i] ** 2
+        w[0] = (r[0] - r[1]) / 2.0 * r[0] ** 2
+        w[n - 1] = (r[n - 2] - r[n - 1]) / 2.0 * r[n - 1] ** 2
+        self.integration_weights = w / w.sum()
+
+    def to_spectral(self, f):
+        return np.array(f, copy=True)
+
+    def from_spectral(self, c):
+        return np.array(c, copy=True)
+
+    def dealias(self, c):
+        return np.array(c, copy=True)
+
+    def deriv(self, c, d):
+        return np.einsum("rk,...k->...r", self.dcheby[d], c)
+
+
+# ---------------------------------------------------------------------------
 # Chebyshev grid (Chebyshev_Polynomials.F90:65-644), single domain
 # ---------------------------------------------------------------------------
 
@@ -461,14 +588,17 @@ class Oracle:
         rmax = cfg.shell_depth / (1.0 - cfg.aspect_ratio)
         rmin = rmax * cfg.aspect_ratio
         self.rmin, self.rmax = rmin, rmax
-        self.cg = Chebyshev(cfg.n_r, rmin, rmax)
+        self.cg = Chebyshev(cfg.n_r, rmin, rmax) if cfg.chebyshev else FiniteDifference(cfg.n_r, rmin, rmax)
         r = self.cg.radius
         self.radius = r
         nr = cfg.n_r
-        # Delta_r (ProblemSize.F90:541-549)
-        dr = np.empty(nr)
-        dr[0] = r[0] - r[1]
-        dr[1:] = r[:-1] - r[1:]
+        if cfg.chebyshev:
+            # Delta_r (ProblemSize.F90:541-549)
+            dr = np.empty(nr)
+            dr[0] = r[0] - r[1]
+            dr[1:] = r[:-1] - r[1:]
+        else:
+            dr = self.cg.delta_r                               # uniform_dr (:611-613)
         self.delta_r = dr
         self._reference_state()
         self.ls, self.ms = lm_pairs(cfg.l_max)
@@ -803,7 +933,9 @@ class Oracle:
 
     # ----- the five stages of one step (Sphere_Driver.F90:305-328) -----
     def post_solve(self):
-        """Sphere_Spectral_Space.F90:178-413 (Chebyshev branch), ending with Transpose_1a2a."""
+        """Sphere_Spectral_Space.F90:178-413 (Chebyshev branch; the finite-difference branch
+        Post_Solve_FD :37-176 is the same with identity transforms and the deriv_cluge),
+        ending with Transpose_1a2a."""
         cg = self.cg
         if self.iteration == 1:
             self.new_ab, self.old_ab = self.dt, 0.0
@@ -849,6 +981,11 @@ class Oracle:
         self._add_derivative(p1b, WEQ, TVAR, 0, Tg)
         self._add_derivative(p1b, ZEQ, ZVAR, 0, Zg)
         self._add_derivative(p1b, ZEQ, ZVAR, 1, dZg)
+        if not self.cfg.chebyshev:
+            # Post_Solve_FD's deriv_cluge (Sphere_Spectral_Space.F90:96-98, Controls.F90:44): the
+            # d2W/dr2 that goes on to rlm_spacea is d/dr of dW/dr
+            g = g.copy()
+            g[7] = cg.deriv(dWg, 1)
         if self.mag:                                            # :370-384
             Cg, Ag, dCg, dAg, d2Cg = g[8:13]
             self._add_derivative(p1b, AEQ, AVAR, 0, Ag)
@@ -1279,6 +1416,8 @@ class Oracle:
         3 pi scaling / ((r_o^3 - r_i^3) N) r^2 sqrt(1 - x^2), halved at the two end
         points; they sum to ~1 (a volume average over the shell)."""
         cg, n = self.cg, self.cfg.n_r
+        if not self.cfg.chebyshev:   # finite differences: Initialize_Derivatives (Finite_Difference.F90:69-93)
+            return cg.integration_weights.copy()
         scaling = (self.rmax - self.rmin) / (cg.x[0] - cg.x[n - 1])
         int_scale = 3.0 * math.pi * scaling / ((self.rmax ** 3 - self.rmin ** 3) * n)
         w = int_scale * self.radius ** 2 * np.sqrt(1.0 - cg.x * cg.x)
@@ -1424,14 +1563,15 @@ class Oracle:
         return self.last_cfl
 
 
-def c2001_case0_config(n_r=48, n_theta=64):
+def c2001_case0_config(n_r=48, n_theta=64, chebyshev=True):
     """The settings benchmark_mode = 1 imposes (Benchmarking.F90:107-149: Christensen
     et al. 2001, hydrodynamic case 0) on an n_r x n_theta grid; l_max from n_theta as
-    ProblemSize.F90:431-436 derives it (2 n_theta / 3 - 1)."""
+    ProblemSize.F90:431-436 derives it (2 n_theta / 3 - 1).  chebyshev=False: the
+    finite-difference radial mode on its uniform grid."""
     return Config(n_r=n_r, l_max=(2 * n_theta) // 3 - 1, n_theta=n_theta, aspect_ratio=0.35, shell_depth=1.0,
                   rayleigh=1.0e5, ekman=1.0e-3, prandtl=1.0, gravity_power=1.0, rotation=True,
                   no_slip_top=True, no_slip_bottom=True, fix_tvar_top=True, fix_tvar_bottom=True,
-                  t_top=0.0, t_bottom=1.0, dt=1.0e-4, alpha_implicit=0.50001)
+                  t_top=0.0, t_bottom=1.0, dt=1.0e-4, alpha_implicit=0.50001, chebyshev=chebyshev)
 
 
 def c2001_case1_config(n_r=64, n_theta=96):

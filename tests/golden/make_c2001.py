@@ -11,8 +11,11 @@ Run from the repository root in a container that has the reference tree:
 
     python tests/golden/make_c2001.py /path/to/reference
 
-The output ``tests/golden/c2001_case0.json`` is committed; nothing at test
-time reads the reference tree.
+The reference also ships the same run in its finite-difference radial mode,
+``tests/c2001_case0_FD_uniform`` (chebyshev = .false., uniform grid); its report goes
+to ``tests/golden/c2001_case0_fd_uniform.json``.
+
+The outputs are committed; nothing at test time reads the reference tree.
 """
 import json
 import os
@@ -22,11 +25,11 @@ import sys
 if len(sys.argv) != 2:
     sys.exit("usage: python %s /path/to/reference" % os.path.relpath(__file__))
 REF = sys.argv[1]
-CASE = os.path.join(REF, "tests", "c2001_case0")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def main():
+def extract(case, out_name):
+    CASE = os.path.join(REF, "tests", case)
     inp = open(os.path.join(CASE, "main_input")).read()
     rep = open(os.path.join(CASE, "Benchmark_Reports", "00000400")).read()
 
@@ -42,7 +45,8 @@ def main():
         m = re.search(re.escape(name) + r"\s*:\s*([-0-9.]+)\s+([-0-9.]+)\s+([-0-9.]+)\s+([-0-9.]+)", rep)
         obs[name] = {"measured": float(m.group(1)), "suggested": float(m.group(2)), "sdev": float(m.group(4))}
     out = {
-        "source": "tests/c2001_case0/main_input and tests/c2001_case0/Benchmark_Reports/00000400 of the reference",
+        "source": "tests/%s/main_input and tests/%s/Benchmark_Reports/00000400 of the reference" % (case, case),
+        "chebyshev": not re.search(r"chebyshev\s*=\s*\.false\.", inp, re.I),
         "n_r": int(nml("n_r")),
         "n_theta": int(nml("n_theta")),
         "max_time_step": nml("max_time_step"),
@@ -53,9 +57,14 @@ def main():
         "samples": iline("Number of Samples"),
         "observables": obs,
     }
-    with open(os.path.join(HERE, "c2001_case0.json"), "w") as f:
+    with open(os.path.join(HERE, out_name), "w") as f:
         json.dump(out, f, indent=1)
     print(json.dumps(out, indent=1))
+
+
+def main():
+    extract("c2001_case0", "c2001_case0.json")
+    extract("c2001_case0_FD_uniform", "c2001_case0_fd_uniform.json")
 
 
 if __name__ == "__main__":

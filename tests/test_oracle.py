@@ -165,18 +165,21 @@ def test_perturbation_evolves_and_stays_finite():
     assert cfl > 0.0
 
 
-def test_c2001_case0_matches_the_reference_regression_report():
-    """The reference's own regression run of its accuracy benchmark
+@pytest.mark.parametrize("golden", ["c2001_case0.json", "c2001_case0_fd_uniform.json"])
+def test_c2001_case0_matches_the_reference_regression_report(golden):
+    """The reference's own regression runs of its accuracy benchmark
     (tests/c2001_case0: Christensen et al. 2001 case 0 from Benchmark_Init_Hydro,
-    N_r = 48, N_theta = 64, 400 steps of dt = 1e-4, alpha = 0.50001): mean and
-    standard deviation of the volume-averaged kinetic energy at iterations 100,
-    200, 300, 400, and of the point observations T and v_phi where v_r = 0 at
-    mid-depth on the equator, as its Benchmark_Reports/00000400 prints them (6
-    decimals).  This pins the oracle's whole time step, not only its transforms."""
+    N_r = 48, N_theta = 64, 400 steps of dt = 1e-4, alpha = 0.50001; and
+    tests/c2001_case0_FD_uniform, the same run in the finite-difference radial mode on
+    its uniform grid): mean and standard deviation of the volume-averaged kinetic
+    energy at iterations 100, 200, 300, 400, and of the point observations T and
+    v_phi where v_r = 0 at mid-depth on the equator, as each run's
+    Benchmark_Reports/00000400 prints them (6 decimals).  This pins the oracle's whole
+    time step, not only its transforms, in both radial discretisations."""
     import json
     import os
-    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c2001_case0.json")))
-    cfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"])
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", golden)))
+    cfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"], chebyshev=gold.get("chebyshev", True))
     o = O.Oracle(cfg)
     wpt, z = o.benchmark_init_hydro()
     o.init_state(wpt, z)

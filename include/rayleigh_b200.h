@@ -89,6 +89,10 @@ typedef struct ra_config {
     double nu_top, kappa_top, eta_top;
     /* Controls.F90:64-65, both on by default; Constant_Reference turns both off */
     int    viscous_heating, ohmic_heating;
+    /* Numerical_Controls: 1 Chebyshev collocation (default); 0 finite differences on the
+       uniform grid (ProblemSize.F90:607-618) with the default 5-point stencils
+       (Finite_Difference.F90:464-689); the state then holds grid values */
+    int    chebyshev;
 } ra_config;
 
 /* Fills *cfg with the defaults of the reference (Controls.F90, PDE_Coefficients.F90). */

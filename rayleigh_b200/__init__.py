@@ -60,6 +60,7 @@ class _Config(ctypes.Structure):
         ("nu_power", ctypes.c_double), ("kappa_power", ctypes.c_double), ("eta_power", ctypes.c_double),
         ("nu_top", ctypes.c_double), ("kappa_top", ctypes.c_double), ("eta_top", ctypes.c_double),
         ("viscous_heating", ctypes.c_int), ("ohmic_heating", ctypes.c_int),
+        ("chebyshev", ctypes.c_int),
     ]
 
 
@@ -147,6 +148,7 @@ class Config:
     eta_top: float = -1.0
     viscous_heating: bool = True
     ohmic_heating: bool = True
+    chebyshev: bool = True           # False: the finite-difference radial mode
 
     def to_c(self):
         c = _Config()

@@ -54,8 +54,13 @@ static Dims make_dims(const ra_config& cfg) {
     d.nphi = 2 * d.nth;
     d.nr = cfg.n_r;
     d.nlm = (long)d.L * (d.L + 1) / 2;
-    d.rda = (2 * d.nr) / 3 + 1;
-    d.kc = d.rda - 1;
+    if (cfg.chebyshev) {
+        d.rda = (2 * d.nr) / 3 + 1;
+        d.kc = d.rda - 1;
+    } else {   // finite differences: no dealiasing, boundary rows over every column
+        d.rda = d.nr + 1;
+        d.kc = d.nr;
+    }
     return d;
 }
 
@@ -143,6 +148,122 @@ static void chebyshev_setup(Ctx& c, double rmin, double rmax) {
     }
 }
 
+// One stencil of Generate_Coefs (Finite_Difference.F90:525-689): the weights of derivative
+// order deriv at offsets dees (scaled by dmean) from the inverse of their Vandermonde matrix,
+// each row times (j - 1)! / dmean^(j - 1).  Gauss-Jordan with partial pivoting on the small
+// matrix (at most 5 x 5), in long double.
+static std::vector<double> fd_weights(const std::vector<double>& dees, double dmean, int deriv) {
+    const int n = (int)dees.size();
+    std::vector<long double> a((size_t)n * 2 * n, 0.0L);
+    for (int j = 0; j < n; ++j) {
+        long double p = 1.0L;
+        for (int k = 0; k < n; ++k) {
+            a[(size_t)j * 2 * n + k] = p;
+            p *= dees[j];
+        }
+        a[(size_t)j * 2 * n + n + j] = 1.0L;
+    }
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int i = col + 1; i < n; ++i)
+            if (fabsl(a[(size_t)i * 2 * n + col]) > fabsl(a[(size_t)piv * 2 * n + col])) piv = i;
+        if (a[(size_t)piv * 2 * n + col] == 0.0L) throw ArgError("finite-difference stencil is singular");
+        if (piv != col)
+            for (int k = 0; k < 2 * n; ++k) std::swap(a[(size_t)piv * 2 * n + k], a[(size_t)col * 2 * n + k]);
+        const long double inv = 1.0L / a[(size_t)col * 2 * n + col];
+        for (int k = 0; k < 2 * n; ++k) a[(size_t)col * 2 * n + k] *= inv;
+        for (int i = 0; i < n; ++i)
+            if (i != col) {
+                const long double f = a[(size_t)i * 2 * n + col];
+                if (f != 0.0L)
+                    for (int k = 0; k < 2 * n; ++k) a[(size_t)i * 2 * n + k] -= f * a[(size_t)col * 2 * n + k];
+            }
+    }
+    // row deriv of the inverse, times deriv! / dmean^deriv
+    long double fact = 1.0L;
+    for (int j = 2; j <= deriv; ++j) fact *= j;
+    const long double sc = fact / powl((long double)dmean, deriv);
+    std::vector<double> w(n);
+    for (int k = 0; k < n; ++k) w[k] = (double)(a[(size_t)deriv * 2 * n + n + k] * sc);
+    return w;
+}
+
+// Finite-difference radial mode (chebyshev = 0): the uniform grid (ProblemSize.F90:607-618),
+// the derivative matrices D_d (d = 1..3) of the default 5-point stencils with one-sided
+// boundary stencils of d + 2 points (Initialize_dcoefs and Generate_Coefs,
+// Finite_Difference.F90:464-689; the rows d_by_dx3d3 and Load_Interior_RowsFD apply,
+// :374-460, :717-777), D_0 = I, and Initialize_Derivatives' integration weights (:69-93).
+static void fd_setup(Ctx& c, double rmin, double rmax) {
+    const int n = c.d.nr, ns = 5, kd = 3, sc = 3;
+    c.rad.rmin = rmin;
+    c.rad.rmax = rmax;
+    std::vector<double>& r = c.rad.radius;
+    r.assign(n, 0.0);
+    r[n - 1] = rmin;
+    const double dr = 1.0 / (n - 1.0) * (rmax - rmin);
+    for (int i = n - 2; i >= 0; --i) r[i] = dr + r[i + 1];
+    c.rad.fd_dr = dr;
+    c.cheb_D.assign((size_t)4 * n * n, 0.0);
+    for (int i = 0; i < n; ++i) c.cheb_D[(size_t)i * n + i] = 1.0;
+    for (int dd = 1; dd <= 3; ++dd) {
+        double* D = c.cheb_D.data() + (size_t)dd * n * n;
+        // interior rows (Fortran i = 2 .. n-1): the centred stencil clipped at the ends
+        for (int i = 2; i <= n - 1; ++i) {
+            const int jstart = std::max(1, sc - i + 1), jend = std::min(ns, (n - i) + sc);
+            const int nxy = jend - jstart + 1;
+            std::vector<double> dees(nxy);
+            double dsum = 0.0;
+            for (int j = jstart; j <= jend; ++j) {
+                dees[j - jstart] = r[i + j - sc - 1] - r[i - 1];
+                dsum += fabs(dees[j - jstart]);
+            }
+            dees[sc - jstart] = 0.0;
+            const double dmean = dsum / (double)(nxy - 1);
+            for (double& v : dees) v /= dmean;
+            const std::vector<double> w = fd_weights(dees, dmean, dd);
+            for (int j = jstart; j <= jend; ++j) {   // stencil point j -> column i + j - kd (1-based)
+                const int col = i + j - kd - 1;
+                D[(size_t)(i - 1) * n + col] = w[j - jstart];
+            }
+        }
+        // the end points: one-sided stencils of dd + 2 points
+        const int nxy = dd + 2;
+        for (int side = 0; side < 2; ++side) {
+            const int pt = side ? n : 1;
+            std::vector<double> dees(nxy, 0.0);
+            double dsum = 0.0;
+            for (int j = (side ? 1 : 2); j <= (side ? nxy - 1 : nxy); ++j) {
+                dees[j - 1] = side ? r[pt + (j - nxy) - 1] - r[pt - 1] : r[pt + j - 2] - r[pt - 1];
+                dsum += dees[j - 1];
+            }
+            const double dmean = dsum / (double)(nxy - 1);
+            for (double& v : dees) v /= dmean;
+            const std::vector<double> w = fd_weights(dees, dmean, dd);
+            for (int k = 0; k < nxy; ++k) {
+                if (side) D[(size_t)(n - 1) * n + (n - nxy + k)] = w[k];
+                else D[k] = w[k];
+            }
+        }
+    }
+    // integration weights (r_{i-1} - r_{i+1}) / 2 r_i^2, one-sided at the ends, normalised
+    std::vector<double>& w = c.rad.int_w;
+    w.assign(n, 0.0);
+    for (int i = 1; i < n - 1; ++i) w[i] = (r[i - 1] - r[i + 1]) / 2.0 * r[i] * r[i];
+    w[0] = (r[0] - r[1]) / 2.0 * r[0] * r[0];
+    w[n - 1] = (r[n - 2] - r[n - 1]) / 2.0 * r[n - 1] * r[n - 1];
+    double sum = 0.0;
+    for (double v : w) sum += v;
+    for (double& v : w) v /= sum;
+    c.deriv_scaling = 1.0;
+}
+
+static void radial_setup(Ctx& c, double rmin, double rmax) {
+    if (c.cfg.chebyshev)
+        chebyshev_setup(c, rmin, rmax);
+    else
+        fd_setup(c, rmin, rmax);
+}
+
 // Reference state and transport coefficients (PDE_Coefficients.F90:216-257, 335-537, 925-1051,
 // 1766-2098): Constant_Reference (Boussinesq), Polytropic_Reference (cgs) or
 // Polytropic_ReferenceND, then Initialize_Diffusivity and Compute_Diffusion_Coefs.
@@ -155,6 +276,7 @@ static void reference_setup(Ctx& c) {
     R.delta_r.resize(n);
     R.delta_r[0] = r[0] - r[1];
     for (int i = 1; i < n; ++i) R.delta_r[i] = r[i - 1] - r[i];
+    if (!cfg.chebyshev) R.delta_r.assign(n, R.fd_dr);   // Delta_r(:) = uniform_dr (ProblemSize.F90:613)
     R.density.assign(n, 1.0);
     R.dlnrho.assign(n, 0.0);
     R.d2lnrho.assign(n, 0.0);
@@ -333,6 +455,10 @@ static void build_l_mag(const Ctx& c, int l, std::vector<double>& Cm, std::vecto
 // (Cheby_Deriv_Buffer_4D) -> dealias -> grid (From_Spectral4D), formed in long double.
 static void emf_matrix(const Ctx& c, std::vector<double>& M) {
     const int n = c.d.nr, kc = c.d.kc;
+    if (!c.cfg.chebyshev) {   // finite differences: d_by_dx of order 1 (Finalize_EMF's FD branch)
+        M.assign(c.cheb_D.begin() + (size_t)n * n, c.cheb_D.begin() + (size_t)2 * n * n);
+        return;
+    }
     std::vector<long double> T((size_t)n * n), Dr((size_t)n * n, 0.0L);
     // To_Spectral4D: c_k = (2/N) sum_r f(r) cos(k theta_r), theta_r accumulated in double as
     // Gen_Colocation_Points does (Chebyshev_Polynomials.F90:233-244)
@@ -570,6 +696,9 @@ static void autotune(Ctx& c, int nreps, double* ms_out);
 
 static void setup(Ctx& c) {
     const Dims& d = c.d;
+    if (!c.cfg.chebyshev)
+        throw ArgError("the finite-difference radial mode is provided by ra_build_matrices only (host); "
+                       "the device step takes chebyshev = 1");
     c.mag = c.cfg.magnetism != 0;
     c.mixed_solve = c.cfg.precision == RA_PREC_MIXED && c.cfg.reference_type != 2;
     c.nfa = c.mag ? (int)NP2A_MAG : (int)NP2A;
@@ -581,7 +710,7 @@ static void setup(Ctx& c) {
     c.old_dt = c.cfg.dt;
     const double rmax = c.cfg.shell_depth / (1.0 - c.cfg.aspect_ratio);
     const double rmin = rmax * c.cfg.aspect_ratio;
-    chebyshev_setup(c, rmin, rmax);
+    radial_setup(c, rmin, rmax);
     reference_setup(c);
     // horizontal grid
     std::vector<long double> xq, wq;
@@ -1258,6 +1387,7 @@ int ra_default_config(ra_config* cfg) {
     cfg->nu_type = cfg->kappa_type = cfg->eta_type = 1;
     cfg->nu_top = cfg->kappa_top = cfg->eta_top = -1.0;
     cfg->viscous_heating = cfg->ohmic_heating = 1;
+    cfg->chebyshev = 1;
     return RA_OK;
 }
 
@@ -1418,7 +1548,7 @@ int ra_build_matrices(const ra_config* cfg, int sys, int l0, int nl, double* lhs
         c.d = make_dims(*cfg);
         c.dt = cfg->dt;
         const double rmax = cfg->shell_depth / (1.0 - cfg->aspect_ratio);
-        chebyshev_setup(c, rmax * cfg->aspect_ratio, rmax);
+        radial_setup(c, rmax * cfg->aspect_ratio, rmax);
         reference_setup(c);
         const int nr = c.d.nr, n = sys ? nr : 3 * nr;
         std::vector<double> A, Z, cf((size_t)NSLOT * nr), cm((size_t)NMSLOT * nr);

@@ -82,6 +82,7 @@ struct Radial {
     std::vector<double> eta;     // magnetic diffusivity (magnetism)
     double lorentz = 0.0;        // Lorentz_Coeff
     double rmin = 0.0, rmax = 0.0;
+    double fd_dr = 0.0;          // the uniform spacing of the finite-difference grid
     // the rest of the reference state and of the transport profiles (anelastic terms)
     std::vector<double> d2lnrho, temperature, dlnT, dlnu, dlnkappa, dlneta;
     // Compute_Diffusion_Coefs (PDE_Coefficients.F90:2032-2098)

@@ -34,6 +34,10 @@ def _slots():
          poly_nrho=5.0, poly_mass=1.9e30, poly_rho_i=1.1, pressure_specific_heat=1.0509e8,
          angular_velocity=1.76e-4, nu_top=3.64364e12, kappa_top=3.64364e12, no_slip_top=False,
          no_slip_bottom=False, t_bottom=851225.7),
+    # the finite-difference radial mode (uniform grid, 5-point stencils): no-slip and stress-free
+    dict(n_r=48, l_max=7, dt=1e-4, chebyshev=False),
+    dict(n_r=32, l_max=7, dt=1e-4, chebyshev=False, no_slip_top=False, no_slip_bottom=False,
+         fix_tvar_bottom=False, dtdr_bottom=-1.0),
 ])
 def test_build_matrices_match_oracle(cfg):
     import rayleigh_b200 as rb
@@ -67,8 +71,9 @@ def test_build_matrices_argument_errors():
         rb.build_matrices(rb.Config(n_r=7, l_max=7), 0, 0, 1)
 
 
-@pytest.mark.parametrize("n_r,anelastic", [(24, False), (128, False), (32, True)])
-def test_build_magnetic_matrices_match_oracle(n_r, anelastic):
+@pytest.mark.parametrize("n_r,anelastic,chebyshev", [(24, False, True), (128, False, True), (32, True, True),
+                                                     (32, False, False)])
+def test_build_magnetic_matrices_match_oracle(n_r, anelastic, chebyshev):
     """The C (poloidal) and A (toroidal) systems of the dynamo equation set with the
     insulating (potential-field) boundary rows (Sphere_Linear_Terms.F90:473-499, 1041-1077)
     and their Post_Solve coefficients; on the polytrope with a density-dependent eta the
@@ -77,6 +82,7 @@ def test_build_magnetic_matrices_match_oracle(n_r, anelastic):
     cfg = dict(n_r=n_r, l_max=7, dt=2e-4, ekman=1e-3, rayleigh=1e5, magnetism=True, magnetic_prandtl=5.0)
     if anelastic:
         cfg.update(ANEL, n_r=n_r, magnetism=True, magnetic_prandtl=2.0, eta_type=2, eta_power=-0.5)
+    cfg["chebyshev"] = chebyshev
     o = O.Oracle(O.Config(**cfg))
     L = 8
     rc = rb.Config(**cfg)

@@ -115,7 +115,87 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
     }
 }
 
+// The finite-difference radial mode's synthesis: the state holds grid values, and every grid
+// output is one banded matrix (I, D_1, D_2, D_3 of Finite_Difference.F90, or D_1 D_1 for the
+// deriv_cluge plane) applied to a field's radial columns (d_by_dx3d3, Post_Solve_FD,
+// Sphere_Spectral_Space.F90:37-176), on the FP64 tensor-core tile engine, all outputs in one
+// launch (grid z = output).
+struct FdOuts {
+    int n;
+    int o[NG_MAG + 1], var[NG_MAG + 1], mat[NG_MAG + 1];
+};
+
+__global__ void __launch_bounds__(GEMM_THREADS) fd_synthesis_kernel(const double* __restrict__ Dfd,
+                                                                    const double* __restrict__ sol_wpt,
+                                                                    const double* __restrict__ sol_z,
+                                                                    const double* __restrict__ sol_c,
+                                                                    const double* __restrict__ sol_a,
+                                                                    double* __restrict__ g, int nr, long ncols,
+                                                                    FdOuts outs) {
+    __shared__ GemmSmem sm;
+    const int oi = blockIdx.z;
+    const int var = outs.var[oi];
+    const double* src;
+    long cstride;
+    if (var < 3) {
+        src = sol_wpt + (long)var * nr;
+        cstride = 3L * nr;
+    } else {
+        src = var == 3 ? sol_z : (var == 4 ? sol_c : sol_a);
+        cstride = nr;
+    }
+    const double* M = Dfd + (long)outs.mat[oi] * nr * nr;
+    double* out = g + (long)outs.o[oi] * ncols * nr;
+    const int r0 = blockIdx.y * Sq::BM;
+    const long c0 = (long)blockIdx.x * Sq::BN;
+    auto fa = [&](int k, int x) -> double {   // M(r0 + x, k)
+        const int rr = r0 + x;
+        return (k < nr && rr < nr) ? __ldg(M + (long)rr * nr + k) : 0.0;
+    };
+    auto fb = [&](int k, int y) -> double {   // the field's value at radius k of column c0 + y
+        const long col = c0 + y;
+        return (k < nr && col < ncols) ? __ldg(src + col * cstride + k) : 0.0;
+    };
+    Acc acc;
+    acc.zero();
+    gemm_tile<false, false>(acc, fa, fb, nr, sm);
+    acc_foreach(acc, [&](int x, int y, double v) {
+        const int rr = r0 + x;
+        const long col = c0 + y;
+        if (rr < nr && col < ncols) out[col * nr + rr] = v;
+    });
+}
+
+static void launch_fd_synthesis(Ctx& c) {
+    const long ncols = 2 * c.d.nlm;
+    FdOuts outs{};
+    auto add = [&](int o, int var, int mat) {
+        outs.o[outs.n] = o;
+        outs.var[outs.n] = var;
+        outs.mat[outs.n] = mat;
+        ++outs.n;
+    };
+    for (int d = 0; d < 4; ++d) add(G_W0 + d, 0, d);
+    for (int d = 0; d < 2; ++d) add(G_P0 + d, 1, d);
+    for (int d = 0; d < 3; ++d) add(G_T0 + d, 2, d);
+    for (int d = 0; d < 3; ++d) add(G_Z0 + d, 3, d);
+    if (c.mag) {
+        for (int d = 0; d < 3; ++d) add(G_C0 + d, 4, d);
+        for (int d = 0; d < 3; ++d) add(G_A0 + d, 5, d);
+    }
+    add(c.ng, 0, 4);   // the deriv_cluge plane: D_1 D_1 W
+    dim3 grid((unsigned)((ncols + Sq::BN - 1) / Sq::BN), (unsigned)((c.d.nr + Sq::BM - 1) / Sq::BM), outs.n);
+    fd_synthesis_kernel<<<grid, GEMM_THREADS, 0, c.stream>>>(c.d_Dfd, c.d_sol_wpt, c.d_sol_z, c.d_sol_c, c.d_sol_a,
+                                                             c.d_g, c.d.nr, ncols, outs);
+    RA_CUDA(cudaGetLastError());
+    ++c.launches;
+}
+
 void launch_cheb_synthesis(Ctx& c) {
+    if (!c.cfg.chebyshev) {
+        launch_fd_synthesis(c);
+        return;
+    }
     const long ncols = 2 * c.d.nlm;
     const size_t smem = sizeof(ChebSmem);
     // the limit is per device: set it on every launch (a host-side call, also legal during capture)
@@ -144,10 +224,12 @@ __host__ __device__ constexpr int slot_g(int s) {
 }
 static_assert(slot_eq(3) == kSlots[3].eq && slot_g(8) == kSlots[8].g && slot_g(15) == kSlots[15].g, "slot table");
 
+// w2s (finite-difference mode only, else NULL): the plane of d/dr (dW/dr) that Post_Solve_FD's
+// deriv_cluge sends on to rlm_spacea in place of d2W/dr2 (Sphere_Spectral_Space.F90:96-98).
 __global__ void post_assemble_kernel(const double* __restrict__ g, const double* __restrict__ ab,
                                      const double* __restrict__ coef, double* __restrict__ rhs_wpt,
                                      double* __restrict__ rhs_z, double* __restrict__ s2a, long nlm, int nr,
-                                     int L, double old_ab) {
+                                     int L, double old_ab, const double* __restrict__ w2s) {
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (lm, r), r fastest; both re/im
     if (idx >= nlm * nr) return;
     const int r = (int)(idx % nr);
@@ -189,14 +271,17 @@ __global__ void post_assemble_kernel(const double* __restrict__ g, const double*
     const long fs = 2L * nr;
     constexpr int kOut[NS2A] = {G_W0, G_T0, G_Z0, G_W1, G_T1, G_Z1, G_W2};
 #pragma unroll
-    for (int f = 0; f < NS2A; ++f)
+    for (int f = 0; f < NS2A - 1; ++f)
         *reinterpret_cast<double2*>(o + f * fs) = make_double2(gv[kOut[f]][0], gv[kOut[f]][1]);
+    const double2 w2 = w2s ? make_double2(w2s[i0], w2s[i0 + nr]) : make_double2(gv[G_W2][0], gv[G_W2][1]);
+    *reinterpret_cast<double2*>(o + (NS2A - 1) * fs) = w2;
 }
 
 void launch_post_assemble(Ctx& c, double old_ab) {
     const long total = c.d.nlm * c.d.nr;
+    const double* w2s = c.cfg.chebyshev ? nullptr : c.d_g + (size_t)c.ng * c.d.nlm * 2 * c.d.nr;
     post_assemble_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
-        c.d_g, c.d_ab, c.d_coef, c.d_rhs_wpt, c.d_rhs_z, c.d_s2a, c.d.nlm, c.d.nr, c.d.L, old_ab);
+        c.d_g, c.d_ab, c.d_coef, c.d_rhs_wpt, c.d_rhs_z, c.d_s2a, c.d.nlm, c.d.nr, c.d.L, old_ab, w2s);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }

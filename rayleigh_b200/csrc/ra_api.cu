@@ -696,11 +696,8 @@ static void autotune(Ctx& c, int nreps, double* ms_out);
 
 static void setup(Ctx& c) {
     const Dims& d = c.d;
-    if (!c.cfg.chebyshev)
-        throw ArgError("the finite-difference radial mode is provided by ra_build_matrices only (host); "
-                       "the device step takes chebyshev = 1");
     c.mag = c.cfg.magnetism != 0;
-    c.mixed_solve = c.cfg.precision == RA_PREC_MIXED && c.cfg.reference_type != 2;
+    c.mixed_solve = c.cfg.precision == RA_PREC_MIXED && c.cfg.reference_type != 2 && c.cfg.chebyshev;
     c.nfa = c.mag ? (int)NP2A_MAG : (int)NP2A;
     c.nfb = c.mag ? (int)NP2B_MAG : (int)NP2B;
     c.ng = c.mag ? (int)NG_MAG : (int)NG;
@@ -783,7 +780,8 @@ static void setup(Ctx& c) {
     dalloc(c.d_rhs_z, (size_t)nlm * 2 * nr);
     const int nab = c.mag ? 6 : 4;   // AB history: W P T Z (C A)
     dalloc(c.d_ab, (size_t)nab * nlm * 2 * nr);
-    dalloc(c.d_g, (size_t)c.ng * nlm * 2 * nr);
+    // grids; the finite-difference mode adds the deriv_cluge plane behind them
+    dalloc(c.d_g, (size_t)(c.ng + (c.cfg.chebyshev ? 0 : 1)) * nlm * 2 * nr);
     dalloc(c.d_s2a, (size_t)nlm * NS2A * 2 * nr);
     dalloc(c.d_s2a11, (size_t)nlm * c.nfa * 2 * nr);
     dalloc(c.d_p2a, (size_t)d.L * d.nth * c.nfa * 2 * nr);
@@ -845,6 +843,22 @@ static void setup(Ctx& c) {
         RA_CUDA(cudaMemcpyAsync(c.d_Dpar, dp.data(), dp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
     }
+    if (!c.cfg.chebyshev) {
+        // the finite-difference synthesis matrices [I, D_1, D_2, D_3, D_1 D_1]
+        const size_t nn = (size_t)nr * nr;
+        std::vector<double> fdm(5 * nn, 0.0);
+        std::copy(c.cheb_D.begin(), c.cheb_D.begin() + 4 * nn, fdm.begin());
+        const double* D1 = c.cheb_D.data() + nn;
+        for (int i = 0; i < nr; ++i)
+            for (int j = 0; j < nr; ++j) {
+                long double s = 0.0L;
+                for (int k = 0; k < nr; ++k) s += (long double)D1[(size_t)i * nr + k] * D1[(size_t)k * nr + j];
+                fdm[4 * nn + (size_t)i * nr + j] = (double)s;
+            }
+        dalloc(c.d_Dfd, fdm.size());
+        RA_CUDA(cudaMemcpyAsync(c.d_Dfd, fdm.data(), fdm.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        RA_CUDA(cudaStreamSynchronize(c.stream));
+    }
     RA_CUDA(cudaMemcpyAsync(c.d_radial, rp.data(), rp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_costh, trig.data(), trig.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     RA_CUDA(cudaMemcpyAsync(c.d_twid, twid.data(), twid.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
@@ -874,7 +888,7 @@ static void release(Ctx& c) {
     if (c.d_adapt) cudaFree(c.d_adapt);
     if (c.d_adapt_dt) cudaFree(c.d_adapt_dt);
     lu_workspace_free(c.lu_work);
-    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp,
+    double* bufs[] = {c.d_Ptab, c.d_iPtab, c.d_D, c.d_Dpar, c.d_Dfd, c.d_coef, c.d_radial, c.d_costh, c.d_twid, c.d_twp,
                       c.d_Awpt, c.d_Az,
                       c.d_Ainv_wpt, c.d_Ainv_z,
                       c.d_sol_wpt, c.d_sol_z, c.d_rhs_wpt, c.d_rhs_z, c.d_ab, c.d_g, c.d_s2a, c.d_s2a11,
@@ -2450,6 +2464,9 @@ static int cheb_op(ra_ctx* ctx, const double* in, double* out, long ncols, int m
     if (mode == 2 && (order < 1 || order > 3)) return RA_ERR_ARG;
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
+        if (!c.cfg.chebyshev)
+            throw StateError("the Chebyshev operators need a context with chebyshev = 1 (finite differences hold "
+                             "grid values: to_spectral and from_spectral are the identity)");
         const size_t n = (size_t)ncols * c.d.nr;
         double *di = nullptr, *dout = nullptr;
         dalloc(di, n);

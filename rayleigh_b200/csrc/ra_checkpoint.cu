@@ -167,7 +167,8 @@ int ra_write_checkpoint(ra_ctx* ctx, const char* dir, double elapsed_time) {
         const unsigned char* b = static_cast<const unsigned char*>(p);
         g.insert(g.end(), b, b + n);
     };
-    const int32_t tag = 314, version = 2, n_r32 = nr, grid_type = 2, l_max32 = lmax;
+    // grid_type 2: Chebyshev, 1: finite differences (ProblemSize.F90:60, 537)
+    const int32_t tag = 314, version = 2, n_r32 = nr, grid_type = c.cfg.chebyshev ? 2 : 1, l_max32 = lmax;
     const int32_t iter = c.iteration - 1;   // the last completed step
     const double dt = c.old_dt, new_dt = c.dt;
     put(&tag, 4);
@@ -207,7 +208,7 @@ int ra_read_checkpoint(ra_ctx* ctx, const char* dir, int* iteration, double* ela
     bool ok = get(&version, 4) && get(&n_r_old, 4) && get(&grid_type, 4) && get(&l_max_old, 4) && get(&dt, 8) &&
               get(&new_dt, 8);
     if (!ok || version != 2) return last_err(ctx, "grid_etc: not a version-2 checkpoint", RA_ERR_ARG);
-    if (n_r_old != nr || l_max_old != lmax || grid_type != 2)
+    if (n_r_old != nr || l_max_old != lmax || grid_type != (c.cfg.chebyshev ? 2 : 1))
         return last_err(ctx, "checkpoint grid (n_r " + std::to_string(n_r_old) + ", l_max " +
                                  std::to_string(l_max_old) + ", grid_type " + std::to_string(grid_type) +
                                  ") differs from the context's; interpolation is not provided", RA_ERR_ARG);

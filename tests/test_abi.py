@@ -86,7 +86,7 @@ def test_reference_state_arguments_are_checked():
     for kw, word in ((dict(reference_type=4), b"reference_type"), (dict(reference_type=3), b"poly"),
                      (dict(reference_type=3, poly_n=2.0, poly_nrho=5.0), b"modified_rayleigh"),
                      (dict(reference_type=2, poly_n=2.0, poly_nrho=5.0), b"poly_mass"),
-                     (dict(nu_type=3), b"transport"), (dict(chebyshev=False), b"finite-difference")):
+                     (dict(nu_type=3), b"transport")):
         cfg = rb.Config(**kw).to_c()
         h = ctypes.c_void_p()
         assert lib.ra_create(ctypes.byref(h), ctypes.byref(cfg)) == rb.RA_ERR_ARG, kw

@@ -12,7 +12,8 @@ the point observations are the oracle's restatement of Point_Observations run
 on v_r, v_phi and T shell slices formed on the device (ra_shell_slices), as the
 host side of the benchmark would; both are checked against the oracle's step
 on the way.  Both precision forms must reproduce the reference's report to its
-6 printed decimals."""
+6 printed decimals, for the Chebyshev run and for tests/c2001_case0_FD_uniform, the same
+run in the finite-difference radial mode (uniform grid, chebyshev = .false.)."""
 import dataclasses
 import json
 import os
@@ -25,13 +26,14 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("report", ["c2001_case0.json", "c2001_case0_fd_uniform.json"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_c2001_case0_reproduces_the_reference_report(precision):
+def test_c2001_case0_reproduces_the_reference_report(precision, report):
     import rayleigh_b200 as rb
     from rayleigh_b200 import build as rbuild
     rbuild.build()
-    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c2001_case0.json")))
-    ocfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"])
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", report)))
+    ocfg = O.c2001_case0_config(gold["n_r"], gold["n_theta"], chebyshev=gold.get("chebyshev", True))
     o = O.Oracle(ocfg)
     wpt, z = o.benchmark_init_hydro()
     names = {f.name for f in dataclasses.fields(rb.Config)}

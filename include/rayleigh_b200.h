@@ -202,13 +202,13 @@ int ra_get_magnetic_state(ra_ctx* ctx, double* c, double* a, double* ab);
 /* Checkpoint files in the reference's format (Write_Checkpoint / Read_Checkpoint,
  * Checkpointing.F90:143-801, version 2): a directory holding one file per field
  * (W P T Z, C A with magnetism, their AB terms WAB ..., boundary_conditions) and
- * grid_etc (endian tag 314, version, n_r, grid type, l_max, dt, new_dt, radius,
- * elapsed time, iteration).  A field file is n_r (l_max+1)(l_max+2) float64: the
+ * grid_etc (endian tag 314, version, n_r, grid type: 2 Chebyshev, 1 finite differences,
+ * l_max, dt, new_dt, radius, elapsed time, iteration).  A field file is n_r (l_max+1)(l_max+2) float64: the
  * real parts, then the imaginary parts, one chunk per radial index, each chunk
  * the (l, m) pairs m-major with l fastest.  ra_write_checkpoint writes the
  * context's state (its last completed iteration, the last and the next dt)
  * into dir (created if missing); ra_read_checkpoint puts a checkpoint of the
- * same grid (no interpolation: RA_ERR_ARG otherwise) into the context, rebuilds
+ * same grid and grid type (no interpolation: RA_ERR_ARG otherwise) into the context, rebuilds
  * the implicit matrices if its next dt differs, and continues from the
  * following iteration.  The field helpers convert one field between the state
  * layout (n_r, 2, n_lm) and a file; they use no device. */
@@ -392,7 +392,8 @@ int ra_transform_dev(ra_ctx* ctx, int direction, int precision, double* d_spec, 
 int ra_fft_r2c(ra_ctx* ctx, double* x, long howmany);
 
 /* Chebyshev_Polynomials.F90: To_Spectral4D (:375), From_Spectral4D (:450) and
- * Cheby_Deriv_Buffer_4D (:560) of order 1..3 on columns f(n_r, ncols). */
+ * Cheby_Deriv_Buffer_4D (:560) of order 1..3 on columns f(n_r, ncols).  A context
+ * in the finite-difference mode returns RA_ERR_STATE. */
 int ra_cheby_to_spectral(ra_ctx* ctx, const double* f, double* c, long ncols);
 int ra_cheby_from_spectral(ra_ctx* ctx, const double* c, double* f, long ncols);
 int ra_cheby_deriv(ra_ctx* ctx, const double* c, double* dc, int order, long ncols);

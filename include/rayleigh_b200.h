@@ -283,6 +283,9 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_B_R          801   /* magnetism only (magnetic_field_codes.F) */
 #define RA_Q_B_THETA      802
 #define RA_Q_B_PHI        803
+#define RA_Q_J_R         1001   /* magnetism only: the current density curl B (current_density_codes.F) */
+#define RA_Q_J_THETA     1004
+#define RA_Q_J_PHI       1007
 /* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);

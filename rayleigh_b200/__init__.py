@@ -500,7 +500,8 @@ class Rayleigh:
     QUANTITIES = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
                   "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 301, "entropy": 501,
                   "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519, "pressure": 502,
-                  "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802, "b_phi": 803}
+                  "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802, "b_phi": 803,
+                  "j_r": 1001, "j_theta": 1004, "j_phi": 1007}
 
     def shell_slices(self, quantities, levels):
         """Shell slices of the current state: array [quantity][level][theta][phi] of the

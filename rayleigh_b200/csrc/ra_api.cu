@@ -1961,7 +1961,9 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
 // as (dv_phi/dtheta + cot v_phi - csc dv_theta/dphi) / r, is the spectral
 // l(l+1) Z / r^2 here: the same band-limited field, equal up to rounding.
 // With magnetism, magnetic_field_codes.F (boffset = 800): B_r, B_theta, B_phi, the last two
-// formed from the r sin(theta) B_theta, B_phi fields the step transforms (rsintheta_div).
+// formed from the r sin(theta) B_theta, B_phi fields the step transforms (rsintheta_div), and
+// current_density_codes.F (joffset = boffset + 200): J_r, J_theta, J_phi, the curl of B as
+// Compute_J_Components reads it (Diagnostics_Current_Density.F90), the last two likewise.
 struct QuantitySource { int code, field, dphi, csc, pressure, orad; };
 static const QuantitySource kQuantities[] = {
     {1, A_VR, 0, 0, 0, 0},     {2, A_VT, 0, 1, 0, 0},     {3, A_VP, 0, 1, 0, 0},     {10, A_DVRDR, 0, 0, 0, 0},
@@ -1973,6 +1975,7 @@ static const QuantitySource kQuantities[] = {
     {508, A_DTDR, 0, 0, 1, 0}, // d pressure / dr, in dT/dr's place
     {520, A_T, 1, 0, 1, 0},    // d pressure / d phi
     {801, A_BR, 0, 0, 0, 0},   {802, A_BT, 0, 1, 0, 1},   {803, A_BP, 0, 1, 0, 1},
+    {1001, A_CBR, 0, 0, 0, 0}, {1004, A_CBT, 0, 1, 0, 1}, {1007, A_CBP, 0, 1, 0, 1},
 };
 
 static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {

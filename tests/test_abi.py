@@ -99,7 +99,8 @@ def test_reference_state_arguments_are_checked():
 def test_diagnostic_quantity_codes_are_the_references():
     """RA_Q_* in the header, the Python names and the reference's output codes
     (velocity_field_codes.F: voffset = 0; vorticity_field_codes.F: vort_off = 300;
-    thermal_field_codes.F: pt_off = 500; magnetic_field_codes.F: boffset = teoffset + 100 = 800)
+    thermal_field_codes.F: pt_off = 500; magnetic_field_codes.F: boffset = teoffset + 100 = 800;
+    current_density_codes.F: joffset = boffset + 200)
     agree; context-less diagnostic calls report a state error."""
     import rayleigh_b200 as rb
     src = open(os.path.join(ROOT, "include", "rayleigh_b200.h")).read()
@@ -109,7 +110,8 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 300 + 1,
                  "entropy": 500 + 1, "entropy_dr": 500 + 7, "entropy_dtheta": 500 + 13, "entropy_dphi": 500 + 19,
                  "pressure": 500 + 2, "pressure_dr": 500 + 8, "pressure_dphi": 500 + 20,
-                 "b_r": 800 + 1, "b_theta": 800 + 2, "b_phi": 800 + 3}
+                 "b_r": 800 + 1, "b_theta": 800 + 2, "b_phi": 800 + 3,
+                 "j_r": 800 + 200 + 1, "j_theta": 800 + 200 + 4, "j_phi": 800 + 200 + 7}
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()

@@ -92,7 +92,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     levels = [(7 * i) % oc.n_r for i in range(70)]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -125,7 +125,7 @@ def test_shell_averages_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
@@ -155,7 +155,7 @@ def test_azimuthal_averages_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
@@ -182,7 +182,7 @@ def test_shell_spectra_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     levels = [(5 * i + 1) % oc.n_r for i in range(30)]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -210,7 +210,7 @@ def test_equatorial_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
@@ -239,7 +239,7 @@ def test_meridional_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         phis = [(13 * i + 3) % g.n_phi for i in range(70)]
         g.put_state(wpt, z, None, iteration=1)
@@ -269,7 +269,7 @@ def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith("b_")]   # the hydrodynamic quantities
+    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
     ri, ti, pi = [0, 5, 11, 12, 23], [0, 3, 23, 24, 40, 46, 47], [0, 1, 17, 40, 41, 63, 64, 80, 95]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -292,3 +292,51 @@ def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
         e_pp = np.abs(pp[i] - ref).max() / scale
         print(precision, name, e_ga, e_pp)
         assert e_ga < tol and e_pp < tol, (name, e_ga, e_pp)
+
+
+# the oracle's physical-space buffer names of the magnetic quantities (after rsintheta_div)
+_ORACLE_MAG = {"b_r": "br", "b_theta": "bt", "b_phi": "bp", "j_r": "curlbr", "j_theta": "curlbt", "j_phi": "curlbp"}
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
+def test_magnetic_quantities_match_the_oracle(precision, tol):
+    """B (magnetic_field_codes.F) and the current density J = curl B (current_density_codes.F,
+    Compute_J_Components) of a dynamo state: shell slices at 30 levels (relative L2),
+    azimuthal averages and shell means (on the quantity's largest magnitude) against the
+    oracle's physical-space buffer; a hydrodynamic context refuses them (RA_ERR_ARG)."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, magnetism=True, magnetic_prandtl=5.0,
+               precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    c, a = O.seeded_magnetic_state(oc, amp=1e-1, lmax_pert=10)
+    names = list(_ORACLE_MAG)
+    levels = [(5 * i) % oc.n_r for i in range(30)]
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.put_magnetic_state(c, a)
+        g.step(3)
+        sl = g.shell_slices(names, levels)
+        az = g.azimuthal_averages(names)
+        av = g.shell_averages(names)
+        sw, sz, sab = g.get_state()
+        sc, sa, sabm = g.get_magnetic_state()
+    o = O.Oracle(oc)
+    o.init_state(sw, sz, np.concatenate([sab, sabm]), c_coeffs=sc, a_coeffs=sa)
+    o.step()   # its physical-space stage sees the state after 3 steps
+    ref_av = o.shell_averages([_ORACLE_MAG[n] for n in names])
+    for i, name in enumerate(names):
+        q = o.last_fields[_ORACLE_MAG[name]]           # [theta, r, phi]
+        scale = np.abs(q).max()
+        ref = q[:, levels, :].transpose(1, 0, 2)
+        e_sl = np.linalg.norm(sl[i] - ref) / np.linalg.norm(ref)
+        e_az = np.abs(az[i] - q.mean(axis=2)).max() / scale
+        e_av = np.abs(av[i, 0] - ref_av[i, 0]).max() / scale
+        print(precision, name, e_sl, e_az, e_av)
+        assert e_sl < tol and e_az < tol and e_av < tol, (name, e_sl, e_az, e_av)
+    hydro = dict(cfg, magnetism=False)
+    with _ctx(hydro) as h:
+        h.put_state(wpt, z, None, iteration=1)
+        with pytest.raises(rb.RayleighError) as ei:
+            h.shell_slices(["j_r"], [0])
+        assert ei.value.code == rb.RA_ERR_ARG

@@ -286,6 +286,56 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_J_R         1001   /* magnetism only: the current density curl B (current_density_codes.F) */
 #define RA_Q_J_THETA     1004
 #define RA_Q_J_PHI       1007
+/* The fluctuating part (the field minus its azimuthal mean: m > 0) and the azimuthal mean
+ * (m = 0) of each quantity above, under the reference's codes: */
+#define RA_Q_VP_R           4
+#define RA_Q_VP_THETA       5
+#define RA_Q_VP_PHI         6
+#define RA_Q_VM_R           7
+#define RA_Q_VM_THETA       8
+#define RA_Q_VM_PHI         9
+#define RA_Q_DVP_R_DR      13
+#define RA_Q_DVP_THETA_DR  14
+#define RA_Q_DVP_PHI_DR    15
+#define RA_Q_DVM_R_DR      16
+#define RA_Q_DVM_THETA_DR  17
+#define RA_Q_DVM_PHI_DR    18
+#define RA_Q_DVP_R_DT      22
+#define RA_Q_DVM_R_DT      25
+#define RA_Q_DVP_R_DP      31
+#define RA_Q_DVP_THETA_DP  32
+#define RA_Q_DVP_PHI_DP    33
+#define RA_Q_DVM_R_DP      34   /* the mean of a phi derivative: zero */
+#define RA_Q_DVM_THETA_DP  35
+#define RA_Q_DVM_PHI_DP    36
+#define RA_Q_VORTP_R      304
+#define RA_Q_VORTM_R      307
+#define RA_Q_ENTROPY_P    503
+#define RA_Q_PRESSURE_P   504
+#define RA_Q_ENTROPY_M    505
+#define RA_Q_PRESSURE_M   506
+#define RA_Q_ENTROPY_P_DR 509
+#define RA_Q_PRESSURE_P_DR 510
+#define RA_Q_ENTROPY_M_DR 511
+#define RA_Q_PRESSURE_M_DR 512
+#define RA_Q_ENTROPY_P_DTHETA 515
+#define RA_Q_ENTROPY_M_DTHETA 517
+#define RA_Q_ENTROPY_P_DPHI 521
+#define RA_Q_PRESSURE_P_DPHI 522
+#define RA_Q_ENTROPY_M_DPHI 523
+#define RA_Q_PRESSURE_M_DPHI 524
+#define RA_Q_BP_R         804
+#define RA_Q_BP_THETA     805
+#define RA_Q_BP_PHI       806
+#define RA_Q_BM_R         807
+#define RA_Q_BM_THETA     808
+#define RA_Q_BM_PHI       809
+#define RA_Q_JP_R        1002
+#define RA_Q_JM_R        1003
+#define RA_Q_JP_THETA    1005
+#define RA_Q_JM_THETA    1006
+#define RA_Q_JP_PHI      1008
+#define RA_Q_JM_PHI      1009
 /* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);

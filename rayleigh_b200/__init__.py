@@ -501,7 +501,18 @@ class Rayleigh:
                   "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 301, "entropy": 501,
                   "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519, "pressure": 502,
                   "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802, "b_phi": 803,
-                  "j_r": 1001, "j_theta": 1004, "j_phi": 1007}
+                  "j_r": 1001, "j_theta": 1004, "j_phi": 1007,
+                  # fluctuating (m > 0) and azimuthal-mean (m = 0) parts, the reference's codes
+                  "vp_r": 4, "vp_theta": 5, "vp_phi": 6, "vm_r": 7, "vm_theta": 8, "vm_phi": 9,
+                  "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
+                  "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
+                  "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36, "vortp_r": 304,
+                  "vortm_r": 307, "entropy_p": 503, "pressure_p": 504, "entropy_m": 505, "pressure_m": 506,
+                  "entropy_p_dr": 509, "pressure_p_dr": 510, "entropy_m_dr": 511, "pressure_m_dr": 512,
+                  "entropy_p_dtheta": 515, "entropy_m_dtheta": 517, "entropy_p_dphi": 521,
+                  "pressure_p_dphi": 522, "entropy_m_dphi": 523, "pressure_m_dphi": 524,
+                  "bp_r": 804, "bp_theta": 805, "bp_phi": 806, "bm_r": 807, "bm_theta": 808, "bm_phi": 809,
+                  "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005, "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009}
 
     def shell_slices(self, quantities, levels):
         """Shell slices of the current state: array [quantity][level][theta][phi] of the

@@ -432,9 +432,10 @@ __device__ __forceinline__ void fft_dit(double2* buf, const double2* twp, int ti
 // h = 1), as StP_4d_dgp2 reflects the even-l / odd-l products
 // (Legendre_Transforms.F90:1030-1064); d/dphi (i m X) when dp; Im X_0 = 0 as
 // FFTW's c2r ignores it; X_m = 0 for m >= L.
+// mpart (diagnostics): 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean (m = 0)
 __device__ __forceinline__ double2 spec_value(const double* __restrict__ base, long mstride, long ostride, int m,
-                                              int L, int h, bool dp) {
-    if (m >= L) return make_double2(0.0, 0.0);
+                                              int L, int h, bool dp, int mpart = 0) {
+    if (m >= L || (mpart == 1 && m == 0) || (mpart == 2 && m != 0)) return make_double2(0.0, 0.0);
     const double2 e = __ldg(reinterpret_cast<const double2*>(base + m * mstride));
     const double2 o = __ldg(reinterpret_cast<const double2*>(base + m * mstride + ostride));
     double2 x = h ? csub(e, o) : cadd(e, o);
@@ -462,14 +463,14 @@ __device__ __forceinline__ T pick(const T (&a)[NB], int b) {
     return v;
 }
 
-// c2r of NB fields of this row (fields fo[b], d/dphi where dp[b]): the input
-// Z is formed straight from the spectrum loads (one (k, N-k) pair per work
-// item), then the DIF passes.  On return y[b][q] holds the physical pair
+// c2r of NB fields of this row (fields fo[b], d/dphi where dp[b]; mpart as in spec_value,
+// 0 in the time step): the input Z is formed straight from the spectrum loads (one (k, N-k)
+// pair per work item), then the DIF passes.  On return y[b][q] holds the physical pair
 // (y[2n], y[2n+1]) of field b at the buffer position t + q*ROW_THREADS.
 template <int N, int NB, int ZPT>
 __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __restrict__ rowbase, int h,
                                         const int (&fo)[NB], const bool (&dp)[NB], double2* sm, int t,
-                                        double2 (&y)[FB][ZPT]) {
+                                        double2 (&y)[FB][ZPT], int mpart = 0) {
     constexpr int FS = fstride(N);
     constexpr int NI = N / 2 + 1;                                   // k = 0 .. N/2
     constexpr int QI = (NB * NI + ROW_THREADS - 1) / ROW_THREADS;   // items per thread
@@ -505,8 +506,8 @@ __device__ __forceinline__ void row_c2r(const PhysParams& P, const double* __res
                 item(g, k, b);
                 const double* base = rowbase + (long)pick(fo, b) * 2;
                 const bool d = pick(dp, b);
-                xk[qq] = spec_value(base, mstride, ostride, k, L, h, d);
-                xn[qq] = spec_value(base, mstride, ostride, N - k, L, h, d);   // N - k >= L for k = 0
+                xk[qq] = spec_value(base, mstride, ostride, k, L, h, d, mpart);
+                xn[qq] = spec_value(base, mstride, ostride, N - k, L, h, d, mpart);   // N - k >= L for k = 0
             }
         }
 #pragma unroll
@@ -1590,7 +1591,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_slice_kernel(PhysParams P, 
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     double2* row = reinterpret_cast<double2*>(out + ((long)lv * N + th) * (2L * N));
 #pragma unroll
@@ -1664,7 +1665,7 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_moment_rows_kernel(PhysPara
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     const double mu = MOMENTS ? mean[r] : 0.0;
     double s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -1837,7 +1838,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
@@ -1962,7 +1963,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
@@ -2039,7 +2040,7 @@ __global__ void __launch_bounds__(ROW_THREADS) meridional_slice_kernel(PhysParam
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll
@@ -2167,7 +2168,7 @@ __global__ void __launch_bounds__(ROW_THREADS) point_probe_kernel(PhysParams P, 
     const int fo[1] = {S.field};
     const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y);
+    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
     const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll

@@ -1978,12 +1978,32 @@ static const QuantitySource kQuantities[] = {
     {1001, A_CBR, 0, 0, 0, 0}, {1004, A_CBT, 0, 1, 0, 1}, {1007, A_CBP, 0, 1, 0, 1},
 };
 
+// The fluctuating (m > 0) and azimuthal-mean (m = 0) codes of each quantity above, as the
+// reference numbers them (velocity_field_codes.F: vp_r = v_r + 3, vm_r = v_r + 6, ...;
+// thermal_field_codes.F: entropy_p = entropy + 2, entropy_m = entropy + 4, ...;
+// vorticity_field_codes.F, magnetic_field_codes.F; current_density_codes.F: jp_r = j_r + 1,
+// jm_r = j_r + 2).  Diagnostics_Base forms them from the buffer minus, or as, its phi average
+// (fbuffer, m0_values); here the m = 0 term of the spectrum is dropped or kept alone.
+struct QuantityParts { int full, fluct, mean; };
+static const QuantityParts kParts[] = {
+    {1, 4, 7},          {2, 5, 8},          {3, 6, 9},          {10, 13, 16},       {11, 14, 17},
+    {12, 15, 18},       {19, 22, 25},       {28, 31, 34},       {29, 32, 35},       {30, 33, 36},
+    {301, 304, 307},    {501, 503, 505},    {502, 504, 506},    {507, 509, 511},    {508, 510, 512},
+    {513, 515, 517},    {519, 521, 523},    {520, 522, 524},    {801, 804, 807},    {802, 805, 808},
+    {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009},
+};
+
 static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {
     std::vector<SliceSpec> spec(nq);
     for (int q = 0; q < nq; ++q) {
+        int code = quantities[q], mpart = 0;
+        for (const QuantityParts& p : kParts) {
+            if (p.fluct == code) { code = p.full; mpart = 1; break; }
+            if (p.mean == code) { code = p.full; mpart = 2; break; }
+        }
         const QuantitySource* src = nullptr;
         for (const QuantitySource& k : kQuantities)
-            if (k.code == quantities[q]) src = &k;
+            if (k.code == code) src = &k;
         if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " is not provided");
         if (src->field >= c.nfa)
             throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
@@ -1995,6 +2015,7 @@ static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities
         spec[q].csc = src->csc;
         spec[q].pressure = src->pressure;
         spec[q].orad = src->orad;
+        spec[q].mpart = mpart;
     }
     return spec;
 }

@@ -258,6 +258,7 @@ struct SliceSpec {
     int field, dphi, csc, nl;   // p2a field, d/dphi, times 1/sin(theta), levels in this launch
     int pressure;               // formed with the P grid in T's place (pressure quantities)
     int orad;                   // times 1/r (the r sin(theta) B_theta, B_phi fields)
+    int mpart;                  // 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);

@@ -111,7 +111,20 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "entropy": 500 + 1, "entropy_dr": 500 + 7, "entropy_dtheta": 500 + 13, "entropy_dphi": 500 + 19,
                  "pressure": 500 + 2, "pressure_dr": 500 + 8, "pressure_dphi": 500 + 20,
                  "b_r": 800 + 1, "b_theta": 800 + 2, "b_phi": 800 + 3,
-                 "j_r": 800 + 200 + 1, "j_theta": 800 + 200 + 4, "j_phi": 800 + 200 + 7}
+                 "j_r": 800 + 200 + 1, "j_theta": 800 + 200 + 4, "j_phi": 800 + 200 + 7,
+                 "vp_r": 4, "vp_theta": 5, "vp_phi": 6, "vm_r": 7, "vm_theta": 8, "vm_phi": 9,
+                 "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
+                 "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
+                 "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36,
+                 "vortp_r": 300 + 4, "vortm_r": 300 + 7,
+                 "entropy_p": 500 + 3, "pressure_p": 500 + 4, "entropy_m": 500 + 5, "pressure_m": 500 + 6,
+                 "entropy_p_dr": 500 + 9, "pressure_p_dr": 500 + 10, "entropy_m_dr": 500 + 11,
+                 "pressure_m_dr": 500 + 12, "entropy_p_dtheta": 500 + 15, "entropy_m_dtheta": 500 + 17,
+                 "entropy_p_dphi": 500 + 21, "pressure_p_dphi": 500 + 22, "entropy_m_dphi": 500 + 23,
+                 "pressure_m_dphi": 500 + 24,
+                 "bp_r": 800 + 4, "bp_theta": 800 + 5, "bp_phi": 800 + 6, "bm_r": 800 + 7, "bm_theta": 800 + 8,
+                 "bm_phi": 800 + 9, "jp_r": 1000 + 2, "jm_r": 1000 + 3, "jp_theta": 1000 + 5, "jm_theta": 1000 + 6,
+                 "jp_phi": 1000 + 8, "jm_phi": 1000 + 9}
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()

@@ -92,7 +92,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     levels = [(7 * i) % oc.n_r for i in range(70)]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -101,7 +101,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
         again = g.shell_slices(["v_r"], [levels[5]])
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_slices([503], [0])                 # entropy_p (fluctuating part): not provided
+            g.shell_slices([302], [0])                 # vort_theta: not provided
         with pytest.raises(rb.RayleighError):
             g.shell_slices(["v_r"], [oc.n_r])
     o = O.Oracle(oc)
@@ -125,14 +125,14 @@ def test_shell_averages_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
         av = g.shell_averages(names)
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_averages([503])
+            g.shell_averages([302])
     o = O.Oracle(oc)
     o.init_state(sw, sz, sab)
     _oracle_step(o)
@@ -155,7 +155,7 @@ def test_azimuthal_averages_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
@@ -182,7 +182,7 @@ def test_shell_spectra_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     levels = [(5 * i + 1) % oc.n_r for i in range(30)]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -210,7 +210,7 @@ def test_equatorial_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
         g.step(3)
@@ -239,7 +239,7 @@ def test_meridional_slices_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     with _ctx(cfg) as g:
         phis = [(13 * i + 3) % g.n_phi for i in range(70)]
         g.put_state(wpt, z, None, iteration=1)
@@ -269,7 +269,7 @@ def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
     oc = _ocfg(cfg)
     wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
-    names = [q for q in rb.Rayleigh.QUANTITIES if not q.startswith(("b_", "j_"))]   # the hydrodynamic quantities
+    names = list(_ORACLE_NAME)   # the hydrodynamic quantities
     ri, ti, pi = [0, 5, 11, 12, 23], [0, 3, 23, 24, 40, 46, 47], [0, 1, 17, 40, 41, 63, 64, 80, 95]
     with _ctx(cfg) as g:
         g.put_state(wpt, z, None, iteration=1)
@@ -303,7 +303,8 @@ def test_magnetic_quantities_match_the_oracle(precision, tol):
     """B (magnetic_field_codes.F) and the current density J = curl B (current_density_codes.F,
     Compute_J_Components) of a dynamo state: shell slices at 30 levels (relative L2),
     azimuthal averages and shell means (on the quantity's largest magnitude) against the
-    oracle's physical-space buffer; a hydrodynamic context refuses them (RA_ERR_ARG)."""
+    oracle's physical-space buffer; their fluctuating and mean parts in every family as in
+    the hydrodynamic parts test; a hydrodynamic context refuses them (RA_ERR_ARG)."""
     import rayleigh_b200 as rb
     cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, magnetism=True, magnetic_prandtl=5.0,
                precision=precision)
@@ -321,9 +322,12 @@ def test_magnetic_quantities_match_the_oracle(precision, tol):
         av = g.shell_averages(names)
         sw, sz, sab = g.get_state()
         sc, sa, sabm = g.get_magnetic_state()
-    o = O.Oracle(oc)
-    o.init_state(sw, sz, np.concatenate([sab, sabm]), c_coeffs=sc, a_coeffs=sa)
-    o.step()   # its physical-space stage sees the state after 3 steps
+        o = O.Oracle(oc)
+        o.init_state(sw, sz, np.concatenate([sab, sabm]), c_coeffs=sc, a_coeffs=sa)
+        o.step()   # its physical-space stage sees the state after 3 steps
+        parts = _part_fields(o, _ORACLE_MAG)   # bp_r .. bm_phi (804-809), jp_r .. jm_phi (1002-1009)
+        assert len(parts) == 12
+        _check_parts(g, o, list(parts), parts, tol, 1e-12 if precision == 0 else 1e-8)
     ref_av = o.shell_averages([_ORACLE_MAG[n] for n in names])
     for i, name in enumerate(names):
         q = o.last_fields[_ORACLE_MAG[name]]           # [theta, r, phi]
@@ -340,3 +344,95 @@ def test_magnetic_quantities_match_the_oracle(precision, tol):
         with pytest.raises(rb.RayleighError) as ei:
             h.shell_slices(["j_r"], [0])
         assert ei.value.code == rb.RA_ERR_ARG
+
+
+# fluctuating (m > 0) and azimuthal-mean (m = 0) parts of each full quantity, the reference's names
+_PARTS = {"v_r": ("vp_r", "vm_r"), "v_theta": ("vp_theta", "vm_theta"), "v_phi": ("vp_phi", "vm_phi"),
+          "dv_r_dr": ("dvp_r_dr", "dvm_r_dr"), "dv_theta_dr": ("dvp_theta_dr", "dvm_theta_dr"),
+          "dv_phi_dr": ("dvp_phi_dr", "dvm_phi_dr"), "dv_r_dt": ("dvp_r_dt", "dvm_r_dt"),
+          "dv_r_dp": ("dvp_r_dp", "dvm_r_dp"), "dv_theta_dp": ("dvp_theta_dp", "dvm_theta_dp"),
+          "dv_phi_dp": ("dvp_phi_dp", "dvm_phi_dp"), "vort_r": ("vortp_r", "vortm_r"),
+          "entropy": ("entropy_p", "entropy_m"), "pressure": ("pressure_p", "pressure_m"),
+          "entropy_dr": ("entropy_p_dr", "entropy_m_dr"), "pressure_dr": ("pressure_p_dr", "pressure_m_dr"),
+          "entropy_dtheta": ("entropy_p_dtheta", "entropy_m_dtheta"),
+          "entropy_dphi": ("entropy_p_dphi", "entropy_m_dphi"), "pressure_dphi": ("pressure_p_dphi", "pressure_m_dphi"),
+          "b_r": ("bp_r", "bm_r"), "b_theta": ("bp_theta", "bm_theta"), "b_phi": ("bp_phi", "bm_phi"),
+          "j_r": ("jp_r", "jm_r"), "j_theta": ("jp_theta", "jm_theta"), "j_phi": ("jp_phi", "jm_phi")}
+_ZERO_MEANS = {"dvm_r_dp", "dvm_theta_dp", "dvm_phi_dp", "entropy_m_dphi", "pressure_m_dphi"}   # means of d/dphi
+
+
+def _part_fields(o, oracle_names):
+    """name -> (the part's field, its full quantity's field), [theta, r, phi], from the oracle's
+    buffer: the field minus its phi average, or the phi average (fbuffer, m0_values); the
+    parts are also added to last_fields for the oracle's own averages and spectra."""
+    out = {}
+    for full, (fl, mn) in _PARTS.items():
+        if full not in oracle_names:
+            continue
+        q = o.last_fields[oracle_names[full]]
+        mean = np.broadcast_to(q.mean(axis=2, keepdims=True), q.shape).copy()
+        for name, part in ((fl, q - mean), (mn, mean)):
+            o.last_fields[name] = part
+            out[name] = (part, q, oracle_names[full])
+    return out
+
+
+def _check_parts(g, o, names, parts, tol, ptol):
+    """Every family of the parts against the oracle, each on its full quantity's scale."""
+    nth = o.cfg.n_theta
+    levels = [0, 5, 11, 12, 23]
+    phis = [0, 7, 40, 95]
+    ri, ti, pi = [0, 12, 23], [0, 23, 24, 47], [0, 17, 80]
+    sl = g.shell_slices(names, levels)
+    az = g.azimuthal_averages(names)
+    av = g.shell_averages(names)
+    sp = g.shell_spectra(names, levels)
+    eq = g.equatorial_slices(names)
+    me = g.meridional_slices(names, phis)
+    ga = g.global_averages(names)
+    pp = g.point_probes(names, ri, ti, pi)
+    ref_av = o.shell_averages(names)
+    ref_sp = o.shell_spectra(names, levels)
+    full_sp = o.shell_spectra([parts[n][2] for n in names], levels)
+    w = o.radial_integration_weights()
+    for i, name in enumerate(names):
+        part, full, _ = parts[name]
+        S = np.abs(full).max()
+        errs = {"slice": np.abs(sl[i] - part[:, levels, :].transpose(1, 0, 2)).max() / S,
+                "azimuthal": np.abs(az[i] - part.mean(axis=2)).max() / S,
+                "mean": np.abs(av[i, 0] - ref_av[i, 0]).max() / S,
+                "moment2": np.abs(av[i, 1] - ref_av[i, 1]).max() / S ** 2,
+                "spectra": np.abs(sp[i] - ref_sp[i]).max() / np.abs(full_sp[i]).max(),
+                "equatorial": np.abs(eq[i] - 0.5 * (part[nth // 2 - 1] + part[nth // 2])).max() / S,
+                "meridional": np.abs(me[i] - part[:, :, phis].transpose(2, 0, 1)).max() / S,
+                "global": abs(ga[i] - float(np.dot(w, ref_av[i, 0]))) / S,
+                "probe": np.abs(pp[i] - part[np.ix_(ti, ri, pi)].transpose(1, 0, 2)).max() / S}
+        print(name, {k: f"{v:.1e}" for k, v in errs.items()})
+        bound = {k: (ptol if k in ("slice", "meridional", "probe") else tol) for k in errs}
+        assert all(errs[k] < bound[k] for k in errs), (name, errs)
+
+
+@pytest.mark.parametrize("precision,tol,ptol", [(0, 1e-12, 1e-12), (1, 1e-9, 1e-8)])
+def test_fluctuating_and_mean_parts_match_the_oracle(precision, tol, ptol):
+    """The fluctuating (m > 0) and azimuthal-mean (m = 0) codes of every hydrodynamic quantity
+    (velocity_field_codes.F vp_r = 4 .. dvm_phi_dp = 36, vorticity 304 / 307, thermal 503 ..
+    524) in every output family against the field minus its phi average, or that average,
+    of the oracle's buffer, on the full quantity's largest magnitude (the pointwise families
+    with the meridional slices' mixed bound); the means of phi derivatives are exactly zero."""
+    import rayleigh_b200 as rb
+    cfg = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, precision=precision)
+    oc = _ocfg(cfg)
+    wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+    with _ctx(cfg) as g:
+        g.put_state(wpt, z, None, iteration=1)
+        g.step(3)
+        sw, sz, sab = g.get_state()
+        o = O.Oracle(oc)
+        o.init_state(sw, sz, sab)
+        _oracle_step(o)
+        parts = _part_fields(o, _ORACLE_NAME)
+        names = [n for n in parts if n not in _ZERO_MEANS]
+        assert len(names) == 31 and all(n in rb.Rayleigh.QUANTITIES for n in parts)
+        _check_parts(g, o, names, parts, tol, ptol)
+        zeros = sorted(_ZERO_MEANS)
+        assert not g.shell_slices(zeros, [0, 7]).any() and not g.point_probes(zeros, [3], [5], [9]).any()

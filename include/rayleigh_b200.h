@@ -336,6 +336,57 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_JM_THETA    1006
 #define RA_Q_JP_PHI      1008
 #define RA_Q_JM_PHI      1009
+/* Squares (Diagnostics_Energies.F90, Diagnostics_Current_Density.F90): 1/2 rho |v|^2 and its
+ * parts, of the mean flow and of the fluctuations (kinetic_energy_codes.F), the same without
+ * rho, J.J and its parts, and 1/2 Lorentz_Coeff |B|^2 likewise (magnetic_energy_codes.F): */
+#define RA_Q_KINETIC_ENERGY     401
+#define RA_Q_RADIAL_KE          402
+#define RA_Q_THETA_KE           403
+#define RA_Q_PHI_KE             404
+#define RA_Q_MKINETIC_ENERGY    405
+#define RA_Q_RADIAL_MKE         406
+#define RA_Q_THETA_MKE          407
+#define RA_Q_PHI_MKE            408
+#define RA_Q_PKINETIC_ENERGY    409
+#define RA_Q_RADIAL_PKE         410
+#define RA_Q_THETA_PKE          411
+#define RA_Q_PHI_PKE            412
+#define RA_Q_VSQ                413
+#define RA_Q_RADIAL_VSQ         414
+#define RA_Q_THETA_VSQ          415
+#define RA_Q_PHI_VSQ            416
+#define RA_Q_MVSQ               417
+#define RA_Q_RADIAL_MVSQ        418
+#define RA_Q_THETA_MVSQ         419
+#define RA_Q_PHI_MVSQ           420
+#define RA_Q_PVSQ               421
+#define RA_Q_RADIAL_PVSQ        422
+#define RA_Q_THETA_PVSQ         423
+#define RA_Q_PHI_PVSQ           424
+#define RA_Q_J_SQ              1010
+#define RA_Q_JP_SQ             1011
+#define RA_Q_JM_SQ             1012
+#define RA_Q_J_R_SQ            1014
+#define RA_Q_JP_R_SQ           1015
+#define RA_Q_JM_R_SQ           1016
+#define RA_Q_J_THETA_SQ        1017
+#define RA_Q_JP_THETA_SQ       1018
+#define RA_Q_JM_THETA_SQ       1019
+#define RA_Q_J_PHI_SQ          1020
+#define RA_Q_JP_PHI_SQ         1021
+#define RA_Q_JM_PHI_SQ         1022
+#define RA_Q_MAGNETIC_ENERGY   1101
+#define RA_Q_RADIAL_ME         1102
+#define RA_Q_THETA_ME          1103
+#define RA_Q_PHI_ME            1104
+#define RA_Q_MMAGNETIC_ENERGY  1105
+#define RA_Q_RADIAL_MME        1106
+#define RA_Q_THETA_MME         1107
+#define RA_Q_PHI_MME           1108
+#define RA_Q_PMAGNETIC_ENERGY  1109
+#define RA_Q_RADIAL_PME        1110
+#define RA_Q_THETA_PME         1111
+#define RA_Q_PHI_PME           1112
 /* Runs the stages that form the fields on the grid (as ra_kinetic_energy);
  * another code, or a level outside 0 .. n_r-1, returns RA_ERR_ARG. */
 int ra_shell_slices(ra_ctx* ctx, const int* quantities, int nq, const int* levels, int nlev, double* out);

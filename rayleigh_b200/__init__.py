@@ -512,7 +512,20 @@ class Rayleigh:
                   "entropy_p_dtheta": 515, "entropy_m_dtheta": 517, "entropy_p_dphi": 521,
                   "pressure_p_dphi": 522, "entropy_m_dphi": 523, "pressure_m_dphi": 524,
                   "bp_r": 804, "bp_theta": 805, "bp_phi": 806, "bm_r": 807, "bm_theta": 808, "bm_phi": 809,
-                  "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005, "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009}
+                  "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005, "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009,
+                  # sums of squares: kinetic energy densities, v^2, J.J, magnetic energy densities
+                  "kinetic_energy": 401, "radial_ke": 402, "theta_ke": 403, "phi_ke": 404,
+                  "mkinetic_energy": 405, "radial_mke": 406, "theta_mke": 407, "phi_mke": 408,
+                  "pkinetic_energy": 409, "radial_pke": 410, "theta_pke": 411, "phi_pke": 412,
+                  "vsq": 413, "radial_vsq": 414, "theta_vsq": 415, "phi_vsq": 416, "mvsq": 417,
+                  "radial_mvsq": 418, "theta_mvsq": 419, "phi_mvsq": 420, "pvsq": 421,
+                  "radial_pvsq": 422, "theta_pvsq": 423, "phi_pvsq": 424, "j_sq": 1010, "jp_sq":
+                  1011, "jm_sq": 1012, "j_r_sq": 1014, "jp_r_sq": 1015, "jm_r_sq": 1016,
+                  "j_theta_sq": 1017, "jp_theta_sq": 1018, "jm_theta_sq": 1019, "j_phi_sq": 1020,
+                  "jp_phi_sq": 1021, "jm_phi_sq": 1022, "magnetic_energy": 1101, "radial_me": 1102,
+                  "theta_me": 1103, "phi_me": 1104, "mmagnetic_energy": 1105, "radial_mme": 1106,
+                  "theta_mme": 1107, "phi_mme": 1108, "pmagnetic_energy": 1109, "radial_pme": 1110,
+                  "theta_pme": 1111, "phi_pme": 1112}
 
     def shell_slices(self, quantities, levels):
         """Shell slices of the current state: array [quantity][level][theta][phi] of the

@@ -1571,6 +1571,43 @@ __device__ __forceinline__ int natural_index(int p) {
     return n;
 }
 
+// The diagnostic quantity S on the row (theta index th, radial index r) into y[0][.]: one
+// field through the c2r (d/dphi in the spectrum, its fluctuating or mean part by mpart), or
+// for the energy and |J|^2 codes the sum of the squares of up to three fields (each with its
+// own 1/sin(theta), 1/r), times 1, rho(r) / 2 or a constant.  Returns the factor the caller
+// still applies: the single field's 1/sin(theta) and 1/r, 1 for a sum of squares.
+template <int N, int ZPT>
+__device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceSpec& S, const double* rowbase,
+                                               int h, int th, int r, double2* sm, int t, double2 (&y)[FB][ZPT]) {
+    const double csc = P.trig[2 * N + th], orad = P.radial[R_OVER_R * P.nr + r];
+    if (S.nsq == 0) {
+        const int fo[1] = {S.field};
+        const bool dp[1] = {S.dphi != 0};
+        row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
+        return (S.csc ? csc : 1.0) * (S.orad ? orad : 1.0);
+    }
+    double2 acc[ZPT];
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) acc[q] = make_double2(0.0, 0.0);
+#pragma unroll 1
+    for (int i = 0; i < S.nsq; ++i) {
+        const int fo[1] = {S.sqf[i]};
+        const bool dp[1] = {false};
+        row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
+        const double s = (S.sqcsc[i] ? csc : 1.0) * (S.sqorad[i] ? orad : 1.0);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            const double a = y[0][q].x * s, b = y[0][q].y * s;
+            acc[q].x += a * a;
+            acc[q].y += b * b;
+        }
+    }
+    const double c = S.coef == 1 ? 0.5 * P.radial[R_DENSITY * P.nr + r] : (S.coef == 2 ? S.cval : 1.0);
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) y[0][q] = make_double2(acc[q].x * c, acc[q].y * c);
+    return 1.0;
+}
+
 // Shell slices (Spherical_IO.F90 Shell_Slices) of one diagnostic quantity: one
 // CTA per (theta, level) row forms the quantity on the phi grid from p2a with
 // the physics kernel's c2r (d/dphi in the spectrum, 1/sin(theta) where the
@@ -1588,11 +1625,8 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_slice_kernel(PhysParams P, 
     const int lv = (int)blockIdx.y;
     const int r = S.level[lv];
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, sm, t, y);
     double2* row = reinterpret_cast<double2*>(out + ((long)lv * N + th) * (2L * N));
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
@@ -1662,11 +1696,8 @@ __global__ void __launch_bounds__(ROW_THREADS) shell_moment_rows_kernel(PhysPara
     const int r = (int)blockIdx.y;
     const int nr = P.nr;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, sm, t, y);
     const double mu = MOMENTS ? mean[r] : 0.0;
     double s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
@@ -1835,11 +1866,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int lv = (int)blockIdx.y;
     const int r = S.level[lv];
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, buf, t, y);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
         const int p = t + q * ROW_THREADS;
@@ -1960,11 +1988,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ROW_THREADS)
     const int th = h ? (N - 1 - thh) : thh;
     const int r = (int)blockIdx.y;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, buf, t, y);
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {   // each thread rewrites the positions it read
         const int p = t + q * ROW_THREADS;
@@ -2037,11 +2062,8 @@ __global__ void __launch_bounds__(ROW_THREADS) meridional_slice_kernel(PhysParam
     const int r = (int)blockIdx.y;
     const int nr = P.nr;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, buf, t, y);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {
@@ -2165,11 +2187,8 @@ __global__ void __launch_bounds__(ROW_THREADS) point_probe_kernel(PhysParams P, 
     const int h = th >= N / 2 ? 1 : 0;
     const int thh = h ? (N - 1 - th) : th;
     const double* rowbase = P.p2a + (long)thh * (2L * P.L * P.ncola) + (long)r * (2 * P.nfa);
-    const int fo[1] = {S.field};
-    const bool dp[1] = {S.dphi != 0};
     double2 y[FB][ZPT];
-    row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, buf, t, y, S.mpart);
-    const double scale = (S.csc ? P.trig[2 * N + th] : 1.0) * (S.orad ? P.radial[R_OVER_R * P.nr + r] : 1.0);
+    const double scale = row_quantity<N, ZPT>(P, S, rowbase, h, th, r, buf, t, y);
     __syncthreads();   // every thread has read its points out of the buffer
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) {

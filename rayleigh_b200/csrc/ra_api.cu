@@ -1993,9 +1993,66 @@ static const QuantityParts kParts[] = {
     {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009},
 };
 
+// Sums of squares (Diagnostics_Energies.F90 Compute_Kinetic_Energy, Compute_Magnetic_Energy;
+// Diagnostics_Current_Density.F90): kinetic_energy_codes.F (keoffset = 400: 1/2 rho v^2 and
+// its r, theta, phi parts 401-404, of the mean flow 405-408, of the fluctuations 409-412; v^2
+// likewise without rho 413-424), magnetic_energy_codes.F (meoffset = 1100: 1/2 Lorentz_Coeff
+// B^2, 1101-1112 in the same order) and current_density_codes.F (J.J 1010, J'.J' 1011,
+// mean J.J 1012; J_r^2, J_theta^2, J_phi^2 with their fluctuating and mean parts 1014-1022).
+struct SquareSource { int code, nsq, f0, f1, f2, mpart, coef; };
+enum { SQ_V = -1, SQ_B = -2, SQ_J = -3 };   // f0 of the three-component sums
+static const SquareSource kSquares[] = {
+    {401, 3, SQ_V, 0, 0, 0, 1}, {402, 1, A_VR, 0, 0, 0, 1}, {403, 1, A_VT, 0, 0, 0, 1}, {404, 1, A_VP, 0, 0, 0, 1},
+    {405, 3, SQ_V, 0, 0, 2, 1}, {406, 1, A_VR, 0, 0, 2, 1}, {407, 1, A_VT, 0, 0, 2, 1}, {408, 1, A_VP, 0, 0, 2, 1},
+    {409, 3, SQ_V, 0, 0, 1, 1}, {410, 1, A_VR, 0, 0, 1, 1}, {411, 1, A_VT, 0, 0, 1, 1}, {412, 1, A_VP, 0, 0, 1, 1},
+    {413, 3, SQ_V, 0, 0, 0, 0}, {414, 1, A_VR, 0, 0, 0, 0}, {415, 1, A_VT, 0, 0, 0, 0}, {416, 1, A_VP, 0, 0, 0, 0},
+    {417, 3, SQ_V, 0, 0, 2, 0}, {418, 1, A_VR, 0, 0, 2, 0}, {419, 1, A_VT, 0, 0, 2, 0}, {420, 1, A_VP, 0, 0, 2, 0},
+    {421, 3, SQ_V, 0, 0, 1, 0}, {422, 1, A_VR, 0, 0, 1, 0}, {423, 1, A_VT, 0, 0, 1, 0}, {424, 1, A_VP, 0, 0, 1, 0},
+    {1101, 3, SQ_B, 0, 0, 0, 2}, {1102, 1, A_BR, 0, 0, 0, 2}, {1103, 1, A_BT, 0, 0, 0, 2}, {1104, 1, A_BP, 0, 0, 0, 2},
+    {1105, 3, SQ_B, 0, 0, 2, 2}, {1106, 1, A_BR, 0, 0, 2, 2}, {1107, 1, A_BT, 0, 0, 2, 2}, {1108, 1, A_BP, 0, 0, 2, 2},
+    {1109, 3, SQ_B, 0, 0, 1, 2}, {1110, 1, A_BR, 0, 0, 1, 2}, {1111, 1, A_BT, 0, 0, 1, 2}, {1112, 1, A_BP, 0, 0, 1, 2},
+    {1010, 3, SQ_J, 0, 0, 0, 0}, {1011, 3, SQ_J, 0, 0, 1, 0}, {1012, 3, SQ_J, 0, 0, 2, 0},
+    {1014, 1, A_CBR, 0, 0, 0, 0}, {1015, 1, A_CBR, 0, 0, 1, 0}, {1016, 1, A_CBR, 0, 0, 2, 0},
+    {1017, 1, A_CBT, 0, 0, 0, 0}, {1018, 1, A_CBT, 0, 0, 1, 0}, {1019, 1, A_CBT, 0, 0, 2, 0},
+    {1020, 1, A_CBP, 0, 0, 0, 0}, {1021, 1, A_CBP, 0, 0, 1, 0}, {1022, 1, A_CBP, 0, 0, 2, 0},
+};
+
+// A squared field's factors: v_theta, v_phi are formed divided by sin(theta); the r sin(theta)
+// B_theta, B_phi and curl B theta, phi fields by r sin(theta) (rsintheta_div)
+static void square_term(SliceSpec& S, int i, int field) {
+    S.sqf[i] = field;
+    S.sqcsc[i] = (field == A_VT || field == A_VP || field == A_BT || field == A_BP || field == A_CBT ||
+                  field == A_CBP) ? 1 : 0;
+    S.sqorad[i] = (field == A_BT || field == A_BP || field == A_CBT || field == A_CBP) ? 1 : 0;
+}
+
 static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {
     std::vector<SliceSpec> spec(nq);
     for (int q = 0; q < nq; ++q) {
+        const SquareSource* sq = nullptr;
+        for (const SquareSource& k : kSquares)
+            if (k.code == quantities[q]) sq = &k;
+        if (sq) {
+            SliceSpec S{};
+            S.nsq = sq->nsq;
+            if (sq->nsq == 3) {
+                static const int kV[3] = {A_VR, A_VT, A_VP}, kB[3] = {A_BR, A_BT, A_BP},
+                                 kJ[3] = {A_CBR, A_CBT, A_CBP};
+                const int* tri = sq->f0 == SQ_V ? kV : (sq->f0 == SQ_B ? kB : kJ);
+                for (int i = 0; i < 3; ++i) square_term(S, i, tri[i]);
+            } else {
+                square_term(S, 0, sq->f0);
+            }
+            for (int i = 0; i < S.nsq; ++i)
+                if (S.sqf[i] >= c.nfa)
+                    throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
+            S.field = S.sqf[0];
+            S.mpart = sq->mpart;
+            S.coef = sq->coef;
+            S.cval = 0.5 * c.rad.lorentz;   // magnetic_energy: 1/2 Lorentz_Coeff
+            spec[q] = S;
+            continue;
+        }
         int code = quantities[q], mpart = 0;
         for (const QuantityParts& p : kParts) {
             if (p.fluct == code) { code = p.full; mpart = 1; break; }

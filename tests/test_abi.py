@@ -125,6 +125,23 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "bp_r": 800 + 4, "bp_theta": 800 + 5, "bp_phi": 800 + 6, "bm_r": 800 + 7, "bm_theta": 800 + 8,
                  "bm_phi": 800 + 9, "jp_r": 1000 + 2, "jm_r": 1000 + 3, "jp_theta": 1000 + 5, "jm_theta": 1000 + 6,
                  "jp_phi": 1000 + 8, "jm_phi": 1000 + 9}
+    # kinetic_energy_codes.F: keoffset = vort_off + 100; magnetic_energy_codes.F: meoffset = joffset + 100
+    reference.update({"kinetic_energy": 400 + 1, "radial_ke": 400 + 2, "theta_ke": 400 + 3,
+                      "phi_ke": 400 + 4, "mkinetic_energy": 400 + 5, "radial_mke": 400 + 6,
+                      "theta_mke": 400 + 7, "phi_mke": 400 + 8, "pkinetic_energy": 400 + 9,
+                      "radial_pke": 400 + 10, "theta_pke": 400 + 11, "phi_pke": 400 + 12, "vsq": 400 + 13,
+                      "radial_vsq": 400 + 14, "theta_vsq": 400 + 15, "phi_vsq": 400 + 16, "mvsq": 400 + 17,
+                      "radial_mvsq": 400 + 18, "theta_mvsq": 400 + 19, "phi_mvsq": 400 + 20,
+                      "pvsq": 400 + 21, "radial_pvsq": 400 + 22, "theta_pvsq": 400 + 23,
+                      "phi_pvsq": 400 + 24})
+    reference.update({"j_sq": 1000 + 10, "jp_sq": 1000 + 11, "jm_sq": 1000 + 12, "j_r_sq": 1000 + 14,
+                      "jp_r_sq": 1000 + 15, "jm_r_sq": 1000 + 16, "j_theta_sq": 1000 + 17,
+                      "jp_theta_sq": 1000 + 18, "jm_theta_sq": 1000 + 19, "j_phi_sq": 1000 + 20,
+                      "jp_phi_sq": 1000 + 21, "jm_phi_sq": 1000 + 22})
+    reference.update({"magnetic_energy": 1100 + 1, "radial_me": 1100 + 2, "theta_me": 1100 + 3,
+                      "phi_me": 1100 + 4, "mmagnetic_energy": 1100 + 5, "radial_mme": 1100 + 6,
+                      "theta_mme": 1100 + 7, "phi_mme": 1100 + 8, "pmagnetic_energy": 1100 + 9,
+                      "radial_pme": 1100 + 10, "theta_pme": 1100 + 11, "phi_pme": 1100 + 12})
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()

@@ -379,10 +379,10 @@ def _part_fields(o, oracle_names):
 
 def _check_parts(g, o, names, parts, tol, ptol):
     """Every family of the parts against the oracle, each on its full quantity's scale."""
-    nth = o.cfg.n_theta
-    levels = [0, 5, 11, 12, 23]
-    phis = [0, 7, 40, 95]
-    ri, ti, pi = [0, 12, 23], [0, 23, 24, 47], [0, 17, 80]
+    nth, nphi, nr = o.cfg.n_theta, 2 * o.cfg.n_theta, o.cfg.n_r
+    levels = [0, 5, nr // 2 - 1, nr // 2, nr - 1]
+    phis = [0, 7, nphi // 2 - 8, nphi - 1]
+    ri, ti, pi = [0, nr // 2, nr - 1], [0, nth // 2 - 1, nth // 2, nth - 1], [0, 17, nphi - 16]
     sl = g.shell_slices(names, levels)
     az = g.azimuthal_averages(names)
     av = g.shell_averages(names)
@@ -436,3 +436,74 @@ def test_fluctuating_and_mean_parts_match_the_oracle(precision, tol, ptol):
         _check_parts(g, o, names, parts, tol, ptol)
         zeros = sorted(_ZERO_MEANS)
         assert not g.shell_slices(zeros, [0, 7]).any() and not g.point_probes(zeros, [3], [5], [9]).any()
+
+
+def _square_fields(o, kind):
+    """name -> (sum of squares, the full quantity's sum, its name) from the oracle's buffer
+    (Compute_Kinetic_Energy, Compute_Magnetic_Energy, Compute_J_Components): the fields, their
+    phi means (m0_values) or the fluctuations (fbuffer), squared and summed, times rho / 2
+    (kinetic energy), Lorentz_Coeff / 2 (magnetic energy) or 1; added to last_fields too."""
+    comps = {"v": ("vr", "vt", "vp"), "b": ("br", "bt", "bp"), "j": ("curlbr", "curlbt", "curlbp")}
+    if kind == "hydro":
+        fams = [("v", 0.5 * o.density[None, :, None], ("kinetic_energy", "radial_ke", "theta_ke", "phi_ke"),
+                 ("mkinetic_energy", "radial_mke", "theta_mke", "phi_mke"),
+                 ("pkinetic_energy", "radial_pke", "theta_pke", "phi_pke")),
+                ("v", 1.0, ("vsq", "radial_vsq", "theta_vsq", "phi_vsq"), ("mvsq", "radial_mvsq", "theta_mvsq",
+                 "phi_mvsq"), ("pvsq", "radial_pvsq", "theta_pvsq", "phi_pvsq"))]
+    else:
+        fams = [("b", 0.5 * o.lorentz, ("magnetic_energy", "radial_me", "theta_me", "phi_me"),
+                 ("mmagnetic_energy", "radial_mme", "theta_mme", "phi_mme"),
+                 ("pmagnetic_energy", "radial_pme", "theta_pme", "phi_pme")),
+                ("j", 1.0, ("j_sq", "j_r_sq", "j_theta_sq", "j_phi_sq"), ("jm_sq", "jm_r_sq", "jm_theta_sq",
+                 "jm_phi_sq"), ("jp_sq", "jp_r_sq", "jp_theta_sq", "jp_phi_sq"))]
+    out = {}
+    for comp, fac, full_names, mean_names, fluct_names in fams:
+        fields = [o.last_fields[k] for k in comps[comp]]
+        means = [np.broadcast_to(q.mean(axis=2, keepdims=True), q.shape) for q in fields]
+        parts = {"full": fields, "mean": means, "fluct": [q - m for q, m in zip(fields, means)]}
+        for which, names in (("full", full_names), ("mean", mean_names), ("fluct", fluct_names)):
+            for i, name in enumerate(names):
+                terms = parts[which] if i == 0 else [parts[which][i - 1]]
+                val = fac * sum(t * t for t in terms)
+                o.last_fields[name] = np.ascontiguousarray(val)
+                out[name] = [o.last_fields[name], None, full_names[i]]
+    for v in out.values():
+        v[1] = o.last_fields[v[2]]
+    return {k: tuple(v) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("precision,tol,ptol", [(0, 1e-12, 1e-12), (1, 1e-9, 1e-8)])
+def test_energy_densities_match_the_oracle(precision, tol, ptol):
+    """The sums of squares in every output family (kinetic_energy_codes.F 401-424 on the
+    anelastic polytrope, where rho varies with radius; with magnetism magnetic_energy_codes.F
+    1101-1112 and the J.J codes 1010-1012, 1014-1022) against the oracle's buffer, on the
+    largest magnitude of the full (not the mean or fluctuating) sum."""
+    import rayleigh_b200 as rb
+    anel = dict(n_r=24, l_max=15, dt=1e-4, reference_type=3, poly_n=2.0, poly_nrho=3.0, modified_rayleigh=0.5,
+                ekman=1e-3, prandtl=1.0, magnetic_prandtl=2.0, no_slip_top=False, no_slip_bottom=False)
+    mhd = dict(n_r=24, l_max=31, dt=2e-4, rayleigh=1e5, ekman=1e-3, magnetism=True, magnetic_prandtl=5.0)
+    for cfg, kind in ((anel, "hydro"), (mhd, "mag")):
+        cfg = dict(cfg, precision=precision)
+        oc = _ocfg(cfg)
+        wpt, z = O.seeded_state(oc, amp=1e-2, lmax_pert=10)
+        with _ctx(cfg) as g:
+            g.put_state(wpt, z, None, iteration=1)
+            if kind == "mag":
+                c, a = O.seeded_magnetic_state(oc, amp=1e-1, lmax_pert=10)
+                g.put_magnetic_state(c, a)
+            g.step(3)
+            sw, sz, sab = g.get_state()
+            o = O.Oracle(oc)
+            if kind == "mag":
+                sc, sa, sabm = g.get_magnetic_state()
+                o.init_state(sw, sz, np.concatenate([sab, sabm]), c_coeffs=sc, a_coeffs=sa)
+            else:
+                o.init_state(sw, sz, sab)
+            o.step()
+            sq = _square_fields(o, kind)
+            assert len(sq) == 24 and all(n in rb.Rayleigh.QUANTITIES for n in sq)
+            _check_parts(g, o, list(sq), sq, tol, ptol)
+            if kind == "hydro":
+                with pytest.raises(rb.RayleighError) as ei:
+                    g.shell_slices(["magnetic_energy"], [0])
+                assert ei.value.code == rb.RA_ERR_ARG

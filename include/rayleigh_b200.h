@@ -336,6 +336,16 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_JM_THETA    1006
 #define RA_Q_JP_PHI      1008
 #define RA_Q_JM_PHI      1009
+/* with magnetism, the phi derivatives of B and their parts (the means are zero): */
+#define RA_Q_DB_R_DP           828
+#define RA_Q_DB_THETA_DP       829
+#define RA_Q_DB_PHI_DP         830
+#define RA_Q_DBP_R_DP          831
+#define RA_Q_DBP_THETA_DP      832
+#define RA_Q_DBP_PHI_DP        833
+#define RA_Q_DBM_R_DP          834
+#define RA_Q_DBM_THETA_DP      835
+#define RA_Q_DBM_PHI_DP        836
 /* Squares (Diagnostics_Energies.F90, Diagnostics_Current_Density.F90): 1/2 rho |v|^2 and its
  * parts, of the mean flow and of the fluctuations (kinetic_energy_codes.F), the same without
  * rho, J.J and its parts, and 1/2 Lorentz_Coeff |B|^2 likewise (magnetic_energy_codes.F): */

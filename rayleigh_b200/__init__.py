@@ -513,6 +513,8 @@ class Rayleigh:
                   "pressure_p_dphi": 522, "entropy_m_dphi": 523, "pressure_m_dphi": 524,
                   "bp_r": 804, "bp_theta": 805, "bp_phi": 806, "bm_r": 807, "bm_theta": 808, "bm_phi": 809,
                   "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005, "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009,
+                  "db_r_dp": 828, "db_theta_dp": 829, "db_phi_dp": 830, "dbp_r_dp": 831, "dbp_theta_dp": 832,
+                  "dbp_phi_dp": 833, "dbm_r_dp": 834, "dbm_theta_dp": 835, "dbm_phi_dp": 836,
                   # sums of squares: kinetic energy densities, v^2, J.J, magnetic energy densities
                   "kinetic_energy": 401, "radial_ke": 402, "theta_ke": 403, "phi_ke": 404,
                   "mkinetic_energy": 405, "radial_mke": 406, "theta_mke": 407, "phi_mke": 408,

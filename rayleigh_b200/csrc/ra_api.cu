@@ -1960,7 +1960,8 @@ int ra_kinetic_energy(ra_ctx* ctx, double* ke) {
 // comes from in p2a.  vort_r, which Diagnostics_Vorticity_Field.F90:89-93 forms
 // as (dv_phi/dtheta + cot v_phi - csc dv_theta/dphi) / r, is the spectral
 // l(l+1) Z / r^2 here: the same band-limited field, equal up to rounding.
-// With magnetism, magnetic_field_codes.F (boffset = 800): B_r, B_theta, B_phi, the last two
+// With magnetism, magnetic_field_codes.F (boffset = 800): B_r, B_theta, B_phi and their phi
+// derivatives (828-830, d/dphi in the spectrum as for the velocity), the B_theta, B_phi ones
 // formed from the r sin(theta) B_theta, B_phi fields the step transforms (rsintheta_div), and
 // current_density_codes.F (joffset = boffset + 200): J_r, J_theta, J_phi, the curl of B as
 // Compute_J_Components reads it (Diagnostics_Current_Density.F90), the last two likewise.
@@ -1976,6 +1977,7 @@ static const QuantitySource kQuantities[] = {
     {520, A_T, 1, 0, 1, 0},    // d pressure / d phi
     {801, A_BR, 0, 0, 0, 0},   {802, A_BT, 0, 1, 0, 1},   {803, A_BP, 0, 1, 0, 1},
     {1001, A_CBR, 0, 0, 0, 0}, {1004, A_CBT, 0, 1, 0, 1}, {1007, A_CBP, 0, 1, 0, 1},
+    {828, A_BR, 1, 0, 0, 0},   {829, A_BT, 1, 1, 0, 1},   {830, A_BP, 1, 1, 0, 1},   // dB/dphi
 };
 
 // The fluctuating (m > 0) and azimuthal-mean (m = 0) codes of each quantity above, as the
@@ -1990,7 +1992,8 @@ static const QuantityParts kParts[] = {
     {12, 15, 18},       {19, 22, 25},       {28, 31, 34},       {29, 32, 35},       {30, 33, 36},
     {301, 304, 307},    {501, 503, 505},    {502, 504, 506},    {507, 509, 511},    {508, 510, 512},
     {513, 515, 517},    {519, 521, 523},    {520, 522, 524},    {801, 804, 807},    {802, 805, 808},
-    {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009},
+    {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009}, {828, 831, 834},
+    {829, 832, 835},    {830, 833, 836},
 };
 
 // Sums of squares (Diagnostics_Energies.F90 Compute_Kinetic_Energy, Compute_Magnetic_Energy;

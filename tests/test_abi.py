@@ -124,7 +124,9 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "pressure_m_dphi": 500 + 24,
                  "bp_r": 800 + 4, "bp_theta": 800 + 5, "bp_phi": 800 + 6, "bm_r": 800 + 7, "bm_theta": 800 + 8,
                  "bm_phi": 800 + 9, "jp_r": 1000 + 2, "jm_r": 1000 + 3, "jp_theta": 1000 + 5, "jm_theta": 1000 + 6,
-                 "jp_phi": 1000 + 8, "jm_phi": 1000 + 9}
+                 "jp_phi": 1000 + 8, "jm_phi": 1000 + 9, "db_r_dp": 800 + 28, "db_theta_dp": 800 + 29,
+                 "db_phi_dp": 800 + 30, "dbp_r_dp": 800 + 31, "dbp_theta_dp": 800 + 32, "dbp_phi_dp": 800 + 33,
+                 "dbm_r_dp": 800 + 34, "dbm_theta_dp": 800 + 35, "dbm_phi_dp": 800 + 36}
     # kinetic_energy_codes.F: keoffset = vort_off + 100; magnetic_energy_codes.F: meoffset = joffset + 100
     reference.update({"kinetic_energy": 400 + 1, "radial_ke": 400 + 2, "theta_ke": 400 + 3,
                       "phi_ke": 400 + 4, "mkinetic_energy": 400 + 5, "radial_mke": 400 + 6,

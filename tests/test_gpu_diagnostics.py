@@ -295,13 +295,23 @@ def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
 
 
 # the oracle's physical-space buffer names of the magnetic quantities (after rsintheta_div)
-_ORACLE_MAG = {"b_r": "br", "b_theta": "bt", "b_phi": "bp", "j_r": "curlbr", "j_theta": "curlbt", "j_phi": "curlbp"}
+_ORACLE_MAG = {"b_r": "br", "b_theta": "bt", "b_phi": "bp", "j_r": "curlbr", "j_theta": "curlbt", "j_phi": "curlbp",
+               "db_r_dp": "dbrdp", "db_theta_dp": "dbtdp", "db_phi_dp": "dbpdp"}
+
+
+def _add_dphi_of_b(o):
+    """d/dphi of the oracle's B components (band-limited in phi: the spectral derivative is exact)."""
+    for src, dst in (("br", "dbrdp"), ("bt", "dbtdp"), ("bp", "dbpdp")):
+        q = o.last_fields[src]
+        m = np.arange(q.shape[2] // 2 + 1)
+        o.last_fields[dst] = np.fft.irfft(1j * m * np.fft.rfft(q, axis=2), n=q.shape[2], axis=2)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
 def test_magnetic_quantities_match_the_oracle(precision, tol):
-    """B (magnetic_field_codes.F) and the current density J = curl B (current_density_codes.F,
-    Compute_J_Components) of a dynamo state: shell slices at 30 levels (relative L2),
+    """B and its phi derivatives (magnetic_field_codes.F) and the current density J = curl B
+    (current_density_codes.F, Compute_J_Components) of a dynamo state: shell slices at 30
+    levels (relative L2),
     azimuthal averages and shell means (on the quantity's largest magnitude) against the
     oracle's physical-space buffer; their fluctuating and mean parts in every family as in
     the hydrodynamic parts test; a hydrodynamic context refuses them (RA_ERR_ARG)."""
@@ -325,8 +335,9 @@ def test_magnetic_quantities_match_the_oracle(precision, tol):
         o = O.Oracle(oc)
         o.init_state(sw, sz, np.concatenate([sab, sabm]), c_coeffs=sc, a_coeffs=sa)
         o.step()   # its physical-space stage sees the state after 3 steps
-        parts = _part_fields(o, _ORACLE_MAG)   # bp_r .. bm_phi (804-809), jp_r .. jm_phi (1002-1009)
-        assert len(parts) == 12
+        _add_dphi_of_b(o)
+        parts = _part_fields(o, _ORACLE_MAG)   # bp_r .. bm_phi (804-809), jp_r .. jm_phi, dbp_r_dp .. dbm_phi_dp
+        assert len(parts) == 18
         _check_parts(g, o, list(parts), parts, tol, 1e-12 if precision == 0 else 1e-8)
     ref_av = o.shell_averages([_ORACLE_MAG[n] for n in names])
     for i, name in enumerate(names):
@@ -357,7 +368,9 @@ _PARTS = {"v_r": ("vp_r", "vm_r"), "v_theta": ("vp_theta", "vm_theta"), "v_phi":
           "entropy_dtheta": ("entropy_p_dtheta", "entropy_m_dtheta"),
           "entropy_dphi": ("entropy_p_dphi", "entropy_m_dphi"), "pressure_dphi": ("pressure_p_dphi", "pressure_m_dphi"),
           "b_r": ("bp_r", "bm_r"), "b_theta": ("bp_theta", "bm_theta"), "b_phi": ("bp_phi", "bm_phi"),
-          "j_r": ("jp_r", "jm_r"), "j_theta": ("jp_theta", "jm_theta"), "j_phi": ("jp_phi", "jm_phi")}
+          "j_r": ("jp_r", "jm_r"), "j_theta": ("jp_theta", "jm_theta"), "j_phi": ("jp_phi", "jm_phi"),
+          "db_r_dp": ("dbp_r_dp", "dbm_r_dp"), "db_theta_dp": ("dbp_theta_dp", "dbm_theta_dp"),
+          "db_phi_dp": ("dbp_phi_dp", "dbm_phi_dp")}
 _ZERO_MEANS = {"dvm_r_dp", "dvm_theta_dp", "dvm_phi_dp", "entropy_m_dphi", "pressure_m_dphi"}   # means of d/dphi
 
 

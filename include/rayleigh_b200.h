@@ -273,6 +273,8 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_DV_THETA_DP   29
 #define RA_Q_DV_PHI_DP     30
 #define RA_Q_VORT_R       301   /* l(l+1) Z / (rho r^2), the radial vorticity */
+#define RA_Q_VORT_THETA   302   /* (csc dv_r/dphi - v_phi) / r - dv_phi/dr */
+#define RA_Q_VORT_PHI     303   /* dv_theta/dr + (v_theta - dv_r/dtheta) / r */
 #define RA_Q_ENTROPY      501
 #define RA_Q_PRESSURE     502   /* formed with the P grid in T's place; the pressure codes need reference_type 1 */
 #define RA_Q_ENTROPY_DR   507
@@ -310,6 +312,10 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_DVM_PHI_DP    36
 #define RA_Q_VORTP_R      304
 #define RA_Q_VORTM_R      307
+#define RA_Q_VORTP_THETA  305
+#define RA_Q_VORTP_PHI    306
+#define RA_Q_VORTM_THETA  308
+#define RA_Q_VORTM_PHI    309
 #define RA_Q_ENTROPY_P    503
 #define RA_Q_PRESSURE_P   504
 #define RA_Q_ENTROPY_M    505

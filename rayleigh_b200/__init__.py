@@ -507,7 +507,9 @@ class Rayleigh:
                   "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
                   "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
                   "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36, "vortp_r": 304,
-                  "vortm_r": 307, "entropy_p": 503, "pressure_p": 504, "entropy_m": 505, "pressure_m": 506,
+                  "vortm_r": 307, "vort_theta": 302, "vort_phi": 303, "vortp_theta": 305,
+                  "vortp_phi": 306, "vortm_theta": 308, "vortm_phi": 309,
+                  "entropy_p": 503, "pressure_p": 504, "entropy_m": 505, "pressure_m": 506,
                   "entropy_p_dr": 509, "pressure_p_dr": 510, "entropy_m_dr": 511, "pressure_m_dr": 512,
                   "entropy_p_dtheta": 515, "entropy_m_dtheta": 517, "entropy_p_dphi": 521,
                   "pressure_p_dphi": 522, "entropy_m_dphi": 523, "pressure_m_dphi": 524,

@@ -1573,9 +1573,10 @@ __device__ __forceinline__ int natural_index(int p) {
 
 // The diagnostic quantity S on the row (theta index th, radial index r) into y[0][.]: one
 // field through the c2r (d/dphi in the spectrum, its fluctuating or mean part by mpart), or
-// for the energy and |J|^2 codes the sum of the squares of up to three fields (each with its
-// own 1/sin(theta), 1/r), times 1, rho(r) / 2 or a constant.  Returns the factor the caller
-// still applies: the single field's 1/sin(theta) and 1/r, 1 for a sum of squares.
+// for the energy and |J|^2 codes the sum of the squares of up to three fields, for the theta
+// and phi vorticity a sum of three fields with coefficients (each field with its own d/dphi,
+// 1/sin(theta), 1/r), times 1, rho(r) / 2 or a constant.  Returns the factor the caller still
+// applies: the single field's 1/sin(theta) and 1/r, 1 for a sum.
 template <int N, int ZPT>
 __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceSpec& S, const double* rowbase,
                                                int h, int th, int r, double2* sm, int t, double2 (&y)[FB][ZPT]) {
@@ -1592,14 +1593,23 @@ __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceS
 #pragma unroll 1
     for (int i = 0; i < S.nsq; ++i) {
         const int fo[1] = {S.sqf[i]};
-        const bool dp[1] = {false};
+        const bool dp[1] = {S.sqdp[i] != 0};
         row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
         const double s = (S.sqcsc[i] ? csc : 1.0) * (S.sqorad[i] ? orad : 1.0);
+        if (S.lin) {
+            const double cs = S.sqc[i] * s;
 #pragma unroll
-        for (int q = 0; q < ZPT; ++q) {
-            const double a = y[0][q].x * s, b = y[0][q].y * s;
-            acc[q].x += a * a;
-            acc[q].y += b * b;
+            for (int q = 0; q < ZPT; ++q) {
+                acc[q].x += cs * y[0][q].x;
+                acc[q].y += cs * y[0][q].y;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < ZPT; ++q) {
+                const double a = y[0][q].x * s, b = y[0][q].y * s;
+                acc[q].x += a * a;
+                acc[q].y += b * b;
+            }
         }
     }
     const double c = S.coef == 1 ? 0.5 * P.radial[R_DENSITY * P.nr + r] : (S.coef == 2 ? S.cval : 1.0);

@@ -1993,7 +1993,7 @@ static const QuantityParts kParts[] = {
     {301, 304, 307},    {501, 503, 505},    {502, 504, 506},    {507, 509, 511},    {508, 510, 512},
     {513, 515, 517},    {519, 521, 523},    {520, 522, 524},    {801, 804, 807},    {802, 805, 808},
     {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009}, {828, 831, 834},
-    {829, 832, 835},    {830, 833, 836},
+    {829, 832, 835},    {830, 833, 836},    {302, 305, 308},    {303, 306, 309},
 };
 
 // Sums of squares (Diagnostics_Energies.F90 Compute_Kinetic_Energy, Compute_Magnetic_Energy;
@@ -2029,6 +2029,17 @@ static void square_term(SliceSpec& S, int i, int field) {
     S.sqorad[i] = (field == A_BT || field == A_BP || field == A_CBT || field == A_CBP) ? 1 : 0;
 }
 
+// Sums of fields (Diagnostics_Vorticity_Field.F90 Compute_Vorticity_Field): vort_theta (302)
+// = (csc dv_r/dphi - v_phi) / r - dv_phi/dr, vort_phi (303) = dv_theta/dr + (v_theta -
+// dv_r/dtheta) / r, from the buffer fields as the other codes form them (v_theta, v_phi and
+// their r and theta derivatives divided by sin(theta)).
+struct LinearTerm { int field, dphi, csc, orad; double c; };
+struct LinearSource { int code; LinearTerm t[3]; };
+static const LinearSource kLinear[] = {
+    {302, {{A_VR, 1, 1, 1, 1.0}, {A_VP, 0, 1, 1, -1.0}, {A_DVPDR, 0, 1, 0, -1.0}}},
+    {303, {{A_DVTDR, 0, 1, 0, 1.0}, {A_VT, 0, 1, 1, 1.0}, {A_DVRDT, 0, 1, 1, -1.0}}},
+};
+
 static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {
     std::vector<SliceSpec> spec(nq);
     for (int q = 0; q < nq; ++q) {
@@ -2060,6 +2071,25 @@ static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities
         for (const QuantityParts& p : kParts) {
             if (p.fluct == code) { code = p.full; mpart = 1; break; }
             if (p.mean == code) { code = p.full; mpart = 2; break; }
+        }
+        const LinearSource* ls = nullptr;
+        for (const LinearSource& k : kLinear)
+            if (k.code == code) ls = &k;
+        if (ls) {
+            SliceSpec S{};
+            S.nsq = 3;
+            S.lin = 1;
+            for (int i = 0; i < 3; ++i) {
+                S.sqf[i] = ls->t[i].field;
+                S.sqdp[i] = ls->t[i].dphi;
+                S.sqcsc[i] = ls->t[i].csc;
+                S.sqorad[i] = ls->t[i].orad;
+                S.sqc[i] = ls->t[i].c;
+            }
+            S.field = S.sqf[0];
+            S.mpart = mpart;
+            spec[q] = S;
+            continue;
         }
         const QuantitySource* src = nullptr;
         for (const QuantitySource& k : kQuantities)

@@ -259,11 +259,11 @@ struct SliceSpec {
     int pressure;               // formed with the P grid in T's place (pressure quantities)
     int orad;                   // times 1/r (the r sin(theta) B_theta, B_phi fields)
     int mpart;                  // 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean
-    // nsq > 0: the sum of the squares of the fields sqf[0..nsq) (each times 1/sin(theta) where
-    // sqcsc, 1/r where sqorad), times coef 0: one, 1: rho(r) / 2, 2: cval (field, dphi, csc,
-    // orad unused)
-    int nsq, sqf[3], sqcsc[3], sqorad[3], coef;
-    double cval;
+    // nsq > 0: the sum of the squares (lin = 0) or the sum sqc[i] x (lin = 1) of the fields
+    // sqf[0..nsq) (each d/dphi where sqdp, times 1/sin(theta) where sqcsc, 1/r where sqorad),
+    // times coef 0: one, 1: rho(r) / 2, 2: cval (field, dphi, csc, orad unused)
+    int nsq, lin, sqf[3], sqdp[3], sqcsc[3], sqorad[3], coef;
+    double sqc[3], cval;
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);

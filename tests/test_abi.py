@@ -116,7 +116,8 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
                  "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
                  "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36,
-                 "vortp_r": 300 + 4, "vortm_r": 300 + 7,
+                 "vortp_r": 300 + 4, "vortm_r": 300 + 7, "vort_theta": 300 + 2, "vort_phi": 300 + 3,
+                 "vortp_theta": 300 + 5, "vortp_phi": 300 + 6, "vortm_theta": 300 + 8, "vortm_phi": 300 + 9,
                  "entropy_p": 500 + 3, "pressure_p": 500 + 4, "entropy_m": 500 + 5, "pressure_m": 500 + 6,
                  "entropy_p_dr": 500 + 9, "pressure_p_dr": 500 + 10, "entropy_m_dr": 500 + 11,
                  "pressure_m_dr": 500 + 12, "entropy_p_dtheta": 500 + 15, "entropy_m_dtheta": 500 + 17,

@@ -73,14 +73,20 @@ def test_diagnostics_leave_the_run_unchanged(precision):
 _ORACLE_NAME = {"v_r": "vr", "v_theta": "vt", "v_phi": "vp", "dv_r_dr": "dvrdr", "dv_theta_dr": "dvtdr",
                 "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp", "vort_r": "omr",
                 "dv_phi_dp": "dvpdp", "entropy": "t", "entropy_dr": "dtdr", "entropy_dtheta": "dtdt",
-                "entropy_dphi": "dtdp", "pressure": "p", "pressure_dphi": "dpdp", "pressure_dr": "dpdr"}
+                "entropy_dphi": "dtdp", "pressure": "p", "pressure_dphi": "dpdp", "pressure_dr": "dpdr",
+                "vort_theta": "omt", "vort_phi": "omp"}
 
 
 def _oracle_step(o):
     """One oracle step; its physical-space buffer then also holds dP/dr, which the step
-    itself does not form."""
+    itself does not form, and the theta and phi vorticity as Compute_Vorticity_Field forms
+    them from the buffer (Diagnostics_Vorticity_Field.F90)."""
     o.step()
-    o.last_fields.update(o.pressure_fields())
+    f = o.last_fields
+    f.update(o.pressure_fields())
+    csc, orad = o.h.csctheta[:, None, None], (1.0 / o.radius)[None, :, None]
+    f["omt"] = (csc * f["dvrdp"] - f["vp"]) * orad - f["dvpdr"]
+    f["omp"] = f["dvtdr"] + (f["vt"] - f["dvrdt"]) * orad
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -101,7 +107,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
         again = g.shell_slices(["v_r"], [levels[5]])
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_slices([302], [0])                 # vort_theta: not provided
+            g.shell_slices([310], [0])                 # enstrophy: not provided
         with pytest.raises(rb.RayleighError):
             g.shell_slices(["v_r"], [oc.n_r])
     o = O.Oracle(oc)
@@ -132,7 +138,7 @@ def test_shell_averages_match_the_oracle(precision, tol):
         av = g.shell_averages(names)
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_averages([302])
+            g.shell_averages([310])
     o = O.Oracle(oc)
     o.init_state(sw, sz, sab)
     _oracle_step(o)
@@ -363,6 +369,7 @@ _PARTS = {"v_r": ("vp_r", "vm_r"), "v_theta": ("vp_theta", "vm_theta"), "v_phi":
           "dv_phi_dr": ("dvp_phi_dr", "dvm_phi_dr"), "dv_r_dt": ("dvp_r_dt", "dvm_r_dt"),
           "dv_r_dp": ("dvp_r_dp", "dvm_r_dp"), "dv_theta_dp": ("dvp_theta_dp", "dvm_theta_dp"),
           "dv_phi_dp": ("dvp_phi_dp", "dvm_phi_dp"), "vort_r": ("vortp_r", "vortm_r"),
+          "vort_theta": ("vortp_theta", "vortm_theta"), "vort_phi": ("vortp_phi", "vortm_phi"),
           "entropy": ("entropy_p", "entropy_m"), "pressure": ("pressure_p", "pressure_m"),
           "entropy_dr": ("entropy_p_dr", "entropy_m_dr"), "pressure_dr": ("pressure_p_dr", "pressure_m_dr"),
           "entropy_dtheta": ("entropy_p_dtheta", "entropy_m_dtheta"),
@@ -428,7 +435,7 @@ def _check_parts(g, o, names, parts, tol, ptol):
 @pytest.mark.parametrize("precision,tol,ptol", [(0, 1e-12, 1e-12), (1, 1e-9, 1e-8)])
 def test_fluctuating_and_mean_parts_match_the_oracle(precision, tol, ptol):
     """The fluctuating (m > 0) and azimuthal-mean (m = 0) codes of every hydrodynamic quantity
-    (velocity_field_codes.F vp_r = 4 .. dvm_phi_dp = 36, vorticity 304 / 307, thermal 503 ..
+    (velocity_field_codes.F vp_r = 4 .. dvm_phi_dp = 36, vorticity 304-309, thermal 503 ..
     524) in every output family against the field minus its phi average, or that average,
     of the oracle's buffer, on the full quantity's largest magnitude (the pointwise families
     with the meridional slices' mixed bound); the means of phi derivatives are exactly zero."""
@@ -445,7 +452,7 @@ def test_fluctuating_and_mean_parts_match_the_oracle(precision, tol, ptol):
         _oracle_step(o)
         parts = _part_fields(o, _ORACLE_NAME)
         names = [n for n in parts if n not in _ZERO_MEANS]
-        assert len(names) == 31 and all(n in rb.Rayleigh.QUANTITIES for n in parts)
+        assert len(names) == 35 and all(n in rb.Rayleigh.QUANTITIES for n in parts)
         _check_parts(g, o, names, parts, tol, ptol)
         zeros = sorted(_ZERO_MEANS)
         assert not g.shell_slices(zeros, [0, 7]).any() and not g.point_probes(zeros, [3], [5], [9]).any()

@@ -342,6 +342,43 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_JM_THETA    1006
 #define RA_Q_JP_PHI      1008
 #define RA_Q_JM_PHI      1009
+/* Products (Diagnostics_Vorticity_Field.F90): enstrophy and its mean / fluctuating forms, the
+ * squared vorticity components, the kinetic helicity v.omega by component and in total with
+ * the (velocity, vorticity) part pairs pp, mm, mp, pm; with magnetism mean J . J': */
+#define RA_Q_ENSTROPHY              310
+#define RA_Q_ENSTROPHY_PM           311
+#define RA_Q_ENSTROPHY_MM           312
+#define RA_Q_ENSTROPHY_PP           313
+#define RA_Q_VORT_R_SQ              314
+#define RA_Q_VORT_THETA_SQ          315
+#define RA_Q_VORT_PHI_SQ            316
+#define RA_Q_VORTP_R_SQ             317
+#define RA_Q_VORTP_THETA_SQ         318
+#define RA_Q_VORTP_PHI_SQ           319
+#define RA_Q_VORTM_R_SQ             320
+#define RA_Q_VORTM_THETA_SQ         321
+#define RA_Q_VORTM_PHI_SQ           322
+#define RA_Q_KIN_HELICITY_R         324
+#define RA_Q_KIN_HELICITY_THETA     325
+#define RA_Q_KIN_HELICITY_PHI       326
+#define RA_Q_KIN_HELICITY_PP_R      327
+#define RA_Q_KIN_HELICITY_PP_THETA  328
+#define RA_Q_KIN_HELICITY_PP_PHI    329
+#define RA_Q_KIN_HELICITY_MM_R      330
+#define RA_Q_KIN_HELICITY_MM_THETA  331
+#define RA_Q_KIN_HELICITY_MM_PHI    332
+#define RA_Q_KIN_HELICITY_MP_R      333
+#define RA_Q_KIN_HELICITY_MP_THETA  334
+#define RA_Q_KIN_HELICITY_MP_PHI    335
+#define RA_Q_KIN_HELICITY_PM_R      336
+#define RA_Q_KIN_HELICITY_PM_THETA  337
+#define RA_Q_KIN_HELICITY_PM_PHI    338
+#define RA_Q_KIN_HELICITY           339
+#define RA_Q_KIN_HELICITY_PP        340
+#define RA_Q_KIN_HELICITY_MM        341
+#define RA_Q_KIN_HELICITY_MP        342
+#define RA_Q_KIN_HELICITY_PM        343
+#define RA_Q_JPM_SQ                1013
 /* with magnetism, the phi derivatives of B and their parts (the means are zero): */
 #define RA_Q_DB_R_DP           828
 #define RA_Q_DB_THETA_DP       829

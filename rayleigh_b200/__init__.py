@@ -498,38 +498,48 @@ class Rayleigh:
         return dt.value, nch.value
 
     QUANTITIES = {"v_r": 1, "v_theta": 2, "v_phi": 3, "dv_r_dr": 10, "dv_theta_dr": 11, "dv_phi_dr": 12,
-                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 301, "entropy": 501,
-                  "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519, "pressure": 502,
-                  "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802, "b_phi": 803,
-                  "j_r": 1001, "j_theta": 1004, "j_phi": 1007,
+                  "dv_r_dt": 19, "dv_r_dp": 28, "dv_theta_dp": 29, "dv_phi_dp": 30, "vort_r": 301,
+                  "entropy": 501, "entropy_dr": 507, "entropy_dtheta": 513, "entropy_dphi": 519,
+                  "pressure": 502, "pressure_dr": 508, "pressure_dphi": 520, "b_r": 801, "b_theta": 802,
+                  "b_phi": 803, "j_r": 1001, "j_theta": 1004, "j_phi": 1007,
                   # fluctuating (m > 0) and azimuthal-mean (m = 0) parts, the reference's codes
                   "vp_r": 4, "vp_theta": 5, "vp_phi": 6, "vm_r": 7, "vm_theta": 8, "vm_phi": 9,
                   "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
                   "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
                   "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36, "vortp_r": 304,
-                  "vortm_r": 307, "vort_theta": 302, "vort_phi": 303, "vortp_theta": 305,
-                  "vortp_phi": 306, "vortm_theta": 308, "vortm_phi": 309,
-                  "entropy_p": 503, "pressure_p": 504, "entropy_m": 505, "pressure_m": 506,
-                  "entropy_p_dr": 509, "pressure_p_dr": 510, "entropy_m_dr": 511, "pressure_m_dr": 512,
-                  "entropy_p_dtheta": 515, "entropy_m_dtheta": 517, "entropy_p_dphi": 521,
-                  "pressure_p_dphi": 522, "entropy_m_dphi": 523, "pressure_m_dphi": 524,
-                  "bp_r": 804, "bp_theta": 805, "bp_phi": 806, "bm_r": 807, "bm_theta": 808, "bm_phi": 809,
-                  "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005, "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009,
-                  "db_r_dp": 828, "db_theta_dp": 829, "db_phi_dp": 830, "dbp_r_dp": 831, "dbp_theta_dp": 832,
-                  "dbp_phi_dp": 833, "dbm_r_dp": 834, "dbm_theta_dp": 835, "dbm_phi_dp": 836,
+                  "vortm_r": 307, "vort_theta": 302, "vort_phi": 303, "vortp_theta": 305, "vortp_phi": 306,
+                  "vortm_theta": 308, "vortm_phi": 309, "entropy_p": 503, "pressure_p": 504,
+                  "entropy_m": 505, "pressure_m": 506, "entropy_p_dr": 509, "pressure_p_dr": 510,
+                  "entropy_m_dr": 511, "pressure_m_dr": 512, "entropy_p_dtheta": 515,
+                  "entropy_m_dtheta": 517, "entropy_p_dphi": 521, "pressure_p_dphi": 522,
+                  "entropy_m_dphi": 523, "pressure_m_dphi": 524, "bp_r": 804, "bp_theta": 805, "bp_phi": 806,
+                  "bm_r": 807, "bm_theta": 808, "bm_phi": 809, "jp_r": 1002, "jm_r": 1003, "jp_theta": 1005,
+                  "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009, "db_r_dp": 828, "db_theta_dp": 829,
+                  "db_phi_dp": 830, "dbp_r_dp": 831, "dbp_theta_dp": 832, "dbp_phi_dp": 833, "dbm_r_dp": 834,
+                  "dbm_theta_dp": 835, "dbm_phi_dp": 836,
+                  # products: enstrophy, squared vorticity, kinetic helicity, mean J . J'
+                  "enstrophy": 310, "enstrophy_pm": 311, "enstrophy_mm": 312, "enstrophy_pp": 313,
+                  "vort_r_sq": 314, "vort_theta_sq": 315, "vort_phi_sq": 316, "vortp_r_sq": 317,
+                  "vortp_theta_sq": 318, "vortp_phi_sq": 319, "vortm_r_sq": 320, "vortm_theta_sq": 321,
+                  "vortm_phi_sq": 322, "kin_helicity_r": 324, "kin_helicity_theta": 325,
+                  "kin_helicity_phi": 326, "kin_helicity_pp_r": 327, "kin_helicity_pp_theta": 328,
+                  "kin_helicity_pp_phi": 329, "kin_helicity_mm_r": 330, "kin_helicity_mm_theta": 331,
+                  "kin_helicity_mm_phi": 332, "kin_helicity_mp_r": 333, "kin_helicity_mp_theta": 334,
+                  "kin_helicity_mp_phi": 335, "kin_helicity_pm_r": 336, "kin_helicity_pm_theta": 337,
+                  "kin_helicity_pm_phi": 338, "kin_helicity": 339, "kin_helicity_pp": 340,
+                  "kin_helicity_mm": 341, "kin_helicity_mp": 342, "kin_helicity_pm": 343, "jpm_sq": 1013,
                   # sums of squares: kinetic energy densities, v^2, J.J, magnetic energy densities
                   "kinetic_energy": 401, "radial_ke": 402, "theta_ke": 403, "phi_ke": 404,
                   "mkinetic_energy": 405, "radial_mke": 406, "theta_mke": 407, "phi_mke": 408,
-                  "pkinetic_energy": 409, "radial_pke": 410, "theta_pke": 411, "phi_pke": 412,
-                  "vsq": 413, "radial_vsq": 414, "theta_vsq": 415, "phi_vsq": 416, "mvsq": 417,
-                  "radial_mvsq": 418, "theta_mvsq": 419, "phi_mvsq": 420, "pvsq": 421,
-                  "radial_pvsq": 422, "theta_pvsq": 423, "phi_pvsq": 424, "j_sq": 1010, "jp_sq":
-                  1011, "jm_sq": 1012, "j_r_sq": 1014, "jp_r_sq": 1015, "jm_r_sq": 1016,
-                  "j_theta_sq": 1017, "jp_theta_sq": 1018, "jm_theta_sq": 1019, "j_phi_sq": 1020,
-                  "jp_phi_sq": 1021, "jm_phi_sq": 1022, "magnetic_energy": 1101, "radial_me": 1102,
-                  "theta_me": 1103, "phi_me": 1104, "mmagnetic_energy": 1105, "radial_mme": 1106,
-                  "theta_mme": 1107, "phi_mme": 1108, "pmagnetic_energy": 1109, "radial_pme": 1110,
-                  "theta_pme": 1111, "phi_pme": 1112}
+                  "pkinetic_energy": 409, "radial_pke": 410, "theta_pke": 411, "phi_pke": 412, "vsq": 413,
+                  "radial_vsq": 414, "theta_vsq": 415, "phi_vsq": 416, "mvsq": 417, "radial_mvsq": 418,
+                  "theta_mvsq": 419, "phi_mvsq": 420, "pvsq": 421, "radial_pvsq": 422, "theta_pvsq": 423,
+                  "phi_pvsq": 424, "j_sq": 1010, "jp_sq": 1011, "jm_sq": 1012, "j_r_sq": 1014,
+                  "jp_r_sq": 1015, "jm_r_sq": 1016, "j_theta_sq": 1017, "jp_theta_sq": 1018,
+                  "jm_theta_sq": 1019, "j_phi_sq": 1020, "jp_phi_sq": 1021, "jm_phi_sq": 1022,
+                  "magnetic_energy": 1101, "radial_me": 1102, "theta_me": 1103, "phi_me": 1104,
+                  "mmagnetic_energy": 1105, "radial_mme": 1106, "theta_mme": 1107, "phi_mme": 1108,
+                  "pmagnetic_energy": 1109, "radial_pme": 1110, "theta_pme": 1111, "phi_pme": 1112}
 
     def shell_slices(self, quantities, levels):
         """Shell slices of the current state: array [quantity][level][theta][phi] of the

@@ -1571,45 +1571,62 @@ __device__ __forceinline__ int natural_index(int p) {
     return n;
 }
 
+// One buffer-field sum C (DiagCombo) on the row into e[.]: a c2r per term.
+template <int N, int ZPT>
+__device__ __forceinline__ void row_combo(const PhysParams& P, const DiagCombo& C, const double* rowbase, int h,
+                                          double csc, double orad, double2* sm, int t, double2 (&y)[FB][ZPT],
+                                          double2 (&e)[ZPT]) {
+#pragma unroll
+    for (int q = 0; q < ZPT; ++q) e[q] = make_double2(0.0, 0.0);
+#pragma unroll 1
+    for (int j = 0; j < C.nt; ++j) {
+        const DiagTerm T = C.t[j];
+        const int fo[1] = {T.field};
+        const bool dp[1] = {T.dphi != 0};
+        row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, C.mpart);
+        const double cs = T.c * (T.csc ? csc : 1.0) * (T.orad ? orad : 1.0);
+#pragma unroll
+        for (int q = 0; q < ZPT; ++q) {
+            e[q].x += cs * y[0][q].x;
+            e[q].y += cs * y[0][q].y;
+        }
+    }
+}
+
 // The diagnostic quantity S on the row (theta index th, radial index r) into y[0][.]: one
 // field through the c2r (d/dphi in the spectrum, its fluctuating or mean part by mpart), or
-// for the energy and |J|^2 codes the sum of the squares of up to three fields, for the theta
-// and phi vorticity a sum of three fields with coefficients (each field with its own d/dphi,
-// 1/sin(theta), 1/r), times 1, rho(r) / 2 or a constant.  Returns the factor the caller still
-// applies: the single field's 1/sin(theta) and 1/r, 1 for a sum.
+// a sum of products of buffer-field sums (the vorticity components, the energy densities,
+// enstrophy, helicity, J.J: SliceSpec.nprod), times 1, rho(r) / 2 or a constant.  Returns the
+// factor the caller still applies: the single field's 1/sin(theta) and 1/r, 1 for a product.
 template <int N, int ZPT>
 __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceSpec& S, const double* rowbase,
                                                int h, int th, int r, double2* sm, int t, double2 (&y)[FB][ZPT]) {
     const double csc = P.trig[2 * N + th], orad = P.radial[R_OVER_R * P.nr + r];
-    if (S.nsq == 0) {
+    if (S.nprod == 0) {
         const int fo[1] = {S.field};
         const bool dp[1] = {S.dphi != 0};
         row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
         return (S.csc ? csc : 1.0) * (S.orad ? orad : 1.0);
     }
-    double2 acc[ZPT];
+    double2 acc[ZPT], a[ZPT], b[ZPT];
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) acc[q] = make_double2(0.0, 0.0);
 #pragma unroll 1
-    for (int i = 0; i < S.nsq; ++i) {
-        const int fo[1] = {S.sqf[i]};
-        const bool dp[1] = {S.sqdp[i] != 0};
-        row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, S.mpart);
-        const double s = (S.sqcsc[i] ? csc : 1.0) * (S.sqorad[i] ? orad : 1.0);
-        if (S.lin) {
-            const double cs = S.sqc[i] * s;
+    for (int i = 0; i < S.nprod; ++i) {
+        row_combo<N, ZPT>(P, S.a[i], rowbase, h, csc, orad, sm, t, y, a);
+        if (S.bsame[i]) {
 #pragma unroll
-            for (int q = 0; q < ZPT; ++q) {
-                acc[q].x += cs * y[0][q].x;
-                acc[q].y += cs * y[0][q].y;
-            }
+            for (int q = 0; q < ZPT; ++q) b[q] = a[q];
+        } else if (S.b[i].nt == 0) {
+#pragma unroll
+            for (int q = 0; q < ZPT; ++q) b[q] = make_double2(1.0, 1.0);
         } else {
+            row_combo<N, ZPT>(P, S.b[i], rowbase, h, csc, orad, sm, t, y, b);
+        }
 #pragma unroll
-            for (int q = 0; q < ZPT; ++q) {
-                const double a = y[0][q].x * s, b = y[0][q].y * s;
-                acc[q].x += a * a;
-                acc[q].y += b * b;
-            }
+        for (int q = 0; q < ZPT; ++q) {
+            acc[q].x += a[q].x * b[q].x;
+            acc[q].y += a[q].y * b[q].y;
         }
     }
     const double c = S.coef == 1 ? 0.5 * P.radial[R_DENSITY * P.nr + r] : (S.coef == 2 ? S.cval : 1.0);

@@ -1996,107 +1996,141 @@ static const QuantityParts kParts[] = {
     {829, 832, 835},    {830, 833, 836},    {302, 305, 308},    {303, 306, 309},
 };
 
-// Sums of squares (Diagnostics_Energies.F90 Compute_Kinetic_Energy, Compute_Magnetic_Energy;
-// Diagnostics_Current_Density.F90): kinetic_energy_codes.F (keoffset = 400: 1/2 rho v^2 and
-// its r, theta, phi parts 401-404, of the mean flow 405-408, of the fluctuations 409-412; v^2
-// likewise without rho 413-424), magnetic_energy_codes.F (meoffset = 1100: 1/2 Lorentz_Coeff
-// B^2, 1101-1112 in the same order) and current_density_codes.F (J.J 1010, J'.J' 1011,
-// mean J.J 1012; J_r^2, J_theta^2, J_phi^2 with their fluctuating and mean parts 1014-1022).
-struct SquareSource { int code, nsq, f0, f1, f2, mpart, coef; };
-enum { SQ_V = -1, SQ_B = -2, SQ_J = -3 };   // f0 of the three-component sums
-static const SquareSource kSquares[] = {
-    {401, 3, SQ_V, 0, 0, 0, 1}, {402, 1, A_VR, 0, 0, 0, 1}, {403, 1, A_VT, 0, 0, 0, 1}, {404, 1, A_VP, 0, 0, 0, 1},
-    {405, 3, SQ_V, 0, 0, 2, 1}, {406, 1, A_VR, 0, 0, 2, 1}, {407, 1, A_VT, 0, 0, 2, 1}, {408, 1, A_VP, 0, 0, 2, 1},
-    {409, 3, SQ_V, 0, 0, 1, 1}, {410, 1, A_VR, 0, 0, 1, 1}, {411, 1, A_VT, 0, 0, 1, 1}, {412, 1, A_VP, 0, 0, 1, 1},
-    {413, 3, SQ_V, 0, 0, 0, 0}, {414, 1, A_VR, 0, 0, 0, 0}, {415, 1, A_VT, 0, 0, 0, 0}, {416, 1, A_VP, 0, 0, 0, 0},
-    {417, 3, SQ_V, 0, 0, 2, 0}, {418, 1, A_VR, 0, 0, 2, 0}, {419, 1, A_VT, 0, 0, 2, 0}, {420, 1, A_VP, 0, 0, 2, 0},
-    {421, 3, SQ_V, 0, 0, 1, 0}, {422, 1, A_VR, 0, 0, 1, 0}, {423, 1, A_VT, 0, 0, 1, 0}, {424, 1, A_VP, 0, 0, 1, 0},
-    {1101, 3, SQ_B, 0, 0, 0, 2}, {1102, 1, A_BR, 0, 0, 0, 2}, {1103, 1, A_BT, 0, 0, 0, 2}, {1104, 1, A_BP, 0, 0, 0, 2},
-    {1105, 3, SQ_B, 0, 0, 2, 2}, {1106, 1, A_BR, 0, 0, 2, 2}, {1107, 1, A_BT, 0, 0, 2, 2}, {1108, 1, A_BP, 0, 0, 2, 2},
-    {1109, 3, SQ_B, 0, 0, 1, 2}, {1110, 1, A_BR, 0, 0, 1, 2}, {1111, 1, A_BT, 0, 0, 1, 2}, {1112, 1, A_BP, 0, 0, 1, 2},
-    {1010, 3, SQ_J, 0, 0, 0, 0}, {1011, 3, SQ_J, 0, 0, 1, 0}, {1012, 3, SQ_J, 0, 0, 2, 0},
-    {1014, 1, A_CBR, 0, 0, 0, 0}, {1015, 1, A_CBR, 0, 0, 1, 0}, {1016, 1, A_CBR, 0, 0, 2, 0},
-    {1017, 1, A_CBT, 0, 0, 0, 0}, {1018, 1, A_CBT, 0, 0, 1, 0}, {1019, 1, A_CBT, 0, 0, 2, 0},
-    {1020, 1, A_CBP, 0, 0, 0, 0}, {1021, 1, A_CBP, 0, 0, 1, 0}, {1022, 1, A_CBP, 0, 0, 2, 0},
-};
-
-// A squared field's factors: v_theta, v_phi are formed divided by sin(theta); the r sin(theta)
-// B_theta, B_phi and curl B theta, phi fields by r sin(theta) (rsintheta_div)
-static void square_term(SliceSpec& S, int i, int field) {
-    S.sqf[i] = field;
-    S.sqcsc[i] = (field == A_VT || field == A_VP || field == A_BT || field == A_BP || field == A_CBT ||
-                  field == A_CBP) ? 1 : 0;
-    S.sqorad[i] = (field == A_BT || field == A_BP || field == A_CBT || field == A_CBP) ? 1 : 0;
-}
-
 // Sums of fields (Diagnostics_Vorticity_Field.F90 Compute_Vorticity_Field): vort_theta (302)
 // = (csc dv_r/dphi - v_phi) / r - dv_phi/dr, vort_phi (303) = dv_theta/dr + (v_theta -
 // dv_r/dtheta) / r, from the buffer fields as the other codes form them (v_theta, v_phi and
 // their r and theta derivatives divided by sin(theta)).
-struct LinearTerm { int field, dphi, csc, orad; double c; };
-struct LinearSource { int code; LinearTerm t[3]; };
+struct LinearSource { int code; DiagTerm t[3]; };
 static const LinearSource kLinear[] = {
     {302, {{A_VR, 1, 1, 1, 1.0}, {A_VP, 0, 1, 1, -1.0}, {A_DVPDR, 0, 1, 0, -1.0}}},
     {303, {{A_DVTDR, 0, 1, 0, 1.0}, {A_VT, 0, 1, 1, 1.0}, {A_DVRDT, 0, 1, 1, -1.0}}},
 };
 
+// The buffer-field sum of quantity `code` (a row of kQuantities or kLinear), of its part mpart.
+static DiagCombo combo_of(const Ctx& c, int code, int mpart, int asked) {
+    DiagCombo C{};
+    C.mpart = mpart;
+    for (const LinearSource& k : kLinear)
+        if (k.code == code) {
+            C.nt = 3;
+            for (int i = 0; i < 3; ++i) C.t[i] = k.t[i];
+            return C;
+        }
+    for (const QuantitySource& k : kQuantities)
+        if (k.code == code) {
+            if (k.field >= c.nfa)
+                throw ArgError("diagnostics: quantity code " + std::to_string(asked) + " needs magnetism");
+            C.nt = 1;
+            C.t[0] = DiagTerm{k.field, k.dphi, k.csc, k.orad, 1.0};
+            return C;
+        }
+    throw ArgError("diagnostics: quantity code " + std::to_string(asked) + " is not provided");
+}
+
+// Products of vector components (parts: 0 the field, 1 fluctuating, 2 mean), summed over the
+// three components (comp 0) or of one (comp 1..3):
+//   kinetic_energy_codes.F (keoffset = 400): 1/2 rho |v|^2 and its parts 401-404, of the mean
+//     flow 405-408, of the fluctuations 409-412; v^2 likewise without rho 413-424
+//     (Diagnostics_Energies.F90 Compute_Kinetic_Energy);
+//   magnetic_energy_codes.F (meoffset = 1100): 1/2 Lorentz_Coeff |B|^2 in the same order,
+//     1101-1112 (Compute_Magnetic_Energy);
+//   current_density_codes.F: J.J 1010, J'.J' 1011, mean J.J 1012, mean J . J' 1013, J_r^2,
+//     J_theta^2, J_phi^2 each with its fluctuating and mean forms 1014-1022;
+//   vorticity_field_codes.F (vort_off = 300): enstrophy 310, omega'.mean omega 311, of the
+//     mean 312, of the fluctuations 313; omega_r^2, omega_theta^2, omega_phi^2 314-316, of the
+//     fluctuations 317-319, of the means 320-322; kinetic helicity v_i omega_i 324-326 and its
+//     (v, omega) parts (fluct, fluct) 327-329, (mean, mean) 330-332, (mean, fluct) 333-335,
+//     (fluct, mean) 336-338; v.omega 339 and the same four part pairs 340-343
+//     (Diagnostics_Vorticity_Field.F90).
+struct Product { const int* a; int apart; const int* b; int bpart; int comp, coef; bool square; };
+static const int kVelocity[3] = {1, 2, 3}, kVorticity[3] = {301, 302, 303}, kBfield[3] = {801, 802, 803},
+                 kCurrent[3] = {1001, 1004, 1007};
+static bool product_of(int code, Product& p) {
+    static const int kGroupPart[3] = {0, 2, 1};   // field, mean, fluctuations
+    if (code >= 401 && code <= 424) {
+        const int k = code - 401, g = k / 4;
+        p = Product{kVelocity, kGroupPart[g % 3], kVelocity, kGroupPart[g % 3], k % 4, g < 3 ? 1 : 0, true};
+        return true;
+    }
+    if (code >= 1101 && code <= 1112) {
+        const int k = code - 1101, g = k / 4;
+        p = Product{kBfield, kGroupPart[g], kBfield, kGroupPart[g], k % 4, 2, true};
+        return true;
+    }
+    if (code >= 1010 && code <= 1013) {
+        static const int ap[4] = {0, 1, 2, 2}, bp[4] = {0, 1, 2, 1};
+        const int k = code - 1010;
+        p = Product{kCurrent, ap[k], kCurrent, bp[k], 0, 0, k < 3};
+        return true;
+    }
+    if (code >= 1014 && code <= 1022) {
+        const int k = code - 1014;
+        p = Product{kCurrent, k % 3, kCurrent, k % 3, k / 3 + 1, 0, true};
+        return true;
+    }
+    if (code >= 310 && code <= 313) {
+        static const int ap[4] = {0, 1, 2, 1}, bp[4] = {0, 2, 2, 1};
+        const int k = code - 310;
+        p = Product{kVorticity, ap[k], kVorticity, bp[k], 0, 0, k != 1};
+        return true;
+    }
+    if (code >= 314 && code <= 322) {
+        static const int part[3] = {0, 1, 2};
+        const int k = code - 314;
+        p = Product{kVorticity, part[k / 3], kVorticity, part[k / 3], k % 3 + 1, 0, true};
+        return true;
+    }
+    if (code >= 324 && code <= 343) {   // (velocity part, vorticity part) per group
+        static const int vp[5] = {0, 1, 2, 2, 1}, wp[5] = {0, 1, 2, 1, 2};
+        const int k = code - 324;
+        const int g = k < 15 ? k / 3 : k - 15, comp = k < 15 ? k % 3 + 1 : 0;
+        p = Product{kVelocity, vp[g], kVorticity, wp[g], comp, 0, false};
+        return true;
+    }
+    return false;
+}
+
 static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities, int nq) {
     std::vector<SliceSpec> spec(nq);
     for (int q = 0; q < nq; ++q) {
-        const SquareSource* sq = nullptr;
-        for (const SquareSource& k : kSquares)
-            if (k.code == quantities[q]) sq = &k;
-        if (sq) {
+        const int asked = quantities[q];
+        Product pr;
+        if (product_of(asked, pr)) {
             SliceSpec S{};
-            S.nsq = sq->nsq;
-            if (sq->nsq == 3) {
-                static const int kV[3] = {A_VR, A_VT, A_VP}, kB[3] = {A_BR, A_BT, A_BP},
-                                 kJ[3] = {A_CBR, A_CBT, A_CBP};
-                const int* tri = sq->f0 == SQ_V ? kV : (sq->f0 == SQ_B ? kB : kJ);
-                for (int i = 0; i < 3; ++i) square_term(S, i, tri[i]);
-            } else {
-                square_term(S, 0, sq->f0);
+            S.nprod = pr.comp ? 1 : 3;
+            for (int i = 0; i < S.nprod; ++i) {
+                const int j = pr.comp ? pr.comp - 1 : i;
+                S.a[i] = combo_of(c, pr.a[j], pr.apart, asked);
+                S.bsame[i] = pr.square ? 1 : 0;
+                if (!pr.square) S.b[i] = combo_of(c, pr.b[j], pr.bpart, asked);
             }
-            for (int i = 0; i < S.nsq; ++i)
-                if (S.sqf[i] >= c.nfa)
-                    throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
-            S.field = S.sqf[0];
-            S.mpart = sq->mpart;
-            S.coef = sq->coef;
+            S.field = S.a[0].t[0].field;
+            S.coef = pr.coef;
             S.cval = 0.5 * c.rad.lorentz;   // magnetic_energy: 1/2 Lorentz_Coeff
             spec[q] = S;
             continue;
         }
-        int code = quantities[q], mpart = 0;
+        int code = asked, mpart = 0;
         for (const QuantityParts& p : kParts) {
             if (p.fluct == code) { code = p.full; mpart = 1; break; }
             if (p.mean == code) { code = p.full; mpart = 2; break; }
         }
-        const LinearSource* ls = nullptr;
-        for (const LinearSource& k : kLinear)
-            if (k.code == code) ls = &k;
-        if (ls) {
+        bool linear = false;
+        for (const LinearSource& k : kLinear) linear |= k.code == code;
+        if (linear) {   // nprod 1 with b the constant 1
             SliceSpec S{};
-            S.nsq = 3;
-            S.lin = 1;
-            for (int i = 0; i < 3; ++i) {
-                S.sqf[i] = ls->t[i].field;
-                S.sqdp[i] = ls->t[i].dphi;
-                S.sqcsc[i] = ls->t[i].csc;
-                S.sqorad[i] = ls->t[i].orad;
-                S.sqc[i] = ls->t[i].c;
-            }
-            S.field = S.sqf[0];
-            S.mpart = mpart;
+            S.nprod = 1;
+            S.a[0] = combo_of(c, code, mpart, asked);
+            S.field = S.a[0].t[0].field;
             spec[q] = S;
             continue;
         }
         const QuantitySource* src = nullptr;
         for (const QuantitySource& k : kQuantities)
             if (k.code == code) src = &k;
-        if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " is not provided");
+        if (!src) throw ArgError("diagnostics: quantity code " + std::to_string(asked) + " is not provided");
         if (src->field >= c.nfa)
-            throw ArgError("diagnostics: quantity code " + std::to_string(quantities[q]) + " needs magnetism");
+            throw ArgError("diagnostics: quantity code " + std::to_string(asked) + " needs magnetism");
         if (src->pressure && (c.cfg.reference_type != 1 || c.custom_reference))   // the anelastic state holds P / rho
             throw ArgError("diagnostics: the pressure codes are provided for the Boussinesq reference only");
         spec[q] = SliceSpec{};

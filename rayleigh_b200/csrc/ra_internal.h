@@ -253,17 +253,24 @@ void launch_rlm_a(Ctx& c);
 void launch_physics(Ctx& c);
 void launch_kinetic_energy(Ctx& c, bool magnetic = false);
 // one diagnostic quantity on the phi grid at up to MAXL radial levels
+// A diagnostic quantity's buffer-field sum: sum over j < nt of c x field (d/dphi where dphi,
+// times 1/sin(theta) where csc, 1/r where orad), of the part mpart (0 the field, 1 its
+// fluctuations, m > 0, 2 its azimuthal mean, m = 0); nt = 0: the constant 1.
+struct DiagTerm { int field, dphi, csc, orad; double c; };
+struct DiagCombo { int nt, mpart; DiagTerm t[3]; };
+
 struct SliceSpec {
     static constexpr int MAXL = 64;
     int field, dphi, csc, nl;   // p2a field, d/dphi, times 1/sin(theta), levels in this launch
     int pressure;               // formed with the P grid in T's place (pressure quantities)
     int orad;                   // times 1/r (the r sin(theta) B_theta, B_phi fields)
     int mpart;                  // 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean
-    // nsq > 0: the sum of the squares (lin = 0) or the sum sqc[i] x (lin = 1) of the fields
-    // sqf[0..nsq) (each d/dphi where sqdp, times 1/sin(theta) where sqcsc, 1/r where sqorad),
-    // times coef 0: one, 1: rho(r) / 2, 2: cval (field, dphi, csc, orad unused)
-    int nsq, lin, sqf[3], sqdp[3], sqcsc[3], sqorad[3], coef;
-    double sqc[3], cval;
+    // nprod > 0: coef x sum over i < nprod of a[i] b[i] (b[i] = a[i] where bsame[i], the
+    // constant 1 where b[i].nt = 0), coef 0: one, 1: rho(r) / 2, 2: cval (field, dphi, csc,
+    // orad and mpart then unused)
+    int nprod, bsame[3], coef;
+    double cval;
+    DiagCombo a[3], b[3];
     int level[MAXL];            // radial indices
 };
 void launch_shell_slice(Ctx& c, const SliceSpec& S, double* out);

@@ -145,6 +145,21 @@ def test_diagnostic_quantity_codes_are_the_references():
                       "phi_me": 1100 + 4, "mmagnetic_energy": 1100 + 5, "radial_mme": 1100 + 6,
                       "theta_mme": 1100 + 7, "phi_mme": 1100 + 8, "pmagnetic_energy": 1100 + 9,
                       "radial_pme": 1100 + 10, "theta_pme": 1100 + 11, "phi_pme": 1100 + 12})
+    # vorticity_field_codes.F: enstrophy = vort_off + 10 ... kin_helicity_pm = vort_off + 43
+    reference.update({"enstrophy": 300 + 10, "enstrophy_pm": 300 + 11, "enstrophy_mm": 300 + 12,
+                      "enstrophy_pp": 300 + 13, "vort_r_sq": 300 + 14, "vort_theta_sq": 300 + 15,
+                      "vort_phi_sq": 300 + 16, "vortp_r_sq": 300 + 17, "vortp_theta_sq": 300 + 18,
+                      "vortp_phi_sq": 300 + 19, "vortm_r_sq": 300 + 20, "vortm_theta_sq": 300 + 21,
+                      "vortm_phi_sq": 300 + 22, "kin_helicity_r": 300 + 24, "kin_helicity_theta": 300 + 25,
+                      "kin_helicity_phi": 300 + 26, "kin_helicity_pp_r": 300 + 27,
+                      "kin_helicity_pp_theta": 300 + 28, "kin_helicity_pp_phi": 300 + 29,
+                      "kin_helicity_mm_r": 300 + 30, "kin_helicity_mm_theta": 300 + 31,
+                      "kin_helicity_mm_phi": 300 + 32, "kin_helicity_mp_r": 300 + 33,
+                      "kin_helicity_mp_theta": 300 + 34, "kin_helicity_mp_phi": 300 + 35,
+                      "kin_helicity_pm_r": 300 + 36, "kin_helicity_pm_theta": 300 + 37,
+                      "kin_helicity_pm_phi": 300 + 38, "kin_helicity": 300 + 39,
+                      "kin_helicity_pp": 300 + 40, "kin_helicity_mm": 300 + 41,
+                      "kin_helicity_mp": 300 + 42, "kin_helicity_pm": 300 + 43, "jpm_sq": 1000 + 13})
     assert header == reference
     lib = rb.load_library()
     ke = ctypes.c_double()

@@ -82,8 +82,12 @@ def _oracle_step(o):
     itself does not form, and the theta and phi vorticity as Compute_Vorticity_Field forms
     them from the buffer (Diagnostics_Vorticity_Field.F90)."""
     o.step()
+    o.last_fields.update(o.pressure_fields())
+    _add_vorticity(o)
+
+
+def _add_vorticity(o):
     f = o.last_fields
-    f.update(o.pressure_fields())
     csc, orad = o.h.csctheta[:, None, None], (1.0 / o.radius)[None, :, None]
     f["omt"] = (csc * f["dvrdp"] - f["vp"]) * orad - f["dvpdr"]
     f["omp"] = f["dvtdr"] + (f["vt"] - f["dvrdt"]) * orad
@@ -107,7 +111,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
         again = g.shell_slices(["v_r"], [levels[5]])
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_slices([310], [0])                 # enstrophy: not provided
+            g.shell_slices([323], [0])                 # zstream: not provided
         with pytest.raises(rb.RayleighError):
             g.shell_slices(["v_r"], [oc.n_r])
     o = O.Oracle(oc)
@@ -138,7 +142,7 @@ def test_shell_averages_match_the_oracle(precision, tol):
         av = g.shell_averages(names)
         sw, sz, sab = g.get_state()
         with pytest.raises(rb.RayleighError):
-            g.shell_averages([310])
+            g.shell_averages([323])
     o = O.Oracle(oc)
     o.init_state(sw, sz, sab)
     _oracle_step(o)
@@ -463,7 +467,8 @@ def _square_fields(o, kind):
     (Compute_Kinetic_Energy, Compute_Magnetic_Energy, Compute_J_Components): the fields, their
     phi means (m0_values) or the fluctuations (fbuffer), squared and summed, times rho / 2
     (kinetic energy), Lorentz_Coeff / 2 (magnetic energy) or 1; added to last_fields too."""
-    comps = {"v": ("vr", "vt", "vp"), "b": ("br", "bt", "bp"), "j": ("curlbr", "curlbt", "curlbp")}
+    comps = {"v": ("vr", "vt", "vp"), "b": ("br", "bt", "bp"), "j": ("curlbr", "curlbt", "curlbp"),
+             "w": ("omr", "omt", "omp")}
     if kind == "hydro":
         fams = [("v", 0.5 * o.density[None, :, None], ("kinetic_energy", "radial_ke", "theta_ke", "phi_ke"),
                  ("mkinetic_energy", "radial_mke", "theta_mke", "phi_mke"),
@@ -477,27 +482,53 @@ def _square_fields(o, kind):
                 ("j", 1.0, ("j_sq", "j_r_sq", "j_theta_sq", "j_phi_sq"), ("jm_sq", "jm_r_sq", "jm_theta_sq",
                  "jm_phi_sq"), ("jp_sq", "jp_r_sq", "jp_theta_sq", "jp_phi_sq"))]
     out = {}
-    for comp, fac, full_names, mean_names, fluct_names in fams:
+
+    def parts_of(comp):
         fields = [o.last_fields[k] for k in comps[comp]]
         means = [np.broadcast_to(q.mean(axis=2, keepdims=True), q.shape) for q in fields]
-        parts = {"full": fields, "mean": means, "fluct": [q - m for q, m in zip(fields, means)]}
+        return {"full": fields, "mean": means, "fluct": [q - m for q, m in zip(fields, means)]}
+
+    def put(name, val, scale_name):
+        o.last_fields[name] = np.ascontiguousarray(val)
+        out[name] = [o.last_fields[name], None, scale_name]
+
+    for comp, fac, full_names, mean_names, fluct_names in fams:
+        parts = parts_of(comp)
         for which, names in (("full", full_names), ("mean", mean_names), ("fluct", fluct_names)):
             for i, name in enumerate(names):
                 terms = parts[which] if i == 0 else [parts[which][i - 1]]
-                val = fac * sum(t * t for t in terms)
-                o.last_fields[name] = np.ascontiguousarray(val)
-                out[name] = [o.last_fields[name], None, full_names[i]]
-    for v in out.values():
-        v[1] = o.last_fields[v[2]]
-    return {k: tuple(v) for k, v in out.items()}
+                put(name, fac * sum(t * t for t in terms), full_names[i])
+    if kind == "hydro":   # Compute_Vorticity_Field: enstrophy, squared vorticity, kinetic helicity
+        w, v = parts_of("w"), parts_of("v")
+        put("enstrophy", sum(x * x for x in w["full"]), "enstrophy")
+        put("enstrophy_pm", sum(x * y for x, y in zip(w["fluct"], w["mean"])), "enstrophy")
+        put("enstrophy_mm", sum(x * x for x in w["mean"]), "enstrophy")
+        put("enstrophy_pp", sum(x * x for x in w["fluct"]), "enstrophy")
+        for i, c in enumerate(("r", "theta", "phi")):
+            put(f"vort_{c}_sq", w["full"][i] ** 2, f"vort_{c}_sq")
+            put(f"vortp_{c}_sq", w["fluct"][i] ** 2, f"vort_{c}_sq")
+            put(f"vortm_{c}_sq", w["mean"][i] ** 2, f"vort_{c}_sq")
+        pairs = {"": ("full", "full"), "_pp": ("fluct", "fluct"), "_mm": ("mean", "mean"),
+                 "_mp": ("mean", "fluct"), "_pm": ("fluct", "mean")}
+        for suf, (pv, pw) in pairs.items():
+            for i, c in enumerate(("r", "theta", "phi")):
+                put(f"kin_helicity{suf}_{c}", v[pv][i] * w[pw][i], f"kin_helicity_{c}")
+            put(f"kin_helicity{suf}", sum(x * y for x, y in zip(v[pv], w[pw])), "kin_helicity")
+    else:
+        j = parts_of("j")
+        put("jpm_sq", sum(x * y for x, y in zip(j["mean"], j["fluct"])), "j_sq")
+    for val in out.values():
+        val[1] = o.last_fields[val[2]]
+    return {k: tuple(val) for k, val in out.items()}
 
 
 @pytest.mark.parametrize("precision,tol,ptol", [(0, 1e-12, 1e-12), (1, 1e-9, 1e-8)])
 def test_energy_densities_match_the_oracle(precision, tol, ptol):
-    """The sums of squares in every output family (kinetic_energy_codes.F 401-424 on the
-    anelastic polytrope, where rho varies with radius; with magnetism magnetic_energy_codes.F
-    1101-1112 and the J.J codes 1010-1012, 1014-1022) against the oracle's buffer, on the
-    largest magnitude of the full (not the mean or fluctuating) sum."""
+    """The products in every output family (kinetic_energy_codes.F 401-424 on the anelastic
+    polytrope, where rho varies with radius, with the enstrophy, squared vorticity and kinetic
+    helicity codes 310-322, 324-343 of vorticity_field_codes.F; with magnetism
+    magnetic_energy_codes.F 1101-1112 and the J.J codes 1010-1022) against the oracle's buffer,
+    on the largest magnitude of the full (not the mean or fluctuating) product."""
     import rayleigh_b200 as rb
     anel = dict(n_r=24, l_max=15, dt=1e-4, reference_type=3, poly_n=2.0, poly_nrho=3.0, modified_rayleigh=0.5,
                 ekman=1e-3, prandtl=1.0, magnetic_prandtl=2.0, no_slip_top=False, no_slip_bottom=False)
@@ -520,8 +551,9 @@ def test_energy_densities_match_the_oracle(precision, tol, ptol):
             else:
                 o.init_state(sw, sz, sab)
             o.step()
+            _add_vorticity(o)
             sq = _square_fields(o, kind)
-            assert len(sq) == 24 and all(n in rb.Rayleigh.QUANTITIES for n in sq)
+            assert len(sq) == (57 if kind == "hydro" else 25) and all(n in rb.Rayleigh.QUANTITIES for n in sq)
             _check_parts(g, o, list(sq), sq, tol, ptol)
             if kind == "hydro":
                 with pytest.raises(rb.RayleighError) as ei:

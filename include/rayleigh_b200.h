@@ -379,6 +379,13 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_KIN_HELICITY_MP        342
 #define RA_Q_KIN_HELICITY_PM        343
 #define RA_Q_JPM_SQ                1013
+/* thermal_energy_codes.F: rho T S of the reference state, its parts and their squares: */
+#define RA_Q_THERMAL_ENERGY_FULL    701
+#define RA_Q_THERMAL_ENERGY_P       702
+#define RA_Q_THERMAL_ENERGY_M       703
+#define RA_Q_THERMAL_ENERGY_SQ      707
+#define RA_Q_THERMAL_ENERGYP_SQ     708
+#define RA_Q_THERMAL_ENERGYM_SQ     709
 /* with magnetism, the phi derivatives of B and their parts (the means are zero): */
 #define RA_Q_DB_R_DP           828
 #define RA_Q_DB_THETA_DP       829

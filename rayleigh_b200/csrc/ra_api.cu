@@ -682,6 +682,7 @@ static std::vector<double> radial_table(const Ctx& c) {
         rp[R_OVER_RSQ * nr + i] = oor2;
         rp[R_VISC_HEAT * nr + i] = c.rad.visc_heat[i];
         rp[R_OHM_HEAT * nr + i] = c.rad.ohm_heat[i];
+        rp[R_RHO_T * nr + i] = c.rad.density[i] * c.rad.temperature[i];
     }
     return rp;
 }
@@ -2042,11 +2043,20 @@ static DiagCombo combo_of(const Ctx& c, int code, int mpart, int asked) {
 //     (v, omega) parts (fluct, fluct) 327-329, (mean, mean) 330-332, (mean, fluct) 333-335,
 //     (fluct, mean) 336-338; v.omega 339 and the same four part pairs 340-343
 //     (Diagnostics_Vorticity_Field.F90).
+//   thermal_energy_codes.F (teoffset = 700): rho T S of the reference state and its
+//     fluctuating and mean parts 701-703, their squares 707-709 (Diagnostics_Thermal_Energies.F90
+//     Compute_Thermal_Energy); b = nullptr: the constant 1.
 struct Product { const int* a; int apart; const int* b; int bpart; int comp, coef; bool square; };
 static const int kVelocity[3] = {1, 2, 3}, kVorticity[3] = {301, 302, 303}, kBfield[3] = {801, 802, 803},
-                 kCurrent[3] = {1001, 1004, 1007};
+                 kCurrent[3] = {1001, 1004, 1007}, kEntropy[1] = {501};
 static bool product_of(int code, Product& p) {
     static const int kGroupPart[3] = {0, 2, 1};   // field, mean, fluctuations
+    if ((code >= 701 && code <= 703) || (code >= 707 && code <= 709)) {
+        const bool sq = code >= 707;
+        const int part = sq ? code - 707 : code - 701;   // 0 field, 1 fluctuations, 2 mean
+        p = Product{kEntropy, part, sq ? kEntropy : nullptr, part, 1, sq ? 4 : 3, sq};
+        return true;
+    }
     if (code >= 401 && code <= 424) {
         const int k = code - 401, g = k / 4;
         p = Product{kVelocity, kGroupPart[g % 3], kVelocity, kGroupPart[g % 3], k % 4, g < 3 ? 1 : 0, true};
@@ -2098,11 +2108,13 @@ static std::vector<SliceSpec> quantity_specs(const Ctx& c, const int* quantities
         if (product_of(asked, pr)) {
             SliceSpec S{};
             S.nprod = pr.comp ? 1 : 3;
+            if (pr.coef >= 3 && c.custom_reference)   // ra_set_reference gives no temperature
+                throw ArgError("diagnostics: the thermal energy codes need the library's own reference state");
             for (int i = 0; i < S.nprod; ++i) {
                 const int j = pr.comp ? pr.comp - 1 : i;
                 S.a[i] = combo_of(c, pr.a[j], pr.apart, asked);
                 S.bsame[i] = pr.square ? 1 : 0;
-                if (!pr.square) S.b[i] = combo_of(c, pr.b[j], pr.bpart, asked);
+                if (!pr.square && pr.b) S.b[i] = combo_of(c, pr.b[j], pr.bpart, asked);
             }
             S.field = S.a[0].t[0].field;
             S.coef = pr.coef;

@@ -241,7 +241,7 @@ constexpr int RA_STATUS_NONFINITE = 2;   // a NaN/Inf reached the right-hand sid
 
 // radial profile packing in d_radial: index k * nr + r
 enum { R_RADIUS, R_OVER_R, R_DELTA_R, R_DENSITY, R_DLNRHO, R_OVER_RHOR, R_OVER_RHORSQ, R_DRHO_TERM, R_TWO_OVER_R,
-       R_OVER_RSQ, R_VISC_HEAT, R_OHM_HEAT, R_COUNT };
+       R_OVER_RSQ, R_VISC_HEAT, R_OHM_HEAT, R_RHO_T, R_COUNT };   // R_RHO_T: rho T of the reference state
 
 // ---- kernels / launchers (defined in the .cu files) ----
 void launch_plm(Ctx& c, const double* d_x, const double* d_w);
@@ -266,8 +266,8 @@ struct SliceSpec {
     int orad;                   // times 1/r (the r sin(theta) B_theta, B_phi fields)
     int mpart;                  // 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean
     // nprod > 0: coef x sum over i < nprod of a[i] b[i] (b[i] = a[i] where bsame[i], the
-    // constant 1 where b[i].nt = 0), coef 0: one, 1: rho(r) / 2, 2: cval (field, dphi, csc,
-    // orad and mpart then unused)
+    // constant 1 where b[i].nt = 0), coef 0: one, 1: rho(r) / 2, 2: cval, 3: rho(r) T(r),
+    // 4: (rho(r) T(r))^2 (field, dphi, csc, orad and mpart then unused)
     int nprod, bsame[3], coef;
     double cval;
     DiagCombo a[3], b[3];

@@ -145,6 +145,9 @@ def test_diagnostic_quantity_codes_are_the_references():
                       "phi_me": 1100 + 4, "mmagnetic_energy": 1100 + 5, "radial_mme": 1100 + 6,
                       "theta_mme": 1100 + 7, "phi_mme": 1100 + 8, "pmagnetic_energy": 1100 + 9,
                       "radial_pme": 1100 + 10, "theta_pme": 1100 + 11, "phi_pme": 1100 + 12})
+    # thermal_energy_codes.F: teoffset = pt_off + 200
+    reference.update({"thermal_energy_full": 700 + 1, "thermal_energy_p": 700 + 2, "thermal_energy_m": 700 + 3,
+                      "thermal_energy_sq": 700 + 7, "thermal_energyp_sq": 700 + 8, "thermal_energym_sq": 700 + 9})
     # vorticity_field_codes.F: enstrophy = vort_off + 10 ... kin_helicity_pm = vort_off + 43
     reference.update({"enstrophy": 300 + 10, "enstrophy_pm": 300 + 11, "enstrophy_mm": 300 + 12,
                       "enstrophy_pp": 300 + 13, "vort_r_sq": 300 + 14, "vort_theta_sq": 300 + 15,

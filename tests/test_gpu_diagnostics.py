@@ -510,6 +510,13 @@ def _square_fields(o, kind):
             put(f"vortm_{c}_sq", w["mean"][i] ** 2, f"vort_{c}_sq")
         pairs = {"": ("full", "full"), "_pp": ("fluct", "fluct"), "_mm": ("mean", "mean"),
                  "_mp": ("mean", "fluct"), "_pm": ("fluct", "mean")}
+        rt = (o.density * o.temperature)[None, :, None]   # Compute_Thermal_Energy: rho T S
+        S = o.last_fields["t"]
+        Sm = np.broadcast_to(S.mean(axis=2, keepdims=True), S.shape)
+        for name, x in (("thermal_energy_full", S), ("thermal_energy_p", S - Sm), ("thermal_energy_m", Sm)):
+            put(name, rt * x, "thermal_energy_full")
+        for name, x in (("thermal_energy_sq", S), ("thermal_energyp_sq", S - Sm), ("thermal_energym_sq", Sm)):
+            put(name, (rt * x) ** 2, "thermal_energy_sq")
         for suf, (pv, pw) in pairs.items():
             for i, c in enumerate(("r", "theta", "phi")):
                 put(f"kin_helicity{suf}_{c}", v[pv][i] * w[pw][i], f"kin_helicity_{c}")
@@ -526,7 +533,8 @@ def _square_fields(o, kind):
 def test_energy_densities_match_the_oracle(precision, tol, ptol):
     """The products in every output family (kinetic_energy_codes.F 401-424 on the anelastic
     polytrope, where rho varies with radius, with the enstrophy, squared vorticity and kinetic
-    helicity codes 310-322, 324-343 of vorticity_field_codes.F; with magnetism
+    helicity codes 310-322, 324-343 of vorticity_field_codes.F and the thermal energy rho T S
+    701-703, 707-709 of thermal_energy_codes.F; with magnetism
     magnetic_energy_codes.F 1101-1112 and the J.J codes 1010-1022) against the oracle's buffer,
     on the largest magnitude of the full (not the mean or fluctuating) product."""
     import rayleigh_b200 as rb
@@ -553,7 +561,7 @@ def test_energy_densities_match_the_oracle(precision, tol, ptol):
             o.step()
             _add_vorticity(o)
             sq = _square_fields(o, kind)
-            assert len(sq) == (57 if kind == "hydro" else 25) and all(n in rb.Rayleigh.QUANTITIES for n in sq)
+            assert len(sq) == (63 if kind == "hydro" else 25) and all(n in rb.Rayleigh.QUANTITIES for n in sq)
             _check_parts(g, o, list(sq), sq, tol, ptol)
             if kind == "hydro":
                 with pytest.raises(rb.RayleighError) as ei:

@@ -116,25 +116,29 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) cheb_synthesis_kernel(const d
 }
 
 // The finite-difference radial mode's synthesis: the state holds grid values, and every grid
-// output is one banded matrix (I, D_1, D_2, D_3 of Finite_Difference.F90, or D_1 D_1 for the
+// output is one banded operator (I, D_1, D_2, D_3 of Finite_Difference.F90, or D_1 D_1 for the
 // deriv_cluge plane) applied to a field's radial columns (d_by_dx3d3, Post_Solve_FD,
-// Sphere_Spectral_Space.F90:37-176), on the FP64 tensor-core tile engine, all outputs in one
-// launch (grid z = output).
+// Sphere_Spectral_Space.F90:37-176).  Each output point is its row's stencil (at most fd_w
+// coefficients) against the column: one thread per point, r fastest, so that the column
+// reads and the plane writes are coalesced and each field is read from HBM about once; all
+// outputs in one launch (grid y = output).
 struct FdOuts {
     int n;
     int o[NG_MAG + 1], var[NG_MAG + 1], mat[NG_MAG + 1];
 };
 
-__global__ void __launch_bounds__(GEMM_THREADS) fd_synthesis_kernel(const double* __restrict__ Dfd,
-                                                                    const double* __restrict__ sol_wpt,
-                                                                    const double* __restrict__ sol_z,
-                                                                    const double* __restrict__ sol_c,
-                                                                    const double* __restrict__ sol_a,
-                                                                    double* __restrict__ g, int nr, long ncols,
-                                                                    FdOuts outs) {
-    __shared__ GemmSmem sm;
-    const int oi = blockIdx.z;
+__global__ void __launch_bounds__(256) fd_synthesis_kernel(const double* __restrict__ band, int w,
+                                                           const double* __restrict__ sol_wpt,
+                                                           const double* __restrict__ sol_z,
+                                                           const double* __restrict__ sol_c,
+                                                           const double* __restrict__ sol_a,
+                                                           double* __restrict__ g, int nr, long ncols, FdOuts outs) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (column, r), r fastest
+    if (i >= ncols * nr) return;
+    const int oi = blockIdx.y;
     const int var = outs.var[oi];
+    const long col = i / nr;
+    const int r = (int)(i - col * nr);
     const double* src;
     long cstride;
     if (var < 3) {
@@ -144,26 +148,12 @@ __global__ void __launch_bounds__(GEMM_THREADS) fd_synthesis_kernel(const double
         src = var == 3 ? sol_z : (var == 4 ? sol_c : sol_a);
         cstride = nr;
     }
-    const double* M = Dfd + (long)outs.mat[oi] * nr * nr;
-    double* out = g + (long)outs.o[oi] * ncols * nr;
-    const int r0 = blockIdx.y * Sq::BM;
-    const long c0 = (long)blockIdx.x * Sq::BN;
-    auto fa = [&](int k, int x) -> double {   // M(r0 + x, k)
-        const int rr = r0 + x;
-        return (k < nr && rr < nr) ? __ldg(M + (long)rr * nr + k) : 0.0;
-    };
-    auto fb = [&](int k, int y) -> double {   // the field's value at radius k of column c0 + y
-        const long col = c0 + y;
-        return (k < nr && col < ncols) ? __ldg(src + col * cstride + k) : 0.0;
-    };
-    Acc acc;
-    acc.zero();
-    gemm_tile<false, false>(acc, fa, fb, nr, sm);
-    acc_foreach(acc, [&](int x, int y, double v) {
-        const int rr = r0 + x;
-        const long col = c0 + y;
-        if (rr < nr && col < ncols) out[col * nr + rr] = v;
-    });
+    const double* row = band + ((long)outs.mat[oi] * nr + r) * (w + 1);
+    const int first = (int)__ldg(row);   // first + w <= nr
+    const double* x = src + col * cstride + first;
+    double s = 0.0;
+    for (int j = 0; j < w; ++j) s += __ldg(row + 1 + j) * __ldg(x + j);
+    g[(long)outs.o[oi] * ncols * nr + i] = s;
 }
 
 static void launch_fd_synthesis(Ctx& c) {
@@ -184,9 +174,10 @@ static void launch_fd_synthesis(Ctx& c) {
         for (int d = 0; d < 3; ++d) add(G_A0 + d, 5, d);
     }
     add(c.ng, 0, 4);   // the deriv_cluge plane: D_1 D_1 W
-    dim3 grid((unsigned)((ncols + Sq::BN - 1) / Sq::BN), (unsigned)((c.d.nr + Sq::BM - 1) / Sq::BM), outs.n);
-    fd_synthesis_kernel<<<grid, GEMM_THREADS, 0, c.stream>>>(c.d_Dfd, c.d_sol_wpt, c.d_sol_z, c.d_sol_c, c.d_sol_a,
-                                                             c.d_g, c.d.nr, ncols, outs);
+    const long total = ncols * c.d.nr;
+    dim3 grid((unsigned)((total + 255) / 256), (unsigned)outs.n);
+    fd_synthesis_kernel<<<grid, 256, 0, c.stream>>>(c.d_Dfd, c.fd_w, c.d_sol_wpt, c.d_sol_z, c.d_sol_c, c.d_sol_a,
+                                                    c.d_g, c.d.nr, ncols, outs);
     RA_CUDA(cudaGetLastError());
     ++c.launches;
 }

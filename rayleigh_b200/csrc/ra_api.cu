@@ -845,19 +845,46 @@ static void setup(Ctx& c) {
         RA_CUDA(cudaStreamSynchronize(c.stream));
     }
     if (!c.cfg.chebyshev) {
-        // the finite-difference synthesis matrices [I, D_1, D_2, D_3, D_1 D_1]
+        // the finite-difference synthesis operators [I, D_1, D_2, D_3, D_1 D_1] as bands: each row's
+        // nonzero stencil (Generate_Coefs' 5 points, one-sided at the ends; 9 for D_1 D_1) held as
+        // its first column and fd_w coefficients, the first column moved left near the bottom
+        // boundary so that the fd_w columns stay on the grid (the extra coefficients are zeros)
         const size_t nn = (size_t)nr * nr;
         std::vector<double> fdm(5 * nn, 0.0);
         std::copy(c.cheb_D.begin(), c.cheb_D.begin() + 4 * nn, fdm.begin());
         const double* D1 = c.cheb_D.data() + nn;
         for (int i = 0; i < nr; ++i)
             for (int j = 0; j < nr; ++j) {
-                long double s = 0.0L;
-                for (int k = 0; k < nr; ++k) s += (long double)D1[(size_t)i * nr + k] * D1[(size_t)k * nr + j];
-                fdm[4 * nn + (size_t)i * nr + j] = (double)s;
+                long double sum = 0.0L;
+                for (int k = 0; k < nr; ++k) sum += (long double)D1[(size_t)i * nr + k] * D1[(size_t)k * nr + j];
+                fdm[4 * nn + (size_t)i * nr + j] = (double)sum;
             }
-        dalloc(c.d_Dfd, fdm.size());
-        RA_CUDA(cudaMemcpyAsync(c.d_Dfd, fdm.data(), fdm.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        std::vector<int> lo(5 * (size_t)nr), hi(5 * (size_t)nr);
+        int w = 1;
+        for (size_t row = 0; row < 5 * (size_t)nr; ++row) {
+            const double* m = fdm.data() + row * nr;
+            int a = 0, b = -1;
+            for (int j = 0; j < nr; ++j)
+                if (m[j] != 0.0) {
+                    if (b < 0) a = j;
+                    b = j;
+                }
+            if (b < 0) a = b = 0;
+            lo[row] = a;
+            hi[row] = b;
+            w = std::max(w, b - a + 1);
+        }
+        if (w > 16) throw ArgError("finite differences: a stencil wider than 16 points");
+        c.fd_w = w;
+        std::vector<double> band(5 * (size_t)nr * (w + 1), 0.0);
+        for (size_t row = 0; row < 5 * (size_t)nr; ++row) {
+            const int first = std::min(lo[row], nr - w);
+            double* o = band.data() + row * (w + 1);
+            o[0] = first;
+            for (int j = lo[row]; j <= hi[row]; ++j) o[1 + j - first] = fdm[row * nr + j];
+        }
+        dalloc(c.d_Dfd, band.size());
+        RA_CUDA(cudaMemcpyAsync(c.d_Dfd, band.data(), band.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));
         RA_CUDA(cudaStreamSynchronize(c.stream));
     }
     RA_CUDA(cudaMemcpyAsync(c.d_radial, rp.data(), rp.size() * sizeof(double), cudaMemcpyHostToDevice, c.stream));

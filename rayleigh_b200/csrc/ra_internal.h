@@ -169,7 +169,8 @@ struct Ctx {
     double *d_Ptab = nullptr, *d_iPtab = nullptr;     // [row][nth2]
     double *d_D = nullptr;                            // [4][nr][nr]
     double *d_Dpar = nullptr;                         // [4][2][nr/2][(kc+1)/2] parity planes of D, r < nr/2
-    double *d_Dfd = nullptr;                          // finite differences: [5][nr][nr] I, D1, D2, D3, D1 D1
+    double *d_Dfd = nullptr;                          // finite differences: I, D1, D2, D3, D1 D1 in bands:
+    int fd_w = 0;                                     //   [5][nr][1 + fd_w] = first column, fd_w coefficients
     double *d_coef = nullptr;                         // [L][NSLOT][nr]
     double *d_radial = nullptr;                       // packed radial profiles (see kRadial*)
     double *d_costh = nullptr;                        // [nth] cos, then sin, csc, cot

@@ -269,6 +269,8 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_DV_THETA_DR   11
 #define RA_Q_DV_PHI_DR     12
 #define RA_Q_DV_R_DT       19
+#define RA_Q_DV_THETA_DT   20   /* formed as Compute_dvtheta_by_dtheta, Compute_dvphi_by_dtheta do */
+#define RA_Q_DV_PHI_DT     21
 #define RA_Q_DV_R_DP       28
 #define RA_Q_DV_THETA_DP   29
 #define RA_Q_DV_PHI_DP     30
@@ -304,6 +306,10 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_DVM_PHI_DR    18
 #define RA_Q_DVP_R_DT      22
 #define RA_Q_DVM_R_DT      25
+#define RA_Q_DVP_THETA_DT  23
+#define RA_Q_DVP_PHI_DT    24
+#define RA_Q_DVM_THETA_DT  26
+#define RA_Q_DVM_PHI_DT    27
 #define RA_Q_DVP_R_DP      31
 #define RA_Q_DVP_THETA_DP  32
 #define RA_Q_DVP_PHI_DP    33

@@ -505,7 +505,8 @@ class Rayleigh:
                   # fluctuating (m > 0) and azimuthal-mean (m = 0) parts, the reference's codes
                   "vp_r": 4, "vp_theta": 5, "vp_phi": 6, "vm_r": 7, "vm_theta": 8, "vm_phi": 9,
                   "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
-                  "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
+                  "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dv_theta_dt": 20, "dv_phi_dt": 21,
+                  "dvp_theta_dt": 23, "dvp_phi_dt": 24, "dvm_theta_dt": 26, "dvm_phi_dt": 27, "dvp_r_dp": 31, "dvp_theta_dp": 32,
                   "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36, "vortp_r": 304,
                   "vortm_r": 307, "vort_theta": 302, "vort_phi": 303, "vortp_theta": 305, "vortp_phi": 306,
                   "vortm_theta": 308, "vortm_phi": 309, "entropy_p": 503, "pressure_p": 504,

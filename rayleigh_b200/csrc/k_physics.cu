@@ -1574,8 +1574,11 @@ __device__ __forceinline__ int natural_index(int p) {
 // One buffer-field sum C (DiagCombo) on the row into e[.]: a c2r per term.
 template <int N, int ZPT>
 __device__ __forceinline__ void row_combo(const PhysParams& P, const DiagCombo& C, const double* rowbase, int h,
-                                          double csc, double orad, double2* sm, int t, double2 (&y)[FB][ZPT],
+                                          int th, int r, double2* sm, int t, double2 (&y)[FB][ZPT],
                                           double2 (&e)[ZPT]) {
+    const double csc = P.trig[2 * N + th], cot = P.trig[3 * N + th];
+    const double rad = P.radial[R_RADIUS * P.nr + r], orad = P.radial[R_OVER_R * P.nr + r];
+    const double rdl = rad * P.radial[R_DLNRHO * P.nr + r] + 2.0;
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) e[q] = make_double2(0.0, 0.0);
 #pragma unroll 1
@@ -1584,7 +1587,9 @@ __device__ __forceinline__ void row_combo(const PhysParams& P, const DiagCombo& 
         const int fo[1] = {T.field};
         const bool dp[1] = {T.dphi != 0};
         row_c2r<N, 1, ZPT>(P, rowbase, h, fo, dp, sm, t, y, C.mpart);
-        const double cs = T.c * (T.csc ? csc : 1.0) * (T.orad ? orad : 1.0);
+        const double tf = T.th == 1 ? csc : (T.th == 2 ? cot : (T.th == 3 ? csc * cot : (T.th == 4 ? csc * csc : 1.0)));
+        const double rf = T.rad == 1 ? orad : (T.rad == 2 ? rad : (T.rad == 3 ? rdl : 1.0));
+        const double cs = T.c * tf * rf;
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {
             e[q].x += cs * y[0][q].x;
@@ -1614,7 +1619,7 @@ __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceS
     for (int q = 0; q < ZPT; ++q) acc[q] = make_double2(0.0, 0.0);
 #pragma unroll 1
     for (int i = 0; i < S.nprod; ++i) {
-        row_combo<N, ZPT>(P, S.a[i], rowbase, h, csc, orad, sm, t, y, a);
+        row_combo<N, ZPT>(P, S.a[i], rowbase, h, th, r, sm, t, y, a);
         if (S.bsame[i]) {
 #pragma unroll
             for (int q = 0; q < ZPT; ++q) b[q] = a[q];
@@ -1622,7 +1627,7 @@ __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceS
 #pragma unroll
             for (int q = 0; q < ZPT; ++q) b[q] = make_double2(1.0, 1.0);
         } else {
-            row_combo<N, ZPT>(P, S.b[i], rowbase, h, csc, orad, sm, t, y, b);
+            row_combo<N, ZPT>(P, S.b[i], rowbase, h, th, r, sm, t, y, b);
         }
 #pragma unroll
         for (int q = 0; q < ZPT; ++q) {

@@ -2021,17 +2021,25 @@ static const QuantityParts kParts[] = {
     {301, 304, 307},    {501, 503, 505},    {502, 504, 506},    {507, 509, 511},    {508, 510, 512},
     {513, 515, 517},    {519, 521, 523},    {520, 522, 524},    {801, 804, 807},    {802, 805, 808},
     {803, 806, 809},    {1001, 1002, 1003}, {1004, 1005, 1006}, {1007, 1008, 1009}, {828, 831, 834},
-    {829, 832, 835},    {830, 833, 836},    {302, 305, 308},    {303, 306, 309},
+    {829, 832, 835},    {830, 833, 836},    {302, 305, 308},    {303, 306, 309},    {20, 23, 26},
+    {21, 24, 27},
 };
 
 // Sums of fields (Diagnostics_Vorticity_Field.F90 Compute_Vorticity_Field): vort_theta (302)
 // = (csc dv_r/dphi - v_phi) / r - dv_phi/dr, vort_phi (303) = dv_theta/dr + (v_theta -
 // dv_r/dtheta) / r, from the buffer fields as the other codes form them (v_theta, v_phi and
-// their r and theta derivatives divided by sin(theta)).
-struct LinearSource { int code; DiagTerm t[3]; };
+// their r and theta derivatives divided by sin(theta)); dv_theta/dtheta (20) and
+// dv_phi/dtheta (21) as the physical-space stage forms them (Compute_dvtheta_by_dtheta,
+// Compute_dvphi_by_dtheta, Sphere_Physical_Space.F90:226-248): -v_r (r dlnrho + 2) - r
+// dv_r/dr - v_theta cot - csc dv_phi/dphi and r omega_r + csc dv_theta/dphi - v_phi cot.
+// DiagTerm: field, d/dphi, theta factor (1 csc, 2 cot, 3 csc cot, 4 csc^2), radial factor
+// (1 1/r, 2 r, 3 r dlnrho + 2), coefficient.
+struct LinearSource { int code, nt; DiagTerm t[4]; };
 static const LinearSource kLinear[] = {
-    {302, {{A_VR, 1, 1, 1, 1.0}, {A_VP, 0, 1, 1, -1.0}, {A_DVPDR, 0, 1, 0, -1.0}}},
-    {303, {{A_DVTDR, 0, 1, 0, 1.0}, {A_VT, 0, 1, 1, 1.0}, {A_DVRDT, 0, 1, 1, -1.0}}},
+    {302, 3, {{A_VR, 1, 1, 1, 1.0}, {A_VP, 0, 1, 1, -1.0}, {A_DVPDR, 0, 1, 0, -1.0}}},
+    {303, 3, {{A_DVTDR, 0, 1, 0, 1.0}, {A_VT, 0, 1, 1, 1.0}, {A_DVRDT, 0, 1, 1, -1.0}}},
+    {20, 4, {{A_VR, 0, 0, 3, -1.0}, {A_DVRDR, 0, 0, 2, -1.0}, {A_VT, 0, 3, 0, -1.0}, {A_VP, 1, 4, 0, -1.0}}},
+    {21, 3, {{A_OMR, 0, 0, 2, 1.0}, {A_VT, 1, 4, 0, 1.0}, {A_VP, 0, 3, 0, -1.0}}},
 };
 
 // The buffer-field sum of quantity `code` (a row of kQuantities or kLinear), of its part mpart.
@@ -2040,8 +2048,8 @@ static DiagCombo combo_of(const Ctx& c, int code, int mpart, int asked) {
     C.mpart = mpart;
     for (const LinearSource& k : kLinear)
         if (k.code == code) {
-            C.nt = 3;
-            for (int i = 0; i < 3; ++i) C.t[i] = k.t[i];
+            C.nt = k.nt;
+            for (int i = 0; i < k.nt; ++i) C.t[i] = k.t[i];
             return C;
         }
     for (const QuantitySource& k : kQuantities)

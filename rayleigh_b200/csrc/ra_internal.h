@@ -255,10 +255,11 @@ void launch_physics(Ctx& c);
 void launch_kinetic_energy(Ctx& c, bool magnetic = false);
 // one diagnostic quantity on the phi grid at up to MAXL radial levels
 // A diagnostic quantity's buffer-field sum: sum over j < nt of c x field (d/dphi where dphi,
-// times 1/sin(theta) where csc, 1/r where orad), of the part mpart (0 the field, 1 its
+// times the theta factor th: 0 none, 1 csc, 2 cot, 3 csc cot, 4 csc^2, and the radial factor
+// rad: 0 none, 1 1/r, 2 r, 3 r dlnrho + 2), of the part mpart (0 the field, 1 its
 // fluctuations, m > 0, 2 its azimuthal mean, m = 0); nt = 0: the constant 1.
-struct DiagTerm { int field, dphi, csc, orad; double c; };
-struct DiagCombo { int nt, mpart; DiagTerm t[3]; };
+struct DiagTerm { int field, dphi, th, rad; double c; };
+struct DiagCombo { int nt, mpart; DiagTerm t[4]; };
 
 struct SliceSpec {
     static constexpr int MAXL = 64;

@@ -114,7 +114,8 @@ def test_diagnostic_quantity_codes_are_the_references():
                  "j_r": 800 + 200 + 1, "j_theta": 800 + 200 + 4, "j_phi": 800 + 200 + 7,
                  "vp_r": 4, "vp_theta": 5, "vp_phi": 6, "vm_r": 7, "vm_theta": 8, "vm_phi": 9,
                  "dvp_r_dr": 13, "dvp_theta_dr": 14, "dvp_phi_dr": 15, "dvm_r_dr": 16, "dvm_theta_dr": 17,
-                 "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dvp_r_dp": 31, "dvp_theta_dp": 32,
+                 "dvm_phi_dr": 18, "dvp_r_dt": 22, "dvm_r_dt": 25, "dv_theta_dt": 20, "dv_phi_dt": 21,
+                 "dvp_theta_dt": 23, "dvp_phi_dt": 24, "dvm_theta_dt": 26, "dvm_phi_dt": 27, "dvp_r_dp": 31, "dvp_theta_dp": 32,
                  "dvp_phi_dp": 33, "dvm_r_dp": 34, "dvm_theta_dp": 35, "dvm_phi_dp": 36,
                  "vortp_r": 300 + 4, "vortm_r": 300 + 7, "vort_theta": 300 + 2, "vort_phi": 300 + 3,
                  "vortp_theta": 300 + 5, "vortp_phi": 300 + 6, "vortm_theta": 300 + 8, "vortm_phi": 300 + 9,

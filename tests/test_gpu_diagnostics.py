@@ -74,7 +74,18 @@ _ORACLE_NAME = {"v_r": "vr", "v_theta": "vt", "v_phi": "vp", "dv_r_dr": "dvrdr",
                 "dv_phi_dr": "dvpdr", "dv_r_dt": "dvrdt", "dv_r_dp": "dvrdp", "dv_theta_dp": "dvtdp", "vort_r": "omr",
                 "dv_phi_dp": "dvpdp", "entropy": "t", "entropy_dr": "dtdr", "entropy_dtheta": "dtdt",
                 "entropy_dphi": "dtdp", "pressure": "p", "pressure_dphi": "dpdp", "pressure_dr": "dpdr",
-                "vort_theta": "omt", "vort_phi": "omp"}
+                "vort_theta": "omt", "vort_phi": "omp", "dv_theta_dt": "dvtdt", "dv_phi_dt": "dvpdt"}
+
+
+# dv_theta/dtheta and dv_phi/dtheta are formed with csc^2 terms (csc dv_phi/dphi, csc
+# dv_theta/dphi; up to 400 at N_theta = 48), which amplify the split products' error near the
+# poles beyond the other quantities' (measured in the mixed form: 2.2e-9 relative L2 over shell
+# slices, 1.2e-8 pointwise in the meridional slices); their mixed bounds are 4 times the others'.
+_CSC2 = {"dv_theta_dt", "dv_phi_dt", "dvp_theta_dt", "dvp_phi_dt", "dvm_theta_dt", "dvm_phi_dt"}
+
+
+def _amp(name, tol):
+    return 4.0 if (name in _CSC2 and tol >= 1e-10) else 1.0   # the mixed form's bounds only
 
 
 def _oracle_step(o):
@@ -87,10 +98,16 @@ def _oracle_step(o):
 
 
 def _add_vorticity(o):
+    """The theta and phi vorticity (Compute_Vorticity_Field) and dv_theta/dtheta, dv_phi/dtheta
+    as the physical-space stage forms them (Compute_dvtheta_by_dtheta, Compute_dvphi_by_dtheta)
+    from the oracle's buffer."""
     f = o.last_fields
-    csc, orad = o.h.csctheta[:, None, None], (1.0 / o.radius)[None, :, None]
-    f["omt"] = (csc * f["dvrdp"] - f["vp"]) * orad - f["dvpdr"]
-    f["omp"] = f["dvtdr"] + (f["vt"] - f["dvrdt"]) * orad
+    csc, cot = o.h.csctheta[:, None, None], o.h.cottheta[:, None, None]
+    r = o.radius[None, :, None]
+    f["omt"] = (csc * f["dvrdp"] - f["vp"]) / r - f["dvpdr"]
+    f["omp"] = f["dvtdr"] + (f["vt"] - f["dvrdt"]) / r
+    f["dvtdt"] = -f["vr"] * (r * o.dlnrho[None, :, None] + 2.0) - r * f["dvrdr"] - f["vt"] * cot - f["dvpdp"] * csc
+    f["dvpdt"] = r * f["omr"] + f["dvtdp"] * csc - f["vp"] * cot
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -122,7 +139,7 @@ def test_shell_slices_match_the_oracle(precision, tol):
         ref = o.last_fields[_ORACLE_NAME[name]][:, levels, :].transpose(1, 0, 2)   # [level, theta, phi]
         err = np.linalg.norm(sl[i] - ref) / np.linalg.norm(ref)
         print(precision, name, err)
-        assert err < tol, (name, err)
+        assert err < tol * _amp(name, tol), (name, err)
     assert np.array_equal(again[0, 0], sl[0, 5])
 
 
@@ -154,7 +171,7 @@ def test_shell_averages_match_the_oracle(precision, tol):
         for m in range(4):
             err = np.abs(av[i, m] - ref[i, m]).max() / S ** (m + 1)
             print(precision, name, m, err)
-            assert err < tol, (name, m, err)
+            assert err < tol * _amp(name, tol), (name, m, err)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -179,7 +196,7 @@ def test_azimuthal_averages_match_the_oracle(precision, tol):
         ref = q.mean(axis=2)
         err = np.abs(az[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
-        assert err < tol, (name, err)
+        assert err < tol * _amp(name, tol), (name, err)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -209,7 +226,7 @@ def test_shell_spectra_match_the_oracle(precision, tol):
         assert scale > 0
         err = np.abs(sp[i] - ref[i]).max() / scale
         print(precision, name, err)
-        assert err < tol, (name, err)
+        assert err < tol * _amp(name, tol), (name, err)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-9)])
@@ -235,7 +252,7 @@ def test_equatorial_slices_match_the_oracle(precision, tol):
         ref = 0.5 * (q[nth // 2 - 1] + q[nth // 2])
         err = np.abs(eq[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
-        assert err < tol, (name, err)
+        assert err < tol * _amp(name, tol), (name, err)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-8)])
@@ -266,7 +283,7 @@ def test_meridional_slices_match_the_oracle(precision, tol):
         ref = q[:, :, phis].transpose(2, 0, 1)           # [j, theta, r]
         err = np.abs(me[i] - ref).max() / np.abs(q).max()
         print(precision, name, err)
-        assert err < tol, (name, err)
+        assert err < tol * _amp(name, tol), (name, err)
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-8)])
@@ -301,7 +318,7 @@ def test_global_averages_and_point_probes_match_the_oracle(precision, tol):
         ref = q[np.ix_(ti, ri, pi)].transpose(1, 0, 2)  # [r, theta, phi]
         e_pp = np.abs(pp[i] - ref).max() / scale
         print(precision, name, e_ga, e_pp)
-        assert e_ga < tol and e_pp < tol, (name, e_ga, e_pp)
+        assert e_ga < tol * _amp(name, tol) and e_pp < tol * _amp(name, tol), (name, e_ga, e_pp)
 
 
 # the oracle's physical-space buffer names of the magnetic quantities (after rsintheta_div)
@@ -374,6 +391,7 @@ _PARTS = {"v_r": ("vp_r", "vm_r"), "v_theta": ("vp_theta", "vm_theta"), "v_phi":
           "dv_r_dp": ("dvp_r_dp", "dvm_r_dp"), "dv_theta_dp": ("dvp_theta_dp", "dvm_theta_dp"),
           "dv_phi_dp": ("dvp_phi_dp", "dvm_phi_dp"), "vort_r": ("vortp_r", "vortm_r"),
           "vort_theta": ("vortp_theta", "vortm_theta"), "vort_phi": ("vortp_phi", "vortm_phi"),
+          "dv_theta_dt": ("dvp_theta_dt", "dvm_theta_dt"), "dv_phi_dt": ("dvp_phi_dt", "dvm_phi_dt"),
           "entropy": ("entropy_p", "entropy_m"), "pressure": ("pressure_p", "pressure_m"),
           "entropy_dr": ("entropy_p_dr", "entropy_m_dr"), "pressure_dr": ("pressure_p_dr", "pressure_m_dr"),
           "entropy_dtheta": ("entropy_p_dtheta", "entropy_m_dtheta"),
@@ -432,7 +450,7 @@ def _check_parts(g, o, names, parts, tol, ptol):
                 "global": abs(ga[i] - float(np.dot(w, ref_av[i, 0]))) / S,
                 "probe": np.abs(pp[i] - part[np.ix_(ti, ri, pi)].transpose(1, 0, 2)).max() / S}
         print(name, {k: f"{v:.1e}" for k, v in errs.items()})
-        bound = {k: (ptol if k in ("slice", "meridional", "probe") else tol) for k in errs}
+        bound = {k: (ptol if k in ("slice", "meridional", "probe") else tol) * _amp(name, tol) for k in errs}
         assert all(errs[k] < bound[k] for k in errs), (name, errs)
 
 
@@ -456,7 +474,7 @@ def test_fluctuating_and_mean_parts_match_the_oracle(precision, tol, ptol):
         _oracle_step(o)
         parts = _part_fields(o, _ORACLE_NAME)
         names = [n for n in parts if n not in _ZERO_MEANS]
-        assert len(names) == 35 and all(n in rb.Rayleigh.QUANTITIES for n in parts)
+        assert len(names) == 39 and all(n in rb.Rayleigh.QUANTITIES for n in parts)
         _check_parts(g, o, names, parts, tol, ptol)
         zeros = sorted(_ZERO_MEANS)
         assert not g.shell_slices(zeros, [0, 7]).any() and not g.point_probes(zeros, [3], [5], [9]).any()

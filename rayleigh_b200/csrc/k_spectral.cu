@@ -745,15 +745,43 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) emf_radial_kernel(const doubl
     });
 }
 
+// The same in the finite-difference mode, where the grid operator is D_1 (Finalize_EMF's FD
+// branch): its band (operator 1 of the synthesis bands) per point, one thread per point with
+// r fastest, and the same epilogue.
+__global__ void __launch_bounds__(256) emf_band_kernel(const double* __restrict__ band, int w,
+                                                       const double* __restrict__ xemf, double* __restrict__ ab_a,
+                                                       double* __restrict__ rhs_a, int nr, long ncols,
+                                                       double new_ab) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (column, r), r fastest
+    if (i >= ncols * nr) return;
+    const long col = i / nr;
+    const int rr = (int)(i - col * nr);
+    const double* row = band + ((long)nr + rr) * (w + 1);
+    const int first = (int)__ldg(row);   // first + w <= nr
+    const double* x = xemf + col * nr + first;
+    double v = 0.0;
+    for (int j = 0; j < w; ++j) v += __ldg(row + 1 + j) * __ldg(x + j);
+    const double na = ab_a[i] + v;
+    ab_a[i] = na;
+    rhs_a[i] = (rr == 0 || rr == nr - 1) ? 0.0 : rhs_a[i] + new_ab * na;
+}
+
 void launch_rlm_b_mag(Ctx& c, double new_ab) {
     const long total = c.d.nlm * c.d.nr;
     rlm_b_mag_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(
         c.d_s2b, c.d_ab, c.d_rhs_c, c.d_xemf, c.d.nlm, c.d.nr, c.d.L, new_ab, c.nfb, c.d_status);
     RA_CUDA(cudaGetLastError());
     const long ncols = 2 * c.d.nlm;
-    dim3 grid((unsigned)((ncols + Sq::BN - 1) / Sq::BN), (unsigned)((c.d.nr + Sq::BM - 1) / Sq::BM));
-    emf_radial_kernel<<<grid, GEMM_THREADS, 0, c.stream>>>(c.d_Memf, c.d_xemf, c.d_ab + 5 * c.d.nlm * 2 * c.d.nr,
-                                                         c.d_rhs_a, c.d.nr, ncols, new_ab);
+    double* ab_a = c.d_ab + 5 * c.d.nlm * 2 * c.d.nr;
+    if (c.cfg.chebyshev) {
+        dim3 grid((unsigned)((ncols + Sq::BN - 1) / Sq::BN), (unsigned)((c.d.nr + Sq::BM - 1) / Sq::BM));
+        emf_radial_kernel<<<grid, GEMM_THREADS, 0, c.stream>>>(c.d_Memf, c.d_xemf, ab_a, c.d_rhs_a, c.d.nr, ncols,
+                                                             new_ab);
+    } else {
+        const long total = ncols * c.d.nr;
+        emf_band_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.d_Dfd, c.fd_w, c.d_xemf, ab_a,
+                                                                             c.d_rhs_a, c.d.nr, ncols, new_ab);
+    }
     RA_CUDA(cudaGetLastError());
     c.launches += 2;
 }

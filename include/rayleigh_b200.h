@@ -385,6 +385,16 @@ int ra_magnetic_energy(ra_ctx* ctx, double* me);
 #define RA_Q_KIN_HELICITY_MP        342
 #define RA_Q_KIN_HELICITY_PM        343
 #define RA_Q_JPM_SQ                1013
+/* mass_flux_codes.F: rho v and its fluctuating and mean parts: */
+#define RA_Q_RHOV_R                 201
+#define RA_Q_RHOV_THETA             202
+#define RA_Q_RHOV_PHI               203
+#define RA_Q_RHOVP_R                204
+#define RA_Q_RHOVP_THETA            205
+#define RA_Q_RHOVP_PHI              206
+#define RA_Q_RHOVM_R                207
+#define RA_Q_RHOVM_THETA            208
+#define RA_Q_RHOVM_PHI              209
 /* thermal_energy_codes.F: rho T S of the reference state, its parts and their squares: */
 #define RA_Q_THERMAL_ENERGY_FULL    701
 #define RA_Q_THERMAL_ENERGY_P       702

@@ -518,6 +518,8 @@ class Rayleigh:
                   "jm_theta": 1006, "jp_phi": 1008, "jm_phi": 1009, "db_r_dp": 828, "db_theta_dp": 829,
                   "db_phi_dp": 830, "dbp_r_dp": 831, "dbp_theta_dp": 832, "dbp_phi_dp": 833, "dbm_r_dp": 834,
                   "dbm_theta_dp": 835, "dbm_phi_dp": 836,
+                  "rhov_r": 201, "rhov_theta": 202, "rhov_phi": 203, "rhovp_r": 204, "rhovp_theta": 205,
+                  "rhovp_phi": 206, "rhovm_r": 207, "rhovm_theta": 208, "rhovm_phi": 209,
                   "thermal_energy_full": 701, "thermal_energy_p": 702, "thermal_energy_m": 703,
                   "thermal_energy_sq": 707, "thermal_energyp_sq": 708, "thermal_energym_sq": 709,
                   # products: enstrophy, squared vorticity, kinetic helicity, mean J . J'

@@ -1601,8 +1601,8 @@ __device__ __forceinline__ void row_combo(const PhysParams& P, const DiagCombo& 
 // The diagnostic quantity S on the row (theta index th, radial index r) into y[0][.]: one
 // field through the c2r (d/dphi in the spectrum, its fluctuating or mean part by mpart), or
 // a sum of products of buffer-field sums (the vorticity components, the energy densities,
-// enstrophy, helicity, J.J: SliceSpec.nprod), times 1, rho(r) / 2, a constant, rho(r) T(r) or
-// its square.  Returns the
+// enstrophy, helicity, J.J: SliceSpec.nprod), times 1, rho(r) / 2, a constant, rho(r) T(r),
+// its square or rho(r).  Returns the
 // factor the caller still applies: the single field's 1/sin(theta) and 1/r, 1 for a product.
 template <int N, int ZPT>
 __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceSpec& S, const double* rowbase,
@@ -1636,8 +1636,10 @@ __device__ __forceinline__ double row_quantity(const PhysParams& P, const SliceS
         }
     }
     const double rt = P.radial[R_RHO_T * P.nr + r];
-    const double c = S.coef == 1 ? 0.5 * P.radial[R_DENSITY * P.nr + r]
-                                 : (S.coef == 2 ? S.cval : (S.coef == 3 ? rt : (S.coef == 4 ? rt * rt : 1.0)));
+    const double rho = P.radial[R_DENSITY * P.nr + r];
+    const double c = S.coef == 1 ? 0.5 * rho
+                                 : (S.coef == 2 ? S.cval
+                                                : (S.coef == 3 ? rt : (S.coef == 4 ? rt * rt : (S.coef == 5 ? rho : 1.0))));
 #pragma unroll
     for (int q = 0; q < ZPT; ++q) y[0][q] = make_double2(acc[q].x * c, acc[q].y * c);
     return 1.0;

@@ -2078,6 +2078,8 @@ static DiagCombo combo_of(const Ctx& c, int code, int mpart, int asked) {
 //     (v, omega) parts (fluct, fluct) 327-329, (mean, mean) 330-332, (mean, fluct) 333-335,
 //     (fluct, mean) 336-338; v.omega 339 and the same four part pairs 340-343
 //     (Diagnostics_Vorticity_Field.F90).
+//   mass_flux_codes.F (rhovoffset = 200): rho v_r, rho v_theta, rho v_phi 201-203, of the
+//     fluctuations 204-206, of the means 207-209 (Diagnostics_Velocity_Field.F90);
 //   thermal_energy_codes.F (teoffset = 700): rho T S of the reference state and its
 //     fluctuating and mean parts 701-703, their squares 707-709 (Diagnostics_Thermal_Energies.F90
 //     Compute_Thermal_Energy); b = nullptr: the constant 1.
@@ -2086,6 +2088,12 @@ static const int kVelocity[3] = {1, 2, 3}, kVorticity[3] = {301, 302, 303}, kBfi
                  kCurrent[3] = {1001, 1004, 1007}, kEntropy[1] = {501};
 static bool product_of(int code, Product& p) {
     static const int kGroupPart[3] = {0, 2, 1};   // field, mean, fluctuations
+    if (code >= 201 && code <= 209) {
+        static const int part[3] = {0, 1, 2};
+        const int k = code - 201;
+        p = Product{kVelocity, part[k / 3], nullptr, 0, k % 3 + 1, 5, false};
+        return true;
+    }
     if ((code >= 701 && code <= 703) || (code >= 707 && code <= 709)) {
         const bool sq = code >= 707;
         const int part = sq ? code - 707 : code - 701;   // 0 field, 1 fluctuations, 2 mean

@@ -269,7 +269,7 @@ struct SliceSpec {
     int mpart;                  // 0 the field, 1 its fluctuating part (m > 0), 2 its azimuthal mean
     // nprod > 0: coef x sum over i < nprod of a[i] b[i] (b[i] = a[i] where bsame[i], the
     // constant 1 where b[i].nt = 0), coef 0: one, 1: rho(r) / 2, 2: cval, 3: rho(r) T(r),
-    // 4: (rho(r) T(r))^2 (field, dphi, csc, orad and mpart then unused)
+    // 4: (rho(r) T(r))^2, 5: rho(r) (field, dphi, csc, orad and mpart then unused)
     int nprod, bsame[3], coef;
     double cval;
     DiagCombo a[3], b[3];

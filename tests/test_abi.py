@@ -146,6 +146,10 @@ def test_diagnostic_quantity_codes_are_the_references():
                       "phi_me": 1100 + 4, "mmagnetic_energy": 1100 + 5, "radial_mme": 1100 + 6,
                       "theta_mme": 1100 + 7, "phi_mme": 1100 + 8, "pmagnetic_energy": 1100 + 9,
                       "radial_pme": 1100 + 10, "theta_pme": 1100 + 11, "phi_pme": 1100 + 12})
+    # mass_flux_codes.F: rhovoffset = voffset + 200
+    reference.update({"rhov_r": 200 + 1, "rhov_theta": 200 + 2, "rhov_phi": 200 + 3, "rhovp_r": 200 + 4,
+                      "rhovp_theta": 200 + 5, "rhovp_phi": 200 + 6, "rhovm_r": 200 + 7, "rhovm_theta": 200 + 8,
+                      "rhovm_phi": 200 + 9})
     # thermal_energy_codes.F: teoffset = pt_off + 200
     reference.update({"thermal_energy_full": 700 + 1, "thermal_energy_p": 700 + 2, "thermal_energy_m": 700 + 3,
                       "thermal_energy_sq": 700 + 7, "thermal_energyp_sq": 700 + 8, "thermal_energym_sq": 700 + 9})

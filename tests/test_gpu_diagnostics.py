@@ -528,6 +528,11 @@ def _square_fields(o, kind):
             put(f"vortm_{c}_sq", w["mean"][i] ** 2, f"vort_{c}_sq")
         pairs = {"": ("full", "full"), "_pp": ("fluct", "fluct"), "_mm": ("mean", "mean"),
                  "_mp": ("mean", "fluct"), "_pm": ("fluct", "mean")}
+        rho = o.density[None, :, None]   # mass_flux_codes.F: rho v and its parts
+        for i, c in enumerate(("r", "theta", "phi")):
+            put(f"rhov_{c}", rho * v["full"][i], f"rhov_{c}")
+            put(f"rhovp_{c}", rho * v["fluct"][i], f"rhov_{c}")
+            put(f"rhovm_{c}", rho * v["mean"][i], f"rhov_{c}")
         rt = (o.density * o.temperature)[None, :, None]   # Compute_Thermal_Energy: rho T S
         S = o.last_fields["t"]
         Sm = np.broadcast_to(S.mean(axis=2, keepdims=True), S.shape)
@@ -551,8 +556,8 @@ def _square_fields(o, kind):
 def test_energy_densities_match_the_oracle(precision, tol, ptol):
     """The products in every output family (kinetic_energy_codes.F 401-424 on the anelastic
     polytrope, where rho varies with radius, with the enstrophy, squared vorticity and kinetic
-    helicity codes 310-322, 324-343 of vorticity_field_codes.F and the thermal energy rho T S
-    701-703, 707-709 of thermal_energy_codes.F; with magnetism
+    helicity codes 310-322, 324-343 of vorticity_field_codes.F, the mass flux rho v 201-209 and the
+    thermal energy rho T S 701-703, 707-709; with magnetism
     magnetic_energy_codes.F 1101-1112 and the J.J codes 1010-1022) against the oracle's buffer,
     on the largest magnitude of the full (not the mean or fluctuating) product."""
     import rayleigh_b200 as rb
@@ -579,7 +584,7 @@ def test_energy_densities_match_the_oracle(precision, tol, ptol):
             o.step()
             _add_vorticity(o)
             sq = _square_fields(o, kind)
-            assert len(sq) == (63 if kind == "hydro" else 25) and all(n in rb.Rayleigh.QUANTITIES for n in sq)
+            assert len(sq) == (72 if kind == "hydro" else 25) and all(n in rb.Rayleigh.QUANTITIES for n in sq)
             _check_parts(g, o, list(sq), sq, tol, ptol)
             if kind == "hydro":
                 with pytest.raises(rb.RayleighError) as ei:
